@@ -1,0 +1,193 @@
+"""goferro_b200 — Python host layer over the B200 engine's C ABI.
+
+The engine itself is ``libgoferro_b200.so`` (built in-tree from ``csrc/`` by
+``build.py``); this module binds the entry points declared in
+``include/goferro_b200.h`` with ctypes and mirrors the reference's run flow:
+a deck directory in, RK4 steps, averages / fields / probes out.
+
+There is no CPU path: if the library is missing or no sm_100 device is
+present, ``Engine`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import decks  # noqa: F401  (re-exported)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgoferro_b200.so")
+
+GF_OK = 0
+ERRORS = {-1: "GF_EINVAL", -2: "GF_EIO", -3: "GF_ECUDA", -4: "GF_ENOMEM", -5: "GF_ENAN",
+          -6: "GF_ENODEV", -7: "GF_EUNSUPPORTED"}
+
+FIELD = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "q": 4, "u": 5, "v": 6,
+         "Ex": 7, "Ey": 8, "Ez": 9, "Hx": 10, "Hy": 11, "Hz": 12,
+         "Hstat": 13, "Estat": 14, "E_cell": 15, "H_cell": 16, "strain": 17}
+OBS = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "u": 4}
+
+# every symbol include/goferro_b200.h declares
+EXPORTS = ["gf_create_from_deck", "gf_advance", "gf_advance_eager", "gf_average", "gf_probe_em",
+           "gf_field_dims", "gf_download", "gf_upload", "gf_download_device", "gf_upload_device",
+           "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
+           "gf_destroy", "gf_version"]
+
+
+class GFInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+                ("dt", ctypes.c_double), ("time", ctypes.c_double),
+                ("step", ctypes.c_uint64), ("deck_steps", ctypes.c_uint64),
+                ("n_materials", ctypes.c_int32),
+                ("fm", ctypes.c_int32), ("afm", ctypes.c_int32), ("fe", ctypes.c_int32),
+                ("elastic", ctypes.c_int32), ("em", ctypes.c_int32), ("demag_per_stage", ctypes.c_int32),
+                ("n_fm", ctypes.c_uint64), ("n_afm", ctypes.c_uint64), ("n_fe", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64),
+                ("launches_per_step", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
+
+
+class GFKernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 40), ("launches", ctypes.c_int32), ("total_ms", ctypes.c_double)]
+
+
+class GFError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: Optional[str] = None) -> ctypes.CDLL:
+    """Load the engine library (once) and declare the C signatures."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"engine library not built: {p} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(p)
+    vp, c_int, c_u64, c_dbl_p = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)
+    lib.gf_create_from_deck.argtypes = [ctypes.c_char_p, c_int, ctypes.POINTER(vp)]
+    lib.gf_advance.argtypes = [vp, c_u64]
+    lib.gf_advance_eager.argtypes = [vp, c_u64]
+    lib.gf_average.argtypes = [vp, c_int, c_dbl_p]
+    lib.gf_probe_em.argtypes = [vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_dbl_p, c_dbl_p]
+    lib.gf_field_dims.argtypes = [vp, c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_size_t)]
+    lib.gf_download.argtypes = [vp, c_int, c_dbl_p, ctypes.c_size_t]
+    lib.gf_upload.argtypes = [vp, c_int, c_dbl_p, ctypes.c_size_t]
+    lib.gf_download_device.argtypes = [vp, c_int, vp, ctypes.c_size_t]
+    lib.gf_upload_device.argtypes = [vp, c_int, vp, ctypes.c_size_t]
+    lib.gf_get_info.argtypes = [vp, ctypes.POINTER(GFInfo)]
+    lib.gf_profile_steps.argtypes = [vp, c_u64, ctypes.POINTER(GFKernelTime), c_int, ctypes.POINTER(c_int)]
+    lib.gf_synchronize.argtypes = [vp]
+    lib.gf_stream.argtypes = [vp]
+    lib.gf_stream.restype = vp
+    lib.gf_check_finite.argtypes = [vp]
+    lib.gf_last_error.argtypes = [vp]
+    lib.gf_last_error.restype = ctypes.c_char_p
+    lib.gf_destroy.argtypes = [vp]
+    lib.gf_destroy.restype = None
+    lib.gf_version.restype = ctypes.c_char_p
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class Engine:
+    """One engine instance (device memory, stream, CUDA graphs) for a deck."""
+
+    def __init__(self, deck_dir: str, device: int = -1, lib: Optional[ctypes.CDLL] = None):
+        self.lib = lib or load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.gf_create_from_deck(os.fsencode(deck_dir), device, ctypes.byref(h))
+        if rc != GF_OK:
+            raise GFError(rc, self.lib.gf_last_error(None).decode())
+        self.h = h
+        self.info = self.get_info()
+
+    # -- plumbing --------------------------------------------------------
+    def _check(self, rc: int) -> None:
+        if rc != GF_OK:
+            raise GFError(rc, self.lib.gf_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- API -------------------------------------------------------------
+    def get_info(self) -> GFInfo:
+        info = GFInfo()
+        self._check(self.lib.gf_get_info(self.h, ctypes.byref(info)))
+        return info
+
+    def advance(self, nsteps: int, graph: bool = True) -> None:
+        fn = self.lib.gf_advance if graph else self.lib.gf_advance_eager
+        self._check(fn(self.h, int(nsteps)))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.gf_synchronize(self.h))
+
+    def average(self, obs: str) -> np.ndarray:
+        out = (ctypes.c_double * 3)()
+        self._check(self.lib.gf_average(self.h, OBS[obs], out))
+        return np.array(out[:], dtype=np.float64)
+
+    def probe_em(self, i: int, j: int, k: int) -> Tuple[np.ndarray, np.ndarray]:
+        e = (ctypes.c_double * 3)()
+        h = (ctypes.c_double * 3)()
+        self._check(self.lib.gf_probe_em(self.h, i, j, k, e, h))
+        return np.array(e[:]), np.array(h[:])
+
+    def field_dims(self, name: str):
+        dims = (ctypes.c_int64 * 3)()
+        cnt = ctypes.c_size_t()
+        self._check(self.lib.gf_field_dims(self.h, FIELD[name], dims, ctypes.byref(cnt)))
+        return tuple(dims[:]), cnt.value
+
+    def download(self, name: str) -> np.ndarray:
+        dims, cnt = self.field_dims(name)
+        buf = np.empty(cnt, dtype=np.float64)
+        self._check(self.lib.gf_download(self.h, FIELD[name], buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt))
+        ncomp = cnt // (dims[0] * dims[1] * dims[2])
+        return buf.reshape((ncomp,) + dims) if ncomp > 1 else buf.reshape(dims)
+
+    def upload(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        self._check(self.lib.gf_upload(self.h, FIELD[name], a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size))
+
+    def profile_steps(self, nsteps: int) -> dict:
+        """Advance `nsteps` steps with per-launch events; returns
+        {kernel family: (launches, total_ms)}."""
+        recs = (GFKernelTime * 64)()
+        n = ctypes.c_int()
+        self._check(self.lib.gf_profile_steps(self.h, int(nsteps), recs, 64, ctypes.byref(n)))
+        return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(n.value)}
+
+    def check_finite(self) -> None:
+        self._check(self.lib.gf_check_finite(self.h))
+
+    def stream(self) -> int:
+        return self.lib.gf_stream(self.h) or 0
+
+
+def version() -> str:
+    return load_library().gf_version().decode()

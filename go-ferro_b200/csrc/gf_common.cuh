@@ -1,0 +1,155 @@
+// Device-side data layout and helpers shared by every kernel of the engine.
+//
+// Storage is the reference's matrix3d order (matrix.h:46-52): one array per
+// vector component, index (i*dimy + j)*dimz + k, z fastest.  Material ids are
+// one byte per cell (0 = vacuum, id-1 indexes the material table), in place
+// of the reference's unsigned int material_cell (global.h:92).
+//
+// The FP64 parity kernels are compiled with -fmad=false and evaluate every
+// expression in the reference's operation order, so that each multiply and
+// add is rounded exactly as in the reference's host build.
+#pragma once
+
+#include <cstdint>
+
+namespace gf {
+
+constexpr double kMu0 = 1.256637061e-6;     // magnetic_system.h:14, EMdynamic_system.h:12
+constexpr double kE0 = 8.854187817e-12;     // EMdynamic_system.h:13
+constexpr double kC0 = 2.99792458e8;        // EMdynamic_system.h:14
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kMaxMat = 32;
+
+enum MatFlag : uint32_t { MF_FM = 1u, MF_AFM = 2u, MF_FE = 4u, MF_PEC = 8u };
+
+// Per-material constants, precomputed on the host with the same expressions
+// (and operation order) the reference evaluates inside its cell loops.
+struct DevMat {
+    uint32_t flags;
+    int aniso;          // anisotropy_type
+    int cubic_c;        // 1: rotated stiffness has the cubic sparsity pattern
+    int pad_;
+    // FM LLG (magnetic_solver.cpp:84-87, 164-185, 206-208)
+    double Ms, K1c, K2c, B1c, B2c, Aex, dA;   // dA = D/2./A
+    double ex_coef;                            // 2./mu0/Ms
+    double dmi_coef;                           // 2.*D/mu0/Ms
+    double alpha, precess, alpha_precess;      // precess = -gyro/(1+a^2)*dt
+    // AFM sublattices (magnetic_AFM_solver.cpp)
+    double Ms1, Ms2;
+    // elastic (elastic_dynamic_solver.cpp:1295-1297)
+    double cij[6][6];
+    double dens_dt, mass_damp, stiff_damp;
+    // dynamic eigenstrain (elastic_dynamic_solver.cpp:24-61)
+    double l100_15, l111_15, l100a1_075, l100a2_075, l111a1_075, l111a2_075;
+    double Q11, Q12, Q44;
+    // ferroelectric TDGL (ferroelectric_solver.cpp:704-717)
+    double a1, a11, a12, a111, a112, a123, a1111, a1112, a1122, a1123;
+    double tv1, tv2, tv3, G11;
+    double fe_coef, fe_damp;                    // -dt/m, fe_coef*gamma
+    // electromagnetic
+    double er, cond;
+    double comp[3], wp[3], rtau[3];
+};
+
+// Grid, switches and scalars that every kernel needs (passed by value).
+struct Params {
+    int nx, ny, nz;
+    int per_x, per_y, per_z;
+    long n;
+    double dx, dy, dz, dt;
+    int rot;                 // if_OrientRotate
+    double Tg2c[3][3], Tc2g[3][3];
+    // active physics
+    int fm, afm, fe, elastic, em;
+    int elasto_on, elasto_back;   // if_elasto_on_pORm, if_elasto_backaction_from_pORm
+    int em_fromM, em_fromP, em_back_M, em_back_P;
+    int has_eig0, has_strain0, has_hext_nonunif;
+    int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
+    int mag_1D;
+    double liao_w;
+    // elastic boundary coefficients (elastodynamics_AbsorbingBoundary.cpp)
+    double vs_long_1st, vs_tran_1st, vs_long_last, vs_tran_last;
+    double mur_el_half[4], mur_el_full[4];    // long_1st tran_1st long_last tran_last
+    unsigned source_z;
+    int strain_pulse, strain_type;
+    int strain_comp;                           // 0,1,2 for x,y,z
+    // EM Mur coefficients (EMdynamic_initialize.cpp:48-56)
+    double c_top_half, c_bot_half, c_x_half, c_y_half;
+    double c_top, c_bot, c_x, c_y;
+    long plane_z;                               // planeEM_source_z
+    int planeEM;
+    // J_f box (EMdynamic_initialize.cpp:60-68)
+    int jf_on, jf_type, jf_comp;
+    long jf_i0, jf_i1, jf_j0, jf_j1, jf_k0, jf_k1;
+};
+
+// Values that depend on time, computed on the host for every step with the
+// reference's expressions (magnetic_solver.cpp:1833-1861,
+// ferroelectric_solver.cpp:2001-2029, elastic_dynamic_solver.cpp:1195-1223
+// and 3059-3284, EMdynamic_solver.cpp:3828-4316).  Index s = RK stage 0..3.
+struct StageDrive {
+    double Hext[3];
+    double Eext[3];
+    double traction;       // surface traction on the source plane (type 3)
+    double usrc;           // displacement written on the source plane after the update
+    double jf;             // J_f amplitude factor for the stage (types 1,2 times a per-k factor)
+    double plane[3];       // plane-wave E written after the update
+    int usrc_on;
+    int pad_;
+};
+struct StepDrive {
+    double t;
+    StageDrive st[4];
+};
+
+__host__ __device__ inline long cid(const Params& P, long i, long j, long k) {
+    return (i * P.ny + j) * P.nz + k;
+}
+
+// 3x3 frame rotations (mathlib.cpp:45-125); identity when rot == 0
+__device__ inline void glb2crt(const Params& P, double x, double y, double z, double& a, double& b, double& c) {
+    if (P.rot) {
+        a = P.Tg2c[0][0] * x + P.Tg2c[0][1] * y + P.Tg2c[0][2] * z;
+        b = P.Tg2c[1][0] * x + P.Tg2c[1][1] * y + P.Tg2c[1][2] * z;
+        c = P.Tg2c[2][0] * x + P.Tg2c[2][1] * y + P.Tg2c[2][2] * z;
+    } else { a = x; b = y; c = z; }
+}
+__device__ inline void crt2glb(const Params& P, double x, double y, double z, double& a, double& b, double& c) {
+    if (P.rot) {
+        a = P.Tc2g[0][0] * x + P.Tc2g[0][1] * y + P.Tc2g[0][2] * z;
+        b = P.Tc2g[1][0] * x + P.Tc2g[1][1] * y + P.Tc2g[1][2] * z;
+        c = P.Tc2g[2][0] * x + P.Tc2g[2][1] * y + P.Tc2g[2][2] * z;
+    } else { a = x; b = y; c = z; }
+}
+// symmetric tensor rotation out[i][j] = sum_kl T[i][k] T[j][l] in[k][l]
+__device__ inline void rot_tensor(const double T[3][3], const double in[3][3], double out[3][3]) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double acc = 0.;
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) acc = acc + T[i][k] * T[j][l] * in[k][l];
+            out[i][j] = acc;
+        }
+}
+
+// Voigt stress = C * strain with the reference's row accumulation order
+// (mathlib.cpp:127-135).  For the cubic pattern the zero entries are
+// skipped, which leaves every partial sum unchanged.
+__device__ inline void strain2stress(const DevMat& m, const double e[6], double s[6]) {
+    if (m.cubic_c) {
+        s[0] = m.cij[0][0] * e[0] + m.cij[0][1] * e[1] + m.cij[0][2] * e[2];
+        s[1] = m.cij[1][0] * e[0] + m.cij[1][1] * e[1] + m.cij[1][2] * e[2];
+        s[2] = m.cij[2][0] * e[0] + m.cij[2][1] * e[1] + m.cij[2][2] * e[2];
+        s[3] = m.cij[3][3] * e[3];
+        s[4] = m.cij[4][4] * e[4];
+        s[5] = m.cij[5][5] * e[5];
+    } else {
+        for (int i = 0; i < 6; i++) {
+            double acc = 0.;
+            for (int j = 0; j < 6; j++) acc = acc + m.cij[i][j] * e[j];
+            s[i] = acc;
+        }
+    }
+}
+
+}  // namespace gf

@@ -1,0 +1,273 @@
+// Yee-grid Maxwell stage kernels (FP64).
+//
+//   k_em_E<S,C>   one thread per C-edge: curl H of the stage state, the
+//                 4-cell edge averages of permittivity, conductivity, free
+//                 current, polarisation current dP/dt (get_dE_RK{1..4},
+//                 EMdynamic_solver.cpp:337-2238) and the RK4 combination of
+//                 update_DE_RK*/update_DE (:3588-3777).  Edges on a
+//                 non-periodic system boundary get no curl term; the Mur
+//                 kernel sets them afterwards.
+//   k_em_H<S,C>   one thread per C-face: curl E and the 2-cell average of
+//                 Ms dm/dt of the same stage (get_dH_RK{1..4}, :2239-3476)
+//                 with update_DH_RK*/update_DH (:3477-3586).
+//   k_em_plane<S> hard plane-wave source on z = planeEM_source_z
+//                 (update_planeEM*, :3828-3883).
+//   k_em_mur<S,F> first-order Mur on the non-periodic faces of direction F
+//                 (EMdynamic_AbsorbingBoundary.cpp:58-874); directions run
+//                 x, then y, then z, as in the reference.
+//
+// The reference keeps the J_f source in three cell arrays rewritten every
+// stage; here the box test and the per-stage value are evaluated in-kernel.
+#pragma once
+
+#include "gf_state.cuh"
+
+namespace gf {
+
+// free current J_f of cell (i,j,k), component a, stage drive dr
+__device__ inline double jf_cell(const Params& P, const StageIO& io, const StageDrive& dr, int a, long i, long j, long k) {
+    if (!P.jf_on || a != P.jf_comp) return 0.;
+    if (i < P.jf_i0 || i > P.jf_i1 || j < P.jf_j0 || j > P.jf_j1 || k < P.jf_k0 || k > P.jf_k1) return 0.;
+    if (P.jf_type == 1 || P.jf_type == 2) return dr.jf * io.jf_kfac[k];
+    return dr.jf;
+}
+
+template <int S>
+__device__ inline void rk_x(double xv, double d, double* out, double* acc, long e) {
+    if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + d / 6.; }
+    else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + d / 3.; }
+    else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + d / 3.; }
+    else { acc[e] = acc[e] + d / 6.; }
+}
+
+// E edge update.  C = component (0 x, 1 y, 2 z).
+template <int S, int C>
+__global__ void __launch_bounds__(256) k_em_E(Params P, StageIO io) {
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    const long dx_ = nx + (C != 0), dy_ = ny + (C != 1), dz_ = nz + (C != 2);
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= dx_ * dy_ * dz_) return;
+    const long i = e / (dy_ * dz_), j = (e - i * dy_ * dz_) / dz_, k = e - i * dy_ * dz_ - j * dz_;
+    const StageDrive& dr = stage_drive(io, S);
+
+    double d = 0.;
+    bool boundary = false;
+    long cx[4], cy[4], cz[4];
+    // cell quadruples around the edge, in the reference's order 1..4
+    if (C == 0) {
+        if ((j == 0 || j == ny) && !P.per_y) boundary = true;
+        if ((k == 0 || k == nz) && !P.per_z) boundary = true;
+        const long y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y3 = (j == 0 || j == ny) ? 0 : j;
+        const long z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        cx[0] = cx[1] = cx[2] = cx[3] = i;
+        cy[0] = y1; cy[1] = y1; cy[2] = y3; cy[3] = y3;
+        cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
+    } else if (C == 1) {
+        if ((i == 0 || i == nx) && !P.per_x) boundary = true;
+        if ((k == 0 || k == nz) && !P.per_z) boundary = true;
+        const long x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const long z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
+        cy[0] = cy[1] = cy[2] = cy[3] = j;
+        cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
+    } else {
+        if ((i == 0 || i == nx) && !P.per_x) boundary = true;
+        if ((j == 0 || j == ny) && !P.per_y) boundary = true;
+        const long x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const long y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y2 = (j == 0 || j == ny) ? 0 : j;
+        cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
+        cy[0] = y1; cy[1] = y2; cy[2] = y1; cy[3] = y2;
+        cz[0] = cz[1] = cz[2] = cz[3] = k;
+    }
+
+    if (!boundary) {
+        // curl of the stage H
+        double curl;
+        const double* Hx = io.H_in.c[0];
+        const double* Hy = io.H_in.c[1];
+        const double* Hz = io.H_in.c[2];
+        if (C == 0) {
+            const double dHzdy = (Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]) / P.dy;
+            const double dHydz = (Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]) / P.dz;
+            curl = dHzdy - dHydz;
+        } else if (C == 1) {
+            const double dHxdz = (Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]) / P.dz;
+            const double dHzdx = (Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]) / P.dx;
+            curl = dHxdz - dHzdx;
+        } else {
+            const double dHydx = (Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]) / P.dx;
+            const double dHxdy = (Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]) / P.dy;
+            curl = dHydx - dHxdy;
+        }
+        double Jf = 0., dP = 0., er = 0., cond = 0., pc = 0.;
+        for (int q = 0; q < 4; q++) {
+            const long cc = cid(P, cx[q], cy[q], cz[q]);
+            const uint8_t id = io.mid[cc];
+            if (id == 0) {
+                er = er + 1.;
+            } else {
+                const DevMat& mt = io.mats[id - 1];
+                if (P.em_fromP) dP = dP + io.q_in.c[C][cc] * P.dt;
+                if (mt.flags & MF_FE) pc = pc + 1.;
+                er = er + mt.er;
+                cond = cond + mt.cond;
+            }
+            if (P.jf_on) Jf = Jf + jf_cell(P, io, dr, C, cx[q], cy[q], cz[q]);
+        }
+        if (pc < 0.5) pc = 1.;
+        Jf = Jf / 4.;
+        dP = dP / pc; er = er / 4.; cond = cond / 4.;
+        double rhs = curl - Jf;
+        rhs = rhs - cond * io.E_in.c[C][e] - dP / P.dt;
+        d = P.dt / kE0 / er * rhs;
+    }
+    rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], e);
+}
+
+// H face update.  C = component.
+template <int S, int C>
+__global__ void __launch_bounds__(256) k_em_H(Params P, StageIO io) {
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    const long dx_ = nx + (C == 0), dy_ = ny + (C == 1), dz_ = nz + (C == 2);
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= dx_ * dy_ * dz_) return;
+    const long i = e / (dy_ * dz_), j = (e - i * dy_ * dz_) / dz_, k = e - i * dy_ * dz_ - j * dz_;
+    const double* Ex = io.E_in.c[0];
+    const double* Ey = io.E_in.c[1];
+    const double* Ez = io.E_in.c[2];
+    double curl;
+    long a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
+    if (C == 0) {
+        const double dEzdy = (Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]) / P.dy;
+        const double dEydz = (Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]) / P.dz;
+        curl = dEzdy - dEydz;
+        a1x = (i == 0) ? (P.per_x ? nx - 1 : 0) : i - 1;
+        a2x = (i == nx) ? (P.per_x ? 0 : nx - 1) : i;
+    } else if (C == 1) {
+        const double dExdz = (Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]) / P.dz;
+        const double dEzdx = (Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]) / P.dx;
+        curl = dExdz - dEzdx;
+        a1y = (j == 0) ? (P.per_y ? ny - 1 : 0) : j - 1;
+        a2y = (j == ny) ? (P.per_y ? 0 : ny - 1) : j;
+    } else {
+        const double dEydx = (Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]) / P.dx;
+        const double dExdy = (Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]) / P.dy;
+        curl = dEydx - dExdy;
+        a1z = (k == 0) ? (P.per_z ? nz - 1 : 0) : k - 1;
+        a2z = (k == nz) ? (P.per_z ? 0 : nz - 1) : k;
+    }
+    double dM1 = 0., dM2 = 0., cnt = 0.;
+    {
+        const long c1 = cid(P, a1x, a1y, a1z), c2 = cid(P, a2x, a2y, a2z);
+        const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
+        if (i1 != 0) {
+            const DevMat& mt = io.mats[i1 - 1];
+            if (P.em_fromM) dM1 = io.dm.c[C][c1] * mt.Ms;
+            if (mt.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+        }
+        if (i2 != 0) {
+            const DevMat& mt = io.mats[i2 - 1];
+            if (P.em_fromM) dM2 = io.dm.c[C][c2] * mt.Ms;
+            if (mt.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+        }
+    }
+    if (cnt < 0.5) cnt = 1.;
+    const double d = -P.dt / kMu0 * curl - (dM1 + dM2) / cnt;
+    rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], e);
+}
+
+// hard plane-wave source: E on z = plane_z, all three components, i<nx, j<ny
+template <int S>
+__global__ void k_em_plane(Params P, StageIO io) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)P.nx * P.ny) return;
+    const long i = t / P.ny, j = t - i * P.ny;
+    const long nx = P.nx, ny = P.ny, nz = P.nz, z = P.plane_z;
+    const StageDrive& dr = stage_drive(io, S);
+    double* tx = (S < 3) ? io.E_out.c[0] : io.E_acc.c[0];
+    double* ty = (S < 3) ? io.E_out.c[1] : io.E_acc.c[1];
+    double* tz = (S < 3) ? io.E_out.c[2] : io.E_acc.c[2];
+    tx[(i * (ny + 1) + j) * (nz + 1) + z] = dr.plane[0];
+    ty[(i * ny + j) * (nz + 1) + z] = dr.plane[1];
+    tz[(i * (ny + 1) + j) * nz + z] = dr.plane[2];
+    (void)nx;
+}
+
+// Mur boundary on the two faces normal to direction F (0 x, 1 y, 2 z).
+// For S < 3:  out(b) = X(b_in) + c * (X(b) - out(b_in))   (stage store)
+// For S = 3:  new(b) = old(b_in) + c * (old(b) - new(b_in))
+// where X / old is the step-start value and out / new the value written.
+template <int S, int F>
+__global__ void k_em_mur(Params P, StageIO io) {
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool half = (S == 0 || S == 1);
+    // two tangential components per face; index range per component
+    if (F == 0) {
+        // Ey (j<ny, k<=nz) then Ez (j<=ny, k<nz) at i = 0 and i = nx
+        const double cfx = half ? P.c_x_half : P.c_x;
+        const long n1 = ny * (nz + 1), n2 = (ny + 1) * nz;
+        if (t >= n1 + n2) return;
+        const int comp = (t < n1) ? 1 : 2;
+        const long r = (t < n1) ? t : t - n1;
+        long e0, e1, eN, eN1;   // b=0, b_in=1, b=nx, b_in=nx-1
+        if (comp == 1) {
+            const long j = r / (nz + 1), k = r - j * (nz + 1);
+            e0 = (0 * ny + j) * (nz + 1) + k; e1 = (1 * ny + j) * (nz + 1) + k;
+            eN = (nx * ny + j) * (nz + 1) + k; eN1 = ((nx - 1) * ny + j) * (nz + 1) + k;
+        } else {
+            const long j = r / nz, k = r - j * nz;
+            e0 = (0 * (ny + 1) + j) * nz + k; e1 = (1 * (ny + 1) + j) * nz + k;
+            eN = (nx * (ny + 1) + j) * nz + k; eN1 = ((nx - 1) * (ny + 1) + j) * nz + k;
+        }
+        const double* X = io.E_x.c[comp];
+        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        if (!P.pec_xy) {
+            O[e0] = X[e1] + cfx * (X[e0] - O[e1]);
+            O[eN] = X[eN1] + cfx * (X[eN] - O[eN1]);
+        } else { O[e0] = 0.; O[eN] = 0.; }
+    } else if (F == 1) {
+        // Ex (i<nx, k<=nz) then Ez (i<=nx, k<nz) at j = 0 and j = ny
+        const double cfy = half ? P.c_y_half : P.c_y;
+        const long n1 = nx * (nz + 1), n2 = (nx + 1) * nz;
+        if (t >= n1 + n2) return;
+        const int comp = (t < n1) ? 0 : 2;
+        const long r = (t < n1) ? t : t - n1;
+        long e0, e1, eN, eN1;
+        if (comp == 0) {
+            const long i = r / (nz + 1), k = r - i * (nz + 1);
+            e0 = (i * (ny + 1) + 0) * (nz + 1) + k; e1 = (i * (ny + 1) + 1) * (nz + 1) + k;
+            eN = (i * (ny + 1) + ny) * (nz + 1) + k; eN1 = (i * (ny + 1) + ny - 1) * (nz + 1) + k;
+        } else {
+            const long i = r / nz, k = r - i * nz;
+            e0 = (i * (ny + 1) + 0) * nz + k; e1 = (i * (ny + 1) + 1) * nz + k;
+            eN = (i * (ny + 1) + ny) * nz + k; eN1 = (i * (ny + 1) + ny - 1) * nz + k;
+        }
+        const double* X = io.E_x.c[comp];
+        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        if (!P.pec_xy) {
+            O[e0] = X[e1] + cfy * (X[e0] - O[e1]);
+            O[eN] = X[eN1] + cfy * (X[eN] - O[eN1]);
+        } else { O[e0] = 0.; O[eN] = 0.; }
+    } else {
+        // Ex (i<nx, j<=ny) then Ey (i<=nx, j<ny) at k = 0 and k = nz
+        const double ctop = half ? P.c_top_half : P.c_top, cbot = half ? P.c_bot_half : P.c_bot;
+        const long n1 = nx * (ny + 1), n2 = (nx + 1) * ny;
+        if (t >= n1 + n2) return;
+        const int comp = (t < n1) ? 0 : 1;
+        const long r = (t < n1) ? t : t - n1;
+        long base;
+        if (comp == 0) { const long i = r / (ny + 1), j = r - i * (ny + 1); base = (i * (ny + 1) + j) * (nz + 1); }
+        else { const long i = r / ny, j = r - i * ny; base = (i * ny + j) * (nz + 1); }
+        const long e0 = base, e1 = base + 1, eN = base + nz, eN1 = base + nz - 1;
+        const double* X = io.E_x.c[comp];
+        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        if (!P.pec_z) {
+            O[eN] = X[eN1] + ctop * (X[eN] - O[eN1]);
+            if (!P.abc_1D || !P.abc_em_onlytop) O[e0] = X[e1] + cbot * (X[e0] - O[e1]);
+            else O[e0] = 0.;
+        } else { O[e0] = 0.; O[eN] = 0.; }
+    }
+}
+
+}  // namespace gf

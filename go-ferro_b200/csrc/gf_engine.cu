@@ -1,0 +1,1173 @@
+// B200 engine for GO-Ferro's coupled RK4 phase-field step: state ownership,
+// stage sequencing, CUDA-graph replay and the C ABI of goferro_b200.h.
+//
+// One translation unit holds every kernel of the FP64 path (the .cuh files
+// below); it is compiled with -fmad=false so that each multiply and add is
+// rounded separately, as in the reference's host build.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/goferro_b200.h"
+#include "gf_deck.h"
+#include "gf_launch.cuh"
+#include "gf_state.cuh"
+#include "gf_llg.cuh"
+#include "gf_elastic.cuh"
+#include "gf_fe.cuh"
+#include "gf_em.cuh"
+#include "gf_demag.cuh"
+#include "gf_util.cuh"
+
+using namespace gf;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr long kDriveCap = 4096;      // steps of time-dependent drive held on the device (power of two)
+thread_local std::string g_create_err;
+
+struct Field3 {
+    // X, A, S0, S1 per component; len[c] = elements of component c
+    double* X[3] = {nullptr, nullptr, nullptr};
+    double* A[3] = {nullptr, nullptr, nullptr};
+    double* S0[3] = {nullptr, nullptr, nullptr};
+    double* S1[3] = {nullptr, nullptr, nullptr};
+    long len[3] = {0, 0, 0};
+    bool on = false;
+};
+
+}  // namespace
+
+struct gf_engine {
+    Deck deck;
+    Params P{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    // bookkeeping
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    unsigned long long steps_done = 0;     // completed steps (host mirror of the device counter)
+    double t_host = 0.;                    // time_device after the last computed step
+    long presc_H = 0, presc_E = 0;
+    double Hext_cur[3] = {0, 0, 0}, Eext_cur[3] = {0, 0, 0};
+
+    // device data
+    uint8_t* mid = nullptr;
+    DevMat* mats = nullptr;
+    LLGTables* llg_tab = nullptr;
+    StepDrive* drive = nullptr;
+    StepDrive* drive_host = nullptr;       // pinned staging
+    unsigned long long* step_ctr = nullptr;
+    double* jf_kfac = nullptr;
+
+    Field3 m, p, q, u, v, E, H;
+    double* dm[3] = {nullptr, nullptr, nullptr};
+    double* force[3] = {nullptr, nullptr, nullptr};
+    double* force_store[3] = {nullptr, nullptr, nullptr};
+    double* Hstat[3] = {nullptr, nullptr, nullptr};
+    double* Estat[3] = {nullptr, nullptr, nullptr};
+    double* Hnu[3] = {nullptr, nullptr, nullptr};
+    double* eps_g[6] = {}; double* eps_c[6] = {};
+    double* eig_g[6] = {}; double* eig_c[6] = {};
+    double* liao_hist = nullptr; double* liao_last = nullptr;
+    double* scratch = nullptr;             // 6n doubles: output staging and reductions
+    int* flag = nullptr;
+
+    // magnetostatics
+    int demag_mode = -1;                   // -1 none, 0 FFT, 1 factors, 2 1-D
+    bool demag_per_stage = false;
+    double* Mfft = nullptr;                // 3 x n real
+    cufftDoubleComplex* Mk = nullptr;      // 3 x n21
+    cufftDoubleComplex* Nk = nullptr;      // 9 x n21
+    cufftHandle plan_r2c = 0, plan_c2r = 0;
+    bool plans = false;
+
+    StageIO io[2][4];
+    // launch accounting and optional per-launch timing (gf_profile_steps)
+    int launches_per_step = 0;
+    int launch_counter = 0;
+    bool profiling = false;
+    struct ProfRec { const char* name; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    bool graphs_ready = false;
+};
+
+namespace {
+
+#define GF_CU(call)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            eng->err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+            return GF_ECUDA;                                                             \
+        }                                                                                \
+    } while (0)
+
+#define GF_FFT(call)                                                                     \
+    do {                                                                                 \
+        cufftResult r_ = (call);                                                         \
+        if (r_ != CUFFT_SUCCESS) {                                                       \
+            eng->err = std::string(#call) + ": cuFFT error " + std::to_string((int)r_);  \
+            return GF_ECUDA;                                                             \
+        }                                                                                \
+    } while (0)
+
+#define GF_TRY(expr)                      \
+    do {                                  \
+        int rc_ = (expr);                 \
+        if (rc_ != GF_OK) return rc_;     \
+    } while (0)
+
+cudaEvent_t next_event(gf_engine* eng) {
+    if (eng->ev_used == eng->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        eng->ev_pool.push_back(e);
+    }
+    return eng->ev_pool[eng->ev_used++];
+}
+
+// every kernel of the engine is launched through klaunch: it counts the
+// launch and, in profiling mode, brackets it with events on the stream
+template <class Kernel, class... Args>
+cudaError_t klaunch(gf_engine* eng, const char* name, Kernel k, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                    Args... args) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (eng->profiling) { a = next_event(eng); cudaEventRecord(a, s); }
+    cudaError_t e = launch(k, grid, block, smem, s, args...);
+    if (eng->profiling) { b = next_event(eng); cudaEventRecord(b, s); eng->prof.push_back({name, a, b}); }
+    eng->launch_counter++;
+    return e;
+}
+
+int dalloc(gf_engine* eng, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        eng->err = "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e);
+        return GF_ENOMEM;
+    }
+    eng->allocs.push_back(*p);
+    eng->bytes += bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, eng->stream);
+    if (e != cudaSuccess) { eng->err = std::string("cudaMemset: ") + cudaGetErrorString(e); return GF_ECUDA; }
+    return GF_OK;
+}
+
+template <class T>
+int dalloc_n(gf_engine* eng, T** p, size_t count) {
+    return dalloc(eng, reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+int alloc_field(gf_engine* eng, Field3& f, long l0, long l1, long l2) {
+    f.on = true;
+    f.len[0] = l0; f.len[1] = l1; f.len[2] = l2;
+    for (int c = 0; c < 3; c++) {
+        GF_TRY(dalloc_n(eng, &f.X[c], f.len[c]));
+        GF_TRY(dalloc_n(eng, &f.A[c], f.len[c]));
+        GF_TRY(dalloc_n(eng, &f.S0[c], f.len[c]));
+        GF_TRY(dalloc_n(eng, &f.S1[c], f.len[c]));
+    }
+    return GF_OK;
+}
+
+DevMat make_devmat(const Material& m, double dt) {
+    DevMat d;
+    std::memset(&d, 0, sizeof(d));
+    d.flags = (m.fm ? MF_FM : 0u) | (m.afm ? MF_AFM : 0u) | (m.fe ? MF_FE : 0u) | (m.pec ? MF_PEC : 0u);
+    d.aniso = (int)m.aniso_type;
+    // magnetic_solver.cpp:84-87, 164-185, 206-208
+    d.Ms = m.Ms;
+    if (m.fm) {
+        const double mu0 = kMu0;
+        d.K1c = m.K1 / mu0 / m.Ms; d.K2c = m.K2 / mu0 / m.Ms;
+        d.B1c = m.B1 / mu0 / m.Ms; d.B2c = m.B2 / mu0 / m.Ms;
+        d.Aex = m.Aex;
+        d.dA = m.iDMI / 2. / m.Aex;
+        d.ex_coef = 2. / mu0 / m.Ms;
+        d.dmi_coef = 2. * m.iDMI / mu0 / m.Ms;
+        d.alpha = m.alpha;
+        d.precess = -m.gyro / (1 + m.alpha * m.alpha) * dt;
+        d.alpha_precess = m.alpha * d.precess;
+    }
+    d.Ms1 = m.Ms1; d.Ms2 = m.Ms2;
+    // elastic
+    bool cubic = true;
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) {
+            d.cij[a][b] = m.cij[a][b];
+            const bool in_pattern = (a < 3 && b < 3) || (a == b);
+            if (!in_pattern && m.cij[a][b] != 0.) cubic = false;
+        }
+    d.cubic_c = cubic ? 1 : 0;
+    d.dens_dt = dt / m.density;
+    d.mass_damp = -dt * m.mass_damping;
+    d.stiff_damp = m.stiff_damping / m.density;
+    d.l100_15 = 1.5 * m.lam100; d.l111_15 = 1.5 * m.lam111;
+    d.l100a1_075 = 0.5 * 1.5 * m.lam100_1; d.l100a2_075 = 0.5 * 1.5 * m.lam100_2;
+    d.l111a1_075 = 0.5 * 1.5 * m.lam111_1; d.l111a2_075 = 0.5 * 1.5 * m.lam111_2;
+    d.Q11 = m.Q11; d.Q12 = m.Q12; d.Q44 = m.Q44;
+    // ferroelectric (ferroelectric_solver.cpp:704-717)
+    d.a1 = m.a1; d.a11 = m.a11; d.a12 = m.a12; d.a111 = m.a111; d.a112 = m.a112; d.a123 = m.a123;
+    d.a1111 = m.a1111; d.a1112 = m.a1112; d.a1122 = m.a1122; d.a1123 = m.a1123;
+    d.tv1 = m.tv[0]; d.tv2 = m.tv[1]; d.tv3 = m.tv[2]; d.G11 = m.G11;
+    if (m.fe) {
+        d.fe_coef = -1. * dt / m.fe_mass;
+        d.fe_damp = d.fe_coef * m.fe_damping;
+    }
+    d.er = m.er; d.cond = m.cond;
+    for (int k = 0; k < 3; k++) { d.comp[k] = m.comp[k]; d.wp[k] = m.wp[k]; d.rtau[k] = 1. / m.tau[k]; }
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// validation: what this build implements
+// ---------------------------------------------------------------------------
+std::string unsupported(const Deck& d) {
+    if (d.any_afm) return "two-sublattice antiferromagnets (if_AFM) are not supported by this build";
+    if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this build";
+    if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this build";
+    if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this build";
+    if (d.any_pec && d.em_dynamic) return "PEC materials are not supported by this build";
+    if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
+    if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this build";
+    if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
+    if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this build";
+    for (size_t i = 0; i < d.mats.size(); i++) {
+        const Material& m = d.mats[i];
+        if (m.fm && m.aniso_type > 2) return "anisotropy_type must be 0, 1 or 2";
+        if (m.fm && (m.Ms == 0. || m.Aex == 0.)) return "ferromagnetic material needs nonzero Ms and Aex";
+        if (m.fe && m.fe_mass == 0.) return "ferroelectric material needs nonzero FE_mass";
+        if (d.em_dynamic) {
+            for (int k = 0; k < 3; k++)
+                if (m.wp[k] != 0.) return "Drude dispersion (omega_plasma != 0) is not supported by this build";
+            if (!(m.comp[0] == m.comp[0])) return "Drude weights sum to zero: the reference's normalisation yields NaN fields for this deck";
+        }
+    }
+    if (d.elastodynamics) {
+        if (d.nz < 5 && !d.abc_1D) return "the Liao boundary needs nz >= 5";
+        if (d.strain_pulse && d.strain_z >= (unsigned)d.nz) return "input_strain_sourcez outside the grid";
+        // the +z neighbour of get_dv_RK* is read out of the column when the
+        // top face is not stress-free and nz-1 != ny-1 (elastic_dynamic_solver.cpp:1247)
+        const long nx = d.nx, ny = d.ny, nz = d.nz;
+        auto mc = [&](long i, long j, long k) { return d.material_cell[(size_t)((i * ny + j) * nz + k)]; };
+        if (nz - 1 != ny - 1 && d.per_z) {
+            for (long i = 0; i < nx; i++)
+                for (long j = 0; j < ny; j++)
+                    if (mc(i, j, 0) && mc(i, j, nz - 1)) return "periodic z with nz != ny and a solid top/bottom pair: the reference reads outside the array";
+        }
+        if (ny - 1 < nz - 1) {
+            const long kq = ny - 1;
+            for (long i = 0; i < nx; i++)
+                for (long j = 0; j < ny; j++)
+                    if (mc(i, j, kq) && mc(i, j, kq + 1) && !mc(i, j, 0))
+                        return "reference quirk at k = ny-1 reads a vacuum cell's material";
+        }
+    }
+    if (d.em_dynamic && d.planeEM) {
+        if (d.nz_layer.empty()) return "plane-wave source needs at least one layer";
+        if ((long)(d.nz_layer[0] / 5) > d.nz) return "plane-wave source plane outside the grid";
+    }
+    if (d.jf_input && d.em_dynamic) {
+        if (d.jf_i1 >= (unsigned long)d.nx || d.jf_j1 >= (unsigned long)d.ny || d.jf_k1 >= (unsigned long)d.nz ||
+            d.jf_i0 > d.jf_i1 || d.jf_j0 > d.jf_j1 || d.jf_k0 > d.jf_k1)
+            return "J_f box outside the grid";
+        if (d.jf_type > 6) return "Jf_input_type must be 0..6";
+    }
+    return "";
+}
+
+void build_params(gf_engine* eng) {
+    const Deck& d = eng->deck;
+    Params& P = eng->P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = (int)d.nx; P.ny = (int)d.ny; P.nz = (int)d.nz; P.n = d.n();
+    P.per_x = d.per_x; P.per_y = d.per_y; P.per_z = d.per_z;
+    P.dx = d.dx; P.dy = d.dy; P.dz = d.dz; P.dt = d.dt;
+    P.rot = d.orient_rotate;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { P.Tg2c[i][j] = d.Tg2c[i][j]; P.Tc2g[i][j] = d.Tc2g[i][j]; }
+    P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
+    P.elasto_on = d.elasto_on; P.elasto_back = d.elasto_back && d.elastodynamics;
+    P.em_fromM = d.em_fromM && d.em_dynamic && d.any_fm;
+    P.em_fromP = d.em_fromP && d.em_dynamic && d.any_fe;
+    P.em_back_M = d.em_back_M && d.em_dynamic;
+    P.em_back_P = d.em_back_P && d.em_dynamic;
+    P.has_hext_nonunif = d.read_Hext_nonunif;
+    P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
+    P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
+    P.liao_w = d.liao_w;
+
+    // sound speeds of the first and last z planes (elastic_initialize.cpp:43-80)
+    auto first_mat = [&](long k) -> const Material* {
+        for (long i = 0; i < d.nx; i++)
+            for (long j = 0; j < d.ny; j++) {
+                uint8_t id = d.material_cell[(size_t)((i * d.ny + j) * d.nz + k)];
+                if (id) return &d.mats[id - 1];
+            }
+        return nullptr;
+    };
+    double c11_1 = 0., c44_1 = 0., rho_1 = 1.e-8, c11_l = 0., c44_l = 0., rho_l = 1.e-8;
+    if (const Material* m = first_mat(0)) { c11_1 = m->c11; c44_1 = m->c44; rho_1 = m->density; }
+    if (const Material* m = first_mat(d.nz - 1)) { c11_l = m->c11; c44_l = m->c44; rho_l = m->density; }
+    P.vs_long_1st = std::sqrt((c11_1 / rho_1)); P.vs_tran_1st = std::sqrt((c44_1 / rho_1));
+    P.vs_long_last = std::sqrt((c11_l / rho_l)); P.vs_tran_last = std::sqrt((c44_l / rho_l));
+    const double dz = d.dz, dt = d.dt;
+    const double vs[4] = {P.vs_long_1st, P.vs_tran_1st, P.vs_long_last, P.vs_tran_last};
+    for (int a = 0; a < 4; a++) {
+        P.mur_el_half[a] = (2. * dz - vs[a] * dt) / (2. * dz + vs[a] * dt);
+        P.mur_el_full[a] = (dz - vs[a] * dt) / (dz + vs[a] * dt);
+    }
+    P.source_z = d.strain_z;
+    P.strain_pulse = d.strain_pulse; P.strain_type = (int)d.strain_type;
+    P.strain_comp = d.strain_comp == 'y' ? 1 : (d.strain_comp == 'z' ? 2 : 0);
+
+    // Maxwell Mur coefficients (EMdynamic_initialize.cpp:24-56)
+    auto first_er = [&](long k) -> double {
+        for (long i = 0; i < d.nx; i++)
+            for (long j = 0; j < d.ny; j++) {
+                uint8_t id = d.material_cell[(size_t)((i * d.ny + j) * d.nz + k)];
+                if (id) return std::sqrt(d.mats[id - 1].er);
+            }
+        return 1.;
+    };
+    const double sq_bot = first_er(0), sq_top = first_er(d.nz - 1);
+    const double c = kC0, dx = d.dx, dy = d.dy;
+    P.c_top_half = (2. * dz - c / sq_top * dt) / (2. * dz + c / sq_top * dt);
+    P.c_bot_half = (2. * dz - c / sq_bot * dt) / (2. * dz + c / sq_bot * dt);
+    P.c_x_half = (2. * dx - c * dt) / (2. * dx + c * dt);
+    P.c_y_half = (2. * dy - c * dt) / (2. * dy + c * dt);
+    P.c_top = (dz - c / sq_top * dt) / (dz + c / sq_top * dt);
+    P.c_bot = (dz - c / sq_bot * dt) / (dz + c / sq_bot * dt);
+    P.c_x = (dx - c * dt) / (dx + c * dt);
+    P.c_y = (dy - c * dt) / (dy + c * dt);
+    P.plane_z = d.nz_layer.empty() ? 0 : (long)(d.nz_layer[0] / 5);
+    P.planeEM = d.planeEM && d.em_dynamic;
+    P.jf_on = d.jf_input && d.em_dynamic;
+    P.jf_type = (int)d.jf_type;
+    P.jf_comp = d.jf_comp == 'y' ? 1 : (d.jf_comp == 'z' ? 2 : 0);
+    P.jf_i0 = (long)d.jf_i0; P.jf_i1 = (long)d.jf_i1; P.jf_j0 = (long)d.jf_j0; P.jf_j1 = (long)d.jf_j1;
+    P.jf_k0 = (long)d.jf_k0; P.jf_k1 = (long)d.jf_k1;
+}
+
+// ---------------------------------------------------------------------------
+// time-dependent drive of one step (host, reference expressions)
+// ---------------------------------------------------------------------------
+void step_drive(gf_engine* eng, StepDrive& sd) {
+    const Deck& d = eng->deck;
+    const double PI = kPi;
+    const double dt = d.dt;
+    // time_marching_device_serial (global.cpp:512-549)
+    eng->t_host = eng->t_host + dt;
+    const double t = eng->t_host;
+    sd.t = t;
+    if (d.prescribe_E) {
+        if (eng->presc_E < d.n_prescribe_E && (t - dt) > d.tE[eng->presc_E]) eng->presc_E = eng->presc_E + 1;
+        if (eng->presc_E < d.n_prescribe_E) { eng->Eext_cur[0] = d.Ex[eng->presc_E]; eng->Eext_cur[1] = d.Ey[eng->presc_E]; eng->Eext_cur[2] = d.Ez[eng->presc_E]; }
+        else { eng->Eext_cur[0] = eng->Eext_cur[1] = eng->Eext_cur[2] = 0.; }
+    }
+    if (d.prescribe_H) {
+        if (eng->presc_H < d.n_prescribe_H && (t - dt) > d.tH[eng->presc_H]) eng->presc_H = eng->presc_H + 1;
+        if (eng->presc_H < d.n_prescribe_H) { eng->Hext_cur[0] = d.Hx[eng->presc_H]; eng->Hext_cur[1] = d.Hy[eng->presc_H]; eng->Hext_cur[2] = d.Hz[eng->presc_H]; }
+        else { eng->Hext_cur[0] = eng->Hext_cur[1] = eng->Hext_cur[2] = 0.; }
+    }
+    // local times of the four stages
+    const double lt_ext[4] = {t - dt, t - dt * 0.5, t - dt * 0.5, t};
+    for (int s = 0; s < 4; s++) {
+        StageDrive& st = sd.st[s];
+        std::memset(&st, 0, sizeof(st));
+        for (int a = 0; a < 3; a++) {
+            st.Hext[a] = d.prescribe_H ? eng->Hext_cur[a]
+                                       : d.Hext_stat[a] + d.Hext_altr[a] * std::sin(2. * PI * d.H_altr_freq[a] * lt_ext[s]);
+            st.Eext[a] = d.prescribe_E ? eng->Eext_cur[a]
+                                       : d.Eext_stat[a] + d.Eext_altr[a] * std::sin(2. * PI * d.E_altr_freq[a] * lt_ext[s]);
+        }
+        // surface traction (type 3), get_dv_RK*
+        {
+            double tv;
+            if (s == 0) tv = t - dt - 5.0 * d.sigma_gauss;
+            else if (s < 3) tv = t - 0.5 * dt - 5.0 * d.sigma_gauss;
+            else tv = t - 5.0 * d.sigma_gauss;
+            st.traction = d.amp_gauss * std::exp(-1. * std::pow(tv, 2.) / (2. * std::pow(d.sigma_gauss, 2.)));
+        }
+        // displacement source written after the stage update
+        // (update_Du_Gaussian_half for stages 1-2, _full for 3, final for 4)
+        {
+            const double vs = (d.strain_comp == 'z') ? eng->P.vs_long_1st : eng->P.vs_tran_1st;
+            const bool half = (s < 2);
+            const double tl = half ? (t - 0.5 * dt) : t;
+            st.usrc_on = 0;
+            if (d.strain_type == 1 && t < 12.5 * d.sigma_gauss) {
+                st.usrc_on = 1;
+                st.usrc = d.amp_gauss * 1.6487210 * d.sigma_gauss * vs *
+                          std::exp(-1. * std::pow((tl - 5.0 * d.sigma_gauss), 2.) / (2. * d.sigma_gauss * d.sigma_gauss));
+            } else if (d.strain_type == 2) {
+                st.usrc_on = 1;
+                const double val = d.amp_gauss * vs / 2. / PI / d.sigma_gauss * (std::cos(2. * PI * d.sigma_gauss * (tl)) - 1);
+                if (d.strain_cycles == 0) st.usrc = val;
+                else st.usrc = (tl <= static_cast<double>(d.strain_cycles) / d.sigma_gauss) ? val : 0.;
+            }
+        }
+        // free-current source value (update_Jf_input / _half / _full)
+        if (d.jf_input) {
+            // stage 3 keeps the stage-2 value (get_dE_RK3 does not refresh J_f)
+            const int v = (s == 0) ? 0 : (s < 3 ? 1 : 2);
+            const double tl = (v == 0) ? (t - dt) : (v == 1 ? (t - 0.5 * dt) : t);
+            double val = 0.;
+            if (d.jf_type < 3) {
+                double temporal;
+                if (v == 0) temporal = std::sin(2. * PI * d.jf_freq * (t - dt));
+                else if (v == 1) temporal = std::sin(2. * PI * d.jf_freq * (t - 0.5 * dt));
+                else temporal = std::sin(2. * PI * d.jf_freq * t);
+                val = d.jf_amp * temporal;
+            } else if (d.jf_type == 3) {
+                double temporal = 0.;
+                if (tl <= static_cast<double>(d.jf_cycles) / d.jf_freq) {
+                    if (v == 0) temporal = std::sin(2. * PI * d.jf_freq * (t - dt));
+                    else if (v == 1) temporal = std::sin(2. * PI * d.jf_freq * (t - 0.5 * dt));
+                    else temporal = std::sin(2. * PI * d.jf_freq * (t));
+                }
+                val = d.jf_amp * temporal;
+            } else if (d.jf_type == 4 || d.jf_type == 5) {
+                double tv;
+                if (v == 0) tv = t - dt - 5. * d.jf_freq;
+                else if (v == 1) tv = t - 0.5 * dt - 5. * d.jf_freq;
+                else tv = t - 5. * d.jf_freq;
+                if (d.jf_type == 4) val = d.jf_amp * std::exp(-1. * std::pow(tv, 2.) / (2. * std::pow(d.jf_freq, 2.)));
+                else val = d.jf_amp * std::sqrt(std::exp(1.)) * tv / d.jf_freq * std::exp(-1. * std::pow(tv, 2.) / (2. * std::pow(d.jf_freq, 2.)));
+            } else if (d.jf_type == 6) {
+                double tv, sarg;
+                if (v == 0) { tv = t - dt - 5. * d.jf_sigma; sarg = (t - dt); }
+                else if (v == 1) { tv = t - 0.5 * dt - 5. * d.jf_sigma; sarg = (t - 0.5 * dt); }
+                else { tv = t - 5. * d.jf_sigma; sarg = t; }
+                if (v == 2) val = d.jf_amp * std::exp(-1. * std::pow(tv, 2.) / (2. * std::pow(d.jf_sigma, 2.))) * std::sin(2. * PI * d.jf_freq * t);
+                else val = d.jf_amp * std::exp(-1. * std::pow(tv, 2.) / (2. * std::pow(d.jf_sigma, 2.))) * std::sin(2. * PI * d.jf_freq * sarg);
+            }
+            st.jf = val;
+        }
+        // plane wave (update_planeEM_half for stages 1-2, _full for 3 and the final update)
+        for (int a = 0; a < 3; a++) {
+            if (s < 2) st.plane[a] = d.planeEM_E[a] * std::sin(2. * PI * d.planeEM_freq[a] * (t - 0.5 * dt));
+            else st.plane[a] = d.planeEM_E[a] * std::sin(2. * PI * d.planeEM_freq[a] * t);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage IO tables
+// ---------------------------------------------------------------------------
+F3 f3(double* const* p) { F3 r; for (int c = 0; c < 3; c++) r.c[c] = p[c]; return r; }
+
+void set_io_field(const Field3& f, int parity, int s, F3& in, F3& x, F3& acc, F3& out) {
+    // parity 0: X = f.X, A = f.A ; parity 1: roles swapped
+    double* const* X = parity ? f.A : f.X;
+    double* const* A = parity ? f.X : f.A;
+    x = f3(X);
+    acc = f3(A);
+    if (s == 0) { in = f3(X); out = f3(f.S0); }
+    else if (s == 1) { in = f3(f.S0); out = f3(f.S1); }
+    else if (s == 2) { in = f3(f.S1); out = f3(f.S0); }
+    else { in = f3(f.S0); out = f3(A); }
+}
+
+void build_io(gf_engine* eng) {
+    for (int par = 0; par < 2; par++)
+        for (int s = 0; s < 4; s++) {
+            StageIO& io = eng->io[par][s];
+            std::memset(&io, 0, sizeof(io));
+            if (eng->m.on) set_io_field(eng->m, par, s, io.m_in, io.m_x, io.m_acc, io.m_out);
+            if (eng->p.on) set_io_field(eng->p, par, s, io.p_in, io.p_x, io.p_acc, io.p_out);
+            if (eng->q.on) set_io_field(eng->q, par, s, io.q_in, io.q_x, io.q_acc, io.q_out);
+            if (eng->u.on) set_io_field(eng->u, par, s, io.u_in, io.u_x, io.u_acc, io.u_out);
+            if (eng->v.on) set_io_field(eng->v, par, s, io.v_in, io.v_x, io.v_acc, io.v_out);
+            if (eng->E.on) set_io_field(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out);
+            if (eng->H.on) set_io_field(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out);
+            io.dm = f3(eng->dm);
+            io.force = f3(eng->force);
+            io.force_store = f3(eng->force_store);
+            io.Hstat = f3(eng->Hstat);
+            io.Estat = f3(eng->Estat);
+            io.Hnu = f3(eng->Hnu);
+            for (int a = 0; a < 6; a++) {
+                io.eps_g[a] = eng->eps_g[a]; io.eps_c[a] = eng->eps_c[a];
+                io.eig_g[a] = eng->eig_g[a]; io.eig_c[a] = eng->eig_c[a];
+                io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr;
+            }
+            io.liao_hist = eng->liao_hist;
+            io.liao_last = eng->liao_last;
+            io.mid = eng->mid;
+            io.mats = eng->mats;
+            io.drive = eng->drive;
+            io.drive_mask = (unsigned long long)(kDriveCap - 1);
+            io.step = eng->step_ctr;
+            io.jf_kfac = eng->jf_kfac;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// one RK4 step: kernel sequence in the reference's data order
+// ---------------------------------------------------------------------------
+template <int S>
+int enqueue_stage(gf_engine* eng, int parity) {
+    const Params& P = eng->P;
+    const StageIO& io = eng->io[parity][S];
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    if (P.elastic) {
+        GF_CU(klaunch(eng, "k_strain", k_strain, dim3(bn), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_elastic", k_elastic<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
+    }
+    if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(bn), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
+    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+    if (P.em) {
+        const long nx = P.nx, ny = P.ny, nz = P.nz;
+        GF_CU(klaunch(eng, "k_em_E_x", k_em_E<S, 0>, dim3(blocks_for(nx * (ny + 1) * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_E_y", k_em_E<S, 1>, dim3(blocks_for((nx + 1) * ny * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_E_z", k_em_E<S, 2>, dim3(blocks_for((nx + 1) * (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_H_x", k_em_H<S, 0>, dim3(blocks_for((nx + 1) * ny * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_H_y", k_em_H<S, 1>, dim3(blocks_for(nx * (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_H_z", k_em_H<S, 2>, dim3(blocks_for(nx * ny * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
+        if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+    }
+    if (eng->demag_per_stage) {
+        // static field of the new stage state (main.cpp:299-306, 476-483)
+        F3 mnew = io.m_out;
+        if (eng->demag_mode == 0) {
+            GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                         mnew, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+            GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+            const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+            const double vol_neg = -P.dx * P.dy * P.dz;
+            GF_CU(klaunch(eng, "k_demag_mul", k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, vol_neg,
+                         (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+            GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+            for (int a = 0; a < 3; a++)
+                GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+        } else {
+            GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                         mnew, eng->demag_mode, (double*)nullptr, f3(eng->Hstat),
+                         eng->deck.demag_fac[0], eng->deck.demag_fac[1], eng->deck.demag_fac[2]));
+        }
+    }
+    return GF_OK;
+}
+
+int enqueue_step(gf_engine* eng, int parity) {
+    eng->launch_counter = 0;
+    GF_TRY(enqueue_stage<0>(eng, parity));
+    GF_TRY(enqueue_stage<1>(eng, parity));
+    GF_TRY(enqueue_stage<2>(eng, parity));
+    GF_TRY(enqueue_stage<3>(eng, parity));
+    GF_CU(klaunch(eng, "k_step_inc", k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
+    return GF_OK;
+}
+
+// static field from the current m (initial solve, main.cpp:135-146)
+int static_field_now(gf_engine* eng) {
+    const Params& P = eng->P;
+    if (eng->demag_mode < 0) return GF_OK;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    cudaStream_t st = eng->stream;
+    F3 mx = f3(eng->m.X);
+    if (eng->demag_mode == 0) {
+        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, 0,
+                     eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+        GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+        const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+        GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
+                     (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+        GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+        for (int a = 0; a < 3; a++)
+            GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    } else {
+        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx,
+                     eng->demag_mode, (double*)nullptr, f3(eng->Hstat), eng->deck.demag_fac[0], eng->deck.demag_fac[1],
+                     eng->deck.demag_fac[2]));
+    }
+    return GF_OK;
+}
+
+int setup_demag(gf_engine* eng) {
+    const Deck& d = eng->deck;
+    const Params& P = eng->P;
+    if (!(d.any_fm || d.any_afm) || !d.magnetostatics) { eng->demag_mode = -1; return GF_OK; }
+    if (d.mag_1D) eng->demag_mode = 2;
+    else if (d.demag_factor) eng->demag_mode = 1;
+    else eng->demag_mode = 0;
+    eng->demag_per_stage = !d.em_dynamic;
+    if (eng->demag_mode != 0) return GF_OK;
+    const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    GF_TRY(dalloc_n(eng, &eng->Mfft, (size_t)3 * P.n));
+    GF_TRY(dalloc_n(eng, &eng->Mk, (size_t)3 * n21));
+    GF_TRY(dalloc_n(eng, &eng->Nk, (size_t)9 * n21));
+    int dims[3] = {P.nx, P.ny, P.nz};
+    GF_FFT(cufftPlanMany(&eng->plan_r2c, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3));
+    GF_FFT(cufftPlanMany(&eng->plan_c2r, 3, dims, nullptr, 1, (int)n21, nullptr, 1, (int)P.n, CUFFT_Z2D, 3));
+    eng->plans = true;
+    GF_FFT(cufftSetStream(eng->plan_r2c, eng->stream));
+    GF_FFT(cufftSetStream(eng->plan_c2r, eng->stream));
+    // demag tensor tables: 9 x n real on the device, transformed in three batches of 3
+    double* tab = nullptr;
+    GF_TRY(dalloc_n(eng, &tab, (size_t)9 * P.n));
+    GF_CU(launch(k_newell, dim3(blocks_for(P.n, 128)), dim3(128), 0, eng->stream, P, tab));
+    for (int b = 0; b < 3; b++)
+        GF_FFT(cufftExecD2Z(eng->plan_r2c, tab + (size_t)3 * b * P.n, eng->Nk + (size_t)3 * b * n21));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* src, long n) {
+    for (int a = 0; a < 3; a++)
+        GF_CU(cudaMemcpyAsync(dst[a], src[a].data(), sizeof(double) * n, cudaMemcpyHostToDevice, eng->stream));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int initial_state(gf_engine* eng, const std::string& dir) {
+    const Deck& d = eng->deck;
+    const long n = d.n();
+    const double PI = kPi;
+    std::vector<double> buf[3];
+    for (auto& b : buf) b.assign((size_t)n, 0.);
+    if (eng->m.on) {
+        if (d.in_m) {
+            std::string e = read_restart(dir + "/m.in", d.nx, d.ny, d.nz, 3, buf);
+            if (!e.empty()) { eng->err = e; return GF_EIO; }
+        } else {
+            // initialize_magnetization (magnetic_initialize.cpp:1131-1151)
+            const double theta = (d.theta_mag) / 180. * PI;
+            const double phi = (d.phi_mag) / 180 * PI;
+            const double mx = std::sin(theta) * std::cos(phi), my = std::sin(theta) * std::sin(phi), mz = std::cos(theta);
+            for (long c = 0; c < n; c++) {
+                uint8_t id = d.material_cell[(size_t)c];
+                if (id && d.mats[id - 1].fm) { buf[0][c] = mx; buf[1][c] = my; buf[2][c] = mz; }
+            }
+        }
+        GF_TRY(upload_vec(eng, eng->m.X, buf, n));
+    }
+    if (eng->p.on) {
+        for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+        std::vector<double> qb[3];
+        for (auto& b : qb) b.assign((size_t)n, 0.);
+        if (d.in_pq) {
+            std::string e = read_restart(dir + "/p.in", d.nx, d.ny, d.nz, 3, buf);
+            if (e.empty()) e = read_restart(dir + "/q.in", d.nx, d.ny, d.nz, 3, qb);
+            if (!e.empty()) { eng->err = e; return GF_EIO; }
+        } else {
+            for (long c = 0; c < n; c++) {
+                uint8_t id = d.material_cell[(size_t)c];
+                if (id && d.mats[id - 1].fe) { buf[0][c] = d.px_init; buf[1][c] = d.py_init; buf[2][c] = d.pz_init; }
+            }
+        }
+        GF_TRY(upload_vec(eng, eng->p.X, buf, n));
+        GF_TRY(upload_vec(eng, eng->q.X, qb, n));
+    }
+    if (eng->u.on && d.in_uv) {
+        std::vector<double> ub[3], vb[3];
+        for (auto& b : ub) b.assign((size_t)n, 0.);
+        for (auto& b : vb) b.assign((size_t)n, 0.);
+        std::string e = read_restart(dir + "/u.in", d.nx, d.ny, d.nz, 3, ub);
+        if (e.empty()) e = read_restart(dir + "/v.in", d.nx, d.ny, d.nz, 3, vb);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        GF_TRY(upload_vec(eng, eng->u.X, ub, n));
+        GF_TRY(upload_vec(eng, eng->v.X, vb, n));
+    }
+    if (eng->E.on && d.in_em) {
+        const char* names[6] = {"Ex_Yee.in", "Ey_Yee.in", "Ez_Yee.in", "Hx_Yee.in", "Hy_Yee.in", "Hz_Yee.in"};
+        for (int f = 0; f < 6; f++) {
+            const Field3& F = f < 3 ? eng->E : eng->H;
+            const int c = f % 3;
+            long dimx = d.nx, dimy = d.ny, dimz = d.nz;
+            if (f < 3) { dimx += (c != 0); dimy += (c != 1); dimz += (c != 2); }
+            else { dimx += (c == 0); dimy += (c == 1); dimz += (c == 2); }
+            std::vector<double> one((size_t)(dimx * dimy * dimz), 0.);
+            std::string e = read_restart(dir + "/" + names[f], dimx, dimy, dimz, 1, &one);
+            if (!e.empty()) { eng->err = e; return GF_EIO; }
+            GF_CU(cudaMemcpy(F.X[c], one.data(), sizeof(double) * one.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    if (d.in_Hstat && eng->Hstat[0]) {
+        for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+        std::string e = read_restart(dir + "/Hstat.in", d.nx, d.ny, d.nz, 3, buf);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        GF_TRY(upload_vec(eng, eng->Hstat, buf, n));
+    }
+    if (d.in_Estat && eng->Estat[0]) {
+        for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+        std::string e = read_restart(dir + "/Estat.in", d.nx, d.ny, d.nz, 3, buf);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        GF_TRY(upload_vec(eng, eng->Estat, buf, n));
+    }
+    if (d.read_Hext_nonunif) {
+        for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+        std::string e = read_restart(dir + "/Hext_nonunif.in", d.nx, d.ny, d.nz, 3, buf);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        GF_TRY(upload_vec(eng, eng->Hnu, buf, n));
+    }
+    return GF_OK;
+}
+
+int create(gf_engine* eng, const std::string& dir, int device) {
+    std::string e = read_deck(dir, eng->deck);
+    if (!e.empty()) { eng->err = e; return GF_EIO; }
+    const Deck& d = eng->deck;
+    e = unsupported(d);
+    if (!e.empty()) { eng->err = e; return GF_EUNSUPPORTED; }
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { eng->err = "no CUDA device"; return GF_ENODEV; }
+    if (device < 0) GF_CU(cudaGetDevice(&device));
+    GF_CU(cudaSetDevice(device));
+    eng->device = device;
+    cudaDeviceProp prop;
+    GF_CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) { eng->err = std::string("device ") + prop.name + " is not sm_100 or newer"; return GF_ENODEV; }
+    GF_CU(cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking));
+
+    build_params(eng);
+    const Params& P = eng->P;
+    const long n = P.n;
+
+    // materials
+    GF_TRY(dalloc_n(eng, &eng->mid, (size_t)n));
+    GF_CU(cudaMemcpyAsync(eng->mid, d.material_cell.data(), (size_t)n, cudaMemcpyHostToDevice, eng->stream));
+    std::vector<DevMat> dm(d.mats.size());
+    for (size_t i = 0; i < d.mats.size(); i++) dm[i] = make_devmat(d.mats[i], d.dt);
+    GF_TRY(dalloc_n(eng, &eng->mats, dm.size()));
+    GF_CU(cudaMemcpyAsync(eng->mats, dm.data(), sizeof(DevMat) * dm.size(), cudaMemcpyHostToDevice, eng->stream));
+    {
+        LLGTables t;
+        std::memset(&t, 0, sizeof(t));
+        for (size_t a = 0; a < d.mats.size(); a++)
+            for (size_t b = 0; b < d.mats.size(); b++) {
+                const double A1 = d.mats[a].Aex, A2 = d.mats[b].Aex;
+                t.Aij[a + 1][b + 1] = (A1 + A2 != 0.) ? 2. * A1 * A2 / (A1 + A2) : 0.;
+            }
+        GF_TRY(dalloc_n(eng, &eng->llg_tab, 1));
+        GF_CU(cudaMemcpy(eng->llg_tab, &t, sizeof(t), cudaMemcpyHostToDevice));
+    }
+    GF_TRY(dalloc_n(eng, &eng->drive, (size_t)kDriveCap));
+    GF_CU(cudaMallocHost(&eng->drive_host, sizeof(StepDrive) * kDriveCap));
+    GF_TRY(dalloc_n(eng, &eng->step_ctr, 1));
+    {
+        std::vector<double> kf((size_t)P.nz, 0.);
+        if (d.jf_input) {
+            const double PI = kPi;
+            const long Jf_nz = (long)(d.jf_k1 - d.jf_k0 + 1);
+            for (long k = (long)d.jf_k0; k <= (long)d.jf_k1 && k < P.nz; k++) {
+                const double sp = PI / (static_cast<double>(Jf_nz) * P.dz) * (static_cast<double>(k - (long)d.jf_k0) + 0.5) * P.dz;
+                kf[(size_t)k] = (d.jf_type == 1) ? std::sin(sp) : std::cos(sp);
+            }
+        }
+        GF_TRY(dalloc_n(eng, &eng->jf_kfac, (size_t)P.nz));
+        GF_CU(cudaMemcpy(eng->jf_kfac, kf.data(), sizeof(double) * kf.size(), cudaMemcpyHostToDevice));
+    }
+
+    // state fields
+    if (d.any_fm) GF_TRY(alloc_field(eng, eng->m, n, n, n));
+    if (d.any_fe) { GF_TRY(alloc_field(eng, eng->p, n, n, n)); GF_TRY(alloc_field(eng, eng->q, n, n, n)); }
+    if (d.elastodynamics) { GF_TRY(alloc_field(eng, eng->u, n, n, n)); GF_TRY(alloc_field(eng, eng->v, n, n, n)); }
+    if (d.em_dynamic) {
+        const long nx = P.nx, ny = P.ny, nz = P.nz;
+        GF_TRY(alloc_field(eng, eng->E, nx * (ny + 1) * (nz + 1), (nx + 1) * ny * (nz + 1), (nx + 1) * (ny + 1) * nz));
+        GF_TRY(alloc_field(eng, eng->H, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)));
+    }
+    for (int a = 0; a < 3; a++) {
+        if (P.em_fromM) GF_TRY(dalloc_n(eng, &eng->dm[a], (size_t)n));
+        if (d.elastodynamics) {
+            GF_TRY(dalloc_n(eng, &eng->force[a], (size_t)n));
+            GF_TRY(dalloc_n(eng, &eng->force_store[a], (size_t)n));
+        }
+        if (d.any_fm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
+        if (d.any_fe) GF_TRY(dalloc_n(eng, &eng->Estat[a], (size_t)n));
+        if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_n(eng, &eng->Hnu[a], (size_t)n));
+    }
+    if (d.elastodynamics || d.elasto_on) {
+        for (int a = 0; a < 6; a++) {
+            GF_TRY(dalloc_n(eng, &eng->eps_g[a], (size_t)n));
+            if (P.rot) GF_TRY(dalloc_n(eng, &eng->eps_c[a], (size_t)n)); else eng->eps_c[a] = eng->eps_g[a];
+            GF_TRY(dalloc_n(eng, &eng->eig_c[a], (size_t)n));
+            if (P.rot) GF_TRY(dalloc_n(eng, &eng->eig_g[a], (size_t)n)); else eng->eig_g[a] = eng->eig_c[a];
+        }
+    }
+    if (d.elastodynamics) {
+        const size_t plane = (size_t)P.nx * P.ny;
+        GF_TRY(dalloc_n(eng, &eng->liao_hist, 4 * 12 * plane));
+        GF_TRY(dalloc_n(eng, &eng->liao_last, 3 * plane));
+    }
+    GF_TRY(dalloc_n(eng, &eng->scratch, (size_t)6 * n + 16384));
+    GF_TRY(dalloc_n(eng, &eng->flag, 1));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+
+    GF_TRY(initial_state(eng, dir));
+    GF_TRY(setup_demag(eng));
+    build_io(eng);
+
+    // initial static field (main.cpp:135-146 and 229-239)
+    if (!d.in_Hstat) GF_TRY(static_field_now(eng));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int ensure_graphs(gf_engine* eng) {
+    if (eng->graphs_ready) return GF_OK;
+    for (int par = 0; par < 2; par++) {
+        GF_CU(cudaStreamBeginCapture(eng->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(eng, par);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(eng->stream, &g);
+        if (rc != GF_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ce != cudaSuccess) { eng->err = std::string("stream capture: ") + cudaGetErrorString(ce); return GF_ECUDA; }
+        eng->graph[par] = g;
+        GF_CU(cudaGraphInstantiate(&eng->gexec[par], g, 0));
+    }
+    eng->graphs_ready = true;
+    return GF_OK;
+}
+
+int advance(gf_engine* eng, uint64_t nsteps, bool use_graph) {
+    if (use_graph) GF_TRY(ensure_graphs(eng));
+    uint64_t done = 0;
+    while (done < nsteps) {
+        const uint64_t chunk = std::min<uint64_t>(nsteps - done, (uint64_t)kDriveCap / 2);
+        // the device drive ring holds kDriveCap steps; steps are written at
+        // slot (step & (kDriveCap-1)); wait for earlier users of the pinned buffer
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        for (uint64_t s = 0; s < chunk; s++) step_drive(eng, eng->drive_host[s]);
+        const uint64_t first = eng->steps_done + done;
+        uint64_t s = 0;
+        while (s < chunk) {
+            const uint64_t slot = (first + s) & (uint64_t)(kDriveCap - 1);
+            const uint64_t run = std::min<uint64_t>(chunk - s, (uint64_t)kDriveCap - slot);
+            GF_CU(cudaMemcpyAsync(eng->drive + slot, eng->drive_host + s, sizeof(StepDrive) * run, cudaMemcpyHostToDevice, eng->stream));
+            s += run;
+        }
+        for (uint64_t k = 0; k < chunk; k++) {
+            const int parity = (int)((first + k) & 1ull);
+            if (use_graph) GF_CU(cudaGraphLaunch(eng->gexec[parity], eng->stream));
+            else GF_TRY(enqueue_step(eng, parity));
+        }
+        done += chunk;
+    }
+    eng->steps_done += nsteps;
+    return GF_OK;
+}
+
+// current step value of a 3-component state field
+double* const* cur(gf_engine* eng, Field3& f) { return (eng->steps_done & 1ull) ? f.A : f.X; }
+
+int device_sum(gf_engine* eng, const double* in, long n, double* out) {
+    cudaStream_t st = eng->stream;
+    double* p1 = eng->scratch + (size_t)6 * eng->P.n;        // 8192
+    double* p2 = p1 + 8192;                                   // 64
+    double* p3 = p2 + 64;                                     // 1
+    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, in, n, p1, 8192L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
+    GF_CU(cudaMemcpyAsync(out, p3, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GF_CU(cudaStreamSynchronize(st));
+    return GF_OK;
+}
+
+int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vector<long>& lens, bool& writable) {
+    const Params& P = eng->P;
+    writable = true;
+    ptrs.clear(); lens.clear();
+    auto add3 = [&](double* const* p, Field3* f) {
+        for (int a = 0; a < 3; a++) { ptrs.push_back(p[a]); lens.push_back(f ? f->len[a] : P.n); }
+    };
+    switch (field) {
+        case GF_FIELD_M: if (!eng->m.on) break; add3(cur(eng, eng->m), &eng->m); break;
+        case GF_FIELD_P: if (!eng->p.on) break; add3(cur(eng, eng->p), &eng->p); break;
+        case GF_FIELD_Q: if (!eng->q.on) break; add3(cur(eng, eng->q), &eng->q); break;
+        case GF_FIELD_U: if (!eng->u.on) break; add3(cur(eng, eng->u), &eng->u); break;
+        case GF_FIELD_V: if (!eng->v.on) break; add3(cur(eng, eng->v), &eng->v); break;
+        case GF_FIELD_EX: case GF_FIELD_EY: case GF_FIELD_EZ:
+            if (!eng->E.on) break;
+            ptrs.push_back(cur(eng, eng->E)[field - GF_FIELD_EX]); lens.push_back(eng->E.len[field - GF_FIELD_EX]); break;
+        case GF_FIELD_HX: case GF_FIELD_HY: case GF_FIELD_HZ:
+            if (!eng->H.on) break;
+            ptrs.push_back(cur(eng, eng->H)[field - GF_FIELD_HX]); lens.push_back(eng->H.len[field - GF_FIELD_HX]); break;
+        case GF_FIELD_HSTAT: if (!eng->Hstat[0]) break; add3(eng->Hstat, nullptr); break;
+        case GF_FIELD_ESTAT: if (!eng->Estat[0]) break; add3(eng->Estat, nullptr); break;
+        case GF_FIELD_E_CELL: case GF_FIELD_H_CELL: {
+            if (!eng->E.on) break;
+            writable = false;
+            double* s = eng->scratch;
+            F3 Ec{{s, s + P.n, s + 2 * P.n}}, Hc{{s + 3 * P.n, s + 4 * P.n, s + 5 * P.n}};
+            GF_CU(launch(k_em_cell, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
+                         f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc));
+            double* base = (field == GF_FIELD_E_CELL) ? s : s + 3 * P.n;
+            for (int a = 0; a < 3; a++) { ptrs.push_back(base + a * P.n); lens.push_back(P.n); }
+            break;
+        }
+        case GF_FIELD_STRAIN:
+            if (!eng->eps_g[0]) break;
+            writable = false;
+            for (int a = 0; a < 6; a++) { ptrs.push_back(eng->eps_g[a]); lens.push_back(P.n); }
+            break;
+        default: break;
+    }
+    if (ptrs.empty()) { eng->err = "field " + std::to_string(field) + " is not present in this run"; return GF_EINVAL; }
+    return GF_OK;
+}
+
+int check(gf_engine* e) {
+    if (!e) return GF_EINVAL;
+    return GF_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out) {
+    if (!deck_dir || !out) { g_create_err = "null argument"; return GF_EINVAL; }
+    *out = nullptr;
+    gf_engine* eng = new gf_engine();
+    int rc = create(eng, deck_dir, device);
+    if (rc != GF_OK) {
+        g_create_err = eng->err;
+        gf_destroy(eng);
+        return rc;
+    }
+    *out = eng;
+    return GF_OK;
+}
+
+int gf_advance(gf_engine* e, uint64_t nsteps) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    GF_CU(cudaSetDevice(eng->device));
+    return advance(e, nsteps, true);
+}
+
+int gf_advance_eager(gf_engine* e, uint64_t nsteps) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    GF_CU(cudaSetDevice(eng->device));
+    return advance(e, nsteps, false);
+}
+
+int gf_average(gf_engine* e, int obs, double out3[3]) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!out3) { eng->err = "null output"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    double* const* src = nullptr;
+    double denom = 1.;
+    switch (obs) {
+        case GF_OBS_M: if (!eng->m.on) break; src = cur(eng, eng->m); denom = (double)eng->deck.NFM; break;
+        case GF_OBS_P: if (!eng->p.on) break; src = cur(eng, eng->p); denom = (double)eng->deck.NFE; break;
+        case GF_OBS_U: if (!eng->u.on) break; src = cur(eng, eng->u); denom = (double)eng->P.n; break;
+        default: break;
+    }
+    if (!src) { eng->err = "observable " + std::to_string(obs) + " is not present in this run"; return GF_EINVAL; }
+    for (int a = 0; a < 3; a++) {
+        double s = 0.;
+        GF_TRY(device_sum(eng, src[a], eng->P.n, &s));
+        out3[a] = s / denom;
+    }
+    return GF_OK;
+}
+
+int gf_probe_em(gf_engine* e, int64_t i, int64_t j, int64_t k, double e3[3], double h3[3]) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    const Params& P = eng->P;
+    if (!eng->E.on) { eng->err = "no Maxwell fields in this run"; return GF_EINVAL; }
+    if (i < 0 || j < 0 || k < 0 || i >= P.nx || j >= P.ny || k >= P.nz) { eng->err = "probe outside the grid"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    std::vector<double*> ptrs; std::vector<long> lens; bool w;
+    GF_TRY(field_ptrs(eng, GF_FIELD_E_CELL, ptrs, lens, w));
+    const long c = (i * P.ny + j) * P.nz + k;
+    for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&e3[a], ptrs[a] + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
+    double* hb = eng->scratch + 3 * P.n;
+    for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&h3[a], hb + a * P.n + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    const Params& P = eng->P;
+    int64_t dx = P.nx, dy = P.ny, dz = P.nz;
+    size_t ncomp = 3;
+    if (field >= GF_FIELD_EX && field <= GF_FIELD_EZ) { int c = field - GF_FIELD_EX; dx += (c != 0); dy += (c != 1); dz += (c != 2); ncomp = 1; }
+    else if (field >= GF_FIELD_HX && field <= GF_FIELD_HZ) { int c = field - GF_FIELD_HX; dx += (c == 0); dy += (c == 1); dz += (c == 2); ncomp = 1; }
+    else if (field == GF_FIELD_STRAIN) ncomp = 6;
+    else if (field < 0 || field >= GF_FIELD_COUNT) { eng->err = "unknown field"; return GF_EINVAL; }
+    if (dims3) { dims3[0] = dx; dims3[1] = dy; dims3[2] = dz; }
+    if (count) *count = ncomp * (size_t)(dx * dy * dz);
+    return GF_OK;
+}
+
+static int copy_field(gf_engine* eng, int field, double* buf, size_t count, bool to_host_or_dev_out, cudaMemcpyKind kind, bool sync) {
+    std::vector<double*> ptrs; std::vector<long> lens; bool writable;
+    GF_TRY(field_ptrs(eng, field, ptrs, lens, writable));
+    size_t total = 0;
+    for (long l : lens) total += (size_t)l;
+    if (count != total) { eng->err = "field " + std::to_string(field) + " holds " + std::to_string(total) + " doubles, caller gave " + std::to_string(count); return GF_EINVAL; }
+    if (!to_host_or_dev_out && !writable) { eng->err = "field is read-only"; return GF_EINVAL; }
+    size_t off = 0;
+    for (size_t a = 0; a < ptrs.size(); a++) {
+        if (to_host_or_dev_out) GF_CU(cudaMemcpyAsync(buf + off, ptrs[a], sizeof(double) * lens[a], kind, eng->stream));
+        else GF_CU(cudaMemcpyAsync(ptrs[a], buf + off, sizeof(double) * lens[a], kind, eng->stream));
+        off += (size_t)lens[a];
+    }
+    if (sync) GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int gf_download(gf_engine* e, int field, double* host, size_t count) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!host) { eng->err = "null buffer"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    return copy_field(e, field, host, count, true, cudaMemcpyDeviceToHost, true);
+}
+
+int gf_upload(gf_engine* e, int field, const double* host, size_t count) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!host) { eng->err = "null buffer"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    return copy_field(e, field, const_cast<double*>(host), count, false, cudaMemcpyHostToDevice, true);
+}
+
+int gf_download_device(gf_engine* e, int field, double* dev, size_t count) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!dev) { eng->err = "null buffer"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    return copy_field(e, field, dev, count, true, cudaMemcpyDeviceToDevice, false);
+}
+
+int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!dev) { eng->err = "null buffer"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    return copy_field(e, field, const_cast<double*>(dev), count, false, cudaMemcpyDeviceToDevice, false);
+}
+
+int gf_get_info(gf_engine* e, gf_info* info) {
+    GF_TRY(check(e));
+    if (!info) { e->err = "null info"; return GF_EINVAL; }
+    const Deck& d = e->deck;
+    std::memset(info, 0, sizeof(*info));
+    info->nx = (int32_t)d.nx; info->ny = (int32_t)d.ny; info->nz = (int32_t)d.nz;
+    info->dx = d.dx; info->dy = d.dy; info->dz = d.dz; info->dt = d.dt;
+    info->time = e->t_host; info->step = e->steps_done; info->deck_steps = d.steps;
+    info->n_materials = (int32_t)d.num_materials;
+    info->fm = d.any_fm; info->afm = d.any_afm; info->fe = d.any_fe;
+    info->elastic = d.elastodynamics; info->em = d.em_dynamic; info->demag_per_stage = e->demag_per_stage;
+    info->n_fm = d.NFM; info->n_afm = d.NAFM; info->n_fe = d.NFE;
+    info->device_bytes = e->bytes;
+    info->launches_per_step = e->launches_per_step;
+    return GF_OK;
+}
+
+int gf_profile_steps(gf_engine* e, uint64_t nsteps, gf_kernel_time* out, int max_records, int* n_records) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!out || !n_records || max_records <= 0) { eng->err = "null output"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    eng->profiling = true;
+    eng->prof.clear();
+    eng->ev_used = 0;
+    int rc = advance(e, nsteps, false);
+    eng->profiling = false;
+    if (rc != GF_OK) return rc;
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    int n = 0;
+    for (auto& r : eng->prof) {
+        float ms = 0.f;
+        GF_CU(cudaEventElapsedTime(&ms, r.a, r.b));
+        int slot = -1;
+        for (int q = 0; q < n; q++) if (std::strncmp(out[q].name, r.name, sizeof(out[q].name)) == 0) { slot = q; break; }
+        if (slot < 0) {
+            if (n == max_records) continue;
+            slot = n++;
+            std::memset(&out[slot], 0, sizeof(out[slot]));
+            std::strncpy(out[slot].name, r.name, sizeof(out[slot].name) - 1);
+        }
+        out[slot].launches += 1;
+        out[slot].total_ms += (double)ms;
+    }
+    *n_records = n;
+    eng->prof.clear();
+    return GF_OK;
+}
+
+int gf_synchronize(gf_engine* e) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+void* gf_stream(gf_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+int gf_check_finite(gf_engine* e) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    GF_CU(cudaSetDevice(eng->device));
+    struct Named { const char* name; Field3* f; };
+    Named fs[] = {{"m", &eng->m}, {"p", &eng->p}, {"q", &eng->q}, {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H}};
+    for (auto& nf : fs) {
+        if (!nf.f->on) continue;
+        for (int a = 0; a < 3; a++) {
+            GF_CU(cudaMemsetAsync(eng->flag, 0, sizeof(int), eng->stream));
+            GF_CU(launch(k_check_finite, dim3(296), dim3(256), 0, eng->stream, (const double*)cur(eng, *nf.f)[a], nf.f->len[a], eng->flag));
+            int h = 0;
+            GF_CU(cudaMemcpyAsync(&h, eng->flag, sizeof(int), cudaMemcpyDeviceToHost, eng->stream));
+            GF_CU(cudaStreamSynchronize(eng->stream));
+            if (h) { eng->err = std::string("non-finite value in field ") + nf.name + " component " + std::to_string(a); return GF_ENAN; }
+        }
+    }
+    return GF_OK;
+}
+
+const char* gf_last_error(const gf_engine* e) {
+    if (!e) return g_create_err.c_str();
+    return e->err.c_str();
+}
+
+void gf_destroy(gf_engine* e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (int p = 0; p < 2; p++) {
+        if (e->gexec[p]) cudaGraphExecDestroy(e->gexec[p]);
+        if (e->graph[p]) cudaGraphDestroy(e->graph[p]);
+    }
+    if (e->plans) { cufftDestroy(e->plan_r2c); cufftDestroy(e->plan_c2r); }
+    for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
+    for (void* p : e->allocs) cudaFree(p);
+    if (e->drive_host) cudaFreeHost(e->drive_host);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* gf_version(void) { return "goferro_b200 0.1 (FP64 parity path, sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,159 @@
+// Ferroelectric second-order TDGL stage kernel (FP64).
+//
+// One thread per cell: q-increment of ferroelectric_system::get_dq_RK{1..4}
+// (ferroelectric_solver.cpp:534-842: 8th-order Landau polynomial,
+// electrostriction, gradient energy with the mirror interface condition of
+// get_laplacian_p_local :3-131, static, external and Maxwell fields, damping),
+// p-increment of get_dp_RK* (:1786-1832) and the RK4 combination of
+// update_q*/update_p* (:1835-1999), fused in one pass.  Integer powers are
+// evaluated by multiplication instead of pow().
+#pragma once
+
+#include "gf_state.cuh"
+
+namespace gf {
+
+__device__ inline bool is_fe(const DevMat* mats, uint8_t id) {
+    return id != 0 && (mats[id - 1].flags & MF_FE);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long nyz = (long)P.ny * P.nz;
+    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const uint8_t id = io.mid[c];
+    double dq[3] = {0., 0., 0.};
+
+    if (is_fe(io.mats, id)) {
+        const DevMat& mt = io.mats[id - 1];
+        const double pxg = io.p_in.c[0][c], pyg = io.p_in.c[1][c], pzg = io.p_in.c[2][c];
+
+        // ---- Laplacian with mirror condition at FE interfaces ----
+        const long ib = (i == 0) ? P.nx - 1 : i - 1, iF = (i == P.nx - 1) ? 0 : i + 1;
+        const long jb = (j == 0) ? P.ny - 1 : j - 1, jF = (j == P.ny - 1) ? 0 : j + 1;
+        const long kb = (k == 0) ? P.nz - 1 : k - 1, kF = (k == P.nz - 1) ? 0 : k + 1;
+        const long nb[6] = {cid(P, ib, j, k), cid(P, iF, j, k), cid(P, i, jb, k),
+                            cid(P, i, jF, k), cid(P, i, j, kb), cid(P, i, j, kF)};
+        const bool surf[6] = {(i == 0 && !P.per_x) || !is_fe(io.mats, io.mid[nb[0]]),
+                              (i == P.nx - 1 && !P.per_x) || !is_fe(io.mats, io.mid[nb[1]]),
+                              (j == 0 && !P.per_y) || !is_fe(io.mats, io.mid[nb[2]]),
+                              (j == P.ny - 1 && !P.per_y) || !is_fe(io.mats, io.mid[nb[3]]),
+                              (k == 0 && !P.per_z) || !is_fe(io.mats, io.mid[nb[4]]),
+                              (k == P.nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
+        const double h[3] = {P.dx, P.dy, P.dz};
+        double lap[3];   // sum of the three second derivatives per component
+        for (int a = 0; a < 3; a++) {
+            const double pc = io.p_in.c[a][c];
+            double d2[3];
+            for (int dir = 0; dir < 3; dir++) {
+                const double pb = surf[2 * dir] ? pc : io.p_in.c[a][nb[2 * dir]];
+                const double pf = surf[2 * dir + 1] ? pc : io.p_in.c[a][nb[2 * dir + 1]];
+                d2[dir] = (pf - 2. * pc + pb) / h[dir] / h[dir];
+            }
+            lap[a] = d2[0] + d2[1] + d2[2];
+        }
+
+        double px, py, pz;
+        glb2crt(P, pxg, pyg, pzg, px, py, pz);
+
+        double exx = 0, eyy = 0, ezz = 0, eyz = 0, exz = 0, exy = 0;
+        double exx0 = 0, eyy0 = 0, ezz0 = 0, eyz0 = 0, exz0 = 0, exy0 = 0;
+        if (P.elasto_on) {
+            exx = io.eps_c[0][c]; eyy = io.eps_c[1][c]; ezz = io.eps_c[2][c];
+            eyz = io.eps_c[3][c]; exz = io.eps_c[4][c]; exy = io.eps_c[5][c];
+            if (P.elasto_back) {
+                exx0 = io.eig_c[0][c]; eyy0 = io.eig_c[1][c]; ezz0 = io.eig_c[2][c];
+                eyz0 = io.eig_c[3][c]; exz0 = io.eig_c[4][c]; exy0 = io.eig_c[5][c];
+            }
+        }
+
+        const double px2 = px * px, py2 = py * py, pz2 = pz * pz;
+        const double px3 = px2 * px, py3 = py2 * py, pz3 = pz2 * pz;
+        const double px4 = px2 * px2, py4 = py2 * py2, pz4 = pz2 * pz2;
+        const double px5 = px4 * px, py5 = py4 * py, pz5 = pz4 * pz;
+        const double px6 = px4 * px2, py6 = py4 * py2, pz6 = pz4 * pz2;
+        const double px7 = px6 * px, py7 = py6 * py, pz7 = pz6 * pz;
+        const double fm = mt.fe_coef;
+
+        const double qxc = fm * (2. * mt.a1 * px + 4. * mt.a11 * px3
+            + 2. * mt.a12 * (py2 + pz2) * px
+            + 6. * mt.a111 * px5
+            + 4. * mt.a112 * px3 * (py2 + pz2)
+            + 2. * mt.a112 * (py4 + pz4) * px
+            + 2. * mt.a123 * px * py2 * pz2
+            + 8. * mt.a1111 * px7
+            + 2. * mt.a1112 * px * (py6 + pz6 + 3. * px4 * (py2 + pz2))
+            + 4. * mt.a1122 * px3 * (py4 + pz4)
+            + 2. * mt.a1123 * px * py2 * pz2 * (2. * px2 + py2 + pz2)
+            + (mt.tv1 * (exx0 - exx) + mt.tv2 * (eyy0 - eyy + ezz0 - ezz)) * px
+            + mt.tv3 * ((exy0 - exy) * py + (exz0 - exz) * pz));
+        const double qyc = fm * (2. * mt.a1 * py + 4. * mt.a11 * py3
+            + 2. * mt.a12 * (pz2 + px2) * py
+            + 6. * mt.a111 * py5
+            + 4. * mt.a112 * py3 * (px2 + pz2)
+            + 2. * mt.a112 * (px4 + pz4) * py
+            + 2. * mt.a123 * py * px2 * pz2
+            + 8. * mt.a1111 * py7
+            + 2. * mt.a1112 * py * (px6 + pz6 + 3. * py4 * (px2 + pz2))
+            + 4. * mt.a1122 * py3 * (px4 + pz4)
+            + 2. * mt.a1123 * py * px2 * pz2 * (px2 + 2. * py2 + pz2)
+            + (mt.tv1 * (eyy0 - eyy) + mt.tv2 * (exx0 - exx + ezz0 - ezz)) * py
+            + mt.tv3 * ((exy0 - exy) * px + (eyz0 - eyz) * pz));
+        const double qzc = fm * (2. * mt.a1 * pz + 4. * mt.a11 * pz3
+            + 2. * mt.a12 * (py2 + px2) * pz
+            + 6. * mt.a111 * pz5
+            + 4. * mt.a112 * pz3 * (py2 + px2)
+            + 2. * mt.a112 * (py4 + px4) * pz
+            + 2. * mt.a123 * pz * py2 * px2
+            + 8. * mt.a1111 * pz7
+            + 2. * mt.a1112 * pz * (py6 + px6 + 3. * pz4 * (py2 + px2))
+            + 4. * mt.a1122 * pz3 * (py4 + px4)
+            + 2. * mt.a1123 * pz * px2 * py2 * (px2 + py2 + 2. * pz2)
+            + (mt.tv1 * (ezz0 - ezz) + mt.tv2 * (exx0 - exx + eyy0 - eyy)) * pz
+            + mt.tv3 * ((exz0 - exz) * px + (eyz0 - eyz) * py));
+        double gx, gy, gz;
+        crt2glb(P, qxc, qyc, qzc, gx, gy, gz);
+
+        const StageDrive& dr = stage_drive(io, S);
+        const double g[3] = {gx, gy, gz};
+        for (int a = 0; a < 3; a++)
+            dq[a] = g[a] + fm * (-1. * mt.G11 * lap[a] - io.Estat.c[a][c] - dr.Eext[a]) + mt.fe_damp * io.q_in.c[a][c];
+
+        if (P.em_back_P) {
+            // cell-centred Maxwell E of the stage state (EMdynamic_solver.cpp:3813-3826)
+            const long ny1 = P.ny + 1, nz1 = P.nz + 1;
+            const long ex = (i * ny1 + j) * nz1 + k;
+            const long ey = (i * P.ny + j) * nz1 + k;
+            const long ez = (i * ny1 + j) * P.nz + k;
+            const double Ecx = (io.E_in.c[0][ex] + io.E_in.c[0][ex + nz1] + io.E_in.c[0][ex + 1] + io.E_in.c[0][ex + nz1 + 1]) / 4.;
+            const double Ecy = (io.E_in.c[1][ey] + io.E_in.c[1][ey + P.ny * nz1] + io.E_in.c[1][ey + 1] + io.E_in.c[1][ey + P.ny * nz1 + 1]) / 4.;
+            const double Ecz = (io.E_in.c[2][ez] + io.E_in.c[2][ez + ny1 * P.nz] + io.E_in.c[2][ez + P.nz] + io.E_in.c[2][ez + ny1 * P.nz + P.nz]) / 4.;
+            dq[0] = dq[0] - fm * Ecx;
+            dq[1] = dq[1] - fm * Ecy;
+            dq[2] = dq[2] - fm * Ecz;
+        }
+    }
+
+    // ---- RK4 combination for q and p (dp = q_stage * dt) ----
+    for (int a = 0; a < 3; a++) {
+        const double dp = io.q_in.c[a][c] * P.dt;
+        const double qx = io.q_x.c[a][c], px = io.p_x.c[a][c];
+        if (S == 0) {
+            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = qx + dq[a] / 6.;
+            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = px + dp / 6.;
+        } else if (S == 1) {
+            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 3.;
+            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 3.;
+        } else if (S == 2) {
+            io.q_out.c[a][c] = qx + dq[a];       io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 3.;
+            io.p_out.c[a][c] = px + dp;          io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 3.;
+        } else {
+            io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 6.;
+            io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 6.;
+        }
+    }
+}
+
+}  // namespace gf

@@ -1,0 +1,20 @@
+// Kernel launch helper: every launch of the engine goes through launch(), so
+// that launch failures are checked in one place.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace gf {
+
+inline unsigned blocks_for(long n, int threads) {
+    long b = (n + threads - 1) / threads;
+    return (unsigned)(b > 0 ? b : 1);
+}
+
+template <class Kernel, class... Args>
+inline cudaError_t launch(Kernel k, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    k<<<grid, block, smem, s>>>(args...);
+    return cudaGetLastError();
+}
+
+}  // namespace gf

@@ -1,0 +1,62 @@
+// Device pointers that one RK stage of one step reads and writes.
+//
+// Every state field F keeps four device arrays per component:
+//   X  — value at the start of the step (the reference's F_glb),
+//   A  — RK4 accumulator; after the last stage it holds the new step value,
+//        and the engine swaps the roles of X and A (two captured graphs,
+//        one per parity of the step counter),
+//   S0, S1 — stage states (the reference's F_glb_store), ping-ponged so a
+//        stencil can read stage s while stage s+1 is written.
+// Stage s reads `in` (X for s=0, S0, S1, S0) and writes `out` (S0, S1, S0,
+// and for the last stage the A buffer in place).  This replaces the
+// reference's five arrays per component (F_glb, F_glb_store, dF_rk1..4).
+#pragma once
+
+#include "gf_common.cuh"
+
+namespace gf {
+
+struct F3 { double* c[3]; };
+
+struct StageIO {
+    // ferromagnet m and its stage increment (read by the Maxwell H update)
+    F3 m_in, m_x, m_acc, m_out, dm;
+    // ferroelectric p and q = dp/dt
+    F3 p_in, p_x, p_acc, p_out, q_in, q_x, q_acc, q_out;
+    // elastic displacement u and velocity v
+    F3 u_in, u_x, u_acc, u_out, v_in, v_x, v_acc, v_out;
+    F3 force, force_store;
+    // Yee E and H: component c of E lives on the c-edges, of H on the c-faces
+    F3 E_in, E_x, E_acc, E_out, H_in, H_x, H_acc, H_out;
+    // static and external fields
+    F3 Hstat, Estat, Hnu;
+    // strain scratch written by the strain kernel each stage (6 Voigt-order
+    // components xx yy zz yz xz xy): dynamic strain (global / crystal frame)
+    // and dynamic eigenstrain (global / crystal frame)
+    double* eps_g[6];
+    double* eps_c[6];
+    double* eig_g[6];
+    double* eig_c[6];
+    // optional static inputs (null when absent): static strain and static
+    // eigenstrain in the crystal frame
+    const double* eps0_c[6];
+    const double* eig0_c[6];
+    // Liao absorbing-boundary history: 4 slots of planes k=1..4 of u
+    // (3 comps), plus the last boundary value written on plane 0
+    double* liao_hist;
+    double* liao_last;
+    // geometry / materials / time
+    const uint8_t* mid;
+    const DevMat* mats;
+    const StepDrive* drive;
+    const unsigned long long* step;   // index of the step being computed (0-based)
+    unsigned long long drive_mask;    // drive ring holds drive_mask+1 steps
+    const double* jf_kfac;            // per-k spatial factor of J_f types 1,2
+};
+
+// time-dependent values of RK stage s of the step being computed
+__device__ inline const StageDrive& stage_drive(const StageIO& io, int s) {
+    return io.drive[(*io.step) & io.drive_mask].st[s];
+}
+
+}  // namespace gf

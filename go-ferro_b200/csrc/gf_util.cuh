@@ -1,0 +1,55 @@
+// Small utility kernels: step counter, deterministic FP64 sums, health
+// check, cell-centred E/H for output.
+#pragma once
+
+#include "gf_state.cuh"
+
+namespace gf {
+
+__global__ void k_step_inc(unsigned long long* step) { *step = *step + 1ull; }
+
+// Deterministic sum: thread t of T adds elements t, t+T, t+2T, ... of
+// `in` (length n) in index order and writes partial[t].  Applied three times
+// (n -> 8192 -> 64 -> 1) the result depends only on n, never on scheduling.
+__global__ void k_sum_stride(const double* __restrict__ in, long n, double* __restrict__ partial, long T) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    double acc = 0.;
+    for (long i = t; i < n; i += T) acc = acc + in[i];
+    partial[t] = acc;
+}
+
+// flag := 1 if any element of in[0..n) is not finite
+__global__ void k_check_finite(const double* __restrict__ in, long n, int* flag) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long T = (long)gridDim.x * blockDim.x;
+    for (long i = t; i < n; i += T) {
+        const double v = in[i];
+        if (!(v - v == 0.)) { *flag = 1; return; }
+    }
+}
+
+// cell-centred E (4-edge means) and H (2-face means) of the current step
+// value, as update_DE_cell / update_DH_cell compute them
+// (EMdynamic_solver.cpp:3780-3826)
+__global__ void k_em_cell(Params P, F3 E, F3 H, F3 Ec, F3 Hc) {
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long nyz = (long)P.ny * P.nz;
+    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const long ny1 = P.ny + 1, nz1 = P.nz + 1;
+    const long ex = (i * ny1 + j) * nz1 + k;
+    const long ey = (i * P.ny + j) * nz1 + k;
+    const long ez = (i * ny1 + j) * P.nz + k;
+    Ec.c[0][c] = (E.c[0][ex] + E.c[0][ex + nz1] + E.c[0][ex + 1] + E.c[0][ex + nz1 + 1]) / 4.;
+    Ec.c[1][c] = (E.c[1][ey] + E.c[1][ey + P.ny * nz1] + E.c[1][ey + 1] + E.c[1][ey + P.ny * nz1 + 1]) / 4.;
+    Ec.c[2][c] = (E.c[2][ez] + E.c[2][ez + ny1 * P.nz] + E.c[2][ez + P.nz] + E.c[2][ez + ny1 * P.nz + P.nz]) / 4.;
+    const long hx0 = (i * P.ny + j) * P.nz + k, hx1 = ((i + 1) * P.ny + j) * P.nz + k;
+    const long hy0 = (i * ny1 + j) * P.nz + k, hy1 = (i * ny1 + j + 1) * P.nz + k;
+    const long hz0 = (i * P.ny + j) * nz1 + k;
+    Hc.c[0][c] = (H.c[0][hx0] + H.c[0][hx1]) / 2.;
+    Hc.c[1][c] = (H.c[1][hy0] + H.c[1][hy1]) / 2.;
+    Hc.c[2][c] = (H.c[2][hz0] + H.c[2][hz0 + 1]) / 2.;
+}
+
+}  // namespace gf

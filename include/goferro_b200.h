@@ -1,0 +1,182 @@
+/*
+ * goferro_b200.h — C ABI of the B200 engine for GO-Ferro's coupled dynamical
+ * phase-field RK4 time step (LLG magnetisation, second-order ferroelectric
+ * polarisation dynamics, elastodynamics, Yee-grid Maxwell, FFT
+ * magnetostatics).
+ *
+ * The reference has no plugin API: its boundary is the public methods and
+ * fields of four C++ system classes that main.cpp drives
+ * (magnetic_system.h:158-211, ferroelectric_system.h:95-132,
+ * elastic_system.h:172-225, EMdynamic_system.h:131-180).  Each entry point
+ * below replaces a group of those methods; the reference interface it stands
+ * in for is cited beside it.  Plain pointers and sizes only; every call
+ * returns GF_OK (0) or a negative GF_E* code, and gf_last_error() gives the
+ * message.  One engine owns its device memory and CUDA stream; engines are
+ * independent and may live on different host threads.
+ *
+ * Storage order of every field is the reference's matrix3d order
+ * (matrix.h:46-52): index = (i*dimy + j)*dimz + k, z fastest, one array per
+ * vector component.  Cell fields have dims (nx, ny, nz); the Yee fields have
+ * the staggered dims of EMdynamic_initialize.cpp:71-93:
+ *   Ex (nx, ny+1, nz+1)  Ey (nx+1, ny, nz+1)  Ez (nx+1, ny+1, nz)
+ *   Hx (nx+1, ny, nz)    Hy (nx, ny+1, nz)    Hz (nx, ny, nz+1)
+ */
+#ifndef GOFERRO_B200_H
+#define GOFERRO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gf_engine gf_engine;
+
+/* status codes */
+#define GF_OK 0
+#define GF_EINVAL (-1)       /* bad argument or unsupported deck option   */
+#define GF_EIO (-2)          /* deck or restart file missing / malformed  */
+#define GF_ECUDA (-3)        /* CUDA runtime or cuFFT failure              */
+#define GF_ENOMEM (-4)       /* device allocation failed                   */
+#define GF_ENAN (-5)         /* non-finite value found by a health check   */
+#define GF_ENODEV (-6)       /* no usable sm_100 device                    */
+#define GF_EUNSUPPORTED (-7) /* deck asks for physics this build lacks     */
+
+/* fields for gf_upload / gf_download / gf_field_dims (component-major:
+ * a vector field is 3 consecutive arrays x, y, z of the field's dims) */
+enum gf_field {
+    GF_FIELD_M = 0,       /* FM magnetisation m (cell, 3)       mx_glb..   */
+    GF_FIELD_M_AFM1 = 1,  /* AFM sublattice 1 (cell, 3)         mx_AFM1_glb */
+    GF_FIELD_M_AFM2 = 2,  /* AFM sublattice 2 (cell, 3)         mx_AFM2_glb */
+    GF_FIELD_P = 3,       /* polarisation p (cell, 3)           px_glb..    */
+    GF_FIELD_Q = 4,       /* dp/dt (cell, 3)                    qx_glb..    */
+    GF_FIELD_U = 5,       /* displacement (cell, 3)             Dux_glb..   */
+    GF_FIELD_V = 6,       /* velocity (cell, 3)                 vx_glb..    */
+    GF_FIELD_EX = 7,      /* Yee E components, one array each   DEx_em..    */
+    GF_FIELD_EY = 8,
+    GF_FIELD_EZ = 9,
+    GF_FIELD_HX = 10,     /* Yee H components                   DHx_em..    */
+    GF_FIELD_HY = 11,
+    GF_FIELD_HZ = 12,
+    GF_FIELD_HSTAT = 13,  /* magnetostatic field (cell, 3)      Hx_stat..   */
+    GF_FIELD_ESTAT = 14,  /* electrostatic field (cell, 3)      Ex_stat..   */
+    GF_FIELD_E_CELL = 15, /* cell-centred E (cell, 3), read-only DEx_em_cell */
+    GF_FIELD_H_CELL = 16, /* cell-centred H (cell, 3), read-only DHx_em_cell */
+    GF_FIELD_STRAIN = 17, /* dynamic cell strain, global frame (cell, 6:
+                             xx yy zz yz xz xy), read-only   Dexx_glb..    */
+    GF_FIELD_COUNT = 18
+};
+
+/* observables for gf_average (global averages, FP64 sums) */
+enum gf_obs {
+    GF_OBS_M = 0,     /* sum(m)/NFM           magnetic_solver.cpp:1863-1888   */
+    GF_OBS_M_AFM1 = 1,/* sum(m1)/NAFM         magnetic_AFM_solver.cpp:2221    */
+    GF_OBS_M_AFM2 = 2,/* sum(m2)/NAFM                                          */
+    GF_OBS_P = 3,     /* sum(p)/NFE           ferroelectric_solver.cpp:2031   */
+    GF_OBS_U = 4      /* sum(u)/n  (mean displacement over all cells)          */
+};
+
+typedef struct gf_info {
+    int32_t nx, ny, nz;
+    double dx, dy, dz;
+    double dt;
+    double time;            /* physical time reached (time_device)           */
+    uint64_t step;          /* completed steps                               */
+    uint64_t deck_steps;    /* `step` line of system_setting.in              */
+    int32_t n_materials;
+    int32_t fm, afm, fe, elastic, em, demag_per_stage; /* active physics     */
+    uint64_t n_fm, n_afm, n_fe;  /* NFM, NAFM, NFE (global.cpp:103-118)      */
+    uint64_t device_bytes;  /* device memory the engine holds                */
+    int32_t launches_per_step;  /* engine kernels launched per RK4 step      */
+    int32_t reserved_;
+} gf_info;
+
+/* Accumulated device time of one kernel family (gf_profile_steps). */
+typedef struct gf_kernel_time {
+    char name[40];
+    int32_t launches;
+    double total_ms;
+} gf_kernel_time;
+
+/* Create an engine from a GO-Ferro input deck directory: system_setting.in,
+ * materials.in and whatever restart / table files the deck switches on
+ * (m.in, m_AFM.in, Hstat.in, p.in, q.in, Estat.in, u.in, v.in, E?_Yee.in,
+ * H?_Yee.in, Hext.in, Eext.in, struct.in).  Replaces the reference's set-up
+ * sequence main.cpp:21-167 (readgeo, read_global, *initialize_host,
+ * input_*, copy_to_device, initialize_device and the initial static
+ * solves).  `device` selects the CUDA device (-1 = current). */
+int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out);
+
+/* Advance `nsteps` full RK4 steps.  Replaces the body of the reference time
+ * loop main.cpp:243-484: time_marching_device_serial, the four stages of
+ * get_d*_RK{1..4} / update_*_RK{1..3} / update_* for every active system,
+ * and the between-stage magnetostatic solves.  Asynchronous on the engine's
+ * stream; the step is captured once as a CUDA graph and replayed. */
+int gf_advance(gf_engine* e, uint64_t nsteps);
+
+/* Same as gf_advance but launches the kernels directly without a graph
+ * (used for debugging and for timing the graph's benefit). */
+int gf_advance_eager(gf_engine* e, uint64_t nsteps);
+
+/* Global average of an observable (gf_obs) of the current state, FP64.
+ * Replaces get_averagem / get_averagem_AFM / get_averagep. Synchronous. */
+int gf_average(gf_engine* e, int obs, double out3[3]);
+
+/* Cell-centred E and H at cell (i,j,k) (0-based), as the reference's
+ * output_em_onecell reads them (DE?_em_cell / DH?_em_cell). Synchronous. */
+int gf_probe_em(gf_engine* e, int64_t i, int64_t j, int64_t k, double e3[3], double h3[3]);
+
+/* Number of doubles and dims of one array of a field (for vector fields the
+ * dims of one component; count = 3 * dims product, 6 for GF_FIELD_STRAIN). */
+int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count);
+
+/* Copy a field to / from host memory (count doubles, component-major).
+ * Replace the reference's copy*_from_device and input_* restart readers.
+ * Synchronous. */
+int gf_download(gf_engine* e, int field, double* host, size_t count);
+int gf_upload(gf_engine* e, int field, const double* host, size_t count);
+
+/* Same as gf_download but into device memory owned by the caller
+ * (cudaMemcpyAsync device-to-device on the engine stream, no host sync). */
+int gf_download_device(gf_engine* e, int field, double* dev, size_t count);
+/* Same as gf_upload but from caller-owned device memory. */
+int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count);
+
+/* Advance `nsteps` steps like gf_advance_eager, with a CUDA event pair
+ * around every kernel launch, and report the summed device time per kernel
+ * family (at most max_records records; *n_records gets the count).  The
+ * state advances exactly as with gf_advance.  Replaces nothing in the
+ * reference, which has only a wall-clock stamp around the loop
+ * (main.cpp:209-211, 720-726). */
+int gf_profile_steps(gf_engine* e, uint64_t nsteps, gf_kernel_time* out, int max_records, int* n_records);
+
+/* Engine facts (grid, active physics, counters). */
+int gf_get_info(gf_engine* e, gf_info* info);
+
+/* Wait for all work queued on the engine stream. */
+int gf_synchronize(gf_engine* e);
+
+/* The engine's CUDA stream (a cudaStream_t), for callers that queue their
+ * own work behind the engine. */
+void* gf_stream(gf_engine* e);
+
+/* Check every state field for non-finite values on the device; returns
+ * GF_ENAN and names the first offending field in gf_last_error. */
+int gf_check_finite(gf_engine* e);
+
+/* Message of the last failing call on this engine (or of the last failing
+ * gf_create_from_deck when e is NULL).  Never NULL. */
+const char* gf_last_error(const gf_engine* e);
+
+/* Free the engine and all its device memory. */
+void gf_destroy(gf_engine* e);
+
+/* Library version string. */
+const char* gf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOFERRO_B200_H */

@@ -1,0 +1,293 @@
+/*
+ * Oracle driver: runs GO-Ferro's own (unmodified) system classes on the CPU
+ * through the same call sequence as the reference time loop
+ * (main.cpp:17-714), and records full-precision traces instead of the
+ * reference's %.7e output files.
+ *
+ * TEST INFRASTRUCTURE: built into oracle/_ref/goferro_ref together with the
+ * reference sources, oracle/ref_stubs.cpp and the host cuFFT shim.  Only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg run it.
+ *
+ * Usage:
+ *   goferro_ref DECK_DIR OUT_DIR [--steps K] [--trace-every N]
+ *               [--probe I J K] [--dump]
+ *
+ * DECK_DIR holds system_setting.in, materials.in and any restart files the
+ * deck asks for (the reference reads them from the working directory,
+ * read.cpp:8,120).  OUT_DIR receives:
+ *   trace.txt  one line per traced step (step 0 = initial state):
+ *              step  <m>x y z  <mAFM1>x y z  <mAFM2>x y z  <p>x y z
+ *              <u>x y z  E_cell(probe)x y z  H_cell(probe)x y z   (%.17e)
+ *   *.bin      with --dump: raw float64 fields after the last step, in the
+ *              reference's storage order (matrix.h:51)
+ *   timing.json  {"steps":K,"seconds":S,"cells":n} for the time loop only.
+ */
+#define _USE_SINGLETON_MACRO
+#include "_MACRO_SINGLETON.h"
+#include "geometry.h"
+#include "global.h"
+#include "mathlib.h"
+#include "ferroelectric_system.h"
+#include "magnetic_system.h"
+#include "elastic_system.h"
+#include "EMdynamic_system.h"
+#include "inoutput.h"
+
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <unistd.h>
+
+namespace {
+
+struct Systems {
+    ferroelectric_system fe;
+    magnetic_system mag;
+    elastic_system el;
+    EMdynamic_system em;
+};
+
+// One RK stage's method set for each system (stage index 0..3).
+struct StageCalls {
+    void (elastic_system::*dv)();
+    void (elastic_system::*du)();
+    void (elastic_system::*upd_v)();
+    void (elastic_system::*upd_u)();
+    void (magnetic_system::*dm)();
+    void (magnetic_system::*dm_afm)();
+    void (magnetic_system::*upd_m)();
+    void (magnetic_system::*upd_m_afm)();
+    void (ferroelectric_system::*dq)();
+    void (ferroelectric_system::*dp)();
+    void (ferroelectric_system::*upd_q)();
+    void (ferroelectric_system::*upd_p)();
+    void (EMdynamic_system::*dE)();
+    void (EMdynamic_system::*dH)();
+    void (EMdynamic_system::*upd_E)();
+    void (EMdynamic_system::*upd_H)();
+};
+
+const StageCalls kStages[4] = {
+    {&elastic_system::get_dv_RK1, &elastic_system::get_du_RK1, &elastic_system::update_v_RK1, &elastic_system::update_u_RK1,
+     &magnetic_system::get_dm_RK1, &magnetic_system::get_dm_AFM_RK1, &magnetic_system::update_m_RK1, &magnetic_system::update_m_AFM_RK1,
+     &ferroelectric_system::get_dq_RK1, &ferroelectric_system::get_dp_RK1, &ferroelectric_system::update_q_RK1, &ferroelectric_system::update_p_RK1,
+     &EMdynamic_system::get_dE_RK1, &EMdynamic_system::get_dH_RK1, &EMdynamic_system::update_DE_RK1, &EMdynamic_system::update_DH_RK1},
+    {&elastic_system::get_dv_RK2, &elastic_system::get_du_RK2, &elastic_system::update_v_RK2, &elastic_system::update_u_RK2,
+     &magnetic_system::get_dm_RK2, &magnetic_system::get_dm_AFM_RK2, &magnetic_system::update_m_RK2, &magnetic_system::update_m_AFM_RK2,
+     &ferroelectric_system::get_dq_RK2, &ferroelectric_system::get_dp_RK2, &ferroelectric_system::update_q_RK2, &ferroelectric_system::update_p_RK2,
+     &EMdynamic_system::get_dE_RK2, &EMdynamic_system::get_dH_RK2, &EMdynamic_system::update_DE_RK2, &EMdynamic_system::update_DH_RK2},
+    {&elastic_system::get_dv_RK3, &elastic_system::get_du_RK3, &elastic_system::update_v_RK3, &elastic_system::update_u_RK3,
+     &magnetic_system::get_dm_RK3, &magnetic_system::get_dm_AFM_RK3, &magnetic_system::update_m_RK3, &magnetic_system::update_m_AFM_RK3,
+     &ferroelectric_system::get_dq_RK3, &ferroelectric_system::get_dp_RK3, &ferroelectric_system::update_q_RK3, &ferroelectric_system::update_p_RK3,
+     &EMdynamic_system::get_dE_RK3, &EMdynamic_system::get_dH_RK3, &EMdynamic_system::update_DE_RK3, &EMdynamic_system::update_DH_RK3},
+    {&elastic_system::get_dv_RK4, &elastic_system::get_du_RK4, &elastic_system::update_v, &elastic_system::update_u,
+     &magnetic_system::get_dm_RK4, &magnetic_system::get_dm_AFM_RK4, &magnetic_system::update_m, &magnetic_system::update_m_AFM,
+     &ferroelectric_system::get_dq_RK4, &ferroelectric_system::get_dp_RK4, &ferroelectric_system::update_q, &ferroelectric_system::update_p,
+     &EMdynamic_system::get_dE_RK4, &EMdynamic_system::get_dH_RK4, &EMdynamic_system::update_DE, &EMdynamic_system::update_DH},
+};
+
+// Static solves that the reference runs between stages and after the last
+// one when the fields are not dynamical (main.cpp:299-306, 476-483).
+void between_stage_statics(Systems& s) {
+    if (!_GLB.if_EMdynamic) {
+        if (_GLB.if_FE_all && !_GLB.if_elec_1Dmodel) s.fe.get_E_static();
+        if ((_GLB.if_FM_all || _GLB.if_AFM_all) && !_GLB.if_mag_1Dmodel && _GLB.if_magnetostatics)
+            s.mag.get_H_static();
+    }
+}
+
+void run_stage(Systems& s, int st) {
+    const StageCalls& c = kStages[st];
+    if (_GLB.if_elastodynamics) { (s.el.*c.dv)(); (s.el.*c.du)(); }
+    if (_GLB.if_FM_all) { (s.mag.*c.dm)(); if (st == 3) s.mag.get_dm(); }
+    if (_GLB.if_AFM_all) { (s.mag.*c.dm_afm)(); if (st == 3) s.mag.get_dm_AFM(); }
+    if (_GLB.if_FE_all) { (s.fe.*c.dq)(); (s.fe.*c.dp)(); }
+    if (_GLB.if_EMdynamic) { (s.em.*c.dE)(); (s.em.*c.dH)(); }
+
+    if (_GLB.if_elastodynamics) { (s.el.*c.upd_v)(); (s.el.*c.upd_u)(); }
+    if (_GLB.if_FM_all) (s.mag.*c.upd_m)();
+    if (_GLB.if_AFM_all) (s.mag.*c.upd_m_afm)();
+    if (_GLB.if_FE_all) { (s.fe.*c.upd_q)(); (s.fe.*c.upd_p)(); }
+    if (_GLB.if_EMdynamic) { (s.em.*c.upd_E)(); (s.em.*c.upd_H)(); }
+}
+
+double mean(const matrix3d<double>& a) {
+    double acc = 0.;
+    for (long i = 0; i < a.dim; ++i) acc += a.matrix[i];
+    return acc / (double)a.dim;
+}
+
+void write_trace_line(FILE* f, unsigned long long step, Systems& s, long probe) {
+    double v[21] = {0.};
+    if (_GLB.if_FM_all) { s.mag.get_averagem(); v[0] = s.mag.mx_ave; v[1] = s.mag.my_ave; v[2] = s.mag.mz_ave; }
+    if (_GLB.if_AFM_all) {
+        s.mag.get_averagem_AFM();
+        v[3] = s.mag.mx_AFM1_ave; v[4] = s.mag.my_AFM1_ave; v[5] = s.mag.mz_AFM1_ave;
+        v[6] = s.mag.mx_AFM2_ave; v[7] = s.mag.my_AFM2_ave; v[8] = s.mag.mz_AFM2_ave;
+    }
+    if (_GLB.if_FE_all) { s.fe.get_averagep(); v[9] = s.fe.px_ave; v[10] = s.fe.py_ave; v[11] = s.fe.pz_ave; }
+    if (_GLB.if_elastodynamics) { v[12] = mean(s.el.Dux_glb); v[13] = mean(s.el.Duy_glb); v[14] = mean(s.el.Duz_glb); }
+    if (_GLB.if_EMdynamic) {
+        v[15] = s.em.DEx_em_cell(probe); v[16] = s.em.DEy_em_cell(probe); v[17] = s.em.DEz_em_cell(probe);
+        v[18] = s.em.DHx_em_cell(probe); v[19] = s.em.DHy_em_cell(probe); v[20] = s.em.DHz_em_cell(probe);
+    }
+    fprintf(f, "%llu", step);
+    for (double x : v) fprintf(f, " %.17e", x);
+    fprintf(f, "\n");
+}
+
+void dump(const std::string& dir, const char* name, const matrix3d<double>& a) {
+    std::string path = dir + "/" + name + ".bin";
+    FILE* f = fopen(path.c_str(), "wb");
+    if (!f) return;
+    fwrite(a.matrix, sizeof(double), (size_t)a.dim, f);
+    fclose(f);
+}
+
+void dump_all(const std::string& d, Systems& s) {
+    if (_GLB.if_FM_all) { dump(d, "mx", s.mag.mx_glb); dump(d, "my", s.mag.my_glb); dump(d, "mz", s.mag.mz_glb);
+        dump(d, "Hx_stat", s.mag.Hx_stat); dump(d, "Hy_stat", s.mag.Hy_stat); dump(d, "Hz_stat", s.mag.Hz_stat); }
+    if (_GLB.if_AFM_all) {
+        dump(d, "mx_AFM1", s.mag.mx_AFM1_glb); dump(d, "my_AFM1", s.mag.my_AFM1_glb); dump(d, "mz_AFM1", s.mag.mz_AFM1_glb);
+        dump(d, "mx_AFM2", s.mag.mx_AFM2_glb); dump(d, "my_AFM2", s.mag.my_AFM2_glb); dump(d, "mz_AFM2", s.mag.mz_AFM2_glb);
+    }
+    if (_GLB.if_FE_all) {
+        dump(d, "px", s.fe.px_glb); dump(d, "py", s.fe.py_glb); dump(d, "pz", s.fe.pz_glb);
+        dump(d, "qx", s.fe.qx_glb); dump(d, "qy", s.fe.qy_glb); dump(d, "qz", s.fe.qz_glb);
+    }
+    if (_GLB.if_elastodynamics) {
+        dump(d, "ux", s.el.Dux_glb); dump(d, "uy", s.el.Duy_glb); dump(d, "uz", s.el.Duz_glb);
+        dump(d, "vx", s.el.vx_glb); dump(d, "vy", s.el.vy_glb); dump(d, "vz", s.el.vz_glb);
+    }
+    if (_GLB.if_EMdynamic) {
+        dump(d, "Ex", s.em.DEx_em); dump(d, "Ey", s.em.DEy_em); dump(d, "Ez", s.em.DEz_em);
+        dump(d, "Hx", s.em.DHx_em); dump(d, "Hy", s.em.DHy_em); dump(d, "Hz", s.em.DHz_em);
+    }
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 3) {
+        fprintf(stderr, "usage: %s DECK_DIR OUT_DIR [--steps K] [--trace-every N] [--probe I J K] [--dump]\n", argv[0]);
+        return 2;
+    }
+    char outbuf[PATH_MAX];
+    if (!realpath(argv[2], outbuf)) { fprintf(stderr, "bad OUT_DIR %s\n", argv[2]); return 2; }
+    std::string out = outbuf;
+    long long steps_override = -1;
+    unsigned long long trace_every = 1;
+    long pi = -1, pj = -1, pk = -1;
+    bool do_dump = false;
+    for (int a = 3; a < argc; ++a) {
+        if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps_override = atoll(argv[++a]);
+        else if (!strcmp(argv[a], "--trace-every") && a + 1 < argc) trace_every = strtoull(argv[++a], 0, 10);
+        else if (!strcmp(argv[a], "--probe") && a + 3 < argc) { pi = atol(argv[++a]); pj = atol(argv[++a]); pk = atol(argv[++a]); }
+        else if (!strcmp(argv[a], "--dump")) do_dump = true;
+        else { fprintf(stderr, "unknown argument %s\n", argv[a]); return 2; }
+    }
+    if (chdir(argv[1]) != 0) { fprintf(stderr, "cannot enter %s\n", argv[1]); return 2; }
+
+    // ---- set-up, in the order of main.cpp:21-116 ----
+    _GEO.readgeo();
+    _GEO.copy_to_device();
+    _GLB.read_global();
+    _GLB.copy_to_device();
+    _IO.get_dimension(_GEO.nx_system, _GEO.ny_system, _GEO.nz_system, &(global_parameters::glb));
+    _MLB.copy_to_device();
+    if (steps_override >= 0) _GLB.step = (unsigned long long)steps_override;
+    if (trace_every == 0) trace_every = 1;
+
+    Systems* sp = new Systems();
+    Systems& s = *sp;
+    s.fe.initialize_host();
+    s.mag.initialize_host();
+    s.el.initialize_host();
+    s.em.initialize_host();
+
+    if (_GLB.if_input_m) _IO.input_m(&s.mag);
+    if (_GLB.if_input_AFMm) _IO.input_AFMm(&s.mag);
+    if (_GLB.if_input_Hstat) _IO.input_Hstat(&s.mag);
+    if (_GLB.if_input_pandq) _IO.input_pandq(&s.fe);
+    if (_GLB.if_input_Estat) _IO.input_Estat(&s.fe);
+    if (_GLB.if_input_em) _IO.input_em_Yee(&s.em);
+    if (_GLB.if_input_uandv) _IO.input_uandv(&s.el);
+    if (_GLB.if_input_elastoforce) _IO.input_elastoforce(&s.el);
+    if (_GLB.if_input_straint0) _IO.input_straint0(&s.el);
+    if (_GLB.if_input_eigenstraint0_crt) _IO.input_eigenstraint0(&s.el);
+    if (_GLB.if_input_Jp) _IO.input_Jp(&s.em);
+
+    s.fe.copy_to_device();
+    s.mag.copy_to_device();
+    s.el.copy_to_device();
+    s.em.copy_to_device();
+
+    s.fe.pt_elas = &s.el; s.fe.pt_EM = &s.em;
+    s.mag.pt_elas = &s.el; s.mag.pt_EM = &s.em;
+    s.el.pt_mag = &s.mag; s.el.pt_fe = &s.fe;
+    s.em.pt_mag = &s.mag; s.em.pt_fe = &s.fe;
+
+    s.mag.initialize_device();
+    s.fe.initialize_device();
+    s.em.initialize_device();
+    s.el.initialize_device();
+
+    // ---- initial static fields (main.cpp:120-167) ----
+    if (_GLB.if_FE_all && !_GLB.if_input_Estat) {
+        if (_GLB.if_elec_1Dmodel) s.fe.get_E_static_1D(); else s.fe.get_E_static();
+    }
+    if ((_GLB.if_FM_all || _GLB.if_AFM_all) && !_GLB.if_input_Hstat && _GLB.if_magnetostatics) {
+        if (_GLB.if_mag_1Dmodel) s.mag.get_H_static_1D(); else s.mag.get_H_static();
+    }
+    if (_GLB.if_elastodynamics && !_GLB.if_input_straint0 && !_GLB.if_input_eigenstraint0_crt) {
+        s.el.get_strain_static();
+        s.el.get_strain_static_glb();
+    }
+    if (_GLB.if_FE_all && _GLB.if_flexo) s.fe.get_p_gradient();
+
+    const long n = _GEO.nx_system * _GEO.ny_system * _GEO.nz_system;
+    long probe = 0;
+    if (pi >= 0) probe = (pi * _GEO.ny_system + pj) * _GEO.nz_system + pk;
+
+    std::string tpath = out + "/trace.txt";
+    FILE* tf = fopen(tpath.c_str(), "w");
+    if (!tf) { fprintf(stderr, "cannot write %s\n", tpath.c_str()); return 2; }
+    write_trace_line(tf, 0, s, probe);
+
+    // ---- statics before the loop (main.cpp:213-240) ----
+    if (!_GLB.if_elastodynamics) s.el.get_strain_static();
+    if (!_GLB.if_EMdynamic) {
+        if (_GLB.if_FE_all) { if (_GLB.if_elec_1Dmodel) s.fe.get_E_static_1D(); else s.fe.get_E_static(); }
+        if ((_GLB.if_FM_all || _GLB.if_AFM_all) && _GLB.if_magnetostatics) {
+            if (_GLB.if_mag_1Dmodel) s.mag.get_H_static_1D(); else s.mag.get_H_static();
+        }
+    }
+
+    // ---- time loop (main.cpp:243-484) ----
+    auto t0 = std::chrono::steady_clock::now();
+    for (unsigned long long nstep = 1; nstep < _GLB.step + 1; ++nstep) {
+        _GLB.time_marching_device_serial();
+        for (int st = 0; st < 4; ++st) {
+            run_stage(s, st);
+            if (st < 3) between_stage_statics(s);
+        }
+        if (!_GLB.if_elastodynamics) s.el.get_strain_static();
+        between_stage_statics(s);
+        if (nstep % trace_every == 0 || nstep == _GLB.step) write_trace_line(tf, nstep, s, probe);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    fclose(tf);
+
+    double secs = std::chrono::duration<double>(t1 - t0).count();
+    std::string jpath = out + "/timing.json";
+    FILE* jf = fopen(jpath.c_str(), "w");
+    if (jf) {
+        fprintf(jf, "{\"steps\": %llu, \"seconds\": %.9f, \"cells\": %ld}\n", _GLB.step, secs, n);
+        fclose(jf);
+    }
+    if (do_dump) dump_all(out, s);
+    return 0;
+}

@@ -1,0 +1,172 @@
+"""GPU parity: the B200 engine, called through the C ABI, against GO-Ferro's
+own solver (golden fixtures made by the oracle build, and the oracle binary
+run live on extra decks).
+
+Tolerance (FP64 form): every traced observable and every final field agrees
+with the reference to 1e-10 relative to the observable's largest magnitude.
+"""
+import importlib.util
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+TOL = 1e-10
+
+FIELDS = {"m": ("mx", "my", "mz"), "u": ("ux", "uy", "uz"), "v": ("vx", "vy", "vz"),
+          "p": ("px", "py", "pz"), "q": ("qx", "qy", "qz"), "Hstat": ("Hx_stat", "Hy_stat", "Hz_stat")}
+YEE = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def _mg():
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+def engine_trace(eng, steps, probe, graph=True):
+    rows = []
+    for s in range(steps + 1):
+        if s:
+            eng.advance(1, graph=graph)
+        row = np.zeros(22)
+        row[0] = s
+        if eng.info.fm:
+            row[1:4] = eng.average("m")
+        if eng.info.fe:
+            row[10:13] = eng.average("p")
+        if eng.info.elastic:
+            row[13:16] = eng.average("u")
+        if eng.info.em:
+            e, h = eng.probe_em(*probe)
+            row[16:19] = e
+            row[19:22] = h
+        rows.append(row)
+    return np.array(rows)
+
+
+def assert_trace_close(mine, ref, tol=TOL):
+    for c in range(1, 22):
+        scale = np.max(np.abs(ref[:, c]))
+        err = np.max(np.abs(mine[:, c] - ref[:, c]))
+        if scale == 0.0:
+            assert err == 0.0, f"column {c}: expected zeros, got {err}"
+        else:
+            assert err <= tol * scale, f"column {c}: rel err {err / scale:.3e}"
+
+
+def assert_fields_close(eng, ref_fields, tol=TOL):
+    checked = 0
+    for name, parts in FIELDS.items():
+        if parts[0] not in ref_fields:
+            continue
+        mine = eng.download(name)
+        for c, p in enumerate(parts):
+            r = ref_fields[p]
+            scale = np.max(np.abs(r))
+            err = np.max(np.abs(mine[c].ravel() - r))
+            assert err <= tol * max(scale, 1e-300) or (scale == 0 and err == 0), f"{p}: {err / max(scale, 1e-300):.3e}"
+            checked += 1
+    for p in YEE:
+        if p not in ref_fields:
+            continue
+        mine = eng.download(p).ravel()
+        r = ref_fields[p]
+        scale = np.max(np.abs(r))
+        err = np.max(np.abs(mine - r))
+        assert err <= tol * max(scale, 1e-300) or (scale == 0 and err == 0), f"{p}: {err / max(scale, 1e-300):.3e}"
+        checked += 1
+    assert checked > 0
+
+
+@pytest.mark.parametrize("name", json.load(open(os.path.join(GOLDEN, "cases.json"))).keys())
+def test_engine_matches_golden(gf, tmp_path, name):
+    mg = _mg()
+    d, steps, probe = mg.make_deck(name)
+    gf.decks.write_deck(d, str(tmp_path))
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    with gf.Engine(str(tmp_path), device=0) as eng:
+        mine = engine_trace(eng, steps, probe)
+        assert_trace_close(mine, g["trace"])
+        assert_fields_close(eng, {k: g[k] for k in g.files if k != "trace"})
+        eng.check_finite()
+
+
+def test_graph_and_eager_paths_are_identical(gf, tmp_path):
+    d = gf.decks.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=9)
+    d.amp_gauss *= 1e6
+    gf.decks.write_deck(d, str(tmp_path))
+    out = []
+    for graph in (True, False):
+        with gf.Engine(str(tmp_path), device=0) as eng:
+            eng.advance(9, graph=graph)
+            out.append([eng.download(f) for f in ("m", "u", "v", "Ex", "Hz")])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_upload_download_roundtrip(gf, tmp_path):
+    d = gf.decks.preset_ferroelectric(nx=8, ny=8, nz=10, steps=2)
+    gf.decks.write_deck(d, str(tmp_path))
+    with gf.Engine(str(tmp_path), device=0) as eng:
+        p = eng.download("p")
+        assert p.shape == (3, 8, 8, 10)
+        assert np.array_equal(p, d.p0)
+        new = np.random.default_rng(0).standard_normal(p.shape) * 1e-3
+        eng.upload("p", new)
+        assert np.array_equal(eng.download("p"), new)
+        dims, cnt = eng.field_dims("Ez")
+        assert dims == (9, 9, 10) and cnt == 810
+
+
+# ---------------------------------------------------------------------------
+# live oracle on deck variants that exercise further branches
+# ---------------------------------------------------------------------------
+def _variants(gf):
+    D = gf.decks
+    v = {}
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=25)
+    d.abc_1D = True
+    d.strain_type, d.sigma_gauss, d.amp_gauss, d.strain_z = 1, 2e-16, 1e-3, 1
+    v["mur_elastic_gauss_source"] = (d, 25, (4, 8, 7))
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=25)
+    d.strain_type, d.sigma_gauss, d.amp_gauss, d.strain_z = 3, 2e-16, 1e7, 8
+    d.layers = [(5, 1), (4, 2), (3, 1)]
+    d.periodic = (False, False, False)
+    v["traction_source_open_box"] = (d, 25, (4, 8, 7))
+    d = D.preset_ferroelectric(nx=8, ny=8, nz=10, steps=25)
+    d.jf_type, d.jf_freq, d.jf_sigma, d.jf_amp = 6, 3e15, 5e-18, 1e12
+    d.planeEM, d.planeEM_E, d.planeEM_freq = True, (1e5, 0.0, 0.0), (1e15, 1e15, 1e15)
+    d.Eext_altr, d.E_altr_freq = (1e6, 0.0, 2e6), (1e14, 0.0, 3e14)
+    v["fe_jf6_plane_wave_eext"] = (d, 25, (4, 4, 5))
+    d = D.preset_fm_demag(nx=12, ny=8, nz=6, steps=25)
+    d.Hext_table = None
+    d.Hext_stat, d.Hext_altr, d.H_altr_freq = (0, 0, 8e4), (2e3, 0, 0), (2e11, 0, 0)
+    m2 = D.yig(0.02)
+    m2.Aex, m2.iDMI, m2.aniso_type, m2.K1 = 2.0e-12, 1e-3, 2, 3e3
+    d.materials.append(m2)
+    d.layers = [(3, 1), (3, 2)]
+    d.periodic = (True, False, False)
+    v["two_fm_materials_dmi_uniaxial"] = (d, 25, None)
+    d = D.preset_fm_demag(nx=8, ny=8, nz=4, steps=15)
+    d.demag_factor, d.demag_fac = True, (0.1, 0.2, 0.7)
+    v["demag_factor"] = (d, 15, None)
+    return v
+
+
+@pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box",
+                                   "fe_jf6_plane_wave_eext", "two_fm_materials_dmi_uniaxial", "demag_factor"])
+def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
+    d, steps, probe = _variants(gf)[vname]
+    gf.decks.write_deck(d, str(tmp_path / "deck"))
+    r = refrun.run(str(tmp_path / "deck"), str(tmp_path / "ref"), steps=steps, probe=probe, dump=True)
+    with gf.Engine(str(tmp_path / "deck"), device=0) as eng:
+        mine = engine_trace(eng, steps, probe if probe else (0, 0, 0))
+        assert_trace_close(mine, r["trace"])
+        assert_fields_close(eng, r["fields"])
