@@ -61,6 +61,8 @@ struct Params {
     double Tg2c[3][3], Tc2g[3][3];
     // active physics
     int fm, afm, fe, elastic, em;
+    // bounding box of the ferromagnetic cells (the LLG kernel covers only it)
+    long fm_i0, fm_j0, fm_k0, fm_bi, fm_bj, fm_bk;
     int elasto_on, elasto_back;   // if_elasto_on_pORm, if_elasto_backaction_from_pORm
     int em_fromM, em_fromP, em_back_M, em_back_P;
     int has_eig0, has_strain0, has_hext_nonunif;

@@ -1,245 +1,275 @@
 // Elastodynamics stage kernels (FP64).
 //
-//   k_strain      per cell: dynamic strain of the stage displacement from
-//                 face-normal gradients (get_dudxyz_glb + get_Dstrain,
-//                 elastic_dynamic_solver.cpp:106-227) and the dynamic
-//                 eigenstrain of m and p (get_eigenstrain_dynamic, :3-104).
-//   k_elastic     per cell: face stresses, stress divergence, velocity and
-//                 displacement increments and their RK4 combination
-//                 (get_dv_RK{1..4} :841-2800, get_du_RK* :2801-2847,
-//                 update_v*/update_u* :2849-3057).
+//   k_face_grad   per cell: the face-normal displacement gradients on the
+//                 cell's -x, -y and -z faces, 3 components each, 0 on
+//                 stress-free faces (get_dudxyz_glb, elastic_dynamic_solver.cpp:
+//                 106-187).  Each gradient is computed once per stage.
+//   k_elastic     per cell: cell strains (get_Dstrain, :189-227) and dynamic
+//                 eigenstrains of m and p (get_eigenstrain_dynamic, :3-104) of
+//                 the cell and its six face neighbours, the six face stresses,
+//                 stress divergence, velocity and displacement increments and
+//                 their RK4 combination (get_dv_RK{1..4} :841-2800,
+//                 get_du_RK* :2801-2847, update_v*/update_u* :2849-3057).
 //   k_elastic_bc  per (i,j) column: z absorbing boundary (Liao 4th order or
 //                 first-order Mur, elastodynamics_AbsorbingBoundary.cpp:91-230)
 //                 and the displacement source plane (update_Du_Gaussian*,
 //                 elastic_dynamic_solver.cpp:3059-3284), in that order.
 //
-// The reference materialises nine face-gradient arrays per stage; here they
-// are recomputed where used from the stage displacement and the material
-// ids, so only the cell strains are written.
+// Face f of an axis with n cells is stored at cell index f for f < n; face n
+// is read from index 0, which holds the same value (periodic axis) or the
+// same zero (non-periodic axis: both end faces are stress-free).  Strains and
+// eigenstrains are recomputed where used instead of being stored.
 #pragma once
 
 #include "gf_state.cuh"
 
 namespace gf {
 
-struct UGrad {
+__device__ inline bool solid_at(const Params& P, const uint8_t* mid, long i, long j, long k) {
+    return mid[cid(P, i, j, k)] != 0;
+}
+// stress-free masks (elastic_initialize.cpp:245-335)
+__device__ inline bool free_x(const Params& P, const uint8_t* mid, long f, long j, long k) {
+    if (f == 0 || f == P.nx) return P.per_x ? !(solid_at(P, mid, 0, j, k) && solid_at(P, mid, P.nx - 1, j, k)) : true;
+    return !(solid_at(P, mid, f - 1, j, k) && solid_at(P, mid, f, j, k));
+}
+__device__ inline bool free_y(const Params& P, const uint8_t* mid, long i, long f, long k) {
+    if (f == 0 || f == P.ny) return P.per_y ? !(solid_at(P, mid, i, 0, k) && solid_at(P, mid, i, P.ny - 1, k)) : true;
+    return !(solid_at(P, mid, i, f - 1, k) && solid_at(P, mid, i, f, k));
+}
+__device__ inline bool free_z(const Params& P, const uint8_t* mid, long i, long j, long f) {
+    if (f == 0 || f == P.nz) return P.per_z ? !(solid_at(P, mid, i, j, 0) && solid_at(P, mid, i, j, P.nz - 1)) : true;
+    return !(solid_at(P, mid, i, j, f - 1) && solid_at(P, mid, i, j, f));
+}
+
+__global__ void __launch_bounds__(256) k_face_grad(Params P, StageIO io) {
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long nyz = (long)P.ny * P.nz;
+    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const bool fx = free_x(P, io.mid, i, j, k), fy = free_y(P, io.mid, i, j, k), fz = free_z(P, io.mid, i, j, k);
+    const long cx = cid(P, i == 0 ? P.nx - 1 : i - 1, j, k);
+    const long cy = cid(P, i, j == 0 ? P.ny - 1 : j - 1, k);
+    const long cz = cid(P, i, j, k == 0 ? P.nz - 1 : k - 1);
+    for (int a = 0; a < 3; a++) {
+        const double* u = io.u_in.c[a];
+        const double uc = u[c];
+        io.fg[a][c] = fx ? 0. : (uc - u[cx]) / P.dx;
+        io.fg[3 + a][c] = fy ? 0. : (uc - u[cy]) / P.dy;
+        io.fg[6 + a][c] = fz ? 0. : (uc - u[cz]) / P.dz;
+    }
+}
+
+// read access to the stored face gradients; f may equal n
+struct GradView {
     const Params& P;
     const StageIO& io;
-    __device__ UGrad(const Params& p, const StageIO& s) : P(p), io(s) {}
-    __device__ bool solid(long i, long j, long k) const { return io.mid[cid(P, i, j, k)] != 0; }
-    // stress-free masks (elastic_initialize.cpp:245-335)
-    __device__ bool free_x(long f, long j, long k) const {
-        if (f == 0 || f == P.nx) return P.per_x ? !(solid(0, j, k) && solid(P.nx - 1, j, k)) : true;
-        return !(solid(f - 1, j, k) && solid(f, j, k));
+    __device__ GradView(const Params& p, const StageIO& s) : P(p), io(s) {}
+    __device__ double gx(int a, long f, long j, long k) const { return io.fg[a][cid(P, f == P.nx ? 0 : f, j, k)]; }
+    __device__ double gy(int a, long i, long f, long k) const { return io.fg[3 + a][cid(P, i, f == P.ny ? 0 : f, k)]; }
+    __device__ double gz(int a, long i, long j, long f) const { return io.fg[6 + a][cid(P, i, j, f == P.nz ? 0 : f)]; }
+    // cell strain components in the global frame (get_Dstrain)
+    __device__ double exx(long i, long j, long k) const { return (gx(0, i, j, k) + gx(0, i + 1, j, k)) / 2.; }
+    __device__ double eyy(long i, long j, long k) const { return (gy(1, i, j, k) + gy(1, i, j + 1, k)) / 2.; }
+    __device__ double ezz(long i, long j, long k) const { return (gz(2, i, j, k) + gz(2, i, j, k + 1)) / 2.; }
+    __device__ double eyz(long i, long j, long k) const {
+        return (gz(1, i, j, k) + gz(1, i, j, k + 1) + gy(2, i, j, k) + gy(2, i, j + 1, k)) / 4.;
     }
-    __device__ bool free_y(long i, long f, long k) const {
-        if (f == 0 || f == P.ny) return P.per_y ? !(solid(i, 0, k) && solid(i, P.ny - 1, k)) : true;
-        return !(solid(i, f - 1, k) && solid(i, f, k));
+    __device__ double exz(long i, long j, long k) const {
+        return (gz(0, i, j, k) + gz(0, i, j, k + 1) + gx(2, i, j, k) + gx(2, i + 1, j, k)) / 4.;
     }
-    __device__ bool free_z(long i, long j, long f) const {
-        if (f == 0 || f == P.nz) return P.per_z ? !(solid(i, j, 0) && solid(i, j, P.nz - 1)) : true;
-        return !(solid(i, j, f - 1) && solid(i, j, f));
+    __device__ double exy(long i, long j, long k) const {
+        return (gy(0, i, j, k) + gy(0, i, j + 1, k) + gx(1, i, j, k) + gx(1, i + 1, j, k)) / 4.;
     }
-    __device__ double u(int a, long i, long j, long k) const { return io.u_in.c[a][cid(P, i, j, k)]; }
-    // face-normal gradients of component a (get_dudxyz_glb)
-    __device__ double gx(int a, long f, long j, long k) const {
-        if (free_x(f, j, k)) return 0.;
-        if (f == 0 || f == P.nx) return (u(a, 0, j, k) - u(a, P.nx - 1, j, k)) / P.dx;
-        return (u(a, f, j, k) - u(a, f - 1, j, k)) / P.dx;
-    }
-    __device__ double gy(int a, long i, long f, long k) const {
-        if (free_y(i, f, k)) return 0.;
-        if (f == 0 || f == P.ny) return (u(a, i, 0, k) - u(a, i, P.ny - 1, k)) / P.dy;
-        return (u(a, i, f, k) - u(a, i, f - 1, k)) / P.dy;
-    }
-    __device__ double gz(int a, long i, long j, long f) const {
-        if (free_z(i, j, f)) return 0.;
-        if (f == 0 || f == P.nz) return (u(a, i, j, 0) - u(a, i, j, P.nz - 1)) / P.dz;
-        return (u(a, i, j, f) - u(a, i, j, f - 1)) / P.dz;
+    __device__ void strain_glb(long i, long j, long k, double e[6]) const {
+        e[0] = exx(i, j, k); e[1] = eyy(i, j, k); e[2] = ezz(i, j, k);
+        e[3] = eyz(i, j, k); e[4] = exz(i, j, k); e[5] = exy(i, j, k);
     }
 };
 
-__global__ void __launch_bounds__(256) k_strain(Params P, StageIO io) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    const long nyz = (long)P.ny * P.nz;
-    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
-    UGrad g(P, io);
-
-    // ---- dynamic strain (get_Dstrain) ----
-    double s[3][3];
-    s[0][0] = (g.gx(0, i, j, k) + g.gx(0, i + 1, j, k)) / 2.;
-    s[1][1] = (g.gy(1, i, j, k) + g.gy(1, i, j + 1, k)) / 2.;
-    s[2][2] = (g.gz(2, i, j, k) + g.gz(2, i, j, k + 1)) / 2.;
-    s[1][2] = (g.gz(1, i, j, k) + g.gz(1, i, j, k + 1) + g.gy(2, i, j, k) + g.gy(2, i, j + 1, k)) / 4.;
-    s[0][2] = (g.gz(0, i, j, k) + g.gz(0, i, j, k + 1) + g.gx(2, i, j, k) + g.gx(2, i + 1, j, k)) / 4.;
-    s[0][1] = (g.gy(0, i, j, k) + g.gy(0, i, j + 1, k) + g.gx(1, i, j, k) + g.gx(1, i + 1, j, k)) / 4.;
-    s[2][1] = s[1][2]; s[2][0] = s[0][2]; s[1][0] = s[0][1];
-    io.eps_g[0][c] = s[0][0]; io.eps_g[1][c] = s[1][1]; io.eps_g[2][c] = s[2][2];
-    io.eps_g[3][c] = s[1][2]; io.eps_g[4][c] = s[0][2]; io.eps_g[5][c] = s[0][1];
+// cell strain in the crystal frame (Dexx_crt ..., get_Dstrain)
+__device__ inline void strain_crt(const Params& P, const GradView& g, long i, long j, long k, double e[6]) {
+    g.strain_glb(i, j, k, e);
     if (P.rot) {
-        double o[3][3];
+        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
         rot_tensor(P.Tg2c, s, o);
-        io.eps_c[0][c] = o[0][0]; io.eps_c[1][c] = o[1][1]; io.eps_c[2][c] = o[2][2];
-        io.eps_c[3][c] = o[1][2]; io.eps_c[4][c] = o[0][2]; io.eps_c[5][c] = o[0][1];
-    }
-
-    // ---- dynamic eigenstrain (get_eigenstrain_dynamic) ----
-    if (!P.elasto_back) return;
-    const uint8_t id = io.mid[c];
-    double e[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
-    if (id != 0) {
-        const DevMat& mt = io.mats[id - 1];
-        double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
-        if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
-        if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
-        const double third = 1. / 3.;
-        double e0[6] = {0., 0., 0., 0., 0., 0.};
-        if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
-        // (the reference's two-sublattice terms are exact zeros for decks
-        // without antiferromagnets, which this build rejects)
-        e[0][0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz)) - e0[0];
-        e[1][1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz)) - e0[1];
-        e[2][2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px)) - e0[2];
-        e[1][2] = mt.l111_15 * my * mz + mt.Q44 * py * pz - e0[3];
-        e[0][2] = mt.l111_15 * mx * mz + mt.Q44 * px * pz - e0[4];
-        e[0][1] = mt.l111_15 * my * mx + mt.Q44 * py * px - e0[5];
-        e[2][1] = e[1][2]; e[2][0] = e[0][2]; e[1][0] = e[0][1];
-    }
-    io.eig_c[0][c] = e[0][0]; io.eig_c[1][c] = e[1][1]; io.eig_c[2][c] = e[2][2];
-    io.eig_c[3][c] = e[1][2]; io.eig_c[4][c] = e[0][2]; io.eig_c[5][c] = e[0][1];
-    if (P.rot) {
-        double o[3][3];
-        rot_tensor(P.Tc2g, e, o);
-        io.eig_g[0][c] = o[0][0]; io.eig_g[1][c] = o[1][1]; io.eig_g[2][c] = o[2][2];
-        io.eig_g[3][c] = o[1][2]; io.eig_g[4][c] = o[0][2]; io.eig_g[5][c] = o[0][1];
+        e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
     }
 }
 
-// Stress on one face, averaged over the two cells sharing it (each with its
-// own stiffness, strain and eigenstrain), in the reference's order.
-__device__ inline void face_avg(const double sa[6], const double sb[6], double out[6]) {
-    for (int a = 0; a < 6; a++) out[a] = (sa[a] + sb[a]) / 2.;
+// dynamic eigenstrain of cell c in the crystal frame (Dexx0_crt ...,
+// get_eigenstrain_dynamic); the reference's two-sublattice terms are exact
+// zeros for decks without antiferromagnets, which this build rejects
+__device__ inline void eigen_crt(const Params& P, const StageIO& io, long c, double e[6]) {
+    const uint8_t id = io.mid[c];
+    for (int a = 0; a < 6; a++) e[a] = 0.;
+    if (id == 0) return;
+    const DevMat& mt = io.mats[id - 1];
+    double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
+    if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
+    if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
+    const double third = 1. / 3.;
+    double e0[6] = {0., 0., 0., 0., 0., 0.};
+    if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
+    e[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz)) - e0[0];
+    e[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz)) - e0[1];
+    e[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px)) - e0[2];
+    e[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz - e0[3];
+    e[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz - e0[4];
+    e[5] = mt.l111_15 * my * mx + mt.Q44 * py * px - e0[5];
+}
+
+// eigenstrain in the global frame (Dexx0_glb ...)
+__device__ inline void eigen_glb(const Params& P, const StageIO& io, long c, double e[6]) {
+    eigen_crt(P, io, c, e);
+    if (P.rot) {
+        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
+        rot_tensor(P.Tc2g, s, o);
+        e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
+    }
+}
+
+// Rows of the Voigt stress that the divergence uses from a face normal to
+// direction d: x-face -> xx, xy, xz; y-face -> xy, yy, yz; z-face -> xz, yz, zz
+__constant__ const int kFaceRows[3][3] = {{0, 5, 4}, {5, 1, 3}, {4, 3, 2}};
+
+// rows r[0..2] of C * e with the accumulation order of strain2stress_glb
+// (mathlib.cpp:127-135); zero entries of the cubic pattern are skipped,
+// which leaves every partial sum unchanged
+__device__ inline double stress_row(const DevMat& m, const double e[6], int r) {
+    if (m.cubic_c) {
+        if (r < 3) return m.cij[r][0] * e[0] + m.cij[r][1] * e[1] + m.cij[r][2] * e[2];
+        return m.cij[r][r] * e[r];
+    }
+    double acc = 0.;
+    for (int q = 0; q < 6; q++) acc = acc + m.cij[r][q] * e[q];
+    return acc;
+}
+
+// Face-normal component d, side 0 (-face) or 1 (+face) of cell (i,j,k):
+// the three stress rows averaged over the two cells sharing the face
+// (get_dv_RK*, elastic_dynamic_solver.cpp:876-1289), 0 on stress-free faces
+// except the surface traction source.
+template <int S, int D>
+__device__ inline void face_stress(const Params& P, const StageIO& io, const GradView& g, long i, long j, long k,
+                                   int side, const double d0c[6], double out[3]) {
+    const bool back = P.elasto_back;
+    long f, ii = i, jj = j, kk = k;
+    bool fr;
+    if (D == 0) { f = i + side; fr = free_x(P, io.mid, f, j, k); }
+    else if (D == 1) { f = j + side; fr = free_y(P, io.mid, i, f, k); }
+    else { f = k + side; fr = free_z(P, io.mid, i, j, f); }
+    if (fr) {
+        out[0] = out[1] = out[2] = 0.;
+        if (D == 2 && side == 1 && P.strain_pulse && P.strain_type == 3 && k == (long)P.source_z) {
+            const double tr = stage_drive(io, S).traction;   // x -> xz, y -> yz, z -> zz
+            if (P.strain_comp == 0) out[0] = tr; else if (P.strain_comp == 1) out[1] = tr; else out[2] = tr;
+        }
+        return;
+    }
+    // neighbour across the face (the +z neighbour wraps when k == ny-1, sic:
+    // elastic_dynamic_solver.cpp:1247; k == nz-1 != ny-1 with a non-free top
+    // face reads out of the column in the reference and is rejected at creation)
+    if (D == 0) ii = side ? ((i == P.nx - 1) ? 0 : i + 1) : ((i == 0) ? P.nx - 1 : i - 1);
+    else if (D == 1) jj = side ? ((j == P.ny - 1) ? 0 : j + 1) : ((j == 0) ? P.ny - 1 : j - 1);
+    else { kk = side ? ((k == P.ny - 1) ? 0 : k + 1) : ((k == 0) ? P.nz - 1 : k - 1); if (kk >= P.nz) kk = 0; }
+    double ga, gb, gc;   // face gradients: normal comp, and the two shear comps used below
+    if (D == 0) { ga = g.gx(0, f, j, k); gb = g.gx(2, f, j, k); gc = g.gx(1, f, j, k); }
+    else if (D == 1) { ga = g.gy(1, i, f, k); gb = g.gy(2, i, f, k); gc = g.gy(0, i, f, k); }
+    else { ga = g.gz(2, i, j, f); gb = g.gz(1, i, j, f); gc = g.gz(0, i, j, f); }
+    double sa[3], sb[3];
+    for (int which = 0; which < 2; which++) {
+        const long ci = which ? ii : i, cj = which ? jj : j, ck = which ? kk : k;
+        const long cc = cid(P, ci, cj, ck);
+        double d0[6];
+        if (which == 0) { for (int a = 0; a < 6; a++) d0[a] = d0c[a]; }
+        else if (back) eigen_glb(P, io, cc, d0);
+        else { for (int a = 0; a < 6; a++) d0[a] = 0.; }
+        double st[6];
+        if (D == 0) {
+            st[0] = ga - d0[0];
+            st[1] = g.eyy(ci, cj, ck) - d0[1];
+            st[2] = g.ezz(ci, cj, ck) - d0[2];
+            st[3] = (g.eyz(ci, cj, ck) - d0[3]) * 2.;
+            st[4] = ((g.gz(0, ci, cj, ck) + g.gz(0, ci, cj, ck + 1) + gb * 2.) / 4. - d0[4]) * 2.;
+            st[5] = ((g.gy(0, ci, cj, ck) + g.gy(0, ci, cj + 1, ck) + gc * 2.) / 4. - d0[5]) * 2.;
+        } else if (D == 1) {
+            st[0] = g.exx(ci, cj, ck) - d0[0];
+            st[1] = ga - d0[1];
+            st[2] = g.ezz(ci, cj, ck) - d0[2];
+            st[3] = ((g.gz(1, ci, cj, ck) + g.gz(1, ci, cj, ck + 1) + gb * 2.) / 4. - d0[3]) * 2.;
+            st[4] = (g.exz(ci, cj, ck) - d0[4]) * 2.;
+            st[5] = ((gc * 2. + g.gx(1, ci, cj, ck) + g.gx(1, ci + 1, cj, ck)) / 4. - d0[5]) * 2.;
+        } else {
+            st[0] = g.exx(ci, cj, ck) - d0[0];
+            st[1] = g.eyy(ci, cj, ck) - d0[1];
+            st[2] = ga - d0[2];
+            st[3] = ((gb * 2. + g.gy(2, ci, cj, ck) + g.gy(2, ci, cj + 1, ck)) / 4. - d0[3]) * 2.;
+            st[4] = ((gc * 2. + g.gx(2, ci, cj, ck) + g.gx(2, ci + 1, cj, ck)) / 4. - d0[4]) * 2.;
+            st[5] = (g.exy(ci, cj, ck) - d0[5]) * 2.;
+        }
+        const DevMat& m = io.mats[io.mid[cc] - 1];
+        if (which == 0) { for (int r = 0; r < 3; r++) sa[r] = stress_row(m, st, kFaceRows[D][r]); }
+        else { for (int r = 0; r < 3; r++) sb[r] = stress_row(m, st, kFaceRows[D][r]); }
+    }
+    for (int r = 0; r < 3; r++) out[r] = (sa[r] + sb[r]) / 2.;
+}
+
+// divergence term of direction D: (sigma(+face) - sigma(-face)) / h for the
+// three rows of kFaceRows[D], ordered as force x, y, z components
+template <int S, int D>
+__device__ inline void div_term(const Params& P, const StageIO& io, const GradView& g, long i, long j, long k,
+                                const double d0c[6], double t[3]) {
+    double s1[3], s2[3];
+    face_stress<S, D>(P, io, g, i, j, k, 0, d0c, s1);
+    face_stress<S, D>(P, io, g, i, j, k, 1, d0c, s2);
+    const double h = (D == 0) ? P.dx : (D == 1 ? P.dy : P.dz);
+    // kFaceRows[D][r] is the row feeding force component r
+    for (int r = 0; r < 3; r++) t[r] = (s2[r] - s1[r]) / h;
 }
 
 template <int S>
-__global__ void __launch_bounds__(256) k_elastic(Params P, StageIO io) {
+__global__ void __launch_bounds__(256, 2) k_elastic(Params P, StageIO io) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long nyz = (long)P.ny * P.nz;
     const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
-    UGrad g(P, io);
-    const StageDrive& dr = stage_drive(io, S);
+    const GradView g(P, io);
     const uint8_t id = io.mid[c];
-
-    auto E = [&](int a, long cc) { return io.eps_g[a][cc]; };
-    auto D0 = [&](int a, long cc) { return P.elasto_back ? io.eig_g[a][cc] : 0.; };
-    auto stress_of = [&](long cc, const double st[6], double out[6]) {
-        strain2stress(io.mats[io.mid[cc] - 1], st, out);
-    };
 
     double dv[3] = {0., 0., 0.};
     if (id != 0) {
-        double s1x[6], s2x[6], s1y[6], s2y[6], s1z[6], s2z[6];
-        double st[6], sa[6], sb[6];
-        // ---------------- x faces ----------------
-        for (int side = 0; side < 2; side++) {
-            const long f = i + side;                 // face index
-            double* out = side ? s2x : s1x;
-            if (g.free_x(f, j, k)) { for (int a = 0; a < 6; a++) out[a] = 0.; continue; }
-            const long io2 = side ? ((i == P.nx - 1) ? 0 : i + 1) : ((i == 0) ? P.nx - 1 : i - 1);
-            const double gxx = g.gx(0, f, j, k), gxz = g.gx(2, f, j, k), gxy = g.gx(1, f, j, k);
-            for (int which = 0; which < 2; which++) {
-                const long ii = which ? io2 : i;
-                const long cc = cid(P, ii, j, k);
-                st[0] = gxx - D0(0, cc);
-                st[1] = E(1, cc) - D0(1, cc);
-                st[2] = E(2, cc) - D0(2, cc);
-                st[3] = (E(3, cc) - D0(3, cc)) * 2.;
-                st[4] = ((g.gz(0, ii, j, k) + g.gz(0, ii, j, k + 1) + gxz * 2.) / 4. - D0(4, cc)) * 2.;
-                st[5] = ((g.gy(0, ii, j, k) + g.gy(0, ii, j + 1, k) + gxy * 2.) / 4. - D0(5, cc)) * 2.;
-                stress_of(cc, st, which ? sb : sa);
-            }
-            face_avg(sa, sb, out);
-        }
-        // ---------------- y faces ----------------
-        for (int side = 0; side < 2; side++) {
-            const long f = j + side;
-            double* out = side ? s2y : s1y;
-            if (g.free_y(i, f, k)) { for (int a = 0; a < 6; a++) out[a] = 0.; continue; }
-            const long jo = side ? ((j == P.ny - 1) ? 0 : j + 1) : ((j == 0) ? P.ny - 1 : j - 1);
-            const double gyy = g.gy(1, i, f, k), gyz = g.gy(2, i, f, k), gyx = g.gy(0, i, f, k);
-            for (int which = 0; which < 2; which++) {
-                const long jj = which ? jo : j;
-                const long cc = cid(P, i, jj, k);
-                st[0] = E(0, cc) - D0(0, cc);
-                st[1] = gyy - D0(1, cc);
-                st[2] = E(2, cc) - D0(2, cc);
-                st[3] = ((g.gz(1, i, jj, k) + g.gz(1, i, jj, k + 1) + gyz * 2.) / 4. - D0(3, cc)) * 2.;
-                st[4] = (E(4, cc) - D0(4, cc)) * 2.;
-                st[5] = ((gyx * 2. + g.gx(1, i, jj, k) + g.gx(1, i + 1, jj, k)) / 4. - D0(5, cc)) * 2.;
-                stress_of(cc, st, which ? sb : sa);
-            }
-            face_avg(sa, sb, out);
-        }
-        // ---------------- z faces ----------------
-        for (int side = 0; side < 2; side++) {
-            const long f = k + side;
-            double* out = side ? s2z : s1z;
-            if (g.free_z(i, j, f)) {
-                for (int a = 0; a < 6; a++) out[a] = 0.;
-                if (side == 1 && P.strain_pulse && P.strain_type == 3 && k == (long)P.source_z)
-                    out[4 - P.strain_comp] = dr.traction;   // x -> [4], y -> [3], z -> [2]
-                continue;
-            }
-            // +z neighbour: the reference wraps when k == ny-1 (sic), see
-            // elastic_dynamic_solver.cpp:1247
-            // (k == nz-1 != ny-1 with a non-free top face reads out of the
-            // column in the reference; such decks are rejected at creation)
-            long ko = side ? ((k == P.ny - 1) ? 0 : k + 1) : ((k == 0) ? P.nz - 1 : k - 1);
-            if (ko >= P.nz) ko = 0;
-            const double gzz = g.gz(2, i, j, f), gzy = g.gz(1, i, j, f), gzx = g.gz(0, i, j, f);
-            for (int which = 0; which < 2; which++) {
-                const long kk = which ? ko : k;
-                const long cc = cid(P, i, j, kk);
-                st[0] = E(0, cc) - D0(0, cc);
-                st[1] = E(1, cc) - D0(1, cc);
-                st[2] = gzz - D0(2, cc);
-                st[3] = ((gzy * 2. + g.gy(2, i, j, kk) + g.gy(2, i, j + 1, kk)) / 4. - D0(3, cc)) * 2.;
-                st[4] = ((gzx * 2. + g.gx(2, i, j, kk) + g.gx(2, i + 1, j, kk)) / 4. - D0(4, cc)) * 2.;
-                st[5] = (E(5, cc) - D0(5, cc)) * 2.;
-                stress_of(cc, st, which ? sb : sa);
-            }
-            face_avg(sa, sb, out);
-        }
-
+        double d0c[6];
+        if (P.elasto_back) eigen_glb(P, io, c, d0c); else for (int a = 0; a < 6; a++) d0c[a] = 0.;
+        double tx[3], ty[3], tz[3];
+        div_term<S, 0>(P, io, g, i, j, k, d0c, tx);
+        div_term<S, 1>(P, io, g, i, j, k, d0c, ty);
+        div_term<S, 2>(P, io, g, i, j, k, d0c, tz);
         const DevMat& mt = io.mats[id - 1];
-        double f3[3];
-        f3[0] = (s2x[0] - s1x[0]) / P.dx + (s2y[5] - s1y[5]) / P.dy + (s2z[4] - s1z[4]) / P.dz;
-        f3[1] = (s2x[5] - s1x[5]) / P.dx + (s2y[1] - s1y[1]) / P.dy + (s2z[3] - s1z[3]) / P.dz;
-        f3[2] = (s2x[4] - s1x[4]) / P.dx + (s2y[3] - s1y[3]) / P.dy + (s2z[2] - s1z[2]) / P.dz;
         for (int a = 0; a < 3; a++) {
+            const double f = tx[a] + ty[a] + tz[a];
             const double fs = io.force_store.c[a][c];
             if (S == 1 || S == 2)
-                dv[a] = f3[a] * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f3[a] - fs) * 2.;
+                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs) * 2.;
             else
-                dv[a] = f3[a] * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f3[a] - fs);
-            io.force.c[a][c] = f3[a];
-            if (S == 0) io.force_store.c[a][c] = f3[a];
+                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs);
+            if (S == 0) io.force_store.c[a][c] = f;
         }
     }
 
     // ---- RK4 combination for v and u (du = v_stage * dt) ----
     for (int a = 0; a < 3; a++) {
         const double du = io.v_in.c[a][c] * P.dt;
-        const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
         if (S == 0) {
+            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
             io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + dv[a] / 6.;
             io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + du / 6.;
         } else if (S == 1) {
+            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
             io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 3.;
             io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 3.;
         } else if (S == 2) {
+            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
             io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 3.;
             io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 3.;
         } else {
@@ -247,6 +277,18 @@ __global__ void __launch_bounds__(256) k_elastic(Params P, StageIO io) {
             io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 6.;
         }
     }
+}
+
+// cell strain (global frame) of the current step for output (Dexx_glb ...)
+__global__ void k_cell_strain(Params P, StageIO io, double* out6) {
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long nyz = (long)P.ny * P.nz;
+    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const GradView g(P, io);
+    double e[6];
+    g.strain_glb(i, j, k, e);
+    for (int a = 0; a < 6; a++) out6[(long)a * P.n + c] = e[a];
 }
 
 // Boundary planes of u after the stage update, one thread per (i,j).

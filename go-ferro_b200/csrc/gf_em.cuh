@@ -1,13 +1,15 @@
 // Yee-grid Maxwell stage kernels (FP64).
 //
-//   k_em_E<S,C>   one thread per C-edge: curl H of the stage state, the
+//   k_em_fused<S> one thread per Yee vertex, updating the E edges and H
+//                 faces that share its index:
+//   E edges:      curl H of the stage state, the
 //                 4-cell edge averages of permittivity, conductivity, free
 //                 current, polarisation current dP/dt (get_dE_RK{1..4},
 //                 EMdynamic_solver.cpp:337-2238) and the RK4 combination of
 //                 update_DE_RK*/update_DE (:3588-3777).  Edges on a
 //                 non-periodic system boundary get no curl term; the Mur
 //                 kernel sets them afterwards.
-//   k_em_H<S,C>   one thread per C-face: curl E and the 2-cell average of
+//   H faces:      curl E and the 2-cell average of
 //                 Ms dm/dt of the same stage (get_dH_RK{1..4}, :2239-3476)
 //                 with update_DH_RK*/update_DH (:3477-3586).
 //   k_em_plane<S> hard plane-wave source on z = planeEM_source_z
@@ -40,15 +42,10 @@ __device__ inline void rk_x(double xv, double d, double* out, double* acc, long 
     else { acc[e] = acc[e] + d / 6.; }
 }
 
-// E edge update.  C = component (0 x, 1 y, 2 z).
+// E edge update of component C at edge (i,j,k) (index e in C's array).
 template <int S, int C>
-__global__ void __launch_bounds__(256) k_em_E(Params P, StageIO io) {
+__device__ inline void em_E_edge(const Params& P, const StageIO& io, const StageDrive& dr, long i, long j, long k, long e) {
     const long nx = P.nx, ny = P.ny, nz = P.nz;
-    const long dx_ = nx + (C != 0), dy_ = ny + (C != 1), dz_ = nz + (C != 2);
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= dx_ * dy_ * dz_) return;
-    const long i = e / (dy_ * dz_), j = (e - i * dy_ * dz_) / dz_, k = e - i * dy_ * dz_ - j * dz_;
-    const StageDrive& dr = stage_drive(io, S);
 
     double d = 0.;
     bool boundary = false;
@@ -124,14 +121,10 @@ __global__ void __launch_bounds__(256) k_em_E(Params P, StageIO io) {
     rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], e);
 }
 
-// H face update.  C = component.
+// H face update of component C at face (i,j,k) (index e in C's array).
 template <int S, int C>
-__global__ void __launch_bounds__(256) k_em_H(Params P, StageIO io) {
+__device__ inline void em_H_face(const Params& P, const StageIO& io, long i, long j, long k, long e) {
     const long nx = P.nx, ny = P.ny, nz = P.nz;
-    const long dx_ = nx + (C == 0), dy_ = ny + (C == 1), dz_ = nz + (C == 2);
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= dx_ * dy_ * dz_) return;
-    const long i = e / (dy_ * dz_), j = (e - i * dy_ * dz_) / dz_, k = e - i * dy_ * dz_ - j * dz_;
     const double* Ex = io.E_in.c[0];
     const double* Ey = io.E_in.c[1];
     const double* Ez = io.E_in.c[2];
@@ -174,6 +167,26 @@ __global__ void __launch_bounds__(256) k_em_H(Params P, StageIO io) {
     if (cnt < 0.5) cnt = 1.;
     const double d = -P.dt / kMu0 * curl - (dM1 + dM2) / cnt;
     rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], e);
+}
+
+// All six Yee components of one stage: thread (i,j,k) on the vertex grid
+// (nx+1)(ny+1)(nz+1) updates every E edge and H face with index (i,j,k)
+// inside that component's staggered extent.  E reads only the stage H and
+// H only the stage E and dm, so the six updates are independent.
+template <int S>
+__global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io) {
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long vyz = (ny + 1) * (nz + 1);
+    if (t >= (nx + 1) * vyz) return;
+    const long i = t / vyz, j = (t - i * vyz) / (nz + 1), k = t - i * vyz - j * (nz + 1);
+    const StageDrive& dr = stage_drive(io, S);
+    if (i < nx) em_E_edge<S, 0>(P, io, dr, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
+    if (j < ny) em_E_edge<S, 1>(P, io, dr, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (k < nz) em_E_edge<S, 2>(P, io, dr, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (j < ny && k < nz) em_H_face<S, 0>(P, io, i, j, k, (i * ny + j) * nz + k);
+    if (i < nx && k < nz) em_H_face<S, 1>(P, io, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (i < nx && j < ny) em_H_face<S, 2>(P, io, i, j, k, (i * ny + j) * (nz + 1) + k);
 }
 
 // hard plane-wave source: E on z = plane_z, all three components, i<nx, j<ny

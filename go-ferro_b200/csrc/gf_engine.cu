@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,8 +18,8 @@
 #include "gf_deck.h"
 #include "gf_launch.cuh"
 #include "gf_state.cuh"
-#include "gf_llg.cuh"
 #include "gf_elastic.cuh"
+#include "gf_llg.cuh"
 #include "gf_fe.cuh"
 #include "gf_em.cuh"
 #include "gf_demag.cuh"
@@ -70,13 +71,11 @@ struct gf_engine {
 
     Field3 m, p, q, u, v, E, H;
     double* dm[3] = {nullptr, nullptr, nullptr};
-    double* force[3] = {nullptr, nullptr, nullptr};
     double* force_store[3] = {nullptr, nullptr, nullptr};
     double* Hstat[3] = {nullptr, nullptr, nullptr};
     double* Estat[3] = {nullptr, nullptr, nullptr};
     double* Hnu[3] = {nullptr, nullptr, nullptr};
-    double* eps_g[6] = {}; double* eps_c[6] = {};
-    double* eig_g[6] = {}; double* eig_c[6] = {};
+    double* fg[9] = {};
     double* liao_hist = nullptr; double* liao_last = nullptr;
     double* scratch = nullptr;             // 6n doubles: output staging and reductions
     int* flag = nullptr;
@@ -298,6 +297,20 @@ void build_params(gf_engine* eng) {
     P.rot = d.orient_rotate;
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { P.Tg2c[i][j] = d.Tg2c[i][j]; P.Tc2g[i][j] = d.Tc2g[i][j]; }
     P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
+    {
+        long lo[3] = {d.nx, d.ny, d.nz}, hi[3] = {-1, -1, -1};
+        for (long i = 0; i < d.nx; i++)
+            for (long j = 0; j < d.ny; j++)
+                for (long k = 0; k < d.nz; k++) {
+                    const uint8_t id = d.material_cell[(size_t)((i * d.ny + j) * d.nz + k)];
+                    if (!id || !d.mats[id - 1].fm) continue;
+                    const long x[3] = {i, j, k};
+                    for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], x[a]); hi[a] = std::max(hi[a], x[a]); }
+                }
+        if (hi[0] < 0) { lo[0] = lo[1] = lo[2] = 0; hi[0] = hi[1] = hi[2] = -1; }
+        P.fm_i0 = lo[0]; P.fm_j0 = lo[1]; P.fm_k0 = lo[2];
+        P.fm_bi = hi[0] - lo[0] + 1; P.fm_bj = hi[1] - lo[1] + 1; P.fm_bk = hi[2] - lo[2] + 1;
+    }
     P.elasto_on = d.elasto_on; P.elasto_back = d.elasto_back && d.elastodynamics;
     P.em_fromM = d.em_fromM && d.em_dynamic && d.any_fm;
     P.em_fromP = d.em_fromP && d.em_dynamic && d.any_fe;
@@ -493,16 +506,12 @@ void build_io(gf_engine* eng) {
             if (eng->E.on) set_io_field(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out);
             if (eng->H.on) set_io_field(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out);
             io.dm = f3(eng->dm);
-            io.force = f3(eng->force);
             io.force_store = f3(eng->force_store);
             io.Hstat = f3(eng->Hstat);
             io.Estat = f3(eng->Estat);
             io.Hnu = f3(eng->Hnu);
-            for (int a = 0; a < 6; a++) {
-                io.eps_g[a] = eng->eps_g[a]; io.eps_c[a] = eng->eps_c[a];
-                io.eig_g[a] = eng->eig_g[a]; io.eig_c[a] = eng->eig_c[a];
-                io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr;
-            }
+            for (int a = 0; a < 9; a++) io.fg[a] = eng->fg[a];
+            for (int a = 0; a < 6; a++) { io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr; }
             io.liao_hist = eng->liao_hist;
             io.liao_last = eng->liao_last;
             io.mid = eng->mid;
@@ -524,20 +533,15 @@ int enqueue_stage(gf_engine* eng, int parity) {
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     if (P.elastic) {
-        GF_CU(klaunch(eng, "k_strain", k_strain, dim3(bn), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_face_grad", k_face_grad, dim3(bn), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic", k_elastic<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
-    if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(bn), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
+    if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
     if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
-        GF_CU(klaunch(eng, "k_em_E_x", k_em_E<S, 0>, dim3(blocks_for(nx * (ny + 1) * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_em_E_y", k_em_E<S, 1>, dim3(blocks_for((nx + 1) * ny * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_em_E_z", k_em_E<S, 2>, dim3(blocks_for((nx + 1) * (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_em_H_x", k_em_H<S, 0>, dim3(blocks_for((nx + 1) * ny * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_em_H_y", k_em_H<S, 1>, dim3(blocks_for(nx * (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_em_H_z", k_em_H<S, 2>, dim3(blocks_for(nx * ny * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_em_fused", k_em_fused<S>, dim3(blocks_for((nx + 1) * (ny + 1) * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
         if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
@@ -573,6 +577,7 @@ int enqueue_step(gf_engine* eng, int parity) {
     GF_TRY(enqueue_stage<2>(eng, parity));
     GF_TRY(enqueue_stage<3>(eng, parity));
     GF_CU(klaunch(eng, "k_step_inc", k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
+    eng->launches_per_step = eng->launch_counter;
     return GF_OK;
 }
 
@@ -633,6 +638,23 @@ int setup_demag(gf_engine* eng) {
 int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* src, long n) {
     for (int a = 0; a < 3; a++)
         GF_CU(cudaMemcpyAsync(dst[a], src[a].data(), sizeof(double) * n, cudaMemcpyHostToDevice, eng->stream));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+// copy the current-step buffer of every state field into its other three
+// buffers, so cells a stage kernel does not cover stay consistent
+int replicate_state(gf_engine* eng) {
+    Field3* fs[] = {&eng->m, &eng->p, &eng->q, &eng->u, &eng->v, &eng->E, &eng->H};
+    for (Field3* f : fs) {
+        if (!f->on) continue;
+        double* const* c = (eng->steps_done & 1ull) ? f->A : f->X;
+        for (int a = 0; a < 3; a++) {
+            double* others[3] = {(c == f->A) ? f->X[a] : f->A[a], f->S0[a], f->S1[a]};
+            for (double* o : others)
+                GF_CU(cudaMemcpyAsync(o, c[a], sizeof(double) * f->len[a], cudaMemcpyDeviceToDevice, eng->stream));
+        }
+    }
     GF_CU(cudaStreamSynchronize(eng->stream));
     return GF_OK;
 }
@@ -789,21 +811,14 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     for (int a = 0; a < 3; a++) {
         if (P.em_fromM) GF_TRY(dalloc_n(eng, &eng->dm[a], (size_t)n));
         if (d.elastodynamics) {
-            GF_TRY(dalloc_n(eng, &eng->force[a], (size_t)n));
             GF_TRY(dalloc_n(eng, &eng->force_store[a], (size_t)n));
         }
         if (d.any_fm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
         if (d.any_fe) GF_TRY(dalloc_n(eng, &eng->Estat[a], (size_t)n));
         if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_n(eng, &eng->Hnu[a], (size_t)n));
     }
-    if (d.elastodynamics || d.elasto_on) {
-        for (int a = 0; a < 6; a++) {
-            GF_TRY(dalloc_n(eng, &eng->eps_g[a], (size_t)n));
-            if (P.rot) GF_TRY(dalloc_n(eng, &eng->eps_c[a], (size_t)n)); else eng->eps_c[a] = eng->eps_g[a];
-            GF_TRY(dalloc_n(eng, &eng->eig_c[a], (size_t)n));
-            if (P.rot) GF_TRY(dalloc_n(eng, &eng->eig_g[a], (size_t)n)); else eng->eig_g[a] = eng->eig_c[a];
-        }
-    }
+    if (d.elastodynamics)
+        for (int a = 0; a < 9; a++) GF_TRY(dalloc_n(eng, &eng->fg[a], (size_t)n));
     if (d.elastodynamics) {
         const size_t plane = (size_t)P.nx * P.ny;
         GF_TRY(dalloc_n(eng, &eng->liao_hist, 4 * 12 * plane));
@@ -814,6 +829,7 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     GF_CU(cudaStreamSynchronize(eng->stream));
 
     GF_TRY(initial_state(eng, dir));
+    GF_TRY(replicate_state(eng));
     GF_TRY(setup_demag(eng));
     build_io(eng);
 
@@ -915,11 +931,16 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
             for (int a = 0; a < 3; a++) { ptrs.push_back(base + a * P.n); lens.push_back(P.n); }
             break;
         }
-        case GF_FIELD_STRAIN:
-            if (!eng->eps_g[0]) break;
+        case GF_FIELD_STRAIN: {
+            // strain of the current step value (face gradients recomputed from it)
+            if (!eng->u.on) break;
             writable = false;
-            for (int a = 0; a < 6; a++) { ptrs.push_back(eng->eps_g[a]); lens.push_back(P.n); }
+            StageIO io = eng->io[eng->steps_done & 1ull][0];
+            GF_CU(launch(k_face_grad, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+            GF_CU(launch(k_cell_strain, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io, eng->scratch));
+            for (int a = 0; a < 6; a++) { ptrs.push_back(eng->scratch + (size_t)a * P.n); lens.push_back(P.n); }
             break;
+        }
         default: break;
     }
     if (ptrs.empty()) { eng->err = "field " + std::to_string(field) + " is not present in this run"; return GF_EINVAL; }
@@ -1050,7 +1071,8 @@ int gf_upload(gf_engine* e, int field, const double* host, size_t count) {
     gf_engine* eng = e;
     if (!host) { eng->err = "null buffer"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
-    return copy_field(e, field, const_cast<double*>(host), count, false, cudaMemcpyHostToDevice, true);
+    GF_TRY(copy_field(e, field, const_cast<double*>(host), count, false, cudaMemcpyHostToDevice, true));
+    return replicate_state(e);
 }
 
 int gf_download_device(gf_engine* e, int field, double* dev, size_t count) {
@@ -1066,7 +1088,8 @@ int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count) {
     gf_engine* eng = e;
     if (!dev) { eng->err = "null buffer"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
-    return copy_field(e, field, const_cast<double*>(dev), count, false, cudaMemcpyDeviceToDevice, false);
+    GF_TRY(copy_field(e, field, const_cast<double*>(dev), count, false, cudaMemcpyDeviceToDevice, false));
+    return replicate_state(e);
 }
 
 int gf_get_info(gf_engine* e, gf_info* info) {

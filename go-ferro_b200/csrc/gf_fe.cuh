@@ -9,7 +9,7 @@
 // evaluated by multiplication instead of pow().
 #pragma once
 
-#include "gf_state.cuh"
+#include "gf_elastic.cuh"
 
 namespace gf {
 
@@ -61,11 +61,17 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
         double exx = 0, eyy = 0, ezz = 0, eyz = 0, exz = 0, exy = 0;
         double exx0 = 0, eyy0 = 0, ezz0 = 0, eyz0 = 0, exz0 = 0, exy0 = 0;
         if (P.elasto_on) {
-            exx = io.eps_c[0][c]; eyy = io.eps_c[1][c]; ezz = io.eps_c[2][c];
-            eyz = io.eps_c[3][c]; exz = io.eps_c[4][c]; exy = io.eps_c[5][c];
+            // dynamic strain and eigenstrain of the stage state, crystal frame
+            // (Dexx_crt, Dexx0_crt: ferroelectric_solver.cpp:624-652)
+            if (P.elastic) {
+                double e[6];
+                strain_crt(P, GradView(P, io), i, j, k, e);
+                exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
+            }
             if (P.elasto_back) {
-                exx0 = io.eig_c[0][c]; eyy0 = io.eig_c[1][c]; ezz0 = io.eig_c[2][c];
-                eyz0 = io.eig_c[3][c]; exz0 = io.eig_c[4][c]; exy0 = io.eig_c[5][c];
+                double e0[6];
+                eigen_crt(P, io, c, e0);
+                exx0 = e0[0]; eyy0 = e0[1]; ezz0 = e0[2]; eyz0 = e0[3]; exz0 = e0[4]; exy0 = e0[5];
             }
         }
 

@@ -16,7 +16,7 @@
 // of reads per cell and stage.
 #pragma once
 
-#include "gf_state.cuh"
+#include "gf_elastic.cuh"
 
 namespace gf {
 
@@ -28,22 +28,27 @@ __device__ inline bool is_fm(const DevMat* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FM);
 }
 
-// cell strain in the crystal frame plus the static strain (if any)
-__device__ inline void cell_strain_total(const StageIO& io, long c, double e[6]) {
+// static strain plus the cell strain of the stage displacement, crystal
+// frame (exxt0_crt + Dexx_crt, magnetic_solver.cpp:89-96)
+__device__ inline void cell_strain_total(const Params& P, const StageIO& io, long i, long j, long k, long c, double e[6]) {
+    double d[6] = {0., 0., 0., 0., 0., 0.};
+    if (P.elastic) strain_crt(P, GradView(P, io), i, j, k, d);
     for (int a = 0; a < 6; a++) {
         double t = io.eps0_c[a] ? io.eps0_c[a][c] : 0.;
-        e[a] = t + io.eps_c[a][c];
+        e[a] = t + d[a];
     }
 }
 
+// One thread per cell of the ferromagnetic bounding box; cells outside it
+// hold their initial m in all four buffers and are never touched.
 template <int S>
 __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGTables* __restrict__ tab) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    const long nyz = (long)P.ny * P.nz;
-    const long i = c / nyz;
-    const long j = (c - i * nyz) / P.nz;
-    const long k = c - i * nyz - j * P.nz;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long bjk = P.fm_bj * P.fm_bk;
+    if (t >= P.fm_bi * bjk) return;
+    const long bi = t / bjk, r = t - bi * bjk, bj = r / P.fm_bk;
+    const long i = P.fm_i0 + bi, j = P.fm_j0 + bj, k = P.fm_k0 + (r - bj * P.fm_bk);
+    const long c = cid(P, i, j, k);
 
     const uint8_t id = io.mid[c];
     double dmx = 0., dmy = 0., dmz = 0.;
@@ -56,7 +61,7 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
         double exx = 0., eyy = 0., ezz = 0., eyz = 0., exz = 0., exy = 0.;
         if (P.elasto_on) {
             double e[6];
-            cell_strain_total(io, c, e);
+            cell_strain_total(P, io, i, j, k, c, e);
             exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
         }
 

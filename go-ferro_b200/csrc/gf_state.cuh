@@ -25,18 +25,14 @@ struct StageIO {
     F3 p_in, p_x, p_acc, p_out, q_in, q_x, q_acc, q_out;
     // elastic displacement u and velocity v
     F3 u_in, u_x, u_acc, u_out, v_in, v_x, v_acc, v_out;
-    F3 force, force_store;
+    F3 force_store;   // stage-1 stress divergence (stiffness damping)
     // Yee E and H: component c of E lives on the c-edges, of H on the c-faces
     F3 E_in, E_x, E_acc, E_out, H_in, H_x, H_acc, H_out;
     // static and external fields
     F3 Hstat, Estat, Hnu;
-    // strain scratch written by the strain kernel each stage (6 Voigt-order
-    // components xx yy zz yz xz xy): dynamic strain (global / crystal frame)
-    // and dynamic eigenstrain (global / crystal frame)
-    double* eps_g[6];
-    double* eps_c[6];
-    double* eig_g[6];
-    double* eig_c[6];
+    // face-normal displacement gradients of the stage state, written by
+    // k_face_grad: fg[3*d + a] = d u_a / d x_d on the cell's -d face
+    double* fg[9];
     // optional static inputs (null when absent): static strain and static
     // eigenstrain in the crystal frame
     const double* eps0_c[6];
