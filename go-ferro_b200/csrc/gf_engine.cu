@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1192,5 +1193,70 @@ void gf_destroy(gf_engine* e) {
 }
 
 const char* gf_version(void) { return "goferro_b200 0.1 (FP64 parity path, sm_100a)"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free mean of a device array (gf_field_mean_noalloc).
+//
+// Same deterministic three-pass strided sum as gf_average, with its partial
+// sums in a file-scope device array instead of engine-owned scratch.  Pass 1
+// uses one partial per 1024 input elements, so the array bounds the input
+// length; passes 2 and 3 reduce the partials to 64 values and then one.
+// Every pass writes all the partials the next pass reads, so nothing in the
+// array has to start at zero.  The array is shared by all calls on a device
+// and keeps the last call's partials; calls that overlap on the GPU (two
+// streams, two host threads) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr long kNoAllocPass1 = 65536;                       // pass-1 partials
+constexpr long kNoAllocChunk = 1024;                        // elements per pass-1 partial
+constexpr long kNoAllocMaxElems = kNoAllocPass1 * kNoAllocChunk;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPass1 + 64 + 8];
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" {
+
+int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, double* dev_out, void* stream) {
+    auto fail = [](int code, const std::string& m) { g_create_err = m; return code; };
+    if (!dev_in || !dev_out) return fail(GF_EINVAL, "gf_field_mean_noalloc: null device pointer");
+    if (n == 0) return fail(GF_EINVAL, "gf_field_mean_noalloc: empty input");
+    if (n > (uint64_t)kNoAllocMaxElems)
+        return fail(GF_EINVAL, "gf_field_mean_noalloc: " + std::to_string(n) + " elements exceed the maximum of " +
+                                   std::to_string(kNoAllocMaxElems) + " (fixed scratch of " +
+                                   std::to_string(kNoAllocPass1) + " partial sums)");
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
+    if (dev < 0 || dev >= kMaxDevices) return fail(GF_ENODEV, "gf_field_mean_noalloc: device index out of range");
+    double* scratch = nullptr;
+    {
+        // once per device, with that device current: the device address of
+        // the file-scope array (its host-side name is not a device address)
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* addr = nullptr;
+            ce = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+            g_noalloc_addr[dev] = static_cast<double*>(addr);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* p1 = scratch;
+    double* p2 = scratch + kNoAllocPass1;
+    const long T1 = (long)((n + kNoAllocChunk - 1) / kNoAllocChunk);
+    launch(k_sum_stride, dim3(blocks_for(T1, 256)), dim3(256), 0, st, dev_in, (long)n, p1, T1);
+    launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, T1, p2, 64L);
+    launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, dev_out, 1L);
+    launch(k_scale, dim3(1), dim3(1), 0, st, dev_out, divisor);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
+    return GF_OK;
+}
+
 
 }  // extern "C"

@@ -19,6 +19,9 @@ __global__ void k_sum_stride(const double* __restrict__ in, long n, double* __re
     partial[t] = acc;
 }
 
+// x[0] := x[0] / d  (single thread; the mean of gf_field_mean_noalloc)
+__global__ void k_scale(double* x, double d) { x[0] = x[0] / d; }
+
 // flag := 1 if any element of in[0..n) is not finite
 __global__ void k_check_finite(const double* __restrict__ in, long n, int* flag) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

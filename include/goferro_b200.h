@@ -172,6 +172,28 @@ const char* gf_last_error(const gf_engine* e);
 /* Free the engine and all its device memory. */
 void gf_destroy(gf_engine* e);
 
+/* Mean of a device array, allocating nothing: *dev_out = sum(dev_in[0..n)) /
+ * divisor, as a deterministic FP64 sum queued on `stream` (a cudaStream_t;
+ * NULL = legacy default stream).  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they run: code whose
+ * device memory belongs to another runtime (the reference's OpenACC data
+ * regions, a caller-managed pool), or that runs where cudaMalloc is not
+ * allowed or would stall the device (it synchronises the whole device, and
+ * it cannot be called while a stream is being captured).  Inputs and output
+ * are caller-owned device pointers; the partial sums live in a fixed
+ * file-scope device array of 65,600 doubles (about 513 KB) that every GPU
+ * which loads the library holds until the process exits.
+ *   - n must be 1..67,108,864 (64 Mi); larger inputs return GF_EINVAL with
+ *     the limit in gf_last_error(NULL).
+ *   - The first call on a device looks up that array's device address; make
+ *     that first call before any stream capture on the device.
+ *   - All calls on a device share the array: calls that overlap on the GPU
+ *     (two streams, two host threads) race and give wrong sums.  Serialise
+ *     them on one stream.
+ * Errors are reported through gf_last_error(NULL). */
+int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, double* dev_out, void* stream);
+
 /* Library version string. */
 const char* gf_version(void);
 
