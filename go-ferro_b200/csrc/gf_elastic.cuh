@@ -1,24 +1,24 @@
 // Elastodynamics stage kernels (FP64).
 //
-//   k_face_grad   per cell: the face-normal displacement gradients on the
-//                 cell's -x, -y and -z faces, 3 components each, 0 on
-//                 stress-free faces (get_dudxyz_glb, elastic_dynamic_solver.cpp:
-//                 106-187).  Each gradient is computed once per stage.
-//   k_elastic     per cell: cell strains (get_Dstrain, :189-227) and dynamic
-//                 eigenstrains of m and p (get_eigenstrain_dynamic, :3-104) of
-//                 the cell and its six face neighbours, the six face stresses,
+//   k_elastic_tile  per cell, tiled over (j,k) and marching along x: the
+//                 face-normal displacement gradients (get_dudxyz_glb,
+//                 elastic_dynamic_solver.cpp:106-187), cell strains (get_Dstrain,
+//                 :189-227) and dynamic eigenstrains of m and p
+//                 (get_eigenstrain_dynamic, :3-104), the six face stresses,
 //                 stress divergence, velocity and displacement increments and
-//                 their RK4 combination (get_dv_RK{1..4} :841-2800,
-//                 get_du_RK* :2801-2847, update_v*/update_u* :2849-3057).
+//                 their RK4 combination (get_dv_RK{1..4} :841-2800, get_du_RK*
+//                 :2801-2847, update_v*/update_u* :2849-3057); it also stores
+//                 the crystal-frame cell strain of magnetic/ferroelectric cells.
 //   k_elastic_bc  per (i,j) column: z absorbing boundary (Liao 4th order or
 //                 first-order Mur, elastodynamics_AbsorbingBoundary.cpp:91-230)
 //                 and the displacement source plane (update_Du_Gaussian*,
 //                 elastic_dynamic_solver.cpp:3059-3284), in that order.
+//   k_face_grad, k_cell_strain  the cell strain of the current state, for
+//                 output only.
 //
 // Face f of an axis with n cells is stored at cell index f for f < n; face n
 // is read from index 0, which holds the same value (periodic axis) or the
-// same zero (non-periodic axis: both end faces are stress-free).  Strains and
-// eigenstrains are recomputed where used instead of being stored.
+// same zero (non-periodic axis: both end faces are stress-free).
 #pragma once
 
 #include "gf_state.cuh"
@@ -87,19 +87,9 @@ struct GradView {
     }
 };
 
-// cell strain in the crystal frame (Dexx_crt ..., get_Dstrain)
-__device__ inline void strain_crt(const Params& P, const GradView& g, long i, long j, long k, double e[6]) {
-    g.strain_glb(i, j, k, e);
-    if (P.rot) {
-        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
-        rot_tensor(P.Tg2c, s, o);
-        e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
-    }
-}
-
 // dynamic eigenstrain of cell c in the crystal frame (Dexx0_crt ...,
 // get_eigenstrain_dynamic); the reference's two-sublattice terms are exact
-// zeros for decks without antiferromagnets, which this build rejects
+// zeros for decks without antiferromagnets, which the engine rejects at creation
 __device__ inline void eigen_crt(const Params& P, const StageIO& io, long c, double e[6]) {
     const uint8_t id = io.mid[c];
     for (int a = 0; a < 6; a++) e[a] = 0.;
@@ -146,120 +136,113 @@ __device__ inline double stress_row(const DevMat& m, const double e[6], int r) {
     return acc;
 }
 
-// Face-normal component d, side 0 (-face) or 1 (+face) of cell (i,j,k):
-// the three stress rows averaged over the two cells sharing the face
-// (get_dv_RK*, elastic_dynamic_solver.cpp:876-1289), 0 on stress-free faces
-// except the surface traction source.
-template <int S, int D>
-__device__ inline void face_stress(const Params& P, const StageIO& io, const GradView& g, long i, long j, long k,
-                                   int side, const double d0c[6], double out[3]) {
-    const bool back = P.elasto_back;
-    long f, ii = i, jj = j, kk = k;
-    bool fr;
-    if (D == 0) { f = i + side; fr = free_x(P, io.mid, f, j, k); }
-    else if (D == 1) { f = j + side; fr = free_y(P, io.mid, i, f, k); }
-    else { f = k + side; fr = free_z(P, io.mid, i, j, f); }
-    if (fr) {
-        out[0] = out[1] = out[2] = 0.;
-        if (D == 2 && side == 1 && P.strain_pulse && P.strain_type == 3 && k == (long)P.source_z) {
-            const double tr = stage_drive(io, S).traction;   // x -> xz, y -> yz, z -> zz
-            if (P.strain_comp == 0) out[0] = tr; else if (P.strain_comp == 1) out[1] = tr; else out[2] = tr;
-        }
-        return;
+// ---------------------------------------------------------------------------
+// Tiled stage kernel.  A block owns a TJ x TK tile of (j,k) columns and
+// marches along x over `chunk` planes.  For every plane it stages in shared
+// memory the face-normal displacement gradients of the tile and a one-cell
+// halo (GX on the x-faces, two planes; GY, GZ on the y- and z-faces) and the
+// global-frame eigenstrains, so that each gradient and eigenstrain is
+// computed once.  Each thread then forms its cell's y- and z-face stresses
+// from shared memory, and the x-face stresses are computed once per face:
+// the cell below a face contributes its half while the previous plane is
+// processed and the sum is completed one plane later.
+//
+// A face stress (get_dv_RK*, elastic_dynamic_solver.cpp:876-1289) is the
+// mean over the two cells sharing the face of three rows of C (strain -
+// eigenstrain), where each cell's strain takes the face's own gradient for
+// the normal component and for the shear components that involve it; it is
+// 0 on stress-free faces, except for the surface traction source.  Every
+// expression keeps the reference's operation order (rounding included).
+// ---------------------------------------------------------------------------
+namespace etile {
+constexpr int TJ = 8, TK = 32, NT = TJ * TK;
+constexpr int HJ = TJ + 2, HK = TK + 2;      // cells of the tile and halo
+constexpr int GYR = TJ + 3, GZC = TK + 3;    // face rows (y) / columns (z)
+constexpr int kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
+constexpr size_t kSmemBytes = (size_t)(2 * kGX + kGY + kGZ + kD0) * sizeof(double) + (size_t)HJ * HK;
+}  // namespace etile
+
+__device__ inline int wrapm(int x, int n) { return x < 0 ? x + n : (x >= n ? x % n : x); }
+
+// gradients of a cell held in the shared tile: gm(d,a) on the -d face,
+// gp(d,a) on the +d face, d0(a) the global-frame eigenstrain
+struct TileCell {
+    const double *gxm, *gxp, *gy, *gz, *d0s;
+    int r, s;
+    __device__ double gm(int d, int a) const {
+        using namespace etile;
+        return d == 0 ? gxm[(a * HJ + r) * HK + s] : (d == 1 ? gy[(a * GYR + r) * HK + s] : gz[(a * HJ + r) * GZC + s]);
     }
-    // neighbour across the face (the +z neighbour wraps when k == ny-1, sic:
-    // elastic_dynamic_solver.cpp:1247; k == nz-1 != ny-1 with a non-free top
-    // face reads out of the column in the reference and is rejected at creation)
-    if (D == 0) ii = side ? ((i == P.nx - 1) ? 0 : i + 1) : ((i == 0) ? P.nx - 1 : i - 1);
-    else if (D == 1) jj = side ? ((j == P.ny - 1) ? 0 : j + 1) : ((j == 0) ? P.ny - 1 : j - 1);
-    else { kk = side ? ((k == P.ny - 1) ? 0 : k + 1) : ((k == 0) ? P.nz - 1 : k - 1); if (kk >= P.nz) kk = 0; }
-    double ga, gb, gc;   // face gradients: normal comp, and the two shear comps used below
-    if (D == 0) { ga = g.gx(0, f, j, k); gb = g.gx(2, f, j, k); gc = g.gx(1, f, j, k); }
-    else if (D == 1) { ga = g.gy(1, i, f, k); gb = g.gy(2, i, f, k); gc = g.gy(0, i, f, k); }
-    else { ga = g.gz(2, i, j, f); gb = g.gz(1, i, j, f); gc = g.gz(0, i, j, f); }
-    double sa[3], sb[3];
-    for (int which = 0; which < 2; which++) {
-        const long ci = which ? ii : i, cj = which ? jj : j, ck = which ? kk : k;
-        const long cc = cid(P, ci, cj, ck);
-        double d0[6];
-        if (which == 0) { for (int a = 0; a < 6; a++) d0[a] = d0c[a]; }
-        else if (back) eigen_glb(P, io, cc, d0);
-        else { for (int a = 0; a < 6; a++) d0[a] = 0.; }
-        double st[6];
-        if (D == 0) {
-            st[0] = ga - d0[0];
-            st[1] = g.eyy(ci, cj, ck) - d0[1];
-            st[2] = g.ezz(ci, cj, ck) - d0[2];
-            st[3] = (g.eyz(ci, cj, ck) - d0[3]) * 2.;
-            st[4] = ((g.gz(0, ci, cj, ck) + g.gz(0, ci, cj, ck + 1) + gb * 2.) / 4. - d0[4]) * 2.;
-            st[5] = ((g.gy(0, ci, cj, ck) + g.gy(0, ci, cj + 1, ck) + gc * 2.) / 4. - d0[5]) * 2.;
-        } else if (D == 1) {
-            st[0] = g.exx(ci, cj, ck) - d0[0];
-            st[1] = ga - d0[1];
-            st[2] = g.ezz(ci, cj, ck) - d0[2];
-            st[3] = ((g.gz(1, ci, cj, ck) + g.gz(1, ci, cj, ck + 1) + gb * 2.) / 4. - d0[3]) * 2.;
-            st[4] = (g.exz(ci, cj, ck) - d0[4]) * 2.;
-            st[5] = ((gc * 2. + g.gx(1, ci, cj, ck) + g.gx(1, ci + 1, cj, ck)) / 4. - d0[5]) * 2.;
-        } else {
-            st[0] = g.exx(ci, cj, ck) - d0[0];
-            st[1] = g.eyy(ci, cj, ck) - d0[1];
-            st[2] = ga - d0[2];
-            st[3] = ((gb * 2. + g.gy(2, ci, cj, ck) + g.gy(2, ci, cj + 1, ck)) / 4. - d0[3]) * 2.;
-            st[4] = ((gc * 2. + g.gx(2, ci, cj, ck) + g.gx(2, ci + 1, cj, ck)) / 4. - d0[4]) * 2.;
-            st[5] = (g.exy(ci, cj, ck) - d0[5]) * 2.;
-        }
-        const DevMat& m = io.mats[io.mid[cc] - 1];
-        if (which == 0) { for (int r = 0; r < 3; r++) sa[r] = stress_row(m, st, kFaceRows[D][r]); }
-        else { for (int r = 0; r < 3; r++) sb[r] = stress_row(m, st, kFaceRows[D][r]); }
+    __device__ double gp(int d, int a) const {
+        using namespace etile;
+        return d == 0 ? gxp[(a * HJ + r) * HK + s] : (d == 1 ? gy[(a * GYR + r + 1) * HK + s] : gz[(a * HJ + r) * GZC + s + 1]);
     }
-    for (int r = 0; r < 3; r++) out[r] = (sa[r] + sb[r]) / 2.;
+    __device__ double d0(int a) const { return d0s[(a * etile::HJ + r) * etile::HK + s]; }
+};
+
+// the same quantities read from global memory (face gradients recomputed as
+// k_face_grad does); used for the k == ny-1 neighbour of the z-face quirk
+struct GlobalCell {
+    const Params& P;
+    const StageIO& io;
+    long i, j, k;
+    double d0v[6];
+    __device__ GlobalCell(const Params& p, const StageIO& s, long i_, long j_, long k_) : P(p), io(s), i(i_), j(j_), k(k_) {
+        if (P.elasto_back) eigen_glb(P, io, cid(P, i, j, k), d0v); else for (int a = 0; a < 6; a++) d0v[a] = 0.;
+    }
+    __device__ double grad(int d, int a, long ci, long cj, long ck) const {
+        const double* u = io.u_in.c[a];
+        const long c = cid(P, ci, cj, ck);
+        if (d == 0) return free_x(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci == 0 ? P.nx - 1 : ci - 1, cj, ck)]) / P.dx;
+        if (d == 1) return free_y(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci, cj == 0 ? P.ny - 1 : cj - 1, ck)]) / P.dy;
+        return free_z(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci, cj, ck == 0 ? P.nz - 1 : ck - 1)]) / P.dz;
+    }
+    __device__ double gm(int d, int a) const { return grad(d, a, i, j, k); }
+    __device__ double gp(int d, int a) const {
+        if (d == 0) return grad(0, a, i == P.nx - 1 ? 0 : i + 1, j, k);
+        if (d == 1) return grad(1, a, i, j == P.ny - 1 ? 0 : j + 1, k);
+        return grad(2, a, i, j, k == P.nz - 1 ? 0 : k + 1);
+    }
+    __device__ double d0(int a) const { return d0v[a]; }
+};
+
+// One cell's contribution to the stress rows of a face normal to D; ga is
+// the face's gradient of the normal displacement component, gb and gc those
+// of the two tangential components (x-face: u_z, u_y; y-face: u_z, u_x;
+// z-face: u_y, u_x).
+template <int D, class V>
+__device__ inline void side_rows(const V& v, const DevMat& m, double ga, double gb, double gc, double out[3]) {
+    double st[6];
+    if (D == 0) {
+        st[0] = ga - v.d0(0);
+        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / 2. - v.d0(1);
+        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / 2. - v.d0(2);
+        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + v.gm(1, 2) + v.gp(1, 2)) / 4. - v.d0(3)) * 2.;
+        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + gb * 2.) / 4. - v.d0(4)) * 2.;
+        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + gc * 2.) / 4. - v.d0(5)) * 2.;
+    } else if (D == 1) {
+        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / 2. - v.d0(0);
+        st[1] = ga - v.d0(1);
+        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / 2. - v.d0(2);
+        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + gb * 2.) / 4. - v.d0(3)) * 2.;
+        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + v.gm(0, 2) + v.gp(0, 2)) / 4. - v.d0(4)) * 2.;
+        st[5] = ((gc * 2. + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
+    } else {
+        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / 2. - v.d0(0);
+        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / 2. - v.d0(1);
+        st[2] = ga - v.d0(2);
+        st[3] = ((gb * 2. + v.gm(1, 2) + v.gp(1, 2)) / 4. - v.d0(3)) * 2.;
+        st[4] = ((gc * 2. + v.gm(0, 2) + v.gp(0, 2)) / 4. - v.d0(4)) * 2.;
+        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
+    }
+    for (int r = 0; r < 3; r++) out[r] = stress_row(m, st, kFaceRows[D][r]);
 }
 
-// divergence term of direction D: (sigma(+face) - sigma(-face)) / h for the
-// three rows of kFaceRows[D], ordered as force x, y, z components
-template <int S, int D>
-__device__ inline void div_term(const Params& P, const StageIO& io, const GradView& g, long i, long j, long k,
-                                const double d0c[6], double t[3]) {
-    double s1[3], s2[3];
-    face_stress<S, D>(P, io, g, i, j, k, 0, d0c, s1);
-    face_stress<S, D>(P, io, g, i, j, k, 1, d0c, s2);
-    const double h = (D == 0) ? P.dx : (D == 1 ? P.dy : P.dz);
-    // kFaceRows[D][r] is the row feeding force component r
-    for (int r = 0; r < 3; r++) t[r] = (s2[r] - s1[r]) / h;
-}
-
+// RK4 combination for v and u of one cell (du = v_stage * dt)
 template <int S>
-__global__ void __launch_bounds__(256, 2) k_elastic(Params P, StageIO io) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    const long nyz = (long)P.ny * P.nz;
-    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
-    const GradView g(P, io);
-    const uint8_t id = io.mid[c];
-
-    double dv[3] = {0., 0., 0.};
-    if (id != 0) {
-        double d0c[6];
-        if (P.elasto_back) eigen_glb(P, io, c, d0c); else for (int a = 0; a < 6; a++) d0c[a] = 0.;
-        double tx[3], ty[3], tz[3];
-        div_term<S, 0>(P, io, g, i, j, k, d0c, tx);
-        div_term<S, 1>(P, io, g, i, j, k, d0c, ty);
-        div_term<S, 2>(P, io, g, i, j, k, d0c, tz);
-        const DevMat& mt = io.mats[id - 1];
-        for (int a = 0; a < 3; a++) {
-            const double f = tx[a] + ty[a] + tz[a];
-            const double fs = io.force_store.c[a][c];
-            if (S == 1 || S == 2)
-                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs) * 2.;
-            else
-                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs);
-            if (S == 0) io.force_store.c[a][c] = f;
-        }
-    }
-
-    // ---- RK4 combination for v and u (du = v_stage * dt) ----
+__device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], double dt) {
     for (int a = 0; a < 3; a++) {
-        const double du = io.v_in.c[a][c] * P.dt;
+        const double du = io.v_in.c[a][c] * dt;
         if (S == 0) {
             const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
             io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + dv[a] / 6.;
@@ -276,6 +259,196 @@ __global__ void __launch_bounds__(256, 2) k_elastic(Params P, StageIO io) {
             io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 6.;
             io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 6.;
         }
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO io, int chunk) {
+    using namespace etile;
+    GF_EXTERN_SMEM(double, smem);
+    double* sGX[2] = {smem, smem + kGX};
+    double* sGY = smem + 2 * kGX;
+    double* sGZ = sGY + kGY;
+    double* sD0 = sGZ + kGZ;
+    uint8_t* sMid = reinterpret_cast<uint8_t*>(sD0 + kD0);
+
+    const int tid = threadIdx.x;
+    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+    const int i0 = blockIdx.z * chunk;
+    const int i1 = min(i0 + chunk, P.nx) - 1;            // last plane of the chunk
+    const int L = i1 - i0 + 1;
+    const int jl = tid / TK, kl = tid - (tid / TK) * TK;
+    const int j = j0 + jl, k = k0 + kl;
+    const bool valid = (j < P.ny) && (k < P.nz);
+    const int r = jl + 1, s = kl + 1;
+    const bool back = P.elasto_back;
+    const bool want_strain = io.strain_c[0] != nullptr;
+    const bool quirk = valid && (k == P.ny - 1) && (P.ny < P.nz);
+    const bool traction_here = P.strain_pulse && P.strain_type == 3 && k == (int)P.source_z;
+
+    double sa[3] = {0., 0., 0.};       // lower cell's half of the next x-face stress
+    double sxp[3] = {0., 0., 0.};      // stress on the previous x-face
+    double ty[3] = {0., 0., 0.}, tz[3] = {0., 0., 0.};
+    uint8_t mid_prev = 0;
+
+    for (int q = 0; q <= L + 1; q++) {
+        const int p = i0 - 1 + q;                        // plane of this pass
+        const int pw = wrapm(p, P.nx);
+        double* gxc = sGX[(q + 1) & 1];                  // face p
+        double* gxn = sGX[q & 1];                        // face p+1
+        // ---- phase A: stage gradients and eigenstrains of plane p ----
+        if (q <= L) {
+            const int fw = wrapm(p + 1, P.nx);
+            for (int it = tid; it < HJ * HK; it += blockDim.x) {
+                const int rr = it / HK, ss = it - (it / HK) * HK;
+                const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
+                const bool fr = free_x(P, io.mid, fw, jj, kk);
+                const long c1 = cid(P, fw, jj, kk), c0 = cid(P, pw, jj, kk);
+                for (int a = 0; a < 3; a++)
+                    gxn[(a * HJ + rr) * HK + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dx;
+            }
+        }
+        for (int it = tid; it < GYR * HK; it += blockDim.x) {
+            const int rr = it / HK, ss = it - (it / HK) * HK;
+            const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
+            const bool fr = free_y(P, io.mid, pw, jj, kk);
+            const long c1 = cid(P, pw, jj, kk), c0 = cid(P, pw, jj == 0 ? P.ny - 1 : jj - 1, kk);
+            for (int a = 0; a < 3; a++)
+                sGY[(a * GYR + rr) * HK + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dy;
+        }
+        for (int it = tid; it < HJ * GZC; it += blockDim.x) {
+            const int rr = it / GZC, ss = it - (it / GZC) * GZC;
+            const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
+            const bool fr = free_z(P, io.mid, pw, jj, kk);
+            const long c1 = cid(P, pw, jj, kk), c0 = cid(P, pw, jj, kk == 0 ? P.nz - 1 : kk - 1);
+            for (int a = 0; a < 3; a++)
+                sGZ[(a * HJ + rr) * GZC + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dz;
+        }
+        for (int it = tid; it < HJ * HK; it += blockDim.x) {
+            const int rr = it / HK, ss = it - (it / HK) * HK;
+            const long c = cid(P, pw, wrapm(j0 - 1 + rr, P.ny), wrapm(k0 - 1 + ss, P.nz));
+            sMid[it] = io.mid[c];
+            double e[6];
+            if (back) eigen_glb(P, io, c, e); else for (int a = 0; a < 6; a++) e[a] = 0.;
+            for (int a = 0; a < 6; a++) sD0[(a * HJ + rr) * HK + ss] = e[a];
+        }
+        __syncthreads();
+
+        // ---- phase B: one column per thread ----
+        if (valid) {
+            const TileCell me{gxc, gxn, sGY, sGZ, sD0, r, s};
+            const uint8_t id = sMid[r * HK + s];
+            // x-face p: between planes p-1 and p
+            if (q >= 1) {
+                double sx[3] = {0., 0., 0.};
+                const bool fr = ((p == 0 || p == P.nx) && !P.per_x) || !(mid_prev != 0 && id != 0);
+                if (!fr) {
+                    const double ga = gxc[(0 * HJ + r) * HK + s], gb = gxc[(2 * HJ + r) * HK + s], gc = gxc[(1 * HJ + r) * HK + s];
+                    double sb[3];
+                    side_rows<0>(me, io.mats[id - 1], ga, gb, gc, sb);
+                    for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / 2.;
+                }
+                if (q >= 2) {
+                    // cell (p-1, j, k) is complete
+                    const long c = cid(P, p - 1, j, k);
+                    double dv[3] = {0., 0., 0.};
+                    if (mid_prev != 0) {
+                        const DevMat& mt = io.mats[mid_prev - 1];
+                        for (int a = 0; a < 3; a++) {
+                            const double tx = (sx[a] - sxp[a]) / P.dx;
+                            const double f = tx + ty[a] + tz[a];
+                            const double fs = io.force_store.c[a][c];
+                            if (S == 1 || S == 2)
+                                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs) * 2.;
+                            else
+                                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs);
+                            if (S == 0) io.force_store.c[a][c] = f;
+                        }
+                    }
+                    rk_vu<S>(io, c, dv, P.dt);
+                }
+                for (int a = 0; a < 3; a++) sxp[a] = sx[a];
+            }
+            // y- and z-faces of the interior plane p
+            if (q >= 1 && q <= L && id != 0) {
+                const DevMat& m = io.mats[id - 1];
+                double s1[3], s2[3];
+                // -y face j (neighbour row r-1), +y face j+1 (row r+1)
+                for (int side = 0; side < 2; side++) {
+                    const int f = j + side;
+                    const bool fr = ((f == 0 || f == P.ny) && !P.per_y) ||
+                                    !(sMid[(r - 1 + side) * HK + s] != 0 && sMid[(r + side) * HK + s] != 0);
+                    double* o = side ? s2 : s1;
+                    if (fr) { o[0] = o[1] = o[2] = 0.; continue; }
+                    const int rf = r + side;
+                    const double ga = sGY[(1 * GYR + rf) * HK + s], gb = sGY[(2 * GYR + rf) * HK + s], gc = sGY[(0 * GYR + rf) * HK + s];
+                    const TileCell nb{gxc, gxn, sGY, sGZ, sD0, side ? r + 1 : r - 1, s};
+                    double a1[3], a2[3];
+                    side_rows<1>(me, m, ga, gb, gc, a1);
+                    side_rows<1>(nb, io.mats[sMid[nb.r * HK + s] - 1], ga, gb, gc, a2);
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                }
+                for (int a = 0; a < 3; a++) ty[a] = (s2[a] - s1[a]) / P.dy;
+                // -z face k (neighbour column s-1), +z face k+1 (column s+1)
+                for (int side = 0; side < 2; side++) {
+                    const int f = k + side;
+                    const bool fr = ((f == 0 || f == P.nz) && !P.per_z) ||
+                                    !(sMid[r * HK + s - 1 + side] != 0 && sMid[r * HK + s + side] != 0);
+                    double* o = side ? s2 : s1;
+                    if (fr) {
+                        o[0] = o[1] = o[2] = 0.;
+                        if (side == 1 && traction_here) {
+                            // surface traction: x -> xz, y -> yz, z -> zz
+                            const double tr = stage_drive(io, S).traction;
+                            if (P.strain_comp == 0) o[0] = tr; else if (P.strain_comp == 1) o[1] = tr; else o[2] = tr;
+                        }
+                        continue;
+                    }
+                    const int sf = s + side;
+                    const double ga = sGZ[(2 * HJ + r) * GZC + sf], gb = sGZ[(1 * HJ + r) * GZC + sf], gc = sGZ[(0 * HJ + r) * GZC + sf];
+                    double a1[3], a2[3];
+                    side_rows<2>(me, m, ga, gb, gc, a1);
+                    if (side == 1 && quirk) {
+                        // the reference's +z neighbour of k == ny-1 is k = 0
+                        // (elastic_dynamic_solver.cpp:1247); creation rejects
+                        // decks where that cell is vacuum
+                        const GlobalCell nb(P, io, pw, j, 0);
+                        side_rows<2>(nb, io.mats[io.mid[cid(P, pw, j, 0)] - 1], ga, gb, gc, a2);
+                    } else {
+                        const TileCell nb{gxc, gxn, sGY, sGZ, sD0, r, side ? s + 1 : s - 1};
+                        side_rows<2>(nb, io.mats[sMid[r * HK + nb.s] - 1], ga, gb, gc, a2);
+                    }
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                }
+                for (int a = 0; a < 3; a++) tz[a] = (s2[a] - s1[a]) / P.dz;
+                // cell strain for the magnetic and ferroelectric kernels
+                if (want_strain && (m.flags & (MF_FM | MF_FE))) {
+                    double e[6];
+                    e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
+                    e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;
+                    e[2] = (me.gm(2, 2) + me.gp(2, 2)) / 2.;
+                    e[3] = (me.gm(2, 1) + me.gp(2, 1) + me.gm(1, 2) + me.gp(1, 2)) / 4.;
+                    e[4] = (me.gm(2, 0) + me.gp(2, 0) + me.gm(0, 2) + me.gp(0, 2)) / 4.;
+                    e[5] = (me.gm(1, 0) + me.gp(1, 0) + me.gm(0, 1) + me.gp(0, 1)) / 4.;
+                    if (P.rot) {
+                        double t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
+                        rot_tensor(P.Tg2c, t3, o3);
+                        e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
+                    }
+                    const long c = cid(P, p, j, k);
+                    for (int a = 0; a < 6; a++) io.strain_c[a][c] = e[a];
+                }
+            } else if (q >= 1 && q <= L) {
+                for (int a = 0; a < 3; a++) ty[a] = tz[a] = 0.;
+            }
+            // lower cell's half of x-face p+1
+            if (q <= L && id != 0) {
+                const double ga = gxn[(0 * HJ + r) * HK + s], gb = gxn[(2 * HJ + r) * HK + s], gc = gxn[(1 * HJ + r) * HK + s];
+                side_rows<0>(me, io.mats[id - 1], ga, gb, gc, sa);
+            }
+            mid_prev = id;
+        }
+        __syncthreads();
     }
 }
 

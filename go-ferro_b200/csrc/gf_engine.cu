@@ -77,6 +77,8 @@ struct gf_engine {
     double* Estat[3] = {nullptr, nullptr, nullptr};
     double* Hnu[3] = {nullptr, nullptr, nullptr};
     double* fg[9] = {};
+    double* strain_c[6] = {};
+    int el_chunk = 1;                  // x-planes per block of k_elastic_tile
     double* liao_hist = nullptr; double* liao_last = nullptr;
     double* scratch = nullptr;             // 6n doubles: output staging and reductions
     int* flag = nullptr;
@@ -141,12 +143,14 @@ cudaEvent_t next_event(gf_engine* eng) {
 
 // every kernel of the engine is launched through klaunch: it counts the
 // launch and, in profiling mode, brackets it with events on the stream
-template <class Kernel, class... Args>
+template <bool Tiled = false, class Kernel, class... Args>
 cudaError_t klaunch(gf_engine* eng, const char* name, Kernel k, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                     Args... args) {
     cudaEvent_t a = nullptr, b = nullptr;
     if (eng->profiling) { a = next_event(eng); cudaEventRecord(a, s); }
-    cudaError_t e = launch(k, grid, block, smem, s, args...);
+    cudaError_t e;
+    if constexpr (Tiled) e = launch_tiled(k, grid, block, smem, s, args...);
+    else e = launch(k, grid, block, smem, s, args...);
     if (eng->profiling) { b = next_event(eng); cudaEventRecord(b, s); eng->prof.push_back({name, a, b}); }
     eng->launch_counter++;
     return e;
@@ -232,18 +236,18 @@ DevMat make_devmat(const Material& m, double dt) {
 }
 
 // ---------------------------------------------------------------------------
-// validation: what this build implements
+// validation: what this engine implements
 // ---------------------------------------------------------------------------
 std::string unsupported(const Deck& d) {
-    if (d.any_afm) return "two-sublattice antiferromagnets (if_AFM) are not supported by this build";
-    if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this build";
-    if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this build";
-    if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this build";
-    if (d.any_pec && d.em_dynamic) return "PEC materials are not supported by this build";
+    if (d.any_afm) return "two-sublattice antiferromagnets (if_AFM) are not supported by this engine";
+    if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
+    if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this engine";
+    if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
+    if (d.any_pec && d.em_dynamic) return "PEC materials are not supported by this engine";
     if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
-    if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this build";
+    if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this engine";
     if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
-    if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this build";
+    if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this engine";
     for (size_t i = 0; i < d.mats.size(); i++) {
         const Material& m = d.mats[i];
         if (m.fm && m.aniso_type > 2) return "anisotropy_type must be 0, 1 or 2";
@@ -251,7 +255,7 @@ std::string unsupported(const Deck& d) {
         if (m.fe && m.fe_mass == 0.) return "ferroelectric material needs nonzero FE_mass";
         if (d.em_dynamic) {
             for (int k = 0; k < 3; k++)
-                if (m.wp[k] != 0.) return "Drude dispersion (omega_plasma != 0) is not supported by this build";
+                if (m.wp[k] != 0.) return "Drude dispersion (omega_plasma != 0) is not supported by this engine";
             if (!(m.comp[0] == m.comp[0])) return "Drude weights sum to zero: the reference's normalisation yields NaN fields for this deck";
         }
     }
@@ -512,6 +516,7 @@ void build_io(gf_engine* eng) {
             io.Estat = f3(eng->Estat);
             io.Hnu = f3(eng->Hnu);
             for (int a = 0; a < 9; a++) io.fg[a] = eng->fg[a];
+            for (int a = 0; a < 6; a++) io.strain_c[a] = eng->strain_c[a];
             for (int a = 0; a < 6; a++) { io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr; }
             io.liao_hist = eng->liao_hist;
             io.liao_last = eng->liao_last;
@@ -527,6 +532,27 @@ void build_io(gf_engine* eng) {
 // ---------------------------------------------------------------------------
 // one RK4 step: kernel sequence in the reference's data order
 // ---------------------------------------------------------------------------
+// Shared-memory opt-in and the x-chunk of the tiled elastic kernel: enough
+// chunks that every SM holds as many blocks as fit, for about two waves.
+int setup_elastic_tile(gf_engine* eng) {
+    const Params& P = eng->P;
+    const int smem = (int)etile::kSmemBytes;
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 1, sms = 1;
+    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1>, etile::NT, etile::kSmemBytes));
+    GF_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, eng->device));
+    const long tiles = (long)((P.nz + etile::TK - 1) / etile::TK) * ((P.ny + etile::TJ - 1) / etile::TJ);
+    const long want = 2L * (per_sm > 0 ? per_sm : 1) * sms;
+    long chunks = (want + tiles - 1) / tiles;
+    if (chunks < 1) chunks = 1;
+    if (chunks > P.nx) chunks = P.nx;
+    eng->el_chunk = (int)((P.nx + chunks - 1) / chunks);
+    return GF_OK;
+}
+
 template <int S>
 int enqueue_stage(gf_engine* eng, int parity) {
     const Params& P = eng->P;
@@ -534,8 +560,10 @@ int enqueue_stage(gf_engine* eng, int parity) {
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     if (P.elastic) {
-        GF_CU(klaunch(eng, "k_face_grad", k_face_grad, dim3(bn), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_elastic", k_elastic<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
+                        (P.nx + eng->el_chunk - 1) / eng->el_chunk);
+        GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S>, grid, dim3(etile::NT), etile::kSmemBytes, st, P, io,
+                            eng->el_chunk));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
@@ -820,6 +848,9 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     }
     if (d.elastodynamics)
         for (int a = 0; a < 9; a++) GF_TRY(dalloc_n(eng, &eng->fg[a], (size_t)n));
+    if (d.elastodynamics && P.elasto_on && (P.fm || P.fe))
+        for (int a = 0; a < 6; a++) GF_TRY(dalloc_n(eng, &eng->strain_c[a], (size_t)n));
+    if (d.elastodynamics) GF_TRY(setup_elastic_tile(eng));
     if (d.elastodynamics) {
         const size_t plane = (size_t)P.nx * P.ny;
         GF_TRY(dalloc_n(eng, &eng->liao_hist, 4 * 12 * plane));

@@ -64,9 +64,9 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
             // dynamic strain and eigenstrain of the stage state, crystal frame
             // (Dexx_crt, Dexx0_crt: ferroelectric_solver.cpp:624-652)
             if (P.elastic) {
-                double e[6];
-                strain_crt(P, GradView(P, io), i, j, k, e);
-                exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
+                // written by k_elastic_tile earlier in the same stage
+                exx = io.strain_c[0][c]; eyy = io.strain_c[1][c]; ezz = io.strain_c[2][c];
+                eyz = io.strain_c[3][c]; exz = io.strain_c[4][c]; exy = io.strain_c[5][c];
             }
             if (P.elasto_back) {
                 double e0[6];

@@ -17,4 +17,14 @@ inline cudaError_t launch(Kernel k, dim3 grid, dim3 block, size_t smem, cudaStre
     return cudaGetLastError();
 }
 
+// Dynamic shared memory of a block-cooperative kernel.
+#define GF_EXTERN_SMEM(T, name) extern __shared__ T name[]
+
+// Launch of a block-cooperative kernel (one that synchronises its threads
+// with __syncthreads and carries per-thread state across the barriers).
+template <class Kernel, class... Args>
+inline cudaError_t launch_tiled(Kernel k, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    return launch(k, grid, block, smem, s, args...);
+}
+
 }  // namespace gf

@@ -29,10 +29,11 @@ __device__ inline bool is_fm(const DevMat* mats, uint8_t id) {
 }
 
 // static strain plus the cell strain of the stage displacement, crystal
-// frame (exxt0_crt + Dexx_crt, magnetic_solver.cpp:89-96)
+// frame (exxt0_crt + Dexx_crt, magnetic_solver.cpp:89-96); the dynamic part
+// is written by k_elastic_tile earlier in the same stage
 __device__ inline void cell_strain_total(const Params& P, const StageIO& io, long i, long j, long k, long c, double e[6]) {
     double d[6] = {0., 0., 0., 0., 0., 0.};
-    if (P.elastic) strain_crt(P, GradView(P, io), i, j, k, d);
+    if (P.elastic) for (int a = 0; a < 6; a++) d[a] = io.strain_c[a][c];
     for (int a = 0; a < 6; a++) {
         double t = io.eps0_c[a] ? io.eps0_c[a][c] : 0.;
         e[a] = t + d[a];

@@ -30,9 +30,14 @@ struct StageIO {
     F3 E_in, E_x, E_acc, E_out, H_in, H_x, H_acc, H_out;
     // static and external fields
     F3 Hstat, Estat, Hnu;
-    // face-normal displacement gradients of the stage state, written by
-    // k_face_grad: fg[3*d + a] = d u_a / d x_d on the cell's -d face
+    // face-normal displacement gradients of the current state, written by
+    // k_face_grad for the strain output: fg[3*d + a] = d u_a / d x_d on the
+    // cell's -d face
     double* fg[9];
+    // crystal-frame cell strain of the stage displacement (Dexx_crt ...),
+    // written by k_elastic_tile for ferromagnetic and ferroelectric cells and
+    // read by the LLG and TDGL kernels of the same stage; null when unused
+    double* strain_c[6];
     // optional static inputs (null when absent): static strain and static
     // eigenstrain in the crystal frame
     const double* eps0_c[6];

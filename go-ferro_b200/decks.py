@@ -365,7 +365,7 @@ def write_deck(deck: Deck, directory: str) -> str:
 # material sets used by the presets
 # --------------------------------------------------------------------------
 def yig(alpha: float = 0.01, magnetoelastic: bool = False) -> Material:
-    """YIG-like ferrimagnet treated as a ferromagnet (2)."""
+    """YIG-like ferrimagnet treated as a ferromagnet (FM and magnetoelastic presets)."""
     c11, c12, c44 = 2.69e11, 1.077e11, 0.764e11
     lam100 = lam111 = 0.0
     if magnetoelastic:
@@ -379,14 +379,14 @@ def yig(alpha: float = 0.01, magnetoelastic: bool = False) -> Material:
 
 def ggg() -> Material:
     """GGG-like non-magnetic garnet substrate (constants chosen for the
-    coupled magnetoelastic preset; not given by the benchmark)."""
+    coupled magnetoelastic preset)."""
     return Material(title="GGG", c11=2.86e11, c12=1.16e11, c44=0.905e11, density=7080.0, er=12.0)
 
 
 def pto() -> Material:
-    """PbTiO3-like ferroelectric at 300 K.  FE mass,
+    """PbTiO3-like ferroelectric at 300 K (ferroelectric preset).  FE mass,
     damping, gradient coefficient and background permittivity are chosen
-    here (not given by the benchmark)."""
+    here."""
     return Material(title="PTO", c11=2.3e11, c12=1.0e11, c44=1.2e11, density=7.9e3,
                     fe=True, fe_mass=1.7e-18, fe_damping=1.7e-6,
                     a1=3.8e5 * (300.0 - 479.0), a11=-7.3e7, a12=7.5e8,
@@ -417,10 +417,10 @@ def gaussian_derivative_pulse(steps: int, dt: float, peak_T: float, sigma: float
 
 
 # --------------------------------------------------------------------------
-# presets (BASELINE configurations, optionally scaled down for tests)
+# presets (the three benchmark workloads, optionally scaled down for tests)
 # --------------------------------------------------------------------------
 def preset_fm_demag(nx=64, ny=64, nz=16, steps=4000, dt=5e-15) -> Deck:
-    """Config 1: FM LLG + FFT magnetostatics, YIG-like, 0.1 T bias along z,
+    """FM LLG + FFT magnetostatics, YIG-like, 0.1 T bias along z,
     1 mT Gaussian-derivative x pulse of 1 ps width, seeded <=1 deg tilt."""
     d = Deck(nx=nx, ny=ny, nz=nz, dx=2e-9, dy=2e-9, dz=2e-9, periodic=(True, True, False),
              layers=[(nz, 1)], steps=steps, dt=dt, materials=[yig(0.01)],
@@ -431,7 +431,7 @@ def preset_fm_demag(nx=64, ny=64, nz=16, steps=4000, dt=5e-15) -> Deck:
 
 
 def preset_magnetoelastic(nx=128, ny=128, nz=96, sub=56, film=32, steps=10000, dt=None) -> Deck:
-    """Config 2: magnetoelastic YIG film on a GGG-like substrate with
+    """Magnetoelastic YIG film on a GGG-like substrate with
     elastodynamics and Maxwell FDTD; bottom-plane 0.3 THz shear source of
     1 pm amplitude; vacuum above the film; Courant-limited dt."""
     dx = 2e-9
@@ -456,7 +456,7 @@ def preset_magnetoelastic(nx=128, ny=128, nz=96, sub=56, film=32, steps=10000, d
 
 
 def preset_ferroelectric(nx=128, ny=128, nz=128, steps=40000, dt=None, pulse=True) -> Deck:
-    """Config 3: PbTiO3-like TDGL + electrostriction + elastodynamics + FDTD,
+    """PbTiO3-like TDGL + electrostriction + elastodynamics + FDTD,
     seeded uniform random P within +-1e-3 C/m^2, z-polarised Gaussian sheet
     current (J_f type 4, width 1 ps) radiating ~100 kV/cm."""
     dx = 1e-9

@@ -41,7 +41,7 @@ typedef struct gf_engine gf_engine;
 #define GF_ENOMEM (-4)       /* device allocation failed                   */
 #define GF_ENAN (-5)         /* non-finite value found by a health check   */
 #define GF_ENODEV (-6)       /* no usable sm_100 device                    */
-#define GF_EUNSUPPORTED (-7) /* deck asks for physics this build lacks     */
+#define GF_EUNSUPPORTED (-7) /* deck asks for physics the engine lacks    */
 
 /* fields for gf_upload / gf_download / gf_field_dims (component-major:
  * a vector field is 3 consecutive arrays x, y, z of the field's dims) */
