@@ -119,34 +119,17 @@ __device__ inline void eigen_glb(const Params& P, const StageIO& io, long c, dou
     }
 }
 
-// Rows of the Voigt stress that the divergence uses from a face normal to
-// direction d: x-face -> xx, xy, xz; y-face -> xy, yy, yz; z-face -> xz, yz, zz
-__constant__ const int kFaceRows[3][3] = {{0, 5, 4}, {5, 1, 3}, {4, 3, 2}};
-
-// rows r[0..2] of C * e with the accumulation order of strain2stress_glb
-// (mathlib.cpp:127-135); zero entries of the cubic pattern are skipped,
-// which leaves every partial sum unchanged
-__device__ inline double stress_row(const DevMat& m, const double e[6], int r) {
-    if (m.cubic_c) {
-        if (r < 3) return m.cij[r][0] * e[0] + m.cij[r][1] * e[1] + m.cij[r][2] * e[2];
-        return m.cij[r][r] * e[r];
-    }
-    double acc = 0.;
-    for (int q = 0; q < 6; q++) acc = acc + m.cij[r][q] * e[q];
-    return acc;
-}
-
 // ---------------------------------------------------------------------------
 // Tiled stage kernel.  A block owns a TJ x TK tile of (j,k) columns and
-// marches along x over `chunk` planes.  For every plane it stages in shared
-// memory the face-normal displacement gradients of the tile and a one-cell
-// halo (GX on the x-faces, two planes; GY, GZ on the y- and z-faces) and the
-// global-frame eigenstrains, so that each gradient and eigenstrain is
-// computed once.  Each thread then forms its cell's y- and z-face stresses
-// from shared memory, and the x-face stresses are computed once per face:
-// the cell below a face contributes its half while the previous plane is
-// processed and the sum is completed one plane later.
-//
+// marches along x over `chunk` planes.  Per plane p it
+//   A. computes from a two-plane ring of staged u and material ids the
+//      face-normal gradients of the tile's cells and a one-cell halo (x-faces
+//      on two planes, y- and z-faces) and the cells' eigenstrains,
+//   B1. computes every y- and z-face stress of the tile once (one thread per
+//      face) while the next plane's u and ids are staged,
+//   B2. per column: the x-face stress (the cell below a face contributes its
+//      half one plane earlier), the divergence of the previous plane's cell,
+//      its RK4 update, and the strain output of this plane's cell.
 // A face stress (get_dv_RK*, elastic_dynamic_solver.cpp:876-1289) is the
 // mean over the two cells sharing the face of three rows of C (strain -
 // eigenstrain), where each cell's strain takes the face's own gradient for
@@ -154,15 +137,77 @@ __device__ inline double stress_row(const DevMat& m, const double e[6], int r) {
 // 0 on stress-free faces, except for the surface traction source.  Every
 // expression keeps the reference's operation order (rounding included).
 // ---------------------------------------------------------------------------
+
+// elastic constants of one material, staged in shared memory
+struct ElMat {
+    double cij[6][6];
+    double dens_dt, mass_damp, stiff_damp;
+    double l100_15, l111_15, Q11, Q12, Q44;
+    uint32_t flags;
+    int cubic_c;
+};
+
 namespace etile {
 constexpr int TJ = 8, TK = 32, NT = TJ * TK;
-constexpr int HJ = TJ + 2, HK = TK + 2;      // cells of the tile and halo
-constexpr int GYR = TJ + 3, GZC = TK + 3;    // face rows (y) / columns (z)
-constexpr int kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
-constexpr size_t kSmemBytes = (size_t)(2 * kGX + kGY + kGZ + kD0) * sizeof(double) + (size_t)HJ * HK;
+constexpr int UR = TJ + 4, UC = TK + 4;      // staged u and ids: rows j0-2..j0+TJ+1, columns k0-2..k0+TK+1
+constexpr int HJ = TJ + 2, HK = TK + 2;      // cells with gradients: rows j0-1..j0+TJ, columns k0-1..k0+TK
+constexpr int GYR = TJ + 3, GZC = TK + 3;    // -y face gradients of rows j0-1..j0+TJ+1; -z of columns k0-1..k0+TK+1
+constexpr int FYR = TJ + 1, FZC = TK + 1;    // face stresses: y-faces j0..j0+TJ, z-faces k0..k0+TK
+constexpr int kU = 3 * UR * UC, kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
+constexpr int kFY = 3 * FYR * TK, kFZ = 3 * TJ * FZC;
+constexpr int kDoubles = 2 * kU + 2 * kGX + kGY + kGZ + kD0 + kFY + kFZ;
+constexpr size_t kFixedBytes = (size_t)kDoubles * sizeof(double) + (size_t)(2 * UR + UC) * sizeof(int)
+                               + (size_t)(2 * UR * UC + HJ * HK);
+inline size_t smem_bytes(int nmat) { return (size_t)nmat * sizeof(ElMat) + kFixedBytes; }
+constexpr size_t kMaxSmemBytes = (size_t)kMaxMat * sizeof(ElMat) + kFixedBytes;
 }  // namespace etile
 
-__device__ inline int wrapm(int x, int n) { return x < 0 ? x + n : (x >= n ? x % n : x); }
+// index x in [-n, 2n) wrapped into [0, n)
+__device__ inline int wrapm(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
+
+// Rows of the Voigt stress that the divergence uses from a face normal to
+// direction d: x-face -> xx, xy, xz; y-face -> xy, yy, yz; z-face -> xz, yz, zz
+__host__ __device__ constexpr int face_row(int d, int r) {
+    return d == 0 ? (r == 0 ? 0 : (r == 1 ? 5 : 4)) : (d == 1 ? (r == 0 ? 5 : (r == 1 ? 1 : 3)) : (r == 0 ? 4 : (r == 1 ? 3 : 2)));
+}
+
+// row r of C * e with the accumulation order of strain2stress_glb
+// (mathlib.cpp:127-135); zero entries of the cubic pattern are skipped,
+// which leaves every partial sum unchanged
+template <class M>
+__device__ inline double stress_row(const M& m, const double e[6], int r) {
+    if (m.cubic_c) {
+        if (r < 3) return m.cij[r][0] * e[0] + m.cij[r][1] * e[1] + m.cij[r][2] * e[2];
+        return m.cij[r][r] * e[r];
+    }
+    double acc = 0.;
+#pragma unroll
+    for (int q = 0; q < 6; q++) acc = acc + m.cij[r][q] * e[q];
+    return acc;
+}
+
+// global-frame dynamic eigenstrain of cell c with material constants mt
+// (get_eigenstrain_dynamic; eigen_glb with the constants taken from mt)
+template <class M>
+__device__ inline void eigen_glb_m(const Params& P, const StageIO& io, long c, const M& mt, double e[6]) {
+    double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
+    if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
+    if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
+    const double third = 1. / 3.;
+    double e0[6] = {0., 0., 0., 0., 0., 0.};
+    if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
+    e[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz)) - e0[0];
+    e[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz)) - e0[1];
+    e[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px)) - e0[2];
+    e[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz - e0[3];
+    e[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz - e0[4];
+    e[5] = mt.l111_15 * my * mx + mt.Q44 * py * px - e0[5];
+    if (P.rot) {
+        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
+        rot_tensor(P.Tc2g, s, o);
+        e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
+    }
+}
 
 // gradients of a cell held in the shared tile: gm(d,a) on the -d face,
 // gp(d,a) on the +d face, d0(a) the global-frame eigenstrain
@@ -210,8 +255,8 @@ struct GlobalCell {
 // the face's gradient of the normal displacement component, gb and gc those
 // of the two tangential components (x-face: u_z, u_y; y-face: u_z, u_x;
 // z-face: u_y, u_x).
-template <int D, class V>
-__device__ inline void side_rows(const V& v, const DevMat& m, double ga, double gb, double gc, double out[3]) {
+template <int D, class V, class M>
+__device__ inline void side_rows(const V& v, const M& m, double ga, double gb, double gc, double out[3]) {
     double st[6];
     if (D == 0) {
         st[0] = ga - v.d0(0);
@@ -235,12 +280,14 @@ __device__ inline void side_rows(const V& v, const DevMat& m, double ga, double 
         st[4] = ((gc * 2. + v.gm(0, 2) + v.gp(0, 2)) / 4. - v.d0(4)) * 2.;
         st[5] = ((v.gm(1, 0) + v.gp(1, 0) + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
     }
-    for (int r = 0; r < 3; r++) out[r] = stress_row(m, st, kFaceRows[D][r]);
+#pragma unroll
+    for (int r = 0; r < 3; r++) out[r] = stress_row(m, st, face_row(D, r));
 }
 
 // RK4 combination for v and u of one cell (du = v_stage * dt)
 template <int S>
 __device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], double dt) {
+#pragma unroll
     for (int a = 0; a < 3; a++) {
         const double du = io.v_in.c[a][c] * dt;
         if (S == 0) {
@@ -262,15 +309,50 @@ __device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], doub
     }
 }
 
-template <int S>
-__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO io, int chunk) {
+// Shared-memory plan of k_elastic_tile (byte offsets from the dynamic base)
+struct ETileSmem {
+    ElMat* mat;
+    double *u[2], *gx[2], *gy, *gz, *d0, *fy, *fz;
+    int *rowoff, *rowj, *colk;
+    uint8_t *id[2], *idc;
+    __device__ ETileSmem(unsigned char* base, int nmat) {
+        using namespace etile;
+        mat = reinterpret_cast<ElMat*>(base);
+        double* d = reinterpret_cast<double*>(base + (size_t)nmat * sizeof(ElMat));
+        u[0] = d; u[1] = d + kU; d += 2 * kU;
+        gx[0] = d; gx[1] = d + kGX; d += 2 * kGX;
+        gy = d; d += kGY;
+        gz = d; d += kGZ;
+        d0 = d; d += kD0;
+        fy = d; d += kFY;
+        fz = d; d += kFZ;
+        int* ip = reinterpret_cast<int*>(d);
+        rowoff = ip; rowj = ip + UR; colk = ip + 2 * UR;
+        uint8_t* bp = reinterpret_cast<uint8_t*>(ip + 2 * UR + UC);
+        id[0] = bp; id[1] = bp + UR * UC; idc = bp + 2 * UR * UC;
+    }
+};
+
+// stage u and material ids of plane pw into ring slot `slot`
+__device__ inline void etile_stage(const Params& P, const StageIO& io, const ETileSmem& sm, int slot, int pw) {
     using namespace etile;
-    GF_EXTERN_SMEM(double, smem);
-    double* sGX[2] = {smem, smem + kGX};
-    double* sGY = smem + 2 * kGX;
-    double* sGZ = sGY + kGY;
-    double* sD0 = sGZ + kGZ;
-    uint8_t* sMid = reinterpret_cast<uint8_t*>(sD0 + kD0);
+    const int po = pw * P.ny * P.nz;
+    double* su = sm.u[slot];
+    uint8_t* sid = sm.id[slot];
+    for (int it = threadIdx.x; it < UR * UC; it += blockDim.x) {
+        const int ur = it / UC, uc = it - (it / UC) * UC;
+        const int c = po + sm.rowoff[ur] + sm.colk[uc];
+        sid[it] = io.mid[c];
+#pragma unroll
+        for (int a = 0; a < 3; a++) su[a * UR * UC + it] = io.u_in.c[a][c];
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO io, int chunk, int nmat) {
+    using namespace etile;
+    GF_EXTERN_SMEM(unsigned char, smem_raw);
+    const ETileSmem sm(smem_raw, nmat);
 
     const int tid = threadIdx.x;
     const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
@@ -280,11 +362,35 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
     const int jl = tid / TK, kl = tid - (tid / TK) * TK;
     const int j = j0 + jl, k = k0 + kl;
     const bool valid = (j < P.ny) && (k < P.nz);
-    const int r = jl + 1, s = kl + 1;
+    const int r = jl + 1, s = kl + 1;                    // own cell in halo coordinates
     const bool back = P.elasto_back;
     const bool want_strain = io.strain_c[0] != nullptr;
     const bool quirk = valid && (k == P.ny - 1) && (P.ny < P.nz);
     const bool traction_here = P.strain_pulse && P.strain_type == 3 && k == (int)P.source_z;
+    const int nyz = P.ny * P.nz;
+
+    // ---- block set-up: material table, wrapped row/column offsets, first two planes ----
+    for (int it = tid; it < nmat; it += blockDim.x) {
+        const DevMat& d = io.mats[it];
+        ElMat& e = sm.mat[it];
+        for (int a = 0; a < 6; a++) for (int b = 0; b < 6; b++) e.cij[a][b] = d.cij[a][b];
+        e.dens_dt = d.dens_dt; e.mass_damp = d.mass_damp; e.stiff_damp = d.stiff_damp;
+        e.l100_15 = d.l100_15; e.l111_15 = d.l111_15; e.Q11 = d.Q11; e.Q12 = d.Q12; e.Q44 = d.Q44;
+        e.flags = d.flags; e.cubic_c = d.cubic_c;
+    }
+    for (int it = tid; it < UR; it += blockDim.x) {
+        int jj = j0 - 2 + it;
+        jj = jj < 0 ? jj + P.ny : jj % P.ny;
+        sm.rowj[it] = jj; sm.rowoff[it] = jj * P.nz;
+    }
+    for (int it = tid; it < UC; it += blockDim.x) {
+        int kk = k0 - 2 + it;
+        sm.colk[it] = kk < 0 ? kk + P.nz : kk % P.nz;
+    }
+    __syncthreads();
+    etile_stage(P, io, sm, 0, wrapm(i0 - 1, P.nx));
+    etile_stage(P, io, sm, 1, wrapm(i0, P.nx));
+    __syncthreads();
 
     double sa[3] = {0., 0., 0.};       // lower cell's half of the next x-face stress
     double sxp[3] = {0., 0., 0.};      // stress on the previous x-face
@@ -294,66 +400,122 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
     for (int q = 0; q <= L + 1; q++) {
         const int p = i0 - 1 + q;                        // plane of this pass
         const int pw = wrapm(p, P.nx);
-        double* gxc = sGX[(q + 1) & 1];                  // face p
-        double* gxn = sGX[q & 1];                        // face p+1
-        // ---- phase A: stage gradients and eigenstrains of plane p ----
+        const int po = pw * nyz;
+        const int cur = q & 1, nxt = cur ^ 1;           // ring slots of planes p and p+1
+        const double* uc = sm.u[cur];
+        const double* un = sm.u[nxt];
+        const uint8_t* ic = sm.id[cur];
+        const uint8_t* in = sm.id[nxt];
+        double* gxc = sm.gx[cur ^ 1];                    // face p   (computed in the previous pass)
+        double* gxn = sm.gx[cur];                        // face p+1
+        // ---- A: gradients and eigenstrains of plane p ----
         if (q <= L) {
-            const int fw = wrapm(p + 1, P.nx);
+            const int f = p + 1;
+            const bool fb = (f == 0 || f == P.nx) && !P.per_x;
             for (int it = tid; it < HJ * HK; it += blockDim.x) {
                 const int rr = it / HK, ss = it - (it / HK) * HK;
-                const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
-                const bool fr = free_x(P, io.mid, fw, jj, kk);
-                const long c1 = cid(P, fw, jj, kk), c0 = cid(P, pw, jj, kk);
+                const int ui = (rr + 1) * UC + ss + 1;
+                const bool fr = fb || !(ic[ui] != 0 && in[ui] != 0);
+#pragma unroll
                 for (int a = 0; a < 3; a++)
-                    gxn[(a * HJ + rr) * HK + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dx;
+                    gxn[a * HJ * HK + it] = fr ? 0. : (un[a * UR * UC + ui] - uc[a * UR * UC + ui]) / P.dx;
             }
         }
         for (int it = tid; it < GYR * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
-            const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
-            const bool fr = free_y(P, io.mid, pw, jj, kk);
-            const long c1 = cid(P, pw, jj, kk), c0 = cid(P, pw, jj == 0 ? P.ny - 1 : jj - 1, kk);
+            const int u1 = (rr + 1) * UC + ss + 1, u0 = rr * UC + ss + 1;
+            const bool fr = (sm.rowj[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
+#pragma unroll
             for (int a = 0; a < 3; a++)
-                sGY[(a * GYR + rr) * HK + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dy;
+                sm.gy[a * GYR * HK + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dy;
         }
         for (int it = tid; it < HJ * GZC; it += blockDim.x) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
-            const int jj = wrapm(j0 - 1 + rr, P.ny), kk = wrapm(k0 - 1 + ss, P.nz);
-            const bool fr = free_z(P, io.mid, pw, jj, kk);
-            const long c1 = cid(P, pw, jj, kk), c0 = cid(P, pw, jj, kk == 0 ? P.nz - 1 : kk - 1);
+            const int u1 = (rr + 1) * UC + ss + 1, u0 = u1 - 1;
+            const bool fr = (sm.colk[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
+#pragma unroll
             for (int a = 0; a < 3; a++)
-                sGZ[(a * HJ + rr) * GZC + ss] = fr ? 0. : (io.u_in.c[a][c1] - io.u_in.c[a][c0]) / P.dz;
+                sm.gz[a * HJ * GZC + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dz;
         }
         for (int it = tid; it < HJ * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
-            const long c = cid(P, pw, wrapm(j0 - 1 + rr, P.ny), wrapm(k0 - 1 + ss, P.nz));
-            sMid[it] = io.mid[c];
-            double e[6];
-            if (back) eigen_glb(P, io, c, e); else for (int a = 0; a < 6; a++) e[a] = 0.;
-            for (int a = 0; a < 6; a++) sD0[(a * HJ + rr) * HK + ss] = e[a];
+            const uint8_t id = ic[(rr + 1) * UC + ss + 1];
+            sm.idc[it] = id;
+            double e[6] = {0., 0., 0., 0., 0., 0.};
+            if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff[rr + 1] + sm.colk[ss + 1], sm.mat[id - 1], e);
+#pragma unroll
+            for (int a = 0; a < 6; a++) sm.d0[a * HJ * HK + it] = e[a];
         }
         __syncthreads();
 
-        // ---- phase B: one column per thread ----
+        // ---- B1: y- and z-face stresses of the interior plane p; stage plane p+2 ----
+        if (q >= 1 && q <= L) {
+            for (int it = tid; it < FYR * TK; it += blockDim.x) {
+                const int fr_ = it / TK, fc = it - (it / TK) * TK;       // face j0+fr_, column k0+fc
+                const int f = j0 + fr_;
+                const uint8_t ia = sm.idc[fr_ * HK + fc + 1], ib = sm.idc[(fr_ + 1) * HK + fc + 1];
+                double o[3] = {0., 0., 0.};
+                if (!(((f == 0 || f == P.ny) && !P.per_y) || !(ia != 0 && ib != 0))) {
+                    const int g = (fr_ + 1) * HK + fc + 1;
+                    const double ga = sm.gy[1 * GYR * HK + g], gb = sm.gy[2 * GYR * HK + g], gc = sm.gy[g];
+                    const TileCell lo{gxc, gxn, sm.gy, sm.gz, sm.d0, fr_, fc + 1};
+                    const TileCell hi{gxc, gxn, sm.gy, sm.gz, sm.d0, fr_ + 1, fc + 1};
+                    double a1[3], a2[3];
+                    side_rows<1>(lo, sm.mat[ia - 1], ga, gb, gc, a1);
+                    side_rows<1>(hi, sm.mat[ib - 1], ga, gb, gc, a2);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; a++) sm.fy[a * FYR * TK + it] = o[a];
+            }
+            for (int it = tid; it < TJ * FZC; it += blockDim.x) {
+                const int rl = it / FZC, fc = it - (it / FZC) * FZC;      // row j0+rl, face k0+fc
+                const int f = k0 + fc;
+                const int rr = rl + 1;
+                const uint8_t ia = sm.idc[rr * HK + fc], ib = sm.idc[rr * HK + fc + 1];
+                double o[3] = {0., 0., 0.};
+                if (!(((f == 0 || f == P.nz) && !P.per_z) || !(ia != 0 && ib != 0))) {
+                    const int g = rr * GZC + fc + 1;
+                    const double ga = sm.gz[2 * HJ * GZC + g], gb = sm.gz[1 * HJ * GZC + g], gc = sm.gz[g];
+                    const TileCell lo{gxc, gxn, sm.gy, sm.gz, sm.d0, rr, fc};
+                    const TileCell hi{gxc, gxn, sm.gy, sm.gz, sm.d0, rr, fc + 1};
+                    double a1[3], a2[3];
+                    side_rows<2>(lo, sm.mat[ia - 1], ga, gb, gc, a1);
+                    side_rows<2>(hi, sm.mat[ib - 1], ga, gb, gc, a2);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; a++) sm.fz[a * TJ * FZC + it] = o[a];
+            }
+        }
+        if (q + 1 <= L) etile_stage(P, io, sm, cur, wrapm(p + 2, P.nx));
+        __syncthreads();
+
+        // ---- B2: one column per thread ----
         if (valid) {
-            const TileCell me{gxc, gxn, sGY, sGZ, sD0, r, s};
-            const uint8_t id = sMid[r * HK + s];
+            const TileCell me{gxc, gxn, sm.gy, sm.gz, sm.d0, r, s};
+            const uint8_t id = sm.idc[r * HK + s];
             // x-face p: between planes p-1 and p
             if (q >= 1) {
                 double sx[3] = {0., 0., 0.};
                 const bool fr = ((p == 0 || p == P.nx) && !P.per_x) || !(mid_prev != 0 && id != 0);
                 if (!fr) {
-                    const double ga = gxc[(0 * HJ + r) * HK + s], gb = gxc[(2 * HJ + r) * HK + s], gc = gxc[(1 * HJ + r) * HK + s];
+                    const int g = r * HK + s;
+                    const double ga = gxc[g], gb = gxc[2 * HJ * HK + g], gc = gxc[HJ * HK + g];
                     double sb[3];
-                    side_rows<0>(me, io.mats[id - 1], ga, gb, gc, sb);
+                    side_rows<0>(me, sm.mat[id - 1], ga, gb, gc, sb);
+#pragma unroll
                     for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / 2.;
                 }
                 if (q >= 2) {
                     // cell (p-1, j, k) is complete
-                    const long c = cid(P, p - 1, j, k);
+                    const long c = (long)(p - 1) * nyz + (long)j * P.nz + k;
                     double dv[3] = {0., 0., 0.};
                     if (mid_prev != 0) {
-                        const DevMat& mt = io.mats[mid_prev - 1];
+                        const ElMat& mt = sm.mat[mid_prev - 1];
+#pragma unroll
                         for (int a = 0; a < 3; a++) {
                             const double tx = (sx[a] - sxp[a]) / P.dx;
                             const double f = tx + ty[a] + tz[a];
@@ -367,84 +529,76 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     }
                     rk_vu<S>(io, c, dv, P.dt);
                 }
+#pragma unroll
                 for (int a = 0; a < 3; a++) sxp[a] = sx[a];
             }
-            // y- and z-faces of the interior plane p
-            if (q >= 1 && q <= L && id != 0) {
-                const DevMat& m = io.mats[id - 1];
-                double s1[3], s2[3];
-                // -y face j (neighbour row r-1), +y face j+1 (row r+1)
-                for (int side = 0; side < 2; side++) {
-                    const int f = j + side;
-                    const bool fr = ((f == 0 || f == P.ny) && !P.per_y) ||
-                                    !(sMid[(r - 1 + side) * HK + s] != 0 && sMid[(r + side) * HK + s] != 0);
-                    double* o = side ? s2 : s1;
-                    if (fr) { o[0] = o[1] = o[2] = 0.; continue; }
-                    const int rf = r + side;
-                    const double ga = sGY[(1 * GYR + rf) * HK + s], gb = sGY[(2 * GYR + rf) * HK + s], gc = sGY[(0 * GYR + rf) * HK + s];
-                    const TileCell nb{gxc, gxn, sGY, sGZ, sD0, side ? r + 1 : r - 1, s};
-                    double a1[3], a2[3];
-                    side_rows<1>(me, m, ga, gb, gc, a1);
-                    side_rows<1>(nb, io.mats[sMid[nb.r * HK + s] - 1], ga, gb, gc, a2);
-                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
-                }
-                for (int a = 0; a < 3; a++) ty[a] = (s2[a] - s1[a]) / P.dy;
-                // -z face k (neighbour column s-1), +z face k+1 (column s+1)
-                for (int side = 0; side < 2; side++) {
-                    const int f = k + side;
-                    const bool fr = ((f == 0 || f == P.nz) && !P.per_z) ||
-                                    !(sMid[r * HK + s - 1 + side] != 0 && sMid[r * HK + s + side] != 0);
-                    double* o = side ? s2 : s1;
-                    if (fr) {
-                        o[0] = o[1] = o[2] = 0.;
-                        if (side == 1 && traction_here) {
+            if (q >= 1 && q <= L) {
+                if (id != 0) {
+                    double s1[3], s2[3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        s1[a] = sm.fy[(a * FYR + jl) * TK + kl];
+                        s2[a] = sm.fy[(a * FYR + jl + 1) * TK + kl];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; a++) ty[a] = (s2[a] - s1[a]) / P.dy;
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        s1[a] = sm.fz[(a * TJ + jl) * FZC + kl];
+                        s2[a] = sm.fz[(a * TJ + jl) * FZC + kl + 1];
+                    }
+                    if (traction_here || quirk) {
+                        const uint8_t iu = sm.idc[r * HK + s + 1];
+                        const bool top_free = ((k + 1 == P.nz) && !P.per_z) || !(id != 0 && iu != 0);
+                        if (top_free && traction_here) {
                             // surface traction: x -> xz, y -> yz, z -> zz
                             const double tr = stage_drive(io, S).traction;
-                            if (P.strain_comp == 0) o[0] = tr; else if (P.strain_comp == 1) o[1] = tr; else o[2] = tr;
+                            s2[0] = s2[1] = s2[2] = 0.;
+                            if (P.strain_comp == 0) s2[0] = tr; else if (P.strain_comp == 1) s2[1] = tr; else s2[2] = tr;
+                        } else if (!top_free && quirk) {
+                            // the reference's +z neighbour of k == ny-1 is k = 0
+                            // (elastic_dynamic_solver.cpp:1247); creation rejects
+                            // decks where that cell is vacuum
+                            const int g = r * GZC + s + 1;
+                            const double ga = sm.gz[2 * HJ * GZC + g], gb = sm.gz[1 * HJ * GZC + g], gc = sm.gz[g];
+                            const GlobalCell nb(P, io, pw, j, 0);
+                            double a1[3], a2[3];
+                            side_rows<2>(me, sm.mat[id - 1], ga, gb, gc, a1);
+                            side_rows<2>(nb, sm.mat[io.mid[(long)po + (long)j * P.nz] - 1], ga, gb, gc, a2);
+#pragma unroll
+                            for (int a = 0; a < 3; a++) s2[a] = (a1[a] + a2[a]) / 2.;
                         }
-                        continue;
                     }
-                    const int sf = s + side;
-                    const double ga = sGZ[(2 * HJ + r) * GZC + sf], gb = sGZ[(1 * HJ + r) * GZC + sf], gc = sGZ[(0 * HJ + r) * GZC + sf];
-                    double a1[3], a2[3];
-                    side_rows<2>(me, m, ga, gb, gc, a1);
-                    if (side == 1 && quirk) {
-                        // the reference's +z neighbour of k == ny-1 is k = 0
-                        // (elastic_dynamic_solver.cpp:1247); creation rejects
-                        // decks where that cell is vacuum
-                        const GlobalCell nb(P, io, pw, j, 0);
-                        side_rows<2>(nb, io.mats[io.mid[cid(P, pw, j, 0)] - 1], ga, gb, gc, a2);
-                    } else {
-                        const TileCell nb{gxc, gxn, sGY, sGZ, sD0, r, side ? s + 1 : s - 1};
-                        side_rows<2>(nb, io.mats[sMid[r * HK + nb.s] - 1], ga, gb, gc, a2);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) tz[a] = (s2[a] - s1[a]) / P.dz;
+                    // cell strain for the magnetic and ferroelectric kernels
+                    if (want_strain && (sm.mat[id - 1].flags & (MF_FM | MF_FE))) {
+                        double e[6];
+                        e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
+                        e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;
+                        e[2] = (me.gm(2, 2) + me.gp(2, 2)) / 2.;
+                        e[3] = (me.gm(2, 1) + me.gp(2, 1) + me.gm(1, 2) + me.gp(1, 2)) / 4.;
+                        e[4] = (me.gm(2, 0) + me.gp(2, 0) + me.gm(0, 2) + me.gp(0, 2)) / 4.;
+                        e[5] = (me.gm(1, 0) + me.gp(1, 0) + me.gm(0, 1) + me.gp(0, 1)) / 4.;
+                        if (P.rot) {
+                            double t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
+                            rot_tensor(P.Tg2c, t3, o3);
+                            e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
+                        }
+                        const long c = (long)po + (long)j * P.nz + k;
+#pragma unroll
+                        for (int a = 0; a < 6; a++) io.strain_c[a][c] = e[a];
                     }
-                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                } else {
+#pragma unroll
+                    for (int a = 0; a < 3; a++) ty[a] = tz[a] = 0.;
                 }
-                for (int a = 0; a < 3; a++) tz[a] = (s2[a] - s1[a]) / P.dz;
-                // cell strain for the magnetic and ferroelectric kernels
-                if (want_strain && (m.flags & (MF_FM | MF_FE))) {
-                    double e[6];
-                    e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
-                    e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;
-                    e[2] = (me.gm(2, 2) + me.gp(2, 2)) / 2.;
-                    e[3] = (me.gm(2, 1) + me.gp(2, 1) + me.gm(1, 2) + me.gp(1, 2)) / 4.;
-                    e[4] = (me.gm(2, 0) + me.gp(2, 0) + me.gm(0, 2) + me.gp(0, 2)) / 4.;
-                    e[5] = (me.gm(1, 0) + me.gp(1, 0) + me.gm(0, 1) + me.gp(0, 1)) / 4.;
-                    if (P.rot) {
-                        double t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
-                        rot_tensor(P.Tg2c, t3, o3);
-                        e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
-                    }
-                    const long c = cid(P, p, j, k);
-                    for (int a = 0; a < 6; a++) io.strain_c[a][c] = e[a];
-                }
-            } else if (q >= 1 && q <= L) {
-                for (int a = 0; a < 3; a++) ty[a] = tz[a] = 0.;
             }
             // lower cell's half of x-face p+1
             if (q <= L && id != 0) {
-                const double ga = gxn[(0 * HJ + r) * HK + s], gb = gxn[(2 * HJ + r) * HK + s], gc = gxn[(1 * HJ + r) * HK + s];
-                side_rows<0>(me, io.mats[id - 1], ga, gb, gc, sa);
+                const int g = r * HK + s;
+                const double ga = gxn[g], gb = gxn[2 * HJ * HK + g], gc = gxn[HJ * HK + g];
+                side_rows<0>(me, sm.mat[id - 1], ga, gb, gc, sa);
             }
             mid_prev = id;
         }

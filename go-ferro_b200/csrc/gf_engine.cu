@@ -79,6 +79,8 @@ struct gf_engine {
     double* fg[9] = {};
     double* strain_c[6] = {};
     int el_chunk = 1;                  // x-planes per block of k_elastic_tile
+    int el_nmat = 0;                   // materials staged by k_elastic_tile
+    size_t el_smem = 0;                // its dynamic shared memory
     double* liao_hist = nullptr; double* liao_last = nullptr;
     double* scratch = nullptr;             // 6n doubles: output staging and reductions
     int* flag = nullptr;
@@ -532,24 +534,31 @@ void build_io(gf_engine* eng) {
 // ---------------------------------------------------------------------------
 // one RK4 step: kernel sequence in the reference's data order
 // ---------------------------------------------------------------------------
-// Shared-memory opt-in and the x-chunk of the tiled elastic kernel: enough
-// chunks that every SM holds as many blocks as fit, for about two waves.
+// Shared-memory opt-in and the x-chunk of the tiled elastic kernel.  A
+// block of `L` planes costs L+2 plane passes (one halo plane each side), so
+// the chunk count minimises waves x (L+2) over the blocks that fit at once.
 int setup_elastic_tile(gf_engine* eng) {
     const Params& P = eng->P;
-    const int smem = (int)etile::kSmemBytes;
+    eng->el_nmat = (int)eng->deck.mats.size();
+    eng->el_smem = etile::smem_bytes(eng->el_nmat);
+    const int smem = (int)eng->el_smem;
     GF_CU(cudaFuncSetAttribute(k_elastic_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     GF_CU(cudaFuncSetAttribute(k_elastic_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     GF_CU(cudaFuncSetAttribute(k_elastic_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     GF_CU(cudaFuncSetAttribute(k_elastic_tile<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 1, sms = 1;
-    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1>, etile::NT, etile::kSmemBytes));
+    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1>, etile::NT, eng->el_smem));
     GF_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, eng->device));
+    if (per_sm < 1) { eng->err = "elastic tile does not fit on an SM"; return GF_ECUDA; }
+    const long slots = (long)per_sm * sms;
     const long tiles = (long)((P.nz + etile::TK - 1) / etile::TK) * ((P.ny + etile::TJ - 1) / etile::TJ);
-    const long want = 2L * (per_sm > 0 ? per_sm : 1) * sms;
-    long chunks = (want + tiles - 1) / tiles;
-    if (chunks < 1) chunks = 1;
-    if (chunks > P.nx) chunks = P.nx;
-    eng->el_chunk = (int)((P.nx + chunks - 1) / chunks);
+    long best_cost = -1;
+    for (long c = 1; c <= P.nx; c++) {
+        const long L = (P.nx + c - 1) / c;
+        const long blocks = tiles * ((P.nx + L - 1) / L);
+        const long cost = ((blocks + slots - 1) / slots) * (L + 2);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; eng->el_chunk = (int)L; }
+    }
     return GF_OK;
 }
 
@@ -562,8 +571,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
     if (P.elastic) {
         const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
                         (P.nx + eng->el_chunk - 1) / eng->el_chunk);
-        GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S>, grid, dim3(etile::NT), etile::kSmemBytes, st, P, io,
-                            eng->el_chunk));
+        GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
+                            eng->el_chunk, eng->el_nmat));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
