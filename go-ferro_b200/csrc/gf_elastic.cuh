@@ -158,8 +158,9 @@ constexpr int kFY = 3 * FYR * TK, kFZ = 3 * TJ * FZC;
 constexpr int kDoubles = 2 * kU + 2 * kGX + kGY + kGZ + kD0 + kFY + kFZ;
 constexpr size_t kFixedBytes = (size_t)kDoubles * sizeof(double) + (size_t)(2 * UR + UC) * sizeof(int)
                                + (size_t)(2 * UR * UC + HJ * HK);
-inline size_t smem_bytes(int nmat) { return (size_t)nmat * sizeof(ElMat) + kFixedBytes; }
-constexpr size_t kMaxSmemBytes = (size_t)kMaxMat * sizeof(ElMat) + kFixedBytes;
+constexpr size_t kMatOffset = (kFixedBytes + 15) / 16 * 16;
+inline size_t smem_bytes(int nmat) { return kMatOffset + (size_t)nmat * sizeof(ElMat); }
+constexpr size_t kMaxSmemBytes = kMatOffset + (size_t)kMaxMat * sizeof(ElMat);
 }  // namespace etile
 
 // index x in [-n, 2n) wrapped into [0, n)
@@ -173,10 +174,11 @@ __host__ __device__ constexpr int face_row(int d, int r) {
 
 // row r of C * e with the accumulation order of strain2stress_glb
 // (mathlib.cpp:127-135); zero entries of the cubic pattern are skipped,
-// which leaves every partial sum unchanged
-template <class M>
+// which leaves every partial sum unchanged.  CUB: every material of the
+// run has the cubic pattern.
+template <bool CUB, class M>
 __device__ inline double stress_row(const M& m, const double e[6], int r) {
-    if (m.cubic_c) {
+    if (CUB || m.cubic_c) {
         if (r < 3) return m.cij[r][0] * e[0] + m.cij[r][1] * e[1] + m.cij[r][2] * e[2];
         return m.cij[r][r] * e[r];
     }
@@ -255,7 +257,7 @@ struct GlobalCell {
 // the face's gradient of the normal displacement component, gb and gc those
 // of the two tangential components (x-face: u_z, u_y; y-face: u_z, u_x;
 // z-face: u_y, u_x).
-template <int D, class V, class M>
+template <int D, bool CUB, class V, class M>
 __device__ inline void side_rows(const V& v, const M& m, double ga, double gb, double gc, double out[3]) {
     double st[6];
     if (D == 0) {
@@ -281,7 +283,7 @@ __device__ inline void side_rows(const V& v, const M& m, double ga, double gb, d
         st[5] = ((v.gm(1, 0) + v.gp(1, 0) + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
     }
 #pragma unroll
-    for (int r = 0; r < 3; r++) out[r] = stress_row(m, st, face_row(D, r));
+    for (int r = 0; r < 3; r++) out[r] = stress_row<CUB>(m, st, face_row(D, r));
 }
 
 // RK4 combination for v and u of one cell (du = v_stage * dt)
@@ -309,50 +311,48 @@ __device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], doub
     }
 }
 
-// Shared-memory plan of k_elastic_tile (byte offsets from the dynamic base)
+// Shared-memory plan of k_elastic_tile: every array sits at a compile-time
+// offset from the dynamic base; the material table (sized at launch) is last.
 struct ETileSmem {
-    ElMat* mat;
-    double *u[2], *gx[2], *gy, *gz, *d0, *fy, *fz;
-    int *rowoff, *rowj, *colk;
-    uint8_t *id[2], *idc;
-    __device__ ETileSmem(unsigned char* base, int nmat) {
-        using namespace etile;
-        mat = reinterpret_cast<ElMat*>(base);
-        double* d = reinterpret_cast<double*>(base + (size_t)nmat * sizeof(ElMat));
-        u[0] = d; u[1] = d + kU; d += 2 * kU;
-        gx[0] = d; gx[1] = d + kGX; d += 2 * kGX;
-        gy = d; d += kGY;
-        gz = d; d += kGZ;
-        d0 = d; d += kD0;
-        fy = d; d += kFY;
-        fz = d; d += kFZ;
-        int* ip = reinterpret_cast<int*>(d);
-        rowoff = ip; rowj = ip + UR; colk = ip + 2 * UR;
-        uint8_t* bp = reinterpret_cast<uint8_t*>(ip + 2 * UR + UC);
-        id[0] = bp; id[1] = bp + UR * UC; idc = bp + 2 * UR * UC;
-    }
+    unsigned char* base;
+    __device__ double* dp() const { return reinterpret_cast<double*>(base); }
+    __device__ double* u(int slot) const { return dp() + slot * etile::kU; }
+    __device__ double* gx(int slot) const { return dp() + 2 * etile::kU + slot * etile::kGX; }
+    __device__ double* gy() const { return dp() + 2 * etile::kU + 2 * etile::kGX; }
+    __device__ double* gz() const { return gy() + etile::kGY; }
+    __device__ double* d0() const { return gz() + etile::kGZ; }
+    __device__ double* fy() const { return d0() + etile::kD0; }
+    __device__ double* fz() const { return fy() + etile::kFY; }
+    __device__ int* ip() const { return reinterpret_cast<int*>(dp() + etile::kDoubles); }
+    __device__ int* rowoff() const { return ip(); }
+    __device__ int* rowj() const { return ip() + etile::UR; }
+    __device__ int* colk() const { return ip() + 2 * etile::UR; }
+    __device__ uint8_t* bp() const { return reinterpret_cast<uint8_t*>(ip() + 2 * etile::UR + etile::UC); }
+    __device__ uint8_t* id(int slot) const { return bp() + slot * etile::UR * etile::UC; }
+    __device__ uint8_t* idc() const { return bp() + 2 * etile::UR * etile::UC; }
+    __device__ ElMat* mat() const { return reinterpret_cast<ElMat*>(base + etile::kMatOffset); }
 };
 
 // stage u and material ids of plane pw into ring slot `slot`
 __device__ inline void etile_stage(const Params& P, const StageIO& io, const ETileSmem& sm, int slot, int pw) {
     using namespace etile;
     const int po = pw * P.ny * P.nz;
-    double* su = sm.u[slot];
-    uint8_t* sid = sm.id[slot];
+    double* su = sm.u(slot);
+    uint8_t* sid = sm.id(slot);
     for (int it = threadIdx.x; it < UR * UC; it += blockDim.x) {
         const int ur = it / UC, uc = it - (it / UC) * UC;
-        const int c = po + sm.rowoff[ur] + sm.colk[uc];
+        const int c = po + sm.rowoff()[ur] + sm.colk()[uc];
         sid[it] = io.mid[c];
 #pragma unroll
         for (int a = 0; a < 3; a++) su[a * UR * UC + it] = io.u_in.c[a][c];
     }
 }
 
-template <int S>
+template <int S, bool CUB>
 __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO io, int chunk, int nmat) {
     using namespace etile;
     GF_EXTERN_SMEM(unsigned char, smem_raw);
-    const ETileSmem sm(smem_raw, nmat);
+    const ETileSmem sm{smem_raw};
 
     const int tid = threadIdx.x;
     const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
     // ---- block set-up: material table, wrapped row/column offsets, first two planes ----
     for (int it = tid; it < nmat; it += blockDim.x) {
         const DevMat& d = io.mats[it];
-        ElMat& e = sm.mat[it];
+        ElMat& e = sm.mat()[it];
         for (int a = 0; a < 6; a++) for (int b = 0; b < 6; b++) e.cij[a][b] = d.cij[a][b];
         e.dens_dt = d.dens_dt; e.mass_damp = d.mass_damp; e.stiff_damp = d.stiff_damp;
         e.l100_15 = d.l100_15; e.l111_15 = d.l111_15; e.Q11 = d.Q11; e.Q12 = d.Q12; e.Q44 = d.Q44;
@@ -381,11 +381,11 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
     for (int it = tid; it < UR; it += blockDim.x) {
         int jj = j0 - 2 + it;
         jj = jj < 0 ? jj + P.ny : jj % P.ny;
-        sm.rowj[it] = jj; sm.rowoff[it] = jj * P.nz;
+        sm.rowj()[it] = jj; sm.rowoff()[it] = jj * P.nz;
     }
     for (int it = tid; it < UC; it += blockDim.x) {
         int kk = k0 - 2 + it;
-        sm.colk[it] = kk < 0 ? kk + P.nz : kk % P.nz;
+        sm.colk()[it] = kk < 0 ? kk + P.nz : kk % P.nz;
     }
     __syncthreads();
     etile_stage(P, io, sm, 0, wrapm(i0 - 1, P.nx));
@@ -402,12 +402,12 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         const int pw = wrapm(p, P.nx);
         const int po = pw * nyz;
         const int cur = q & 1, nxt = cur ^ 1;           // ring slots of planes p and p+1
-        const double* uc = sm.u[cur];
-        const double* un = sm.u[nxt];
-        const uint8_t* ic = sm.id[cur];
-        const uint8_t* in = sm.id[nxt];
-        double* gxc = sm.gx[cur ^ 1];                    // face p   (computed in the previous pass)
-        double* gxn = sm.gx[cur];                        // face p+1
+        const double* uc = sm.u(cur);
+        const double* un = sm.u(nxt);
+        const uint8_t* ic = sm.id(cur);
+        const uint8_t* in = sm.id(nxt);
+        double* gxc = sm.gx(cur ^ 1);                    // face p   (computed in the previous pass)
+        double* gxn = sm.gx(cur);                        // face p+1
         // ---- A: gradients and eigenstrains of plane p ----
         if (q <= L) {
             const int f = p + 1;
@@ -424,27 +424,27 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         for (int it = tid; it < GYR * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
             const int u1 = (rr + 1) * UC + ss + 1, u0 = rr * UC + ss + 1;
-            const bool fr = (sm.rowj[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
+            const bool fr = (sm.rowj()[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gy[a * GYR * HK + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dy;
+                sm.gy()[a * GYR * HK + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dy;
         }
         for (int it = tid; it < HJ * GZC; it += blockDim.x) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
             const int u1 = (rr + 1) * UC + ss + 1, u0 = u1 - 1;
-            const bool fr = (sm.colk[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
+            const bool fr = (sm.colk()[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gz[a * HJ * GZC + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dz;
+                sm.gz()[a * HJ * GZC + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dz;
         }
         for (int it = tid; it < HJ * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
             const uint8_t id = ic[(rr + 1) * UC + ss + 1];
-            sm.idc[it] = id;
+            sm.idc()[it] = id;
             double e[6] = {0., 0., 0., 0., 0., 0.};
-            if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff[rr + 1] + sm.colk[ss + 1], sm.mat[id - 1], e);
+            if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff()[rr + 1] + sm.colk()[ss + 1], sm.mat()[id - 1], e);
 #pragma unroll
-            for (int a = 0; a < 6; a++) sm.d0[a * HJ * HK + it] = e[a];
+            for (int a = 0; a < 6; a++) sm.d0()[a * HJ * HK + it] = e[a];
         }
         __syncthreads();
 
@@ -453,41 +453,41 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             for (int it = tid; it < FYR * TK; it += blockDim.x) {
                 const int fr_ = it / TK, fc = it - (it / TK) * TK;       // face j0+fr_, column k0+fc
                 const int f = j0 + fr_;
-                const uint8_t ia = sm.idc[fr_ * HK + fc + 1], ib = sm.idc[(fr_ + 1) * HK + fc + 1];
+                const uint8_t ia = sm.idc()[fr_ * HK + fc + 1], ib = sm.idc()[(fr_ + 1) * HK + fc + 1];
                 double o[3] = {0., 0., 0.};
                 if (!(((f == 0 || f == P.ny) && !P.per_y) || !(ia != 0 && ib != 0))) {
                     const int g = (fr_ + 1) * HK + fc + 1;
-                    const double ga = sm.gy[1 * GYR * HK + g], gb = sm.gy[2 * GYR * HK + g], gc = sm.gy[g];
-                    const TileCell lo{gxc, gxn, sm.gy, sm.gz, sm.d0, fr_, fc + 1};
-                    const TileCell hi{gxc, gxn, sm.gy, sm.gz, sm.d0, fr_ + 1, fc + 1};
+                    const double ga = sm.gy()[1 * GYR * HK + g], gb = sm.gy()[2 * GYR * HK + g], gc = sm.gy()[g];
+                    const TileCell lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_, fc + 1};
+                    const TileCell hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_ + 1, fc + 1};
                     double a1[3], a2[3];
-                    side_rows<1>(lo, sm.mat[ia - 1], ga, gb, gc, a1);
-                    side_rows<1>(hi, sm.mat[ib - 1], ga, gb, gc, a2);
+                    side_rows<1, CUB>(lo, sm.mat()[ia - 1], ga, gb, gc, a1);
+                    side_rows<1, CUB>(hi, sm.mat()[ib - 1], ga, gb, gc, a2);
 #pragma unroll
                     for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
                 }
 #pragma unroll
-                for (int a = 0; a < 3; a++) sm.fy[a * FYR * TK + it] = o[a];
+                for (int a = 0; a < 3; a++) sm.fy()[a * FYR * TK + it] = o[a];
             }
             for (int it = tid; it < TJ * FZC; it += blockDim.x) {
                 const int rl = it / FZC, fc = it - (it / FZC) * FZC;      // row j0+rl, face k0+fc
                 const int f = k0 + fc;
                 const int rr = rl + 1;
-                const uint8_t ia = sm.idc[rr * HK + fc], ib = sm.idc[rr * HK + fc + 1];
+                const uint8_t ia = sm.idc()[rr * HK + fc], ib = sm.idc()[rr * HK + fc + 1];
                 double o[3] = {0., 0., 0.};
                 if (!(((f == 0 || f == P.nz) && !P.per_z) || !(ia != 0 && ib != 0))) {
                     const int g = rr * GZC + fc + 1;
-                    const double ga = sm.gz[2 * HJ * GZC + g], gb = sm.gz[1 * HJ * GZC + g], gc = sm.gz[g];
-                    const TileCell lo{gxc, gxn, sm.gy, sm.gz, sm.d0, rr, fc};
-                    const TileCell hi{gxc, gxn, sm.gy, sm.gz, sm.d0, rr, fc + 1};
+                    const double ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
+                    const TileCell lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc};
+                    const TileCell hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc + 1};
                     double a1[3], a2[3];
-                    side_rows<2>(lo, sm.mat[ia - 1], ga, gb, gc, a1);
-                    side_rows<2>(hi, sm.mat[ib - 1], ga, gb, gc, a2);
+                    side_rows<2, CUB>(lo, sm.mat()[ia - 1], ga, gb, gc, a1);
+                    side_rows<2, CUB>(hi, sm.mat()[ib - 1], ga, gb, gc, a2);
 #pragma unroll
                     for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
                 }
 #pragma unroll
-                for (int a = 0; a < 3; a++) sm.fz[a * TJ * FZC + it] = o[a];
+                for (int a = 0; a < 3; a++) sm.fz()[a * TJ * FZC + it] = o[a];
             }
         }
         if (q + 1 <= L) etile_stage(P, io, sm, cur, wrapm(p + 2, P.nx));
@@ -495,8 +495,8 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 
         // ---- B2: one column per thread ----
         if (valid) {
-            const TileCell me{gxc, gxn, sm.gy, sm.gz, sm.d0, r, s};
-            const uint8_t id = sm.idc[r * HK + s];
+            const TileCell me{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), r, s};
+            const uint8_t id = sm.idc()[r * HK + s];
             // x-face p: between planes p-1 and p
             if (q >= 1) {
                 double sx[3] = {0., 0., 0.};
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     const int g = r * HK + s;
                     const double ga = gxc[g], gb = gxc[2 * HJ * HK + g], gc = gxc[HJ * HK + g];
                     double sb[3];
-                    side_rows<0>(me, sm.mat[id - 1], ga, gb, gc, sb);
+                    side_rows<0, CUB>(me, sm.mat()[id - 1], ga, gb, gc, sb);
 #pragma unroll
                     for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / 2.;
                 }
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     const long c = (long)(p - 1) * nyz + (long)j * P.nz + k;
                     double dv[3] = {0., 0., 0.};
                     if (mid_prev != 0) {
-                        const ElMat& mt = sm.mat[mid_prev - 1];
+                        const ElMat& mt = sm.mat()[mid_prev - 1];
 #pragma unroll
                         for (int a = 0; a < 3; a++) {
                             const double tx = (sx[a] - sxp[a]) / P.dx;
@@ -537,18 +537,18 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     double s1[3], s2[3];
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        s1[a] = sm.fy[(a * FYR + jl) * TK + kl];
-                        s2[a] = sm.fy[(a * FYR + jl + 1) * TK + kl];
+                        s1[a] = sm.fy()[(a * FYR + jl) * TK + kl];
+                        s2[a] = sm.fy()[(a * FYR + jl + 1) * TK + kl];
                     }
 #pragma unroll
                     for (int a = 0; a < 3; a++) ty[a] = (s2[a] - s1[a]) / P.dy;
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        s1[a] = sm.fz[(a * TJ + jl) * FZC + kl];
-                        s2[a] = sm.fz[(a * TJ + jl) * FZC + kl + 1];
+                        s1[a] = sm.fz()[(a * TJ + jl) * FZC + kl];
+                        s2[a] = sm.fz()[(a * TJ + jl) * FZC + kl + 1];
                     }
                     if (traction_here || quirk) {
-                        const uint8_t iu = sm.idc[r * HK + s + 1];
+                        const uint8_t iu = sm.idc()[r * HK + s + 1];
                         const bool top_free = ((k + 1 == P.nz) && !P.per_z) || !(id != 0 && iu != 0);
                         if (top_free && traction_here) {
                             // surface traction: x -> xz, y -> yz, z -> zz
@@ -560,11 +560,11 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                             // (elastic_dynamic_solver.cpp:1247); creation rejects
                             // decks where that cell is vacuum
                             const int g = r * GZC + s + 1;
-                            const double ga = sm.gz[2 * HJ * GZC + g], gb = sm.gz[1 * HJ * GZC + g], gc = sm.gz[g];
+                            const double ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
                             const GlobalCell nb(P, io, pw, j, 0);
                             double a1[3], a2[3];
-                            side_rows<2>(me, sm.mat[id - 1], ga, gb, gc, a1);
-                            side_rows<2>(nb, sm.mat[io.mid[(long)po + (long)j * P.nz] - 1], ga, gb, gc, a2);
+                            side_rows<2, CUB>(me, sm.mat()[id - 1], ga, gb, gc, a1);
+                            side_rows<2, CUB>(nb, sm.mat()[io.mid[(long)po + (long)j * P.nz] - 1], ga, gb, gc, a2);
 #pragma unroll
                             for (int a = 0; a < 3; a++) s2[a] = (a1[a] + a2[a]) / 2.;
                         }
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 #pragma unroll
                     for (int a = 0; a < 3; a++) tz[a] = (s2[a] - s1[a]) / P.dz;
                     // cell strain for the magnetic and ferroelectric kernels
-                    if (want_strain && (sm.mat[id - 1].flags & (MF_FM | MF_FE))) {
+                    if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_FE))) {
                         double e[6];
                         e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
                         e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;
@@ -598,7 +598,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             if (q <= L && id != 0) {
                 const int g = r * HK + s;
                 const double ga = gxn[g], gb = gxn[2 * HJ * HK + g], gc = gxn[HJ * HK + g];
-                side_rows<0>(me, sm.mat[id - 1], ga, gb, gc, sa);
+                side_rows<0, CUB>(me, sm.mat()[id - 1], ga, gb, gc, sa);
             }
             mid_prev = id;
         }

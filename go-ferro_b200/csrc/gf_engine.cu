@@ -81,6 +81,7 @@ struct gf_engine {
     int el_chunk = 1;                  // x-planes per block of k_elastic_tile
     int el_nmat = 0;                   // materials staged by k_elastic_tile
     size_t el_smem = 0;                // its dynamic shared memory
+    bool el_cubic = false;             // every material has the cubic stiffness pattern
     double* liao_hist = nullptr; double* liao_last = nullptr;
     double* scratch = nullptr;             // 6n doubles: output staging and reductions
     int* flag = nullptr;
@@ -542,12 +543,21 @@ int setup_elastic_tile(gf_engine* eng) {
     eng->el_nmat = (int)eng->deck.mats.size();
     eng->el_smem = etile::smem_bytes(eng->el_nmat);
     const int smem = (int)eng->el_smem;
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    eng->el_cubic = true;
+    for (const Material& m : eng->deck.mats)
+        for (int a = 0; a < 6; a++)
+            for (int b = 0; b < 6; b++)
+                if (!((a < 3 && b < 3) || a == b) && m.cij[a][b] != 0.) eng->el_cubic = false;
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 1, sms = 1;
-    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1>, etile::NT, eng->el_smem));
+    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false>, etile::NT, eng->el_smem));
     GF_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, eng->device));
     if (per_sm < 1) { eng->err = "elastic tile does not fit on an SM"; return GF_ECUDA; }
     const long slots = (long)per_sm * sms;
@@ -571,8 +581,12 @@ int enqueue_stage(gf_engine* eng, int parity) {
     if (P.elastic) {
         const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
                         (P.nx + eng->el_chunk - 1) / eng->el_chunk);
-        GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
-                            eng->el_chunk, eng->el_nmat));
+        if (eng->el_cubic)
+            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, true>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
+                                eng->el_chunk, eng->el_nmat));
+        else
+            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
+                                eng->el_chunk, eng->el_nmat));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
