@@ -34,7 +34,7 @@ OBS = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "u": 4}
 EXPORTS = ["gf_create_from_deck", "gf_advance", "gf_advance_eager", "gf_average", "gf_probe_em",
            "gf_field_dims", "gf_download", "gf_upload", "gf_download_device", "gf_upload_device",
            "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
-           "gf_destroy", "gf_version", "gf_field_mean_noalloc"]
+           "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients"]
 
 
 class GFInfo(ctypes.Structure):
@@ -95,6 +95,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_destroy.restype = None
     lib.gf_version.restype = ctypes.c_char_p
     lib.gf_field_mean_noalloc.argtypes = [vp, c_u64, ctypes.c_double, vp, vp]
+    lib.gf_check_quotients.argtypes = [ctypes.c_double, c_u64, c_u64, ctypes.POINTER(c_u64)]
     if path is None:
         _lib = lib
     return lib

@@ -57,6 +57,8 @@ struct Params {
     int per_x, per_y, per_z;
     long n;
     double dx, dy, dz, dt;
+    double rdx, rdy, rdz, rdt;   // correctly rounded reciprocals (host 1./dx ...), for qdiv
+    double dt_e0, mdt_mu0;       // dt / e0 and -dt / mu0, rounded as the reference does
     int rot;                 // if_OrientRotate
     double Tg2c[3][3], Tc2g[3][3];
     // active physics
@@ -103,6 +105,30 @@ struct StepDrive {
     double t;
     StageDrive st[4];
 };
+
+constexpr double kInv3 = 1. / 3.;
+constexpr double kInv6 = 1. / 6.;
+
+// x / d rounded to nearest, for a divisor d that is fixed for the run, given
+// rd = RN(1/d) (computed once on the host by IEEE division).  This is
+// Markstein's correction step (P. W. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1),
+// 1990): if q is within one ulp of x/d and rd is the correctly rounded
+// reciprocal, the residual r = x - d*q is exact in one FMA and RN(q + r*rd)
+// is the correctly rounded quotient.  q0 = RN(x*rd) can be up to two ulps
+// off, so a first correction makes it faithful and a second rounds it
+// correctly.  The identity needs normal residuals, which holds for every
+// field value here (|x| far above 1e-290); a zero x keeps its sign.  Five
+// FP64 operations and no branch, against the general division's reciprocal
+// refinement and slow-path test.
+__device__ __forceinline__ double qdiv(double x, double d, double rd) {
+    const double q0 = __dmul_rn(x, rd);
+    double r = __fma_rn(-q0, d, x);
+    const double q1 = __fma_rn(r, rd, q0);
+    r = __fma_rn(-q1, d, x);
+    const double q2 = __fma_rn(r, rd, q1);
+    return x == 0. ? q0 : q2;
+}
 
 __host__ __device__ inline long cid(const Params& P, long i, long j, long k) {
     return (i * P.ny + j) * P.nz + k;

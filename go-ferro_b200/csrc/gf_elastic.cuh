@@ -54,9 +54,9 @@ __global__ void __launch_bounds__(256) k_face_grad(Params P, StageIO io) {
     for (int a = 0; a < 3; a++) {
         const double* u = io.u_in.c[a];
         const double uc = u[c];
-        io.fg[a][c] = fx ? 0. : (uc - u[cx]) / P.dx;
-        io.fg[3 + a][c] = fy ? 0. : (uc - u[cy]) / P.dy;
-        io.fg[6 + a][c] = fz ? 0. : (uc - u[cz]) / P.dz;
+        io.fg[a][c] = fx ? 0. : qdiv((uc - u[cx]), P.dx, P.rdx);
+        io.fg[3 + a][c] = fy ? 0. : qdiv((uc - u[cy]), P.dy, P.rdy);
+        io.fg[6 + a][c] = fz ? 0. : qdiv((uc - u[cz]), P.dz, P.rdz);
     }
 }
 
@@ -240,9 +240,9 @@ struct GlobalCell {
     __device__ double grad(int d, int a, long ci, long cj, long ck) const {
         const double* u = io.u_in.c[a];
         const long c = cid(P, ci, cj, ck);
-        if (d == 0) return free_x(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci == 0 ? P.nx - 1 : ci - 1, cj, ck)]) / P.dx;
-        if (d == 1) return free_y(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci, cj == 0 ? P.ny - 1 : cj - 1, ck)]) / P.dy;
-        return free_z(P, io.mid, ci, cj, ck) ? 0. : (u[c] - u[cid(P, ci, cj, ck == 0 ? P.nz - 1 : ck - 1)]) / P.dz;
+        if (d == 0) return free_x(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci == 0 ? P.nx - 1 : ci - 1, cj, ck)]), P.dx, P.rdx);
+        if (d == 1) return free_y(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci, cj == 0 ? P.ny - 1 : cj - 1, ck)]), P.dy, P.rdy);
+        return free_z(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci, cj, ck == 0 ? P.nz - 1 : ck - 1)]), P.dz, P.rdz);
     }
     __device__ double gm(int d, int a) const { return grad(d, a, i, j, k); }
     __device__ double gp(int d, int a) const {
@@ -294,19 +294,19 @@ __device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], doub
         const double du = io.v_in.c[a][c] * dt;
         if (S == 0) {
             const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + dv[a] / 6.;
-            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + du / 6.;
+            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + qdiv(dv[a], 6., kInv6);
+            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + qdiv(du, 6., kInv6);
         } else if (S == 1) {
             const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 3.;
-            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 3.;
+            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
+            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
         } else if (S == 2) {
             const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 3.;
-            io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 3.;
+            io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
+            io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
         } else {
-            io.v_acc.c[a][c] = io.v_acc.c[a][c] + dv[a] / 6.;
-            io.u_acc.c[a][c] = io.u_acc.c[a][c] + du / 6.;
+            io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 6., kInv6);
+            io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 6., kInv6);
         }
     }
 }
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                 const bool fr = fb || !(ic[ui] != 0 && in[ui] != 0);
 #pragma unroll
                 for (int a = 0; a < 3; a++)
-                    gxn[a * HJ * HK + it] = fr ? 0. : (un[a * UR * UC + ui] - uc[a * UR * UC + ui]) / P.dx;
+                    gxn[a * HJ * HK + it] = fr ? 0. : qdiv((un[a * UR * UC + ui] - uc[a * UR * UC + ui]), P.dx, P.rdx);
             }
         }
         for (int it = tid; it < GYR * HK; it += blockDim.x) {
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             const bool fr = (sm.rowj()[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gy()[a * GYR * HK + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dy;
+                sm.gy()[a * GYR * HK + it] = fr ? 0. : qdiv((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dy, P.rdy);
         }
         for (int it = tid; it < HJ * GZC; it += blockDim.x) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             const bool fr = (sm.colk()[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gz()[a * HJ * GZC + it] = fr ? 0. : (uc[a * UR * UC + u1] - uc[a * UR * UC + u0]) / P.dz;
+                sm.gz()[a * HJ * GZC + it] = fr ? 0. : qdiv((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dz, P.rdz);
         }
         for (int it = tid; it < HJ * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                         const ElMat& mt = sm.mat()[mid_prev - 1];
 #pragma unroll
                         for (int a = 0; a < 3; a++) {
-                            const double tx = (sx[a] - sxp[a]) / P.dx;
+                            const double tx = qdiv((sx[a] - sxp[a]), P.dx, P.rdx);
                             const double f = tx + ty[a] + tz[a];
                             const double fs = io.force_store.c[a][c];
                             if (S == 1 || S == 2)
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                         s2[a] = sm.fy()[(a * FYR + jl + 1) * TK + kl];
                     }
 #pragma unroll
-                    for (int a = 0; a < 3; a++) ty[a] = (s2[a] - s1[a]) / P.dy;
+                    for (int a = 0; a < 3; a++) ty[a] = qdiv((s2[a] - s1[a]), P.dy, P.rdy);
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
                         s1[a] = sm.fz()[(a * TJ + jl) * FZC + kl];
@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                         }
                     }
 #pragma unroll
-                    for (int a = 0; a < 3; a++) tz[a] = (s2[a] - s1[a]) / P.dz;
+                    for (int a = 0; a < 3; a++) tz[a] = qdiv((s2[a] - s1[a]), P.dz, P.rdz);
                     // cell strain for the magnetic and ferroelectric kernels
                     if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_FE))) {
                         double e[6];

@@ -36,10 +36,10 @@ __device__ inline double jf_cell(const Params& P, const StageIO& io, const Stage
 
 template <int S>
 __device__ inline void rk_x(double xv, double d, double* out, double* acc, long e) {
-    if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + d / 6.; }
-    else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + d / 3.; }
-    else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + d / 3.; }
-    else { acc[e] = acc[e] + d / 6.; }
+    if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
+    else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
+    else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
+    else { acc[e] = acc[e] + qdiv(d, 6., kInv6); }
 }
 
 // E edge update of component C at edge (i,j,k) (index e in C's array).
@@ -84,16 +84,16 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
         const double* Hy = io.H_in.c[1];
         const double* Hz = io.H_in.c[2];
         if (C == 0) {
-            const double dHzdy = (Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]) / P.dy;
-            const double dHydz = (Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]) / P.dz;
+            const double dHzdy = qdiv((Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]), P.dy, P.rdy);
+            const double dHydz = qdiv((Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]), P.dz, P.rdz);
             curl = dHzdy - dHydz;
         } else if (C == 1) {
-            const double dHxdz = (Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]) / P.dz;
-            const double dHzdx = (Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]) / P.dx;
+            const double dHxdz = qdiv((Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]), P.dz, P.rdz);
+            const double dHzdx = qdiv((Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]), P.dx, P.rdx);
             curl = dHxdz - dHzdx;
         } else {
-            const double dHydx = (Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]) / P.dx;
-            const double dHxdy = (Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]) / P.dy;
+            const double dHydx = qdiv((Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]), P.dx, P.rdx);
+            const double dHxdy = qdiv((Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]), P.dy, P.rdy);
             curl = dHydx - dHxdy;
         }
         double Jf = 0., dP = 0., er = 0., cond = 0., pc = 0.;
@@ -113,10 +113,12 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
         }
         if (pc < 0.5) pc = 1.;
         Jf = Jf / 4.;
-        dP = dP / pc; er = er / 4.; cond = cond / 4.;
+        // pc counts the ferroelectric cells (1..4): divisions by 1, 2 and 4 are exact
+        dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
+        er = er / 4.; cond = cond / 4.;
         double rhs = curl - Jf;
-        rhs = rhs - cond * io.E_in.c[C][e] - dP / P.dt;
-        d = P.dt / kE0 / er * rhs;
+        rhs = rhs - cond * io.E_in.c[C][e] - qdiv(dP, P.dt, P.rdt);
+        d = P.dt_e0 / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
     }
     rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], e);
 }
@@ -131,20 +133,20 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, long i, lon
     double curl;
     long a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
     if (C == 0) {
-        const double dEzdy = (Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]) / P.dy;
-        const double dEydz = (Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]) / P.dz;
+        const double dEzdy = qdiv((Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dy, P.rdy);
+        const double dEydz = qdiv((Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]), P.dz, P.rdz);
         curl = dEzdy - dEydz;
         a1x = (i == 0) ? (P.per_x ? nx - 1 : 0) : i - 1;
         a2x = (i == nx) ? (P.per_x ? 0 : nx - 1) : i;
     } else if (C == 1) {
-        const double dExdz = (Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]) / P.dz;
-        const double dEzdx = (Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]) / P.dx;
+        const double dExdz = qdiv((Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dz, P.rdz);
+        const double dEzdx = qdiv((Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dx, P.rdx);
         curl = dExdz - dEzdx;
         a1y = (j == 0) ? (P.per_y ? ny - 1 : 0) : j - 1;
         a2y = (j == ny) ? (P.per_y ? 0 : ny - 1) : j;
     } else {
-        const double dEydx = (Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]) / P.dx;
-        const double dExdy = (Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]) / P.dy;
+        const double dEydx = qdiv((Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]), P.dx, P.rdx);
+        const double dExdy = qdiv((Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dy, P.rdy);
         curl = dEydx - dExdy;
         a1z = (k == 0) ? (P.per_z ? nz - 1 : 0) : k - 1;
         a2z = (k == nz) ? (P.per_z ? 0 : nz - 1) : k;
@@ -165,7 +167,9 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, long i, lon
         }
     }
     if (cnt < 0.5) cnt = 1.;
-    const double d = -P.dt / kMu0 * curl - (dM1 + dM2) / cnt;
+    // -dt/mu0 rounded once on the host; cnt is 1 or 2, so the division is exact
+    const double dMs = dM1 + dM2;
+    const double d = P.mdt_mu0 * curl - (cnt == 2. ? dMs * 0.5 : dMs);
     rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], e);
 }
 

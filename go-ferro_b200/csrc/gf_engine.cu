@@ -302,6 +302,8 @@ void build_params(gf_engine* eng) {
     P.nx = (int)d.nx; P.ny = (int)d.ny; P.nz = (int)d.nz; P.n = d.n();
     P.per_x = d.per_x; P.per_y = d.per_y; P.per_z = d.per_z;
     P.dx = d.dx; P.dy = d.dy; P.dz = d.dz; P.dt = d.dt;
+    P.rdx = 1. / d.dx; P.rdy = 1. / d.dy; P.rdz = 1. / d.dz; P.rdt = 1. / d.dt;
+    P.dt_e0 = d.dt / kE0; P.mdt_mu0 = -d.dt / kMu0;
     P.rot = d.orient_rotate;
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { P.Tg2c[i][j] = d.Tg2c[i][j]; P.Tc2g[i][j] = d.Tc2g[i][j]; }
     P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
@@ -1244,6 +1246,21 @@ void gf_destroy(gf_engine* e) {
     if (e->drive_host) cudaFreeHost(e->drive_host);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
+}
+
+int gf_check_quotients(double d, uint64_t n, uint64_t seed, uint64_t* mismatches) {
+    if (!mismatches || !(d != 0.) || !(d - d == 0.)) { g_create_err = "gf_check_quotients: need a finite nonzero d and an output"; return GF_EINVAL; }
+    unsigned long long* bad = nullptr;
+    cudaError_t ce = cudaMalloc(&bad, sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemset(bad, 0, sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = launch(k_check_quotients, dim3(1184), dim3(256), 0, (cudaStream_t)0, d, 1. / d,
+                                       (unsigned long long)n, (unsigned long long)seed, bad);
+    unsigned long long h = 0;
+    if (ce == cudaSuccess) ce = cudaMemcpy(&h, bad, sizeof(h), cudaMemcpyDeviceToHost);
+    if (bad) cudaFree(bad);
+    if (ce != cudaSuccess) { g_create_err = std::string("gf_check_quotients: ") + cudaGetErrorString(ce); return GF_ECUDA; }
+    *mismatches = (uint64_t)h;
+    return GF_OK;
 }
 
 const char* gf_version(void) { return "goferro_b200 0.1 (FP64 parity path, sm_100a)"; }

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
                               (j == P.ny - 1 && !P.per_y) || !is_fe(io.mats, io.mid[nb[3]]),
                               (k == 0 && !P.per_z) || !is_fe(io.mats, io.mid[nb[4]]),
                               (k == P.nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
-        const double h[3] = {P.dx, P.dy, P.dz};
+        const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
         double lap[3];   // sum of the three second derivatives per component
         for (int a = 0; a < 3; a++) {
             const double pc = io.p_in.c[a][c];
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
             for (int dir = 0; dir < 3; dir++) {
                 const double pb = surf[2 * dir] ? pc : io.p_in.c[a][nb[2 * dir]];
                 const double pf = surf[2 * dir + 1] ? pc : io.p_in.c[a][nb[2 * dir + 1]];
-                d2[dir] = (pf - 2. * pc + pb) / h[dir] / h[dir];
+                d2[dir] = qdiv(qdiv(pf - 2. * pc + pb, h[dir], rh[dir]), h[dir], rh[dir]);
             }
             lap[a] = d2[0] + d2[1] + d2[2];
         }
@@ -147,17 +147,17 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
         const double dp = io.q_in.c[a][c] * P.dt;
         const double qx = io.q_x.c[a][c], px = io.p_x.c[a][c];
         if (S == 0) {
-            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = qx + dq[a] / 6.;
-            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = px + dp / 6.;
+            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = qx + qdiv(dq[a], 6., kInv6);
+            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = px + qdiv(dp, 6., kInv6);
         } else if (S == 1) {
-            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 3.;
-            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 3.;
+            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
+            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
         } else if (S == 2) {
-            io.q_out.c[a][c] = qx + dq[a];       io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 3.;
-            io.p_out.c[a][c] = px + dp;          io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 3.;
+            io.q_out.c[a][c] = qx + dq[a];       io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
+            io.p_out.c[a][c] = px + dp;          io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
         } else {
-            io.q_acc.c[a][c] = io.q_acc.c[a][c] + dq[a] / 6.;
-            io.p_acc.c[a][c] = io.p_acc.c[a][c] + dp / 6.;
+            io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 6., kInv6);
+            io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 6., kInv6);
         }
     }
 }

@@ -87,17 +87,17 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
 
         double dxb[3], dxf[3], dyb[3], dyf[3], dzb[3], dzf[3];
         if (sxb) { dxb[0] = -dA * mzc; dxb[1] = 0.; dxb[2] = dA * mxc; }
-        else { dxb[0] = (mxc - io.m_in.c[0][cxb]) / P.dx; dxb[1] = (myc - io.m_in.c[1][cxb]) / P.dx; dxb[2] = (mzc - io.m_in.c[2][cxb]) / P.dx; }
+        else { dxb[0] = qdiv((mxc - io.m_in.c[0][cxb]), P.dx, P.rdx); dxb[1] = qdiv((myc - io.m_in.c[1][cxb]), P.dx, P.rdx); dxb[2] = qdiv((mzc - io.m_in.c[2][cxb]), P.dx, P.rdx); }
         if (sxf) { dxf[0] = -dA * mzc; dxf[1] = 0.; dxf[2] = dA * mxc; }
-        else { dxf[0] = (io.m_in.c[0][cxf] - mxc) / P.dx; dxf[1] = (io.m_in.c[1][cxf] - myc) / P.dx; dxf[2] = (io.m_in.c[2][cxf] - mzc) / P.dx; }
+        else { dxf[0] = qdiv((io.m_in.c[0][cxf] - mxc), P.dx, P.rdx); dxf[1] = qdiv((io.m_in.c[1][cxf] - myc), P.dx, P.rdx); dxf[2] = qdiv((io.m_in.c[2][cxf] - mzc), P.dx, P.rdx); }
         if (syb) { dyb[0] = 0.; dyb[1] = -dA * mzc; dyb[2] = dA * myc; }
-        else { dyb[0] = (mxc - io.m_in.c[0][cyb]) / P.dy; dyb[1] = (myc - io.m_in.c[1][cyb]) / P.dy; dyb[2] = (mzc - io.m_in.c[2][cyb]) / P.dy; }
+        else { dyb[0] = qdiv((mxc - io.m_in.c[0][cyb]), P.dy, P.rdy); dyb[1] = qdiv((myc - io.m_in.c[1][cyb]), P.dy, P.rdy); dyb[2] = qdiv((mzc - io.m_in.c[2][cyb]), P.dy, P.rdy); }
         if (syf) { dyf[0] = 0.; dyf[1] = -dA * mzc; dyf[2] = dA * myc; }
-        else { dyf[0] = (io.m_in.c[0][cyf] - mxc) / P.dy; dyf[1] = (io.m_in.c[1][cyf] - myc) / P.dy; dyf[2] = (io.m_in.c[2][cyf] - mzc) / P.dy; }
+        else { dyf[0] = qdiv((io.m_in.c[0][cyf] - mxc), P.dy, P.rdy); dyf[1] = qdiv((io.m_in.c[1][cyf] - myc), P.dy, P.rdy); dyf[2] = qdiv((io.m_in.c[2][cyf] - mzc), P.dy, P.rdy); }
         if (szb) { dzb[0] = 0.; dzb[1] = 0.; dzb[2] = 0.; }
-        else { dzb[0] = (mxc - io.m_in.c[0][czb]) / P.dz; dzb[1] = (myc - io.m_in.c[1][czb]) / P.dz; dzb[2] = (mzc - io.m_in.c[2][czb]) / P.dz; }
+        else { dzb[0] = qdiv((mxc - io.m_in.c[0][czb]), P.dz, P.rdz); dzb[1] = qdiv((myc - io.m_in.c[1][czb]), P.dz, P.rdz); dzb[2] = qdiv((mzc - io.m_in.c[2][czb]), P.dz, P.rdz); }
         if (szf) { dzf[0] = 0.; dzf[1] = 0.; dzf[2] = 0.; }
-        else { dzf[0] = (io.m_in.c[0][czf] - mxc) / P.dz; dzf[1] = (io.m_in.c[1][czf] - myc) / P.dz; dzf[2] = (io.m_in.c[2][czf] - mzc) / P.dz; }
+        else { dzf[0] = qdiv((io.m_in.c[0][czf] - mxc), P.dz, P.rdz); dzf[1] = qdiv((io.m_in.c[1][czf] - myc), P.dz, P.rdz); dzf[2] = qdiv((io.m_in.c[2][czf] - mzc), P.dz, P.rdz); }
 
         const double dmxdx = (dxb[0] + dxf[0]) * 0.5;
         const double dmzdx = (dxb[2] + dxf[2]) * 0.5;
@@ -114,9 +114,9 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
 
         double Hex[3];
         for (int a = 0; a < 3; a++) {
-            const double d2xf = dxf[a] / P.dx, d2xb = -dxb[a] / P.dx;
-            const double d2yf = dyf[a] / P.dy, d2yb = -dyb[a] / P.dy;
-            const double d2zf = dzf[a] / P.dz, d2zb = -dzb[a] / P.dz;
+            const double d2xf = qdiv(dxf[a], P.dx, P.rdx), d2xb = -qdiv(dxb[a], P.dx, P.rdx);
+            const double d2yf = qdiv(dyf[a], P.dy, P.rdy), d2yb = -qdiv(dyb[a], P.dy, P.rdy);
+            const double d2zf = qdiv(dzf[a], P.dz, P.rdz), d2zb = -qdiv(dzb[a], P.dz, P.rdz);
             Hex[a] = mat.ex_coef * (Axf * d2xf + Axb * d2xb + Ayf * d2yf + Ayb * d2yb + Azf * d2zf + Azb * d2zb);
         }
 
@@ -179,10 +179,10 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
     const double d[3] = {dmx, dmy, dmz};
     for (int a = 0; a < 3; a++) {
         const double xv = io.m_x.c[a][c];
-        if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = d[a] / 6.; }
-        else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = io.m_acc.c[a][c] + d[a] / 3.; }
-        else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = io.m_acc.c[a][c] + d[a] / 3.; }
-        else { io.m_acc.c[a][c] = xv + (io.m_acc.c[a][c] + d[a] / 6.); }
+        if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
+        else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
+        else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
+        else { io.m_acc.c[a][c] = xv + (io.m_acc.c[a][c] + qdiv(d[a], 6., kInv6)); }
     }
 }
 

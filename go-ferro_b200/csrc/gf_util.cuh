@@ -19,6 +19,38 @@ __global__ void k_sum_stride(const double* __restrict__ in, long n, double* __re
     partial[t] = acc;
 }
 
+// numerators for gf_check_quotients: odd i draws a random double with
+// exponent in about 2^-100..2^100; even i a value whose quotient by d lies
+// within rounding noise of a midpoint between two doubles.  Counts the
+// quotients where qdiv and IEEE division differ in any bit.
+__device__ inline unsigned long long mix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__global__ void k_check_quotients(double d, double rd, unsigned long long n, unsigned long long seed,
+                                  unsigned long long* bad) {
+    const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
+    unsigned long long local = 0;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += T) {
+        const unsigned long long z = mix64(seed ^ mix64(i));
+        const int e = (int)((z >> 52) % 201ull) - 100;
+        const double mant = 1. + (double)(z & ((1ull << 52) - 1)) * 0x1p-52;
+        double x = ldexp(mant, e);
+        if (i & 1ull) {
+            if (z >> 63) x = -x;
+        } else {
+            // t = mant + half an ulp of mant, scaled: x = RN(d * t)
+            const double t = ldexp(mant, e), half_ulp = ldexp(0x1p-53, e);
+            x = __fma_rn(d, t, __dmul_rn(d, half_ulp));
+        }
+        const double a = qdiv(x, d, rd), b = x / d;
+        if (__double_as_longlong(a) != __double_as_longlong(b)) local++;
+    }
+    if (local) atomicAdd(bad, local);
+}
+
 // x[0] := x[0] / d  (single thread; the mean of gf_field_mean_noalloc)
 __global__ void k_scale(double* x, double d) { x[0] = x[0] / d; }
 

@@ -194,6 +194,16 @@ void gf_destroy(gf_engine* e);
  * Errors are reported through gf_last_error(NULL). */
 int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, double* dev_out, void* stream);
 
+/* Diagnostic: the stencil kernels divide by run constants (cell sizes, dt,
+ * the RK4 weights 3 and 6) with a reciprocal-and-correction sequence
+ * instead of the general division.  This queues, on the current device,
+ * n quotients x / d for pseudo-random x of magnitude 1e-30..1e30 (half of
+ * them close to rounding midpoints) with seed `seed`, computes each both
+ * ways and stores in *mismatches how many differ in any bit.  No
+ * counterpart in the reference; the reference divides with IEEE division,
+ * so 0 mismatches means the kernels' quotients equal the reference's. */
+int gf_check_quotients(double d, uint64_t n, uint64_t seed, uint64_t* mismatches);
+
 /* Library version string. */
 const char* gf_version(void);
 
