@@ -562,7 +562,7 @@ int setup_elastic_tile(gf_engine* eng) {
     GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false>, etile::NT, eng->el_smem));
     GF_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, eng->device));
     if (per_sm < 1) { eng->err = "elastic tile does not fit on an SM"; return GF_ECUDA; }
-    const long slots = (long)per_sm * sms;
+    const long slots = (long)per_sm * (sms > 0 ? sms : 1);
     const long tiles = (long)((P.nz + etile::TK - 1) / etile::TK) * ((P.ny + etile::TJ - 1) / etile::TJ);
     long best_cost = -1;
     for (long c = 1; c <= P.nx; c++) {
