@@ -333,19 +333,37 @@ struct ETileSmem {
     __device__ ElMat* mat() const { return reinterpret_cast<ElMat*>(base + etile::kMatOffset); }
 };
 
-// stage u and material ids of plane pw into ring slot `slot`
-__device__ inline void etile_stage(const Params& P, const StageIO& io, const ETileSmem& sm, int slot, int pw) {
+// Staging of plane pw into ring slot `slot`: the u copies go out as cp.async
+// (no register or stall while they fly), the ids are loaded into registers
+// and stored by etile_stage_finish, which also waits for the copies.
+constexpr int kStageItems = (etile::UR * etile::UC + etile::NT - 1) / etile::NT;
+__device__ inline void etile_stage_issue(const Params& P, const StageIO& io, const ETileSmem& sm, int slot, int pw,
+                                         uint8_t idp[kStageItems]) {
     using namespace etile;
     const int po = pw * P.ny * P.nz;
     double* su = sm.u(slot);
-    uint8_t* sid = sm.id(slot);
-    for (int it = threadIdx.x; it < UR * UC; it += blockDim.x) {
-        const int ur = it / UC, uc = it - (it / UC) * UC;
-        const int c = po + sm.rowoff()[ur] + sm.colk()[uc];
-        sid[it] = io.mid[c];
 #pragma unroll
-        for (int a = 0; a < 3; a++) su[a * UR * UC + it] = io.u_in.c[a][c];
+    for (int t = 0; t < kStageItems; t++) {
+        const int it = threadIdx.x + t * NT;
+        if (it < UR * UC) {
+            const int ur = it / UC, uc = it - (it / UC) * UC;
+            const int c = po + sm.rowoff()[ur] + sm.colk()[uc];
+            idp[t] = io.mid[c];
+#pragma unroll
+            for (int a = 0; a < 3; a++) cp_async8(&su[a * UR * UC + it], &io.u_in.c[a][c]);
+        }
     }
+    cp_async_commit();
+}
+__device__ inline void etile_stage_finish(const ETileSmem& sm, int slot, const uint8_t idp[kStageItems]) {
+    using namespace etile;
+    uint8_t* sid = sm.id(slot);
+#pragma unroll
+    for (int t = 0; t < kStageItems; t++) {
+        const int it = threadIdx.x + t * NT;
+        if (it < UR * UC) sid[it] = idp[t];
+    }
+    cp_async_wait_all();
 }
 
 template <int S, bool CUB>
@@ -388,9 +406,15 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         sm.colk()[it] = kk < 0 ? kk + P.nz : kk % P.nz;
     }
     __syncthreads();
-    etile_stage(P, io, sm, 0, wrapm(i0 - 1, P.nx));
-    etile_stage(P, io, sm, 1, wrapm(i0, P.nx));
+    {
+        uint8_t id0[kStageItems], id1[kStageItems];
+        etile_stage_issue(P, io, sm, 0, wrapm(i0 - 1, P.nx), id0);
+        etile_stage_issue(P, io, sm, 1, wrapm(i0, P.nx), id1);
+        etile_stage_finish(sm, 0, id0);
+        etile_stage_finish(sm, 1, id1);
+    }
     __syncthreads();
+    uint8_t idp[kStageItems];          // ids of the plane being staged
 
     double sa[3] = {0., 0., 0.};       // lower cell's half of the next x-face stress
     double sxp[3] = {0., 0., 0.};      // stress on the previous x-face
@@ -449,8 +473,11 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         __syncthreads();
 
         // ---- B1: y- and z-face stresses of the interior plane p; stage plane p+2 ----
+        const bool stage_next = q + 1 <= L;
+        if (stage_next) etile_stage_issue(P, io, sm, cur, wrapm(p + 2, P.nx), idp);
         if (q >= 1 && q <= L) {
-            for (int it = tid; it < FYR * TK; it += blockDim.x) {
+            for (int it = tid; it < FYR * TK + TJ * FZC; it += blockDim.x) {
+              if (it < FYR * TK) {
                 const int fr_ = it / TK, fc = it - (it / TK) * TK;       // face j0+fr_, column k0+fc
                 const int f = j0 + fr_;
                 const uint8_t ia = sm.idc()[fr_ * HK + fc + 1], ib = sm.idc()[(fr_ + 1) * HK + fc + 1];
@@ -468,9 +495,9 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                 }
 #pragma unroll
                 for (int a = 0; a < 3; a++) sm.fy()[a * FYR * TK + it] = o[a];
-            }
-            for (int it = tid; it < TJ * FZC; it += blockDim.x) {
-                const int rl = it / FZC, fc = it - (it / FZC) * FZC;      // row j0+rl, face k0+fc
+              } else {
+                const int iz = it - FYR * TK;
+                const int rl = iz / FZC, fc = iz - (iz / FZC) * FZC;      // row j0+rl, face k0+fc
                 const int f = k0 + fc;
                 const int rr = rl + 1;
                 const uint8_t ia = sm.idc()[rr * HK + fc], ib = sm.idc()[rr * HK + fc + 1];
@@ -487,10 +514,10 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
                 }
 #pragma unroll
-                for (int a = 0; a < 3; a++) sm.fz()[a * TJ * FZC + it] = o[a];
+                for (int a = 0; a < 3; a++) sm.fz()[a * TJ * FZC + iz] = o[a];
+              }
             }
         }
-        if (q + 1 <= L) etile_stage(P, io, sm, cur, wrapm(p + 2, P.nx));
         __syncthreads();
 
         // ---- B2: one column per thread ----
@@ -602,6 +629,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             }
             mid_prev = id;
         }
+        if (stage_next) etile_stage_finish(sm, cur, idp);
         __syncthreads();
     }
 }

@@ -17,6 +17,16 @@ inline cudaError_t launch(Kernel k, dim3 grid, dim3 block, size_t smem, cudaStre
     return cudaGetLastError();
 }
 
+// Asynchronous 8-byte global -> shared copy (cp.async, sm_80 and later).
+// The data is visible to the issuing thread after cp_async_wait_all() and
+// to the block after a barrier that follows it.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Dynamic shared memory of a block-cooperative kernel.
 #define GF_EXTERN_SMEM(T, name) extern __shared__ T name[]
 
