@@ -59,11 +59,17 @@ def alg_bytes_per_unit(kernel: str, info, mfe_frac: float = 0.0) -> float:
     mfe_frac: fraction of cells that are ferromagnetic or ferroelectric."""
     D = 8.0
     if kernel == "k_elastic":
-        # u_in, v_in, v_x, u_x, force_store (read), m and p for the eigenstrain,
-        # v/u accumulators; writes: v/u stage outputs and accumulators,
-        # force_store at stage 1, crystal-frame strain of magnetic/ferroelectric cells
-        reads = 3 + 3 + 3 + 3 * 0.75 + 3 + 3 * info.fm + 3 * info.fe + 6 * 0.75
-        writes = 6 * 0.75 + 6 + 3 * 0.25 + 6 * mfe_frac
+        # tiled stress-divergence kernel: u_in, m and p for the eigenstrain,
+        # material ids; writes the divergence and the crystal-frame strain of
+        # magnetic/ferroelectric cells
+        reads = 3 + 3 * info.fm + 3 * info.fe
+        writes = 3 + 6 * mfe_frac
+        return (reads + writes) * D + 1
+    if kernel == "k_elastic_rk":
+        # divergence, force_store, v_x, v_in, u_x (stages 1-3), v/u accumulators
+        # (stages 2-4); writes v/u stage outputs, accumulators, force_store (stage 1)
+        reads = 3 + 3 + 3 + 3 + 3 * 0.75 + 6 * 0.75
+        writes = 6 * 0.75 + 6 + 3 * 0.25
         return (reads + writes) * D + 1
     if kernel == "k_llg_fm":
         reads = 3 + 3 + 3 * 0.75 + 3 + 6 * info.elastic + 3 * info.em

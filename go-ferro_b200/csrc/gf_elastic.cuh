@@ -536,25 +536,14 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 #pragma unroll
                     for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / 2.;
                 }
-                if (q >= 2) {
-                    // cell (p-1, j, k) is complete
+                if (q >= 2 && mid_prev != 0) {
+                    // cell (p-1, j, k) is complete: its stress divergence
                     const long c = (long)(p - 1) * nyz + (long)j * P.nz + k;
-                    double dv[3] = {0., 0., 0.};
-                    if (mid_prev != 0) {
-                        const ElMat& mt = sm.mat()[mid_prev - 1];
 #pragma unroll
-                        for (int a = 0; a < 3; a++) {
-                            const double tx = qdiv((sx[a] - sxp[a]), P.dx, P.rdx);
-                            const double f = tx + ty[a] + tz[a];
-                            const double fs = io.force_store.c[a][c];
-                            if (S == 1 || S == 2)
-                                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs) * 2.;
-                            else
-                                dv[a] = f * mt.dens_dt + mt.mass_damp * io.v_x.c[a][c] + mt.stiff_damp * (f - fs);
-                            if (S == 0) io.force_store.c[a][c] = f;
-                        }
+                    for (int a = 0; a < 3; a++) {
+                        const double tx = qdiv((sx[a] - sxp[a]), P.dx, P.rdx);
+                        io.force.c[a][c] = tx + ty[a] + tz[a];
                     }
-                    rk_vu<S>(io, c, dv, P.dt);
                 }
 #pragma unroll
                 for (int a = 0; a < 3; a++) sxp[a] = sx[a];
@@ -632,6 +621,35 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         if (stage_next) etile_stage_finish(sm, cur, idp);
         __syncthreads();
     }
+}
+
+// Per cell after k_elastic_tile: velocity increment from the stress
+// divergence f with mass and stiffness damping (get_dv_RK*,
+// elastic_dynamic_solver.cpp:1295-1329: weights 1, 2, 2, 1 on f - f_store,
+// f_store := f in stage 1 only), then the RK4 combination of v and u.  A
+// streaming kernel at full occupancy, so these loads and stores overlap
+// across many warps instead of waiting inside the tiled kernel's phases.
+template <int S>
+__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIO io) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const uint8_t id = io.mid[c];
+    double dv[3] = {0., 0., 0.};
+    if (id != 0) {
+        const DevMat& mt = io.mats[id - 1];
+        const double dens_dt = mt.dens_dt, mass_damp = mt.mass_damp, stiff_damp = mt.stiff_damp;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const double f = io.force.c[a][c];
+            const double fs = io.force_store.c[a][c];
+            if (S == 1 || S == 2)
+                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs) * 2.;
+            else
+                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs);
+            if (S == 0) io.force_store.c[a][c] = f;
+        }
+    }
+    rk_vu<S>(io, c, dv, P.dt);
 }
 
 // cell strain (global frame) of the current step for output (Dexx_glb ...)

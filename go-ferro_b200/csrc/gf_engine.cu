@@ -73,6 +73,7 @@ struct gf_engine {
     Field3 m, p, q, u, v, E, H;
     double* dm[3] = {nullptr, nullptr, nullptr};
     double* force_store[3] = {nullptr, nullptr, nullptr};
+    double* force[3] = {nullptr, nullptr, nullptr};
     double* Hstat[3] = {nullptr, nullptr, nullptr};
     double* Estat[3] = {nullptr, nullptr, nullptr};
     double* Hnu[3] = {nullptr, nullptr, nullptr};
@@ -242,6 +243,9 @@ DevMat make_devmat(const Material& m, double dt) {
 // validation: what this engine implements
 // ---------------------------------------------------------------------------
 std::string unsupported(const Deck& d) {
+    // kernels index cells and Yee vertices with 32-bit integers
+    if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
+        return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
     if (d.any_afm) return "two-sublattice antiferromagnets (if_AFM) are not supported by this engine";
     if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
     if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this engine";
@@ -517,6 +521,7 @@ void build_io(gf_engine* eng) {
             if (eng->H.on) set_io_field(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out);
             io.dm = f3(eng->dm);
             io.force_store = f3(eng->force_store);
+            io.force = f3(eng->force);
             io.Hstat = f3(eng->Hstat);
             io.Estat = f3(eng->Estat);
             io.Hnu = f3(eng->Hnu);
@@ -589,6 +594,7 @@ int enqueue_stage(gf_engine* eng, int parity) {
         else
             GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
                                 eng->el_chunk, eng->el_nmat));
+        GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
@@ -866,6 +872,7 @@ int create(gf_engine* eng, const std::string& dir, int device) {
         if (P.em_fromM) GF_TRY(dalloc_n(eng, &eng->dm[a], (size_t)n));
         if (d.elastodynamics) {
             GF_TRY(dalloc_n(eng, &eng->force_store[a], (size_t)n));
+            GF_TRY(dalloc_n(eng, &eng->force[a], (size_t)n));
         }
         if (d.any_fm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
         if (d.any_fe) GF_TRY(dalloc_n(eng, &eng->Estat[a], (size_t)n));

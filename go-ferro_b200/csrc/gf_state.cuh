@@ -26,6 +26,7 @@ struct StageIO {
     // elastic displacement u and velocity v
     F3 u_in, u_x, u_acc, u_out, v_in, v_x, v_acc, v_out;
     F3 force_store;   // stage-1 stress divergence (stiffness damping)
+    F3 force;         // stress divergence of the stage, k_elastic_tile -> k_elastic_rk
     // Yee E and H: component c of E lives on the c-edges, of H on the c-faces
     F3 E_in, E_x, E_acc, E_out, H_in, H_x, H_acc, H_out;
     // static and external fields
