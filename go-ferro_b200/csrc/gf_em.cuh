@@ -26,8 +26,15 @@
 
 namespace gf {
 
+// per-material constants the Yee updates read, staged in shared memory
+struct EmMat {
+    double er, cond, Ms;
+    uint32_t flags;
+    int pad_;
+};
+
 // free current J_f of cell (i,j,k), component a, stage drive dr
-__device__ inline double jf_cell(const Params& P, const StageIO& io, const StageDrive& dr, int a, long i, long j, long k) {
+__device__ inline double jf_cell(const Params& P, const StageIO& io, const StageDrive& dr, int a, int i, int j, int k) {
     if (!P.jf_on || a != P.jf_comp) return 0.;
     if (i < P.jf_i0 || i > P.jf_i1 || j < P.jf_j0 || j > P.jf_j1 || k < P.jf_k0 || k > P.jf_k1) return 0.;
     if (P.jf_type == 1 || P.jf_type == 2) return dr.jf * io.jf_kfac[k];
@@ -35,7 +42,7 @@ __device__ inline double jf_cell(const Params& P, const StageIO& io, const Stage
 }
 
 template <int S>
-__device__ inline void rk_x(double xv, double d, double* out, double* acc, long e) {
+__device__ inline void rk_x(double xv, double d, double* out, double* acc, int e) {
     if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
     else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
     else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
@@ -44,34 +51,35 @@ __device__ inline void rk_x(double xv, double d, double* out, double* acc, long 
 
 // E edge update of component C at edge (i,j,k) (index e in C's array).
 template <int S, int C>
-__device__ inline void em_E_edge(const Params& P, const StageIO& io, const StageDrive& dr, long i, long j, long k, long e) {
-    const long nx = P.nx, ny = P.ny, nz = P.nz;
+__device__ inline void em_E_edge(const Params& P, const StageIO& io, const StageDrive& dr, const EmMat* mt,
+                                 int i, int j, int k, int e) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
 
     double d = 0.;
     bool boundary = false;
-    long cx[4], cy[4], cz[4];
+    int cx[4], cy[4], cz[4];
     // cell quadruples around the edge, in the reference's order 1..4
     if (C == 0) {
         if ((j == 0 || j == ny) && !P.per_y) boundary = true;
         if ((k == 0 || k == nz) && !P.per_z) boundary = true;
-        const long y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y3 = (j == 0 || j == ny) ? 0 : j;
-        const long z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y3 = (j == 0 || j == ny) ? 0 : j;
+        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
         cx[0] = cx[1] = cx[2] = cx[3] = i;
         cy[0] = y1; cy[1] = y1; cy[2] = y3; cy[3] = y3;
         cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
     } else if (C == 1) {
         if ((i == 0 || i == nx) && !P.per_x) boundary = true;
         if ((k == 0 || k == nz) && !P.per_z) boundary = true;
-        const long x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
-        const long z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
         cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
         cy[0] = cy[1] = cy[2] = cy[3] = j;
         cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
     } else {
         if ((i == 0 || i == nx) && !P.per_x) boundary = true;
         if ((j == 0 || j == ny) && !P.per_y) boundary = true;
-        const long x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
-        const long y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y2 = (j == 0 || j == ny) ? 0 : j;
+        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y2 = (j == 0 || j == ny) ? 0 : j;
         cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
         cy[0] = y1; cy[1] = y2; cy[2] = y1; cy[3] = y2;
         cz[0] = cz[1] = cz[2] = cz[3] = k;
@@ -97,17 +105,18 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
             curl = dHydx - dHxdy;
         }
         double Jf = 0., dP = 0., er = 0., cond = 0., pc = 0.;
+#pragma unroll
         for (int q = 0; q < 4; q++) {
-            const long cc = cid(P, cx[q], cy[q], cz[q]);
+            const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
             const uint8_t id = io.mid[cc];
             if (id == 0) {
                 er = er + 1.;
             } else {
-                const DevMat& mt = io.mats[id - 1];
+                const EmMat& m = mt[id - 1];
                 if (P.em_fromP) dP = dP + io.q_in.c[C][cc] * P.dt;
-                if (mt.flags & MF_FE) pc = pc + 1.;
-                er = er + mt.er;
-                cond = cond + mt.cond;
+                if (m.flags & MF_FE) pc = pc + 1.;
+                er = er + m.er;
+                cond = cond + m.cond;
             }
             if (P.jf_on) Jf = Jf + jf_cell(P, io, dr, C, cx[q], cy[q], cz[q]);
         }
@@ -125,13 +134,13 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
 
 // H face update of component C at face (i,j,k) (index e in C's array).
 template <int S, int C>
-__device__ inline void em_H_face(const Params& P, const StageIO& io, long i, long j, long k, long e) {
-    const long nx = P.nx, ny = P.ny, nz = P.nz;
+__device__ inline void em_H_face(const Params& P, const StageIO& io, const EmMat* mt, int i, int j, int k, int e) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
     const double* Ex = io.E_in.c[0];
     const double* Ey = io.E_in.c[1];
     const double* Ez = io.E_in.c[2];
     double curl;
-    long a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
+    int a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
     if (C == 0) {
         const double dEzdy = qdiv((Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dy, P.rdy);
         const double dEydz = qdiv((Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]), P.dz, P.rdz);
@@ -153,17 +162,17 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, long i, lon
     }
     double dM1 = 0., dM2 = 0., cnt = 0.;
     {
-        const long c1 = cid(P, a1x, a1y, a1z), c2 = cid(P, a2x, a2y, a2z);
+        const int c1 = (a1x * ny + a1y) * nz + a1z, c2 = (a2x * ny + a2y) * nz + a2z;
         const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
         if (i1 != 0) {
-            const DevMat& mt = io.mats[i1 - 1];
-            if (P.em_fromM) dM1 = io.dm.c[C][c1] * mt.Ms;
-            if (mt.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+            const EmMat& m = mt[i1 - 1];
+            if (P.em_fromM) dM1 = io.dm.c[C][c1] * m.Ms;
+            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
         }
         if (i2 != 0) {
-            const DevMat& mt = io.mats[i2 - 1];
-            if (P.em_fromM) dM2 = io.dm.c[C][c2] * mt.Ms;
-            if (mt.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+            const EmMat& m = mt[i2 - 1];
+            if (P.em_fromM) dM2 = io.dm.c[C][c2] * m.Ms;
+            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
         }
     }
     if (cnt < 0.5) cnt = 1.;
@@ -176,21 +185,29 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, long i, lon
 // All six Yee components of one stage: thread (i,j,k) on the vertex grid
 // (nx+1)(ny+1)(nz+1) updates every E edge and H face with index (i,j,k)
 // inside that component's staggered extent.  E reads only the stage H and
-// H only the stage E and dm, so the six updates are independent.
+// H only the stage E and dm, so the six updates are independent.  The grid
+// is (blocks over the (j,k) vertex plane) x (nx+1 planes); the material
+// constants are staged in shared memory.
 template <int S>
-__global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io) {
-    const long nx = P.nx, ny = P.ny, nz = P.nz;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long vyz = (ny + 1) * (nz + 1);
-    if (t >= (nx + 1) * vyz) return;
-    const long i = t / vyz, j = (t - i * vyz) / (nz + 1), k = t - i * vyz - j * (nz + 1);
+__global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io, int nmat) {
+    __shared__ EmMat mt[kMaxMat];
+    for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
+        const DevMat& d = io.mats[q];
+        mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].flags = d.flags;
+    }
+    __syncthreads();
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (ny + 1) * (nz + 1)) return;
+    const int i = blockIdx.y;
+    const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
     const StageDrive& dr = stage_drive(io, S);
-    if (i < nx) em_E_edge<S, 0>(P, io, dr, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
-    if (j < ny) em_E_edge<S, 1>(P, io, dr, i, j, k, (i * ny + j) * (nz + 1) + k);
-    if (k < nz) em_E_edge<S, 2>(P, io, dr, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (j < ny && k < nz) em_H_face<S, 0>(P, io, i, j, k, (i * ny + j) * nz + k);
-    if (i < nx && k < nz) em_H_face<S, 1>(P, io, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (i < nx && j < ny) em_H_face<S, 2>(P, io, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (i < nx) em_E_edge<S, 0>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
+    if (j < ny) em_E_edge<S, 1>(P, io, dr, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (k < nz) em_E_edge<S, 2>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (j < ny && k < nz) em_H_face<S, 0>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
+    if (i < nx && k < nz) em_H_face<S, 1>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (i < nx && j < ny) em_H_face<S, 2>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
 }
 
 // hard plane-wave source: E on z = plane_z, all three components, i<nx, j<ny

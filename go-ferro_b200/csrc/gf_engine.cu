@@ -597,11 +597,13 @@ int enqueue_stage(gf_engine* eng, int parity) {
         GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
-    if (P.fm) GF_CU(klaunch(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bi * P.fm_bj * P.fm_bk, kThreads)), dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab));
+    if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
+                                  dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
     if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
-        GF_CU(klaunch(eng, "k_em_fused", k_em_fused<S>, dim3(blocks_for((nx + 1) * (ny + 1) * (nz + 1), kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                      dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size()));
         if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));

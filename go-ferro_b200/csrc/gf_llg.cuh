@@ -40,22 +40,44 @@ __device__ inline void cell_strain_total(const Params& P, const StageIO& io, lon
     }
 }
 
+// per-material LLG constants, staged in shared memory
+struct LLGMat {
+    double Aex, dA, ex_coef, dmi_coef, K1c, K2c, B1c, B2c, precess, alpha_precess;
+    int aniso;
+    uint32_t fm;
+};
+
 // One thread per cell of the ferromagnetic bounding box; cells outside it
-// hold their initial m in all four buffers and are never touched.
+// hold their initial m in all four buffers and are never touched.  Grid:
+// (blocks over the box's (j,k) plane) x (box planes in i).
 template <int S>
-__global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGTables* __restrict__ tab) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long bjk = P.fm_bj * P.fm_bk;
-    if (t >= P.fm_bi * bjk) return;
-    const long bi = t / bjk, r = t - bi * bjk, bj = r / P.fm_bk;
-    const long i = P.fm_i0 + bi, j = P.fm_j0 + bj, k = P.fm_k0 + (r - bj * P.fm_bk);
-    const long c = cid(P, i, j, k);
+__global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGTables* __restrict__ tab, int nmat) {
+    __shared__ LLGMat mt[kMaxMat];
+    __shared__ double sA[kMaxMat + 1][kMaxMat + 1];
+    for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
+        const DevMat& d = io.mats[q];
+        mt[q] = LLGMat{d.Aex, d.dA, d.ex_coef, d.dmi_coef, d.K1c, d.K2c, d.B1c, d.B2c, d.precess, d.alpha_precess,
+                       d.aniso, (d.flags & MF_FM) ? 1u : 0u};
+    }
+    for (int q = threadIdx.x; q < (nmat + 1) * (nmat + 1); q += blockDim.x) {
+        const int a = q / (nmat + 1), b = q - (q / (nmat + 1)) * (nmat + 1);
+        sA[a][b] = tab->Aij[a][b];
+    }
+    __syncthreads();
+    const int bjk = (int)(P.fm_bj * P.fm_bk);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bjk) return;
+    const int bj = t / (int)P.fm_bk;
+    const int i = (int)P.fm_i0 + blockIdx.y, j = (int)P.fm_j0 + bj, k = (int)P.fm_k0 + (t - bj * (int)P.fm_bk);
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int c = (i * ny + j) * nz + k;
+    auto fm_at = [&](uint8_t q) { return q != 0 && mt[q - 1].fm != 0u; };
 
     const uint8_t id = io.mid[c];
     double dmx = 0., dmy = 0., dmz = 0.;
     const double mxc = io.m_in.c[0][c], myc = io.m_in.c[1][c], mzc = io.m_in.c[2][c];
-    if (is_fm(io.mats, id)) {
-        const DevMat& mat = io.mats[id - 1];
+    if (fm_at(id)) {
+        const LLGMat& mat = mt[id - 1];
         double mx, my, mz;
         glb2crt(P, mxc, myc, mzc, mx, my, mz);
 
@@ -70,20 +92,22 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
         const double A = mat.Aex;
         const double dA = mat.dA;   // D/2./A
         // neighbour ids and linear indices with periodic wrap at array ends
-        const long ib = (i == 0) ? P.nx - 1 : i - 1, iF = (i == P.nx - 1) ? 0 : i + 1;
-        const long jb = (j == 0) ? P.ny - 1 : j - 1, jF = (j == P.ny - 1) ? 0 : j + 1;
-        const long kb = (k == 0) ? P.nz - 1 : k - 1, kF = (k == P.nz - 1) ? 0 : k + 1;
-        const long cxb = cid(P, ib, j, k), cxf = cid(P, iF, j, k);
-        const long cyb = cid(P, i, jb, k), cyf = cid(P, i, jF, k);
-        const long czb = cid(P, i, j, kb), czf = cid(P, i, j, kF);
+        const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
+        const int jb = (j == 0) ? ny - 1 : j - 1, jF = (j == ny - 1) ? 0 : j + 1;
+        const int kb = (k == 0) ? nz - 1 : k - 1, kF = (k == nz - 1) ? 0 : k + 1;
+        const int cxb = (ib * ny + j) * nz + k, cxf = (iF * ny + j) * nz + k;
+        const int cyb = (i * ny + jb) * nz + k, cyf = (i * ny + jF) * nz + k;
+        const int czb = (i * ny + j) * nz + kb, czf = (i * ny + j) * nz + kF;
+        const uint8_t idxb = io.mid[cxb], idxf = io.mid[cxf], idyb = io.mid[cyb], idyf = io.mid[cyf];
+        const uint8_t idzb = io.mid[czb], idzf = io.mid[czf];
         // a face is an FM surface when the neighbour across it is not FM, or
         // it is a non-periodic system boundary
-        const bool sxb = (i == 0 && !P.per_x) || !is_fm(io.mats, io.mid[cxb]);
-        const bool sxf = (i == P.nx - 1 && !P.per_x) || !is_fm(io.mats, io.mid[cxf]);
-        const bool syb = (j == 0 && !P.per_y) || !is_fm(io.mats, io.mid[cyb]);
-        const bool syf = (j == P.ny - 1 && !P.per_y) || !is_fm(io.mats, io.mid[cyf]);
-        const bool szb = (k == 0 && !P.per_z) || !is_fm(io.mats, io.mid[czb]);
-        const bool szf = (k == P.nz - 1 && !P.per_z) || !is_fm(io.mats, io.mid[czf]);
+        const bool sxb = (i == 0 && !P.per_x) || !fm_at(idxb);
+        const bool sxf = (i == nx - 1 && !P.per_x) || !fm_at(idxf);
+        const bool syb = (j == 0 && !P.per_y) || !fm_at(idyb);
+        const bool syf = (j == ny - 1 && !P.per_y) || !fm_at(idyf);
+        const bool szb = (k == 0 && !P.per_z) || !fm_at(idzb);
+        const bool szf = (k == nz - 1 && !P.per_z) || !fm_at(idzf);
 
         double dxb[3], dxf[3], dyb[3], dyf[3], dzb[3], dzf[3];
         if (sxb) { dxb[0] = -dA * mzc; dxb[1] = 0.; dxb[2] = dA * mxc; }
@@ -105,12 +129,12 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
         const double dmzdy = (dyb[2] + dyf[2]) * 0.5;
 
         // exchange coefficients per face
-        const double Axf = sxf ? A : tab->Aij[id][io.mid[cxf]];
-        const double Axb = sxb ? A : tab->Aij[id][io.mid[cxb]];
-        const double Ayf = syf ? A : tab->Aij[id][io.mid[cyf]];
-        const double Ayb = syb ? A : tab->Aij[id][io.mid[cyb]];
-        const double Azf = szf ? A : tab->Aij[id][io.mid[czf]];
-        const double Azb = szb ? A : tab->Aij[id][io.mid[czb]];
+        const double Axf = sxf ? A : sA[id][idxf];
+        const double Axb = sxb ? A : sA[id][idxb];
+        const double Ayf = syf ? A : sA[id][idyf];
+        const double Ayb = syb ? A : sA[id][idyb];
+        const double Azf = szf ? A : sA[id][idzf];
+        const double Azb = szb ? A : sA[id][idzb];
 
         double Hex[3];
         for (int a = 0; a < 3; a++) {
@@ -153,9 +177,9 @@ __global__ void __launch_bounds__(256) k_llg_fm(Params P, StageIO io, const LLGT
 
         if (P.em_back_M) {
             // cell-centred Maxwell H of the stage state (EMdynamic_solver.cpp:3780-3810)
-            const long hx0 = (i * P.ny + j) * P.nz + k, hx1 = ((i + 1) * P.ny + j) * P.nz + k;
-            const long hy0 = (i * (P.ny + 1) + j) * P.nz + k, hy1 = (i * (P.ny + 1) + j + 1) * P.nz + k;
-            const long hz0 = (i * P.ny + j) * (P.nz + 1) + k, hz1 = hz0 + 1;
+            const int hx0 = (i * ny + j) * nz + k, hx1 = ((i + 1) * ny + j) * nz + k;
+            const int hy0 = (i * (ny + 1) + j) * nz + k, hy1 = (i * (ny + 1) + j + 1) * nz + k;
+            const int hz0 = (i * ny + j) * (nz + 1) + k, hz1 = hz0 + 1;
             Hx = Hx + (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / 2.;
             Hy = Hy + (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / 2.;
             Hz = Hz + (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / 2.;
