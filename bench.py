@@ -292,7 +292,7 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
         e2e_value = world * ncell * e2e_steps / e2e_s
-        h2d = 424     # one StepDrive row per step
+        h2d = 520     # one StepDrive row per step (time + 4 stage rows of 128 B)
         d2h = 8 * 12  # <m>, <u>, E and H at the probe cell
 
         # ---- per-kernel device time for the roofline ----

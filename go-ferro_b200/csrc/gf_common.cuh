@@ -34,8 +34,14 @@ struct DevMat {
     double ex_coef;                            // 2./mu0/Ms
     double dmi_coef;                           // 2.*D/mu0/Ms
     double alpha, precess, alpha_precess;      // precess = -gyro/(1+a^2)*dt
-    // AFM sublattices (magnetic_AFM_solver.cpp)
+    // AFM sublattices s = 0, 1 (magnetic_AFM_solver.cpp:106-112, 181-191)
     double Ms1, Ms2;
+    double aAex[2];                 // Aex_AFM
+    double aK1c[2], aB1c[2], aB2c[2];   // K1/mu0/Ms, B1/mu0/Ms, B2/mu0/Ms
+    double aJ[2];                   // -1*J_AFM/mu0/Ms
+    double aex[2];                  // 2./mu0/Ms
+    double aprec[2], aaprec[2];     // -gyro/(1+a^2)*dt and alpha times it
+    double au[3];                   // uniaxial axis (crystal frame, normalised)
     // elastic (elastic_dynamic_solver.cpp:1295-1297)
     double cij[6][6];
     double dens_dt, mass_damp, stiff_damp;
@@ -63,8 +69,10 @@ struct Params {
     double Tg2c[3][3], Tc2g[3][3];
     // active physics
     int fm, afm, fe, elastic, em;
-    // bounding box of the ferromagnetic cells (the LLG kernel covers only it)
+    // bounding boxes of the ferromagnetic and antiferromagnetic cells (the
+    // LLG kernels cover only them)
     long fm_i0, fm_j0, fm_k0, fm_bi, fm_bj, fm_bk;
+    long afm_i0, afm_j0, afm_k0, afm_bi, afm_bj, afm_bk;
     int elasto_on, elasto_back;   // if_elasto_on_pORm, if_elasto_backaction_from_pORm
     int em_fromM, em_fromP, em_back_M, em_back_P;
     int has_eig0, has_strain0, has_hext_nonunif;
@@ -92,7 +100,8 @@ struct Params {
 // ferroelectric_solver.cpp:2001-2029, elastic_dynamic_solver.cpp:1195-1223
 // and 3059-3284, EMdynamic_solver.cpp:3828-4316).  Index s = RK stage 0..3.
 struct StageDrive {
-    double Hext[3];
+    double Hext[3];        // external H seen by the ferromagnet
+    double Hext_afm[3];    // external H seen by the antiferromagnet (differs with a prescribed table)
     double Eext[3];
     double traction;       // surface traction on the source plane (type 3)
     double usrc;           // displacement written on the source plane after the update

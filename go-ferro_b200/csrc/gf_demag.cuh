@@ -154,21 +154,38 @@ __global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_neg, con
     Hk[2 * n21 + q] = make_cuDoubleComplex(hz.x / vol_neg, hz.y / vol_neg);
 }
 
-// mode 0: M = Ms m into the FFT input (magnetic cells only);
-// mode 1: demag factors H = Ms m N_i; mode 2: 1-D model Hz = -Ms mz
-__global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F3 m, int mode, double* M3,
+// mode 0: M into the FFT input, Ms m for ferromagnetic cells and
+//         Ms1 m1 + Ms2 m2 for antiferromagnetic cells, 0 elsewhere (the
+//         buffer holds the previous inverse transform, so every cell is set);
+// mode 1: demag factors H = M N_i; mode 2: 1-D model Hz = -Mz
+// (magnetostatic_solver.cpp:114-249)
+__global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F3 m, F3 a1, F3 a2, int mode, double* M3,
                              F3 Hs, double f0, double f1, double f2) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
-    if (id == 0 || !(mats[id - 1].flags & MF_FM)) return;
-    const double Ms = mats[id - 1].Ms;
-    if (mode == 0) {
-        M3[c] = Ms * m.c[0][c]; M3[P.n + c] = Ms * m.c[1][c]; M3[2 * P.n + c] = Ms * m.c[2][c];
-    } else if (mode == 1) {
-        Hs.c[0][c] = Ms * m.c[0][c] * f0; Hs.c[1][c] = Ms * m.c[1][c] * f1; Hs.c[2][c] = Ms * m.c[2][c] * f2;
-    } else {
-        Hs.c[0][c] = 0.; Hs.c[1][c] = 0.; Hs.c[2][c] = -Ms * m.c[2][c];
+    const uint32_t fl = id ? mats[id - 1].flags : 0u;
+    if (fl & MF_FM) {
+        const double Ms = mats[id - 1].Ms;
+        if (mode == 0) {
+            M3[c] = Ms * m.c[0][c]; M3[P.n + c] = Ms * m.c[1][c]; M3[2 * P.n + c] = Ms * m.c[2][c];
+        } else if (mode == 1) {
+            Hs.c[0][c] = Ms * m.c[0][c] * f0; Hs.c[1][c] = Ms * m.c[1][c] * f1; Hs.c[2][c] = Ms * m.c[2][c] * f2;
+        } else {
+            Hs.c[0][c] = 0.; Hs.c[1][c] = 0.; Hs.c[2][c] = -Ms * m.c[2][c];
+        }
+    } else if (fl & MF_AFM) {
+        const double Ms1 = mats[id - 1].Ms1, Ms2 = mats[id - 1].Ms2;
+        if (mode == 0) {
+            for (int a = 0; a < 3; a++) M3[a * P.n + c] = Ms1 * a1.c[a][c] + Ms2 * a2.c[a][c];
+        } else if (mode == 1) {
+            const double f[3] = {f0, f1, f2};
+            for (int a = 0; a < 3; a++) Hs.c[a][c] = (Ms1 * a1.c[a][c] + Ms2 * a2.c[a][c]) * f[a];
+        } else {
+            Hs.c[0][c] = 0.; Hs.c[1][c] = 0.; Hs.c[2][c] = -Ms1 * a1.c[2][c] - Ms2 * a2.c[2][c];
+        }
+    } else if (mode == 0) {
+        M3[c] = 0.; M3[P.n + c] = 0.; M3[2 * P.n + c] = 0.;
     }
 }
 

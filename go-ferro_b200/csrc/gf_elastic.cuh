@@ -87,9 +87,38 @@ struct GradView {
     }
 };
 
+// ε0 of the cell from the crystal-frame m and p (get_eigenstrain_dynamic,
+// elastic_dynamic_solver.cpp:38-61): magnetostriction of m, electrostriction
+// of p, then the two AFM sublattices with half weight, minus the static
+// eigenstrain e0.  The sublattice terms are added only when the run has
+// antiferromagnets; without them they are exact zeros in the reference.
+template <class M>
+__device__ inline void eigen_terms(const Params& P, const StageIO& io, long c, const M& mt, double mx, double my,
+                                   double mz, double px, double py, double pz, const double e0[6], double e[6]) {
+    const double third = 1. / 3.;
+    double t[6];
+    t[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
+    t[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
+    t[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
+    t[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz;
+    t[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz;
+    t[5] = mt.l111_15 * my * mx + mt.Q44 * py * px;
+    if (P.afm) {
+        double a1x, a1y, a1z, a2x, a2y, a2z;
+        glb2crt(P, io.a1_in.c[0][c], io.a1_in.c[1][c], io.a1_in.c[2][c], a1x, a1y, a1z);
+        glb2crt(P, io.a2_in.c[0][c], io.a2_in.c[1][c], io.a2_in.c[2][c], a2x, a2y, a2z);
+        t[0] = t[0] + mt.l100a1_075 * (a1x * a1x - third) + mt.l100a2_075 * (a2x * a2x - third);
+        t[1] = t[1] + mt.l100a1_075 * (a1y * a1y - third) + mt.l100a2_075 * (a2y * a2y - third);
+        t[2] = t[2] + mt.l100a1_075 * (a1z * a1z - third) + mt.l100a2_075 * (a2z * a2z - third);
+        t[3] = t[3] + mt.l111a1_075 * a1y * a1z + mt.l111a2_075 * a2y * a2z;
+        t[4] = t[4] + mt.l111a1_075 * a1x * a1z + mt.l111a2_075 * a2x * a2z;
+        t[5] = t[5] + mt.l111a1_075 * a1y * a1x + mt.l111a2_075 * a2y * a2x;
+    }
+    for (int a = 0; a < 6; a++) e[a] = t[a] - e0[a];
+}
+
 // dynamic eigenstrain of cell c in the crystal frame (Dexx0_crt ...,
-// get_eigenstrain_dynamic); the reference's two-sublattice terms are exact
-// zeros for decks without antiferromagnets, which the engine rejects at creation
+// get_eigenstrain_dynamic)
 __device__ inline void eigen_crt(const Params& P, const StageIO& io, long c, double e[6]) {
     const uint8_t id = io.mid[c];
     for (int a = 0; a < 6; a++) e[a] = 0.;
@@ -98,15 +127,9 @@ __device__ inline void eigen_crt(const Params& P, const StageIO& io, long c, dou
     double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
     if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
     if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
-    const double third = 1. / 3.;
     double e0[6] = {0., 0., 0., 0., 0., 0.};
     if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
-    e[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz)) - e0[0];
-    e[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz)) - e0[1];
-    e[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px)) - e0[2];
-    e[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz - e0[3];
-    e[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz - e0[4];
-    e[5] = mt.l111_15 * my * mx + mt.Q44 * py * px - e0[5];
+    eigen_terms(P, io, c, mt, mx, my, mz, px, py, pz, e0, e);
 }
 
 // eigenstrain in the global frame (Dexx0_glb ...)
@@ -143,6 +166,7 @@ struct ElMat {
     double cij[6][6];
     double dens_dt, mass_damp, stiff_damp;
     double l100_15, l111_15, Q11, Q12, Q44;
+    double l100a1_075, l100a2_075, l111a1_075, l111a2_075;
     uint32_t flags;
     int cubic_c;
 };
@@ -195,15 +219,9 @@ __device__ inline void eigen_glb_m(const Params& P, const StageIO& io, long c, c
     double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
     if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
     if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
-    const double third = 1. / 3.;
     double e0[6] = {0., 0., 0., 0., 0., 0.};
     if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
-    e[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz)) - e0[0];
-    e[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz)) - e0[1];
-    e[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px)) - e0[2];
-    e[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz - e0[3];
-    e[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz - e0[4];
-    e[5] = mt.l111_15 * my * mx + mt.Q44 * py * px - e0[5];
+    eigen_terms(P, io, c, mt, mx, my, mz, px, py, pz, e0, e);
     if (P.rot) {
         double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
         rot_tensor(P.Tc2g, s, o);
@@ -394,6 +412,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         for (int a = 0; a < 6; a++) for (int b = 0; b < 6; b++) e.cij[a][b] = d.cij[a][b];
         e.dens_dt = d.dens_dt; e.mass_damp = d.mass_damp; e.stiff_damp = d.stiff_damp;
         e.l100_15 = d.l100_15; e.l111_15 = d.l111_15; e.Q11 = d.Q11; e.Q12 = d.Q12; e.Q44 = d.Q44;
+        e.l100a1_075 = d.l100a1_075; e.l100a2_075 = d.l100a2_075; e.l111a1_075 = d.l111a1_075; e.l111a2_075 = d.l111a2_075;
         e.flags = d.flags; e.cubic_c = d.cubic_c;
     }
     for (int it = tid; it < UR; it += blockDim.x) {
@@ -588,7 +607,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 #pragma unroll
                     for (int a = 0; a < 3; a++) tz[a] = qdiv((s2[a] - s1[a]), P.dz, P.rdz);
                     // cell strain for the magnetic and ferroelectric kernels
-                    if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_FE))) {
+                    if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_AFM | MF_FE))) {
                         double e[6];
                         e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
                         e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;

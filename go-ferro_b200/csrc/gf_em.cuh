@@ -28,7 +28,7 @@ namespace gf {
 
 // per-material constants the Yee updates read, staged in shared memory
 struct EmMat {
-    double er, cond, Ms;
+    double er, cond, Ms, Ms1, Ms2;
     uint32_t flags;
     int pad_;
 };
@@ -164,14 +164,21 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, const EmMat
     {
         const int c1 = (a1x * ny + a1y) * nz + a1z, c2 = (a2x * ny + a2y) * nz + a2z;
         const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
+        // Ms dm + Ms1 dm1 + Ms2 dm2 of each face cell (EMdynamic_solver.cpp:2300-2306)
         if (i1 != 0) {
             const EmMat& m = mt[i1 - 1];
-            if (P.em_fromM) dM1 = io.dm.c[C][c1] * m.Ms;
+            if (P.em_fromM) {
+                dM1 = io.dm.c[C][c1] * m.Ms;
+                if (P.afm) dM1 = dM1 + io.da1.c[C][c1] * m.Ms1 + io.da2.c[C][c1] * m.Ms2;
+            }
             if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
         }
         if (i2 != 0) {
             const EmMat& m = mt[i2 - 1];
-            if (P.em_fromM) dM2 = io.dm.c[C][c2] * m.Ms;
+            if (P.em_fromM) {
+                dM2 = io.dm.c[C][c2] * m.Ms;
+                if (P.afm) dM2 = dM2 + io.da1.c[C][c2] * m.Ms1 + io.da2.c[C][c2] * m.Ms2;
+            }
             if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
         }
     }
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io, int nmat
     __shared__ EmMat mt[kMaxMat];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMat& d = io.mats[q];
-        mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].flags = d.flags;
+        mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].Ms1 = d.Ms1; mt[q].Ms2 = d.Ms2; mt[q].flags = d.flags;
     }
     __syncthreads();
     const int nx = P.nx, ny = P.ny, nz = P.nz;

@@ -70,8 +70,10 @@ struct gf_engine {
     unsigned long long* step_ctr = nullptr;
     double* jf_kfac = nullptr;
 
-    Field3 m, p, q, u, v, E, H;
+    Field3 m, a1, a2, p, q, u, v, E, H;
     double* dm[3] = {nullptr, nullptr, nullptr};
+    double* da1[3] = {nullptr, nullptr, nullptr};
+    double* da2[3] = {nullptr, nullptr, nullptr};
     double* force_store[3] = {nullptr, nullptr, nullptr};
     double* force[3] = {nullptr, nullptr, nullptr};
     double* Hstat[3] = {nullptr, nullptr, nullptr};
@@ -210,6 +212,22 @@ DevMat make_devmat(const Material& m, double dt) {
         d.alpha_precess = m.alpha * d.precess;
     }
     d.Ms1 = m.Ms1; d.Ms2 = m.Ms2;
+    if (m.afm) {
+        // magnetic_AFM_solver.cpp:106-112, 181-191 (per sublattice)
+        const double mu0 = kMu0;
+        const double Ms[2] = {m.Ms1, m.Ms2}, K1[2] = {m.K1_1, m.K1_2}, B1[2] = {m.B1_1, m.B1_2}, B2[2] = {m.B2_1, m.B2_2};
+        const double Aex[2] = {m.Aex1, m.Aex2}, gyro[2] = {m.gyro1, m.gyro2}, alpha[2] = {m.alpha1, m.alpha2};
+        for (int s = 0; s < 2; s++) {
+            d.aAex[s] = Aex[s];
+            d.aK1c[s] = K1[s] / mu0 / Ms[s];
+            d.aB1c[s] = B1[s] / mu0 / Ms[s]; d.aB2c[s] = B2[s] / mu0 / Ms[s];
+            d.aJ[s] = -1. * m.J_AFM / mu0 / Ms[s];
+            d.aex[s] = 2. / mu0 / Ms[s];
+            d.aprec[s] = -gyro[s] / (1. + alpha[s] * alpha[s]) * dt;
+            d.aaprec[s] = alpha[s] * d.aprec[s];
+        }
+        for (int a = 0; a < 3; a++) d.au[a] = m.uaxis[a];
+    }
     // elastic
     bool cubic = true;
     for (int a = 0; a < 6; a++)
@@ -246,7 +264,6 @@ std::string unsupported(const Deck& d) {
     // kernels index cells and Yee vertices with 32-bit integers
     if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
         return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
-    if (d.any_afm) return "two-sublattice antiferromagnets (if_AFM) are not supported by this engine";
     if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
     if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this engine";
     if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
@@ -259,6 +276,9 @@ std::string unsupported(const Deck& d) {
         const Material& m = d.mats[i];
         if (m.fm && m.aniso_type > 2) return "anisotropy_type must be 0, 1 or 2";
         if (m.fm && (m.Ms == 0. || m.Aex == 0.)) return "ferromagnetic material needs nonzero Ms and Aex";
+        if (m.afm && (m.Ms1 == 0. || m.Ms2 == 0. || m.Aex1 == 0. || m.Aex2 == 0.))
+            return "antiferromagnetic material needs nonzero Ms_AFM1/2 and Aex_AFM1/2";
+        if (m.fm && m.afm) return "a material cannot be both ferromagnetic and antiferromagnetic";
         if (m.fe && m.fe_mass == 0.) return "ferroelectric material needs nonzero FE_mass";
         if (d.em_dynamic) {
             for (int k = 0; k < 3; k++)
@@ -325,8 +345,22 @@ void build_params(gf_engine* eng) {
         P.fm_i0 = lo[0]; P.fm_j0 = lo[1]; P.fm_k0 = lo[2];
         P.fm_bi = hi[0] - lo[0] + 1; P.fm_bj = hi[1] - lo[1] + 1; P.fm_bk = hi[2] - lo[2] + 1;
     }
+    {
+        long lo[3] = {d.nx, d.ny, d.nz}, hi[3] = {-1, -1, -1};
+        for (long i = 0; i < d.nx; i++)
+            for (long j = 0; j < d.ny; j++)
+                for (long k = 0; k < d.nz; k++) {
+                    const uint8_t id = d.material_cell[(size_t)((i * d.ny + j) * d.nz + k)];
+                    if (!id || !d.mats[id - 1].afm) continue;
+                    const long x[3] = {i, j, k};
+                    for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], x[a]); hi[a] = std::max(hi[a], x[a]); }
+                }
+        if (hi[0] < 0) { lo[0] = lo[1] = lo[2] = 0; hi[0] = hi[1] = hi[2] = -1; }
+        P.afm_i0 = lo[0]; P.afm_j0 = lo[1]; P.afm_k0 = lo[2];
+        P.afm_bi = hi[0] - lo[0] + 1; P.afm_bj = hi[1] - lo[1] + 1; P.afm_bk = hi[2] - lo[2] + 1;
+    }
     P.elasto_on = d.elasto_on; P.elasto_back = d.elasto_back && d.elastodynamics;
-    P.em_fromM = d.em_fromM && d.em_dynamic && d.any_fm;
+    P.em_fromM = d.em_fromM && d.em_dynamic && (d.any_fm || d.any_afm);
     P.em_fromP = d.em_fromP && d.em_dynamic && d.any_fe;
     P.em_back_M = d.em_back_M && d.em_dynamic;
     P.em_back_P = d.em_back_P && d.em_dynamic;
@@ -410,12 +444,23 @@ void step_drive(gf_engine* eng, StepDrive& sd) {
     }
     // local times of the four stages
     const double lt_ext[4] = {t - dt, t - dt * 0.5, t - dt * 0.5, t};
+    // static + alternating H of each stage (update_external_Hfield*, magnetic_solver.cpp:1834-1861)
+    double Hf[4][3];
+    for (int s = 0; s < 4; s++)
+        for (int a = 0; a < 3; a++) Hf[s][a] = d.Hext_stat[a] + d.Hext_altr[a] * std::sin(2. * PI * d.H_altr_freq[a] * lt_ext[s]);
     for (int s = 0; s < 4; s++) {
         StageDrive& st = sd.st[s];
         std::memset(&st, 0, sizeof(st));
         for (int a = 0; a < 3; a++) {
-            st.Hext[a] = d.prescribe_H ? eng->Hext_cur[a]
-                                       : d.Hext_stat[a] + d.Hext_altr[a] * std::sin(2. * PI * d.H_altr_freq[a] * lt_ext[s]);
+            // With a prescribed table the ferromagnet keeps the shared Hext
+            // (magnetic_solver.cpp:35-40) while get_dm_AFM_RK* always
+            // recomputes it (magnetic_AFM_solver.cpp:63, 491, 919, 1347), so
+            // the ferromagnet's stages 2-4 see the value the antiferromagnet
+            // set one stage earlier.
+            st.Hext_afm[a] = Hf[s][a];
+            if (!d.prescribe_H) st.Hext[a] = Hf[s][a];
+            else if (d.any_afm && s > 0) st.Hext[a] = Hf[s - 1][a];
+            else st.Hext[a] = eng->Hext_cur[a];
             st.Eext[a] = d.prescribe_E ? eng->Eext_cur[a]
                                        : d.Eext_stat[a] + d.Eext_altr[a] * std::sin(2. * PI * d.E_altr_freq[a] * lt_ext[s]);
         }
@@ -513,6 +558,8 @@ void build_io(gf_engine* eng) {
             StageIO& io = eng->io[par][s];
             std::memset(&io, 0, sizeof(io));
             if (eng->m.on) set_io_field(eng->m, par, s, io.m_in, io.m_x, io.m_acc, io.m_out);
+            if (eng->a1.on) set_io_field(eng->a1, par, s, io.a1_in, io.a1_x, io.a1_acc, io.a1_out);
+            if (eng->a2.on) set_io_field(eng->a2, par, s, io.a2_in, io.a2_x, io.a2_acc, io.a2_out);
             if (eng->p.on) set_io_field(eng->p, par, s, io.p_in, io.p_x, io.p_acc, io.p_out);
             if (eng->q.on) set_io_field(eng->q, par, s, io.q_in, io.q_x, io.q_acc, io.q_out);
             if (eng->u.on) set_io_field(eng->u, par, s, io.u_in, io.u_x, io.u_acc, io.u_out);
@@ -520,6 +567,8 @@ void build_io(gf_engine* eng) {
             if (eng->E.on) set_io_field(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out);
             if (eng->H.on) set_io_field(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out);
             io.dm = f3(eng->dm);
+            io.da1 = f3(eng->da1);
+            io.da2 = f3(eng->da2);
             io.force_store = f3(eng->force_store);
             io.force = f3(eng->force);
             io.Hstat = f3(eng->Hstat);
@@ -599,6 +648,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
     }
     if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
                                   dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
+    if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
+                                   dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
     if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
@@ -614,7 +665,7 @@ int enqueue_stage(gf_engine* eng, int parity) {
         F3 mnew = io.m_out;
         if (eng->demag_mode == 0) {
             GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
-                         mnew, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+                         mnew, io.a1_out, io.a2_out, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
             GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
             const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
             const double vol_neg = -P.dx * P.dy * P.dz;
@@ -625,7 +676,7 @@ int enqueue_stage(gf_engine* eng, int parity) {
                 GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
         } else {
             GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
-                         mnew, eng->demag_mode, (double*)nullptr, f3(eng->Hstat),
+                         mnew, io.a1_out, io.a2_out, eng->demag_mode, (double*)nullptr, f3(eng->Hstat),
                          eng->deck.demag_fac[0], eng->deck.demag_fac[1], eng->deck.demag_fac[2]));
         }
     }
@@ -651,7 +702,7 @@ int static_field_now(gf_engine* eng) {
     cudaStream_t st = eng->stream;
     F3 mx = f3(eng->m.X);
     if (eng->demag_mode == 0) {
-        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, 0,
+        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, f3(eng->a1.X), f3(eng->a2.X), 0,
                      eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
         GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
         const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
@@ -661,7 +712,7 @@ int static_field_now(gf_engine* eng) {
         for (int a = 0; a < 3; a++)
             GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
     } else {
-        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx,
+        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, f3(eng->a1.X), f3(eng->a2.X),
                      eng->demag_mode, (double*)nullptr, f3(eng->Hstat), eng->deck.demag_fac[0], eng->deck.demag_fac[1],
                      eng->deck.demag_fac[2]));
     }
@@ -707,7 +758,7 @@ int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* sr
 // copy the current-step buffer of every state field into its other three
 // buffers, so cells a stage kernel does not cover stay consistent
 int replicate_state(gf_engine* eng) {
-    Field3* fs[] = {&eng->m, &eng->p, &eng->q, &eng->u, &eng->v, &eng->E, &eng->H};
+    Field3* fs[] = {&eng->m, &eng->a1, &eng->a2, &eng->p, &eng->q, &eng->u, &eng->v, &eng->E, &eng->H};
     for (Field3* f : fs) {
         if (!f->on) continue;
         double* const* c = (eng->steps_done & 1ull) ? f->A : f->X;
@@ -742,6 +793,29 @@ int initial_state(gf_engine* eng, const std::string& dir) {
             }
         }
         GF_TRY(upload_vec(eng, eng->m.X, buf, n));
+    }
+    if (eng->a1.on) {
+        std::vector<double> b6[6];
+        for (auto& b : b6) b.assign((size_t)n, 0.);
+        if (d.in_afm) {
+            // input_AFMm (inoutput.cpp:29-50): "i j k m1x m1y m1z m2x m2y m2z"
+            std::string e = read_restart(dir + "/m_AFM.in", d.nx, d.ny, d.nz, 6, b6);
+            if (!e.empty()) { eng->err = e; return GF_EIO; }
+        } else {
+            // initialize_magnetization_AFM (magnetic_initialize.cpp:1153-1174): m2 = -m1
+            const double theta = (d.theta_mag) / 180. * PI;
+            const double phi = (d.phi_mag) / 180 * PI;
+            const double mx = std::sin(theta) * std::cos(phi), my = std::sin(theta) * std::sin(phi), mz = std::cos(theta);
+            for (long c = 0; c < n; c++) {
+                uint8_t id = d.material_cell[(size_t)c];
+                if (id && d.mats[id - 1].afm) {
+                    b6[0][c] = mx; b6[1][c] = my; b6[2][c] = mz;
+                    b6[3][c] = -mx; b6[4][c] = -my; b6[5][c] = -mz;
+                }
+            }
+        }
+        GF_TRY(upload_vec(eng, eng->a1.X, b6, n));
+        GF_TRY(upload_vec(eng, eng->a2.X, b6 + 3, n));
     }
     if (eng->p.on) {
         for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
@@ -840,6 +914,10 @@ int create(gf_engine* eng, const std::string& dir, int device) {
             for (size_t b = 0; b < d.mats.size(); b++) {
                 const double A1 = d.mats[a].Aex, A2 = d.mats[b].Aex;
                 t.Aij[a + 1][b + 1] = (A1 + A2 != 0.) ? 2. * A1 * A2 / (A1 + A2) : 0.;
+                // magnetic_initialize.cpp:877-1071: 2 A1 A2 / (A1 + A2) per sublattice
+                const double B1[2] = {d.mats[a].Aex1, d.mats[a].Aex2}, B2[2] = {d.mats[b].Aex1, d.mats[b].Aex2};
+                for (int s = 0; s < 2; s++)
+                    t.AijA[s][a + 1][b + 1] = (B1[s] + B2[s] != 0.) ? 2. * B1[s] * B2[s] / (B1[s] + B2[s]) : 0.;
             }
         GF_TRY(dalloc_n(eng, &eng->llg_tab, 1));
         GF_CU(cudaMemcpy(eng->llg_tab, &t, sizeof(t), cudaMemcpyHostToDevice));
@@ -863,6 +941,7 @@ int create(gf_engine* eng, const std::string& dir, int device) {
 
     // state fields
     if (d.any_fm) GF_TRY(alloc_field(eng, eng->m, n, n, n));
+    if (d.any_afm) { GF_TRY(alloc_field(eng, eng->a1, n, n, n)); GF_TRY(alloc_field(eng, eng->a2, n, n, n)); }
     if (d.any_fe) { GF_TRY(alloc_field(eng, eng->p, n, n, n)); GF_TRY(alloc_field(eng, eng->q, n, n, n)); }
     if (d.elastodynamics) { GF_TRY(alloc_field(eng, eng->u, n, n, n)); GF_TRY(alloc_field(eng, eng->v, n, n, n)); }
     if (d.em_dynamic) {
@@ -872,17 +951,18 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     }
     for (int a = 0; a < 3; a++) {
         if (P.em_fromM) GF_TRY(dalloc_n(eng, &eng->dm[a], (size_t)n));
+        if (P.em_fromM && d.any_afm) { GF_TRY(dalloc_n(eng, &eng->da1[a], (size_t)n)); GF_TRY(dalloc_n(eng, &eng->da2[a], (size_t)n)); }
         if (d.elastodynamics) {
             GF_TRY(dalloc_n(eng, &eng->force_store[a], (size_t)n));
             GF_TRY(dalloc_n(eng, &eng->force[a], (size_t)n));
         }
-        if (d.any_fm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
+        if (d.any_fm || d.any_afm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
         if (d.any_fe) GF_TRY(dalloc_n(eng, &eng->Estat[a], (size_t)n));
         if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_n(eng, &eng->Hnu[a], (size_t)n));
     }
     if (d.elastodynamics)
         for (int a = 0; a < 9; a++) GF_TRY(dalloc_n(eng, &eng->fg[a], (size_t)n));
-    if (d.elastodynamics && P.elasto_on && (P.fm || P.fe))
+    if (d.elastodynamics && P.elasto_on && (P.fm || P.afm || P.fe))
         for (int a = 0; a < 6; a++) GF_TRY(dalloc_n(eng, &eng->strain_c[a], (size_t)n));
     if (d.elastodynamics) GF_TRY(setup_elastic_tile(eng));
     if (d.elastodynamics) {
@@ -974,6 +1054,8 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
     };
     switch (field) {
         case GF_FIELD_M: if (!eng->m.on) break; add3(cur(eng, eng->m), &eng->m); break;
+        case GF_FIELD_M_AFM1: if (!eng->a1.on) break; add3(cur(eng, eng->a1), &eng->a1); break;
+        case GF_FIELD_M_AFM2: if (!eng->a2.on) break; add3(cur(eng, eng->a2), &eng->a2); break;
         case GF_FIELD_P: if (!eng->p.on) break; add3(cur(eng, eng->p), &eng->p); break;
         case GF_FIELD_Q: if (!eng->q.on) break; add3(cur(eng, eng->q), &eng->q); break;
         case GF_FIELD_U: if (!eng->u.on) break; add3(cur(eng, eng->u), &eng->u); break;
@@ -1062,6 +1144,8 @@ int gf_average(gf_engine* e, int obs, double out3[3]) {
     double denom = 1.;
     switch (obs) {
         case GF_OBS_M: if (!eng->m.on) break; src = cur(eng, eng->m); denom = (double)eng->deck.NFM; break;
+        case GF_OBS_M_AFM1: if (!eng->a1.on) break; src = cur(eng, eng->a1); denom = (double)eng->deck.NAFM; break;
+        case GF_OBS_M_AFM2: if (!eng->a2.on) break; src = cur(eng, eng->a2); denom = (double)eng->deck.NAFM; break;
         case GF_OBS_P: if (!eng->p.on) break; src = cur(eng, eng->p); denom = (double)eng->deck.NFE; break;
         case GF_OBS_U: if (!eng->u.on) break; src = cur(eng, eng->u); denom = (double)eng->P.n; break;
         default: break;
@@ -1222,7 +1306,7 @@ int gf_check_finite(gf_engine* e) {
     gf_engine* eng = e;
     GF_CU(cudaSetDevice(eng->device));
     struct Named { const char* name; Field3* f; };
-    Named fs[] = {{"m", &eng->m}, {"p", &eng->p}, {"q", &eng->q}, {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H}};
+    Named fs[] = {{"m", &eng->m}, {"m_afm1", &eng->a1}, {"m_afm2", &eng->a2}, {"p", &eng->p}, {"q", &eng->q}, {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H}};
     for (auto& nf : fs) {
         if (!nf.f->on) continue;
         for (int a = 0; a < 3; a++) {

@@ -21,6 +21,9 @@ struct F3 { double* c[3]; };
 struct StageIO {
     // ferromagnet m and its stage increment (read by the Maxwell H update)
     F3 m_in, m_x, m_acc, m_out, dm;
+    // antiferromagnet sublattices m1, m2 and their stage increments
+    F3 a1_in, a1_x, a1_acc, a1_out, da1;
+    F3 a2_in, a2_x, a2_acc, a2_out, da2;
     // ferroelectric p and q = dp/dt
     F3 p_in, p_x, p_acc, p_out, q_in, q_x, q_acc, q_out;
     // elastic displacement u and velocity v

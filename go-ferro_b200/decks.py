@@ -227,6 +227,7 @@ class Deck:
     jf_cycles: int = 0
     # initial conditions / tables (None = deck's own uniform initialisation)
     m0: Optional[np.ndarray] = None        # (3, nx, ny, nz)
+    afm0: Optional[np.ndarray] = None      # (6, nx, ny, nz): m1 then m2
     p0: Optional[np.ndarray] = None
     q0: Optional[np.ndarray] = None
     u0: Optional[np.ndarray] = None
@@ -300,7 +301,7 @@ class Deck:
              "false false",
              "false",
              "false",
-             f"{_b(self.m0 is not None)} false false",
+             f"{_b(self.m0 is not None)} {_b(self.afm0 is not None)} false",
              f"{_b(self.p0 is not None)} false",
              "false false",
              f"{_b(self.u0 is not None)} false false",
@@ -348,6 +349,8 @@ def write_deck(deck: Deck, directory: str) -> str:
             f.write(material_text(m))
     if deck.m0 is not None:
         _write_restart(os.path.join(directory, "m.in"), deck.m0)
+    if deck.afm0 is not None:
+        _write_restart(os.path.join(directory, "m_AFM.in"), deck.afm0)
     if deck.p0 is not None:
         _write_restart(os.path.join(directory, "p.in"), deck.p0)
         q = deck.q0 if deck.q0 is not None else np.zeros_like(deck.p0)
@@ -381,6 +384,25 @@ def ggg() -> Material:
     """GGG-like non-magnetic garnet substrate (constants chosen for the
     coupled magnetoelastic preset)."""
     return Material(title="GGG", c11=2.86e11, c12=1.16e11, c44=0.905e11, density=7080.0, er=12.0)
+
+
+def afm_uniaxial(alpha: float = 0.01, magnetoelastic: bool = False) -> Material:
+    """Two-sublattice uniaxial antiferromagnet (NiO-like magnitudes; easy
+    axis z, inter-sublattice exchange field of order 10^7 A/m), on GGG-like
+    elastic constants."""
+    lam = (2e-5, 2e-5) if magnetoelastic else (0.0, 0.0)
+    return Material(title="AFM", c11=2.86e11, c12=1.16e11, c44=0.905e11, density=6800.0,
+                    afm=True, afm_Ms=(4.0e5, 4.0e5), afm_gyro=(1.76e11 * MU0, 1.76e11 * MU0),
+                    afm_alpha=(alpha, alpha), afm_K1=(2.0e4, 2.0e4), afm_axis=(0.0, 0.0, 1.0),
+                    afm_Aex=(2.0e-12, 2.0e-12), J_AFM=5.0e6, afm_lam100=lam, afm_lam111=lam, er=12.0)
+
+
+def tilt_afm0(shape, seed: int, mc: np.ndarray, max_deg: float = 2.0) -> np.ndarray:
+    """m1 along +z and m2 along -z in cells where mc is true, each tilted by
+    an independent seeded angle of at most max_deg (splitmix64 draws)."""
+    a = tilt_m0(shape, seed, mc, max_deg)
+    b = -tilt_m0(shape, seed + 7, mc, max_deg)
+    return np.concatenate([a, b], axis=0)
 
 
 def pto() -> Material:

@@ -18,7 +18,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 TOL = 1e-10
 
-FIELDS = {"m": ("mx", "my", "mz"), "u": ("ux", "uy", "uz"), "v": ("vx", "vy", "vz"),
+FIELDS = {"m": ("mx", "my", "mz"), "m_afm1": ("mx_AFM1", "my_AFM1", "mz_AFM1"),
+          "m_afm2": ("mx_AFM2", "my_AFM2", "mz_AFM2"), "u": ("ux", "uy", "uz"), "v": ("vx", "vy", "vz"),
           "p": ("px", "py", "pz"), "q": ("qx", "qy", "qz"), "Hstat": ("Hx_stat", "Hy_stat", "Hz_stat")}
 YEE = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 
@@ -39,6 +40,9 @@ def engine_trace(eng, steps, probe, graph=True):
         row[0] = s
         if eng.info.fm:
             row[1:4] = eng.average("m")
+        if eng.info.afm:
+            row[4:7] = eng.average("m_afm1")
+            row[7:10] = eng.average("m_afm2")
         if eng.info.fe:
             row[10:13] = eng.average("p")
         if eng.info.elastic:
@@ -170,12 +174,47 @@ def _variants(gf):
     d = D.preset_magnetoelastic(nx=4, ny=36, nz=40, sub=20, film=12, steps=6)
     d.amp_gauss *= 1e6
     v["elastic_quirk_far_tile"] = (d, 6, (2, 10, 30))
+    # ferromagnetic film on a non-magnetic substrate with vacuum above:
+    # magnetostatics every stage with non-magnetic cells in the FFT input
+    d = D.preset_fm_demag(nx=8, ny=8, nz=10, steps=15)
+    d.materials = [D.ggg(), D.yig(0.01)]
+    d.layers = [(4, 1), (4, 2), (2, 0)]
+    d.m0 = D.tilt_m0((8, 8, 10), 5, d.material_cell() == 2)
+    v["fm_film_demag_substrate"] = (d, 15, None)
+    # two-sublattice antiferromagnet film: uniaxial anisotropy, inter-sublattice
+    # exchange, magnetostatics every stage, external pulse, seeded tilted m1/m2
+    d = D.preset_fm_demag(nx=8, ny=8, nz=10, steps=20)
+    d.materials = [D.ggg(), D.afm_uniaxial(0.02)]
+    d.layers = [(4, 1), (4, 2), (2, 0)]
+    d.m0 = None
+    d.afm0 = D.tilt_afm0((8, 8, 10), 99, d.material_cell() == 2)
+    v["afm_film_demag"] = (d, 20, None)
+    # antiferromagnet with magnetoelastic coupling and eigenstrain, elastic
+    # source, Maxwell fields driven by and acting on the sublattices
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=20)
+    d.materials = [D.ggg(), D.afm_uniaxial(0.01, magnetoelastic=True)]
+    d.m0 = None
+    d.afm0 = D.tilt_afm0((8, 16, 12), 11, d.material_cell() == 2)
+    d.amp_gauss *= 1e6
+    v["afm_magnetoelastic_em"] = (d, 20, (4, 8, 7))
+    # ferromagnet on an antiferromagnet with a prescribed H table and a static
+    # + alternating field: the antiferromagnet recomputes the shared external
+    # field every stage and the ferromagnet's later stages see that value
+    d = D.preset_fm_demag(nx=8, ny=8, nz=10, steps=20)
+    d.materials = [D.afm_uniaxial(0.02), D.yig(0.01)]
+    d.layers = [(4, 1), (4, 2), (2, 0)]
+    mc = d.material_cell()
+    d.m0 = D.tilt_m0((8, 8, 10), 21, mc == 2)
+    d.afm0 = D.tilt_afm0((8, 8, 10), 22, mc == 1)
+    d.Hext_stat, d.Hext_altr, d.H_altr_freq = (0.0, 0.0, 4e4), (3e3, 0.0, 0.0), (5e11, 0.0, 0.0)
+    v["fm_on_afm_prescribed_h"] = (d, 20, None)
     return v
 
 
 @pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box",
                                    "fe_jf6_plane_wave_eext", "two_fm_materials_dmi_uniaxial", "demag_factor",
-                                   "elastic_multi_tile", "elastic_quirk_far_tile"])
+                                   "elastic_multi_tile", "elastic_quirk_far_tile", "fm_film_demag_substrate",
+                                   "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
