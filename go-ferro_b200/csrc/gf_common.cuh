@@ -77,6 +77,8 @@ struct Params {
     int em_fromM, em_fromP, em_back_M, em_back_P;
     int has_eig0, has_strain0, has_hext_nonunif;
     int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
+    int drude;                // some material has a Drude pole (omega_plasma != 0)
+    int pec;                  // some material is a perfect electric conductor
     int mag_1D;
     double liao_w;
     // elastic boundary coefficients (elastodynamics_AbsorbingBoundary.cpp)

@@ -126,6 +126,16 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
         dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
         er = er / 4.; cond = cond / 4.;
         double rhs = curl - Jf;
+        if (P.drude) {
+            // Drude current: 4-cell mean of the three poles' stage values
+            double Jp = 0.;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
+                Jp = Jp + io.jp_in[0].c[C][cc] + io.jp_in[1].c[C][cc] + io.jp_in[2].c[C][cc];
+            }
+            rhs = rhs - Jp / 4.;
+        }
         rhs = rhs - cond * io.E_in.c[C][e] - qdiv(dP, P.dt, P.rdt);
         d = P.dt_e0 / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
     }
@@ -215,6 +225,103 @@ __global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io, int nmat
     if (j < ny && k < nz) em_H_face<S, 0>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
     if (i < nx && k < nz) em_H_face<S, 1>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
     if (i < nx && j < ny) em_H_face<S, 2>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
+}
+
+// Drude polarisation current, per cell: dJp_n = (e0 wp_n^2 E_cell c_n -
+// Jp_n / tau_n) dt for the three poles (get_dJp_RK{1..4},
+// EMdynamic_solver.cpp:4318-4452) with E_cell the 4-edge mean of the stage E
+// (update_DE_cell, :3813-3826), and the RK4 combination of update_Jp_RK*/
+// update_Jp (:4454-4524).
+template <int S>
+__global__ void __launch_bounds__(256) k_drude(Params P, StageIO io) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const uint8_t id = io.mid[c];
+    const int nyz = P.ny * P.nz;
+    const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const int ny = P.ny, nz = P.nz;
+    double dJ[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+    if (id != 0) {
+        const DevMat& mt = io.mats[id - 1];
+        const int ex = (i * (ny + 1) + j) * (nz + 1) + k;
+        const int ey = (i * ny + j) * (nz + 1) + k;
+        const int ez = (i * (ny + 1) + j) * nz + k;
+        const double* Ex = io.E_in.c[0];
+        const double* Ey = io.E_in.c[1];
+        const double* Ez = io.E_in.c[2];
+        const double Ec[3] = {(Ex[ex] + Ex[ex + nz + 1] + Ex[ex + 1] + Ex[ex + nz + 1 + 1]) / 4.,
+                              (Ey[ey] + Ey[ey + ny * (nz + 1)] + Ey[ey + 1] + Ey[ey + ny * (nz + 1) + 1]) / 4.,
+                              (Ez[ez] + Ez[ez + (ny + 1) * nz] + Ez[ez + nz] + Ez[ez + (ny + 1) * nz + nz]) / 4.};
+#pragma unroll
+        for (int pole = 0; pole < 3; pole++)
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                dJ[pole][a] = (kE0 * mt.wp[pole] * mt.wp[pole] * Ec[a] * mt.comp[pole] - mt.rtau[pole] * io.jp_in[pole].c[a][c]) * P.dt;
+    }
+#pragma unroll
+    for (int pole = 0; pole < 3; pole++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const double d = dJ[pole][a];
+            double* out = io.jp_out[pole].c[a];
+            double* acc = io.jp_acc[pole].c[a];
+            const double xv = io.jp_x[pole].c[a][c];
+            if (S == 0) { out[c] = xv + d * 0.5; acc[c] = xv + qdiv(d, 6., kInv6); }
+            else if (S == 1) { out[c] = xv + d * 0.5; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
+            else if (S == 2) { out[c] = xv + d; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
+            else { acc[c] = acc[c] + qdiv(d, 6., kInv6); }
+        }
+}
+
+// Perfect electric conductor: E = 0 on every edge with a PEC cell among its
+// four cells, edges on non-periodic system faces excepted (DE?_ifPEC,
+// EMdynamic_initialize.cpp:160-330), after the Mur update (update_DE_PEC,
+// EMdynamic_solver.cpp:4526-4556).  The reference zeroes both the step value
+// and the stage value, so stages 1-3 also clear the step-start buffer.
+__device__ inline bool pec_cell(const StageIO& io, int c) {
+    const uint8_t id = io.mid[c];
+    return id != 0 && (io.mats[id - 1].flags & MF_PEC);
+}
+template <int S>
+__global__ void __launch_bounds__(256) k_em_pec(Params P, StageIO io) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (ny + 1) * (nz + 1)) return;
+    const int i = blockIdx.y;
+    const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
+    for (int C = 0; C < 3; C++) {
+        if ((C == 0 && i >= nx) || (C == 1 && j >= ny) || (C == 2 && k >= nz)) continue;
+        // the two directions across the edge and their wrapped cell indices
+        int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+        bool skip = false;
+        for (int d = 0; d < 3; d++) {
+            if (d == C) continue;
+            const int nd = d == 0 ? nx : (d == 1 ? ny : nz);
+            const int per = d == 0 ? P.per_x : (d == 1 ? P.per_y : P.per_z);
+            const int v = d == 0 ? i : (d == 1 ? j : k);
+            if (v == 0 || v == nd) {
+                if (!per) { skip = true; break; }
+                lo[d] = nd - 1; hi[d] = 0;
+            } else { lo[d] = v - 1; hi[d] = v; }
+        }
+        if (skip) continue;
+        bool pec = false;
+        for (int q = 0; q < 4; q++) {
+            int x[3];
+            int bit = 0;
+            for (int d = 0; d < 3; d++) {
+                if (d == C) { x[d] = d == 0 ? i : (d == 1 ? j : k); continue; }
+                x[d] = ((q >> bit) & 1) ? hi[d] : lo[d];
+                bit++;
+            }
+            pec = pec || pec_cell(io, (x[0] * ny + x[1]) * nz + x[2]);
+        }
+        if (!pec) continue;
+        const int e = C == 0 ? (i * (ny + 1) + j) * (nz + 1) + k
+                             : (C == 1 ? (i * ny + j) * (nz + 1) + k : (i * (ny + 1) + j) * nz + k);
+        if (S < 3) { io.E_out.c[C][e] = 0.; io.E_x.c[C][e] = 0.; }
+        else io.E_acc.c[C][e] = 0.;
+    }
 }
 
 // hard plane-wave source: E on z = plane_z, all three components, i<nx, j<ny

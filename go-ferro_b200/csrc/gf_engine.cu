@@ -71,6 +71,7 @@ struct gf_engine {
     double* jf_kfac = nullptr;
 
     Field3 m, a1, a2, p, q, u, v, E, H;
+    Field3 jp[3];                      // Drude pole currents
     double* dm[3] = {nullptr, nullptr, nullptr};
     double* da1[3] = {nullptr, nullptr, nullptr};
     double* da2[3] = {nullptr, nullptr, nullptr};
@@ -267,7 +268,6 @@ std::string unsupported(const Deck& d) {
     if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
     if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this engine";
     if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
-    if (d.any_pec && d.em_dynamic) return "PEC materials are not supported by this engine";
     if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
     if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this engine";
     if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
@@ -281,9 +281,10 @@ std::string unsupported(const Deck& d) {
         if (m.fm && m.afm) return "a material cannot be both ferromagnetic and antiferromagnetic";
         if (m.fe && m.fe_mass == 0.) return "ferroelectric material needs nonzero FE_mass";
         if (d.em_dynamic) {
-            for (int k = 0; k < 3; k++)
-                if (m.wp[k] != 0.) return "Drude dispersion (omega_plasma != 0) is not supported by this engine";
             if (!(m.comp[0] == m.comp[0])) return "Drude weights sum to zero: the reference's normalisation yields NaN fields for this deck";
+            // get_dJp_RK* runs for every material cell and divides by tao_e
+            for (int k = 0; k < 3; k++)
+                if (m.tau[k] == 0.) return "tao_e = 0: the reference's Drude update divides by it and its fields become NaN";
         }
     }
     if (d.elastodynamics) {
@@ -367,6 +368,12 @@ void build_params(gf_engine* eng) {
     P.has_hext_nonunif = d.read_Hext_nonunif;
     P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
+    P.drude = 0; P.pec = 0;
+    if (d.em_dynamic)
+        for (const Material& m : d.mats) {
+            for (int k = 0; k < 3; k++) if (m.wp[k] != 0.) P.drude = 1;
+            if (m.pec) P.pec = 1;
+        }
     P.liao_w = d.liao_w;
 
     // sound speeds of the first and last z planes (elastic_initialize.cpp:43-80)
@@ -566,6 +573,9 @@ void build_io(gf_engine* eng) {
             if (eng->v.on) set_io_field(eng->v, par, s, io.v_in, io.v_x, io.v_acc, io.v_out);
             if (eng->E.on) set_io_field(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out);
             if (eng->H.on) set_io_field(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out);
+            for (int pole = 0; pole < 3; pole++)
+                if (eng->jp[pole].on)
+                    set_io_field(eng->jp[pole], par, s, io.jp_in[pole], io.jp_x[pole], io.jp_acc[pole], io.jp_out[pole]);
             io.dm = f3(eng->dm);
             io.da1 = f3(eng->da1);
             io.da2 = f3(eng->da2);
@@ -659,6 +669,9 @@ int enqueue_stage(gf_engine* eng, int parity) {
         if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                                 dim3(kThreads), 0, st, P, io));
+        if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
     }
     if (eng->demag_per_stage) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
@@ -758,7 +771,8 @@ int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* sr
 // copy the current-step buffer of every state field into its other three
 // buffers, so cells a stage kernel does not cover stay consistent
 int replicate_state(gf_engine* eng) {
-    Field3* fs[] = {&eng->m, &eng->a1, &eng->a2, &eng->p, &eng->q, &eng->u, &eng->v, &eng->E, &eng->H};
+    Field3* fs[] = {&eng->m, &eng->a1, &eng->a2, &eng->p, &eng->q, &eng->u, &eng->v, &eng->E, &eng->H,
+                    &eng->jp[0], &eng->jp[1], &eng->jp[2]};
     for (Field3* f : fs) {
         if (!f->on) continue;
         double* const* c = (eng->steps_done & 1ull) ? f->A : f->X;
@@ -942,6 +956,8 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     // state fields
     if (d.any_fm) GF_TRY(alloc_field(eng, eng->m, n, n, n));
     if (d.any_afm) { GF_TRY(alloc_field(eng, eng->a1, n, n, n)); GF_TRY(alloc_field(eng, eng->a2, n, n, n)); }
+    if (P.drude)
+        for (int pole = 0; pole < 3; pole++) GF_TRY(alloc_field(eng, eng->jp[pole], n, n, n));
     if (d.any_fe) { GF_TRY(alloc_field(eng, eng->p, n, n, n)); GF_TRY(alloc_field(eng, eng->q, n, n, n)); }
     if (d.elastodynamics) { GF_TRY(alloc_field(eng, eng->u, n, n, n)); GF_TRY(alloc_field(eng, eng->v, n, n, n)); }
     if (d.em_dynamic) {

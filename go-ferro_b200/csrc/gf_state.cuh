@@ -32,6 +32,8 @@ struct StageIO {
     F3 force;         // stress divergence of the stage, k_elastic_tile -> k_elastic_rk
     // Yee E and H: component c of E lives on the c-edges, of H on the c-faces
     F3 E_in, E_x, E_acc, E_out, H_in, H_x, H_acc, H_out;
+    // Drude polarisation currents of the three poles (cell arrays)
+    F3 jp_in[3], jp_x[3], jp_acc[3], jp_out[3];
     // static and external fields
     F3 Hstat, Estat, Hnu;
     // face-normal displacement gradients of the current state, written by

@@ -208,13 +208,27 @@ def _variants(gf):
     d.afm0 = D.tilt_afm0((8, 8, 10), 22, mc == 1)
     d.Hext_stat, d.Hext_altr, d.H_altr_freq = (0.0, 0.0, 4e4), (3e3, 0.0, 0.0), (5e11, 0.0, 0.0)
     v["fm_on_afm_prescribed_h"] = (d, 20, None)
+    # metal layer with two Drude poles under the ferroelectric, sheet-current source in the metal
+    d = D.preset_ferroelectric(nx=8, ny=8, nz=10, steps=20)
+    metal = D.Material(title="metal", c11=2.3e11, c12=1.0e11, c44=1.2e11, density=8.9e3, er=1.0,
+                       drude=((0.6, 2e16, 1e-14), (0.4, 5e15, 5e-15), (0.0, 0.0, 1.0)))
+    d.materials.append(metal)
+    d.layers = [(3, 2), (7, 1)]
+    v["drude_metal_layer"] = (d, 20, (4, 4, 2))
+    # the same stack with a perfect-conductor bottom layer
+    d = D.preset_ferroelectric(nx=8, ny=8, nz=10, steps=20)
+    d.materials.append(D.Material(title="pec", c11=2.3e11, c12=1.0e11, c44=1.2e11, density=8.9e3, pec=True))
+    d.layers = [(3, 2), (7, 1)]
+    d.jf_lo, d.jf_hi = (0, 0, 5), (7, 7, 5)
+    v["pec_layer"] = (d, 20, (4, 4, 6))
     return v
 
 
 @pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box",
                                    "fe_jf6_plane_wave_eext", "two_fm_materials_dmi_uniaxial", "demag_factor",
                                    "elastic_multi_tile", "elastic_quirk_far_tile", "fm_film_demag_substrate",
-                                   "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h"])
+                                   "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
+                                   "drude_metal_layer", "pec_layer"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
