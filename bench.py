@@ -279,13 +279,16 @@ def run_ours(args, rank, world, local_rank):
 
         # ---- end-to-end through the C ABI with host buffers ----
         e2e_steps = max(1, min(args.steps, 20))
+        obs = [o for o, on in (("m", info.fm), ("m_afm1", info.afm), ("m_afm2", info.afm), ("p", info.fe),
+                               ("u", info.elastic)) if on]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             eng.advance(1)                      # uploads the step's drive row (pinned H2D)
-            eng.average("m")                    # D2H reads of the step's observables
-            eng.average("u")
-            eng.probe_em(d.nx // 2, d.ny // 2, sum(l[0] for l in d.layers[:2]) - 2)
+            for o in obs:                       # D2H reads of the step's observables
+                eng.average(o)
+            if info.em:
+                eng.probe_em(d.nx // 2, d.ny // 2, min(d.nz - 1, sum(l[0] for l in d.layers[:2]) - 2))
         e2e_s = time.perf_counter() - t0
         if dist:
             t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -293,7 +296,7 @@ def run_ours(args, rank, world, local_rank):
             e2e_s = float(t.item())
         e2e_value = world * ncell * e2e_steps / e2e_s
         h2d = 520     # one StepDrive row per step (time + 4 stage rows of 128 B)
-        d2h = 8 * 12  # <m>, <u>, E and H at the probe cell
+        d2h = 8 * 3 * len(obs) + (8 * 6 if info.em else 0)  # averages, E and H at the probe cell
 
         # ---- per-kernel device time for the roofline ----
         prof = eng.profile_steps(2)

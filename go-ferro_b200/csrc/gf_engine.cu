@@ -660,7 +660,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
                                   dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
     if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
                                    dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
-    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
+                            dim3(kThreads), 0, st, P, io));
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
         GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),

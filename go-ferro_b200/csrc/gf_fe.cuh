@@ -17,12 +17,14 @@ __device__ inline bool is_fe(const DevMat* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FE);
 }
 
+// Grid: (blocks over the (j,k) plane) x (nx planes), 32-bit indices.
 template <int S>
 __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    const long nyz = (long)P.ny * P.nz;
-    const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ny * nz) return;
+    const int i = blockIdx.y, j = t / nz, k = t - (t / nz) * nz;
+    const int c = (i * ny + j) * nz + k;
     const uint8_t id = io.mid[c];
     double dq[3] = {0., 0., 0.};
 
@@ -31,17 +33,17 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
         const double pxg = io.p_in.c[0][c], pyg = io.p_in.c[1][c], pzg = io.p_in.c[2][c];
 
         // ---- Laplacian with mirror condition at FE interfaces ----
-        const long ib = (i == 0) ? P.nx - 1 : i - 1, iF = (i == P.nx - 1) ? 0 : i + 1;
-        const long jb = (j == 0) ? P.ny - 1 : j - 1, jF = (j == P.ny - 1) ? 0 : j + 1;
-        const long kb = (k == 0) ? P.nz - 1 : k - 1, kF = (k == P.nz - 1) ? 0 : k + 1;
-        const long nb[6] = {cid(P, ib, j, k), cid(P, iF, j, k), cid(P, i, jb, k),
-                            cid(P, i, jF, k), cid(P, i, j, kb), cid(P, i, j, kF)};
+        const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
+        const int jb = (j == 0) ? ny - 1 : j - 1, jF = (j == ny - 1) ? 0 : j + 1;
+        const int kb = (k == 0) ? nz - 1 : k - 1, kF = (k == nz - 1) ? 0 : k + 1;
+        const int nb[6] = {(ib * ny + j) * nz + k, (iF * ny + j) * nz + k, (i * ny + jb) * nz + k,
+                           (i * ny + jF) * nz + k, (i * ny + j) * nz + kb, (i * ny + j) * nz + kF};
         const bool surf[6] = {(i == 0 && !P.per_x) || !is_fe(io.mats, io.mid[nb[0]]),
-                              (i == P.nx - 1 && !P.per_x) || !is_fe(io.mats, io.mid[nb[1]]),
+                              (i == nx - 1 && !P.per_x) || !is_fe(io.mats, io.mid[nb[1]]),
                               (j == 0 && !P.per_y) || !is_fe(io.mats, io.mid[nb[2]]),
-                              (j == P.ny - 1 && !P.per_y) || !is_fe(io.mats, io.mid[nb[3]]),
+                              (j == ny - 1 && !P.per_y) || !is_fe(io.mats, io.mid[nb[3]]),
                               (k == 0 && !P.per_z) || !is_fe(io.mats, io.mid[nb[4]]),
-                              (k == P.nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
+                              (k == nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
         double lap[3];   // sum of the three second derivatives per component
         for (int a = 0; a < 3; a++) {
@@ -129,13 +131,13 @@ __global__ void __launch_bounds__(256) k_fe(Params P, StageIO io) {
 
         if (P.em_back_P) {
             // cell-centred Maxwell E of the stage state (EMdynamic_solver.cpp:3813-3826)
-            const long ny1 = P.ny + 1, nz1 = P.nz + 1;
-            const long ex = (i * ny1 + j) * nz1 + k;
-            const long ey = (i * P.ny + j) * nz1 + k;
-            const long ez = (i * ny1 + j) * P.nz + k;
+            const int ny1 = ny + 1, nz1 = nz + 1;
+            const int ex = (i * ny1 + j) * nz1 + k;
+            const int ey = (i * ny + j) * nz1 + k;
+            const int ez = (i * ny1 + j) * nz + k;
             const double Ecx = (io.E_in.c[0][ex] + io.E_in.c[0][ex + nz1] + io.E_in.c[0][ex + 1] + io.E_in.c[0][ex + nz1 + 1]) / 4.;
-            const double Ecy = (io.E_in.c[1][ey] + io.E_in.c[1][ey + P.ny * nz1] + io.E_in.c[1][ey + 1] + io.E_in.c[1][ey + P.ny * nz1 + 1]) / 4.;
-            const double Ecz = (io.E_in.c[2][ez] + io.E_in.c[2][ez + ny1 * P.nz] + io.E_in.c[2][ez + P.nz] + io.E_in.c[2][ez + ny1 * P.nz + P.nz]) / 4.;
+            const double Ecy = (io.E_in.c[1][ey] + io.E_in.c[1][ey + ny * nz1] + io.E_in.c[1][ey + 1] + io.E_in.c[1][ey + ny * nz1 + 1]) / 4.;
+            const double Ecz = (io.E_in.c[2][ez] + io.E_in.c[2][ez + ny1 * nz] + io.E_in.c[2][ez + nz] + io.E_in.c[2][ez + ny1 * nz + nz]) / 4.;
             dq[0] = dq[0] - fm * Ecx;
             dq[1] = dq[1] - fm * Ecy;
             dq[2] = dq[2] - fm * Ecz;
