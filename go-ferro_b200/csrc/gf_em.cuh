@@ -206,7 +206,9 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, const EmMat
 // is (blocks over the (j,k) vertex plane) x (nx+1 planes); the material
 // constants are staged in shared memory.
 template <int S>
-__global__ void __launch_bounds__(256) k_em_fused(Params P, StageIO io, int nmat) {
+// (256, 8): 32 registers, 64 resident warps per SM; the kernel is bound by
+// the latency of its neighbour loads, and full occupancy beats the spills
+__global__ void __launch_bounds__(256, 8) k_em_fused(Params P, StageIO io, int nmat) {
     __shared__ EmMat mt[kMaxMat];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMat& d = io.mats[q];
