@@ -178,16 +178,18 @@ def build_deck(gf, wl: str, sample: bool):
     return d
 
 
-def cpu_reference(gf, wl: str, steps: int, tmp: str):
-    """GO-Ferro's own solver on the bounded CPU sample; returns (cell-steps/s, info)."""
+def cpu_reference(gf, wl: str, steps: int, tmp: str, warmup: int = 0):
+    """GO-Ferro's own solver on the bounded CPU sample: `warmup` untimed steps,
+    then `steps` timed ones; returns (cell-steps/s, info)."""
     from oracle import refrun
     if not refrun.available():
         return None, "oracle binary not built"
     d = build_deck(gf, wl, sample=True)
-    d.steps = steps
+    d.steps = steps + warmup
     ddir = os.path.join(tmp, "ref_deck")
     gf.decks.write_deck(d, ddir)
-    r = refrun.run(ddir, os.path.join(tmp, "ref_out"), steps=steps, trace_every=max(steps, 1))
+    r = refrun.run(ddir, os.path.join(tmp, "ref_out"), steps=steps + warmup, trace_every=max(steps + warmup, 1),
+                   warmup=warmup)
     t = r["timing"]
     value = d.n * steps / t["seconds"]
     sample = f"{d.nx}x{d.ny}x{d.nz} sub-grid of the workload's layer stack, {steps} steps, serial reference build"
@@ -202,13 +204,14 @@ def run_reference_arm(args, rank, world):
     spec = WORKLOADS[args.workload]
     with tempfile.TemporaryDirectory() as tmp:
         steps = max(1, min(args.steps, args.ref_steps))
-        value, info = cpu_reference(gf, args.workload, steps, tmp)
+        warm = min(args.warmup, 3)
+        value, info = cpu_reference(gf, args.workload, steps, tmp, warm)
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": info}))
         return
     line = {
         "impl": "reference", "metric": "cell-steps/s FP64", "value": value, "unit": "cell-steps/s",
-        "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * info["seconds"] / steps,
+        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * info["seconds"] / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": spec["desc"], "sample": info["sample"]},
         "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "reference", "sample": info["sample"]},
@@ -323,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as tmp:
-            v, ci = cpu_reference(gf, args.workload, args.ref_steps, tmp)
+            v, ci = cpu_reference(gf, args.workload, args.ref_steps, tmp, 3)
         if v is not None:
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "reference", "sample": ci["sample"]}
     line = {

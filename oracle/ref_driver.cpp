@@ -9,7 +9,7 @@
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg run it.
  *
  * Usage:
- *   goferro_ref DECK_DIR OUT_DIR [--steps K] [--trace-every N]
+ *   goferro_ref DECK_DIR OUT_DIR [--steps K] [--warmup W] [--trace-every N]
  *               [--probe I J K] [--dump]
  *
  * DECK_DIR holds system_setting.in, materials.in and any restart files the
@@ -20,7 +20,8 @@
  *              <u>x y z  E_cell(probe)x y z  H_cell(probe)x y z   (%.17e)
  *   *.bin      with --dump: raw float64 fields after the last step, in the
  *              reference's storage order (matrix.h:51)
- *   timing.json  {"steps":K,"seconds":S,"cells":n} for the time loop only.
+ *   timing.json  {"steps":K-W,"warmup":W,"seconds":S,"cells":n} for the time
+ *                loop after the first W (untimed) steps.
  */
 #define _USE_SINGLETON_MACRO
 #include "_MACRO_SINGLETON.h"
@@ -172,19 +173,21 @@ void dump_all(const std::string& d, Systems& s) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        fprintf(stderr, "usage: %s DECK_DIR OUT_DIR [--steps K] [--trace-every N] [--probe I J K] [--dump]\n", argv[0]);
+        fprintf(stderr, "usage: %s DECK_DIR OUT_DIR [--steps K] [--warmup W] [--trace-every N] [--probe I J K] [--dump]\n", argv[0]);
         return 2;
     }
     char outbuf[PATH_MAX];
     if (!realpath(argv[2], outbuf)) { fprintf(stderr, "bad OUT_DIR %s\n", argv[2]); return 2; }
     std::string out = outbuf;
     long long steps_override = -1;
+    unsigned long long warmup = 0;
     unsigned long long trace_every = 1;
     long pi = -1, pj = -1, pk = -1;
     bool do_dump = false;
     for (int a = 3; a < argc; ++a) {
         if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps_override = atoll(argv[++a]);
         else if (!strcmp(argv[a], "--trace-every") && a + 1 < argc) trace_every = strtoull(argv[++a], 0, 10);
+        else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = strtoull(argv[++a], 0, 10);
         else if (!strcmp(argv[a], "--probe") && a + 3 < argc) { pi = atol(argv[++a]); pj = atol(argv[++a]); pk = atol(argv[++a]); }
         else if (!strcmp(argv[a], "--dump")) do_dump = true;
         else { fprintf(stderr, "unknown argument %s\n", argv[a]); return 2; }
@@ -267,8 +270,10 @@ int main(int argc, char** argv) {
     }
 
     // ---- time loop (main.cpp:243-484) ----
+    // the first `warmup` steps run outside the timed region
     auto t0 = std::chrono::steady_clock::now();
     for (unsigned long long nstep = 1; nstep < _GLB.step + 1; ++nstep) {
+        if (nstep == warmup + 1) t0 = std::chrono::steady_clock::now();
         _GLB.time_marching_device_serial();
         for (int st = 0; st < 4; ++st) {
             run_stage(s, st);
@@ -285,7 +290,8 @@ int main(int argc, char** argv) {
     std::string jpath = out + "/timing.json";
     FILE* jf = fopen(jpath.c_str(), "w");
     if (jf) {
-        fprintf(jf, "{\"steps\": %llu, \"seconds\": %.9f, \"cells\": %ld}\n", _GLB.step, secs, n);
+        const unsigned long long timed = _GLB.step > warmup ? _GLB.step - warmup : 0;
+        fprintf(jf, "{\"steps\": %llu, \"warmup\": %llu, \"seconds\": %.9f, \"cells\": %ld}\n", timed, warmup, secs, n);
         fclose(jf);
     }
     if (do_dump) dump_all(out, s);

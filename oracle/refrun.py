@@ -32,7 +32,8 @@ def build(ref_dir: str = "/root/reference") -> None:
 
 
 def run(deck_dir: str, out_dir: str, steps: Optional[int] = None, trace_every: int = 1,
-        probe: Optional[Sequence[int]] = None, dump: bool = False, timeout: float = 3600.0) -> Dict:
+        probe: Optional[Sequence[int]] = None, dump: bool = False, timeout: float = 3600.0,
+        warmup: int = 0) -> Dict:
     """Run the reference on `deck_dir`; returns {"trace": (K,22) array,
     "timing": {...}, "fields": {name: flat float64 array}}."""
     if not available():
@@ -41,6 +42,8 @@ def run(deck_dir: str, out_dir: str, steps: Optional[int] = None, trace_every: i
     cmd = [REF_BIN, os.path.abspath(deck_dir), os.path.abspath(out_dir), "--trace-every", str(trace_every)]
     if steps is not None:
         cmd += ["--steps", str(int(steps))]
+    if warmup:
+        cmd += ["--warmup", str(int(warmup))]
     if probe is not None:
         cmd += ["--probe"] + [str(int(x)) for x in probe]
     if dump:
