@@ -29,9 +29,10 @@ FIELD = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "q": 4, "u": 5, "v": 6,
          "Ex": 7, "Ey": 8, "Ez": 9, "Hx": 10, "Hy": 11, "Hz": 12,
          "Hstat": 13, "Estat": 14, "E_cell": 15, "H_cell": 16, "strain": 17}
 OBS = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "u": 4}
+PRECISION = {"fp64": 0, "mixed": 1}   # GF_PRECISION_FP64, GF_PRECISION_MIXED_FP32
 
 # every symbol include/goferro_b200.h declares
-EXPORTS = ["gf_create_from_deck", "gf_advance", "gf_advance_eager", "gf_average", "gf_probe_em",
+EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_advance_eager", "gf_average", "gf_probe_em",
            "gf_field_dims", "gf_download", "gf_upload", "gf_download_device", "gf_upload_device",
            "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
            "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients"]
@@ -47,7 +48,7 @@ class GFInfo(ctypes.Structure):
                 ("elastic", ctypes.c_int32), ("em", ctypes.c_int32), ("demag_per_stage", ctypes.c_int32),
                 ("n_fm", ctypes.c_uint64), ("n_afm", ctypes.c_uint64), ("n_fe", ctypes.c_uint64),
                 ("device_bytes", ctypes.c_uint64),
-                ("launches_per_step", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
+                ("launches_per_step", ctypes.c_int32), ("precision", ctypes.c_int32)]
 
 
 class GFKernelTime(ctypes.Structure):
@@ -74,6 +75,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib = ctypes.CDLL(p)
     vp, c_int, c_u64, c_dbl_p = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)
     lib.gf_create_from_deck.argtypes = [ctypes.c_char_p, c_int, ctypes.POINTER(vp)]
+    lib.gf_create_from_deck_ex.argtypes = [ctypes.c_char_p, c_int, c_int, ctypes.POINTER(vp)]
     lib.gf_advance.argtypes = [vp, c_u64]
     lib.gf_advance_eager.argtypes = [vp, c_u64]
     lib.gf_average.argtypes = [vp, c_int, c_dbl_p]
@@ -102,12 +104,15 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
 
 
 class Engine:
-    """One engine instance (device memory, stream, CUDA graphs) for a deck."""
+    """One engine instance (device memory, stream, CUDA graphs) for a deck.
 
-    def __init__(self, deck_dir: str, device: int = -1, lib: Optional[ctypes.CDLL] = None):
+    precision: "fp64" (the parity form) or "mixed" (FP32 state and stencils
+    with compensated RK4 accumulation; FP64 at the interface)."""
+
+    def __init__(self, deck_dir: str, device: int = -1, lib: Optional[ctypes.CDLL] = None, precision: str = "fp64"):
         self.lib = lib or load_library()
         h = ctypes.c_void_p()
-        rc = self.lib.gf_create_from_deck(os.fsencode(deck_dir), device, ctypes.byref(h))
+        rc = self.lib.gf_create_from_deck_ex(os.fsencode(deck_dir), device, PRECISION[precision], ctypes.byref(h))
         if rc != GF_OK:
             raise GFError(rc, self.lib.gf_last_error(None).decode())
         self.h = h

@@ -22,40 +22,51 @@ constexpr int kMaxMat = 32;
 
 enum MatFlag : uint32_t { MF_FM = 1u, MF_AFM = 2u, MF_FE = 4u, MF_PEC = 8u };
 
+// Real type of the mixed-precision form: state and stencils in FP32.
+template <class R> struct is_mixed { static constexpr bool value = false; };
+template <> struct is_mixed<float> { static constexpr bool value = true; };
+
 // Per-material constants, precomputed on the host with the same expressions
-// (and operation order) the reference evaluates inside its cell loops.
-struct DevMat {
+// (and operation order) the reference evaluates inside its cell loops.  The
+// FP64 table is converted member by member for the mixed form: after the
+// four integers every member is a real of type R.
+template <class R>
+struct DevMatT {
     uint32_t flags;
     int aniso;          // anisotropy_type
     int cubic_c;        // 1: rotated stiffness has the cubic sparsity pattern
     int pad_;
     // FM LLG (magnetic_solver.cpp:84-87, 164-185, 206-208)
-    double Ms, K1c, K2c, B1c, B2c, Aex, dA;   // dA = D/2./A
-    double ex_coef;                            // 2./mu0/Ms
-    double dmi_coef;                           // 2.*D/mu0/Ms
-    double alpha, precess, alpha_precess;      // precess = -gyro/(1+a^2)*dt
+    R Ms, K1c, K2c, B1c, B2c, Aex, dA;   // dA = D/2./A
+    R ex_coef;                            // 2./mu0/Ms
+    R dmi_coef;                           // 2.*D/mu0/Ms
+    R alpha, precess, alpha_precess;      // precess = -gyro/(1+a^2)*dt
     // AFM sublattices s = 0, 1 (magnetic_AFM_solver.cpp:106-112, 181-191)
-    double Ms1, Ms2;
-    double aAex[2];                 // Aex_AFM
-    double aK1c[2], aB1c[2], aB2c[2];   // K1/mu0/Ms, B1/mu0/Ms, B2/mu0/Ms
-    double aJ[2];                   // -1*J_AFM/mu0/Ms
-    double aex[2];                  // 2./mu0/Ms
-    double aprec[2], aaprec[2];     // -gyro/(1+a^2)*dt and alpha times it
-    double au[3];                   // uniaxial axis (crystal frame, normalised)
+    R Ms1, Ms2;
+    R aAex[2];                 // Aex_AFM
+    R aK1c[2], aB1c[2], aB2c[2];   // K1/mu0/Ms, B1/mu0/Ms, B2/mu0/Ms
+    R aJ[2];                   // -1*J_AFM/mu0/Ms
+    R aex[2];                  // 2./mu0/Ms
+    R aprec[2], aaprec[2];     // -gyro/(1+a^2)*dt and alpha times it
+    R au[3];                   // uniaxial axis (crystal frame, normalised)
     // elastic (elastic_dynamic_solver.cpp:1295-1297)
-    double cij[6][6];
-    double dens_dt, mass_damp, stiff_damp;
+    R cij[6][6];
+    R dens_dt, mass_damp, stiff_damp;
     // dynamic eigenstrain (elastic_dynamic_solver.cpp:24-61)
-    double l100_15, l111_15, l100a1_075, l100a2_075, l111a1_075, l111a2_075;
-    double Q11, Q12, Q44;
+    R l100_15, l111_15, l100a1_075, l100a2_075, l111a1_075, l111a2_075;
+    R Q11, Q12, Q44;
     // ferroelectric TDGL (ferroelectric_solver.cpp:704-717)
-    double a1, a11, a12, a111, a112, a123, a1111, a1112, a1122, a1123;
-    double tv1, tv2, tv3, G11;
-    double fe_coef, fe_damp;                    // -dt/m, fe_coef*gamma
+    R a1, a11, a12, a111, a112, a123, a1111, a1112, a1122, a1123;
+    R tv1, tv2, tv3, G11;
+    R fe_coef, fe_damp;                    // -dt/m, fe_coef*gamma
     // electromagnetic
-    double er, cond;
-    double comp[3], wp[3], rtau[3];
+    R er, cond;
+    R comp[3], wp[3], rtau[3];
 };
+using DevMat = DevMatT<double>;
+constexpr int kDevMatReals = (int)((sizeof(DevMatT<double>) - 16) / sizeof(double));
+static_assert(sizeof(DevMatT<double>) == 16 + kDevMatReals * sizeof(double), "DevMatT<double> layout");
+static_assert(sizeof(DevMatT<float>) == 16 + kDevMatReals * sizeof(float), "DevMatT<float> layout");
 
 // Grid, switches and scalars that every kernel needs (passed by value).
 struct Params {
@@ -95,6 +106,11 @@ struct Params {
     // J_f box (EMdynamic_initialize.cpp:60-68)
     int jf_on, jf_type, jf_comp;
     long jf_i0, jf_i1, jf_j0, jf_j1, jf_k0, jf_k1;
+    // FP32 copies of the constants the mixed-form stencils use
+    struct {
+        float rdx, rdy, rdz, rdt, dt, dt_e0, mdt_mu0;
+        float Tg2c[3][3], Tc2g[3][3];
+    } f;
 };
 
 // Values that depend on time, computed on the host for every step with the
@@ -141,54 +157,53 @@ __device__ __forceinline__ double qdiv(double x, double d, double rd) {
     return x == 0. ? q0 : q2;
 }
 
+// Division by a run constant d: qdiv in the FP64 form (rd = RN(1/d)); in the
+// mixed form a multiplication by the FP32 reciprocal rdf (within one ulp of
+// the FP32 quotient).
+__device__ __forceinline__ double qdivR(double x, double d, double rd, float) { return qdiv(x, d, rd); }
+__device__ __forceinline__ float qdivR(float x, double, double, float rdf) { return x * rdf; }
+
+// frame-rotation matrices in the kernel's precision
+template <class R> __device__ __forceinline__ const auto& Tg2c(const Params& P) {
+    if constexpr (is_mixed<R>::value) return P.f.Tg2c; else return P.Tg2c;
+}
+template <class R> __device__ __forceinline__ const auto& Tc2g(const Params& P) {
+    if constexpr (is_mixed<R>::value) return P.f.Tc2g; else return P.Tc2g;
+}
+
 __host__ __device__ inline long cid(const Params& P, long i, long j, long k) {
     return (i * P.ny + j) * P.nz + k;
 }
 
 // 3x3 frame rotations (mathlib.cpp:45-125); identity when rot == 0
-__device__ inline void glb2crt(const Params& P, double x, double y, double z, double& a, double& b, double& c) {
+template <class R>
+__device__ inline void glb2crt(const Params& P, R x, R y, R z, R& a, R& b, R& c) {
     if (P.rot) {
-        a = P.Tg2c[0][0] * x + P.Tg2c[0][1] * y + P.Tg2c[0][2] * z;
-        b = P.Tg2c[1][0] * x + P.Tg2c[1][1] * y + P.Tg2c[1][2] * z;
-        c = P.Tg2c[2][0] * x + P.Tg2c[2][1] * y + P.Tg2c[2][2] * z;
+        const auto& T = Tg2c<R>(P);
+        a = T[0][0] * x + T[0][1] * y + T[0][2] * z;
+        b = T[1][0] * x + T[1][1] * y + T[1][2] * z;
+        c = T[2][0] * x + T[2][1] * y + T[2][2] * z;
     } else { a = x; b = y; c = z; }
 }
-__device__ inline void crt2glb(const Params& P, double x, double y, double z, double& a, double& b, double& c) {
+template <class R>
+__device__ inline void crt2glb(const Params& P, R x, R y, R z, R& a, R& b, R& c) {
     if (P.rot) {
-        a = P.Tc2g[0][0] * x + P.Tc2g[0][1] * y + P.Tc2g[0][2] * z;
-        b = P.Tc2g[1][0] * x + P.Tc2g[1][1] * y + P.Tc2g[1][2] * z;
-        c = P.Tc2g[2][0] * x + P.Tc2g[2][1] * y + P.Tc2g[2][2] * z;
+        const auto& T = Tc2g<R>(P);
+        a = T[0][0] * x + T[0][1] * y + T[0][2] * z;
+        b = T[1][0] * x + T[1][1] * y + T[1][2] * z;
+        c = T[2][0] * x + T[2][1] * y + T[2][2] * z;
     } else { a = x; b = y; c = z; }
 }
 // symmetric tensor rotation out[i][j] = sum_kl T[i][k] T[j][l] in[k][l]
-__device__ inline void rot_tensor(const double T[3][3], const double in[3][3], double out[3][3]) {
+template <class R>
+__device__ inline void rot_tensor(const R T[3][3], const R in[3][3], R out[3][3]) {
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) {
-            double acc = 0.;
+            R acc = R(0);
             for (int k = 0; k < 3; k++)
                 for (int l = 0; l < 3; l++) acc = acc + T[i][k] * T[j][l] * in[k][l];
             out[i][j] = acc;
         }
-}
-
-// Voigt stress = C * strain with the reference's row accumulation order
-// (mathlib.cpp:127-135).  For the cubic pattern the zero entries are
-// skipped, which leaves every partial sum unchanged.
-__device__ inline void strain2stress(const DevMat& m, const double e[6], double s[6]) {
-    if (m.cubic_c) {
-        s[0] = m.cij[0][0] * e[0] + m.cij[0][1] * e[1] + m.cij[0][2] * e[2];
-        s[1] = m.cij[1][0] * e[0] + m.cij[1][1] * e[1] + m.cij[1][2] * e[2];
-        s[2] = m.cij[2][0] * e[0] + m.cij[2][1] * e[1] + m.cij[2][2] * e[2];
-        s[3] = m.cij[3][3] * e[3];
-        s[4] = m.cij[4][4] * e[4];
-        s[5] = m.cij[5][5] * e[5];
-    } else {
-        for (int i = 0; i < 6; i++) {
-            double acc = 0.;
-            for (int j = 0; j < 6; j++) acc = acc + m.cij[i][j] * e[j];
-            s[i] = acc;
-        }
-    }
 }
 
 }  // namespace gf

@@ -1,4 +1,4 @@
-// Magnetostatics (FP64): periodic FFT convolution of M with the demag
+// Magnetostatics: periodic FFT convolution of M with the demag
 // tensor of a cuboid cell.
 //
 //   k_newell      builds the nine real-space tensor tables on the device.
@@ -14,7 +14,9 @@
 //   k_mag_source  M = Ms m for the forward transform, and the demag-factor
 //                 and 1-D alternatives (magnetostatic_solver.cpp:114-249).
 // The transforms themselves are cuFFT D2Z / Z2D (batched over the three
-// components), unnormalised as in the reference.
+// components), unnormalised as in the reference.  The mixed form builds the
+// tables and their spectra in FP64 (k_newell, D2Z), stores the spectra in
+// FP32 and runs R2C / C2R per stage.
 #pragma once
 
 #include <cuComplex.h>
@@ -186,6 +188,51 @@ __global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F
         }
     } else if (mode == 0) {
         M3[c] = 0.; M3[P.n + c] = 0.; M3[2 * P.n + c] = 0.;
+    }
+}
+
+// ---- mixed form: FP32 transforms; the spectra are built in FP64 ----
+
+// complex FP64 -> FP32 (the Green spectra after the FP64 transform)
+__global__ void k_spectra_f32(const cuDoubleComplex* __restrict__ in, long n, cuComplex* __restrict__ out) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    out[q] = make_cuComplex((float)in[q].x, (float)in[q].y);
+}
+
+// k_demag_mul on FP32 spectra; inv_vol_neg = -1/(dx dy dz)
+__global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float inv_vol_neg, const cuComplex* __restrict__ Mk,
+                                                       const cuComplex* __restrict__ Nk, cuComplex* __restrict__ Hk) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n21) return;
+    const cuComplex mx = Mk[q], my = Mk[n21 + q], mz = Mk[2 * n21 + q];
+    const cuComplex* N = Nk;
+    const cuComplex hx = cuCaddf(cuCaddf(cuCmulf(mx, N[0 * n21 + q]), cuCmulf(my, N[3 * n21 + q])), cuCmulf(mz, N[8 * n21 + q]));
+    const cuComplex hy = cuCaddf(cuCaddf(cuCmulf(my, N[1 * n21 + q]), cuCmulf(mz, N[4 * n21 + q])), cuCmulf(mx, N[6 * n21 + q]));
+    const cuComplex hz = cuCaddf(cuCaddf(cuCmulf(mz, N[2 * n21 + q]), cuCmulf(mx, N[5 * n21 + q])), cuCmulf(my, N[7 * n21 + q]));
+    Hk[q] = make_cuComplex(hx.x * inv_vol_neg, hx.y * inv_vol_neg);
+    Hk[n21 + q] = make_cuComplex(hy.x * inv_vol_neg, hy.y * inv_vol_neg);
+    Hk[2 * n21 + q] = make_cuComplex(hz.x * inv_vol_neg, hz.y * inv_vol_neg);
+}
+
+// k_mag_source for the mixed form (ferromagnets; the mixed form has no AFM)
+__global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, const uint8_t* mid, F3T<float> m, int mode,
+                                 float* M3, F3T<float> Hs, float f0, float f1, float f2) {
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const uint8_t id = mid[c];
+    const uint32_t fl = id ? mats[id - 1].flags : 0u;
+    if (fl & MF_FM) {
+        const float Ms = mats[id - 1].Ms;
+        if (mode == 0) {
+            M3[c] = Ms * m.c[0][c]; M3[P.n + c] = Ms * m.c[1][c]; M3[2 * P.n + c] = Ms * m.c[2][c];
+        } else if (mode == 1) {
+            Hs.c[0][c] = Ms * m.c[0][c] * f0; Hs.c[1][c] = Ms * m.c[1][c] * f1; Hs.c[2][c] = Ms * m.c[2][c] * f2;
+        } else {
+            Hs.c[0][c] = 0.f; Hs.c[1][c] = 0.f; Hs.c[2][c] = -Ms * m.c[2][c];
+        }
+    } else if (mode == 0) {
+        M3[c] = 0.f; M3[P.n + c] = 0.f; M3[2 * P.n + c] = 0.f;
     }
 }
 

@@ -1,4 +1,4 @@
-// Elastodynamics stage kernels (FP64).
+// Elastodynamics stage kernels (FP64 parity form and FP32 mixed form).
 //
 //   k_elastic_tile  per cell, tiled over (j,k) and marching along x: the
 //                 face-normal displacement gradients (get_dudxyz_glb,
@@ -42,7 +42,8 @@ __device__ inline bool free_z(const Params& P, const uint8_t* mid, long i, long 
     return !(solid_at(P, mid, i, j, f - 1) && solid_at(P, mid, i, j, f));
 }
 
-__global__ void __launch_bounds__(256) k_face_grad(Params P, StageIO io) {
+template <class R = double>
+__global__ void __launch_bounds__(256) k_face_grad(Params P, StageIOT<R> io) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long nyz = (long)P.ny * P.nz;
@@ -52,36 +53,37 @@ __global__ void __launch_bounds__(256) k_face_grad(Params P, StageIO io) {
     const long cy = cid(P, i, j == 0 ? P.ny - 1 : j - 1, k);
     const long cz = cid(P, i, j, k == 0 ? P.nz - 1 : k - 1);
     for (int a = 0; a < 3; a++) {
-        const double* u = io.u_in.c[a];
-        const double uc = u[c];
-        io.fg[a][c] = fx ? 0. : qdiv((uc - u[cx]), P.dx, P.rdx);
-        io.fg[3 + a][c] = fy ? 0. : qdiv((uc - u[cy]), P.dy, P.rdy);
-        io.fg[6 + a][c] = fz ? 0. : qdiv((uc - u[cz]), P.dz, P.rdz);
+        const R* u = io.u_in.c[a];
+        const R uc = u[c];
+        io.fg[a][c] = fx ? R(0.) : qdivR((uc - u[cx]), P.dx, P.rdx, P.f.rdx);
+        io.fg[3 + a][c] = fy ? R(0.) : qdivR((uc - u[cy]), P.dy, P.rdy, P.f.rdy);
+        io.fg[6 + a][c] = fz ? R(0.) : qdivR((uc - u[cz]), P.dz, P.rdz, P.f.rdz);
     }
 }
 
 // read access to the stored face gradients; f may equal n
+template <class R>
 struct GradView {
     const Params& P;
-    const StageIO& io;
-    __device__ GradView(const Params& p, const StageIO& s) : P(p), io(s) {}
-    __device__ double gx(int a, long f, long j, long k) const { return io.fg[a][cid(P, f == P.nx ? 0 : f, j, k)]; }
-    __device__ double gy(int a, long i, long f, long k) const { return io.fg[3 + a][cid(P, i, f == P.ny ? 0 : f, k)]; }
-    __device__ double gz(int a, long i, long j, long f) const { return io.fg[6 + a][cid(P, i, j, f == P.nz ? 0 : f)]; }
+    const StageIOT<R>& io;
+    __device__ GradView(const Params& p, const StageIOT<R>& s) : P(p), io(s) {}
+    __device__ R gx(int a, long f, long j, long k) const { return io.fg[a][cid(P, f == P.nx ? 0 : f, j, k)]; }
+    __device__ R gy(int a, long i, long f, long k) const { return io.fg[3 + a][cid(P, i, f == P.ny ? 0 : f, k)]; }
+    __device__ R gz(int a, long i, long j, long f) const { return io.fg[6 + a][cid(P, i, j, f == P.nz ? 0 : f)]; }
     // cell strain components in the global frame (get_Dstrain)
-    __device__ double exx(long i, long j, long k) const { return (gx(0, i, j, k) + gx(0, i + 1, j, k)) / 2.; }
-    __device__ double eyy(long i, long j, long k) const { return (gy(1, i, j, k) + gy(1, i, j + 1, k)) / 2.; }
-    __device__ double ezz(long i, long j, long k) const { return (gz(2, i, j, k) + gz(2, i, j, k + 1)) / 2.; }
-    __device__ double eyz(long i, long j, long k) const {
-        return (gz(1, i, j, k) + gz(1, i, j, k + 1) + gy(2, i, j, k) + gy(2, i, j + 1, k)) / 4.;
+    __device__ R exx(long i, long j, long k) const { return (gx(0, i, j, k) + gx(0, i + 1, j, k)) / R(2.); }
+    __device__ R eyy(long i, long j, long k) const { return (gy(1, i, j, k) + gy(1, i, j + 1, k)) / R(2.); }
+    __device__ R ezz(long i, long j, long k) const { return (gz(2, i, j, k) + gz(2, i, j, k + 1)) / R(2.); }
+    __device__ R eyz(long i, long j, long k) const {
+        return (gz(1, i, j, k) + gz(1, i, j, k + 1) + gy(2, i, j, k) + gy(2, i, j + 1, k)) / R(4.);
     }
-    __device__ double exz(long i, long j, long k) const {
-        return (gz(0, i, j, k) + gz(0, i, j, k + 1) + gx(2, i, j, k) + gx(2, i + 1, j, k)) / 4.;
+    __device__ R exz(long i, long j, long k) const {
+        return (gz(0, i, j, k) + gz(0, i, j, k + 1) + gx(2, i, j, k) + gx(2, i + 1, j, k)) / R(4.);
     }
-    __device__ double exy(long i, long j, long k) const {
-        return (gy(0, i, j, k) + gy(0, i, j + 1, k) + gx(1, i, j, k) + gx(1, i + 1, j, k)) / 4.;
+    __device__ R exy(long i, long j, long k) const {
+        return (gy(0, i, j, k) + gy(0, i, j + 1, k) + gx(1, i, j, k) + gx(1, i + 1, j, k)) / R(4.);
     }
-    __device__ void strain_glb(long i, long j, long k, double e[6]) const {
+    __device__ void strain_glb(long i, long j, long k, R e[6]) const {
         e[0] = exx(i, j, k); e[1] = eyy(i, j, k); e[2] = ezz(i, j, k);
         e[3] = eyz(i, j, k); e[4] = exz(i, j, k); e[5] = exy(i, j, k);
     }
@@ -92,11 +94,11 @@ struct GradView {
 // of p, then the two AFM sublattices with half weight, minus the static
 // eigenstrain e0.  The sublattice terms are added only when the run has
 // antiferromagnets; without them they are exact zeros in the reference.
-template <class M>
-__device__ inline void eigen_terms(const Params& P, const StageIO& io, long c, const M& mt, double mx, double my,
-                                   double mz, double px, double py, double pz, const double e0[6], double e[6]) {
-    const double third = 1. / 3.;
-    double t[6];
+template <class R, class M>
+__device__ inline void eigen_terms(const Params& P, const StageIOT<R>& io, long c, const M& mt, R mx, R my,
+                                   R mz, R px, R py, R pz, const R e0[6], R e[6]) {
+    const R third = R(1.) / R(3.);
+    R t[6];
     t[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
     t[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
     t[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
@@ -104,7 +106,7 @@ __device__ inline void eigen_terms(const Params& P, const StageIO& io, long c, c
     t[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz;
     t[5] = mt.l111_15 * my * mx + mt.Q44 * py * px;
     if (P.afm) {
-        double a1x, a1y, a1z, a2x, a2y, a2z;
+        R a1x, a1y, a1z, a2x, a2y, a2z;
         glb2crt(P, io.a1_in.c[0][c], io.a1_in.c[1][c], io.a1_in.c[2][c], a1x, a1y, a1z);
         glb2crt(P, io.a2_in.c[0][c], io.a2_in.c[1][c], io.a2_in.c[2][c], a2x, a2y, a2z);
         t[0] = t[0] + mt.l100a1_075 * (a1x * a1x - third) + mt.l100a2_075 * (a2x * a2x - third);
@@ -119,25 +121,27 @@ __device__ inline void eigen_terms(const Params& P, const StageIO& io, long c, c
 
 // dynamic eigenstrain of cell c in the crystal frame (Dexx0_crt ...,
 // get_eigenstrain_dynamic)
-__device__ inline void eigen_crt(const Params& P, const StageIO& io, long c, double e[6]) {
+template <class R>
+__device__ inline void eigen_crt(const Params& P, const StageIOT<R>& io, long c, R e[6]) {
     const uint8_t id = io.mid[c];
-    for (int a = 0; a < 6; a++) e[a] = 0.;
+    for (int a = 0; a < 6; a++) e[a] = R(0.);
     if (id == 0) return;
-    const DevMat& mt = io.mats[id - 1];
-    double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
+    const DevMatT<R>& mt = io.mats[id - 1];
+    R px = R(0.), py = R(0.), pz = R(0.), mx = R(0.), my = R(0.), mz = R(0.);
     if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
     if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
-    double e0[6] = {0., 0., 0., 0., 0., 0.};
+    R e0[6] = {R(0.), R(0.), R(0.), R(0.), R(0.), R(0.)};
     if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
     eigen_terms(P, io, c, mt, mx, my, mz, px, py, pz, e0, e);
 }
 
 // eigenstrain in the global frame (Dexx0_glb ...)
-__device__ inline void eigen_glb(const Params& P, const StageIO& io, long c, double e[6]) {
+template <class R>
+__device__ inline void eigen_glb(const Params& P, const StageIOT<R>& io, long c, R e[6]) {
     eigen_crt(P, io, c, e);
     if (P.rot) {
-        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
-        rot_tensor(P.Tc2g, s, o);
+        R s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
+        rot_tensor(Tc2g<R>(P), s, o);
         e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
     }
 }
@@ -162,11 +166,12 @@ __device__ inline void eigen_glb(const Params& P, const StageIO& io, long c, dou
 // ---------------------------------------------------------------------------
 
 // elastic constants of one material, staged in shared memory
+template <class R>
 struct ElMat {
-    double cij[6][6];
-    double dens_dt, mass_damp, stiff_damp;
-    double l100_15, l111_15, Q11, Q12, Q44;
-    double l100a1_075, l100a2_075, l111a1_075, l111a2_075;
+    R cij[6][6];
+    R dens_dt, mass_damp, stiff_damp;
+    R l100_15, l111_15, Q11, Q12, Q44;
+    R l100a1_075, l100a2_075, l111a1_075, l111a2_075;
     uint32_t flags;
     int cubic_c;
 };
@@ -180,11 +185,14 @@ constexpr int FYR = TJ + 1, FZC = TK + 1;    // face stresses: y-faces j0..j0+TJ
 constexpr int kU = 3 * UR * UC, kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
 constexpr int kFY = 3 * FYR * TK, kFZ = 3 * TJ * FZC;
 constexpr int kDoubles = 2 * kU + 2 * kGX + kGY + kGZ + kD0 + kFY + kFZ;
-constexpr size_t kFixedBytes = (size_t)kDoubles * sizeof(double) + (size_t)(2 * UR + UC) * sizeof(int)
+// kDoubles counts reals of the kernel's type R (FP64 or FP32)
+template <class R>
+constexpr size_t kFixedBytes = (size_t)kDoubles * sizeof(R) + (size_t)(2 * UR + UC) * sizeof(int)
                                + (size_t)(2 * UR * UC + HJ * HK);
-constexpr size_t kMatOffset = (kFixedBytes + 15) / 16 * 16;
-inline size_t smem_bytes(int nmat) { return kMatOffset + (size_t)nmat * sizeof(ElMat); }
-constexpr size_t kMaxSmemBytes = kMatOffset + (size_t)kMaxMat * sizeof(ElMat);
+template <class R>
+constexpr size_t kMatOffset = (kFixedBytes<R> + 15) / 16 * 16;
+template <class R>
+inline size_t smem_bytes(int nmat) { return kMatOffset<R> + (size_t)nmat * sizeof(ElMat<R>); }
 }  // namespace etile
 
 // index x in [-n, 2n) wrapped into [0, n)
@@ -200,13 +208,13 @@ __host__ __device__ constexpr int face_row(int d, int r) {
 // (mathlib.cpp:127-135); zero entries of the cubic pattern are skipped,
 // which leaves every partial sum unchanged.  CUB: every material of the
 // run has the cubic pattern.
-template <bool CUB, class M>
-__device__ inline double stress_row(const M& m, const double e[6], int r) {
+template <bool CUB, class M, class R>
+__device__ inline R stress_row(const M& m, const R e[6], int r) {
     if (CUB || m.cubic_c) {
         if (r < 3) return m.cij[r][0] * e[0] + m.cij[r][1] * e[1] + m.cij[r][2] * e[2];
         return m.cij[r][r] * e[r];
     }
-    double acc = 0.;
+    R acc = R(0.);
 #pragma unroll
     for (int q = 0; q < 6; q++) acc = acc + m.cij[r][q] * e[q];
     return acc;
@@ -214,133 +222,145 @@ __device__ inline double stress_row(const M& m, const double e[6], int r) {
 
 // global-frame dynamic eigenstrain of cell c with material constants mt
 // (get_eigenstrain_dynamic; eigen_glb with the constants taken from mt)
-template <class M>
-__device__ inline void eigen_glb_m(const Params& P, const StageIO& io, long c, const M& mt, double e[6]) {
-    double px = 0., py = 0., pz = 0., mx = 0., my = 0., mz = 0.;
+template <class R, class M>
+__device__ inline void eigen_glb_m(const Params& P, const StageIOT<R>& io, long c, const M& mt, R e[6]) {
+    R px = R(0.), py = R(0.), pz = R(0.), mx = R(0.), my = R(0.), mz = R(0.);
     if (P.fe) glb2crt(P, io.p_in.c[0][c], io.p_in.c[1][c], io.p_in.c[2][c], px, py, pz);
     if (P.fm) glb2crt(P, io.m_in.c[0][c], io.m_in.c[1][c], io.m_in.c[2][c], mx, my, mz);
-    double e0[6] = {0., 0., 0., 0., 0., 0.};
+    R e0[6] = {R(0.), R(0.), R(0.), R(0.), R(0.), R(0.)};
     if (io.eig0_c[0]) for (int a = 0; a < 6; a++) e0[a] = io.eig0_c[a][c];
     eigen_terms(P, io, c, mt, mx, my, mz, px, py, pz, e0, e);
     if (P.rot) {
-        double s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
-        rot_tensor(P.Tc2g, s, o);
+        R s[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o[3][3];
+        rot_tensor(Tc2g<R>(P), s, o);
         e[0] = o[0][0]; e[1] = o[1][1]; e[2] = o[2][2]; e[3] = o[1][2]; e[4] = o[0][2]; e[5] = o[0][1];
     }
 }
 
 // gradients of a cell held in the shared tile: gm(d,a) on the -d face,
 // gp(d,a) on the +d face, d0(a) the global-frame eigenstrain
+template <class R>
 struct TileCell {
-    const double *gxm, *gxp, *gy, *gz, *d0s;
+    const R *gxm, *gxp, *gy, *gz, *d0s;
     int r, s;
-    __device__ double gm(int d, int a) const {
+    __device__ R gm(int d, int a) const {
         using namespace etile;
         return d == 0 ? gxm[(a * HJ + r) * HK + s] : (d == 1 ? gy[(a * GYR + r) * HK + s] : gz[(a * HJ + r) * GZC + s]);
     }
-    __device__ double gp(int d, int a) const {
+    __device__ R gp(int d, int a) const {
         using namespace etile;
         return d == 0 ? gxp[(a * HJ + r) * HK + s] : (d == 1 ? gy[(a * GYR + r + 1) * HK + s] : gz[(a * HJ + r) * GZC + s + 1]);
     }
-    __device__ double d0(int a) const { return d0s[(a * etile::HJ + r) * etile::HK + s]; }
+    __device__ R d0(int a) const { return d0s[(a * etile::HJ + r) * etile::HK + s]; }
 };
 
 // the same quantities read from global memory (face gradients recomputed as
 // k_face_grad does); used for the k == ny-1 neighbour of the z-face quirk
+template <class R>
 struct GlobalCell {
     const Params& P;
-    const StageIO& io;
+    const StageIOT<R>& io;
     long i, j, k;
-    double d0v[6];
-    __device__ GlobalCell(const Params& p, const StageIO& s, long i_, long j_, long k_) : P(p), io(s), i(i_), j(j_), k(k_) {
-        if (P.elasto_back) eigen_glb(P, io, cid(P, i, j, k), d0v); else for (int a = 0; a < 6; a++) d0v[a] = 0.;
+    R d0v[6];
+    __device__ GlobalCell(const Params& p, const StageIOT<R>& s, long i_, long j_, long k_) : P(p), io(s), i(i_), j(j_), k(k_) {
+        if (P.elasto_back) eigen_glb(P, io, cid(P, i, j, k), d0v); else for (int a = 0; a < 6; a++) d0v[a] = R(0.);
     }
-    __device__ double grad(int d, int a, long ci, long cj, long ck) const {
-        const double* u = io.u_in.c[a];
+    __device__ R grad(int d, int a, long ci, long cj, long ck) const {
+        const R* u = io.u_in.c[a];
         const long c = cid(P, ci, cj, ck);
-        if (d == 0) return free_x(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci == 0 ? P.nx - 1 : ci - 1, cj, ck)]), P.dx, P.rdx);
-        if (d == 1) return free_y(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci, cj == 0 ? P.ny - 1 : cj - 1, ck)]), P.dy, P.rdy);
-        return free_z(P, io.mid, ci, cj, ck) ? 0. : qdiv((u[c] - u[cid(P, ci, cj, ck == 0 ? P.nz - 1 : ck - 1)]), P.dz, P.rdz);
+        if (d == 0) return free_x(P, io.mid, ci, cj, ck) ? R(0.) : qdivR((u[c] - u[cid(P, ci == 0 ? P.nx - 1 : ci - 1, cj, ck)]), P.dx, P.rdx, P.f.rdx);
+        if (d == 1) return free_y(P, io.mid, ci, cj, ck) ? R(0.) : qdivR((u[c] - u[cid(P, ci, cj == 0 ? P.ny - 1 : cj - 1, ck)]), P.dy, P.rdy, P.f.rdy);
+        return free_z(P, io.mid, ci, cj, ck) ? R(0.) : qdivR((u[c] - u[cid(P, ci, cj, ck == 0 ? P.nz - 1 : ck - 1)]), P.dz, P.rdz, P.f.rdz);
     }
-    __device__ double gm(int d, int a) const { return grad(d, a, i, j, k); }
-    __device__ double gp(int d, int a) const {
+    __device__ R gm(int d, int a) const { return grad(d, a, i, j, k); }
+    __device__ R gp(int d, int a) const {
         if (d == 0) return grad(0, a, i == P.nx - 1 ? 0 : i + 1, j, k);
         if (d == 1) return grad(1, a, i, j == P.ny - 1 ? 0 : j + 1, k);
         return grad(2, a, i, j, k == P.nz - 1 ? 0 : k + 1);
     }
-    __device__ double d0(int a) const { return d0v[a]; }
+    __device__ R d0(int a) const { return d0v[a]; }
 };
 
 // One cell's contribution to the stress rows of a face normal to D; ga is
 // the face's gradient of the normal displacement component, gb and gc those
 // of the two tangential components (x-face: u_z, u_y; y-face: u_z, u_x;
 // z-face: u_y, u_x).
-template <int D, bool CUB, class V, class M>
-__device__ inline void side_rows(const V& v, const M& m, double ga, double gb, double gc, double out[3]) {
-    double st[6];
+template <int D, bool CUB, class V, class M, class R>
+__device__ inline void side_rows(const V& v, const M& m, R ga, R gb, R gc, R out[3]) {
+    R st[6];
     if (D == 0) {
         st[0] = ga - v.d0(0);
-        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / 2. - v.d0(1);
-        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / 2. - v.d0(2);
-        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + v.gm(1, 2) + v.gp(1, 2)) / 4. - v.d0(3)) * 2.;
-        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + gb * 2.) / 4. - v.d0(4)) * 2.;
-        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + gc * 2.) / 4. - v.d0(5)) * 2.;
+        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / R(2.) - v.d0(1);
+        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / R(2.) - v.d0(2);
+        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + v.gm(1, 2) + v.gp(1, 2)) / R(4.) - v.d0(3)) * R(2.);
+        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + gb * R(2.)) / R(4.) - v.d0(4)) * R(2.);
+        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + gc * R(2.)) / R(4.) - v.d0(5)) * R(2.);
     } else if (D == 1) {
-        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / 2. - v.d0(0);
+        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / R(2.) - v.d0(0);
         st[1] = ga - v.d0(1);
-        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / 2. - v.d0(2);
-        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + gb * 2.) / 4. - v.d0(3)) * 2.;
-        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + v.gm(0, 2) + v.gp(0, 2)) / 4. - v.d0(4)) * 2.;
-        st[5] = ((gc * 2. + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
+        st[2] = (v.gm(2, 2) + v.gp(2, 2)) / R(2.) - v.d0(2);
+        st[3] = ((v.gm(2, 1) + v.gp(2, 1) + gb * R(2.)) / R(4.) - v.d0(3)) * R(2.);
+        st[4] = ((v.gm(2, 0) + v.gp(2, 0) + v.gm(0, 2) + v.gp(0, 2)) / R(4.) - v.d0(4)) * R(2.);
+        st[5] = ((gc * R(2.) + v.gm(0, 1) + v.gp(0, 1)) / R(4.) - v.d0(5)) * R(2.);
     } else {
-        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / 2. - v.d0(0);
-        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / 2. - v.d0(1);
+        st[0] = (v.gm(0, 0) + v.gp(0, 0)) / R(2.) - v.d0(0);
+        st[1] = (v.gm(1, 1) + v.gp(1, 1)) / R(2.) - v.d0(1);
         st[2] = ga - v.d0(2);
-        st[3] = ((gb * 2. + v.gm(1, 2) + v.gp(1, 2)) / 4. - v.d0(3)) * 2.;
-        st[4] = ((gc * 2. + v.gm(0, 2) + v.gp(0, 2)) / 4. - v.d0(4)) * 2.;
-        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + v.gm(0, 1) + v.gp(0, 1)) / 4. - v.d0(5)) * 2.;
+        st[3] = ((gb * R(2.) + v.gm(1, 2) + v.gp(1, 2)) / R(4.) - v.d0(3)) * R(2.);
+        st[4] = ((gc * R(2.) + v.gm(0, 2) + v.gp(0, 2)) / R(4.) - v.d0(4)) * R(2.);
+        st[5] = ((v.gm(1, 0) + v.gp(1, 0) + v.gm(0, 1) + v.gp(0, 1)) / R(4.) - v.d0(5)) * R(2.);
     }
 #pragma unroll
     for (int r = 0; r < 3; r++) out[r] = stress_row<CUB>(m, st, face_row(D, r));
 }
 
 // RK4 combination for v and u of one cell (du = v_stage * dt)
-template <int S>
-__device__ inline void rk_vu(const StageIO& io, long c, const double dv[3], double dt) {
+template <int S, class R>
+__device__ inline void rk_vu(const StageIOT<R>& io, long c, const R dv[3], double dt, float dtf) {
+    if constexpr (is_mixed<R>::value) {
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const double du = io.v_in.c[a][c] * dt;
-        if (S == 0) {
-            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + qdiv(dv[a], 6., kInv6);
-            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + qdiv(du, 6., kInv6);
-        } else if (S == 1) {
-            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
-            io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
-        } else if (S == 2) {
-            const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-            io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
-            io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
-        } else {
-            io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 6., kInv6);
-            io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 6., kInv6);
+        for (int a = 0; a < 3; a++) {
+            const float du = io.v_in.c[a][c] * dtf;
+            rk_mixed<S>(io.v_x.c[a][c], dv[a], io.v_out.c[a], io.v_acc.c[a], io.v_cmp.c[a], (int)c);
+            rk_mixed<S>(io.u_x.c[a][c], du, io.u_out.c[a], io.u_acc.c[a], io.u_cmp.c[a], (int)c);
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const double du = io.v_in.c[a][c] * dt;
+            if (S == 0) {
+                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
+                io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + qdiv(dv[a], 6., kInv6);
+                io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + qdiv(du, 6., kInv6);
+            } else if (S == 1) {
+                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
+                io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
+                io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
+            } else if (S == 2) {
+                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
+                io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
+                io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
+            } else {
+                io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 6., kInv6);
+                io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 6., kInv6);
+            }
         }
     }
 }
 
 // Shared-memory plan of k_elastic_tile: every array sits at a compile-time
 // offset from the dynamic base; the material table (sized at launch) is last.
+template <class R>
 struct ETileSmem {
     unsigned char* base;
-    __device__ double* dp() const { return reinterpret_cast<double*>(base); }
-    __device__ double* u(int slot) const { return dp() + slot * etile::kU; }
-    __device__ double* gx(int slot) const { return dp() + 2 * etile::kU + slot * etile::kGX; }
-    __device__ double* gy() const { return dp() + 2 * etile::kU + 2 * etile::kGX; }
-    __device__ double* gz() const { return gy() + etile::kGY; }
-    __device__ double* d0() const { return gz() + etile::kGZ; }
-    __device__ double* fy() const { return d0() + etile::kD0; }
-    __device__ double* fz() const { return fy() + etile::kFY; }
+    __device__ R* dp() const { return reinterpret_cast<R*>(base); }
+    __device__ R* u(int slot) const { return dp() + slot * etile::kU; }
+    __device__ R* gx(int slot) const { return dp() + 2 * etile::kU + slot * etile::kGX; }
+    __device__ R* gy() const { return dp() + 2 * etile::kU + 2 * etile::kGX; }
+    __device__ R* gz() const { return gy() + etile::kGY; }
+    __device__ R* d0() const { return gz() + etile::kGZ; }
+    __device__ R* fy() const { return d0() + etile::kD0; }
+    __device__ R* fz() const { return fy() + etile::kFY; }
     __device__ int* ip() const { return reinterpret_cast<int*>(dp() + etile::kDoubles); }
     __device__ int* rowoff() const { return ip(); }
     __device__ int* rowj() const { return ip() + etile::UR; }
@@ -348,18 +368,19 @@ struct ETileSmem {
     __device__ uint8_t* bp() const { return reinterpret_cast<uint8_t*>(ip() + 2 * etile::UR + etile::UC); }
     __device__ uint8_t* id(int slot) const { return bp() + slot * etile::UR * etile::UC; }
     __device__ uint8_t* idc() const { return bp() + 2 * etile::UR * etile::UC; }
-    __device__ ElMat* mat() const { return reinterpret_cast<ElMat*>(base + etile::kMatOffset); }
+    __device__ ElMat<R>* mat() const { return reinterpret_cast<ElMat<R>*>(base + etile::kMatOffset<R>); }
 };
 
 // Staging of plane pw into ring slot `slot`: the u copies go out as cp.async
 // (no register or stall while they fly), the ids are loaded into registers
 // and stored by etile_stage_finish, which also waits for the copies.
 constexpr int kStageItems = (etile::UR * etile::UC + etile::NT - 1) / etile::NT;
-__device__ inline void etile_stage_issue(const Params& P, const StageIO& io, const ETileSmem& sm, int slot, int pw,
+template <class R>
+__device__ inline void etile_stage_issue(const Params& P, const StageIOT<R>& io, const ETileSmem<R>& sm, int slot, int pw,
                                          uint8_t idp[kStageItems]) {
     using namespace etile;
     const int po = pw * P.ny * P.nz;
-    double* su = sm.u(slot);
+    R* su = sm.u(slot);
 #pragma unroll
     for (int t = 0; t < kStageItems; t++) {
         const int it = threadIdx.x + t * NT;
@@ -368,12 +389,13 @@ __device__ inline void etile_stage_issue(const Params& P, const StageIO& io, con
             const int c = po + sm.rowoff()[ur] + sm.colk()[uc];
             idp[t] = io.mid[c];
 #pragma unroll
-            for (int a = 0; a < 3; a++) cp_async8(&su[a * UR * UC + it], &io.u_in.c[a][c]);
+            for (int a = 0; a < 3; a++) cp_async_elem(&su[a * UR * UC + it], &io.u_in.c[a][c]);
         }
     }
     cp_async_commit();
 }
-__device__ inline void etile_stage_finish(const ETileSmem& sm, int slot, const uint8_t idp[kStageItems]) {
+template <class R>
+__device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, const uint8_t idp[kStageItems]) {
     using namespace etile;
     uint8_t* sid = sm.id(slot);
 #pragma unroll
@@ -384,11 +406,11 @@ __device__ inline void etile_stage_finish(const ETileSmem& sm, int slot, const u
     cp_async_wait_all();
 }
 
-template <int S, bool CUB>
-__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO io, int chunk, int nmat) {
+template <int S, bool CUB, class R = double>
+__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat) {
     using namespace etile;
     GF_EXTERN_SMEM(unsigned char, smem_raw);
-    const ETileSmem sm{smem_raw};
+    const ETileSmem<R> sm{smem_raw};
 
     const int tid = threadIdx.x;
     const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
@@ -407,8 +429,8 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 
     // ---- block set-up: material table, wrapped row/column offsets, first two planes ----
     for (int it = tid; it < nmat; it += blockDim.x) {
-        const DevMat& d = io.mats[it];
-        ElMat& e = sm.mat()[it];
+        const DevMatT<R>& d = io.mats[it];
+        ElMat<R>& e = sm.mat()[it];
         for (int a = 0; a < 6; a++) for (int b = 0; b < 6; b++) e.cij[a][b] = d.cij[a][b];
         e.dens_dt = d.dens_dt; e.mass_damp = d.mass_damp; e.stiff_damp = d.stiff_damp;
         e.l100_15 = d.l100_15; e.l111_15 = d.l111_15; e.Q11 = d.Q11; e.Q12 = d.Q12; e.Q44 = d.Q44;
@@ -435,9 +457,9 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
     __syncthreads();
     uint8_t idp[kStageItems];          // ids of the plane being staged
 
-    double sa[3] = {0., 0., 0.};       // lower cell's half of the next x-face stress
-    double sxp[3] = {0., 0., 0.};      // stress on the previous x-face
-    double ty[3] = {0., 0., 0.}, tz[3] = {0., 0., 0.};
+    R sa[3] = {R(0.), R(0.), R(0.)};       // lower cell's half of the next x-face stress
+    R sxp[3] = {R(0.), R(0.), R(0.)};      // stress on the previous x-face
+    R ty[3] = {R(0.), R(0.), R(0.)}, tz[3] = {R(0.), R(0.), R(0.)};
     uint8_t mid_prev = 0;
 
     for (int q = 0; q <= L + 1; q++) {
@@ -445,12 +467,12 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
         const int pw = wrapm(p, P.nx);
         const int po = pw * nyz;
         const int cur = q & 1, nxt = cur ^ 1;           // ring slots of planes p and p+1
-        const double* uc = sm.u(cur);
-        const double* un = sm.u(nxt);
+        const R* uc = sm.u(cur);
+        const R* un = sm.u(nxt);
         const uint8_t* ic = sm.id(cur);
         const uint8_t* in = sm.id(nxt);
-        double* gxc = sm.gx(cur ^ 1);                    // face p   (computed in the previous pass)
-        double* gxn = sm.gx(cur);                        // face p+1
+        R* gxc = sm.gx(cur ^ 1);                    // face p   (computed in the previous pass)
+        R* gxn = sm.gx(cur);                        // face p+1
         // ---- A: gradients and eigenstrains of plane p ----
         if (q <= L) {
             const int f = p + 1;
@@ -461,7 +483,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                 const bool fr = fb || !(ic[ui] != 0 && in[ui] != 0);
 #pragma unroll
                 for (int a = 0; a < 3; a++)
-                    gxn[a * HJ * HK + it] = fr ? 0. : qdiv((un[a * UR * UC + ui] - uc[a * UR * UC + ui]), P.dx, P.rdx);
+                    gxn[a * HJ * HK + it] = fr ? R(0.) : qdivR((un[a * UR * UC + ui] - uc[a * UR * UC + ui]), P.dx, P.rdx, P.f.rdx);
             }
         }
         for (int it = tid; it < GYR * HK; it += blockDim.x) {
@@ -470,7 +492,7 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             const bool fr = (sm.rowj()[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gy()[a * GYR * HK + it] = fr ? 0. : qdiv((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dy, P.rdy);
+                sm.gy()[a * GYR * HK + it] = fr ? R(0.) : qdivR((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dy, P.rdy, P.f.rdy);
         }
         for (int it = tid; it < HJ * GZC; it += blockDim.x) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
@@ -478,13 +500,13 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             const bool fr = (sm.colk()[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gz()[a * HJ * GZC + it] = fr ? 0. : qdiv((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dz, P.rdz);
+                sm.gz()[a * HJ * GZC + it] = fr ? R(0.) : qdivR((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dz, P.rdz, P.f.rdz);
         }
         for (int it = tid; it < HJ * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
             const uint8_t id = ic[(rr + 1) * UC + ss + 1];
             sm.idc()[it] = id;
-            double e[6] = {0., 0., 0., 0., 0., 0.};
+            R e[6] = {R(0.), R(0.), R(0.), R(0.), R(0.), R(0.)};
             if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff()[rr + 1] + sm.colk()[ss + 1], sm.mat()[id - 1], e);
 #pragma unroll
             for (int a = 0; a < 6; a++) sm.d0()[a * HJ * HK + it] = e[a];
@@ -500,17 +522,17 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                 const int fr_ = it / TK, fc = it - (it / TK) * TK;       // face j0+fr_, column k0+fc
                 const int f = j0 + fr_;
                 const uint8_t ia = sm.idc()[fr_ * HK + fc + 1], ib = sm.idc()[(fr_ + 1) * HK + fc + 1];
-                double o[3] = {0., 0., 0.};
+                R o[3] = {R(0.), R(0.), R(0.)};
                 if (!(((f == 0 || f == P.ny) && !P.per_y) || !(ia != 0 && ib != 0))) {
                     const int g = (fr_ + 1) * HK + fc + 1;
-                    const double ga = sm.gy()[1 * GYR * HK + g], gb = sm.gy()[2 * GYR * HK + g], gc = sm.gy()[g];
-                    const TileCell lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_, fc + 1};
-                    const TileCell hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_ + 1, fc + 1};
-                    double a1[3], a2[3];
+                    const R ga = sm.gy()[1 * GYR * HK + g], gb = sm.gy()[2 * GYR * HK + g], gc = sm.gy()[g];
+                    const TileCell<R> lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_, fc + 1};
+                    const TileCell<R> hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), fr_ + 1, fc + 1};
+                    R a1[3], a2[3];
                     side_rows<1, CUB>(lo, sm.mat()[ia - 1], ga, gb, gc, a1);
                     side_rows<1, CUB>(hi, sm.mat()[ib - 1], ga, gb, gc, a2);
 #pragma unroll
-                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / R(2.);
                 }
 #pragma unroll
                 for (int a = 0; a < 3; a++) sm.fy()[a * FYR * TK + it] = o[a];
@@ -520,17 +542,17 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                 const int f = k0 + fc;
                 const int rr = rl + 1;
                 const uint8_t ia = sm.idc()[rr * HK + fc], ib = sm.idc()[rr * HK + fc + 1];
-                double o[3] = {0., 0., 0.};
+                R o[3] = {R(0.), R(0.), R(0.)};
                 if (!(((f == 0 || f == P.nz) && !P.per_z) || !(ia != 0 && ib != 0))) {
                     const int g = rr * GZC + fc + 1;
-                    const double ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
-                    const TileCell lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc};
-                    const TileCell hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc + 1};
-                    double a1[3], a2[3];
+                    const R ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
+                    const TileCell<R> lo{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc};
+                    const TileCell<R> hi{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), rr, fc + 1};
+                    R a1[3], a2[3];
                     side_rows<2, CUB>(lo, sm.mat()[ia - 1], ga, gb, gc, a1);
                     side_rows<2, CUB>(hi, sm.mat()[ib - 1], ga, gb, gc, a2);
 #pragma unroll
-                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / 2.;
+                    for (int a = 0; a < 3; a++) o[a] = (a1[a] + a2[a]) / R(2.);
                 }
 #pragma unroll
                 for (int a = 0; a < 3; a++) sm.fz()[a * TJ * FZC + iz] = o[a];
@@ -541,26 +563,26 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 
         // ---- B2: one column per thread ----
         if (valid) {
-            const TileCell me{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), r, s};
+            const TileCell<R> me{gxc, gxn, sm.gy(), sm.gz(), sm.d0(), r, s};
             const uint8_t id = sm.idc()[r * HK + s];
             // x-face p: between planes p-1 and p
             if (q >= 1) {
-                double sx[3] = {0., 0., 0.};
+                R sx[3] = {R(0.), R(0.), R(0.)};
                 const bool fr = ((p == 0 || p == P.nx) && !P.per_x) || !(mid_prev != 0 && id != 0);
                 if (!fr) {
                     const int g = r * HK + s;
-                    const double ga = gxc[g], gb = gxc[2 * HJ * HK + g], gc = gxc[HJ * HK + g];
-                    double sb[3];
+                    const R ga = gxc[g], gb = gxc[2 * HJ * HK + g], gc = gxc[HJ * HK + g];
+                    R sb[3];
                     side_rows<0, CUB>(me, sm.mat()[id - 1], ga, gb, gc, sb);
 #pragma unroll
-                    for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / 2.;
+                    for (int a = 0; a < 3; a++) sx[a] = (sa[a] + sb[a]) / R(2.);
                 }
                 if (q >= 2 && mid_prev != 0) {
                     // cell (p-1, j, k) is complete: its stress divergence
                     const long c = (long)(p - 1) * nyz + (long)j * P.nz + k;
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        const double tx = qdiv((sx[a] - sxp[a]), P.dx, P.rdx);
+                        const R tx = qdivR((sx[a] - sxp[a]), P.dx, P.rdx, P.f.rdx);
                         io.force.c[a][c] = tx + ty[a] + tz[a];
                     }
                 }
@@ -569,14 +591,14 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
             }
             if (q >= 1 && q <= L) {
                 if (id != 0) {
-                    double s1[3], s2[3];
+                    R s1[3], s2[3];
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
                         s1[a] = sm.fy()[(a * FYR + jl) * TK + kl];
                         s2[a] = sm.fy()[(a * FYR + jl + 1) * TK + kl];
                     }
 #pragma unroll
-                    for (int a = 0; a < 3; a++) ty[a] = qdiv((s2[a] - s1[a]), P.dy, P.rdy);
+                    for (int a = 0; a < 3; a++) ty[a] = qdivR((s2[a] - s1[a]), P.dy, P.rdy, P.f.rdy);
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
                         s1[a] = sm.fz()[(a * TJ + jl) * FZC + kl];
@@ -587,37 +609,37 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                         const bool top_free = ((k + 1 == P.nz) && !P.per_z) || !(id != 0 && iu != 0);
                         if (top_free && traction_here) {
                             // surface traction: x -> xz, y -> yz, z -> zz
-                            const double tr = stage_drive(io, S).traction;
-                            s2[0] = s2[1] = s2[2] = 0.;
+                            const R tr = stage_drive(io, S).traction;
+                            s2[0] = s2[1] = s2[2] = R(0.);
                             if (P.strain_comp == 0) s2[0] = tr; else if (P.strain_comp == 1) s2[1] = tr; else s2[2] = tr;
                         } else if (!top_free && quirk) {
                             // the reference's +z neighbour of k == ny-1 is k = 0
                             // (elastic_dynamic_solver.cpp:1247); creation rejects
                             // decks where that cell is vacuum
                             const int g = r * GZC + s + 1;
-                            const double ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
-                            const GlobalCell nb(P, io, pw, j, 0);
-                            double a1[3], a2[3];
+                            const R ga = sm.gz()[2 * HJ * GZC + g], gb = sm.gz()[1 * HJ * GZC + g], gc = sm.gz()[g];
+                            const GlobalCell<R> nb(P, io, pw, j, 0);
+                            R a1[3], a2[3];
                             side_rows<2, CUB>(me, sm.mat()[id - 1], ga, gb, gc, a1);
                             side_rows<2, CUB>(nb, sm.mat()[io.mid[(long)po + (long)j * P.nz] - 1], ga, gb, gc, a2);
 #pragma unroll
-                            for (int a = 0; a < 3; a++) s2[a] = (a1[a] + a2[a]) / 2.;
+                            for (int a = 0; a < 3; a++) s2[a] = (a1[a] + a2[a]) / R(2.);
                         }
                     }
 #pragma unroll
-                    for (int a = 0; a < 3; a++) tz[a] = qdiv((s2[a] - s1[a]), P.dz, P.rdz);
+                    for (int a = 0; a < 3; a++) tz[a] = qdivR((s2[a] - s1[a]), P.dz, P.rdz, P.f.rdz);
                     // cell strain for the magnetic and ferroelectric kernels
                     if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_AFM | MF_FE))) {
-                        double e[6];
-                        e[0] = (me.gm(0, 0) + me.gp(0, 0)) / 2.;
-                        e[1] = (me.gm(1, 1) + me.gp(1, 1)) / 2.;
-                        e[2] = (me.gm(2, 2) + me.gp(2, 2)) / 2.;
-                        e[3] = (me.gm(2, 1) + me.gp(2, 1) + me.gm(1, 2) + me.gp(1, 2)) / 4.;
-                        e[4] = (me.gm(2, 0) + me.gp(2, 0) + me.gm(0, 2) + me.gp(0, 2)) / 4.;
-                        e[5] = (me.gm(1, 0) + me.gp(1, 0) + me.gm(0, 1) + me.gp(0, 1)) / 4.;
+                        R e[6];
+                        e[0] = (me.gm(0, 0) + me.gp(0, 0)) / R(2.);
+                        e[1] = (me.gm(1, 1) + me.gp(1, 1)) / R(2.);
+                        e[2] = (me.gm(2, 2) + me.gp(2, 2)) / R(2.);
+                        e[3] = (me.gm(2, 1) + me.gp(2, 1) + me.gm(1, 2) + me.gp(1, 2)) / R(4.);
+                        e[4] = (me.gm(2, 0) + me.gp(2, 0) + me.gm(0, 2) + me.gp(0, 2)) / R(4.);
+                        e[5] = (me.gm(1, 0) + me.gp(1, 0) + me.gm(0, 1) + me.gp(0, 1)) / R(4.);
                         if (P.rot) {
-                            double t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
-                            rot_tensor(P.Tg2c, t3, o3);
+                            R t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
+                            rot_tensor(Tg2c<R>(P), t3, o3);
                             e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
                         }
                         const long c = (long)po + (long)j * P.nz + k;
@@ -626,13 +648,13 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
                     }
                 } else {
 #pragma unroll
-                    for (int a = 0; a < 3; a++) ty[a] = tz[a] = 0.;
+                    for (int a = 0; a < 3; a++) ty[a] = tz[a] = R(0.);
                 }
             }
             // lower cell's half of x-face p+1
             if (q <= L && id != 0) {
                 const int g = r * HK + s;
-                const double ga = gxn[g], gb = gxn[2 * HJ * HK + g], gc = gxn[HJ * HK + g];
+                const R ga = gxn[g], gb = gxn[2 * HJ * HK + g], gc = gxn[HJ * HK + g];
                 side_rows<0, CUB>(me, sm.mat()[id - 1], ga, gb, gc, sa);
             }
             mid_prev = id;
@@ -648,37 +670,38 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 // f_store := f in stage 1 only), then the RK4 combination of v and u.  A
 // streaming kernel at full occupancy, so these loads and stores overlap
 // across many warps instead of waiting inside the tiled kernel's phases.
-template <int S>
-__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIO io) {
+template <int S, class R = double>
+__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = io.mid[c];
-    double dv[3] = {0., 0., 0.};
+    R dv[3] = {R(0.), R(0.), R(0.)};
     if (id != 0) {
-        const DevMat& mt = io.mats[id - 1];
-        const double dens_dt = mt.dens_dt, mass_damp = mt.mass_damp, stiff_damp = mt.stiff_damp;
+        const DevMatT<R>& mt = io.mats[id - 1];
+        const R dens_dt = mt.dens_dt, mass_damp = mt.mass_damp, stiff_damp = mt.stiff_damp;
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            const double f = io.force.c[a][c];
-            const double fs = io.force_store.c[a][c];
+            const R f = io.force.c[a][c];
+            const R fs = io.force_store.c[a][c];
             if (S == 1 || S == 2)
-                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs) * 2.;
+                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs) * R(2.);
             else
                 dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs);
             if (S == 0) io.force_store.c[a][c] = f;
         }
     }
-    rk_vu<S>(io, c, dv, P.dt);
+    rk_vu<S>(io, c, dv, P.dt, P.f.dt);
 }
 
 // cell strain (global frame) of the current step for output (Dexx_glb ...)
-__global__ void k_cell_strain(Params P, StageIO io, double* out6) {
+template <class R = double>
+__global__ void k_cell_strain(Params P, StageIOT<R> io, double* out6) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long nyz = (long)P.ny * P.nz;
     const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
-    const GradView g(P, io);
-    double e[6];
+    const GradView<R> g(P, io);
+    R e[6];
     g.strain_glb(i, j, k, e);
     for (int a = 0; a < 6; a++) out6[(long)a * P.n + c] = e[a];
 }
@@ -687,8 +710,8 @@ __global__ void k_cell_strain(Params P, StageIO io, double* out6) {
 // For stages 0..2 `tgt` is the stage output (F_glb_store); for the last
 // stage it is the new step value and `old` the step-start value (the
 // reference's history copy Du?_glb_t1).
-template <int S>
-__global__ void k_elastic_bc(Params P, StageIO io) {
+template <int S, class R = double>
+__global__ void k_elastic_bc(Params P, StageIOT<R> io) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)P.nx * P.ny) return;
     const long i = t / P.ny, j = t - i * P.ny;
@@ -700,53 +723,60 @@ __global__ void k_elastic_bc(Params P, StageIO io) {
     if (!P.abc_1D) {
         // Liao 4th-order extrapolation on k = 0.  History slot h holds planes
         // k=1..4 of u at the start of step h (mod 4).
-        const double w = P.liao_w;
-        const double c1 = 4. * w + 2. * (1. - w), c2 = 6. * w + (1. - w), c3 = 4. * w;
+        const R w = P.liao_w;
+        const R c1 = R(4.) * w + R(2.) * (R(1.) - w), c2 = R(6.) * w + (R(1.) - w), c3 = R(4.) * w;
         if (S < 3) {
             // stages 1-3 rewrite u(k=0) with the value of the last full update
             for (int a = 0; a < 3; a++)
                 io.u_x.c[a][cid(P, i, j, 0)] = io.liao_last[a * plane + t];
         } else {
             // shift history: slot (step mod 4) <- planes 1..4 of the step-start u
-            double* slot = io.liao_hist + (size_t)(step & 3ull) * 12 * plane;
+            R* slot = io.liao_hist + (size_t)(step & 3ull) * 12 * plane;
             for (int a = 0; a < 3; a++)
                 for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = io.u_x.c[a][cid(P, i, j, p)];
-            const double* h1 = io.liao_hist + (size_t)((step + 0) & 3ull) * 12 * plane;   // t1 = u(step)
-            const double* h2 = io.liao_hist + (size_t)((step + 3) & 3ull) * 12 * plane;   // t2 = u(step-1)
-            const double* h3 = io.liao_hist + (size_t)((step + 2) & 3ull) * 12 * plane;   // t3 = u(step-2)
-            const double* h4 = io.liao_hist + (size_t)((step + 1) & 3ull) * 12 * plane;   // t4 = u(step-3)
+            const R* h1 = io.liao_hist + (size_t)((step + 0) & 3ull) * 12 * plane;   // t1 = u(step)
+            const R* h2 = io.liao_hist + (size_t)((step + 3) & 3ull) * 12 * plane;   // t2 = u(step-1)
+            const R* h3 = io.liao_hist + (size_t)((step + 2) & 3ull) * 12 * plane;   // t3 = u(step-2)
+            const R* h4 = io.liao_hist + (size_t)((step + 1) & 3ull) * 12 * plane;   // t4 = u(step-3)
             for (int a = 0; a < 3; a++) {
-                const double v = c1 * h1[(a * 4 + 0) * plane + t] - c2 * h2[(a * 4 + 1) * plane + t]
+                const R v = c1 * h1[(a * 4 + 0) * plane + t] - c2 * h2[(a * 4 + 1) * plane + t]
                                  + c3 * h3[(a * 4 + 2) * plane + t] - w * h4[(a * 4 + 3) * plane + t];
                 io.u_acc.c[a][cid(P, i, j, 0)] = v;
                 io.liao_last[a * plane + t] = v;
+                if constexpr (is_mixed<R>::value) io.u_cmp.c[a][cid(P, i, j, 0)] = R(0);
             }
         }
     } else {
         // first-order Mur on k = 0 (unless only the top is absorbing) and k = nz-1
         const double* cf = (S == 0 || S == 1) ? P.mur_el_half : P.mur_el_full;
-        const double cl1 = cf[0], ct1 = cf[1], cll = cf[2], ctl = cf[3];
+        const R cl1 = cf[0], ct1 = cf[1], cll = cf[2], ctl = cf[3];
         const long b0 = cid(P, i, j, 0), b1 = cid(P, i, j, 1), t0 = cid(P, i, j, nz - 1), t1 = cid(P, i, j, nz - 2);
         for (int a = 0; a < 3; a++) {
-            const double c1st = (a == 2) ? cl1 : ct1, clast = (a == 2) ? cll : ctl;
+            const R c1st = (a == 2) ? cl1 : ct1, clast = (a == 2) ? cll : ctl;
             if (S < 3) {
-                double* so = io.u_out.c[a];
-                const double* x = io.u_x.c[a];
+                R* so = io.u_out.c[a];
+                const R* x = io.u_x.c[a];
                 if (!P.abc_elast_onlytop) so[b0] = x[b1] + c1st * (x[b0] - so[b1]);
                 so[t0] = x[t1] + clast * (x[t0] - so[t1]);
             } else {
-                double* nw = io.u_acc.c[a];
-                const double* old = io.u_x.c[a];
+                R* nw = io.u_acc.c[a];
+                const R* old = io.u_x.c[a];
                 if (!P.abc_elast_onlytop) nw[b0] = old[b1] + c1st * (old[b0] - nw[b1]);
                 nw[t0] = old[t1] + clast * (old[t0] - nw[t1]);
+                if constexpr (is_mixed<R>::value) {
+                    if (!P.abc_elast_onlytop) io.u_cmp.c[a][b0] = R(0);
+                    io.u_cmp.c[a][t0] = R(0);
+                }
             }
         }
     }
 
     // displacement source on plane source_z (types 1 and 2)
     if (P.strain_pulse && dr.usrc_on && io.mid[cid(P, i, j, P.source_z)] != 0) {
-        double* tgt = (S < 3) ? io.u_out.c[P.strain_comp] : io.u_acc.c[P.strain_comp];
+        R* tgt = (S < 3) ? io.u_out.c[P.strain_comp] : io.u_acc.c[P.strain_comp];
         tgt[cid(P, i, j, P.source_z)] = dr.usrc;
+        if constexpr (is_mixed<R>::value)
+            if (S == 3) io.u_cmp.c[P.strain_comp][cid(P, i, j, P.source_z)] = R(0);
     }
 }
 

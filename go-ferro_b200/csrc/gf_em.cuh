@@ -1,4 +1,5 @@
-// Yee-grid Maxwell stage kernels (FP64).
+// Yee-grid Maxwell stage kernels (FP64 parity form; the Yee update, plane
+// source and Mur boundary also in the FP32 mixed form).
 //
 //   k_em_fused<S> one thread per Yee vertex, updating the E edges and H
 //                 faces that share its index:
@@ -27,35 +28,43 @@
 namespace gf {
 
 // per-material constants the Yee updates read, staged in shared memory
+template <class R>
 struct EmMat {
-    double er, cond, Ms, Ms1, Ms2;
+    R er, cond, Ms, Ms1, Ms2;
     uint32_t flags;
     int pad_;
 };
 
-// free current J_f of cell (i,j,k), component a, stage drive dr
-__device__ inline double jf_cell(const Params& P, const StageIO& io, const StageDrive& dr, int a, int i, int j, int k) {
-    if (!P.jf_on || a != P.jf_comp) return 0.;
-    if (i < P.jf_i0 || i > P.jf_i1 || j < P.jf_j0 || j > P.jf_j1 || k < P.jf_k0 || k > P.jf_k1) return 0.;
-    if (P.jf_type == 1 || P.jf_type == 2) return dr.jf * io.jf_kfac[k];
-    return dr.jf;
+// free current J_f of cell (i,j,k), component a; jf = the stage's amplitude
+template <class R>
+__device__ inline R jf_cell(const Params& P, const StageIOT<R>& io, R jf, int a, int i, int j, int k) {
+    if (!P.jf_on || a != P.jf_comp) return R(0.);
+    if (i < P.jf_i0 || i > P.jf_i1 || j < P.jf_j0 || j > P.jf_j1 || k < P.jf_k0 || k > P.jf_k1) return R(0.);
+    if (P.jf_type == 1 || P.jf_type == 2) return jf * io.jf_kfac[k];
+    return jf;
 }
 
-template <int S>
-__device__ inline void rk_x(double xv, double d, double* out, double* acc, int e) {
-    if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
-    else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
-    else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
-    else { acc[e] = acc[e] + qdiv(d, 6., kInv6); }
+template <int S, class R>
+__device__ inline void rk_x(R xv, R d, R* out, R* acc, R* cmp, int e) {
+    if constexpr (is_mixed<R>::value) {
+        rk_mixed<S>(xv, d, out, acc, cmp, e);
+    } else {
+        if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
+        else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
+        else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
+        else { acc[e] = acc[e] + qdiv(d, 6., kInv6); }
+    }
 }
 
 // E edge update of component C at edge (i,j,k) (index e in C's array).
-template <int S, int C>
-__device__ inline void em_E_edge(const Params& P, const StageIO& io, const StageDrive& dr, const EmMat* mt,
+template <int S, int C, class R>
+__device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const StageDrive& dr, const EmMat<R>* mt,
                                  int i, int j, int k, int e) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
+    R dt_r, dt_e0_r;
+    if constexpr (is_mixed<R>::value) { dt_r = P.f.dt; dt_e0_r = P.f.dt_e0; } else { dt_r = P.dt; dt_e0_r = P.dt_e0; }
 
-    double d = 0.;
+    R d = R(0.);
     bool boundary = false;
     int cx[4], cy[4], cz[4];
     // cell quadruples around the edge, in the reference's order 1..4
@@ -87,116 +96,121 @@ __device__ inline void em_E_edge(const Params& P, const StageIO& io, const Stage
 
     if (!boundary) {
         // curl of the stage H
-        double curl;
-        const double* Hx = io.H_in.c[0];
-        const double* Hy = io.H_in.c[1];
-        const double* Hz = io.H_in.c[2];
+        R curl;
+        const R* Hx = io.H_in.c[0];
+        const R* Hy = io.H_in.c[1];
+        const R* Hz = io.H_in.c[2];
         if (C == 0) {
-            const double dHzdy = qdiv((Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]), P.dy, P.rdy);
-            const double dHydz = qdiv((Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]), P.dz, P.rdz);
+            const R dHzdy = qdivR((Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]), P.dy, P.rdy, P.f.rdy);
+            const R dHydz = qdivR((Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]), P.dz, P.rdz, P.f.rdz);
             curl = dHzdy - dHydz;
         } else if (C == 1) {
-            const double dHxdz = qdiv((Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]), P.dz, P.rdz);
-            const double dHzdx = qdiv((Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]), P.dx, P.rdx);
+            const R dHxdz = qdivR((Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]), P.dz, P.rdz, P.f.rdz);
+            const R dHzdx = qdivR((Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]), P.dx, P.rdx, P.f.rdx);
             curl = dHxdz - dHzdx;
         } else {
-            const double dHydx = qdiv((Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]), P.dx, P.rdx);
-            const double dHxdy = qdiv((Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]), P.dy, P.rdy);
+            const R dHydx = qdivR((Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]), P.dx, P.rdx, P.f.rdx);
+            const R dHxdy = qdivR((Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]), P.dy, P.rdy, P.f.rdy);
             curl = dHydx - dHxdy;
         }
-        double Jf = 0., dP = 0., er = 0., cond = 0., pc = 0.;
+        R Jf = R(0.), dP = R(0.), er = R(0.), cond = R(0.), pc = R(0.);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
             const uint8_t id = io.mid[cc];
             if (id == 0) {
-                er = er + 1.;
+                er = er + R(1.);
             } else {
-                const EmMat& m = mt[id - 1];
-                if (P.em_fromP) dP = dP + io.q_in.c[C][cc] * P.dt;
-                if (m.flags & MF_FE) pc = pc + 1.;
+                const EmMat<R>& m = mt[id - 1];
+                if (P.em_fromP) dP = dP + io.q_in.c[C][cc] * dt_r;
+                if (m.flags & MF_FE) pc = pc + R(1.);
                 er = er + m.er;
                 cond = cond + m.cond;
             }
-            if (P.jf_on) Jf = Jf + jf_cell(P, io, dr, C, cx[q], cy[q], cz[q]);
+            if (P.jf_on) Jf = Jf + jf_cell(P, io, R(dr.jf), C, cx[q], cy[q], cz[q]);
         }
-        if (pc < 0.5) pc = 1.;
-        Jf = Jf / 4.;
+        if (pc < R(0.5)) pc = R(1.);
+        Jf = Jf / R(4.);
         // pc counts the ferroelectric cells (1..4): divisions by 1, 2 and 4 are exact
-        dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
-        er = er / 4.; cond = cond / 4.;
-        double rhs = curl - Jf;
+        if constexpr (is_mixed<R>::value)
+            dP = dP * (pc == 3.f ? 1.f / 3.f : (pc == 1.f ? 1.f : (pc == 2.f ? 0.5f : 0.25f)));
+        else
+            dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
+        er = er / R(4.); cond = cond / R(4.);
+        R rhs = curl - Jf;
         if (P.drude) {
             // Drude current: 4-cell mean of the three poles' stage values
-            double Jp = 0.;
+            R Jp = R(0.);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
                 Jp = Jp + io.jp_in[0].c[C][cc] + io.jp_in[1].c[C][cc] + io.jp_in[2].c[C][cc];
             }
-            rhs = rhs - Jp / 4.;
+            rhs = rhs - Jp / R(4.);
         }
-        rhs = rhs - cond * io.E_in.c[C][e] - qdiv(dP, P.dt, P.rdt);
-        d = P.dt_e0 / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
+        rhs = rhs - cond * io.E_in.c[C][e] - qdivR(dP, P.dt, P.rdt, P.f.rdt);
+        d = dt_e0_r / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
     }
-    rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], e);
+    rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], io.E_cmp.c[C], e);
 }
 
 // H face update of component C at face (i,j,k) (index e in C's array).
-template <int S, int C>
-__device__ inline void em_H_face(const Params& P, const StageIO& io, const EmMat* mt, int i, int j, int k, int e) {
+template <int S, int C, class R>
+__device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const EmMat<R>* mt, int i, int j, int k, int e) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const double* Ex = io.E_in.c[0];
-    const double* Ey = io.E_in.c[1];
-    const double* Ez = io.E_in.c[2];
-    double curl;
+    R mdt_mu0_r;
+    if constexpr (is_mixed<R>::value) mdt_mu0_r = P.f.mdt_mu0; else mdt_mu0_r = P.mdt_mu0;
+    const R* Ex = io.E_in.c[0];
+    const R* Ey = io.E_in.c[1];
+    const R* Ez = io.E_in.c[2];
+    R curl;
     int a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
     if (C == 0) {
-        const double dEzdy = qdiv((Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dy, P.rdy);
-        const double dEydz = qdiv((Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]), P.dz, P.rdz);
+        const R dEzdy = qdivR((Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dy, P.rdy, P.f.rdy);
+        const R dEydz = qdivR((Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]), P.dz, P.rdz, P.f.rdz);
         curl = dEzdy - dEydz;
         a1x = (i == 0) ? (P.per_x ? nx - 1 : 0) : i - 1;
         a2x = (i == nx) ? (P.per_x ? 0 : nx - 1) : i;
     } else if (C == 1) {
-        const double dExdz = qdiv((Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dz, P.rdz);
-        const double dEzdx = qdiv((Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dx, P.rdx);
+        const R dExdz = qdivR((Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dz, P.rdz, P.f.rdz);
+        const R dEzdx = qdivR((Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dx, P.rdx, P.f.rdx);
         curl = dExdz - dEzdx;
         a1y = (j == 0) ? (P.per_y ? ny - 1 : 0) : j - 1;
         a2y = (j == ny) ? (P.per_y ? 0 : ny - 1) : j;
     } else {
-        const double dEydx = qdiv((Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]), P.dx, P.rdx);
-        const double dExdy = qdiv((Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dy, P.rdy);
+        const R dEydx = qdivR((Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]), P.dx, P.rdx, P.f.rdx);
+        const R dExdy = qdivR((Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dy, P.rdy, P.f.rdy);
         curl = dEydx - dExdy;
         a1z = (k == 0) ? (P.per_z ? nz - 1 : 0) : k - 1;
         a2z = (k == nz) ? (P.per_z ? 0 : nz - 1) : k;
     }
-    double dM1 = 0., dM2 = 0., cnt = 0.;
+    R dM1 = R(0.), dM2 = R(0.), cnt = R(0.);
     {
         const int c1 = (a1x * ny + a1y) * nz + a1z, c2 = (a2x * ny + a2y) * nz + a2z;
         const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
         // Ms dm + Ms1 dm1 + Ms2 dm2 of each face cell (EMdynamic_solver.cpp:2300-2306)
         if (i1 != 0) {
-            const EmMat& m = mt[i1 - 1];
+            const EmMat<R>& m = mt[i1 - 1];
             if (P.em_fromM) {
                 dM1 = io.dm.c[C][c1] * m.Ms;
                 if (P.afm) dM1 = dM1 + io.da1.c[C][c1] * m.Ms1 + io.da2.c[C][c1] * m.Ms2;
             }
-            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
         }
         if (i2 != 0) {
-            const EmMat& m = mt[i2 - 1];
+            const EmMat<R>& m = mt[i2 - 1];
             if (P.em_fromM) {
                 dM2 = io.dm.c[C][c2] * m.Ms;
                 if (P.afm) dM2 = dM2 + io.da1.c[C][c2] * m.Ms1 + io.da2.c[C][c2] * m.Ms2;
             }
-            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + 1.;
+            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
         }
     }
-    if (cnt < 0.5) cnt = 1.;
+    if (cnt < R(0.5)) cnt = R(1.);
     // -dt/mu0 rounded once on the host; cnt is 1 or 2, so the division is exact
-    const double dMs = dM1 + dM2;
-    const double d = P.mdt_mu0 * curl - (cnt == 2. ? dMs * 0.5 : dMs);
-    rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], e);
+    const R dMs = dM1 + dM2;
+    const R d = mdt_mu0_r * curl - (cnt == R(2.) ? dMs * R(0.5) : dMs);
+    rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], io.H_cmp.c[C], e);
 }
 
 // All six Yee components of one stage: thread (i,j,k) on the vertex grid
@@ -205,13 +219,13 @@ __device__ inline void em_H_face(const Params& P, const StageIO& io, const EmMat
 // H only the stage E and dm, so the six updates are independent.  The grid
 // is (blocks over the (j,k) vertex plane) x (nx+1 planes); the material
 // constants are staged in shared memory.
-template <int S>
+template <int S, class R = double>
 // (256, 8): 32 registers, 64 resident warps per SM; the kernel is bound by
 // the latency of its neighbour loads, and full occupancy beats the spills
-__global__ void __launch_bounds__(256, 8) k_em_fused(Params P, StageIO io, int nmat) {
-    __shared__ EmMat mt[kMaxMat];
+__global__ void __launch_bounds__(256, 8) k_em_fused(Params P, StageIOT<R> io, int nmat) {
+    __shared__ EmMat<R> mt[kMaxMat];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
-        const DevMat& d = io.mats[q];
+        const DevMatT<R>& d = io.mats[q];
         mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].Ms1 = d.Ms1; mt[q].Ms2 = d.Ms2; mt[q].flags = d.flags;
     }
     __syncthreads();
@@ -221,12 +235,12 @@ __global__ void __launch_bounds__(256, 8) k_em_fused(Params P, StageIO io, int n
     const int i = blockIdx.y;
     const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
     const StageDrive& dr = stage_drive(io, S);
-    if (i < nx) em_E_edge<S, 0>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
-    if (j < ny) em_E_edge<S, 1>(P, io, dr, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
-    if (k < nz) em_E_edge<S, 2>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (j < ny && k < nz) em_H_face<S, 0>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
-    if (i < nx && k < nz) em_H_face<S, 1>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (i < nx && j < ny) em_H_face<S, 2>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (i < nx) em_E_edge<S, 0, R>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
+    if (j < ny) em_E_edge<S, 1, R>(P, io, dr, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (k < nz) em_E_edge<S, 2, R>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (j < ny && k < nz) em_H_face<S, 0, R>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
+    if (i < nx && k < nz) em_H_face<S, 1, R>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (i < nx && j < ny) em_H_face<S, 2, R>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
 }
 
 // Drude polarisation current, per cell: dJp_n = (e0 wp_n^2 E_cell c_n -
@@ -327,19 +341,26 @@ __global__ void __launch_bounds__(256) k_em_pec(Params P, StageIO io) {
 }
 
 // hard plane-wave source: E on z = plane_z, all three components, i<nx, j<ny
-template <int S>
-__global__ void k_em_plane(Params P, StageIO io) {
+template <int S, class R = double>
+__global__ void k_em_plane(Params P, StageIOT<R> io) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)P.nx * P.ny) return;
     const long i = t / P.ny, j = t - i * P.ny;
     const long nx = P.nx, ny = P.ny, nz = P.nz, z = P.plane_z;
     const StageDrive& dr = stage_drive(io, S);
-    double* tx = (S < 3) ? io.E_out.c[0] : io.E_acc.c[0];
-    double* ty = (S < 3) ? io.E_out.c[1] : io.E_acc.c[1];
-    double* tz = (S < 3) ? io.E_out.c[2] : io.E_acc.c[2];
+    R* tx = (S < 3) ? io.E_out.c[0] : io.E_acc.c[0];
+    R* ty = (S < 3) ? io.E_out.c[1] : io.E_acc.c[1];
+    R* tz = (S < 3) ? io.E_out.c[2] : io.E_acc.c[2];
     tx[(i * (ny + 1) + j) * (nz + 1) + z] = dr.plane[0];
     ty[(i * ny + j) * (nz + 1) + z] = dr.plane[1];
     tz[(i * (ny + 1) + j) * nz + z] = dr.plane[2];
+    if constexpr (is_mixed<R>::value) {
+        if (S == 3) {
+            io.E_cmp.c[0][(i * (ny + 1) + j) * (nz + 1) + z] = R(0);
+            io.E_cmp.c[1][(i * ny + j) * (nz + 1) + z] = R(0);
+            io.E_cmp.c[2][(i * (ny + 1) + j) * nz + z] = R(0);
+        }
+    }
     (void)nx;
 }
 
@@ -347,15 +368,15 @@ __global__ void k_em_plane(Params P, StageIO io) {
 // For S < 3:  out(b) = X(b_in) + c * (X(b) - out(b_in))   (stage store)
 // For S = 3:  new(b) = old(b_in) + c * (old(b) - new(b_in))
 // where X / old is the step-start value and out / new the value written.
-template <int S, int F>
-__global__ void k_em_mur(Params P, StageIO io) {
+template <int S, int F, class R = double>
+__global__ void k_em_mur(Params P, StageIOT<R> io) {
     const long nx = P.nx, ny = P.ny, nz = P.nz;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool half = (S == 0 || S == 1);
     // two tangential components per face; index range per component
     if (F == 0) {
         // Ey (j<ny, k<=nz) then Ez (j<=ny, k<nz) at i = 0 and i = nx
-        const double cfx = half ? P.c_x_half : P.c_x;
+        const R cfx = half ? P.c_x_half : P.c_x;
         const long n1 = ny * (nz + 1), n2 = (ny + 1) * nz;
         if (t >= n1 + n2) return;
         const int comp = (t < n1) ? 1 : 2;
@@ -370,15 +391,16 @@ __global__ void k_em_mur(Params P, StageIO io) {
             e0 = (0 * (ny + 1) + j) * nz + k; e1 = (1 * (ny + 1) + j) * nz + k;
             eN = (nx * (ny + 1) + j) * nz + k; eN1 = ((nx - 1) * (ny + 1) + j) * nz + k;
         }
-        const double* X = io.E_x.c[comp];
-        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        const R* X = io.E_x.c[comp];
+        R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_xy) {
             O[e0] = X[e1] + cfx * (X[e0] - O[e1]);
             O[eN] = X[eN1] + cfx * (X[eN] - O[eN1]);
-        } else { O[e0] = 0.; O[eN] = 0.; }
+        } else { O[e0] = R(0.); O[eN] = R(0.); }
+        if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     } else if (F == 1) {
         // Ex (i<nx, k<=nz) then Ez (i<=nx, k<nz) at j = 0 and j = ny
-        const double cfy = half ? P.c_y_half : P.c_y;
+        const R cfy = half ? P.c_y_half : P.c_y;
         const long n1 = nx * (nz + 1), n2 = (nx + 1) * nz;
         if (t >= n1 + n2) return;
         const int comp = (t < n1) ? 0 : 2;
@@ -393,15 +415,16 @@ __global__ void k_em_mur(Params P, StageIO io) {
             e0 = (i * (ny + 1) + 0) * nz + k; e1 = (i * (ny + 1) + 1) * nz + k;
             eN = (i * (ny + 1) + ny) * nz + k; eN1 = (i * (ny + 1) + ny - 1) * nz + k;
         }
-        const double* X = io.E_x.c[comp];
-        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        const R* X = io.E_x.c[comp];
+        R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_xy) {
             O[e0] = X[e1] + cfy * (X[e0] - O[e1]);
             O[eN] = X[eN1] + cfy * (X[eN] - O[eN1]);
-        } else { O[e0] = 0.; O[eN] = 0.; }
+        } else { O[e0] = R(0.); O[eN] = R(0.); }
+        if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     } else {
         // Ex (i<nx, j<=ny) then Ey (i<=nx, j<ny) at k = 0 and k = nz
-        const double ctop = half ? P.c_top_half : P.c_top, cbot = half ? P.c_bot_half : P.c_bot;
+        const R ctop = half ? P.c_top_half : P.c_top, cbot = half ? P.c_bot_half : P.c_bot;
         const long n1 = nx * (ny + 1), n2 = (nx + 1) * ny;
         if (t >= n1 + n2) return;
         const int comp = (t < n1) ? 0 : 1;
@@ -410,13 +433,14 @@ __global__ void k_em_mur(Params P, StageIO io) {
         if (comp == 0) { const long i = r / (ny + 1), j = r - i * (ny + 1); base = (i * (ny + 1) + j) * (nz + 1); }
         else { const long i = r / ny, j = r - i * ny; base = (i * ny + j) * (nz + 1); }
         const long e0 = base, e1 = base + 1, eN = base + nz, eN1 = base + nz - 1;
-        const double* X = io.E_x.c[comp];
-        double* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
+        const R* X = io.E_x.c[comp];
+        R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_z) {
             O[eN] = X[eN1] + ctop * (X[eN] - O[eN1]);
             if (!P.abc_1D || !P.abc_em_onlytop) O[e0] = X[e1] + cbot * (X[e0] - O[e1]);
-            else O[e0] = 0.;
-        } else { O[e0] = 0.; O[eN] = 0.; }
+            else O[e0] = R(0.);
+        } else { O[e0] = R(0.); O[eN] = R(0.); }
+        if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     }
 }
 

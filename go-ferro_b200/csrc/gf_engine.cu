@@ -1,9 +1,19 @@
 // B200 engine for GO-Ferro's coupled RK4 phase-field step: state ownership,
 // stage sequencing, CUDA-graph replay and the C ABI of goferro_b200.h.
 //
-// One translation unit holds every kernel of the FP64 path (the .cuh files
-// below); it is compiled with -fmad=false so that each multiply and add is
-// rounded separately, as in the reference's host build.
+// One translation unit holds every kernel (the .cuh files below); it is
+// compiled with -fmad=false so that each multiply and add of the FP64 parity
+// form is rounded separately, as in the reference's host build.
+//
+// Two precisions share the engine.  The FP64 form (GF_PRECISION_FP64) is the
+// parity path.  The mixed form (GF_PRECISION_MIXED_FP32) instantiates the
+// same stage kernels with R = float: state arrays, stencils and transforms
+// in FP32, a compensation word per state scalar (gf_state.cuh), |m| = 1 after
+// every stage; FP64 remains in the demag-table build, the averages and the
+// conversions at this ABI, which takes and returns FP64 in both forms.  The
+// device buffers below are held through double* handles in both forms: in
+// the mixed form they are allocated at 4 bytes per element and hold FP32
+// values, and build_io hands the kernels float* views of them.
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -40,6 +50,7 @@ struct Field3 {
     double* A[3] = {nullptr, nullptr, nullptr};
     double* S0[3] = {nullptr, nullptr, nullptr};
     double* S1[3] = {nullptr, nullptr, nullptr};
+    double* C[3] = {nullptr, nullptr, nullptr};   // compensation words (mixed form only)
     long len[3] = {0, 0, 0};
     bool on = false;
 };
@@ -50,6 +61,8 @@ struct gf_engine {
     Deck deck;
     Params P{};
     int device = 0;
+    bool mixed = false;                    // GF_PRECISION_MIXED_FP32
+    size_t esz = sizeof(double);           // bytes per element of the real-valued device buffers
     cudaStream_t stream = nullptr;
     std::string err;
 
@@ -65,6 +78,8 @@ struct gf_engine {
     uint8_t* mid = nullptr;
     DevMat* mats = nullptr;
     LLGTables* llg_tab = nullptr;
+    DevMatT<float>* mats_f = nullptr;      // mixed form: FP32 copies of the tables
+    LLGTablesT<float>* llg_tab_f = nullptr;
     StepDrive* drive = nullptr;
     StepDrive* drive_host = nullptr;       // pinned staging
     unsigned long long* step_ctr = nullptr;
@@ -87,7 +102,8 @@ struct gf_engine {
     size_t el_smem = 0;                // its dynamic shared memory
     bool el_cubic = false;             // every material has the cubic stiffness pattern
     double* liao_hist = nullptr; double* liao_last = nullptr;
-    double* scratch = nullptr;             // 6n doubles: output staging and reductions
+    double* scratch = nullptr;             // output staging (scratch_main doubles), then reduction partials
+    size_t scratch_main = 0;
     int* flag = nullptr;
 
     // magnetostatics
@@ -100,6 +116,7 @@ struct gf_engine {
     bool plans = false;
 
     StageIO io[2][4];
+    StageIOT<float> iof[2][4];             // mixed form
     // launch accounting and optional per-launch timing (gf_profile_steps)
     int launches_per_step = 0;
     int launch_counter = 0;
@@ -181,16 +198,33 @@ int dalloc_n(gf_engine* eng, T** p, size_t count) {
     return dalloc(eng, reinterpret_cast<void**>(p), count * sizeof(T));
 }
 
+// a real-valued device buffer of `count` elements of the run's precision
+int dalloc_r(gf_engine* eng, double** p, size_t count) {
+    return dalloc(eng, reinterpret_cast<void**>(p), count * eng->esz);
+}
+
 int alloc_field(gf_engine* eng, Field3& f, long l0, long l1, long l2) {
     f.on = true;
     f.len[0] = l0; f.len[1] = l1; f.len[2] = l2;
     for (int c = 0; c < 3; c++) {
-        GF_TRY(dalloc_n(eng, &f.X[c], f.len[c]));
-        GF_TRY(dalloc_n(eng, &f.A[c], f.len[c]));
-        GF_TRY(dalloc_n(eng, &f.S0[c], f.len[c]));
-        GF_TRY(dalloc_n(eng, &f.S1[c], f.len[c]));
+        GF_TRY(dalloc_r(eng, &f.X[c], f.len[c]));
+        GF_TRY(dalloc_r(eng, &f.A[c], f.len[c]));
+        GF_TRY(dalloc_r(eng, &f.S0[c], f.len[c]));
+        GF_TRY(dalloc_r(eng, &f.S1[c], f.len[c]));
+        if (eng->mixed) GF_TRY(dalloc_r(eng, &f.C[c], f.len[c]));
     }
     return GF_OK;
+}
+
+// FP32 copy of a material table (member by member, same layout)
+DevMatT<float> devmat_f32(const DevMat& d) {
+    DevMatT<float> f;
+    std::memset(&f, 0, sizeof(f));
+    f.flags = d.flags; f.aniso = d.aniso; f.cubic_c = d.cubic_c;
+    const double* src = &d.Ms;
+    float* dst = &f.Ms;
+    for (int q = 0; q < kDevMatReals; q++) dst[q] = (float)src[q];
+    return f;
 }
 
 DevMat make_devmat(const Material& m, double dt) {
@@ -320,6 +354,14 @@ std::string unsupported(const Deck& d) {
     return "";
 }
 
+// physics the mixed form does not cover
+std::string unsupported_mixed(const Deck& d, const Params& P) {
+    if (d.any_afm) return "the mixed-precision form does not cover antiferromagnets; use GF_PRECISION_FP64";
+    if (P.drude) return "the mixed-precision form does not cover Drude dispersion; use GF_PRECISION_FP64";
+    if (P.pec) return "the mixed-precision form does not cover perfect conductors; use GF_PRECISION_FP64";
+    return "";
+}
+
 void build_params(gf_engine* eng) {
     const Deck& d = eng->deck;
     Params& P = eng->P;
@@ -331,6 +373,10 @@ void build_params(gf_engine* eng) {
     P.dt_e0 = d.dt / kE0; P.mdt_mu0 = -d.dt / kMu0;
     P.rot = d.orient_rotate;
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { P.Tg2c[i][j] = d.Tg2c[i][j]; P.Tc2g[i][j] = d.Tc2g[i][j]; }
+    P.f.rdx = (float)P.rdx; P.f.rdy = (float)P.rdy; P.f.rdz = (float)P.rdz; P.f.rdt = (float)P.rdt;
+    P.f.dt = (float)P.dt; P.f.dt_e0 = (float)P.dt_e0; P.f.mdt_mu0 = (float)P.mdt_mu0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { P.f.Tg2c[i][j] = (float)P.Tg2c[i][j]; P.f.Tc2g[i][j] = (float)P.Tc2g[i][j]; }
     P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
     {
         long lo[3] = {d.nx, d.ny, d.nz}, hi[3] = {-1, -1, -1};
@@ -598,32 +644,93 @@ void build_io(gf_engine* eng) {
         }
 }
 
+// float views of the run's buffers (mixed form)
+F3T<float> f3f(double* const* p) {
+    F3T<float> r;
+    for (int c = 0; c < 3; c++) r.c[c] = reinterpret_cast<float*>(p[c]);
+    return r;
+}
+void set_io_field_f(const Field3& f, int parity, int s, F3T<float>& in, F3T<float>& x, F3T<float>& acc,
+                    F3T<float>& out, F3T<float>& cmp) {
+    double* const* X = parity ? f.A : f.X;
+    double* const* A = parity ? f.X : f.A;
+    x = f3f(X);
+    acc = f3f(A);
+    cmp = f3f(f.C);
+    if (s == 0) { in = f3f(X); out = f3f(f.S0); }
+    else if (s == 1) { in = f3f(f.S0); out = f3f(f.S1); }
+    else if (s == 2) { in = f3f(f.S1); out = f3f(f.S0); }
+    else { in = f3f(f.S0); out = f3f(A); }
+}
+
+void build_io_mixed(gf_engine* eng) {
+    for (int par = 0; par < 2; par++)
+        for (int s = 0; s < 4; s++) {
+            StageIOT<float>& io = eng->iof[par][s];
+            std::memset(&io, 0, sizeof(io));
+            if (eng->m.on) set_io_field_f(eng->m, par, s, io.m_in, io.m_x, io.m_acc, io.m_out, io.m_cmp);
+            if (eng->p.on) set_io_field_f(eng->p, par, s, io.p_in, io.p_x, io.p_acc, io.p_out, io.p_cmp);
+            if (eng->q.on) set_io_field_f(eng->q, par, s, io.q_in, io.q_x, io.q_acc, io.q_out, io.q_cmp);
+            if (eng->u.on) set_io_field_f(eng->u, par, s, io.u_in, io.u_x, io.u_acc, io.u_out, io.u_cmp);
+            if (eng->v.on) set_io_field_f(eng->v, par, s, io.v_in, io.v_x, io.v_acc, io.v_out, io.v_cmp);
+            if (eng->E.on) set_io_field_f(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out, io.E_cmp);
+            if (eng->H.on) set_io_field_f(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out, io.H_cmp);
+            io.dm = f3f(eng->dm);
+            io.force_store = f3f(eng->force_store);
+            io.force = f3f(eng->force);
+            io.Hstat = f3f(eng->Hstat);
+            io.Estat = f3f(eng->Estat);
+            io.Hnu = f3f(eng->Hnu);
+            for (int a = 0; a < 9; a++) io.fg[a] = reinterpret_cast<float*>(eng->fg[a]);
+            for (int a = 0; a < 6; a++) io.strain_c[a] = reinterpret_cast<float*>(eng->strain_c[a]);
+            io.liao_hist = reinterpret_cast<float*>(eng->liao_hist);
+            io.liao_last = reinterpret_cast<float*>(eng->liao_last);
+            io.mid = eng->mid;
+            io.mats = eng->mats_f;
+            io.drive = eng->drive;
+            io.drive_mask = (unsigned long long)(kDriveCap - 1);
+            io.step = eng->step_ctr;
+            io.jf_kfac = reinterpret_cast<const float*>(eng->jf_kfac);
+        }
+}
+
 // ---------------------------------------------------------------------------
 // one RK4 step: kernel sequence in the reference's data order
 // ---------------------------------------------------------------------------
 // Shared-memory opt-in and the x-chunk of the tiled elastic kernel.  A
 // block of `L` planes costs L+2 plane passes (one halo plane each side), so
 // the chunk count minimises waves x (L+2) over the blocks that fit at once.
+template <class R>
+int set_elastic_smem(gf_engine* eng, int smem) {
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return GF_OK;
+}
+
 int setup_elastic_tile(gf_engine* eng) {
     const Params& P = eng->P;
     eng->el_nmat = (int)eng->deck.mats.size();
-    eng->el_smem = etile::smem_bytes(eng->el_nmat);
+    eng->el_smem = eng->mixed ? etile::smem_bytes<float>(eng->el_nmat) : etile::smem_bytes<double>(eng->el_nmat);
     const int smem = (int)eng->el_smem;
     eng->el_cubic = true;
     for (const Material& m : eng->deck.mats)
         for (int a = 0; a < 6; a++)
             for (int b = 0; b < 6; b++)
                 if (!((a < 3 && b < 3) || a == b) && m.cij[a][b] != 0.) eng->el_cubic = false;
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GF_CU(cudaFuncSetAttribute(k_elastic_tile<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 1, sms = 1;
-    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false>, etile::NT, eng->el_smem));
+    if (eng->mixed) {
+        GF_TRY(set_elastic_smem<float>(eng, smem));
+        GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false, float>, etile::NT, eng->el_smem));
+    } else {
+        GF_TRY(set_elastic_smem<double>(eng, smem));
+        GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false, double>, etile::NT, eng->el_smem));
+    }
     GF_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, eng->device));
     if (per_sm < 1) { eng->err = "elastic tile does not fit on an SM"; return GF_ECUDA; }
     const long slots = (long)per_sm * (sms > 0 ? sms : 1);
@@ -638,71 +745,131 @@ int setup_elastic_tile(gf_engine* eng) {
     return GF_OK;
 }
 
-template <int S>
+template <class R> const StageIOT<R>& stage_io(const gf_engine* eng, int parity, int s);
+template <> const StageIOT<double>& stage_io<double>(const gf_engine* eng, int parity, int s) { return eng->io[parity][s]; }
+template <> const StageIOT<float>& stage_io<float>(const gf_engine* eng, int parity, int s) { return eng->iof[parity][s]; }
+template <class R> const LLGTablesT<R>* llg_tables(const gf_engine* eng);
+template <> const LLGTablesT<double>* llg_tables<double>(const gf_engine* eng) { return eng->llg_tab; }
+template <> const LLGTablesT<float>* llg_tables<float>(const gf_engine* eng) { return eng->llg_tab_f; }
+
+// magnetostatic field of magnetisation m into Hstat (FFT, demag factors or
+// the 1-D model), FP64 form
+int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    auto L = [&](const char* name, auto k, dim3 g, dim3 b, auto... args) -> cudaError_t {
+        return counted ? klaunch(eng, name, k, g, b, 0, st, args...) : launch(k, g, b, 0, st, args...);
+    };
+    if (eng->demag_mode == 0) {
+        GF_CU(L("k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                m, a1, a2, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+        GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+        const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+        const double vol_neg = -P.dx * P.dy * P.dz;
+        GF_CU(L("k_demag_mul", k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, vol_neg,
+                (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+        GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+        for (int a = 0; a < 3; a++)
+            GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    } else {
+        GF_CU(L("k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                m, a1, a2, eng->demag_mode, (double*)nullptr, f3(eng->Hstat), eng->deck.demag_fac[0], eng->deck.demag_fac[1],
+                eng->deck.demag_fac[2]));
+    }
+    return GF_OK;
+}
+
+// the same in the mixed form: FP32 source, R2C, spectra product, C2R
+int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    auto L = [&](const char* name, auto k, dim3 g, dim3 b, auto... args) -> cudaError_t {
+        return counted ? klaunch(eng, name, k, g, b, 0, st, args...) : launch(k, g, b, 0, st, args...);
+    };
+    float* M3 = reinterpret_cast<float*>(eng->Mfft);
+    cufftComplex* Mk = reinterpret_cast<cufftComplex*>(eng->Mk);
+    if (eng->demag_mode == 0) {
+        GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
+                (const uint8_t*)eng->mid, m, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
+        GF_FFT(cufftExecR2C(eng->plan_r2c, M3, Mk));
+        const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+        const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
+        GF_CU(L("k_demag_mul", k_demag_mul_f32, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, inv_vol_neg,
+                (const cuComplex*)Mk, (const cuComplex*)eng->Nk, (cuComplex*)Mk));
+        GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));
+        for (int a = 0; a < 3; a++)
+            GF_CU(cudaMemcpyAsync(eng->Hstat[a], M3 + (size_t)a * P.n, sizeof(float) * P.n, cudaMemcpyDeviceToDevice, st));
+    } else {
+        GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
+                (const uint8_t*)eng->mid, m, eng->demag_mode, (float*)nullptr, f3f(eng->Hstat), (float)eng->deck.demag_fac[0],
+                (float)eng->deck.demag_fac[1], (float)eng->deck.demag_fac[2]));
+    }
+    return GF_OK;
+}
+
+template <int S, class R>
 int enqueue_stage(gf_engine* eng, int parity) {
     const Params& P = eng->P;
-    const StageIO& io = eng->io[parity][S];
+    const StageIOT<R>& io = stage_io<R>(eng, parity, S);
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     if (P.elastic) {
         const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
                         (P.nx + eng->el_chunk - 1) / eng->el_chunk);
         if (eng->el_cubic)
-            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, true>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
+            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, true, R>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
                                 eng->el_chunk, eng->el_nmat));
         else
-            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
+            GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false, R>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
                                 eng->el_chunk, eng->el_nmat));
-        GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S, R>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
-    if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
-                                  dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
-    if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
-                                   dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
-    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
+    if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S, R>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
+                                  dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
+    if constexpr (!is_mixed<R>::value) {
+        if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
+                                       dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
+    }
+    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S, R>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
                             dim3(kThreads), 0, st, P, io));
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
-        GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+        GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
                       dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size()));
-        if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
-                                 dim3(kThreads), 0, st, P, io));
-        if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S, R>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0, R>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1, R>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2, R>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        if constexpr (!is_mixed<R>::value) {
+            if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                                     dim3(kThreads), 0, st, P, io));
+            if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        }
     }
     if (eng->demag_per_stage) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
-        F3 mnew = io.m_out;
-        if (eng->demag_mode == 0) {
-            GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
-                         mnew, io.a1_out, io.a2_out, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
-            GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
-            const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
-            const double vol_neg = -P.dx * P.dy * P.dz;
-            GF_CU(klaunch(eng, "k_demag_mul", k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, vol_neg,
-                         (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
-            GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
-            for (int a = 0; a < 3; a++)
-                GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
-        } else {
-            GF_CU(klaunch(eng, "k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
-                         mnew, io.a1_out, io.a2_out, eng->demag_mode, (double*)nullptr, f3(eng->Hstat),
-                         eng->deck.demag_fac[0], eng->deck.demag_fac[1], eng->deck.demag_fac[2]));
-        }
+        if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, true));
+        else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true));
     }
+    return GF_OK;
+}
+
+template <class R>
+int enqueue_step_t(gf_engine* eng, int parity) {
+    GF_TRY((enqueue_stage<0, R>(eng, parity)));
+    GF_TRY((enqueue_stage<1, R>(eng, parity)));
+    GF_TRY((enqueue_stage<2, R>(eng, parity)));
+    GF_TRY((enqueue_stage<3, R>(eng, parity)));
     return GF_OK;
 }
 
 int enqueue_step(gf_engine* eng, int parity) {
     eng->launch_counter = 0;
-    GF_TRY(enqueue_stage<0>(eng, parity));
-    GF_TRY(enqueue_stage<1>(eng, parity));
-    GF_TRY(enqueue_stage<2>(eng, parity));
-    GF_TRY(enqueue_stage<3>(eng, parity));
+    if (eng->mixed) GF_TRY(enqueue_step_t<float>(eng, parity));
+    else GF_TRY(enqueue_step_t<double>(eng, parity));
     GF_CU(klaunch(eng, "k_step_inc", k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
     eng->launches_per_step = eng->launch_counter;
     return GF_OK;
@@ -710,27 +877,9 @@ int enqueue_step(gf_engine* eng, int parity) {
 
 // static field from the current m (initial solve, main.cpp:135-146)
 int static_field_now(gf_engine* eng) {
-    const Params& P = eng->P;
     if (eng->demag_mode < 0) return GF_OK;
-    const unsigned bn = blocks_for(P.n, kThreads);
-    cudaStream_t st = eng->stream;
-    F3 mx = f3(eng->m.X);
-    if (eng->demag_mode == 0) {
-        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, f3(eng->a1.X), f3(eng->a2.X), 0,
-                     eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
-        GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
-        const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
-        GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
-                     (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
-        GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
-        for (int a = 0; a < 3; a++)
-            GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
-    } else {
-        GF_CU(launch(k_mag_source, dim3(bn), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid, mx, f3(eng->a1.X), f3(eng->a2.X),
-                     eng->demag_mode, (double*)nullptr, f3(eng->Hstat), eng->deck.demag_fac[0], eng->deck.demag_fac[1],
-                     eng->deck.demag_fac[2]));
-    }
-    return GF_OK;
+    if (eng->mixed) return demag_solve_f32(eng, f3f(eng->m.X), false);
+    return demag_solve(eng, f3(eng->m.X), f3(eng->a1.X), f3(eng->a2.X), false);
 }
 
 int setup_demag(gf_engine* eng) {
@@ -743,10 +892,43 @@ int setup_demag(gf_engine* eng) {
     eng->demag_per_stage = !d.em_dynamic;
     if (eng->demag_mode != 0) return GF_OK;
     const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    int dims[3] = {P.nx, P.ny, P.nz};
+    if (eng->mixed) {
+        // M (3n real), M_k (3 n21 complex) and the nine spectra in FP32
+        GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Mfft), sizeof(float) * 3 * (size_t)P.n));
+        GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Mk), sizeof(cufftComplex) * 3 * (size_t)n21));
+        GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Nk), sizeof(cufftComplex) * 9 * (size_t)n21));
+        // tables and their spectra in FP64 with a temporary D2Z plan, then rounded to FP32
+        double* tab = nullptr;
+        cufftDoubleComplex* nk64 = nullptr;
+        cufftHandle p64 = 0;
+        cudaError_t ce = cudaMalloc(&tab, sizeof(double) * 9 * (size_t)P.n);
+        if (ce == cudaSuccess) ce = cudaMalloc(&nk64, sizeof(cufftDoubleComplex) * 9 * (size_t)n21);
+        cufftResult fr = CUFFT_SUCCESS;
+        if (ce == cudaSuccess) fr = cufftPlanMany(&p64, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3);
+        if (ce == cudaSuccess && fr == CUFFT_SUCCESS) fr = cufftSetStream(p64, eng->stream);
+        if (ce == cudaSuccess && fr == CUFFT_SUCCESS) ce = launch(k_newell, dim3(blocks_for(P.n, 128)), dim3(128), 0, eng->stream, P, tab);
+        for (int b = 0; b < 3 && ce == cudaSuccess && fr == CUFFT_SUCCESS; b++)
+            fr = cufftExecD2Z(p64, tab + (size_t)3 * b * P.n, nk64 + (size_t)3 * b * n21);
+        if (ce == cudaSuccess && fr == CUFFT_SUCCESS)
+            ce = launch(k_spectra_f32, dim3(blocks_for(9 * n21, kThreads)), dim3(kThreads), 0, eng->stream,
+                        (const cuDoubleComplex*)nk64, 9 * n21, reinterpret_cast<cuComplex*>(eng->Nk));
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(eng->stream);
+        if (p64) cufftDestroy(p64);
+        if (tab) cudaFree(tab);
+        if (nk64) cudaFree(nk64);
+        if (ce != cudaSuccess) { eng->err = std::string("demag tables: ") + cudaGetErrorString(ce); return GF_ECUDA; }
+        if (fr != CUFFT_SUCCESS) { eng->err = "demag tables: cuFFT error " + std::to_string((int)fr); return GF_ECUDA; }
+        GF_FFT(cufftPlanMany(&eng->plan_r2c, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_R2C, 3));
+        GF_FFT(cufftPlanMany(&eng->plan_c2r, 3, dims, nullptr, 1, (int)n21, nullptr, 1, (int)P.n, CUFFT_C2R, 3));
+        eng->plans = true;
+        GF_FFT(cufftSetStream(eng->plan_r2c, eng->stream));
+        GF_FFT(cufftSetStream(eng->plan_c2r, eng->stream));
+        return GF_OK;
+    }
     GF_TRY(dalloc_n(eng, &eng->Mfft, (size_t)3 * P.n));
     GF_TRY(dalloc_n(eng, &eng->Mk, (size_t)3 * n21));
     GF_TRY(dalloc_n(eng, &eng->Nk, (size_t)9 * n21));
-    int dims[3] = {P.nx, P.ny, P.nz};
     GF_FFT(cufftPlanMany(&eng->plan_r2c, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3));
     GF_FFT(cufftPlanMany(&eng->plan_c2r, 3, dims, nullptr, 1, (int)n21, nullptr, 1, (int)P.n, CUFFT_Z2D, 3));
     eng->plans = true;
@@ -762,10 +944,27 @@ int setup_demag(gf_engine* eng) {
     return GF_OK;
 }
 
-int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* src, long n) {
-    for (int a = 0; a < 3; a++)
-        GF_CU(cudaMemcpyAsync(dst[a], src[a].data(), sizeof(double) * n, cudaMemcpyHostToDevice, eng->stream));
+// one host FP64 array into a device buffer of the run's precision; in the
+// mixed form the value is split into an FP32 value and, when `cmp` is given,
+// its FP32 rounding error (the compensation word)
+int upload_one(gf_engine* eng, double* dst, double* cmp, const double* src, long n) {
+    if (!eng->mixed) {
+        GF_CU(cudaMemcpy(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice));
+        return GF_OK;
+    }
+    std::vector<float> hi((size_t)n), lo(cmp ? (size_t)n : 0);
+    for (long i = 0; i < n; i++) {
+        hi[(size_t)i] = (float)src[i];
+        if (cmp) lo[(size_t)i] = (float)(src[i] - (double)hi[(size_t)i]);
+    }
+    GF_CU(cudaMemcpy(dst, hi.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    if (cmp) GF_CU(cudaMemcpy(cmp, lo.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    return GF_OK;
+}
+
+int upload_vec(gf_engine* eng, double* const* dst, const std::vector<double>* src, long n, double* const* cmp = nullptr) {
     GF_CU(cudaStreamSynchronize(eng->stream));
+    for (int a = 0; a < 3; a++) GF_TRY(upload_one(eng, dst[a], cmp ? cmp[a] : nullptr, src[a].data(), n));
     return GF_OK;
 }
 
@@ -780,7 +979,7 @@ int replicate_state(gf_engine* eng) {
         for (int a = 0; a < 3; a++) {
             double* others[3] = {(c == f->A) ? f->X[a] : f->A[a], f->S0[a], f->S1[a]};
             for (double* o : others)
-                GF_CU(cudaMemcpyAsync(o, c[a], sizeof(double) * f->len[a], cudaMemcpyDeviceToDevice, eng->stream));
+                GF_CU(cudaMemcpyAsync(o, c[a], eng->esz * f->len[a], cudaMemcpyDeviceToDevice, eng->stream));
         }
     }
     GF_CU(cudaStreamSynchronize(eng->stream));
@@ -807,7 +1006,7 @@ int initial_state(gf_engine* eng, const std::string& dir) {
                 if (id && d.mats[id - 1].fm) { buf[0][c] = mx; buf[1][c] = my; buf[2][c] = mz; }
             }
         }
-        GF_TRY(upload_vec(eng, eng->m.X, buf, n));
+        GF_TRY(upload_vec(eng, eng->m.X, buf, n, eng->m.C));
     }
     if (eng->a1.on) {
         std::vector<double> b6[6];
@@ -846,8 +1045,8 @@ int initial_state(gf_engine* eng, const std::string& dir) {
                 if (id && d.mats[id - 1].fe) { buf[0][c] = d.px_init; buf[1][c] = d.py_init; buf[2][c] = d.pz_init; }
             }
         }
-        GF_TRY(upload_vec(eng, eng->p.X, buf, n));
-        GF_TRY(upload_vec(eng, eng->q.X, qb, n));
+        GF_TRY(upload_vec(eng, eng->p.X, buf, n, eng->p.C));
+        GF_TRY(upload_vec(eng, eng->q.X, qb, n, eng->q.C));
     }
     if (eng->u.on && d.in_uv) {
         std::vector<double> ub[3], vb[3];
@@ -856,8 +1055,8 @@ int initial_state(gf_engine* eng, const std::string& dir) {
         std::string e = read_restart(dir + "/u.in", d.nx, d.ny, d.nz, 3, ub);
         if (e.empty()) e = read_restart(dir + "/v.in", d.nx, d.ny, d.nz, 3, vb);
         if (!e.empty()) { eng->err = e; return GF_EIO; }
-        GF_TRY(upload_vec(eng, eng->u.X, ub, n));
-        GF_TRY(upload_vec(eng, eng->v.X, vb, n));
+        GF_TRY(upload_vec(eng, eng->u.X, ub, n, eng->u.C));
+        GF_TRY(upload_vec(eng, eng->v.X, vb, n, eng->v.C));
     }
     if (eng->E.on && d.in_em) {
         const char* names[6] = {"Ex_Yee.in", "Ey_Yee.in", "Ez_Yee.in", "Hx_Yee.in", "Hy_Yee.in", "Hz_Yee.in"};
@@ -870,7 +1069,7 @@ int initial_state(gf_engine* eng, const std::string& dir) {
             std::vector<double> one((size_t)(dimx * dimy * dimz), 0.);
             std::string e = read_restart(dir + "/" + names[f], dimx, dimy, dimz, 1, &one);
             if (!e.empty()) { eng->err = e; return GF_EIO; }
-            GF_CU(cudaMemcpy(F.X[c], one.data(), sizeof(double) * one.size(), cudaMemcpyHostToDevice));
+            GF_TRY(upload_one(eng, F.X[c], F.C[c], one.data(), (long)one.size()));
         }
     }
     if (d.in_Hstat && eng->Hstat[0]) {
@@ -894,7 +1093,13 @@ int initial_state(gf_engine* eng, const std::string& dir) {
     return GF_OK;
 }
 
-int create(gf_engine* eng, const std::string& dir, int device) {
+int create(gf_engine* eng, const std::string& dir, int device, int precision) {
+    if (precision != GF_PRECISION_FP64 && precision != GF_PRECISION_MIXED_FP32) {
+        eng->err = "precision must be GF_PRECISION_FP64 or GF_PRECISION_MIXED_FP32";
+        return GF_EINVAL;
+    }
+    eng->mixed = (precision == GF_PRECISION_MIXED_FP32);
+    eng->esz = eng->mixed ? sizeof(float) : sizeof(double);
     std::string e = read_deck(dir, eng->deck);
     if (!e.empty()) { eng->err = e; return GF_EIO; }
     const Deck& d = eng->deck;
@@ -914,6 +1119,10 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     build_params(eng);
     const Params& P = eng->P;
     const long n = P.n;
+    if (eng->mixed) {
+        e = unsupported_mixed(d, P);
+        if (!e.empty()) { eng->err = e; return GF_EUNSUPPORTED; }
+    }
 
     // materials
     GF_TRY(dalloc_n(eng, &eng->mid, (size_t)n));
@@ -922,6 +1131,12 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     for (size_t i = 0; i < d.mats.size(); i++) dm[i] = make_devmat(d.mats[i], d.dt);
     GF_TRY(dalloc_n(eng, &eng->mats, dm.size()));
     GF_CU(cudaMemcpyAsync(eng->mats, dm.data(), sizeof(DevMat) * dm.size(), cudaMemcpyHostToDevice, eng->stream));
+    if (eng->mixed) {
+        std::vector<DevMatT<float>> dmf(dm.size());
+        for (size_t i = 0; i < dm.size(); i++) dmf[i] = devmat_f32(dm[i]);
+        GF_TRY(dalloc_n(eng, &eng->mats_f, dmf.size()));
+        GF_CU(cudaMemcpy(eng->mats_f, dmf.data(), sizeof(DevMatT<float>) * dmf.size(), cudaMemcpyHostToDevice));
+    }
     {
         LLGTables t;
         std::memset(&t, 0, sizeof(t));
@@ -936,6 +1151,16 @@ int create(gf_engine* eng, const std::string& dir, int device) {
             }
         GF_TRY(dalloc_n(eng, &eng->llg_tab, 1));
         GF_CU(cudaMemcpy(eng->llg_tab, &t, sizeof(t), cudaMemcpyHostToDevice));
+        if (eng->mixed) {
+            LLGTablesT<float> tf;
+            for (int a = 0; a <= kMaxMat; a++)
+                for (int b = 0; b <= kMaxMat; b++) {
+                    tf.Aij[a][b] = (float)t.Aij[a][b];
+                    for (int s = 0; s < 2; s++) tf.AijA[s][a][b] = (float)t.AijA[s][a][b];
+                }
+            GF_TRY(dalloc_n(eng, &eng->llg_tab_f, 1));
+            GF_CU(cudaMemcpy(eng->llg_tab_f, &tf, sizeof(tf), cudaMemcpyHostToDevice));
+        }
     }
     GF_TRY(dalloc_n(eng, &eng->drive, (size_t)kDriveCap));
     GF_CU(cudaMallocHost(&eng->drive_host, sizeof(StepDrive) * kDriveCap));
@@ -950,8 +1175,8 @@ int create(gf_engine* eng, const std::string& dir, int device) {
                 kf[(size_t)k] = (d.jf_type == 1) ? std::sin(sp) : std::cos(sp);
             }
         }
-        GF_TRY(dalloc_n(eng, &eng->jf_kfac, (size_t)P.nz));
-        GF_CU(cudaMemcpy(eng->jf_kfac, kf.data(), sizeof(double) * kf.size(), cudaMemcpyHostToDevice));
+        GF_TRY(dalloc_r(eng, &eng->jf_kfac, (size_t)P.nz));
+        GF_TRY(upload_one(eng, eng->jf_kfac, nullptr, kf.data(), (long)kf.size()));
     }
 
     // state fields
@@ -967,27 +1192,31 @@ int create(gf_engine* eng, const std::string& dir, int device) {
         GF_TRY(alloc_field(eng, eng->H, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)));
     }
     for (int a = 0; a < 3; a++) {
-        if (P.em_fromM) GF_TRY(dalloc_n(eng, &eng->dm[a], (size_t)n));
-        if (P.em_fromM && d.any_afm) { GF_TRY(dalloc_n(eng, &eng->da1[a], (size_t)n)); GF_TRY(dalloc_n(eng, &eng->da2[a], (size_t)n)); }
+        if (P.em_fromM) GF_TRY(dalloc_r(eng, &eng->dm[a], (size_t)n));
+        if (P.em_fromM && d.any_afm) { GF_TRY(dalloc_r(eng, &eng->da1[a], (size_t)n)); GF_TRY(dalloc_r(eng, &eng->da2[a], (size_t)n)); }
         if (d.elastodynamics) {
-            GF_TRY(dalloc_n(eng, &eng->force_store[a], (size_t)n));
-            GF_TRY(dalloc_n(eng, &eng->force[a], (size_t)n));
+            GF_TRY(dalloc_r(eng, &eng->force_store[a], (size_t)n));
+            GF_TRY(dalloc_r(eng, &eng->force[a], (size_t)n));
         }
-        if (d.any_fm || d.any_afm) GF_TRY(dalloc_n(eng, &eng->Hstat[a], (size_t)n));
-        if (d.any_fe) GF_TRY(dalloc_n(eng, &eng->Estat[a], (size_t)n));
-        if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_n(eng, &eng->Hnu[a], (size_t)n));
+        if (d.any_fm || d.any_afm) GF_TRY(dalloc_r(eng, &eng->Hstat[a], (size_t)n));
+        if (d.any_fe) GF_TRY(dalloc_r(eng, &eng->Estat[a], (size_t)n));
+        if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_r(eng, &eng->Hnu[a], (size_t)n));
     }
     if (d.elastodynamics)
-        for (int a = 0; a < 9; a++) GF_TRY(dalloc_n(eng, &eng->fg[a], (size_t)n));
+        for (int a = 0; a < 9; a++) GF_TRY(dalloc_r(eng, &eng->fg[a], (size_t)n));
     if (d.elastodynamics && P.elasto_on && (P.fm || P.afm || P.fe))
-        for (int a = 0; a < 6; a++) GF_TRY(dalloc_n(eng, &eng->strain_c[a], (size_t)n));
+        for (int a = 0; a < 6; a++) GF_TRY(dalloc_r(eng, &eng->strain_c[a], (size_t)n));
     if (d.elastodynamics) GF_TRY(setup_elastic_tile(eng));
     if (d.elastodynamics) {
         const size_t plane = (size_t)P.nx * P.ny;
-        GF_TRY(dalloc_n(eng, &eng->liao_hist, 4 * 12 * plane));
-        GF_TRY(dalloc_n(eng, &eng->liao_last, 3 * plane));
+        GF_TRY(dalloc_r(eng, &eng->liao_hist, 4 * 12 * plane));
+        GF_TRY(dalloc_r(eng, &eng->liao_last, 3 * plane));
     }
-    GF_TRY(dalloc_n(eng, &eng->scratch, (size_t)6 * n + 16384));
+    // FP64 scratch: output staging (6 cell arrays, or one widened Yee
+    // component in the mixed form) and the reduction partials
+    const size_t yee_max = (size_t)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);
+    eng->scratch_main = std::max((size_t)6 * n, yee_max);
+    GF_TRY(dalloc_n(eng, &eng->scratch, eng->scratch_main + 16384));
     GF_TRY(dalloc_n(eng, &eng->flag, 1));
     GF_CU(cudaStreamSynchronize(eng->stream));
 
@@ -995,6 +1224,7 @@ int create(gf_engine* eng, const std::string& dir, int device) {
     GF_TRY(replicate_state(eng));
     GF_TRY(setup_demag(eng));
     build_io(eng);
+    if (eng->mixed) build_io_mixed(eng);
 
     // initial static field (main.cpp:135-146 and 229-239)
     if (!d.in_Hstat) GF_TRY(static_field_now(eng));
@@ -1049,12 +1279,18 @@ int advance(gf_engine* eng, uint64_t nsteps, bool use_graph) {
 // current step value of a 3-component state field
 double* const* cur(gf_engine* eng, Field3& f) { return (eng->steps_done & 1ull) ? f.A : f.X; }
 
-int device_sum(gf_engine* eng, const double* in, long n, double* out) {
+// deterministic FP64 sum of a device array of the run's precision; in the
+// mixed form of the values x + c when the compensation words c are given
+int device_sum(gf_engine* eng, const double* in, long n, double* out, const double* cmp = nullptr) {
     cudaStream_t st = eng->stream;
-    double* p1 = eng->scratch + (size_t)6 * eng->P.n;        // 8192
+    double* p1 = eng->scratch + eng->scratch_main;            // 8192
     double* p2 = p1 + 8192;                                   // 64
     double* p3 = p2 + 64;                                     // 1
-    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, in, n, p1, 8192L));
+    if (eng->mixed)
+        GF_CU(launch(k_sum_stride_f32, dim3(32), dim3(256), 0, st, reinterpret_cast<const float*>(in),
+                     reinterpret_cast<const float*>(cmp), n, p1, 8192L));
+    else
+        GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, in, n, p1, 8192L));
     GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
     GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
     GF_CU(cudaMemcpyAsync(out, p3, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1062,12 +1298,22 @@ int device_sum(gf_engine* eng, const double* in, long n, double* out) {
     return GF_OK;
 }
 
-int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vector<long>& lens, bool& writable) {
+// Device arrays of a field, component by component.  `native` is true when
+// they are state buffers of the run's precision (FP32 in the mixed form, with
+// compensation words in `cmps`, null where the field has none) and false
+// when they are FP64 output staged in the scratch buffer.
+int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vector<long>& lens, bool& writable,
+               std::vector<double*>& cmps, bool& native) {
     const Params& P = eng->P;
     writable = true;
-    ptrs.clear(); lens.clear();
+    native = true;
+    ptrs.clear(); lens.clear(); cmps.clear();
     auto add3 = [&](double* const* p, Field3* f) {
-        for (int a = 0; a < 3; a++) { ptrs.push_back(p[a]); lens.push_back(f ? f->len[a] : P.n); }
+        for (int a = 0; a < 3; a++) {
+            ptrs.push_back(p[a]);
+            lens.push_back(f ? f->len[a] : P.n);
+            cmps.push_back(f ? f->C[a] : nullptr);
+        }
     };
     switch (field) {
         case GF_FIELD_M: if (!eng->m.on) break; add3(cur(eng, eng->m), &eng->m); break;
@@ -1077,33 +1323,50 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
         case GF_FIELD_Q: if (!eng->q.on) break; add3(cur(eng, eng->q), &eng->q); break;
         case GF_FIELD_U: if (!eng->u.on) break; add3(cur(eng, eng->u), &eng->u); break;
         case GF_FIELD_V: if (!eng->v.on) break; add3(cur(eng, eng->v), &eng->v); break;
-        case GF_FIELD_EX: case GF_FIELD_EY: case GF_FIELD_EZ:
+        case GF_FIELD_EX: case GF_FIELD_EY: case GF_FIELD_EZ: {
             if (!eng->E.on) break;
-            ptrs.push_back(cur(eng, eng->E)[field - GF_FIELD_EX]); lens.push_back(eng->E.len[field - GF_FIELD_EX]); break;
-        case GF_FIELD_HX: case GF_FIELD_HY: case GF_FIELD_HZ:
+            const int a = field - GF_FIELD_EX;
+            ptrs.push_back(cur(eng, eng->E)[a]); lens.push_back(eng->E.len[a]); cmps.push_back(eng->E.C[a]); break;
+        }
+        case GF_FIELD_HX: case GF_FIELD_HY: case GF_FIELD_HZ: {
             if (!eng->H.on) break;
-            ptrs.push_back(cur(eng, eng->H)[field - GF_FIELD_HX]); lens.push_back(eng->H.len[field - GF_FIELD_HX]); break;
+            const int a = field - GF_FIELD_HX;
+            ptrs.push_back(cur(eng, eng->H)[a]); lens.push_back(eng->H.len[a]); cmps.push_back(eng->H.C[a]); break;
+        }
         case GF_FIELD_HSTAT: if (!eng->Hstat[0]) break; add3(eng->Hstat, nullptr); break;
         case GF_FIELD_ESTAT: if (!eng->Estat[0]) break; add3(eng->Estat, nullptr); break;
         case GF_FIELD_E_CELL: case GF_FIELD_H_CELL: {
             if (!eng->E.on) break;
             writable = false;
+            native = false;
             double* s = eng->scratch;
             F3 Ec{{s, s + P.n, s + 2 * P.n}}, Hc{{s + 3 * P.n, s + 4 * P.n, s + 5 * P.n}};
-            GF_CU(launch(k_em_cell, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
-                         f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc));
+            if (eng->mixed)
+                GF_CU(launch(k_em_cell<float>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
+                             f3f(cur(eng, eng->E)), f3f(cur(eng, eng->H)), Ec, Hc));
+            else
+                GF_CU(launch(k_em_cell<double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
+                             f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc));
             double* base = (field == GF_FIELD_E_CELL) ? s : s + 3 * P.n;
-            for (int a = 0; a < 3; a++) { ptrs.push_back(base + a * P.n); lens.push_back(P.n); }
+            for (int a = 0; a < 3; a++) { ptrs.push_back(base + a * P.n); lens.push_back(P.n); cmps.push_back(nullptr); }
             break;
         }
         case GF_FIELD_STRAIN: {
             // strain of the current step value (face gradients recomputed from it)
             if (!eng->u.on) break;
             writable = false;
-            StageIO io = eng->io[eng->steps_done & 1ull][0];
-            GF_CU(launch(k_face_grad, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
-            GF_CU(launch(k_cell_strain, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io, eng->scratch));
-            for (int a = 0; a < 6; a++) { ptrs.push_back(eng->scratch + (size_t)a * P.n); lens.push_back(P.n); }
+            native = false;
+            const int par = (int)(eng->steps_done & 1ull);
+            if (eng->mixed) {
+                StageIOT<float> io = eng->iof[par][0];
+                GF_CU(launch(k_face_grad<float>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+                GF_CU(launch(k_cell_strain<float>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io, eng->scratch));
+            } else {
+                StageIO io = eng->io[par][0];
+                GF_CU(launch(k_face_grad<double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+                GF_CU(launch(k_cell_strain<double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io, eng->scratch));
+            }
+            for (int a = 0; a < 6; a++) { ptrs.push_back(eng->scratch + (size_t)a * P.n); lens.push_back(P.n); cmps.push_back(nullptr); }
             break;
         }
         default: break;
@@ -1125,10 +1388,14 @@ int check(gf_engine* e) {
 extern "C" {
 
 int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out) {
+    return gf_create_from_deck_ex(deck_dir, device, GF_PRECISION_FP64, out);
+}
+
+int gf_create_from_deck_ex(const char* deck_dir, int device, int precision, gf_engine** out) {
     if (!deck_dir || !out) { g_create_err = "null argument"; return GF_EINVAL; }
     *out = nullptr;
     gf_engine* eng = new gf_engine();
-    int rc = create(eng, deck_dir, device);
+    int rc = create(eng, deck_dir, device, precision);
     if (rc != GF_OK) {
         g_create_err = eng->err;
         gf_destroy(eng);
@@ -1158,19 +1425,20 @@ int gf_average(gf_engine* e, int obs, double out3[3]) {
     if (!out3) { eng->err = "null output"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
     double* const* src = nullptr;
+    const Field3* f = nullptr;
     double denom = 1.;
     switch (obs) {
-        case GF_OBS_M: if (!eng->m.on) break; src = cur(eng, eng->m); denom = (double)eng->deck.NFM; break;
-        case GF_OBS_M_AFM1: if (!eng->a1.on) break; src = cur(eng, eng->a1); denom = (double)eng->deck.NAFM; break;
-        case GF_OBS_M_AFM2: if (!eng->a2.on) break; src = cur(eng, eng->a2); denom = (double)eng->deck.NAFM; break;
-        case GF_OBS_P: if (!eng->p.on) break; src = cur(eng, eng->p); denom = (double)eng->deck.NFE; break;
-        case GF_OBS_U: if (!eng->u.on) break; src = cur(eng, eng->u); denom = (double)eng->P.n; break;
+        case GF_OBS_M: if (!eng->m.on) break; f = &eng->m; src = cur(eng, eng->m); denom = (double)eng->deck.NFM; break;
+        case GF_OBS_M_AFM1: if (!eng->a1.on) break; f = &eng->a1; src = cur(eng, eng->a1); denom = (double)eng->deck.NAFM; break;
+        case GF_OBS_M_AFM2: if (!eng->a2.on) break; f = &eng->a2; src = cur(eng, eng->a2); denom = (double)eng->deck.NAFM; break;
+        case GF_OBS_P: if (!eng->p.on) break; f = &eng->p; src = cur(eng, eng->p); denom = (double)eng->deck.NFE; break;
+        case GF_OBS_U: if (!eng->u.on) break; f = &eng->u; src = cur(eng, eng->u); denom = (double)eng->P.n; break;
         default: break;
     }
     if (!src) { eng->err = "observable " + std::to_string(obs) + " is not present in this run"; return GF_EINVAL; }
     for (int a = 0; a < 3; a++) {
         double s = 0.;
-        GF_TRY(device_sum(eng, src[a], eng->P.n, &s));
+        GF_TRY(device_sum(eng, src[a], eng->P.n, &s, f->C[a]));
         out3[a] = s / denom;
     }
     return GF_OK;
@@ -1183,8 +1451,8 @@ int gf_probe_em(gf_engine* e, int64_t i, int64_t j, int64_t k, double e3[3], dou
     if (!eng->E.on) { eng->err = "no Maxwell fields in this run"; return GF_EINVAL; }
     if (i < 0 || j < 0 || k < 0 || i >= P.nx || j >= P.ny || k >= P.nz) { eng->err = "probe outside the grid"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
-    std::vector<double*> ptrs; std::vector<long> lens; bool w;
-    GF_TRY(field_ptrs(eng, GF_FIELD_E_CELL, ptrs, lens, w));
+    std::vector<double*> ptrs, cmps; std::vector<long> lens; bool w, native;
+    GF_TRY(field_ptrs(eng, GF_FIELD_E_CELL, ptrs, lens, w, cmps, native));
     const long c = (i * P.ny + j) * P.nz + k;
     for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&e3[a], ptrs[a] + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
     double* hb = eng->scratch + 3 * P.n;
@@ -1209,17 +1477,34 @@ int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count) {
 }
 
 static int copy_field(gf_engine* eng, int field, double* buf, size_t count, bool to_host_or_dev_out, cudaMemcpyKind kind, bool sync) {
-    std::vector<double*> ptrs; std::vector<long> lens; bool writable;
-    GF_TRY(field_ptrs(eng, field, ptrs, lens, writable));
+    std::vector<double*> ptrs, cmps; std::vector<long> lens; bool writable, native;
+    GF_TRY(field_ptrs(eng, field, ptrs, lens, writable, cmps, native));
     size_t total = 0;
     for (long l : lens) total += (size_t)l;
     if (count != total) { eng->err = "field " + std::to_string(field) + " holds " + std::to_string(total) + " doubles, caller gave " + std::to_string(count); return GF_EINVAL; }
     if (!to_host_or_dev_out && !writable) { eng->err = "field is read-only"; return GF_EINVAL; }
+    const bool convert = eng->mixed && native;   // FP32 state <-> FP64 caller buffer through the scratch buffer
     size_t off = 0;
     for (size_t a = 0; a < ptrs.size(); a++) {
-        if (to_host_or_dev_out) GF_CU(cudaMemcpyAsync(buf + off, ptrs[a], sizeof(double) * lens[a], kind, eng->stream));
-        else GF_CU(cudaMemcpyAsync(ptrs[a], buf + off, sizeof(double) * lens[a], kind, eng->stream));
-        off += (size_t)lens[a];
+        const long len = lens[a];
+        float* x = reinterpret_cast<float*>(ptrs[a]);
+        float* cm = reinterpret_cast<float*>(cmps[a]);
+        if (to_host_or_dev_out) {
+            if (convert) {
+                GF_CU(launch(k_widen, dim3(blocks_for(len, kThreads)), dim3(kThreads), 0, eng->stream, (const float*)x, (const float*)cm, len, eng->scratch));
+                GF_CU(cudaMemcpyAsync(buf + off, eng->scratch, sizeof(double) * len, kind, eng->stream));
+            } else {
+                GF_CU(cudaMemcpyAsync(buf + off, ptrs[a], sizeof(double) * len, kind, eng->stream));
+            }
+        } else {
+            if (convert) {
+                GF_CU(cudaMemcpyAsync(eng->scratch, buf + off, sizeof(double) * len, kind, eng->stream));
+                GF_CU(launch(k_split, dim3(blocks_for(len, kThreads)), dim3(kThreads), 0, eng->stream, (const double*)eng->scratch, len, x, cm));
+            } else {
+                GF_CU(cudaMemcpyAsync(ptrs[a], buf + off, sizeof(double) * len, kind, eng->stream));
+            }
+        }
+        off += (size_t)len;
     }
     if (sync) GF_CU(cudaStreamSynchronize(eng->stream));
     return GF_OK;
@@ -1273,6 +1558,7 @@ int gf_get_info(gf_engine* e, gf_info* info) {
     info->n_fm = d.NFM; info->n_afm = d.NAFM; info->n_fe = d.NFE;
     info->device_bytes = e->bytes;
     info->launches_per_step = e->launches_per_step;
+    info->precision = e->mixed ? GF_PRECISION_MIXED_FP32 : GF_PRECISION_FP64;
     return GF_OK;
 }
 
@@ -1328,7 +1614,11 @@ int gf_check_finite(gf_engine* e) {
         if (!nf.f->on) continue;
         for (int a = 0; a < 3; a++) {
             GF_CU(cudaMemsetAsync(eng->flag, 0, sizeof(int), eng->stream));
-            GF_CU(launch(k_check_finite, dim3(296), dim3(256), 0, eng->stream, (const double*)cur(eng, *nf.f)[a], nf.f->len[a], eng->flag));
+            if (eng->mixed)
+                GF_CU(launch(k_check_finite_f32, dim3(296), dim3(256), 0, eng->stream,
+                             reinterpret_cast<const float*>(cur(eng, *nf.f)[a]), nf.f->len[a], eng->flag));
+            else
+                GF_CU(launch(k_check_finite, dim3(296), dim3(256), 0, eng->stream, (const double*)cur(eng, *nf.f)[a], nf.f->len[a], eng->flag));
             int h = 0;
             GF_CU(cudaMemcpyAsync(&h, eng->flag, sizeof(int), cudaMemcpyDeviceToHost, eng->stream));
             GF_CU(cudaStreamSynchronize(eng->stream));
@@ -1373,7 +1663,7 @@ int gf_check_quotients(double d, uint64_t n, uint64_t seed, uint64_t* mismatches
     return GF_OK;
 }
 
-const char* gf_version(void) { return "goferro_b200 0.1 (FP64 parity path, sm_100a)"; }
+const char* gf_version(void) { return "goferro_b200 0.2 (FP64 parity form, FP32 mixed form, sm_100a)"; }
 
 }  // extern "C"
 

@@ -1,4 +1,5 @@
-// Ferroelectric second-order TDGL stage kernel (FP64).
+// Ferroelectric second-order TDGL stage kernel (FP64 parity form and FP32
+// mixed form).
 //
 // One thread per cell: q-increment of ferroelectric_system::get_dq_RK{1..4}
 // (ferroelectric_solver.cpp:534-842: 8th-order Landau polynomial,
@@ -13,25 +14,26 @@
 
 namespace gf {
 
-__device__ inline bool is_fe(const DevMat* mats, uint8_t id) {
+template <class R>
+__device__ inline bool is_fe(const DevMatT<R>* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FE);
 }
 
 // Grid: (blocks over the (j,k) plane) x (nx planes), 32-bit indices.
-template <int S>
+template <int S, class R = double>
 // (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4 blocks)
-__global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIO io) {
+__global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIOT<R> io) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ny * nz) return;
     const int i = blockIdx.y, j = t / nz, k = t - (t / nz) * nz;
     const int c = (i * ny + j) * nz + k;
     const uint8_t id = io.mid[c];
-    double dq[3] = {0., 0., 0.};
+    R dq[3] = {R(0.), R(0.), R(0.)};
 
     if (is_fe(io.mats, id)) {
-        const DevMat& mt = io.mats[id - 1];
-        const double pxg = io.p_in.c[0][c], pyg = io.p_in.c[1][c], pzg = io.p_in.c[2][c];
+        const DevMatT<R>& mt = io.mats[id - 1];
+        const R pxg = io.p_in.c[0][c], pyg = io.p_in.c[1][c], pzg = io.p_in.c[2][c];
 
         // ---- Laplacian with mirror condition at FE interfaces ----
         const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
@@ -46,23 +48,24 @@ __global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIO io) {
                               (k == 0 && !P.per_z) || !is_fe(io.mats, io.mid[nb[4]]),
                               (k == nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
-        double lap[3];   // sum of the three second derivatives per component
+        const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
+        R lap[3];   // sum of the three second derivatives per component
         for (int a = 0; a < 3; a++) {
-            const double pc = io.p_in.c[a][c];
-            double d2[3];
+            const R pc = io.p_in.c[a][c];
+            R d2[3];
             for (int dir = 0; dir < 3; dir++) {
-                const double pb = surf[2 * dir] ? pc : io.p_in.c[a][nb[2 * dir]];
-                const double pf = surf[2 * dir + 1] ? pc : io.p_in.c[a][nb[2 * dir + 1]];
-                d2[dir] = qdiv(qdiv(pf - 2. * pc + pb, h[dir], rh[dir]), h[dir], rh[dir]);
+                const R pb = surf[2 * dir] ? pc : io.p_in.c[a][nb[2 * dir]];
+                const R pf = surf[2 * dir + 1] ? pc : io.p_in.c[a][nb[2 * dir + 1]];
+                d2[dir] = qdivR(qdivR(pf - R(2.) * pc + pb, h[dir], rh[dir], rhf[dir]), h[dir], rh[dir], rhf[dir]);
             }
             lap[a] = d2[0] + d2[1] + d2[2];
         }
 
-        double px, py, pz;
+        R px, py, pz;
         glb2crt(P, pxg, pyg, pzg, px, py, pz);
 
-        double exx = 0, eyy = 0, ezz = 0, eyz = 0, exz = 0, exy = 0;
-        double exx0 = 0, eyy0 = 0, ezz0 = 0, eyz0 = 0, exz0 = 0, exy0 = 0;
+        R exx = R(0), eyy = R(0), ezz = R(0), eyz = R(0), exz = R(0), exy = R(0);
+        R exx0 = R(0), eyy0 = R(0), ezz0 = R(0), eyz0 = R(0), exz0 = R(0), exy0 = R(0);
         if (P.elasto_on) {
             // dynamic strain and eigenstrain of the stage state, crystal frame
             // (Dexx_crt, Dexx0_crt: ferroelectric_solver.cpp:624-652)
@@ -72,63 +75,63 @@ __global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIO io) {
                 eyz = io.strain_c[3][c]; exz = io.strain_c[4][c]; exy = io.strain_c[5][c];
             }
             if (P.elasto_back) {
-                double e0[6];
+                R e0[6];
                 eigen_crt(P, io, c, e0);
                 exx0 = e0[0]; eyy0 = e0[1]; ezz0 = e0[2]; eyz0 = e0[3]; exz0 = e0[4]; exy0 = e0[5];
             }
         }
 
-        const double px2 = px * px, py2 = py * py, pz2 = pz * pz;
-        const double px3 = px2 * px, py3 = py2 * py, pz3 = pz2 * pz;
-        const double px4 = px2 * px2, py4 = py2 * py2, pz4 = pz2 * pz2;
-        const double px5 = px4 * px, py5 = py4 * py, pz5 = pz4 * pz;
-        const double px6 = px4 * px2, py6 = py4 * py2, pz6 = pz4 * pz2;
-        const double px7 = px6 * px, py7 = py6 * py, pz7 = pz6 * pz;
-        const double fm = mt.fe_coef;
+        const R px2 = px * px, py2 = py * py, pz2 = pz * pz;
+        const R px3 = px2 * px, py3 = py2 * py, pz3 = pz2 * pz;
+        const R px4 = px2 * px2, py4 = py2 * py2, pz4 = pz2 * pz2;
+        const R px5 = px4 * px, py5 = py4 * py, pz5 = pz4 * pz;
+        const R px6 = px4 * px2, py6 = py4 * py2, pz6 = pz4 * pz2;
+        const R px7 = px6 * px, py7 = py6 * py, pz7 = pz6 * pz;
+        const R fm = mt.fe_coef;
 
-        const double qxc = fm * (2. * mt.a1 * px + 4. * mt.a11 * px3
-            + 2. * mt.a12 * (py2 + pz2) * px
-            + 6. * mt.a111 * px5
-            + 4. * mt.a112 * px3 * (py2 + pz2)
-            + 2. * mt.a112 * (py4 + pz4) * px
-            + 2. * mt.a123 * px * py2 * pz2
-            + 8. * mt.a1111 * px7
-            + 2. * mt.a1112 * px * (py6 + pz6 + 3. * px4 * (py2 + pz2))
-            + 4. * mt.a1122 * px3 * (py4 + pz4)
-            + 2. * mt.a1123 * px * py2 * pz2 * (2. * px2 + py2 + pz2)
+        const R qxc = fm * (R(2.) * mt.a1 * px + R(4.) * mt.a11 * px3
+            + R(2.) * mt.a12 * (py2 + pz2) * px
+            + R(6.) * mt.a111 * px5
+            + R(4.) * mt.a112 * px3 * (py2 + pz2)
+            + R(2.) * mt.a112 * (py4 + pz4) * px
+            + R(2.) * mt.a123 * px * py2 * pz2
+            + R(8.) * mt.a1111 * px7
+            + R(2.) * mt.a1112 * px * (py6 + pz6 + R(3.) * px4 * (py2 + pz2))
+            + R(4.) * mt.a1122 * px3 * (py4 + pz4)
+            + R(2.) * mt.a1123 * px * py2 * pz2 * (R(2.) * px2 + py2 + pz2)
             + (mt.tv1 * (exx0 - exx) + mt.tv2 * (eyy0 - eyy + ezz0 - ezz)) * px
             + mt.tv3 * ((exy0 - exy) * py + (exz0 - exz) * pz));
-        const double qyc = fm * (2. * mt.a1 * py + 4. * mt.a11 * py3
-            + 2. * mt.a12 * (pz2 + px2) * py
-            + 6. * mt.a111 * py5
-            + 4. * mt.a112 * py3 * (px2 + pz2)
-            + 2. * mt.a112 * (px4 + pz4) * py
-            + 2. * mt.a123 * py * px2 * pz2
-            + 8. * mt.a1111 * py7
-            + 2. * mt.a1112 * py * (px6 + pz6 + 3. * py4 * (px2 + pz2))
-            + 4. * mt.a1122 * py3 * (px4 + pz4)
-            + 2. * mt.a1123 * py * px2 * pz2 * (px2 + 2. * py2 + pz2)
+        const R qyc = fm * (R(2.) * mt.a1 * py + R(4.) * mt.a11 * py3
+            + R(2.) * mt.a12 * (pz2 + px2) * py
+            + R(6.) * mt.a111 * py5
+            + R(4.) * mt.a112 * py3 * (px2 + pz2)
+            + R(2.) * mt.a112 * (px4 + pz4) * py
+            + R(2.) * mt.a123 * py * px2 * pz2
+            + R(8.) * mt.a1111 * py7
+            + R(2.) * mt.a1112 * py * (px6 + pz6 + R(3.) * py4 * (px2 + pz2))
+            + R(4.) * mt.a1122 * py3 * (px4 + pz4)
+            + R(2.) * mt.a1123 * py * px2 * pz2 * (px2 + R(2.) * py2 + pz2)
             + (mt.tv1 * (eyy0 - eyy) + mt.tv2 * (exx0 - exx + ezz0 - ezz)) * py
             + mt.tv3 * ((exy0 - exy) * px + (eyz0 - eyz) * pz));
-        const double qzc = fm * (2. * mt.a1 * pz + 4. * mt.a11 * pz3
-            + 2. * mt.a12 * (py2 + px2) * pz
-            + 6. * mt.a111 * pz5
-            + 4. * mt.a112 * pz3 * (py2 + px2)
-            + 2. * mt.a112 * (py4 + px4) * pz
-            + 2. * mt.a123 * pz * py2 * px2
-            + 8. * mt.a1111 * pz7
-            + 2. * mt.a1112 * pz * (py6 + px6 + 3. * pz4 * (py2 + px2))
-            + 4. * mt.a1122 * pz3 * (py4 + px4)
-            + 2. * mt.a1123 * pz * px2 * py2 * (px2 + py2 + 2. * pz2)
+        const R qzc = fm * (R(2.) * mt.a1 * pz + R(4.) * mt.a11 * pz3
+            + R(2.) * mt.a12 * (py2 + px2) * pz
+            + R(6.) * mt.a111 * pz5
+            + R(4.) * mt.a112 * pz3 * (py2 + px2)
+            + R(2.) * mt.a112 * (py4 + px4) * pz
+            + R(2.) * mt.a123 * pz * py2 * px2
+            + R(8.) * mt.a1111 * pz7
+            + R(2.) * mt.a1112 * pz * (py6 + px6 + R(3.) * pz4 * (py2 + px2))
+            + R(4.) * mt.a1122 * pz3 * (py4 + px4)
+            + R(2.) * mt.a1123 * pz * px2 * py2 * (px2 + py2 + R(2.) * pz2)
             + (mt.tv1 * (ezz0 - ezz) + mt.tv2 * (exx0 - exx + eyy0 - eyy)) * pz
             + mt.tv3 * ((exz0 - exz) * px + (eyz0 - eyz) * py));
-        double gx, gy, gz;
+        R gx, gy, gz;
         crt2glb(P, qxc, qyc, qzc, gx, gy, gz);
 
         const StageDrive& dr = stage_drive(io, S);
-        const double g[3] = {gx, gy, gz};
+        const R g[3] = {gx, gy, gz};
         for (int a = 0; a < 3; a++)
-            dq[a] = g[a] + fm * (-1. * mt.G11 * lap[a] - io.Estat.c[a][c] - dr.Eext[a]) + mt.fe_damp * io.q_in.c[a][c];
+            dq[a] = g[a] + fm * (-R(1.) * mt.G11 * lap[a] - io.Estat.c[a][c] - R(dr.Eext[a])) + mt.fe_damp * io.q_in.c[a][c];
 
         if (P.em_back_P) {
             // cell-centred Maxwell E of the stage state (EMdynamic_solver.cpp:3813-3826)
@@ -136,31 +139,42 @@ __global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIO io) {
             const int ex = (i * ny1 + j) * nz1 + k;
             const int ey = (i * ny + j) * nz1 + k;
             const int ez = (i * ny1 + j) * nz + k;
-            const double Ecx = (io.E_in.c[0][ex] + io.E_in.c[0][ex + nz1] + io.E_in.c[0][ex + 1] + io.E_in.c[0][ex + nz1 + 1]) / 4.;
-            const double Ecy = (io.E_in.c[1][ey] + io.E_in.c[1][ey + ny * nz1] + io.E_in.c[1][ey + 1] + io.E_in.c[1][ey + ny * nz1 + 1]) / 4.;
-            const double Ecz = (io.E_in.c[2][ez] + io.E_in.c[2][ez + ny1 * nz] + io.E_in.c[2][ez + nz] + io.E_in.c[2][ez + ny1 * nz + nz]) / 4.;
+            const R Ecx = (io.E_in.c[0][ex] + io.E_in.c[0][ex + nz1] + io.E_in.c[0][ex + 1] + io.E_in.c[0][ex + nz1 + 1]) / R(4.);
+            const R Ecy = (io.E_in.c[1][ey] + io.E_in.c[1][ey + ny * nz1] + io.E_in.c[1][ey + 1] + io.E_in.c[1][ey + ny * nz1 + 1]) / R(4.);
+            const R Ecz = (io.E_in.c[2][ez] + io.E_in.c[2][ez + ny1 * nz] + io.E_in.c[2][ez + nz] + io.E_in.c[2][ez + ny1 * nz + nz]) / R(4.);
             dq[0] = dq[0] - fm * Ecx;
             dq[1] = dq[1] - fm * Ecy;
             dq[2] = dq[2] - fm * Ecz;
         }
     }
 
-    // ---- RK4 combination for q and p (dp = q_stage * dt) ----
-    for (int a = 0; a < 3; a++) {
-        const double dp = io.q_in.c[a][c] * P.dt;
-        const double qx = io.q_x.c[a][c], px = io.p_x.c[a][c];
-        if (S == 0) {
-            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = qx + qdiv(dq[a], 6., kInv6);
-            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = px + qdiv(dp, 6., kInv6);
-        } else if (S == 1) {
-            io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
-            io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
-        } else if (S == 2) {
-            io.q_out.c[a][c] = qx + dq[a];       io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
-            io.p_out.c[a][c] = px + dp;          io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
-        } else {
-            io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 6., kInv6);
-            io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 6., kInv6);
+    if constexpr (is_mixed<R>::value) {
+        // mixed form: compensated RK4 of q and p (dp = q_stage * dt)
+        const float dt = P.f.dt;
+        for (int a = 0; a < 3; a++) {
+            const float dp = io.q_in.c[a][c] * dt;
+            rk_mixed<S>(io.q_x.c[a][c], dq[a], io.q_out.c[a], io.q_acc.c[a], io.q_cmp.c[a], c);
+            rk_mixed<S>(io.p_x.c[a][c], dp, io.p_out.c[a], io.p_acc.c[a], io.p_cmp.c[a], c);
+        }
+        return;
+    } else {
+        // ---- RK4 combination for q and p (dp = q_stage * dt) ----
+        for (int a = 0; a < 3; a++) {
+            const double dp = io.q_in.c[a][c] * P.dt;
+            const double qx = io.q_x.c[a][c], px = io.p_x.c[a][c];
+            if (S == 0) {
+                io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = qx + qdiv(dq[a], 6., kInv6);
+                io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = px + qdiv(dp, 6., kInv6);
+            } else if (S == 1) {
+                io.q_out.c[a][c] = qx + dq[a] * 0.5; io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
+                io.p_out.c[a][c] = px + dp * 0.5;    io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
+            } else if (S == 2) {
+                io.q_out.c[a][c] = qx + dq[a];       io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 3., kInv3);
+                io.p_out.c[a][c] = px + dp;          io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 3., kInv3);
+            } else {
+                io.q_acc.c[a][c] = io.q_acc.c[a][c] + qdiv(dq[a], 6., kInv6);
+                io.p_acc.c[a][c] = io.p_acc.c[a][c] + qdiv(dp, 6., kInv6);
+            }
         }
     }
 }

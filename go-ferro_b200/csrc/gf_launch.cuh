@@ -24,6 +24,13 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+// one element of a real array (8 bytes for FP64, 4 for FP32)
+__device__ __forceinline__ void cp_async_elem(double* smem_dst, const double* gsrc) { cp_async8(smem_dst, gsrc); }
+__device__ __forceinline__ void cp_async_elem(float* smem_dst, const float* gsrc) { cp_async4(smem_dst, gsrc); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 

@@ -1,4 +1,4 @@
-// Ferromagnetic LLG stage kernel (FP64).
+// Ferromagnetic LLG stage kernel (FP64 parity form and FP32 mixed form).
 //
 // One thread per cell.  For every ferromagnetic cell it evaluates the
 // effective field and the LLG increment exactly as magnetic_system::
@@ -20,10 +20,12 @@
 
 namespace gf {
 
-struct LLGTables {
-    double Aij[kMaxMat + 1][kMaxMat + 1];   // 2*A1*A2/(A1+A2) for ids (1-based)
-    double AijA[2][kMaxMat + 1][kMaxMat + 1];   // the same for the AFM sublattice exchange constants
+template <class R>
+struct LLGTablesT {
+    R Aij[kMaxMat + 1][kMaxMat + 1];   // 2*A1*A2/(A1+A2) for ids (1-based)
+    R AijA[2][kMaxMat + 1][kMaxMat + 1];   // the same for the AFM sublattice exchange constants
 };
+using LLGTables = LLGTablesT<double>;
 
 __device__ inline bool is_fm(const DevMat* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FM);
@@ -32,35 +34,38 @@ __device__ inline bool is_fm(const DevMat* mats, uint8_t id) {
 // static strain plus the cell strain of the stage displacement, crystal
 // frame (exxt0_crt + Dexx_crt, magnetic_solver.cpp:89-96); the dynamic part
 // is written by k_elastic_tile earlier in the same stage
-__device__ inline void cell_strain_total(const Params& P, const StageIO& io, long i, long j, long k, long c, double e[6]) {
-    double d[6] = {0., 0., 0., 0., 0., 0.};
+template <class R>
+__device__ inline void cell_strain_total(const Params& P, const StageIOT<R>& io, long i, long j, long k, long c, R e[6]) {
+    R d[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
     if (P.elastic) for (int a = 0; a < 6; a++) d[a] = io.strain_c[a][c];
     for (int a = 0; a < 6; a++) {
-        double t = io.eps0_c[a] ? io.eps0_c[a][c] : 0.;
+        R t = io.eps0_c[a] ? io.eps0_c[a][c] : R(0);
         e[a] = t + d[a];
     }
 }
 
 // per-material LLG constants, staged in shared memory
+template <class R>
 struct LLGMat {
-    double Aex, dA, ex_coef, dmi_coef, K1c, K2c, B1c, B2c, precess, alpha_precess;
+    R Aex, dA, ex_coef, dmi_coef, K1c, K2c, B1c, B2c, precess, alpha_precess;
     int aniso;
     uint32_t fm;
 };
 
 // One thread per cell of the ferromagnetic bounding box; cells outside it
 // hold their initial m in all four buffers and are never touched.  Grid:
-// (blocks over the box's (j,k) plane) x (box planes in i).
-template <int S>
+// (blocks over the box's (j,k) plane) x (box planes in i).  R = float is the
+// mixed form: FP32 stencil, compensated step value, |m| = 1 after every stage.
+template <int S, class R = double>
 // (256, 4): 64 registers, 32 resident warps per SM for its neighbour-load
 // latency; measured faster than 98 registers at 16 warps despite a few spills
-__global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIO io, const LLGTables* __restrict__ tab, int nmat) {
-    __shared__ LLGMat mt[kMaxMat];
-    __shared__ double sA[kMaxMat + 1][kMaxMat + 1];
+__global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, const LLGTablesT<R>* __restrict__ tab, int nmat) {
+    __shared__ LLGMat<R> mt[kMaxMat];
+    __shared__ R sA[kMaxMat + 1][kMaxMat + 1];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
-        const DevMat& d = io.mats[q];
-        mt[q] = LLGMat{d.Aex, d.dA, d.ex_coef, d.dmi_coef, d.K1c, d.K2c, d.B1c, d.B2c, d.precess, d.alpha_precess,
-                       d.aniso, (d.flags & MF_FM) ? 1u : 0u};
+        const DevMatT<R>& d = io.mats[q];
+        mt[q] = LLGMat<R>{d.Aex, d.dA, d.ex_coef, d.dmi_coef, d.K1c, d.K2c, d.B1c, d.B2c, d.precess, d.alpha_precess,
+                          d.aniso, (d.flags & MF_FM) ? 1u : 0u};
     }
     for (int q = threadIdx.x; q < (nmat + 1) * (nmat + 1); q += blockDim.x) {
         const int a = q / (nmat + 1), b = q - (q / (nmat + 1)) * (nmat + 1);
@@ -75,25 +80,27 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIO io, const L
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int c = (i * ny + j) * nz + k;
     auto fm_at = [&](uint8_t q) { return q != 0 && mt[q - 1].fm != 0u; };
+    const R zero = R(0);
 
     const uint8_t id = io.mid[c];
-    double dmx = 0., dmy = 0., dmz = 0.;
-    const double mxc = io.m_in.c[0][c], myc = io.m_in.c[1][c], mzc = io.m_in.c[2][c];
-    if (fm_at(id)) {
-        const LLGMat& mat = mt[id - 1];
-        double mx, my, mz;
+    const bool fm_cell = fm_at(id);
+    R dmx = zero, dmy = zero, dmz = zero;
+    const R mxc = io.m_in.c[0][c], myc = io.m_in.c[1][c], mzc = io.m_in.c[2][c];
+    if (fm_cell) {
+        const LLGMat<R>& mat = mt[id - 1];
+        R mx, my, mz;
         glb2crt(P, mxc, myc, mzc, mx, my, mz);
 
-        double exx = 0., eyy = 0., ezz = 0., eyz = 0., exz = 0., exy = 0.;
+        R exx = zero, eyy = zero, ezz = zero, eyz = zero, exz = zero, exy = zero;
         if (P.elasto_on) {
-            double e[6];
+            R e[6];
             cell_strain_total(P, io, i, j, k, c, e);
             exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
         }
 
         // ---- one-sided differences with interface slopes ----
-        const double A = mat.Aex;
-        const double dA = mat.dA;   // D/2./A
+        const R A = mat.Aex;
+        const R dA = mat.dA;   // D/2./A
         // neighbour ids and linear indices with periodic wrap at array ends
         const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
         const int jb = (j == 0) ? ny - 1 : j - 1, jF = (j == ny - 1) ? 0 : j + 1;
@@ -112,104 +119,130 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIO io, const L
         const bool szb = (k == 0 && !P.per_z) || !fm_at(idzb);
         const bool szf = (k == nz - 1 && !P.per_z) || !fm_at(idzf);
 
-        double dxb[3], dxf[3], dyb[3], dyf[3], dzb[3], dzf[3];
-        if (sxb) { dxb[0] = -dA * mzc; dxb[1] = 0.; dxb[2] = dA * mxc; }
-        else { dxb[0] = qdiv((mxc - io.m_in.c[0][cxb]), P.dx, P.rdx); dxb[1] = qdiv((myc - io.m_in.c[1][cxb]), P.dx, P.rdx); dxb[2] = qdiv((mzc - io.m_in.c[2][cxb]), P.dx, P.rdx); }
-        if (sxf) { dxf[0] = -dA * mzc; dxf[1] = 0.; dxf[2] = dA * mxc; }
-        else { dxf[0] = qdiv((io.m_in.c[0][cxf] - mxc), P.dx, P.rdx); dxf[1] = qdiv((io.m_in.c[1][cxf] - myc), P.dx, P.rdx); dxf[2] = qdiv((io.m_in.c[2][cxf] - mzc), P.dx, P.rdx); }
-        if (syb) { dyb[0] = 0.; dyb[1] = -dA * mzc; dyb[2] = dA * myc; }
-        else { dyb[0] = qdiv((mxc - io.m_in.c[0][cyb]), P.dy, P.rdy); dyb[1] = qdiv((myc - io.m_in.c[1][cyb]), P.dy, P.rdy); dyb[2] = qdiv((mzc - io.m_in.c[2][cyb]), P.dy, P.rdy); }
-        if (syf) { dyf[0] = 0.; dyf[1] = -dA * mzc; dyf[2] = dA * myc; }
-        else { dyf[0] = qdiv((io.m_in.c[0][cyf] - mxc), P.dy, P.rdy); dyf[1] = qdiv((io.m_in.c[1][cyf] - myc), P.dy, P.rdy); dyf[2] = qdiv((io.m_in.c[2][cyf] - mzc), P.dy, P.rdy); }
-        if (szb) { dzb[0] = 0.; dzb[1] = 0.; dzb[2] = 0.; }
-        else { dzb[0] = qdiv((mxc - io.m_in.c[0][czb]), P.dz, P.rdz); dzb[1] = qdiv((myc - io.m_in.c[1][czb]), P.dz, P.rdz); dzb[2] = qdiv((mzc - io.m_in.c[2][czb]), P.dz, P.rdz); }
-        if (szf) { dzf[0] = 0.; dzf[1] = 0.; dzf[2] = 0.; }
-        else { dzf[0] = qdiv((io.m_in.c[0][czf] - mxc), P.dz, P.rdz); dzf[1] = qdiv((io.m_in.c[1][czf] - myc), P.dz, P.rdz); dzf[2] = qdiv((io.m_in.c[2][czf] - mzc), P.dz, P.rdz); }
+        R dxb[3], dxf[3], dyb[3], dyf[3], dzb[3], dzf[3];
+        if (sxb) { dxb[0] = -dA * mzc; dxb[1] = zero; dxb[2] = dA * mxc; }
+        else { dxb[0] = qdivR((mxc - io.m_in.c[0][cxb]), P.dx, P.rdx, P.f.rdx); dxb[1] = qdivR((myc - io.m_in.c[1][cxb]), P.dx, P.rdx, P.f.rdx); dxb[2] = qdivR((mzc - io.m_in.c[2][cxb]), P.dx, P.rdx, P.f.rdx); }
+        if (sxf) { dxf[0] = -dA * mzc; dxf[1] = zero; dxf[2] = dA * mxc; }
+        else { dxf[0] = qdivR((io.m_in.c[0][cxf] - mxc), P.dx, P.rdx, P.f.rdx); dxf[1] = qdivR((io.m_in.c[1][cxf] - myc), P.dx, P.rdx, P.f.rdx); dxf[2] = qdivR((io.m_in.c[2][cxf] - mzc), P.dx, P.rdx, P.f.rdx); }
+        if (syb) { dyb[0] = zero; dyb[1] = -dA * mzc; dyb[2] = dA * myc; }
+        else { dyb[0] = qdivR((mxc - io.m_in.c[0][cyb]), P.dy, P.rdy, P.f.rdy); dyb[1] = qdivR((myc - io.m_in.c[1][cyb]), P.dy, P.rdy, P.f.rdy); dyb[2] = qdivR((mzc - io.m_in.c[2][cyb]), P.dy, P.rdy, P.f.rdy); }
+        if (syf) { dyf[0] = zero; dyf[1] = -dA * mzc; dyf[2] = dA * myc; }
+        else { dyf[0] = qdivR((io.m_in.c[0][cyf] - mxc), P.dy, P.rdy, P.f.rdy); dyf[1] = qdivR((io.m_in.c[1][cyf] - myc), P.dy, P.rdy, P.f.rdy); dyf[2] = qdivR((io.m_in.c[2][cyf] - mzc), P.dy, P.rdy, P.f.rdy); }
+        if (szb) { dzb[0] = zero; dzb[1] = zero; dzb[2] = zero; }
+        else { dzb[0] = qdivR((mxc - io.m_in.c[0][czb]), P.dz, P.rdz, P.f.rdz); dzb[1] = qdivR((myc - io.m_in.c[1][czb]), P.dz, P.rdz, P.f.rdz); dzb[2] = qdivR((mzc - io.m_in.c[2][czb]), P.dz, P.rdz, P.f.rdz); }
+        if (szf) { dzf[0] = zero; dzf[1] = zero; dzf[2] = zero; }
+        else { dzf[0] = qdivR((io.m_in.c[0][czf] - mxc), P.dz, P.rdz, P.f.rdz); dzf[1] = qdivR((io.m_in.c[1][czf] - myc), P.dz, P.rdz, P.f.rdz); dzf[2] = qdivR((io.m_in.c[2][czf] - mzc), P.dz, P.rdz, P.f.rdz); }
 
-        const double dmxdx = (dxb[0] + dxf[0]) * 0.5;
-        const double dmzdx = (dxb[2] + dxf[2]) * 0.5;
-        const double dmydy = (dyb[1] + dyf[1]) * 0.5;
-        const double dmzdy = (dyb[2] + dyf[2]) * 0.5;
+        const R dmxdx = (dxb[0] + dxf[0]) * R(0.5);
+        const R dmzdx = (dxb[2] + dxf[2]) * R(0.5);
+        const R dmydy = (dyb[1] + dyf[1]) * R(0.5);
+        const R dmzdy = (dyb[2] + dyf[2]) * R(0.5);
 
         // exchange coefficients per face
-        const double Axf = sxf ? A : sA[id][idxf];
-        const double Axb = sxb ? A : sA[id][idxb];
-        const double Ayf = syf ? A : sA[id][idyf];
-        const double Ayb = syb ? A : sA[id][idyb];
-        const double Azf = szf ? A : sA[id][idzf];
-        const double Azb = szb ? A : sA[id][idzb];
+        const R Axf = sxf ? A : sA[id][idxf];
+        const R Axb = sxb ? A : sA[id][idxb];
+        const R Ayf = syf ? A : sA[id][idyf];
+        const R Ayb = syb ? A : sA[id][idyb];
+        const R Azf = szf ? A : sA[id][idzf];
+        const R Azb = szb ? A : sA[id][idzb];
 
-        double Hex[3];
+        R Hex[3];
         for (int a = 0; a < 3; a++) {
-            const double d2xf = qdiv(dxf[a], P.dx, P.rdx), d2xb = -qdiv(dxb[a], P.dx, P.rdx);
-            const double d2yf = qdiv(dyf[a], P.dy, P.rdy), d2yb = -qdiv(dyb[a], P.dy, P.rdy);
-            const double d2zf = qdiv(dzf[a], P.dz, P.rdz), d2zb = -qdiv(dzb[a], P.dz, P.rdz);
+            const R d2xf = qdivR(dxf[a], P.dx, P.rdx, P.f.rdx), d2xb = -qdivR(dxb[a], P.dx, P.rdx, P.f.rdx);
+            const R d2yf = qdivR(dyf[a], P.dy, P.rdy, P.f.rdy), d2yb = -qdivR(dyb[a], P.dy, P.rdy, P.f.rdy);
+            const R d2zf = qdivR(dzf[a], P.dz, P.rdz, P.f.rdz), d2zb = -qdivR(dzb[a], P.dz, P.rdz, P.f.rdz);
             Hex[a] = mat.ex_coef * (Axf * d2xf + Axb * d2xb + Ayf * d2yf + Ayb * d2yb + Azf * d2zf + Azb * d2zb);
         }
 
         // ---- anisotropy (crystal frame) ----
-        double hax = 0., hay = 0., haz = 0.;
+        R hax = zero, hay = zero, haz = zero;
         if (mat.aniso == 1) {
-            hax = -2. * (mat.K1c * (my * my + mz * mz) + mat.K2c * my * my * mz * mz) * mx;
-            hay = -2. * (mat.K1c * (mx * mx + mz * mz) + mat.K2c * mx * mx * mz * mz) * my;
-            haz = -2. * (mat.K1c * (mx * mx + my * my) + mat.K2c * mx * mx * my * my) * mz;
+            hax = R(-2.) * (mat.K1c * (my * my + mz * mz) + mat.K2c * my * my * mz * mz) * mx;
+            hay = R(-2.) * (mat.K1c * (mx * mx + mz * mz) + mat.K2c * mx * mx * mz * mz) * my;
+            haz = R(-2.) * (mat.K1c * (mx * mx + my * my) + mat.K2c * mx * mx * my * my) * mz;
         } else if (mat.aniso == 2) {
-            haz = 2. * mat.K1c * mz;
+            haz = R(2.) * mat.K1c * mz;
         }
-        double Hax, Hay, Haz;
+        R Hax, Hay, Haz;
         crt2glb(P, hax, hay, haz, Hax, Hay, Haz);
 
         // ---- magnetoelastic ----
-        const double hex_ = -2. * (mat.B1c * (exx)*mx + mat.B2c * ((exy)*my + (exz)*mz));
-        const double hey_ = -2. * (mat.B1c * (eyy)*my + mat.B2c * ((exy)*mx + (eyz)*mz));
-        const double hez_ = -2. * (mat.B1c * (ezz)*mz + mat.B2c * ((exz)*mx + (eyz)*my));
-        double Hmx, Hmy, Hmz;
+        const R hex_ = R(-2.) * (mat.B1c * (exx)*mx + mat.B2c * ((exy)*my + (exz)*mz));
+        const R hey_ = R(-2.) * (mat.B1c * (eyy)*my + mat.B2c * ((exy)*mx + (eyz)*mz));
+        const R hez_ = R(-2.) * (mat.B1c * (ezz)*mz + mat.B2c * ((exz)*mx + (eyz)*my));
+        R Hmx, Hmy, Hmz;
         crt2glb(P, hex_, hey_, hez_, Hmx, Hmy, Hmz);
 
         // ---- interfacial DMI ----
-        const double Hdx = mat.dmi_coef * dmzdx;
-        const double Hdy = mat.dmi_coef * dmzdy;
-        const double Hdz = -mat.dmi_coef * (dmxdx + dmydy);
+        const R Hdx = mat.dmi_coef * dmzdx;
+        const R Hdy = mat.dmi_coef * dmzdy;
+        const R Hdz = -mat.dmi_coef * (dmxdx + dmydy);
 
         const StageDrive& dr = stage_drive(io, S);
-        double hnx = 0., hny = 0., hnz = 0.;
+        R hnx = zero, hny = zero, hnz = zero;
         if (P.has_hext_nonunif) { hnx = io.Hnu.c[0][c]; hny = io.Hnu.c[1][c]; hnz = io.Hnu.c[2][c]; }
-        double Hx = io.Hstat.c[0][c] + Hax + Hmx + Hex[0] + Hdx + dr.Hext[0] + hnx;
-        double Hy = io.Hstat.c[1][c] + Hay + Hmy + Hex[1] + Hdy + dr.Hext[1] + hny;
-        double Hz = io.Hstat.c[2][c] + Haz + Hmz + Hex[2] + Hdz + dr.Hext[2] + hnz;
+        R Hx = io.Hstat.c[0][c] + Hax + Hmx + Hex[0] + Hdx + R(dr.Hext[0]) + hnx;
+        R Hy = io.Hstat.c[1][c] + Hay + Hmy + Hex[1] + Hdy + R(dr.Hext[1]) + hny;
+        R Hz = io.Hstat.c[2][c] + Haz + Hmz + Hex[2] + Hdz + R(dr.Hext[2]) + hnz;
 
         if (P.em_back_M) {
             // cell-centred Maxwell H of the stage state (EMdynamic_solver.cpp:3780-3810)
             const int hx0 = (i * ny + j) * nz + k, hx1 = ((i + 1) * ny + j) * nz + k;
             const int hy0 = (i * (ny + 1) + j) * nz + k, hy1 = (i * (ny + 1) + j + 1) * nz + k;
             const int hz0 = (i * ny + j) * (nz + 1) + k, hz1 = hz0 + 1;
-            Hx = Hx + (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / 2.;
-            Hy = Hy + (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / 2.;
-            Hz = Hz + (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / 2.;
+            Hx = Hx + (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / R(2.);
+            Hy = Hy + (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / R(2.);
+            Hz = Hz + (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
         }
 
-        const double precess = mat.precess;
-        const double px = myc * Hz - mzc * Hy;
-        const double py = mzc * Hx - mxc * Hz;
-        const double pz = mxc * Hy - myc * Hx;
-        const double qx = myc * pz - mzc * py;
-        const double qy = mzc * px - mxc * pz;
-        const double qz = mxc * py - myc * px;
+        const R precess = mat.precess;
+        const R px = myc * Hz - mzc * Hy;
+        const R py = mzc * Hx - mxc * Hz;
+        const R pz = mxc * Hy - myc * Hx;
+        const R qx = myc * pz - mzc * py;
+        const R qy = mzc * px - mxc * pz;
+        const R qz = mxc * py - myc * px;
         dmx = precess * px + mat.alpha_precess * qx;
         dmy = precess * py + mat.alpha_precess * qy;
         dmz = precess * pz + mat.alpha_precess * qz;
     }
     if (P.em_fromM) { io.dm.c[0][c] = dmx; io.dm.c[1][c] = dmy; io.dm.c[2][c] = dmz; }
 
-    // ---- RK4 combination; the magnetic increment is summed before it is
-    //      added to m (magnetic_solver.cpp:1453-1455, 1601-1603) ----
-    const double d[3] = {dmx, dmy, dmz};
-    for (int a = 0; a < 3; a++) {
-        const double xv = io.m_x.c[a][c];
-        if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
-        else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
-        else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
-        else { io.m_acc.c[a][c] = xv + (io.m_acc.c[a][c] + qdiv(d[a], 6., kInv6)); }
+    if constexpr (is_mixed<R>::value) {
+        // mixed form: compensated RK4, then |m| = 1 (ferromagnetic cells only;
+        // the others hold m = 0)
+        const float d[3] = {dmx, dmy, dmz};
+        if (S < 3) {
+            const float cf = (S == 2) ? 1.f : 0.5f;
+            float o[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                o[a] = io.m_x.c[a][c] + d[a] * cf;
+                io.m_acc.c[a][c] = (S == 0) ? d[a] * (1.f / 6.f) : io.m_acc.c[a][c] + d[a] * (1.f / 3.f);
+            }
+            if (fm_cell) renorm3(o[0], o[1], o[2]);
+#pragma unroll
+            for (int a = 0; a < 3; a++) io.m_out.c[a][c] = o[a];
+        } else {
+            float x[3], cm[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                two_sum(io.m_x.c[a][c], (io.m_acc.c[a][c] + d[a] * (1.f / 6.f)) + io.m_cmp.c[a][c], x[a], cm[a]);
+            if (fm_cell) renorm_pair(x, cm);
+#pragma unroll
+            for (int a = 0; a < 3; a++) { io.m_acc.c[a][c] = x[a]; io.m_cmp.c[a][c] = cm[a]; }
+        }
+    } else {
+        // ---- RK4 combination; the magnetic increment is summed before it is
+        //      added to m (magnetic_solver.cpp:1453-1455, 1601-1603) ----
+        const double d[3] = {dmx, dmy, dmz};
+        for (int a = 0; a < 3; a++) {
+            const double xv = io.m_x.c[a][c];
+            if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
+            else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
+            else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
+            else { io.m_acc.c[a][c] = xv + (io.m_acc.c[a][c] + qdiv(d[a], 6., kInv6)); }
+        }
     }
 }
 

@@ -67,7 +67,8 @@ __global__ void k_check_finite(const double* __restrict__ in, long n, int* flag)
 // cell-centred E (4-edge means) and H (2-face means) of the current step
 // value, as update_DE_cell / update_DH_cell compute them
 // (EMdynamic_solver.cpp:3780-3826)
-__global__ void k_em_cell(Params P, F3 E, F3 H, F3 Ec, F3 Hc) {
+template <class R = double>
+__global__ void k_em_cell(Params P, F3T<R> E, F3T<R> H, F3 Ec, F3 Hc) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long nyz = (long)P.ny * P.nz;
@@ -76,15 +77,56 @@ __global__ void k_em_cell(Params P, F3 E, F3 H, F3 Ec, F3 Hc) {
     const long ex = (i * ny1 + j) * nz1 + k;
     const long ey = (i * P.ny + j) * nz1 + k;
     const long ez = (i * ny1 + j) * P.nz + k;
-    Ec.c[0][c] = (E.c[0][ex] + E.c[0][ex + nz1] + E.c[0][ex + 1] + E.c[0][ex + nz1 + 1]) / 4.;
-    Ec.c[1][c] = (E.c[1][ey] + E.c[1][ey + P.ny * nz1] + E.c[1][ey + 1] + E.c[1][ey + P.ny * nz1 + 1]) / 4.;
-    Ec.c[2][c] = (E.c[2][ez] + E.c[2][ez + ny1 * P.nz] + E.c[2][ez + P.nz] + E.c[2][ez + ny1 * P.nz + P.nz]) / 4.;
+    Ec.c[0][c] = (E.c[0][ex] + E.c[0][ex + nz1] + E.c[0][ex + 1] + E.c[0][ex + nz1 + 1]) / R(4.);
+    Ec.c[1][c] = (E.c[1][ey] + E.c[1][ey + P.ny * nz1] + E.c[1][ey + 1] + E.c[1][ey + P.ny * nz1 + 1]) / R(4.);
+    Ec.c[2][c] = (E.c[2][ez] + E.c[2][ez + ny1 * P.nz] + E.c[2][ez + P.nz] + E.c[2][ez + ny1 * P.nz + P.nz]) / R(4.);
     const long hx0 = (i * P.ny + j) * P.nz + k, hx1 = ((i + 1) * P.ny + j) * P.nz + k;
     const long hy0 = (i * ny1 + j) * P.nz + k, hy1 = (i * ny1 + j + 1) * P.nz + k;
     const long hz0 = (i * P.ny + j) * nz1 + k;
-    Hc.c[0][c] = (H.c[0][hx0] + H.c[0][hx1]) / 2.;
-    Hc.c[1][c] = (H.c[1][hy0] + H.c[1][hy1]) / 2.;
-    Hc.c[2][c] = (H.c[2][hz0] + H.c[2][hz0 + 1]) / 2.;
+    Hc.c[0][c] = (H.c[0][hx0] + H.c[0][hx1]) / R(2.);
+    Hc.c[1][c] = (H.c[1][hy0] + H.c[1][hy1]) / R(2.);
+    Hc.c[2][c] = (H.c[2][hz0] + H.c[2][hz0 + 1]) / R(2.);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed form (FP32 state with a compensation word): FP64 reductions and the
+// conversions at the C ABI, which stays FP64.
+// ---------------------------------------------------------------------------
+
+// as k_sum_stride, over the FP64 values x + c of an FP32 pair (c may be null)
+__global__ void k_sum_stride_f32(const float* __restrict__ x, const float* __restrict__ cm, long n,
+                                 double* __restrict__ partial, long T) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    double acc = 0.;
+    for (long i = t; i < n; i += T) acc = acc + ((double)x[i] + (cm ? (double)cm[i] : 0.));
+    partial[t] = acc;
+}
+
+// out = x + c in FP64 (c may be null)
+__global__ void k_widen(const float* __restrict__ x, const float* __restrict__ cm, long n, double* __restrict__ out) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = (double)x[i] + (cm ? (double)cm[i] : 0.);
+}
+
+// x = RN_f32(in), c = RN_f32(in - x) (c may be null)
+__global__ void k_split(const double* __restrict__ in, long n, float* __restrict__ x, float* __restrict__ cm) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = in[i];
+    const float h = (float)v;
+    x[i] = h;
+    if (cm) cm[i] = (float)(v - (double)h);
+}
+
+__global__ void k_check_finite_f32(const float* __restrict__ in, long n, int* flag) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long T = (long)gridDim.x * blockDim.x;
+    for (long i = t; i < n; i += T) {
+        const float v = in[i];
+        if (!(v - v == 0.f)) { *flag = 1; return; }
+    }
 }
 
 }  // namespace gf

@@ -89,7 +89,7 @@ typedef struct gf_info {
     uint64_t n_fm, n_afm, n_fe;  /* NFM, NAFM, NFE (global.cpp:103-118)      */
     uint64_t device_bytes;  /* device memory the engine holds                */
     int32_t launches_per_step;  /* engine kernels launched per RK4 step      */
-    int32_t reserved_;
+    int32_t precision;          /* GF_PRECISION_FP64 or GF_PRECISION_MIXED_FP32 */
 } gf_info;
 
 /* Accumulated device time of one kernel family (gf_profile_steps). */
@@ -107,6 +107,24 @@ typedef struct gf_kernel_time {
  * input_*, copy_to_device, initialize_device and the initial static
  * solves).  `device` selects the CUDA device (-1 = current). */
 int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out);
+
+/* Arithmetic of an engine (gf_create_from_deck_ex).
+ *   GF_PRECISION_FP64: every field, stencil and transform in FP64, evaluated
+ *     in the reference's operation order (the parity form).
+ *   GF_PRECISION_MIXED_FP32: state arrays, stencils and FFTs in FP32; each
+ *     state scalar carries an FP32 compensation word, so the RK4 step value
+ *     X + C accumulates increments without FP32 rounding drift; |m| is
+ *     renormalised to 1 after every stage (the reference does not
+ *     renormalise).  The demag tensor and its spectra are built in FP64; the
+ *     averages and every upload/download stay FP64 at this ABI.
+ *     Antiferromagnets, Drude dispersion and perfect conductors are FP64
+ *     only (GF_EUNSUPPORTED). */
+#define GF_PRECISION_FP64 0
+#define GF_PRECISION_MIXED_FP32 1
+
+/* gf_create_from_deck with a choice of arithmetic.  Replaces the same set-up
+ * sequence (main.cpp:21-167); the reference has only its FP64 build. */
+int gf_create_from_deck_ex(const char* deck_dir, int device, int precision, gf_engine** out);
 
 /* Advance `nsteps` full RK4 steps.  Replaces the body of the reference time
  * loop main.cpp:243-484: time_marching_device_serial, the four stages of

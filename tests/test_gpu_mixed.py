@@ -1,0 +1,135 @@
+"""GPU tests of the mixed-precision form (GF_PRECISION_MIXED_FP32): FP32
+state and stencils with compensated RK4 accumulation and |m| = 1 after every
+stage, called through the same C ABI as the FP64 form.
+
+Tolerance: every traced observable agrees with GO-Ferro's own FP64 solver
+(golden fixtures and the live oracle) to 1e-5 of the observable's vector
+magnitude, i.e. the largest |component| of <m>, <p>, <u>, the probed E or
+the probed H over the trace.  Per-component scales would divide FP32 noise by
+near-zero means (<m_x> of a film tilted by at most 1 degree), which measures
+the mean, not the solver.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import _mg, _variants, engine_trace
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+TOL_MIXED = 1e-5
+# trace columns of each vector observable (engine_trace layout)
+GROUPS = {"m": (1, 4), "p": (10, 13), "u": (13, 16), "E": (16, 19), "H": (19, 22)}
+
+
+def trace_errors(mine, ref):
+    """Largest error of each vector observable over the trace, relative to
+    the observable's largest component magnitude."""
+    out = {}
+    for name, (a, b) in GROUPS.items():
+        scale = float(np.max(np.abs(ref[:, a:b])))
+        err = float(np.max(np.abs(mine[:, a:b] - ref[:, a:b])))
+        if scale == 0.0:
+            assert err == 0.0, f"{name}: expected zeros, got {err}"
+            continue
+        out[name] = err / scale
+    return out
+
+
+def assert_mixed_close(mine, ref, tol=TOL_MIXED):
+    errs = trace_errors(mine, ref)
+    assert errs, "no observable compared"
+    for name, e in errs.items():
+        assert e <= tol, f"{name}: relative trace error {e:.3e} > {tol:.0e}"
+    return errs
+
+
+@pytest.mark.parametrize("name", json.load(open(os.path.join(GOLDEN, "cases.json"))).keys())
+def test_mixed_matches_golden(gf, tmp_path, name):
+    mg = _mg()
+    d, steps, probe = mg.make_deck(name)
+    gf.decks.write_deck(d, str(tmp_path))
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    with gf.Engine(str(tmp_path), device=0, precision="mixed") as eng:
+        assert eng.info.precision == 1
+        mine = engine_trace(eng, steps, probe if probe else (0, 0, 0))
+        assert_mixed_close(mine, g["trace"])
+        eng.check_finite()
+
+
+@pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box", "fe_jf6_plane_wave_eext",
+                                   "two_fm_materials_dmi_uniaxial", "demag_factor", "elastic_multi_tile",
+                                   "fm_film_demag_substrate"])
+def test_mixed_matches_live_oracle(gf, refrun, tmp_path, vname):
+    d, steps, probe = _variants(gf)[vname]
+    gf.decks.write_deck(d, str(tmp_path / "deck"))
+    r = refrun.run(str(tmp_path / "deck"), str(tmp_path / "ref"), steps=steps, probe=probe, dump=False)
+    with gf.Engine(str(tmp_path / "deck"), device=0, precision="mixed") as eng:
+        mine = engine_trace(eng, steps, probe if probe else (0, 0, 0))
+        assert_mixed_close(mine, r["trace"])
+
+
+def test_mixed_tracks_fp64_engine_long_run(gf, tmp_path):
+    """Longer horizon than the oracle allows in seconds: 400 steps of the
+    coupled magnetoelastic film against the FP64 engine."""
+    d = gf.decks.preset_magnetoelastic(nx=16, ny=16, nz=24, sub=10, film=8, steps=400)
+    d.amp_gauss *= 1e6
+    gf.decks.write_deck(d, str(tmp_path))
+    traces = {}
+    for prec in ("fp64", "mixed"):
+        with gf.Engine(str(tmp_path), device=0, precision=prec) as eng:
+            traces[prec] = engine_trace(eng, 400, (8, 8, 14))
+    assert_mixed_close(traces["mixed"], traces["fp64"])
+
+
+def test_mixed_unit_magnetisation(gf, tmp_path):
+    """|m| = 1 to FP32 rounding in every ferromagnetic cell after many
+    steps (the step value is the compensated pair x + c)."""
+    d = gf.decks.preset_fm_demag(nx=16, ny=16, nz=8, steps=200)
+    gf.decks.write_deck(d, str(tmp_path))
+    with gf.Engine(str(tmp_path), device=0, precision="mixed") as eng:
+        eng.advance(200)
+        m = eng.download("m")
+    norm = np.sqrt((m ** 2).sum(axis=0))
+    fm = norm > 0.5
+    assert fm.sum() > 0
+    assert np.max(np.abs(norm[fm] - 1.0)) < 1e-12
+
+
+def test_mixed_upload_download_roundtrip(gf, tmp_path):
+    """FP64 values survive the FP32 value + compensation split to ~2^-48."""
+    d = gf.decks.preset_ferroelectric(nx=8, ny=8, nz=10, steps=2)
+    gf.decks.write_deck(d, str(tmp_path))
+    with gf.Engine(str(tmp_path), device=0, precision="mixed") as eng:
+        new = np.random.default_rng(1).standard_normal((3, 8, 8, 10)) * 1e-3
+        eng.upload("p", new)
+        back = eng.download("p")
+        assert np.max(np.abs(back - new)) <= 1e-14 * np.max(np.abs(new))
+        ez = eng.download("Ez")
+        assert ez.shape == (9, 9, 10)
+
+
+def test_mixed_graph_and_eager_identical(gf, tmp_path):
+    d = gf.decks.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=9)
+    d.amp_gauss *= 1e6
+    gf.decks.write_deck(d, str(tmp_path))
+    out = []
+    for graph in (True, False):
+        with gf.Engine(str(tmp_path), device=0, precision="mixed") as eng:
+            eng.advance(9, graph=graph)
+            out.append([eng.download(f) for f in ("m", "u", "v", "Ex", "Hz")])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("vname", ["afm_film_demag", "drude_metal_layer", "pec_layer"])
+def test_mixed_rejects_fp64_only_physics(gf, tmp_path, vname):
+    d, _, _ = _variants(gf)[vname]
+    gf.decks.write_deck(d, str(tmp_path))
+    with pytest.raises(gf.GFError) as ei:
+        gf.Engine(str(tmp_path), device=0, precision="mixed")
+    assert ei.value.code == -7
