@@ -2,12 +2,17 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload magnetoelastic|fm_demag|ferroelectric]
+                    [--precision both|fp64|mixed]
 
 Workload (default): the coupled magnetoelastic + elastodynamics + Maxwell FDTD
 run on a 128x128x96 grid (56-layer garnet substrate, 32-layer YIG film,
-8 vacuum layers), FP64, synthetic seeded initial state.  One step = one full
-RK4 step of all active physics.  The metric is cell-steps/s (grid cells x
-steps / device time), whole job over all ranks.
+8 vacuum layers), synthetic seeded initial state.  One step = one full RK4
+step of all active physics.  The metric is cell-steps/s (grid cells x steps /
+device time), whole job over all ranks: the headline `value` is the FP64
+form (the reference's arithmetic); with --precision both (the default) the
+line also carries `mixed`, the same measurement of the FP32 mixed form, its
+speed-up over FP64 and its trace error against the FP64 engine on the same
+initial state.
 
 `--impl ours` times the engine (CUDA events on the engine stream, max over
 ranks), measures the end-to-end rate through the C ABI with host buffers,
@@ -52,12 +57,15 @@ WORKLOADS = {
 # launch, averaged over the four RK stages: every array the kernel must read
 # or write, once (stage-dependent terms weighted 3/4 where they occur in 3 of
 # the 4 stages); neighbour re-reads are not counted.
-def alg_bytes_per_unit(kernel: str, info, mfe_frac: float = 0.0) -> float:
+def alg_bytes_per_unit(kernel: str, info, mfe_frac: float = 0.0, mixed: bool = False) -> float:
     """Bytes one unit (cell, Yee vertex) of a launch must move, averaged over
     the four RK stages (stage outputs are written at stages 1-3, the
     accumulators read at stages 2-4, the step value read at stages 1-3).
-    mfe_frac: fraction of cells that are ferromagnetic or ferroelectric."""
-    D = 8.0
+    mfe_frac: fraction of cells that are ferromagnetic or ferroelectric.
+    Mixed form: 4-byte reals, plus the compensation word of every state
+    scalar read and written in the last stage (0.5 accesses per launch)."""
+    D = 4.0 if mixed else 8.0
+    comp = 0.5 if mixed else 0.0
     if kernel == "k_elastic":
         # tiled stress-divergence kernel: u_in, m and p for the eigenstrain,
         # material ids; writes the divergence and the crystal-frame strain of
@@ -70,19 +78,19 @@ def alg_bytes_per_unit(kernel: str, info, mfe_frac: float = 0.0) -> float:
         # (stages 2-4); writes v/u stage outputs, accumulators, force_store (stage 1)
         reads = 3 + 3 + 3 + 3 + 3 * 0.75 + 6 * 0.75
         writes = 6 * 0.75 + 6 + 3 * 0.25
-        return (reads + writes) * D + 1
+        return (reads + writes + comp * 6) * D + 1
     if kernel == "k_llg_fm":
         reads = 3 + 3 + 3 * 0.75 + 3 + 6 * info.elastic + 3 * info.em
         writes = 3 * 0.75 + 3 + 3 * info.em
-        return (reads + writes) * D + 1
+        return (reads + writes + comp * 3) * D + 1
     if kernel == "k_fe":
         reads = 3 + 3 + 3 * 0.75 + 3 + 3 + 3 * 0.75 + 6 + 6 + 3 + 3 * info.em
         writes = 3 * 0.75 * 2 + 3 * 2
-        return (reads + writes) * D + 1
+        return (reads + writes + comp * 6) * D + 1
     if kernel == "k_em_fused":
         # per Yee vertex: three E edges and three H faces, each with stage input,
         # step value, accumulator read/write and stage output; dM/dt and dP/dt
-        per_comp = 1 + 0.75 + 0.75 + 0.75 + 1
+        per_comp = 1 + 0.75 + 0.75 + 0.75 + 1 + comp
         return (6 * per_comp + 3 * info.fm + 3 * info.fe) * D + 1
     return float("nan")
 
@@ -107,9 +115,9 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(kernel: str, workload: str):
+def committed_traffic(kernel: str, workload: str, mixed: bool = False):
     """dram read+write bytes per launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.json")
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}{'_mixed' if mixed else ''}.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -220,6 +228,126 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+TRACE_GROUPS = {"m": (0, 3), "p": (3, 6), "u": (6, 9), "E": (9, 12), "H": (12, 15)}
+
+
+def observe(eng, info, probe):
+    """<m>, <p>, <u>, probed E and H (zeros where a physics is off)."""
+    row = np.zeros(15)
+    if info.fm:
+        row[0:3] = eng.average("m")
+    if info.fe:
+        row[3:6] = eng.average("p")
+    if info.elastic:
+        row[6:9] = eng.average("u")
+    if info.em:
+        e, h = eng.probe_em(*probe)
+        row[9:12] = e
+        row[12:15] = h
+    return row
+
+
+def trace_error(mine, ref):
+    """Largest deviation of each vector observable over a trace, relative to
+    the observable's largest component magnitude in the FP64 trace."""
+    out = {}
+    for name, (a, b) in TRACE_GROUPS.items():
+        scale = float(np.max(np.abs(ref[:, a:b])))
+        if scale > 0.0:
+            out[name] = float(np.max(np.abs(mine[:, a:b] - ref[:, a:b]))) / scale
+    return out
+
+
+def measure(gf, torch, dist, args, world, local_rank, precision, d, ddir, uploads, probe):
+    """Trace, warm-up, device-timed steps, end-to-end steps and per-kernel
+    times of one engine on the deck in `ddir`."""
+    eng = gf.Engine(ddir, device=local_rank, precision=precision)
+    for name, arr in uploads:
+        eng.upload(name, arr)
+    info = eng.info
+    ncell = d.n
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
+
+    # observable trace from the initial state (compared across the two forms)
+    trace = [observe(eng, info, probe)]
+    for _ in range(args.trace_steps):
+        eng.advance(1)
+        trace.append(observe(eng, info, probe))
+    trace = np.array(trace)
+
+    # warm-up (also builds and uploads the CUDA graphs)
+    eng.advance(max(args.warmup, 1))
+    eng.synchronize()
+
+    # ---- device-timed region ----
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as cs:
+        ev0.record(stream)
+        eng.advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = cs.summary()
+    info = eng.get_info()
+    value = world * ncell * args.steps / (ms / 1e3)
+
+    # ---- end-to-end through the C ABI with host buffers ----
+    e2e_steps = max(1, min(args.steps, 20))
+    obs = [o for o, on in (("m", info.fm), ("m_afm1", info.afm), ("m_afm2", info.afm), ("p", info.fe),
+                           ("u", info.elastic)) if on]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.advance(1)                      # uploads the step's drive row (pinned H2D)
+        for o in obs:                       # D2H reads of the step's observables
+            eng.average(o)
+        if info.em:
+            eng.probe_em(*probe)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * ncell * e2e_steps / e2e_s
+    h2d = 520     # one StepDrive row per step (time + 4 stage rows of 128 B)
+    d2h = 8 * 3 * len(obs) + (8 * 6 if info.em else 0)  # averages, E and H at the probe cell
+
+    # ---- per-kernel device time for the roofline ----
+    prof = eng.profile_steps(2)
+    eng.check_finite()
+    eng.close()
+    return dict(value=value, ms=ms, clocks=clocks, info=info, trace=trace, prof=prof,
+                e2e={"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                     "steps": e2e_steps})
+
+
+def roofline(r, args, mfe_frac, mixed):
+    prof, info = r["prof"], r["info"]
+    kname = max(prof, key=lambda k: prof[k][1])
+    launches, total_ms = prof[kname]
+    avg_s = total_ms / launches / 1e3
+    units = units_per_launch(kname, info)
+    bpu = alg_bytes_per_unit(kname, info, mfe_frac, mixed)
+    achieved = bpu * units / avg_s / 1e9
+    peak, peak_kind = load_peaks()
+    step_ms_prof = sum(v[1] for v in prof.values()) / 2.0
+    return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": committed_traffic(kname, args.workload, mixed),
+            "alg_bytes_per_launch": bpu * units, "avg_launch_ms": avg_s * 1e3,
+            "share_of_step": total_ms / 2.0 / step_ms_prof}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import __graft_entry__
@@ -232,96 +360,34 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local_rank)
     spec = WORKLOADS[args.workload]
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    results = {}
     with tempfile.TemporaryDirectory() as tmp:
         d = build_deck(gf, args.workload, sample=False)
-        m0 = d.m0
-        d.m0 = None          # uploaded below instead of written as text
-        p0, q0 = d.p0, d.q0
+        uploads = []
+        if d.m0 is not None:
+            uploads.append(("m", d.m0))
+        if d.p0 is not None:
+            uploads += [("p", d.p0), ("q", d.q0)]
+        d.m0 = None          # uploaded instead of written as text
         d.p0 = None
         ddir = os.path.join(tmp, "deck")
         gf.decks.write_deck(d, ddir)
-        eng = gf.Engine(ddir, device=local_rank)
-        if m0 is not None:
-            eng.upload("m", m0)
-        if p0 is not None:
-            eng.upload("p", p0)
-            eng.upload("q", q0)
-        info = eng.info
-        ncell = d.n
         mc = d.material_cell()
         mfe_ids = [q + 1 for q, mt in enumerate(d.materials) if mt.fm or mt.fe]
         mfe_frac = float(np.isin(mc, mfe_ids).mean()) if mfe_ids else 0.0
-        stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
-
-        # warm-up (also builds and uploads the CUDA graphs)
-        eng.advance(max(args.warmup, 1))
-        eng.synchronize()
-
-        # ---- device-timed region ----
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local_rank) as cs:
-            ev0.record(stream)
-            eng.advance(args.steps)
-            ev1.record(stream)
-            ev1.synchronize()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        ms = ev0.elapsed_time(ev1)
-        if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        clocks = cs.summary()
-        info = eng.get_info()
-        value = world * ncell * args.steps / (ms / 1e3)
-
-        # ---- end-to-end through the C ABI with host buffers ----
-        e2e_steps = max(1, min(args.steps, 20))
-        obs = [o for o, on in (("m", info.fm), ("m_afm1", info.afm), ("m_afm2", info.afm), ("p", info.fe),
-                               ("u", info.elastic)) if on]
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            eng.advance(1)                      # uploads the step's drive row (pinned H2D)
-            for o in obs:                       # D2H reads of the step's observables
-                eng.average(o)
-            if info.em:
-                eng.probe_em(d.nx // 2, d.ny // 2, min(d.nz - 1, sum(l[0] for l in d.layers[:2]) - 2))
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e_value = world * ncell * e2e_steps / e2e_s
-        h2d = 520     # one StepDrive row per step (time + 4 stage rows of 128 B)
-        d2h = 8 * 3 * len(obs) + (8 * 6 if info.em else 0)  # averages, E and H at the probe cell
-
-        # ---- per-kernel device time for the roofline ----
-        prof = eng.profile_steps(2)
-        eng.check_finite()
-        eng.close()
+        probe = (d.nx // 2, d.ny // 2, min(d.nz - 1, sum(l[0] for l in d.layers[:2]) - 2))
+        for form in forms:
+            results[form] = measure(gf, torch, dist, args, world, local_rank, form, d, ddir, uploads, probe)
 
     if dist:
         dist.destroy_process_group()
     if rank != 0:
         return
-    kname = max(prof, key=lambda k: prof[k][1])
-    launches, total_ms = prof[kname]
-    avg_s = total_ms / launches / 1e3
-    units = units_per_launch(kname, info)
-    bpu = alg_bytes_per_unit(kname, info, mfe_frac)
-    achieved = bpu * units / avg_s / 1e9
-    peak, peak_kind = load_peaks()
-    step_ms_prof = sum(v[1] for v in prof.values()) / 2.0
-    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": committed_traffic(kname, args.workload),
-            "alg_bytes_per_launch": bpu * units, "avg_launch_ms": avg_s * 1e3,
-            "share_of_step": total_ms / 2.0 / step_ms_prof}
+    head_form = forms[0]
+    r = results[head_form]
+    info = r["info"]
+    ncell = d.n
 
     cpu = None
     if not args.no_cpu_baseline:
@@ -329,22 +395,39 @@ def run_ours(args, rank, world, local_rank):
             v, ci = cpu_reference(gf, args.workload, args.ref_steps, tmp, 3)
         if v is not None:
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "reference", "sample": ci["sample"]}
+    head_mixed = head_form == "mixed"
     line = {
-        "metric": "cell-steps/s FP64", "value": value, "unit": "cell-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": "cell-steps/s FP32-mixed" if head_mixed else "cell-steps/s FP64", "value": r["value"],
+        "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head_mixed else "f64",
+        "data": "synthetic",
         "config": {"workload": spec["desc"], "cells": ncell, "steps_timed": args.steps,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": f"state resident in HBM ({info.device_bytes / 1e9:.2f} GB) > L2 (126 MB): no flush needed",
                    "graph": "one CUDA graph per step parity"},
-        "roofline": roof,
+        "roofline": roofline(r, args, mfe_frac, head_mixed),
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps},
-        "clocks": clocks,
+        "e2e": r["e2e"],
+        "clocks": r["clocks"],
         "gpu_launches": int(info.launches_per_step) * args.steps,
-        "kernels_ms_per_step": {k: v[1] / 2.0 for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "kernels_ms_per_step": {k: v[1] / 2.0 for k, v in sorted(r["prof"].items(), key=lambda kv: -kv[1][1])},
     }
+    if "fp64" in results and "mixed" in results:
+        rm = results["mixed"]
+        err = trace_error(rm["trace"], results["fp64"]["trace"])
+        line["mixed"] = {
+            "metric": "cell-steps/s FP32-mixed", "value": rm["value"], "unit": "cell-steps/s",
+            "ms_per_step": rm["ms"] / args.steps, "speedup_vs_fp64": rm["value"] / r["value"],
+            "trace_error_vs_fp64": err, "trace_steps": args.trace_steps,
+            "max_trace_error": max(err.values()) if err else None,
+            "error_definition": "max over the trace of |mixed - fp64| / max|fp64 component| per vector observable",
+            "roofline": roofline(rm, args, mfe_frac, True), "e2e": rm["e2e"], "clocks": rm["clocks"],
+            "gpu_launches": int(rm["info"].launches_per_step) * args.steps,
+            "kernels_ms_per_step": {k: v[1] / 2.0 for k, v in sorted(rm["prof"].items(), key=lambda kv: -kv[1][1])},
+            "device_bytes": int(rm["info"].device_bytes),
+        }
+        line["gpu_launches"] += line["mixed"]["gpu_launches"]
     print(json.dumps(line))
 
 
@@ -357,6 +440,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="magnetoelastic")
     ap.add_argument("--ref-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both")
+    ap.add_argument("--trace-steps", type=int, default=100)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

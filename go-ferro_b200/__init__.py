@@ -19,7 +19,9 @@ import numpy as np
 from . import decks  # noqa: F401  (re-exported)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgoferro_b200.so")
+# GOFERRO_B200_LIB selects another build of the engine library (a build
+# with different tile or occupancy settings); default: the in-tree build
+LIB_PATH = os.environ.get("GOFERRO_B200_LIB") or os.path.join(_HERE, "libgoferro_b200.so")
 
 GF_OK = 0
 ERRORS = {-1: "GF_EINVAL", -2: "GF_EIO", -3: "GF_ECUDA", -4: "GF_ENOMEM", -5: "GF_ENAN",

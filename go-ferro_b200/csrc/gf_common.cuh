@@ -88,6 +88,7 @@ struct Params {
     int em_fromM, em_fromP, em_back_M, em_back_P;
     int has_eig0, has_strain0, has_hext_nonunif;
     int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
+    uint32_t fe_mask, fm_mask;   // bit id-1 set when material id is ferroelectric / ferromagnetic
     int drude;                // some material has a Drude pole (omega_plasma != 0)
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;

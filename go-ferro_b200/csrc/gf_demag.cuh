@@ -108,7 +108,7 @@ __device__ inline bool wrap_offset(long a, long n, long& off) {
 }
 
 // table t: 0 Axyz 1 Ayzx 2 Azxy 3 Bxyz 4 Byzx 5 Bzxy 6 Byxz 7 Bzyx 8 Bxzy
-__global__ void k_newell(Params P, double* tab /* 9 x n */) {
+static __global__ void k_newell(Params P, double* tab /* 9 x n */) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long nyz = (long)P.ny * P.nz;
@@ -142,7 +142,7 @@ __device__ inline cuDoubleComplex cadd(cuDoubleComplex a, cuDoubleComplex b) {
 }
 
 // M_k (3 x n21) and the nine spectra (9 x n21) -> H_k (3 x n21)
-__global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_neg, const cuDoubleComplex* __restrict__ Mk,
+static __global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_neg, const cuDoubleComplex* __restrict__ Mk,
                                                    const cuDoubleComplex* __restrict__ Nk, cuDoubleComplex* __restrict__ Hk) {
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n21) return;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_neg, con
 //         buffer holds the previous inverse transform, so every cell is set);
 // mode 1: demag factors H = M N_i; mode 2: 1-D model Hz = -Mz
 // (magnetostatic_solver.cpp:114-249)
-__global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F3 m, F3 a1, F3 a2, int mode, double* M3,
+static __global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F3 m, F3 a1, F3 a2, int mode, double* M3,
                              F3 Hs, double f0, double f1, double f2) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
@@ -194,14 +194,14 @@ __global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t* mid, F
 // ---- mixed form: FP32 transforms; the spectra are built in FP64 ----
 
 // complex FP64 -> FP32 (the Green spectra after the FP64 transform)
-__global__ void k_spectra_f32(const cuDoubleComplex* __restrict__ in, long n, cuComplex* __restrict__ out) {
+static __global__ void k_spectra_f32(const cuDoubleComplex* __restrict__ in, long n, cuComplex* __restrict__ out) {
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     out[q] = make_cuComplex((float)in[q].x, (float)in[q].y);
 }
 
 // k_demag_mul on FP32 spectra; inv_vol_neg = -1/(dx dy dz)
-__global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float inv_vol_neg, const cuComplex* __restrict__ Mk,
+static __global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float inv_vol_neg, const cuComplex* __restrict__ Mk,
                                                        const cuComplex* __restrict__ Nk, cuComplex* __restrict__ Hk) {
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n21) return;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float inv_vol_n
 }
 
 // k_mag_source for the mixed form (ferromagnets; the mixed form has no AFM)
-__global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, const uint8_t* mid, F3T<float> m, int mode,
+static __global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, const uint8_t* mid, F3T<float> m, int mode,
                                  float* M3, F3T<float> Hs, float f0, float f1, float f2) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;

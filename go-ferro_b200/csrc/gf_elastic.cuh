@@ -406,8 +406,13 @@ __device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, cons
     cp_async_wait_all();
 }
 
+// Resident blocks per SM the register allocation must allow: the FP32 tile
+// needs half the shared memory of the FP64 one, so more blocks fit.
+#ifndef GF_ETILE_MINB_F32
+#define GF_ETILE_MINB_F32 4
+#endif
 template <int S, bool CUB, class R = double>
-__global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat) {
+__global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_F32 : 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat) {
     using namespace etile;
     GF_EXTERN_SMEM(unsigned char, smem_raw);
     const ETileSmem<R> sm{smem_raw};
@@ -670,8 +675,67 @@ __global__ void __launch_bounds__(etile::NT, 2) k_elastic_tile(Params P, StageIO
 // f_store := f in stage 1 only), then the RK4 combination of v and u.  A
 // streaming kernel at full occupancy, so these loads and stores overlap
 // across many warps instead of waiting inside the tiled kernel's phases.
+// Mixed form: one thread updates two cells 256 apart, and every load of both
+// cells is issued before the first store (an FP32 access moves half the bytes
+// of an FP64 one, so twice the accesses must be in flight to stream at the
+// same rate).  The grid covers 512 cells per block.
+template <int S>
+struct RkCellF32 {
+    float f[3], fs[3], vx[3], vin[3], ux[3], vacc[3], uacc[3], vcmp[3], ucmp[3];
+    float dens_dt, mass_damp, stiff_damp;
+    uint8_t id;
+    __device__ void load(const StageIOT<float>& io, int c) {
+        id = io.mid[c];
+        if (id != 0) {
+            const DevMatT<float>& mt = io.mats[id - 1];
+            dens_dt = mt.dens_dt; mass_damp = mt.mass_damp; stiff_damp = mt.stiff_damp;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            f[a] = io.force.c[a][c]; fs[a] = io.force_store.c[a][c];
+            vx[a] = io.v_x.c[a][c]; vin[a] = io.v_in.c[a][c]; ux[a] = io.u_x.c[a][c];
+            if (S > 0) { vacc[a] = io.v_acc.c[a][c]; uacc[a] = io.u_acc.c[a][c]; }
+            if (S == 3) { vcmp[a] = io.v_cmp.c[a][c]; ucmp[a] = io.u_cmp.c[a][c]; }
+        }
+    }
+    __device__ void update(const StageIOT<float>& io, int c, float dt) const {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float dv = 0.f;
+            if (id != 0) {
+                const float w = (S == 1 || S == 2) ? 2.f : 1.f;
+                dv = f[a] * dens_dt + mass_damp * vx[a] + stiff_damp * (f[a] - fs[a]) * w;
+                if (S == 0) io.force_store.c[a][c] = f[a];
+            }
+            const float du = vin[a] * dt;
+            if (S < 3) {
+                const float cf = (S == 2) ? 1.f : 0.5f;
+                io.v_out.c[a][c] = vx[a] + dv * cf;
+                io.u_out.c[a][c] = ux[a] + du * cf;
+                io.v_acc.c[a][c] = (S == 0) ? dv * (1.f / 6.f) : vacc[a] + dv * (1.f / 3.f);
+                io.u_acc.c[a][c] = (S == 0) ? du * (1.f / 6.f) : uacc[a] + du * (1.f / 3.f);
+            } else {
+                float sum, err;
+                two_sum(vx[a], (vacc[a] + dv * (1.f / 6.f)) + vcmp[a], sum, err);
+                io.v_acc.c[a][c] = sum; io.v_cmp.c[a][c] = err;
+                two_sum(ux[a], (uacc[a] + du * (1.f / 6.f)) + ucmp[a], sum, err);
+                io.u_acc.c[a][c] = sum; io.u_cmp.c[a][c] = err;
+            }
+        }
+    }
+};
+
 template <int S, class R = double>
 __global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
+    if constexpr (is_mixed<R>::value) {
+        const int c0 = blockIdx.x * 512 + threadIdx.x, c1 = c0 + 256;
+        RkCellF32<S> a, b;
+        if (c0 < P.n) a.load(io, c0);
+        if (c1 < P.n) b.load(io, c1);
+        if (c0 < P.n) a.update(io, c0, P.f.dt);
+        if (c1 < P.n) b.update(io, c1, P.f.dt);
+        return;
+    }
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = io.mid[c];

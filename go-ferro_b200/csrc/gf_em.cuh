@@ -114,6 +114,12 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
             curl = dHydx - dHxdy;
         }
         R Jf = R(0.), dP = R(0.), er = R(0.), cond = R(0.), pc = R(0.);
+        // dP/dt of the four cells, loaded before their ids are known
+        R qv[4] = {R(0.), R(0.), R(0.), R(0.)};
+        if (P.em_fromP) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) qv[q] = io.q_in.c[C][(cx[q] * ny + cy[q]) * nz + cz[q]];
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
@@ -122,7 +128,7 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
                 er = er + R(1.);
             } else {
                 const EmMat<R>& m = mt[id - 1];
-                if (P.em_fromP) dP = dP + io.q_in.c[C][cc] * dt_r;
+                if (P.em_fromP) dP = dP + qv[q] * dt_r;
                 if (m.flags & MF_FE) pc = pc + R(1.);
                 er = er + m.er;
                 cond = cond + m.cond;
@@ -187,12 +193,14 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
     R dM1 = R(0.), dM2 = R(0.), cnt = R(0.);
     {
         const int c1 = (a1x * ny + a1y) * nz + a1z, c2 = (a2x * ny + a2y) * nz + a2z;
+        // dm of both face cells, loaded before their ids are known
+        const R dm1 = P.em_fromM ? io.dm.c[C][c1] : R(0.), dm2 = P.em_fromM ? io.dm.c[C][c2] : R(0.);
         const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
         // Ms dm + Ms1 dm1 + Ms2 dm2 of each face cell (EMdynamic_solver.cpp:2300-2306)
         if (i1 != 0) {
             const EmMat<R>& m = mt[i1 - 1];
             if (P.em_fromM) {
-                dM1 = io.dm.c[C][c1] * m.Ms;
+                dM1 = dm1 * m.Ms;
                 if (P.afm) dM1 = dM1 + io.da1.c[C][c1] * m.Ms1 + io.da2.c[C][c1] * m.Ms2;
             }
             if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
@@ -200,7 +208,7 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
         if (i2 != 0) {
             const EmMat<R>& m = mt[i2 - 1];
             if (P.em_fromM) {
-                dM2 = io.dm.c[C][c2] * m.Ms;
+                dM2 = dm2 * m.Ms;
                 if (P.afm) dM2 = dM2 + io.da1.c[C][c2] * m.Ms1 + io.da2.c[C][c2] * m.Ms2;
             }
             if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
@@ -219,10 +227,13 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
 // H only the stage E and dm, so the six updates are independent.  The grid
 // is (blocks over the (j,k) vertex plane) x (nx+1 planes); the material
 // constants are staged in shared memory.
+#ifndef GF_EM_MINB_F32
+#define GF_EM_MINB_F32 8
+#endif
 template <int S, class R = double>
 // (256, 8): 32 registers, 64 resident warps per SM; the kernel is bound by
 // the latency of its neighbour loads, and full occupancy beats the spills
-__global__ void __launch_bounds__(256, 8) k_em_fused(Params P, StageIOT<R> io, int nmat) {
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) k_em_fused(Params P, StageIOT<R> io, int nmat) {
     __shared__ EmMat<R> mt[kMaxMat];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMatT<R>& d = io.mats[q];

@@ -38,12 +38,6 @@
 
 using namespace gf;
 
-namespace {
-
-constexpr int kThreads = 256;
-constexpr long kDriveCap = 4096;      // steps of time-dependent drive held on the device (power of two)
-thread_local std::string g_create_err;
-
 struct Field3 {
     // X, A, S0, S1 per component; len[c] = elements of component c
     double* X[3] = {nullptr, nullptr, nullptr};
@@ -54,6 +48,12 @@ struct Field3 {
     long len[3] = {0, 0, 0};
     bool on = false;
 };
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr long kDriveCap = 4096;      // steps of time-dependent drive held on the device (power of two)
+thread_local std::string g_create_err;
 
 }  // namespace
 
@@ -129,6 +129,13 @@ struct gf_engine {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool graphs_ready = false;
 };
+
+// The mixed form's stage kernels are instantiated only in gf_mixed.cu, which
+// includes this file with GF_MIXED_TU defined and is compiled with FMA
+// contraction (the FP64 parity kernels here must not contract).  These two
+// functions are its interface.
+int gf_mixed_enqueue_step(gf_engine* eng, int parity);                 // kernels of one step, mixed form
+int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-memory opt-in, occupancy
 
 namespace {
 
@@ -378,6 +385,11 @@ void build_params(gf_engine* eng) {
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) { P.f.Tg2c[i][j] = (float)P.Tg2c[i][j]; P.f.Tc2g[i][j] = (float)P.Tc2g[i][j]; }
     P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
+    P.fe_mask = 0u; P.fm_mask = 0u;
+    for (size_t q = 0; q < d.mats.size() && q < 32; q++) {
+        if (d.mats[q].fe) P.fe_mask |= 1u << q;
+        if (d.mats[q].fm) P.fm_mask |= 1u << q;
+    }
     {
         long lo[3] = {d.nx, d.ny, d.nz}, hi[3] = {-1, -1, -1};
         for (long i = 0; i < d.nx; i++)
@@ -713,6 +725,7 @@ int set_elastic_smem(gf_engine* eng, int smem) {
     return GF_OK;
 }
 
+#ifndef GF_MIXED_TU
 int setup_elastic_tile(gf_engine* eng) {
     const Params& P = eng->P;
     eng->el_nmat = (int)eng->deck.mats.size();
@@ -725,8 +738,7 @@ int setup_elastic_tile(gf_engine* eng) {
                 if (!((a < 3 && b < 3) || a == b) && m.cij[a][b] != 0.) eng->el_cubic = false;
     int per_sm = 1, sms = 1;
     if (eng->mixed) {
-        GF_TRY(set_elastic_smem<float>(eng, smem));
-        GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false, float>, etile::NT, eng->el_smem));
+        GF_TRY(gf_mixed_elastic_setup(eng, smem, &per_sm));
     } else {
         GF_TRY(set_elastic_smem<double>(eng, smem));
         GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_elastic_tile<1, false, double>, etile::NT, eng->el_smem));
@@ -744,13 +756,17 @@ int setup_elastic_tile(gf_engine* eng) {
     }
     return GF_OK;
 }
+#endif  // GF_MIXED_TU
 
 template <class R> const StageIOT<R>& stage_io(const gf_engine* eng, int parity, int s);
-template <> const StageIOT<double>& stage_io<double>(const gf_engine* eng, int parity, int s) { return eng->io[parity][s]; }
-template <> const StageIOT<float>& stage_io<float>(const gf_engine* eng, int parity, int s) { return eng->iof[parity][s]; }
 template <class R> const LLGTablesT<R>* llg_tables(const gf_engine* eng);
-template <> const LLGTablesT<double>* llg_tables<double>(const gf_engine* eng) { return eng->llg_tab; }
+#ifdef GF_MIXED_TU
+template <> const StageIOT<float>& stage_io<float>(const gf_engine* eng, int parity, int s) { return eng->iof[parity][s]; }
 template <> const LLGTablesT<float>* llg_tables<float>(const gf_engine* eng) { return eng->llg_tab_f; }
+#else
+template <> const StageIOT<double>& stage_io<double>(const gf_engine* eng, int parity, int s) { return eng->io[parity][s]; }
+template <> const LLGTablesT<double>* llg_tables<double>(const gf_engine* eng) { return eng->llg_tab; }
+#endif
 
 // magnetostatic field of magnetisation m into Hstat (FFT, demag factors or
 // the 1-D model), FP64 form
@@ -824,7 +840,9 @@ int enqueue_stage(gf_engine* eng, int parity) {
         else
             GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false, R>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
                                 eng->el_chunk, eng->el_nmat));
-        GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S, R>, dim3(bn), dim3(kThreads), 0, st, P, io));
+        // the mixed form's RK kernel updates two cells per thread
+        const unsigned brk = is_mixed<R>::value ? blocks_for(P.n, 2 * kThreads) : bn;
+        GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S, R>, dim3(brk), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S, R>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
@@ -866,9 +884,22 @@ int enqueue_step_t(gf_engine* eng, int parity) {
     return GF_OK;
 }
 
+}  // namespace
+
+#ifdef GF_MIXED_TU
+int gf_mixed_enqueue_step(gf_engine* eng, int parity) { return enqueue_step_t<float>(eng, parity); }
+
+int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm) {
+    GF_TRY(set_elastic_smem<float>(eng, smem));
+    GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_elastic_tile<1, false, float>, etile::NT, (size_t)smem));
+    return GF_OK;
+}
+#else
+namespace {
+
 int enqueue_step(gf_engine* eng, int parity) {
     eng->launch_counter = 0;
-    if (eng->mixed) GF_TRY(enqueue_step_t<float>(eng, parity));
+    if (eng->mixed) GF_TRY(gf_mixed_enqueue_step(eng, parity));
     else GF_TRY(enqueue_step_t<double>(eng, parity));
     GF_CU(klaunch(eng, "k_step_inc", k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
     eng->launches_per_step = eng->launch_counter;
@@ -1731,3 +1762,5 @@ int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, doub
 
 
 }  // extern "C"
+
+#endif  // GF_MIXED_TU

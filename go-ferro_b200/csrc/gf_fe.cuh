@@ -20,9 +20,14 @@ __device__ inline bool is_fe(const DevMatT<R>* mats, uint8_t id) {
 }
 
 // Grid: (blocks over the (j,k) plane) x (nx planes), 32-bit indices.
+#ifndef GF_FE_MINB_F32
+#define GF_FE_MINB_F32 4
+#endif
 template <int S, class R = double>
-// (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4 blocks)
-__global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIOT<R> io) {
+// FP64 (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4
+// blocks); FP32 (256, 4): 64 registers, 32 warps (0.70 -> 0.56 ms per step
+// on the 128^3 ferroelectric workload)
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : 3) k_fe(Params P, StageIOT<R> io) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ny * nz) return;
@@ -31,7 +36,10 @@ __global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIOT<R> io) {
     const uint8_t id = io.mid[c];
     R dq[3] = {R(0.), R(0.), R(0.)};
 
-    if (is_fe(io.mats, id)) {
+    // material classes from the run's bitmask: no table load on the path to
+    // the neighbour loads
+    auto fe_id = [&](uint8_t q) { return q != 0 && ((P.fe_mask >> (q - 1)) & 1u); };
+    if (fe_id(id)) {
         const DevMatT<R>& mt = io.mats[id - 1];
         const R pxg = io.p_in.c[0][c], pyg = io.p_in.c[1][c], pzg = io.p_in.c[2][c];
 
@@ -41,21 +49,31 @@ __global__ void __launch_bounds__(256, 3) k_fe(Params P, StageIOT<R> io) {
         const int kb = (k == 0) ? nz - 1 : k - 1, kF = (k == nz - 1) ? 0 : k + 1;
         const int nb[6] = {(ib * ny + j) * nz + k, (iF * ny + j) * nz + k, (i * ny + jb) * nz + k,
                            (i * ny + jF) * nz + k, (i * ny + j) * nz + kb, (i * ny + j) * nz + kF};
-        const bool surf[6] = {(i == 0 && !P.per_x) || !is_fe(io.mats, io.mid[nb[0]]),
-                              (i == nx - 1 && !P.per_x) || !is_fe(io.mats, io.mid[nb[1]]),
-                              (j == 0 && !P.per_y) || !is_fe(io.mats, io.mid[nb[2]]),
-                              (j == ny - 1 && !P.per_y) || !is_fe(io.mats, io.mid[nb[3]]),
-                              (k == 0 && !P.per_z) || !is_fe(io.mats, io.mid[nb[4]]),
-                              (k == nz - 1 && !P.per_z) || !is_fe(io.mats, io.mid[nb[5]])};
+        // the six neighbours' p is loaded whether or not it is used (the
+        // wrapped indices are always inside the array), so these loads do not
+        // wait for the neighbour ids
+        R pn[3][6];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int f = 0; f < 6; f++) pn[a][f] = io.p_in.c[a][nb[f]];
+        const bool surf[6] = {(i == 0 && !P.per_x) || !fe_id(io.mid[nb[0]]),
+                              (i == nx - 1 && !P.per_x) || !fe_id(io.mid[nb[1]]),
+                              (j == 0 && !P.per_y) || !fe_id(io.mid[nb[2]]),
+                              (j == ny - 1 && !P.per_y) || !fe_id(io.mid[nb[3]]),
+                              (k == 0 && !P.per_z) || !fe_id(io.mid[nb[4]]),
+                              (k == nz - 1 && !P.per_z) || !fe_id(io.mid[nb[5]])};
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
         const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
         R lap[3];   // sum of the three second derivatives per component
+#pragma unroll
         for (int a = 0; a < 3; a++) {
             const R pc = io.p_in.c[a][c];
             R d2[3];
+#pragma unroll
             for (int dir = 0; dir < 3; dir++) {
-                const R pb = surf[2 * dir] ? pc : io.p_in.c[a][nb[2 * dir]];
-                const R pf = surf[2 * dir + 1] ? pc : io.p_in.c[a][nb[2 * dir + 1]];
+                const R pb = surf[2 * dir] ? pc : pn[a][2 * dir];
+                const R pf = surf[2 * dir + 1] ? pc : pn[a][2 * dir + 1];
                 d2[dir] = qdivR(qdivR(pf - R(2.) * pc + pb, h[dir], rh[dir], rhf[dir]), h[dir], rh[dir], rhf[dir]);
             }
             lap[a] = d2[0] + d2[1] + d2[2];

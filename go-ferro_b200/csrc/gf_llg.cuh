@@ -108,6 +108,17 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
         const int cxb = (ib * ny + j) * nz + k, cxf = (iF * ny + j) * nz + k;
         const int cyb = (i * ny + jb) * nz + k, cyf = (i * ny + jF) * nz + k;
         const int czb = (i * ny + j) * nz + kb, czf = (i * ny + j) * nz + kF;
+        // the six neighbours' m is loaded whether or not the face is a surface
+        // (the wrapped indices are always inside the array), so these loads do
+        // not wait for the neighbour ids
+        R nm[6][3];
+        {
+            const int ncell[6] = {cxb, cxf, cyb, cyf, czb, czf};
+#pragma unroll
+            for (int f = 0; f < 6; f++)
+#pragma unroll
+                for (int a = 0; a < 3; a++) nm[f][a] = io.m_in.c[a][ncell[f]];
+        }
         const uint8_t idxb = io.mid[cxb], idxf = io.mid[cxf], idyb = io.mid[cyb], idyf = io.mid[cyf];
         const uint8_t idzb = io.mid[czb], idzf = io.mid[czf];
         // a face is an FM surface when the neighbour across it is not FM, or
@@ -121,17 +132,17 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
 
         R dxb[3], dxf[3], dyb[3], dyf[3], dzb[3], dzf[3];
         if (sxb) { dxb[0] = -dA * mzc; dxb[1] = zero; dxb[2] = dA * mxc; }
-        else { dxb[0] = qdivR((mxc - io.m_in.c[0][cxb]), P.dx, P.rdx, P.f.rdx); dxb[1] = qdivR((myc - io.m_in.c[1][cxb]), P.dx, P.rdx, P.f.rdx); dxb[2] = qdivR((mzc - io.m_in.c[2][cxb]), P.dx, P.rdx, P.f.rdx); }
+        else { dxb[0] = qdivR((mxc - nm[0][0]), P.dx, P.rdx, P.f.rdx); dxb[1] = qdivR((myc - nm[0][1]), P.dx, P.rdx, P.f.rdx); dxb[2] = qdivR((mzc - nm[0][2]), P.dx, P.rdx, P.f.rdx); }
         if (sxf) { dxf[0] = -dA * mzc; dxf[1] = zero; dxf[2] = dA * mxc; }
-        else { dxf[0] = qdivR((io.m_in.c[0][cxf] - mxc), P.dx, P.rdx, P.f.rdx); dxf[1] = qdivR((io.m_in.c[1][cxf] - myc), P.dx, P.rdx, P.f.rdx); dxf[2] = qdivR((io.m_in.c[2][cxf] - mzc), P.dx, P.rdx, P.f.rdx); }
+        else { dxf[0] = qdivR((nm[1][0] - mxc), P.dx, P.rdx, P.f.rdx); dxf[1] = qdivR((nm[1][1] - myc), P.dx, P.rdx, P.f.rdx); dxf[2] = qdivR((nm[1][2] - mzc), P.dx, P.rdx, P.f.rdx); }
         if (syb) { dyb[0] = zero; dyb[1] = -dA * mzc; dyb[2] = dA * myc; }
-        else { dyb[0] = qdivR((mxc - io.m_in.c[0][cyb]), P.dy, P.rdy, P.f.rdy); dyb[1] = qdivR((myc - io.m_in.c[1][cyb]), P.dy, P.rdy, P.f.rdy); dyb[2] = qdivR((mzc - io.m_in.c[2][cyb]), P.dy, P.rdy, P.f.rdy); }
+        else { dyb[0] = qdivR((mxc - nm[2][0]), P.dy, P.rdy, P.f.rdy); dyb[1] = qdivR((myc - nm[2][1]), P.dy, P.rdy, P.f.rdy); dyb[2] = qdivR((mzc - nm[2][2]), P.dy, P.rdy, P.f.rdy); }
         if (syf) { dyf[0] = zero; dyf[1] = -dA * mzc; dyf[2] = dA * myc; }
-        else { dyf[0] = qdivR((io.m_in.c[0][cyf] - mxc), P.dy, P.rdy, P.f.rdy); dyf[1] = qdivR((io.m_in.c[1][cyf] - myc), P.dy, P.rdy, P.f.rdy); dyf[2] = qdivR((io.m_in.c[2][cyf] - mzc), P.dy, P.rdy, P.f.rdy); }
+        else { dyf[0] = qdivR((nm[3][0] - mxc), P.dy, P.rdy, P.f.rdy); dyf[1] = qdivR((nm[3][1] - myc), P.dy, P.rdy, P.f.rdy); dyf[2] = qdivR((nm[3][2] - mzc), P.dy, P.rdy, P.f.rdy); }
         if (szb) { dzb[0] = zero; dzb[1] = zero; dzb[2] = zero; }
-        else { dzb[0] = qdivR((mxc - io.m_in.c[0][czb]), P.dz, P.rdz, P.f.rdz); dzb[1] = qdivR((myc - io.m_in.c[1][czb]), P.dz, P.rdz, P.f.rdz); dzb[2] = qdivR((mzc - io.m_in.c[2][czb]), P.dz, P.rdz, P.f.rdz); }
+        else { dzb[0] = qdivR((mxc - nm[4][0]), P.dz, P.rdz, P.f.rdz); dzb[1] = qdivR((myc - nm[4][1]), P.dz, P.rdz, P.f.rdz); dzb[2] = qdivR((mzc - nm[4][2]), P.dz, P.rdz, P.f.rdz); }
         if (szf) { dzf[0] = zero; dzf[1] = zero; dzf[2] = zero; }
-        else { dzf[0] = qdivR((io.m_in.c[0][czf] - mxc), P.dz, P.rdz, P.f.rdz); dzf[1] = qdivR((io.m_in.c[1][czf] - myc), P.dz, P.rdz, P.f.rdz); dzf[2] = qdivR((io.m_in.c[2][czf] - mzc), P.dz, P.rdz, P.f.rdz); }
+        else { dzf[0] = qdivR((nm[5][0] - mxc), P.dz, P.rdz, P.f.rdz); dzf[1] = qdivR((nm[5][1] - myc), P.dz, P.rdz, P.f.rdz); dzf[2] = qdivR((nm[5][2] - mzc), P.dz, P.rdz, P.f.rdz); }
 
         const R dmxdx = (dxb[0] + dxf[0]) * R(0.5);
         const R dmzdx = (dxb[2] + dxf[2]) * R(0.5);

@@ -6,12 +6,12 @@
 
 namespace gf {
 
-__global__ void k_step_inc(unsigned long long* step) { *step = *step + 1ull; }
+static __global__ void k_step_inc(unsigned long long* step) { *step = *step + 1ull; }
 
 // Deterministic sum: thread t of T adds elements t, t+T, t+2T, ... of
 // `in` (length n) in index order and writes partial[t].  Applied three times
 // (n -> 8192 -> 64 -> 1) the result depends only on n, never on scheduling.
-__global__ void k_sum_stride(const double* __restrict__ in, long n, double* __restrict__ partial, long T) {
+static __global__ void k_sum_stride(const double* __restrict__ in, long n, double* __restrict__ partial, long T) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     double acc = 0.;
@@ -29,7 +29,7 @@ __device__ inline unsigned long long mix64(unsigned long long z) {
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
     return z ^ (z >> 31);
 }
-__global__ void k_check_quotients(double d, double rd, unsigned long long n, unsigned long long seed,
+static __global__ void k_check_quotients(double d, double rd, unsigned long long n, unsigned long long seed,
                                   unsigned long long* bad) {
     const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
     unsigned long long local = 0;
@@ -52,10 +52,10 @@ __global__ void k_check_quotients(double d, double rd, unsigned long long n, uns
 }
 
 // x[0] := x[0] / d  (single thread; the mean of gf_field_mean_noalloc)
-__global__ void k_scale(double* x, double d) { x[0] = x[0] / d; }
+static __global__ void k_scale(double* x, double d) { x[0] = x[0] / d; }
 
 // flag := 1 if any element of in[0..n) is not finite
-__global__ void k_check_finite(const double* __restrict__ in, long n, int* flag) {
+static __global__ void k_check_finite(const double* __restrict__ in, long n, int* flag) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long T = (long)gridDim.x * blockDim.x;
     for (long i = t; i < n; i += T) {
@@ -94,7 +94,7 @@ __global__ void k_em_cell(Params P, F3T<R> E, F3T<R> H, F3 Ec, F3 Hc) {
 // ---------------------------------------------------------------------------
 
 // as k_sum_stride, over the FP64 values x + c of an FP32 pair (c may be null)
-__global__ void k_sum_stride_f32(const float* __restrict__ x, const float* __restrict__ cm, long n,
+static __global__ void k_sum_stride_f32(const float* __restrict__ x, const float* __restrict__ cm, long n,
                                  double* __restrict__ partial, long T) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
@@ -104,14 +104,14 @@ __global__ void k_sum_stride_f32(const float* __restrict__ x, const float* __res
 }
 
 // out = x + c in FP64 (c may be null)
-__global__ void k_widen(const float* __restrict__ x, const float* __restrict__ cm, long n, double* __restrict__ out) {
+static __global__ void k_widen(const float* __restrict__ x, const float* __restrict__ cm, long n, double* __restrict__ out) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     out[i] = (double)x[i] + (cm ? (double)cm[i] : 0.);
 }
 
 // x = RN_f32(in), c = RN_f32(in - x) (c may be null)
-__global__ void k_split(const double* __restrict__ in, long n, float* __restrict__ x, float* __restrict__ cm) {
+static __global__ void k_split(const double* __restrict__ in, long n, float* __restrict__ x, float* __restrict__ cm) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double v = in[i];
@@ -120,7 +120,7 @@ __global__ void k_split(const double* __restrict__ in, long n, float* __restrict
     if (cm) cm[i] = (float)(v - (double)h);
 }
 
-__global__ void k_check_finite_f32(const float* __restrict__ in, long n, int* flag) {
+static __global__ void k_check_finite_f32(const float* __restrict__ in, long n, int* flag) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long T = (long)gridDim.x * blockDim.x;
     for (long i = t; i < n; i += T) {
