@@ -37,7 +37,9 @@ PRECISION = {"fp64": 0, "mixed": 1}   # GF_PRECISION_FP64, GF_PRECISION_MIXED_FP
 EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_advance_eager", "gf_average", "gf_probe_em",
            "gf_field_dims", "gf_download", "gf_upload", "gf_download_device", "gf_upload_device",
            "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
-           "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients"]
+           "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients",
+           "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
+           "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy"]
 
 
 class GFInfo(ctypes.Structure):
@@ -100,6 +102,14 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_version.restype = ctypes.c_char_p
     lib.gf_field_mean_noalloc.argtypes = [vp, c_u64, ctypes.c_double, vp, vp]
     lib.gf_check_quotients.argtypes = [ctypes.c_double, c_u64, c_u64, ctypes.POINTER(c_u64)]
+    lib.gf_adjoint_create.argtypes = [vp, c_int, c_int, ctypes.POINTER(vp)]
+    lib.gf_adjoint_set_alpha.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
+    lib.gf_adjoint_set_waveform.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
+    lib.gf_adjoint_forward.argtypes = [vp, c_u64, c_dbl_p]
+    lib.gf_adjoint_backward.argtypes = [vp, c_dbl_p, c_dbl_p, c_dbl_p]
+    lib.gf_adjoint_final_m.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
+    lib.gf_adjoint_destroy.argtypes = [vp]
+    lib.gf_adjoint_destroy.restype = None
     if path is None:
         _lib = lib
     return lib
@@ -200,3 +210,71 @@ class Engine:
 
 def version() -> str:
     return load_library().gf_version().decode()
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Adjoint:
+    """Discrete adjoint of an FP64 engine's ferromagnetic RK4 step
+    (gf_adjoint_*): <m_x>(t) forward from the engine's current state, and the
+    gradients of a loss of that trace with respect to an x-directed
+    excitation waveform (n_wave piecewise-constant samples, A/m) and the
+    per-cell damping alpha."""
+
+    def __init__(self, engine: "Engine", n_wave: int, checkpoint_every: int = 200):
+        self.engine = engine
+        self.lib = engine.lib
+        self.n_wave = int(n_wave)
+        h = ctypes.c_void_p()
+        engine._check(self.lib.gf_adjoint_create(engine.h, self.n_wave, int(checkpoint_every), ctypes.byref(h)))
+        self.h = h
+        self.n = engine.info.nx * engine.info.ny * engine.info.nz
+        self.nsteps = None
+
+    def set_alpha(self, alpha: np.ndarray) -> None:
+        a = np.ascontiguousarray(alpha, dtype=np.float64).ravel()
+        self.engine._check(self.lib.gf_adjoint_set_alpha(self.h, _dp(a), a.size))
+
+    def set_waveform(self, w: np.ndarray) -> None:
+        a = np.ascontiguousarray(w, dtype=np.float64).ravel()
+        self.engine._check(self.lib.gf_adjoint_set_waveform(self.h, _dp(a), a.size))
+
+    def forward(self, nsteps: int) -> np.ndarray:
+        tr = np.empty(int(nsteps) + 1, dtype=np.float64)
+        self.engine._check(self.lib.gf_adjoint_forward(self.h, int(nsteps), _dp(tr)))
+        self.nsteps = int(nsteps)
+        return tr
+
+    def backward(self, dloss_dmx: np.ndarray):
+        g = np.ascontiguousarray(dloss_dmx, dtype=np.float64).ravel()
+        if self.nsteps is None or g.size != self.nsteps + 1:
+            raise ValueError("dloss_dmx needs nsteps+1 values of the last forward run")
+        gw = np.empty(self.n_wave, dtype=np.float64)
+        ga = np.empty(self.n, dtype=np.float64)
+        self.engine._check(self.lib.gf_adjoint_backward(self.h, _dp(g), _dp(gw), _dp(ga)))
+        return gw, ga
+
+    def final_m(self) -> np.ndarray:
+        m = np.empty(3 * self.n, dtype=np.float64)
+        self.engine._check(self.lib.gf_adjoint_final_m(self.h, _dp(m), m.size))
+        i = self.engine.info
+        return m.reshape(3, i.nx, i.ny, i.nz)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gf_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -35,6 +35,7 @@
 #include "gf_em.cuh"
 #include "gf_demag.cuh"
 #include "gf_util.cuh"
+#include "gf_adjoint.cuh"
 
 using namespace gf;
 
@@ -1695,6 +1696,426 @@ int gf_check_quotients(double d, uint64_t n, uint64_t seed, uint64_t* mismatches
 }
 
 const char* gf_version(void) { return "goferro_b200 0.2 (FP64 parity form, FP32 mixed form, sm_100a)"; }
+
+}  // extern "C"
+
+
+// ===========================================================================
+// Discrete adjoint of the ferromagnetic RK4 step (gf_adjoint_*)
+//
+// The forward run starts from the engine's current m and external-field
+// clock, keeps the state every `ck_every` steps, and records <m_x> of every
+// step.  The backward run walks the blocks between checkpoints in reverse:
+// it recomputes and stores the block's step values, then for each step
+// recomputes the four stage states and fields (demag of each stage by FFT)
+// and applies the reverse RK4 sweep of gf_adjoint.cuh, accumulating the
+// damping and waveform gradients.
+// ===========================================================================
+struct gf_adjoint {
+    gf_engine* eng = nullptr;
+    int nw = 0, ck_every = 0, nmat = 0;
+    uint64_t nsteps = 0;
+    bool ran = false;
+    std::vector<void*> allocs;
+    AdjMat* am = nullptr;
+    double* aij = nullptr;           // (nmat+1)^2 harmonic-mean exchange constants
+    double* alpha = nullptr;         // per cell
+    std::vector<double> wave;        // excitation samples (A/m, x)
+    std::vector<double> hext;        // nsteps x 4 x 3 external field of the deck per stage
+    double* X[3] = {};               // step value
+    double* Y[3][3] = {};            // stage states y2, y3, y4
+    double* ACC[3] = {};
+    double* HS[4][3] = {};           // effective field of each stage
+    double* XJ[3] = {};              // stage-4 output of a recomputed step (discarded)
+    double* LAM[3] = {}; double* LAMACC[3] = {}; double* U[3] = {};
+    double* YBAR[3] = {}; double* HBAR[3] = {};
+    double* abar = nullptr; double* hbx = nullptr; double* wbar = nullptr;
+    double* trace = nullptr;         // nsteps+1
+    double* dldm = nullptr;          // nsteps+1
+    double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x 3n
+    double* xs = nullptr;            // step values of one block, ck_every x 3n
+    double* zero3 = nullptr;         // 3n zeros (demag field when magnetostatics is off)
+    size_t ck_slots = 0;
+};
+
+namespace {
+
+// zeroed device buffer, complete on return (host copies may follow at once)
+int adj_alloc(gf_adjoint* a, double** p, size_t count) {
+    gf_engine* eng = a->eng;
+    GF_CU(cudaMalloc(p, count * sizeof(double)));
+    a->allocs.push_back(*p);
+    GF_CU(cudaMemsetAsync(*p, 0, count * sizeof(double), eng->stream));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
+}
+
+int adj_alloc3(gf_adjoint* a, double* f[3]) {
+    for (int c = 0; c < 3; c++) GF_TRY(adj_alloc(a, &f[c], (size_t)a->eng->P.n));
+    return GF_OK;
+}
+
+F3 f3v(double* base, long n) { F3 r; for (int c = 0; c < 3; c++) r.c[c] = base + (size_t)c * n; return r; }
+
+// demag field of stage state y (3 x n, left in the FFT buffer), or zeros
+int adj_demag(gf_adjoint* a, F3 y, F3& hd) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    if (eng->demag_mode != 0) { hd = f3v(a->zero3, P.n); return GF_OK; }
+    cudaStream_t st = eng->stream;
+    GF_CU(launch(k_mag_source, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats,
+                 (const uint8_t*)eng->mid, y, F3{}, F3{}, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+    GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+    const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
+                 (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+    GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+    hd = f3v(eng->Mfft, P.n);
+    return GF_OK;
+}
+
+double3 adj_hext(const gf_adjoint* a, uint64_t step, int s) {
+    const double* h = &a->hext[(size_t)(step * 4 + s) * 3];
+    const size_t seg = (size_t)((step * (uint64_t)a->nw) / a->nsteps);
+    return make_double3(h[0] + a->wave[seg], h[1], h[2]);
+}
+
+// stages of step `step` from step value x: the effective fields go to HS,
+// the stage states to Y; stage 4 writes xout (x itself in the forward run)
+int adj_stages(gf_adjoint* a, F3 x, uint64_t step, F3 xout) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    F3 acc = f3(a->ACC);
+    F3 y = x;
+    for (int s = 0; s < 4; s++) {
+        F3 hd;
+        GF_TRY(adj_demag(a, y, hd));
+        const double3 he = adj_hext(a, step, s);
+        // stage 4 reads the step value from and writes the new one to xout:
+        // x itself in the forward run (each thread reads its own cell before
+        // writing it); a discarded buffer when a step is recomputed for the
+        // reverse sweep, which needs only the stage fields
+        F3 ynext = (s < 3) ? f3(a->Y[s]) : xout;
+        F3 xs_ = (s < 3) ? x : xout;
+        cudaError_t e;
+        if (s == 0) e = launch(k_adj_eval<0>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                               (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+        else if (s == 1) e = launch(k_adj_eval<1>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+        else if (s == 2) e = launch(k_adj_eval<2>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+        else e = launch(k_adj_eval<3>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                        (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+        GF_CU(e);
+        if (s < 3) y = f3(a->Y[s]);
+    }
+    return GF_OK;
+}
+
+// the stage-4 update of the forward run writes x in place: k_adj_eval<3>
+// reads x (the step value) and y4 (the stage state), so xout = x is safe
+int adj_step_forward(gf_adjoint* a, F3 x, uint64_t step) {
+    // stage 4 must combine with the step value x while writing it: the kernel
+    // reads x[c] before writing x[c] in the same thread only
+    return adj_stages(a, x, step, x);
+}
+
+int adj_mean_x(gf_adjoint* a, const double* x0, long slot) {
+    gf_engine* eng = a->eng;
+    cudaStream_t st = eng->stream;
+    double* p1 = eng->scratch + eng->scratch_main;
+    double* p2 = p1 + 8192;
+    double* p3 = p2 + 64;
+    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, x0, (long)eng->P.n, p1, 8192L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
+    GF_CU(launch(k_adj_store_slot, dim3(1), dim3(1), 0, st, a->trace, slot, (const double*)p3, 1. / (double)eng->deck.NFM));
+    return GF_OK;
+}
+
+int adj_wave_add(gf_adjoint* a, long seg) {
+    gf_engine* eng = a->eng;
+    cudaStream_t st = eng->stream;
+    double* p1 = eng->scratch + eng->scratch_main;
+    double* p2 = p1 + 8192;
+    double* p3 = p2 + 64;
+    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, (const double*)a->hbx, (long)eng->P.n, p1, 8192L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
+    GF_CU(launch(k_adj_add_slot, dim3(1), dim3(1), 0, st, a->wbar, seg, (const double*)p3));
+    return GF_OK;
+}
+
+// reverse sweep of step `step` (lambda = d loss / d x_{step+1} in LAM on entry,
+// d loss / d x_step on exit); x is the step value x_step
+int adj_step_backward(gf_adjoint* a, F3 x, uint64_t step) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    GF_TRY(adj_stages(a, x, step, f3(a->XJ)));
+    for (int c = 0; c < 3; c++) {
+        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    }
+    // u4 = lambda / 6 (written by a scaled copy: the comb kernel of a virtual stage 4)
+    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    GF_CU(launch(k_scale_f3, dim3(bn), dim3(kThreads), 0, st, P, f3(a->U), 1. / 6.));
+    const long seg = (long)((step * (uint64_t)a->nw) / a->nsteps);
+    for (int s = 3; s >= 0; s--) {
+        F3 y = (s == 0) ? x : f3(a->Y[s - 1]);
+        GF_CU(launch(k_adj_vjp, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, y,
+                     f3(a->HS[s]), f3(a->U), (const double*)a->alpha, f3(a->YBAR), f3(a->HBAR), a->abar, a->hbx));
+        const double* R = nullptr;
+        if (eng->demag_mode == 0) {
+            GF_CU(launch(k_adj_pack, dim3(bn), dim3(kThreads), 0, st, P, f3(a->HBAR), eng->Mfft));
+            GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+            const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+            GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
+                         (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+            GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+            R = eng->Mfft;
+        }
+        GF_CU(launch(k_adj_field_T, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                     (const double*)a->aij, a->nmat, f3(a->HBAR), R, f3(a->YBAR)));
+        GF_TRY(adj_wave_add(a, seg));
+        cudaError_t e;
+        if (s == 3) e = launch(k_adj_comb<3>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
+        else if (s == 2) e = launch(k_adj_comb<2>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
+        else if (s == 1) e = launch(k_adj_comb<1>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
+        else e = launch(k_adj_comb<0>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
+        GF_CU(e);
+    }
+    for (int c = 0; c < 3; c++) std::swap(a->LAM[c], a->LAMACC[c]);
+    return GF_OK;
+}
+
+int adj_check(gf_adjoint* a) {
+    if (!a || !a->eng) return GF_EINVAL;
+    return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint** out) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!out || n_wave < 1 || checkpoint_every < 1) { eng->err = "gf_adjoint_create: need n_wave >= 1, checkpoint_every >= 1 and an output"; return GF_EINVAL; }
+    *out = nullptr;
+    const Deck& d = eng->deck;
+    const Params& P = eng->P;
+    if (eng->mixed) { eng->err = "the adjoint runs on an FP64 engine"; return GF_EUNSUPPORTED; }
+    if (!d.any_fm || d.any_afm || d.any_fe || d.elastodynamics || d.em_dynamic)
+        { eng->err = "the adjoint covers ferromagnetic LLG with magnetostatics only (no AFM, FE, elastic or Maxwell fields)"; return GF_EUNSUPPORTED; }
+    if (P.rot) { eng->err = "the adjoint needs if_OrientRotate off"; return GF_EUNSUPPORTED; }
+    if (eng->demag_mode > 0) { eng->err = "the adjoint covers the FFT magnetostatics (no demag factors / 1-D model)"; return GF_EUNSUPPORTED; }
+    if (d.read_Hext_nonunif) { eng->err = "the adjoint does not cover a non-uniform external field"; return GF_EUNSUPPORTED; }
+    for (const Material& m : d.mats)
+        if (m.fm && m.iDMI != 0.) { eng->err = "the adjoint does not cover interfacial DMI"; return GF_EUNSUPPORTED; }
+    GF_CU(cudaSetDevice(eng->device));
+    gf_adjoint* a = new gf_adjoint();
+    a->eng = eng; a->nw = n_wave; a->ck_every = checkpoint_every;
+    a->nmat = (int)d.mats.size();
+    a->wave.assign((size_t)n_wave, 0.);
+    auto fail = [&](int rc) { gf_adjoint_destroy(a); return rc; };
+    int rc = GF_OK;
+    // material constants and the harmonic-mean exchange table
+    std::vector<AdjMat> am(d.mats.size());
+    for (size_t q = 0; q < d.mats.size(); q++) {
+        const Material& m = d.mats[q];
+        AdjMat& t = am[q];
+        std::memset(&t, 0, sizeof(t));
+        t.fm = m.fm ? 1u : 0u;
+        if (m.fm) {
+            t.gdt = m.gyro * d.dt; t.Ms = m.Ms; t.ex_coef = 2. / kMu0 / m.Ms; t.Aex = m.Aex;
+            t.K1c = m.K1 / kMu0 / m.Ms; t.K2c = m.K2 / kMu0 / m.Ms; t.aniso = (int)m.aniso_type;
+        }
+    }
+    std::vector<double> aij((size_t)(a->nmat + 1) * (a->nmat + 1), 0.);
+    for (int p = 0; p < a->nmat; p++)
+        for (int q = 0; q < a->nmat; q++) {
+            const double A1 = d.mats[p].Aex, A2 = d.mats[q].Aex;
+            aij[(size_t)(p + 1) * (a->nmat + 1) + q + 1] = (A1 + A2 != 0.) ? 2. * A1 * A2 / (A1 + A2) : 0.;
+        }
+    {
+        void* pm = nullptr;
+        if (cudaMalloc(&pm, sizeof(AdjMat) * am.size()) != cudaSuccess) { eng->err = "cudaMalloc (adjoint tables)"; return fail(GF_ENOMEM); }
+        a->allocs.push_back(pm);
+        a->am = (AdjMat*)pm;
+        if (cudaMemcpy(a->am, am.data(), sizeof(AdjMat) * am.size(), cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (adjoint tables)"; return fail(GF_ECUDA); }
+    }
+    if ((rc = adj_alloc(a, &a->aij, aij.size())) != GF_OK) return fail(rc);
+    if (cudaMemcpy(a->aij, aij.data(), sizeof(double) * aij.size(), cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (adjoint tables)"; return fail(GF_ECUDA); }
+    // per-cell damping, default the material's alpha
+    const long n = P.n;
+    if ((rc = adj_alloc(a, &a->alpha, (size_t)n)) != GF_OK) return fail(rc);
+    {
+        std::vector<double> al((size_t)n, 0.);
+        for (long c = 0; c < n; c++) {
+            const uint8_t id = d.material_cell[(size_t)c];
+            if (id && d.mats[id - 1].fm) al[(size_t)c] = d.mats[id - 1].alpha;
+        }
+        if (cudaMemcpy(a->alpha, al.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (alpha)"; return fail(GF_ECUDA); }
+    }
+    double** bufs3[] = {a->X, a->ACC, a->XJ, a->LAM, a->LAMACC, a->U, a->YBAR, a->HBAR,
+                        a->Y[0], a->Y[1], a->Y[2], a->HS[0], a->HS[1], a->HS[2], a->HS[3]};
+    for (double** b : bufs3)
+        if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->abar, (size_t)n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->hbx, (size_t)n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->zero3, (size_t)3 * n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * 3 * n)) != GF_OK) return fail(rc);
+    if (cudaStreamSynchronize(eng->stream) != cudaSuccess) { eng->err = "adjoint set-up"; return fail(GF_ECUDA); }
+    *out = a;
+    return GF_OK;
+}
+
+int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count) {
+    GF_TRY(adj_check(a));
+    gf_engine* eng = a->eng;
+    if (!alpha || count != (size_t)eng->P.n) { eng->err = "gf_adjoint_set_alpha: need nx*ny*nz values"; return GF_EINVAL; }
+    GF_CU(cudaMemcpy(a->alpha, alpha, sizeof(double) * count, cudaMemcpyHostToDevice));
+    return GF_OK;
+}
+
+int gf_adjoint_set_waveform(gf_adjoint* a, const double* w, size_t count) {
+    GF_TRY(adj_check(a));
+    gf_engine* eng = a->eng;
+    if (!w || count != (size_t)a->nw) { eng->err = "gf_adjoint_set_waveform: need n_wave values"; return GF_EINVAL; }
+    a->wave.assign(w, w + count);
+    return GF_OK;
+}
+
+int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace) {
+    GF_TRY(adj_check(a));
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    if (nsteps < 1 || !mx_trace) { eng->err = "gf_adjoint_forward: need nsteps >= 1 and a trace buffer of nsteps+1"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    cudaStream_t st = eng->stream;
+    // external field of every stage from the engine's clock, which is restored
+    const double t0 = eng->t_host;
+    const long pH = eng->presc_H, pE = eng->presc_E;
+    double hc[3], ec[3];
+    std::memcpy(hc, eng->Hext_cur, sizeof(hc)); std::memcpy(ec, eng->Eext_cur, sizeof(ec));
+    a->hext.assign((size_t)nsteps * 12, 0.);
+    for (uint64_t k = 0; k < nsteps; k++) {
+        StepDrive sd;
+        step_drive(eng, sd);
+        for (int s = 0; s < 4; s++)
+            for (int c = 0; c < 3; c++) a->hext[(size_t)(k * 4 + s) * 3 + c] = sd.st[s].Hext[c];
+    }
+    eng->t_host = t0; eng->presc_H = pH; eng->presc_E = pE;
+    std::memcpy(eng->Hext_cur, hc, sizeof(hc)); std::memcpy(eng->Eext_cur, ec, sizeof(ec));
+    a->nsteps = nsteps;
+    // checkpoints and traces sized for this run
+    const size_t slots = (size_t)(nsteps / (uint64_t)a->ck_every) + 1;
+    const long n = P.n;
+    if (slots != a->ck_slots) {
+        for (double** p : {&a->ck, &a->trace, &a->dldm})
+            if (*p) { cudaFree(*p); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)*p), a->allocs.end()); *p = nullptr; }
+        a->ck_slots = 0;
+    }
+    if (!a->ck) {
+        GF_TRY(adj_alloc(a, &a->ck, slots * 3 * (size_t)n));
+        a->ck_slots = slots;
+    }
+    if (a->trace) { cudaFree(a->trace); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->trace), a->allocs.end()); }
+    if (a->dldm) { cudaFree(a->dldm); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->dldm), a->allocs.end()); }
+    GF_TRY(adj_alloc(a, &a->trace, (size_t)nsteps + 1));
+    GF_TRY(adj_alloc(a, &a->dldm, (size_t)nsteps + 1));
+    // initial state: the engine's current m
+    double* const* m0 = cur(eng, eng->m);
+    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->X[c], m0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->ck + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    GF_TRY(adj_mean_x(a, a->X[0], 0));
+    for (uint64_t k = 0; k < nsteps; k++) {
+        GF_TRY(adj_step_forward(a, f3(a->X), k));
+        GF_TRY(adj_mean_x(a, a->X[0], (long)k + 1));
+        if ((k + 1) % (uint64_t)a->ck_every == 0) {
+            const size_t slot = (size_t)((k + 1) / (uint64_t)a->ck_every);
+            for (int c = 0; c < 3; c++)
+                GF_CU(cudaMemcpyAsync(a->ck + (slot * 3 + c) * (size_t)n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    GF_CU(cudaMemcpyAsync(mx_trace, a->trace, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, st));
+    GF_CU(cudaStreamSynchronize(st));
+    a->ran = true;
+    return GF_OK;
+}
+
+int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wave, double* grad_alpha) {
+    GF_TRY(adj_check(a));
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    if (!a->ran) { eng->err = "gf_adjoint_backward: run gf_adjoint_forward first"; return GF_EINVAL; }
+    if (!dloss_dmx || !grad_wave || !grad_alpha) { eng->err = "gf_adjoint_backward: null argument"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    cudaStream_t st = eng->stream;
+    const long n = P.n;
+    const unsigned bn = blocks_for(n, kThreads);
+    const uint64_t N = a->nsteps;
+    const double inv_nfm = 1. / (double)eng->deck.NFM;
+    GF_CU(cudaMemcpyAsync(a->dldm, dloss_dmx, sizeof(double) * (N + 1), cudaMemcpyHostToDevice, st));
+    for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->LAM[c], 0, sizeof(double) * n, st));
+    GF_CU(cudaMemsetAsync(a->abar, 0, sizeof(double) * n, st));
+    GF_CU(cudaMemsetAsync(a->wbar, 0, sizeof(double) * a->nw, st));
+    GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, f3(a->LAM),
+                 (const double*)a->dldm, (long)N, inv_nfm));
+    const uint64_t K = (uint64_t)a->ck_every;
+    const uint64_t nblocks = (N + K - 1) / K;
+    for (uint64_t b = nblocks; b-- > 0;) {
+        const uint64_t s0 = b * K, s1 = std::min(N, s0 + K);
+        // recompute the block's step values x_s0 .. x_{s1-1}
+        for (int c = 0; c < 3; c++) {
+            GF_CU(cudaMemcpyAsync(a->X[c], a->ck + (b * 3 + c) * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        for (uint64_t k = s0; k < s1; k++) {
+            for (int c = 0; c < 3; c++)
+                GF_CU(cudaMemcpyAsync(a->xs + ((k - s0) * 3 + c) * (size_t)n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            if (k + 1 < s1) GF_TRY(adj_step_forward(a, f3(a->X), k));
+        }
+        for (uint64_t k = s1; k-- > s0;) {
+            GF_TRY(adj_step_backward(a, f3v(a->xs + (k - s0) * 3 * (size_t)n, n), k));
+            GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
+                         f3(a->LAM), (const double*)a->dldm, (long)k, inv_nfm));
+        }
+    }
+    GF_CU(cudaMemcpyAsync(grad_wave, a->wbar, sizeof(double) * a->nw, cudaMemcpyDeviceToHost, st));
+    GF_CU(cudaMemcpyAsync(grad_alpha, a->abar, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    GF_CU(cudaStreamSynchronize(st));
+    return GF_OK;
+}
+
+int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count) {
+    GF_TRY(adj_check(a));
+    gf_engine* eng = a->eng;
+    const long n = eng->P.n;
+    if (!host_m || count != (size_t)(3 * n)) { eng->err = "gf_adjoint_final_m: need 3*nx*ny*nz values"; return GF_EINVAL; }
+    if (!a->ran) { eng->err = "gf_adjoint_final_m: run gf_adjoint_forward first"; return GF_EINVAL; }
+    // x of the last forward step: recompute from the last checkpoint
+    const uint64_t K = (uint64_t)a->ck_every, N = a->nsteps;
+    const uint64_t b = N / K;
+    cudaStream_t st = eng->stream;
+    for (int c = 0; c < 3; c++)
+        GF_CU(cudaMemcpyAsync(a->X[c], a->ck + (b * 3 + c) * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_step_forward(a, f3(a->X), k));
+    for (int c = 0; c < 3; c++)
+        GF_CU(cudaMemcpyAsync(host_m + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    GF_CU(cudaStreamSynchronize(st));
+    return GF_OK;
+}
+
+void gf_adjoint_destroy(gf_adjoint* a) {
+    if (!a) return;
+    if (a->eng && a->eng->stream) cudaStreamSynchronize(a->eng->stream);
+    for (void* p : a->allocs) cudaFree(p);
+    delete a;
+}
 
 }  // extern "C"
 

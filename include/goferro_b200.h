@@ -190,6 +190,39 @@ const char* gf_last_error(const gf_engine* e);
 /* Free the engine and all its device memory. */
 void gf_destroy(gf_engine* e);
 
+/* ---- Discrete adjoint of the ferromagnetic RK4 step ---------------------
+ * Gradients of a loss of the <m_x>(t) trace with respect to an x-directed
+ * excitation waveform (n_wave samples, piecewise constant over equal shares
+ * of the run, added to the deck's external field) and to a per-cell damping
+ * alpha (new inputs: the reference has per-material alpha only,
+ * magnetic_solver.cpp:206).  Differentiates the engine's discretisation of
+ * get_dm_RK{1..4} / update_m_RK* / update_m (magnetic_solver.cpp:3-229,
+ * 1515-1636) with per-stage FFT magnetostatics (magnetostatic_solver.cpp:
+ * 114-219): exchange, anisotropy (no frame rotation), Zeeman; decks with
+ * DMI, AFM, FE, elastic or Maxwell fields are GF_EUNSUPPORTED.  The reference
+ * has no adjoint; these entry points have no counterpart there.  FP64 engines
+ * only.  The adjoint uses the engine's stream and FFT buffers: do not advance
+ * the engine while an adjoint call runs. */
+typedef struct gf_adjoint gf_adjoint;
+/* checkpoint_every: steps between stored states (the backward run recomputes
+ * the steps in between; device memory ~ 24 * n * checkpoint_every bytes). */
+int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint** out);
+/* per-cell damping (nx*ny*nz values; default: the material's alpha) */
+int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count);
+/* waveform samples in A/m (n_wave values; default 0) */
+int gf_adjoint_set_waveform(gf_adjoint* a, const double* w, size_t count);
+/* Run nsteps RK4 steps from the engine's current m and external-field clock
+ * (the engine's own state is not advanced); mx_trace gets <m_x> at steps
+ * 0..nsteps (nsteps+1 values). Synchronous. */
+int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace);
+/* Given dloss/d<m_x> at steps 0..nsteps (nsteps+1 values), the gradients
+ * with respect to the waveform (n_wave values) and the per-cell alpha
+ * (nx*ny*nz values). Synchronous. */
+int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wave, double* grad_alpha);
+/* m after the last forward step (3*nx*ny*nz values, component-major). */
+int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count);
+void gf_adjoint_destroy(gf_adjoint* a);
+
 /* Mean of a device array, allocating nothing: *dev_out = sum(dev_in[0..n)) /
  * divisor, as a deterministic FP64 sum queued on `stream` (a cudaStream_t;
  * NULL = legacy default stream).  No counterpart in the reference.
