@@ -12,7 +12,9 @@ device time), whole job over all ranks: the headline `value` is the FP64
 form (the reference's arithmetic); with --precision both (the default) the
 line also carries `mixed`, the same measurement of the FP32 mixed form, its
 speed-up over FP64 and its trace error against the FP64 engine on the same
-initial state.
+initial state; at N=1 it also carries `adjoint`, the cost of the discrete
+adjoint (backward run) against the FP64 forward step on a 256x256x32
+ferromagnetic film (skip with --no-adjoint).
 
 `--impl ours` times the engine (CUDA events on the engine stream, max over
 ranks), measures the end-to-end rate through the C ABI with host buffers,
@@ -348,6 +350,65 @@ def roofline(r, args, mfe_frac, mixed):
             "share_of_step": total_ms / 2.0 / step_ms_prof}
 
 
+def adjoint_cost(gf, torch, args, local_rank):
+    """Cost of the discrete adjoint against a forward pass: FM LLG + FFT
+    magnetostatics on 256x256x32 (the adjoint configuration's grid, YIG-like
+    film, 1 T bias, per-cell damping 1e-3 with 10 % seeded noise, a 256-sample
+    x waveform), FP64.  Forward = the engine's graph-replayed step (CUDA
+    events); the adjoint's own forward run and its backward run (checkpoints
+    every 200 steps, block recomputation) are timed on the host around the
+    synchronous calls."""
+    mu0 = 1.256637061e-6
+    steps, K, nw = args.adjoint_steps, 200, 256
+    with tempfile.TemporaryDirectory() as tmp:
+        d = gf.decks.preset_fm_demag(nx=256, ny=256, nz=32, steps=steps)
+        d.Hext_table = None
+        d.Hext_stat = (0.0, 0.0, 1.0 / mu0)
+        d.materials[0].alpha = 1e-3
+        gf.decks.write_deck(d, tmp)
+        rng = np.random.default_rng(20241208)
+        alpha = 1e-3 * (1.0 + 0.1 * rng.random(d.n))
+        tt = (np.arange(nw) + 0.5) / nw
+        wave = (1e-3 / mu0) * np.sin(2 * np.pi * 8 * tt) * np.exp(-((tt - 0.3) / 0.1) ** 2)
+        with gf.Engine(tmp, device=local_rank) as eng:
+            stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
+            eng.advance(3)
+            eng.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.advance(steps)
+            e1.record(stream)
+            e1.synchronize()
+            t_eng = e0.elapsed_time(e1) / 1e3
+            with gf.Adjoint(eng, nw, K) as adj:
+                adj.set_alpha(alpha)
+                adj.set_waveform(wave)
+                adj.forward(4)
+                t0 = time.perf_counter()
+                tr = adj.forward(steps)
+                t_fwd = time.perf_counter() - t0
+                # d loss / d <m_x>: spectral power of the trace in 0.1-0.5 THz
+                X = np.fft.rfft(tr)
+                f = np.fft.rfftfreq(tr.size, d.dt)
+                band = np.nonzero((f >= 0.1e12) & (f <= 0.5e12))[0]
+                n = np.arange(tr.size)
+                g = np.zeros(tr.size)
+                for k in band:
+                    g += 2.0 * np.real(np.conj(X[k]) * np.exp(-2j * np.pi * k * n / tr.size))
+                t0 = time.perf_counter()
+                adj.backward(g)
+                t_bwd = time.perf_counter() - t0
+    return {"workload": "FM LLG + FFT magnetostatics, 256x256x32, FP64, per-cell alpha and 256-sample waveform",
+            "steps": steps, "checkpoint_every": K,
+            "forward_ms_per_step": 1e3 * t_eng / steps,
+            "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,
+            "backward_ms_per_step": 1e3 * t_bwd / steps,
+            "backward_over_forward": t_bwd / t_eng,
+            "loss_band_bins": int(len(band)),
+            "definition": "backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
+                          "forward = the engine's FP64 step (CUDA graph)"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import __graft_entry__
@@ -428,6 +489,8 @@ def run_ours(args, rank, world, local_rank):
             "device_bytes": int(rm["info"].device_bytes),
         }
         line["gpu_launches"] += line["mixed"]["gpu_launches"]
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_cost(gf, torch, args, local_rank)
     print(json.dumps(line))
 
 
@@ -442,6 +505,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--trace-steps", type=int, default=100)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=400)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
