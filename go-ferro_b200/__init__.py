@@ -39,7 +39,9 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
            "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients",
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
-           "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy"]
+           "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
+           "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
+           "gf_batch_last_error", "gf_batch_destroy"]
 
 
 class GFInfo(ctypes.Structure):
@@ -110,6 +112,16 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_adjoint_final_m.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
     lib.gf_adjoint_destroy.argtypes = [vp]
     lib.gf_adjoint_destroy.restype = None
+    lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
+    lib.gf_batch_advance.argtypes = [vp, c_u64]
+    lib.gf_batch_synchronize.argtypes = [vp]
+    lib.gf_batch_stream.argtypes = [vp]
+    lib.gf_batch_stream.restype = vp
+    lib.gf_batch_tuned_chunk.argtypes = [vp, c_int]
+    lib.gf_batch_last_error.argtypes = [vp]
+    lib.gf_batch_last_error.restype = ctypes.c_char_p
+    lib.gf_batch_destroy.argtypes = [vp]
+    lib.gf_batch_destroy.restype = None
     if path is None:
         _lib = lib
     return lib
@@ -265,6 +277,56 @@ class Adjoint:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.gf_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Batch:
+    """Several engines advanced together by one CUDA graph per step
+    (gf_batch_*); with autotune the elastic tile's x-chunk is picked per
+    engine by timing.  The engines remain owned by the caller and must not be
+    advanced directly while the batch exists."""
+
+    def __init__(self, engines, autotune: bool = True):
+        self.engines = list(engines)
+        self.lib = self.engines[0].lib
+        arr = (ctypes.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
+        h = ctypes.c_void_p()
+        rc = self.lib.gf_batch_create(arr, len(self.engines), int(bool(autotune)), ctypes.byref(h))
+        if rc != GF_OK:
+            raise GFError(rc, self.lib.gf_batch_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != GF_OK:
+            raise GFError(rc, self.lib.gf_batch_last_error(self.h).decode())
+
+    def advance(self, nsteps: int) -> None:
+        self._check(self.lib.gf_batch_advance(self.h, int(nsteps)))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.gf_batch_synchronize(self.h))
+
+    def stream(self) -> int:
+        return self.lib.gf_batch_stream(self.h) or 0
+
+    def tuned_chunk(self, index: int) -> int:
+        return int(self.lib.gf_batch_tuned_chunk(self.h, int(index)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gf_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -137,6 +137,7 @@ struct gf_engine {
 // functions are its interface.
 int gf_mixed_enqueue_step(gf_engine* eng, int parity);                 // kernels of one step, mixed form
 int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-memory opt-in, occupancy
+int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms);          // stage-1 elastic tile, mean ms per launch
 
 namespace {
 
@@ -876,6 +877,38 @@ int enqueue_stage(gf_engine* eng, int parity) {
     return GF_OK;
 }
 
+// Mean device time of `reps` launches of the stage-1 elastic tile kernel at
+// the engine's current x-chunk.  The kernel writes only per-stage scratch (the
+// stress divergence and the cell strain), so timing it leaves the state alone.
+template <class R>
+int time_tile_t(gf_engine* eng, int reps, float* ms) {
+    const Params& P = eng->P;
+    const StageIOT<R>& io = stage_io<R>(eng, (int)(eng->steps_done & 1ull), 0);
+    const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
+                    (P.nx + eng->el_chunk - 1) / eng->el_chunk);
+    cudaEvent_t a, b;
+    GF_CU(cudaEventCreate(&a));
+    GF_CU(cudaEventCreate(&b));
+    auto one = [&]() {
+        return eng->el_cubic ? launch_tiled(k_elastic_tile<0, true, R>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                                            eng->el_chunk, eng->el_nmat)
+                             : launch_tiled(k_elastic_tile<0, false, R>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                                            eng->el_chunk, eng->el_nmat);
+    };
+    cudaError_t e = one();                     // warm
+    if (e == cudaSuccess) e = cudaEventRecord(a, eng->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = one();
+    if (e == cudaSuccess) e = cudaEventRecord(b, eng->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    GF_CU(e);
+    *ms = t / (float)(reps > 0 ? reps : 1);
+    return GF_OK;
+}
+
 template <class R>
 int enqueue_step_t(gf_engine* eng, int parity) {
     GF_TRY((enqueue_stage<0, R>(eng, parity)));
@@ -895,6 +928,8 @@ int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm) {
     GF_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_elastic_tile<1, false, float>, etile::NT, (size_t)smem));
     return GF_OK;
 }
+
+int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms) { return time_tile_t<float>(eng, reps, ms); }
 #else
 namespace {
 
@@ -1699,6 +1734,197 @@ const char* gf_version(void) { return "goferro_b200 0.2 (FP64 parity form, FP32 
 
 }  // extern "C"
 
+
+// ===========================================================================
+// Batched runs (gf_batch_*): many engines advanced by one CUDA graph per step
+//
+// Each engine's step is captured as one branch of a single graph (fork and
+// join events around the engines' own streams), so one graph launch advances
+// every instance and instances of uneven grids run concurrently on the GPU.
+// The autotuner picks, per engine, the x-chunk of the tiled elastic kernel
+// (planes per block) from timed launches of that kernel on the engine's
+// current state; the kernel writes only per-stage scratch, so tuning leaves
+// every state untouched, and chunking does not change results.
+// ===========================================================================
+struct gf_batch {
+    std::vector<gf_engine*> engs;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    std::string err;
+    std::vector<int> tuned_chunk;
+};
+
+namespace {
+
+#define GB_CU(call)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            b->err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+            return GF_ECUDA;                                                             \
+        }                                                                                \
+    } while (0)
+
+int batch_fail(gf_batch* b, gf_engine* e, int rc) {
+    b->err = std::string("engine: ") + (e ? e->err : std::string("?"));
+    return rc;
+}
+
+// time the tile kernel at candidate chunks, keep the fastest
+int autotune_tile(gf_batch* b, gf_engine* e) {
+    const int nx = e->P.nx;
+    const int base = e->el_chunk;
+    std::vector<int> cand = {base};
+    for (int L : {base / 2, base * 2, base * 4, (nx + 1) / 2, nx, 4, 8, 16})
+        if (L >= 1 && L <= nx && std::find(cand.begin(), cand.end(), L) == cand.end()) cand.push_back(L);
+    int best = base;
+    float best_ms = -1.f;
+    for (int L : cand) {
+        e->el_chunk = L;
+        float ms = 0.f;
+        int rc = e->mixed ? gf_mixed_time_tile(e, 5, &ms) : time_tile_t<double>(e, 5, &ms);
+        if (rc != GF_OK) { e->el_chunk = base; return batch_fail(b, e, rc); }
+        if (best_ms < 0.f || ms < best_ms) { best_ms = ms; best = L; }
+    }
+    e->el_chunk = best;
+    e->graphs_ready = false;          // the engine's own graphs hold the old grid
+    for (int p = 0; p < 2; p++) {
+        if (e->gexec[p]) { cudaGraphExecDestroy(e->gexec[p]); e->gexec[p] = nullptr; }
+        if (e->graph[p]) { cudaGraphDestroy(e->graph[p]); e->graph[p] = nullptr; }
+    }
+    b->tuned_chunk.push_back(best);
+    return GF_OK;
+}
+
+int batch_capture(gf_batch* b) {
+    for (int par = 0; par < 2; par++) {
+        GB_CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = GF_OK;
+        cudaError_t ce = cudaEventRecord(b->fork, b->stream);
+        for (size_t i = 0; i < b->engs.size() && rc == GF_OK && ce == cudaSuccess; i++) {
+            gf_engine* e = b->engs[i];
+            ce = cudaStreamWaitEvent(e->stream, b->fork, 0);
+            if (ce == cudaSuccess) {
+                rc = enqueue_step(e, par);
+                if (rc != GF_OK) b->err = std::string("engine: ") + e->err;
+            }
+            if (rc == GF_OK && ce == cudaSuccess) ce = cudaEventRecord(b->join[i], e->stream);
+            if (rc == GF_OK && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[i], 0);
+        }
+        cudaGraph_t g = nullptr;
+        cudaError_t ce2 = cudaStreamEndCapture(b->stream, &g);
+        if (rc != GF_OK || ce != cudaSuccess || ce2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (rc == GF_OK) b->err = std::string("batch capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ce2);
+            return rc != GF_OK ? rc : GF_ECUDA;
+        }
+        b->graph[par] = g;
+        GB_CU(cudaGraphInstantiate(&b->gexec[par], g, 0));
+    }
+    return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out) {
+    if (!engines || count < 1 || !out) { g_create_err = "gf_batch_create: need engines, count >= 1 and an output"; return GF_EINVAL; }
+    *out = nullptr;
+    gf_batch* b = new gf_batch();
+    b->device = engines[0]->device;
+    for (int i = 0; i < count; i++) {
+        gf_engine* e = engines[i];
+        if (!e) { g_create_err = "gf_batch_create: null engine"; delete b; return GF_EINVAL; }
+        if (e->device != b->device) { g_create_err = "gf_batch_create: engines on different devices"; delete b; return GF_EINVAL; }
+        if ((e->steps_done & 1ull) != (engines[0]->steps_done & 1ull)) {
+            g_create_err = "gf_batch_create: engines must be at steps of the same parity"; delete b; return GF_EINVAL;
+        }
+        for (int j = 0; j < i; j++)
+            if (engines[j] == e) { g_create_err = "gf_batch_create: an engine appears twice"; delete b; return GF_EINVAL; }
+        b->engs.push_back(e);
+    }
+    auto fail = [&](int rc) { g_create_err = b->err; gf_batch_destroy(b); return rc; };
+    if (cudaSetDevice(b->device) != cudaSuccess) { b->err = "cudaSetDevice"; return fail(GF_ECUDA); }
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "stream"; return fail(GF_ECUDA); }
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) { b->err = "event"; return fail(GF_ECUDA); }
+    b->join.assign(b->engs.size(), nullptr);
+    for (auto& ev : b->join)
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) { b->err = "event"; return fail(GF_ECUDA); }
+    for (gf_engine* e : b->engs)
+        if (cudaStreamSynchronize(e->stream) != cudaSuccess) { b->err = "engine stream"; return fail(GF_ECUDA); }
+    if (autotune)
+        for (gf_engine* e : b->engs)
+            if (e->P.elastic) {
+                int rc = autotune_tile(b, e);
+                if (rc != GF_OK) return fail(rc);
+            }
+    int rc = batch_capture(b);
+    if (rc != GF_OK) return fail(rc);
+    *out = b;
+    return GF_OK;
+}
+
+int gf_batch_advance(gf_batch* b, uint64_t nsteps) {
+    if (!b) return GF_EINVAL;
+    GB_CU(cudaSetDevice(b->device));
+    uint64_t done = 0;
+    while (done < nsteps) {
+        const uint64_t chunk = std::min<uint64_t>(nsteps - done, (uint64_t)kDriveCap / 2);
+        GB_CU(cudaStreamSynchronize(b->stream));
+        // every engine's drive rows for the chunk, uploaded on the batch stream
+        for (gf_engine* e : b->engs) {
+            for (uint64_t s = 0; s < chunk; s++) step_drive(e, e->drive_host[s]);
+            const uint64_t first = e->steps_done + done;
+            uint64_t s = 0;
+            while (s < chunk) {
+                const uint64_t slot = (first + s) & (uint64_t)(kDriveCap - 1);
+                const uint64_t run = std::min<uint64_t>(chunk - s, (uint64_t)kDriveCap - slot);
+                GB_CU(cudaMemcpyAsync(e->drive + slot, e->drive_host + s, sizeof(StepDrive) * run, cudaMemcpyHostToDevice, b->stream));
+                s += run;
+            }
+        }
+        const uint64_t first = b->engs[0]->steps_done + done;
+        for (uint64_t k = 0; k < chunk; k++) GB_CU(cudaGraphLaunch(b->gexec[(first + k) & 1ull], b->stream));
+        done += chunk;
+    }
+    for (gf_engine* e : b->engs) e->steps_done += nsteps;
+    return GF_OK;
+}
+
+int gf_batch_synchronize(gf_batch* b) {
+    if (!b) return GF_EINVAL;
+    GB_CU(cudaStreamSynchronize(b->stream));
+    return GF_OK;
+}
+
+void* gf_batch_stream(gf_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int gf_batch_tuned_chunk(const gf_batch* b, int index) {
+    if (!b || index < 0 || index >= (int)b->engs.size()) return -1;
+    return b->engs[(size_t)index]->el_chunk;
+}
+
+const char* gf_batch_last_error(const gf_batch* b) { return b ? b->err.c_str() : g_create_err.c_str(); }
+
+void gf_batch_destroy(gf_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (int p = 0; p < 2; p++) {
+        if (b->gexec[p]) cudaGraphExecDestroy(b->gexec[p]);
+        if (b->graph[p]) cudaGraphDestroy(b->graph[p]);
+    }
+    for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // extern "C"
 
 // ===========================================================================
 // Discrete adjoint of the ferromagnetic RK4 step (gf_adjoint_*)

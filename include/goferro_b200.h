@@ -190,6 +190,30 @@ const char* gf_last_error(const gf_engine* e);
 /* Free the engine and all its device memory. */
 void gf_destroy(gf_engine* e);
 
+/* ---- Batched runs --------------------------------------------------------
+ * Many engines (uneven grids, either precision) advanced together: each
+ * engine's RK4 step is one branch of a single CUDA graph per step parity, so
+ * one graph launch advances every instance and small instances run
+ * concurrently.  With autotune != 0 the batch first picks, per engine, the
+ * x-chunk of the tiled elastic kernel by timing it (the state is not
+ * touched; chunking does not change results).  The engines stay owned by
+ * the caller and must not be advanced by other calls while the batch lives;
+ * all must sit at steps of the same parity.  The reference runs one system
+ * per process; these entry points have no counterpart there. */
+typedef struct gf_batch gf_batch;
+int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out);
+/* Advance every engine by nsteps (asynchronous on the batch stream). */
+int gf_batch_advance(gf_batch* b, uint64_t nsteps);
+int gf_batch_synchronize(gf_batch* b);
+/* The batch's CUDA stream (a cudaStream_t). */
+void* gf_batch_stream(gf_batch* b);
+/* Elastic-tile x-chunk engine `index` runs with (-1: bad index). */
+int gf_batch_tuned_chunk(const gf_batch* b, int index);
+/* Message of the last failing batch call (or failed create when b is NULL). */
+const char* gf_batch_last_error(const gf_batch* b);
+/* Free the batch (not the engines). */
+void gf_batch_destroy(gf_batch* b);
+
 /* ---- Discrete adjoint of the ferromagnetic RK4 step ---------------------
  * Gradients of a loss of the <m_x>(t) trace with respect to an x-directed
  * excitation waveform (n_wave samples, piecewise constant over equal shares
