@@ -409,6 +409,109 @@ def adjoint_cost(gf, torch, args, local_rank):
                           "forward = the engine's FP64 step (CUDA graph)"}
 
 
+SWEEP_SIZES = [(32, 32, 32), (48, 48, 32), (64, 64, 32), (96, 96, 24)]
+
+
+def sweep_decks(gf, count, steps, seed=20241207):
+    """Instances of the batched sweep: ferroelectric TDGL + electrostriction +
+    elastodynamics + FDTD (PbTiO3-like, dx = 1 nm), grid drawn by seed from
+    SWEEP_SIZES, z-polarised sheet current J_f type 6 (Gaussian x sine) with
+    amplitude log-uniform over 10-500 kV/cm and carrier uniform over
+    0.5-3 THz.  The Courant-limited step (2.45e-18 s) makes a run of
+    `steps` steps last a few fs, so the Gaussian envelope is centred inside
+    the run (sigma = steps*dt/10) instead of a THz-scale width."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nx, ny, nz = SWEEP_SIZES[int(rng.integers(len(SWEEP_SIZES)))]
+        kvcm = 10.0 ** rng.uniform(1.0, np.log10(500.0))
+        f0 = rng.uniform(0.5e12, 3e12)
+        d = gf.decks.preset_ferroelectric(nx=nx, ny=ny, nz=nz, steps=steps)
+        d.name = f"sweep_{i:02d}_{nx}x{ny}x{nz}"
+        d.jf_type = 6
+        d.jf_freq = f0
+        d.jf_sigma = steps * d.dt / 10.0
+        d.jf_amp = d.jf_amp * kvcm / 100.0        # the preset radiates ~100 kV/cm
+        out.append((d, kvcm, f0))
+    return out
+
+
+def run_sweep(gf, torch, args, local_rank, count, steps, fp64_check):
+    """Batched mixed-form sweep: all instances advanced by one graph per step
+    (gf_batch, autotuned elastic tiles) against the same engines advanced one
+    after another with their own graphs; optional FP64 error per instance."""
+    import shutil
+    decks = sweep_decks(gf, count, steps)
+    tmp = tempfile.mkdtemp()
+    engines = []
+    try:
+        t_create = time.perf_counter()
+        dirs = []
+        for d, _, _ in decks:
+            p0, q0 = d.p0, d.q0
+            d.p0 = None
+            ddir = os.path.join(tmp, d.name)
+            gf.decks.write_deck(d, ddir)
+            d.p0, d.q0 = p0, q0
+            dirs.append(ddir)
+            e = gf.Engine(ddir, device=local_rank, precision="mixed")
+            e.upload("p", p0)
+            e.upload("q", q0)
+            engines.append(e)
+        t_create = time.perf_counter() - t_create
+        cells = sum(d.n for d, _, _ in decks)
+        # sequential: every engine with its own graph, one after another
+        for e in engines:
+            e.advance(2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for e in engines:
+            e.advance(steps)
+        for e in engines:
+            e.synchronize()
+        t_seq = time.perf_counter() - t0
+        with gf.Batch(engines, autotune=True) as b:
+            chunks = sorted({b.tuned_chunk(i) for i in range(len(engines))})
+            stream = torch.cuda.ExternalStream(b.stream(), device=local_rank)
+            b.advance(2)
+            b.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.advance(steps)
+            e1.record(stream)
+            e1.synchronize()
+            t_batch = e0.elapsed_time(e1) / 1e3
+        pz = [float(e.average("p")[2]) for e in engines]
+        result = {"instances": count, "cells": cells, "steps_timed": steps,
+                  "value": cells * steps / t_batch, "unit": "cell-steps/s", "ms_per_step": 1e3 * t_batch / steps,
+                  "sequential_ms_per_step": 1e3 * t_seq / steps, "speedup_vs_sequential": t_seq / t_batch,
+                  "tuned_elastic_chunks": chunks, "create_s": t_create,
+                  "grids": {f"{a}x{b_}x{c}": sum(1 for d, _, _ in decks if (d.nx, d.ny, d.nz) == (a, b_, c))
+                            for a, b_, c in SWEEP_SIZES}}
+        if fp64_check:
+            # the same instances from the same state in FP64, one trace point per step
+            n_check = 2 * steps + 4     # sequential warm-up + timed steps, batch warm-up + timed steps
+            errs, resp = [], []
+            for (d, kvcm, f0), ddir, pzm in zip(decks, dirs, pz):
+                with gf.Engine(ddir, device=local_rank, precision="fp64") as e64:
+                    e64.upload("p", d.p0)
+                    e64.upload("q", d.q0)
+                    e64.advance(n_check)
+                    p64 = e64.average("p")
+                scale = max(abs(float(x)) for x in p64)
+                errs.append(abs(pzm - float(p64[2])) / scale)
+                resp.append({"kV_per_cm": kvcm, "f0_THz": f0 / 1e12, "grid": f"{d.nx}x{d.ny}x{d.nz}",
+                             "pz_mixed": pzm, "pz_fp64": float(p64[2]), "rel_err": errs[-1]})
+            result["fp64_check_steps"] = n_check
+            result["max_rel_err_vs_fp64"] = max(errs)
+            result["instances_detail"] = resp
+        return result
+    finally:
+        for e in engines:
+            e.close()
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import __graft_entry__
@@ -420,6 +523,22 @@ def run_ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local_rank)
+    if args.workload == "sweep":
+        # the batched configuration on its own: one JSON line of the sweep
+        sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.steps, fp64_check=True)
+        if dist:
+            dist.destroy_process_group()
+        if rank == 0:
+            line = {"metric": "cell-steps/s FP32-mixed batched sweep", "value": sw.pop("value") * world,
+                    "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": 2,
+                    "ms_per_step": sw["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": "48 ferroelectric + FDTD instances, grids drawn from 32^3, 48x48x32, "
+                                           "64x64x32, 96x96x24; J_f type 6, 10-500 kV/cm, 0.5-3 THz",
+                               "parallelism": f"replicas{world}" if world > 1 else "single"},
+                    "sweep": sw}
+            print(json.dumps(line))
+        return
     spec = WORKLOADS[args.workload]
     forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     results = {}
@@ -491,6 +610,11 @@ def run_ours(args, rank, world, local_rank):
         line["gpu_launches"] += line["mixed"]["gpu_launches"]
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(gf, torch, args, local_rank)
+    if world == 1 and not args.no_batch:
+        sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.sweep_steps, fp64_check=False)
+        sw["workload"] = ("batched sweep: 48 ferroelectric + FDTD instances, grids drawn from 32^3, 48x48x32, "
+                          "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step")
+        line["batched"] = sw
     print(json.dumps(line))
 
 
@@ -500,12 +624,14 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="magnetoelastic")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep"], default="magnetoelastic")
     ap.add_argument("--ref-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--trace-steps", type=int, default=100)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--sweep-steps", type=int, default=100)
     ap.add_argument("--adjoint-steps", type=int, default=400)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
