@@ -41,7 +41,7 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
            "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
-           "gf_batch_last_error", "gf_batch_destroy"]
+           "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics"]
 
 
 class GFInfo(ctypes.Structure):
@@ -112,6 +112,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_adjoint_final_m.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
     lib.gf_adjoint_destroy.argtypes = [vp]
     lib.gf_adjoint_destroy.restype = None
+    lib.gf_set_electrostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
     lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
     lib.gf_batch_advance.argtypes = [vp, c_u64]
     lib.gf_batch_synchronize.argtypes = [vp]
@@ -212,6 +213,13 @@ class Engine:
         n = ctypes.c_int()
         self._check(self.lib.gf_profile_steps(self.h, int(nsteps), recs, 64, ctypes.byref(n)))
         return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(n.value)}
+
+    def set_electrostatics(self, enable: bool = True) -> int:
+        """Enable the electrostatic (depolarisation) solve; returns the
+        set-up iteration count."""
+        used = ctypes.c_int()
+        self._check(self.lib.gf_set_electrostatics(self.h, int(bool(enable)), ctypes.byref(used)))
+        return used.value
 
     def check_finite(self) -> None:
         self._check(self.lib.gf_check_finite(self.h))

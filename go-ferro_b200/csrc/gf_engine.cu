@@ -36,6 +36,7 @@
 #include "gf_demag.cuh"
 #include "gf_util.cuh"
 #include "gf_adjoint.cuh"
+#include "gf_elec.cuh"
 
 using namespace gf;
 
@@ -115,6 +116,17 @@ struct gf_engine {
     cufftDoubleComplex* Nk = nullptr;      // 9 x n21
     cufftHandle plan_r2c = 0, plan_c2r = 0;
     bool plans = false;
+
+    // electrostatic field of P (gf_set_electrostatics; gf_elec.cuh)
+    bool elec_on = false, elec_per_stage = false;
+    int elec_iters = 1;                    // iterations of each per-stage solve
+    double elec_erh = 1.;                  // homogeneous reference permittivity
+    double* elec_k[3] = {nullptr, nullptr, nullptr};   // kx (nx), ky (ny), kz (nz/2+1)
+    double* elec_q = nullptr;              // 3 x n real
+    cufftDoubleComplex* elec_qk = nullptr; // 3 x n21
+    double* elec_blockmax = nullptr;       // 2 x kElecBlocks
+    cufftHandle elec_r2c = 0, elec_c2r = 0;
+    bool elec_plans = false;
 
     StageIO io[2][4];
     StageIOT<float> iof[2][4];             // mixed form
@@ -827,6 +839,43 @@ int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
     return GF_OK;
 }
 
+constexpr int kElecBlocks = 592;
+
+// `iters` fixed-point iterations of the electrostatic solve with the stage
+// polarisation p, updating Hstat's electric counterpart Estat in place; with
+// tol > 0 (set-up only) stop early once max|E_new - E_old| <= tol max|E_new|
+int elec_solve(gf_engine* eng, F3 p, bool counted, int iters, double tol, int* used) {
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    auto L = [&](const char* name, auto k, dim3 g, dim3 b, auto... args) -> cudaError_t {
+        return counted ? klaunch(eng, name, k, g, b, 0, st, args...) : launch(k, g, b, 0, st, args...);
+    };
+    const double inv = 1. / (kE0 * eng->elec_erh * (double)P.n);
+    std::vector<double> bm(2 * kElecBlocks);
+    int it = 0;
+    for (; it < iters; it++) {
+        GF_CU(L("k_elec_source", k_elec_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                p, f3(eng->Estat), eng->elec_erh, eng->elec_q));
+        GF_FFT(cufftExecD2Z(eng->elec_r2c, eng->elec_q, eng->elec_qk));
+        GF_CU(L("k_elec_mul", k_elec_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), P, n21, (const double*)eng->elec_k[0],
+                (const double*)eng->elec_k[1], (const double*)eng->elec_k[2], inv, eng->elec_qk));
+        GF_FFT(cufftExecZ2D(eng->elec_c2r, eng->elec_qk, eng->elec_q));
+        GF_CU(L("k_elec_update", k_elec_update, dim3(kElecBlocks), dim3(256), P, (const double*)eng->elec_q, f3(eng->Estat),
+                tol > 0. ? eng->elec_blockmax : (double*)nullptr));
+        if (tol > 0.) {
+            GF_CU(cudaMemcpyAsync(bm.data(), eng->elec_blockmax, sizeof(double) * bm.size(), cudaMemcpyDeviceToHost, st));
+            GF_CU(cudaStreamSynchronize(st));
+            double md = 0., me = 0.;
+            for (int b = 0; b < kElecBlocks; b++) { md = std::max(md, bm[2 * b]); me = std::max(me, bm[2 * b + 1]); }
+            if (md <= tol * me) { it++; break; }
+        }
+    }
+    if (used) *used = it;
+    return GF_OK;
+}
+
 template <int S, class R>
 int enqueue_stage(gf_engine* eng, int parity) {
     const Params& P = eng->P;
@@ -873,6 +922,10 @@ int enqueue_stage(gf_engine* eng, int parity) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
         if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, true));
         else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true));
+    }
+    if constexpr (!is_mixed<R>::value) {
+        // electrostatic field of the new stage polarisation (main.cpp:299-302)
+        if (eng->elec_on && eng->elec_per_stage) GF_TRY(elec_solve(eng, io.p_out, true, eng->elec_iters, 0., nullptr));
     }
     return GF_OK;
 }
@@ -1611,6 +1664,77 @@ int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count) {
     return replicate_state(e);
 }
 
+int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    const Deck& d = eng->deck;
+    const Params& P = eng->P;
+    if (iterations_used) *iterations_used = 0;
+    if (!enable) {
+        eng->elec_on = false;
+    } else {
+        if (!d.any_fe) { eng->err = "electrostatics needs a ferroelectric material"; return GF_EINVAL; }
+        if (eng->mixed) { eng->err = "the electrostatic solver runs in the FP64 form"; return GF_EUNSUPPORTED; }
+        if (d.elec_1D) { eng->err = "if_elec_1Dmodel: the 1-D electrostatic model is not implemented"; return GF_EUNSUPPORTED; }
+        GF_CU(cudaSetDevice(eng->device));
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+        if (!eng->elec_q) {
+            // wave vectors of global.cpp:276-316
+            const double PI = kPi;
+            const long dims[3] = {P.nx, P.ny, P.nz};
+            const double h[3] = {P.dx, P.dy, P.dz};
+            for (int a = 0; a < 3; a++) {
+                const long len = (a < 2) ? dims[a] : dims[2] / 2 + 1;
+                std::vector<double> kv((size_t)len);
+                const double dk = 2. * PI / (static_cast<double>(dims[a]) * h[a]);
+                for (long i = 0; i < len; i++) {
+                    long t = i;
+                    if (t > dims[a] / 2) t = t - dims[a];
+                    kv[(size_t)i] = static_cast<double>(t) * dk;
+                }
+                GF_TRY(dalloc_n(eng, &eng->elec_k[a], (size_t)len));
+                GF_CU(cudaStreamSynchronize(eng->stream));
+                GF_CU(cudaMemcpy(eng->elec_k[a], kv.data(), sizeof(double) * len, cudaMemcpyHostToDevice));
+            }
+            GF_TRY(dalloc_n(eng, &eng->elec_q, (size_t)3 * P.n));
+            GF_TRY(dalloc_n(eng, &eng->elec_qk, (size_t)3 * n21));
+            GF_TRY(dalloc_n(eng, &eng->elec_blockmax, (size_t)2 * kElecBlocks));
+            int dimsi[3] = {P.nx, P.ny, P.nz};
+            GF_FFT(cufftPlanMany(&eng->elec_r2c, 3, dimsi, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3));
+            GF_FFT(cufftPlanMany(&eng->elec_c2r, 3, dimsi, nullptr, 1, (int)n21, nullptr, 1, (int)P.n, CUFFT_Z2D, 3));
+            eng->elec_plans = true;
+            GF_FFT(cufftSetStream(eng->elec_r2c, eng->stream));
+            GF_FFT(cufftSetStream(eng->elec_c2r, eng->stream));
+        }
+        // er_homo = max over materials of er, times scale_elec
+        // (ferroelectric_initialize.cpp:310-318)
+        double erh = d.mats[0].er;
+        for (const Material& m : d.mats) erh = std::max(erh, m.er);
+        eng->elec_erh = erh * (d.scale_elec > 0. ? d.scale_elec : 1.);
+        const int limit = d.elec_limit > 0 ? (int)d.elec_limit : 200;
+        const double tol = d.elec_tol > 0. ? d.elec_tol : 1e-12;
+        eng->elec_iters = limit;
+        eng->elec_on = true;
+        eng->elec_per_stage = !d.em_dynamic;
+        // set-up solve from the current polarisation unless Estat.in was given
+        // (main.cpp:122-131); it starts from the current E_stat
+        if (!d.in_Estat) {
+            int used = 0;
+            GF_TRY(elec_solve(eng, f3(cur(eng, eng->p)), false, limit, tol, &used));
+            if (iterations_used) *iterations_used = used;
+        }
+        GF_CU(cudaStreamSynchronize(eng->stream));
+    }
+    // the captured steps change
+    for (int p = 0; p < 2; p++) {
+        if (eng->gexec[p]) { cudaGraphExecDestroy(eng->gexec[p]); eng->gexec[p] = nullptr; }
+        if (eng->graph[p]) { cudaGraphDestroy(eng->graph[p]); eng->graph[p] = nullptr; }
+    }
+    eng->graphs_ready = false;
+    return GF_OK;
+}
+
 int gf_get_info(gf_engine* e, gf_info* info) {
     GF_TRY(check(e));
     if (!info) { e->err = "null info"; return GF_EINVAL; }
@@ -1708,6 +1832,7 @@ void gf_destroy(gf_engine* e) {
         if (e->graph[p]) cudaGraphDestroy(e->graph[p]);
     }
     if (e->plans) { cufftDestroy(e->plan_r2c); cufftDestroy(e->plan_c2r); }
+    if (e->elec_plans) { cufftDestroy(e->elec_r2c); cufftDestroy(e->elec_c2r); }
     for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
     for (void* p : e->allocs) cudaFree(p);
     if (e->drive_host) cudaFreeHost(e->drive_host);

@@ -203,6 +203,11 @@ class Deck:
     em_back_P: bool = False
     em_back_M: bool = False
     elastic: bool = False
+    # electrostatic solver settings (read.cpp:56): scale of the homogeneous
+    # reference permittivity, iteration limit, tolerance
+    scale_elec: float = 1.0
+    elec_limit: int = 0
+    elec_tol: float = 1e-8
     elasto_back: bool = False
     elasto_on: bool = False
     strain_pulse: bool = False
@@ -289,7 +294,7 @@ class Deck:
              f"{_b(self.em_fromP)} {_b(self.em_fromM)}",
              f"{_b(self.em_back_P)} {_b(self.em_back_M)}",
              "0 0 0.0",
-             "1.0 0 1e-8",
+             f"{_f(self.scale_elec)} {int(self.elec_limit)} {_f(self.elec_tol)}",
              f"{_b(self.elastic)} {_b(self.elasto_back)} {_b(self.elasto_on)}",
              f"{_b(self.strain_pulse)} {int(self.strain_type)} {int(self.strain_z)}",
              f"{self.strain_comp} {_f(self.sigma_gauss)} {_f(self.amp_gauss)} {int(self.strain_cycles)}",

@@ -169,6 +169,20 @@ int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count);
  * (main.cpp:209-211, 720-726). */
 int gf_profile_steps(gf_engine* e, uint64_t nsteps, gf_kernel_time* out, int max_records, int* n_records);
 
+/* Electrostatic (depolarisation) field of the polarisation, E_stat.
+ * Replaces ferroelectric_system::get_E_static (ferroelectric_system.h:103),
+ * which the reference declares and calls (main.cpp:122-131, 299-302) but does
+ * not define in its public sources; a build of those sources, like the
+ * oracle, keeps E_stat at zero (or at Estat.in), and so does the engine
+ * until this is enabled.  The solve restates the method the reference's data
+ * imply: spectral, periodic, with the homogeneous reference permittivity
+ * er_h = max(er) * scale_elec (ferroelectric_initialize.cpp:310-338) and a
+ * fixed-point iteration for the cells whose er differs from er_h, up to
+ * elec_solver_limit iterations or elec_solver_tol (read.cpp:56).  Enabling
+ * solves once now (unless Estat.in was read) and, without Maxwell fields,
+ * after every RK stage with elec_solver_limit iterations.  FP64 engines;
+ * *iterations_used (optional) gets the set-up iteration count. */
+int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used);
 /* Engine facts (grid, active physics, counters). */
 int gf_get_info(gf_engine* e, gf_info* info);
 
