@@ -41,7 +41,8 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
            "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
-           "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics"]
+           "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics",
+           "gf_save_state", "gf_load_state"]
 
 
 class GFInfo(ctypes.Structure):
@@ -113,6 +114,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_adjoint_destroy.argtypes = [vp]
     lib.gf_adjoint_destroy.restype = None
     lib.gf_set_electrostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
+    lib.gf_save_state.argtypes = [vp, ctypes.c_char_p]
+    lib.gf_load_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
     lib.gf_batch_advance.argtypes = [vp, c_u64]
     lib.gf_batch_synchronize.argtypes = [vp]
@@ -213,6 +216,13 @@ class Engine:
         n = ctypes.c_int()
         self._check(self.lib.gf_profile_steps(self.h, int(nsteps), recs, 64, ctypes.byref(n)))
         return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(n.value)}
+
+    def save_state(self, path: str) -> None:
+        self._check(self.lib.gf_save_state(self.h, os.fsencode(path)))
+
+    def load_state(self, path: str) -> None:
+        self._check(self.lib.gf_load_state(self.h, os.fsencode(path)))
+        self.info = self.get_info()
 
     def set_electrostatics(self, enable: bool = True) -> int:
         """Enable the electrostatic (depolarisation) solve; returns the

@@ -1664,6 +1664,50 @@ int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count) {
     return replicate_state(e);
 }
 
+// ---------------------------------------------------------------------------
+// Checkpoint / restart (gf_save_state, gf_load_state)
+// ---------------------------------------------------------------------------
+struct CkBlob { std::string name; void* dev; size_t bytes; };
+
+constexpr char kCkMagic[8] = {'G', 'F', 'B', '2', 'C', 'K', 'P', '1'};
+struct CkHeader {
+    char magic[8];
+    int32_t nx, ny, nz, precision;
+    uint64_t steps_done;
+    double t_host;
+    int64_t presc_H, presc_E;
+    double Hext_cur[3], Eext_cur[3];
+    uint32_t nblobs, reserved;
+};
+
+// every device array whose contents carry from one step to the next
+std::vector<CkBlob> ck_blobs(gf_engine* eng) {
+    std::vector<CkBlob> v;
+    struct NF { const char* name; Field3* f; };
+    NF fs[] = {{"m", &eng->m}, {"m_afm1", &eng->a1}, {"m_afm2", &eng->a2}, {"p", &eng->p}, {"q", &eng->q},
+               {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H},
+               {"jp0", &eng->jp[0]}, {"jp1", &eng->jp[1]}, {"jp2", &eng->jp[2]}};
+    for (const NF& nf : fs) {
+        if (!nf.f->on) continue;
+        double* const* c = cur(eng, *nf.f);
+        for (int a = 0; a < 3; a++) {
+            v.push_back({std::string(nf.name) + "." + std::to_string(a), c[a], eng->esz * (size_t)nf.f->len[a]});
+            if (eng->mixed && nf.f->C[a])
+                v.push_back({std::string(nf.name) + ".c" + std::to_string(a), nf.f->C[a], eng->esz * (size_t)nf.f->len[a]});
+        }
+    }
+    const size_t n = (size_t)eng->P.n;
+    for (int a = 0; a < 3; a++) {
+        if (eng->Hstat[a]) v.push_back({"Hstat." + std::to_string(a), eng->Hstat[a], eng->esz * n});
+        if (eng->Estat[a]) v.push_back({"Estat." + std::to_string(a), eng->Estat[a], eng->esz * n});
+        if (eng->force_store[a]) v.push_back({"force_store." + std::to_string(a), eng->force_store[a], eng->esz * n});
+    }
+    const size_t plane = (size_t)eng->P.nx * eng->P.ny;
+    if (eng->liao_hist) v.push_back({"liao_hist", eng->liao_hist, eng->esz * 4 * 12 * plane});
+    if (eng->liao_last) v.push_back({"liao_last", eng->liao_last, eng->esz * 3 * plane});
+    return v;
+}
+
 int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
     GF_TRY(check(e));
     gf_engine* eng = e;
@@ -1733,6 +1777,86 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
     }
     eng->graphs_ready = false;
     return GF_OK;
+}
+
+int gf_save_state(gf_engine* e, const char* path) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!path) { eng->err = "null path"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    std::vector<CkBlob> blobs = ck_blobs(eng);
+    CkHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kCkMagic, 8);
+    h.nx = eng->P.nx; h.ny = eng->P.ny; h.nz = eng->P.nz;
+    h.precision = eng->mixed ? GF_PRECISION_MIXED_FP32 : GF_PRECISION_FP64;
+    h.steps_done = eng->steps_done; h.t_host = eng->t_host;
+    h.presc_H = eng->presc_H; h.presc_E = eng->presc_E;
+    for (int a = 0; a < 3; a++) { h.Hext_cur[a] = eng->Hext_cur[a]; h.Eext_cur[a] = eng->Eext_cur[a]; }
+    h.nblobs = (uint32_t)blobs.size();
+    FILE* f = std::fopen(path, "wb");
+    if (!f) { eng->err = std::string("cannot write ") + path; return GF_EIO; }
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+    std::vector<char> buf;
+    for (const CkBlob& b : blobs) {
+        if (!ok) break;
+        char name[32];
+        std::memset(name, 0, sizeof(name));
+        std::strncpy(name, b.name.c_str(), sizeof(name) - 1);
+        const uint64_t bytes = b.bytes;
+        buf.resize(b.bytes);
+        if (cudaMemcpy(buf.data(), b.dev, b.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) { ok = false; break; }
+        ok = std::fwrite(name, sizeof(name), 1, f) == 1 && std::fwrite(&bytes, sizeof(bytes), 1, f) == 1 &&
+             std::fwrite(buf.data(), 1, b.bytes, f) == b.bytes;
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (!ok) { eng->err = std::string("writing ") + path + " failed"; return GF_EIO; }
+    return GF_OK;
+}
+
+int gf_load_state(gf_engine* e, const char* path) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!path) { eng->err = "null path"; return GF_EINVAL; }
+    FILE* f = std::fopen(path, "rb");
+    if (!f) { eng->err = std::string("cannot read ") + path; return GF_EIO; }
+    CkHeader h;
+    const unsigned long long steps_before = eng->steps_done;
+    // a failed load leaves the step count as it was (field contents already
+    // copied are not restored)
+    auto bad = [&](const std::string& why, int rc) { std::fclose(f); eng->err = why; eng->steps_done = steps_before; return rc; };
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kCkMagic, 8) != 0)
+        return bad(std::string(path) + " is not an engine checkpoint", GF_EIO);
+    if (h.nx != eng->P.nx || h.ny != eng->P.ny || h.nz != eng->P.nz)
+        return bad("checkpoint grid differs from the engine's", GF_EINVAL);
+    if (h.precision != (eng->mixed ? GF_PRECISION_MIXED_FP32 : GF_PRECISION_FP64))
+        return bad("checkpoint precision differs from the engine's", GF_EINVAL);
+    GF_CU(cudaSetDevice(eng->device));
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    // the current-step buffers depend on the step parity: take the file's first
+    eng->steps_done = h.steps_done;
+    std::vector<CkBlob> blobs = ck_blobs(eng);
+    if (h.nblobs != blobs.size()) return bad("checkpoint holds different fields than this engine", GF_EINVAL);
+    std::vector<char> buf;
+    for (const CkBlob& b : blobs) {
+        char name[32];
+        uint64_t bytes = 0;
+        if (std::fread(name, sizeof(name), 1, f) != 1 || std::fread(&bytes, sizeof(bytes), 1, f) != 1)
+            return bad("truncated checkpoint", GF_EIO);
+        name[31] = 0;
+        if (b.name != name || bytes != b.bytes) return bad(std::string("checkpoint field ") + name + " does not match", GF_EINVAL);
+        buf.resize(bytes);
+        if (std::fread(buf.data(), 1, bytes, f) != bytes) return bad("truncated checkpoint", GF_EIO);
+        if (cudaMemcpy(b.dev, buf.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bad("checkpoint upload failed", GF_ECUDA);
+    }
+    std::fclose(f);
+    eng->t_host = h.t_host; eng->presc_H = (long)h.presc_H; eng->presc_E = (long)h.presc_E;
+    for (int a = 0; a < 3; a++) { eng->Hext_cur[a] = h.Hext_cur[a]; eng->Eext_cur[a] = h.Eext_cur[a]; }
+    const unsigned long long ctr = h.steps_done;
+    GF_CU(cudaMemcpy(eng->step_ctr, &ctr, sizeof(ctr), cudaMemcpyHostToDevice));
+    return replicate_state(eng);
 }
 
 int gf_get_info(gf_engine* e, gf_info* info) {

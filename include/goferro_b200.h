@@ -183,6 +183,17 @@ int gf_profile_steps(gf_engine* e, uint64_t nsteps, gf_kernel_time* out, int max
  * after every RK stage with elec_solver_limit iterations.  FP64 engines;
  * *iterations_used (optional) gets the set-up iteration count. */
 int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used);
+/* Full-precision checkpoint of everything that carries from one step to the
+ * next: the state fields (and, in the mixed form, their compensation words),
+ * the static fields, the stage-1 force of the stiffness damping, the Liao
+ * boundary history, the step counter and the external-field clock.  A run
+ * restarted from it continues bit for bit.  The reference restarts from
+ * its %.7e text dumps (inoutput.cpp:330-887, input_* readers); this binary
+ * form has no counterpart there.  Load needs an engine created from the same
+ * deck and precision. Synchronous. */
+int gf_save_state(gf_engine* e, const char* path);
+int gf_load_state(gf_engine* e, const char* path);
+
 /* Engine facts (grid, active physics, counters). */
 int gf_get_info(gf_engine* e, gf_info* info);
 
