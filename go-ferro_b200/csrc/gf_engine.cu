@@ -799,9 +799,9 @@ int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
         const double vol_neg = -P.dx * P.dy * P.dz;
         GF_CU(L("k_demag_mul", k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, vol_neg,
                 (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+        // the inverse transform lands in H_stat itself (H_stat is a view of
+        // the FFT buffer in the FFT mode)
         GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
-        for (int a = 0; a < 3; a++)
-            GF_CU(cudaMemcpyAsync(eng->Hstat[a], eng->Mfft + (size_t)a * P.n, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
     } else {
         GF_CU(L("k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
                 m, a1, a2, eng->demag_mode, (double*)nullptr, f3(eng->Hstat), eng->deck.demag_fac[0], eng->deck.demag_fac[1],
@@ -828,9 +828,7 @@ int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
         const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
         GF_CU(L("k_demag_mul", k_demag_mul_f32, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, inv_vol_neg,
                 (const cuComplex*)Mk, (const cuComplex*)eng->Nk, (cuComplex*)Mk));
-        GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));
-        for (int a = 0; a < 3; a++)
-            GF_CU(cudaMemcpyAsync(eng->Hstat[a], M3 + (size_t)a * P.n, sizeof(float) * P.n, cudaMemcpyDeviceToDevice, st));
+        GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));     // into H_stat (a view of M3)
     } else {
         GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
                 (const uint8_t*)eng->mid, m, eng->demag_mode, (float*)nullptr, f3f(eng->Hstat), (float)eng->deck.demag_fac[0],
@@ -1044,11 +1042,16 @@ int setup_demag(gf_engine* eng) {
         eng->plans = true;
         GF_FFT(cufftSetStream(eng->plan_r2c, eng->stream));
         GF_FFT(cufftSetStream(eng->plan_c2r, eng->stream));
+        for (int a = 0; a < 3; a++) eng->Hstat[a] = reinterpret_cast<double*>(reinterpret_cast<float*>(eng->Mfft) + (size_t)a * P.n);
         return GF_OK;
     }
     GF_TRY(dalloc_n(eng, &eng->Mfft, (size_t)3 * P.n));
     GF_TRY(dalloc_n(eng, &eng->Mk, (size_t)3 * n21));
     GF_TRY(dalloc_n(eng, &eng->Nk, (size_t)9 * n21));
+    // H_stat is a view of the FFT buffer: the inverse transform writes it,
+    // and the next stage's source overwrites it only after the LLG kernels
+    // of that stage have read it
+    for (int a = 0; a < 3; a++) eng->Hstat[a] = eng->Mfft + (size_t)a * P.n;
     GF_FFT(cufftPlanMany(&eng->plan_r2c, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3));
     GF_FFT(cufftPlanMany(&eng->plan_c2r, 3, dims, nullptr, 1, (int)n21, nullptr, 1, (int)P.n, CUFFT_Z2D, 3));
     eng->plans = true;
@@ -1318,7 +1321,9 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
             GF_TRY(dalloc_r(eng, &eng->force_store[a], (size_t)n));
             GF_TRY(dalloc_r(eng, &eng->force[a], (size_t)n));
         }
-        if (d.any_fm || d.any_afm) GF_TRY(dalloc_r(eng, &eng->Hstat[a], (size_t)n));
+        // with the FFT magnetostatics H_stat is a view of the FFT buffer (setup_demag)
+        if ((d.any_fm || d.any_afm) && !(d.magnetostatics && !d.mag_1D && !d.demag_factor))
+            GF_TRY(dalloc_r(eng, &eng->Hstat[a], (size_t)n));
         if (d.any_fe) GF_TRY(dalloc_r(eng, &eng->Estat[a], (size_t)n));
         if (d.any_fm && d.read_Hext_nonunif) GF_TRY(dalloc_r(eng, &eng->Hnu[a], (size_t)n));
     }
@@ -1340,9 +1345,9 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     GF_TRY(dalloc_n(eng, &eng->flag, 1));
     GF_CU(cudaStreamSynchronize(eng->stream));
 
+    GF_TRY(setup_demag(eng));          // before the restart inputs: Hstat.in lands in the FFT buffer
     GF_TRY(initial_state(eng, dir));
     GF_TRY(replicate_state(eng));
-    GF_TRY(setup_demag(eng));
     build_io(eng);
     if (eng->mixed) build_io_mixed(eng);
 
@@ -2518,6 +2523,8 @@ int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace) {
         }
     }
     GF_CU(cudaMemcpyAsync(mx_trace, a->trace, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, st));
+    // the engine's H_stat shares the FFT buffer the adjoint used
+    GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(st));
     a->ran = true;
     return GF_OK;
@@ -2562,6 +2569,7 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     }
     GF_CU(cudaMemcpyAsync(grad_wave, a->wbar, sizeof(double) * a->nw, cudaMemcpyDeviceToHost, st));
     GF_CU(cudaMemcpyAsync(grad_alpha, a->abar, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(st));
     return GF_OK;
 }
@@ -2581,6 +2589,7 @@ int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count) {
     for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_step_forward(a, f3(a->X), k));
     for (int c = 0; c < 3; c++)
         GF_CU(cudaMemcpyAsync(host_m + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(st));
     return GF_OK;
 }
