@@ -215,9 +215,10 @@ static __global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float in
     Hk[2 * n21 + q] = make_cuComplex(hz.x * inv_vol_neg, hz.y * inv_vol_neg);
 }
 
-// k_mag_source for the mixed form (ferromagnets; the mixed form has no AFM)
-static __global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, const uint8_t* mid, F3T<float> m, int mode,
-                                 float* M3, F3T<float> Hs, float f0, float f1, float f2) {
+// k_mag_source for the mixed form
+static __global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, const uint8_t* mid, F3T<float> m,
+                                        F3T<float> a1, F3T<float> a2, int mode, float* M3, F3T<float> Hs, float f0,
+                                        float f1, float f2) {
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
@@ -230,6 +231,16 @@ static __global__ void k_mag_source_f32(Params P, const DevMatT<float>* mats, co
             Hs.c[0][c] = Ms * m.c[0][c] * f0; Hs.c[1][c] = Ms * m.c[1][c] * f1; Hs.c[2][c] = Ms * m.c[2][c] * f2;
         } else {
             Hs.c[0][c] = 0.f; Hs.c[1][c] = 0.f; Hs.c[2][c] = -Ms * m.c[2][c];
+        }
+    } else if (fl & MF_AFM) {
+        const float Ms1 = mats[id - 1].Ms1, Ms2 = mats[id - 1].Ms2;
+        if (mode == 0) {
+            for (int a = 0; a < 3; a++) M3[a * P.n + c] = Ms1 * a1.c[a][c] + Ms2 * a2.c[a][c];
+        } else if (mode == 1) {
+            const float f[3] = {f0, f1, f2};
+            for (int a = 0; a < 3; a++) Hs.c[a][c] = (Ms1 * a1.c[a][c] + Ms2 * a2.c[a][c]) * f[a];
+        } else {
+            Hs.c[0][c] = 0.f; Hs.c[1][c] = 0.f; Hs.c[2][c] = -Ms1 * a1.c[2][c] - Ms2 * a2.c[2][c];
         }
     } else if (mode == 0) {
         M3[c] = 0.f; M3[P.n + c] = 0.f; M3[2 * P.n + c] = 0.f;

@@ -259,45 +259,55 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) 
 // EMdynamic_solver.cpp:4318-4452) with E_cell the 4-edge mean of the stage E
 // (update_DE_cell, :3813-3826), and the RK4 combination of update_Jp_RK*/
 // update_Jp (:4454-4524).
-template <int S>
-__global__ void __launch_bounds__(256) k_drude(Params P, StageIO io) {
+template <int S, class R = double>
+__global__ void __launch_bounds__(256) k_drude(Params P, StageIOT<R> io) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = io.mid[c];
     const int nyz = P.ny * P.nz;
     const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
     const int ny = P.ny, nz = P.nz;
-    double dJ[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+    R dJ[3][3] = {{R(0.), R(0.), R(0.)}, {R(0.), R(0.), R(0.)}, {R(0.), R(0.), R(0.)}};
+    R dt_r;
+    if constexpr (is_mixed<R>::value) dt_r = P.f.dt; else dt_r = P.dt;
     if (id != 0) {
-        const DevMat& mt = io.mats[id - 1];
+        const DevMatT<R>& mt = io.mats[id - 1];
         const int ex = (i * (ny + 1) + j) * (nz + 1) + k;
         const int ey = (i * ny + j) * (nz + 1) + k;
         const int ez = (i * (ny + 1) + j) * nz + k;
-        const double* Ex = io.E_in.c[0];
-        const double* Ey = io.E_in.c[1];
-        const double* Ez = io.E_in.c[2];
-        const double Ec[3] = {(Ex[ex] + Ex[ex + nz + 1] + Ex[ex + 1] + Ex[ex + nz + 1 + 1]) / 4.,
-                              (Ey[ey] + Ey[ey + ny * (nz + 1)] + Ey[ey + 1] + Ey[ey + ny * (nz + 1) + 1]) / 4.,
-                              (Ez[ez] + Ez[ez + (ny + 1) * nz] + Ez[ez + nz] + Ez[ez + (ny + 1) * nz + nz]) / 4.};
+        const R* Ex = io.E_in.c[0];
+        const R* Ey = io.E_in.c[1];
+        const R* Ez = io.E_in.c[2];
+        const R Ec[3] = {(Ex[ex] + Ex[ex + nz + 1] + Ex[ex + 1] + Ex[ex + nz + 1 + 1]) / R(4.),
+                              (Ey[ey] + Ey[ey + ny * (nz + 1)] + Ey[ey + 1] + Ey[ey + ny * (nz + 1) + 1]) / R(4.),
+                              (Ez[ez] + Ez[ez + (ny + 1) * nz] + Ez[ez + nz] + Ez[ez + (ny + 1) * nz + nz]) / R(4.)};
 #pragma unroll
         for (int pole = 0; pole < 3; pole++)
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                dJ[pole][a] = (kE0 * mt.wp[pole] * mt.wp[pole] * Ec[a] * mt.comp[pole] - mt.rtau[pole] * io.jp_in[pole].c[a][c]) * P.dt;
+                dJ[pole][a] = (R(kE0) * mt.wp[pole] * mt.wp[pole] * Ec[a] * mt.comp[pole] - mt.rtau[pole] * io.jp_in[pole].c[a][c]) * dt_r;
     }
+    if constexpr (is_mixed<R>::value) {
 #pragma unroll
-    for (int pole = 0; pole < 3; pole++)
+        for (int pole = 0; pole < 3; pole++)
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const double d = dJ[pole][a];
-            double* out = io.jp_out[pole].c[a];
-            double* acc = io.jp_acc[pole].c[a];
-            const double xv = io.jp_x[pole].c[a][c];
-            if (S == 0) { out[c] = xv + d * 0.5; acc[c] = xv + qdiv(d, 6., kInv6); }
-            else if (S == 1) { out[c] = xv + d * 0.5; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
-            else if (S == 2) { out[c] = xv + d; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
-            else { acc[c] = acc[c] + qdiv(d, 6., kInv6); }
-        }
+            for (int a = 0; a < 3; a++)
+                rk_mixed<S>(io.jp_x[pole].c[a][c], dJ[pole][a], io.jp_out[pole].c[a], io.jp_acc[pole].c[a], io.jp_cmp[pole].c[a], c);
+    } else {
+#pragma unroll
+        for (int pole = 0; pole < 3; pole++)
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const double d = dJ[pole][a];
+                double* out = io.jp_out[pole].c[a];
+                double* acc = io.jp_acc[pole].c[a];
+                const double xv = io.jp_x[pole].c[a][c];
+                if (S == 0) { out[c] = xv + d * 0.5; acc[c] = xv + qdiv(d, 6., kInv6); }
+                else if (S == 1) { out[c] = xv + d * 0.5; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
+                else if (S == 2) { out[c] = xv + d; acc[c] = acc[c] + qdiv(d, 3., kInv3); }
+                else { acc[c] = acc[c] + qdiv(d, 6., kInv6); }
+            }
+    }
 }
 
 // Perfect electric conductor: E = 0 on every edge with a PEC cell among its
@@ -305,12 +315,13 @@ __global__ void __launch_bounds__(256) k_drude(Params P, StageIO io) {
 // EMdynamic_initialize.cpp:160-330), after the Mur update (update_DE_PEC,
 // EMdynamic_solver.cpp:4526-4556).  The reference zeroes both the step value
 // and the stage value, so stages 1-3 also clear the step-start buffer.
-__device__ inline bool pec_cell(const StageIO& io, int c) {
+template <class R>
+__device__ inline bool pec_cell(const StageIOT<R>& io, int c) {
     const uint8_t id = io.mid[c];
     return id != 0 && (io.mats[id - 1].flags & MF_PEC);
 }
-template <int S>
-__global__ void __launch_bounds__(256) k_em_pec(Params P, StageIO io) {
+template <int S, class R = double>
+__global__ void __launch_bounds__(256) k_em_pec(Params P, StageIOT<R> io) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (ny + 1) * (nz + 1)) return;
@@ -346,8 +357,9 @@ __global__ void __launch_bounds__(256) k_em_pec(Params P, StageIO io) {
         if (!pec) continue;
         const int e = C == 0 ? (i * (ny + 1) + j) * (nz + 1) + k
                              : (C == 1 ? (i * ny + j) * (nz + 1) + k : (i * (ny + 1) + j) * nz + k);
-        if (S < 3) { io.E_out.c[C][e] = 0.; io.E_x.c[C][e] = 0.; }
-        else io.E_acc.c[C][e] = 0.;
+        if (S < 3) { io.E_out.c[C][e] = R(0.); io.E_x.c[C][e] = R(0.); }
+        else io.E_acc.c[C][e] = R(0.);
+        if constexpr (is_mixed<R>::value) io.E_cmp.c[C][e] = R(0.);
     }
 }
 

@@ -375,13 +375,9 @@ std::string unsupported(const Deck& d) {
     return "";
 }
 
-// physics the mixed form does not cover
-std::string unsupported_mixed(const Deck& d, const Params& P) {
-    if (d.any_afm) return "the mixed-precision form does not cover antiferromagnets; use GF_PRECISION_FP64";
-    if (P.drude) return "the mixed-precision form does not cover Drude dispersion; use GF_PRECISION_FP64";
-    if (P.pec) return "the mixed-precision form does not cover perfect conductors; use GF_PRECISION_FP64";
-    return "";
-}
+// physics the mixed form does not cover (none at present: every stage
+// kernel has an FP32 instantiation)
+std::string unsupported_mixed(const Deck&, const Params&) { return ""; }
 
 void build_params(gf_engine* eng) {
     const Deck& d = eng->deck;
@@ -695,6 +691,12 @@ void build_io_mixed(gf_engine* eng) {
             StageIOT<float>& io = eng->iof[par][s];
             std::memset(&io, 0, sizeof(io));
             if (eng->m.on) set_io_field_f(eng->m, par, s, io.m_in, io.m_x, io.m_acc, io.m_out, io.m_cmp);
+            if (eng->a1.on) set_io_field_f(eng->a1, par, s, io.a1_in, io.a1_x, io.a1_acc, io.a1_out, io.a1_cmp);
+            if (eng->a2.on) set_io_field_f(eng->a2, par, s, io.a2_in, io.a2_x, io.a2_acc, io.a2_out, io.a2_cmp);
+            for (int pole = 0; pole < 3; pole++)
+                if (eng->jp[pole].on)
+                    set_io_field_f(eng->jp[pole], par, s, io.jp_in[pole], io.jp_x[pole], io.jp_acc[pole], io.jp_out[pole],
+                                   io.jp_cmp[pole]);
             if (eng->p.on) set_io_field_f(eng->p, par, s, io.p_in, io.p_x, io.p_acc, io.p_out, io.p_cmp);
             if (eng->q.on) set_io_field_f(eng->q, par, s, io.q_in, io.q_x, io.q_acc, io.q_out, io.q_cmp);
             if (eng->u.on) set_io_field_f(eng->u, par, s, io.u_in, io.u_x, io.u_acc, io.u_out, io.u_cmp);
@@ -702,6 +704,8 @@ void build_io_mixed(gf_engine* eng) {
             if (eng->E.on) set_io_field_f(eng->E, par, s, io.E_in, io.E_x, io.E_acc, io.E_out, io.E_cmp);
             if (eng->H.on) set_io_field_f(eng->H, par, s, io.H_in, io.H_x, io.H_acc, io.H_out, io.H_cmp);
             io.dm = f3f(eng->dm);
+            io.da1 = f3f(eng->da1);
+            io.da2 = f3f(eng->da2);
             io.force_store = f3f(eng->force_store);
             io.force = f3f(eng->force);
             io.Hstat = f3f(eng->Hstat);
@@ -811,7 +815,7 @@ int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
 }
 
 // the same in the mixed form: FP32 source, R2C, spectra product, C2R
-int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
+int demag_solve_f32(gf_engine* eng, F3T<float> m, F3T<float> a1, F3T<float> a2, bool counted) {
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
@@ -822,7 +826,7 @@ int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
     cufftComplex* Mk = reinterpret_cast<cufftComplex*>(eng->Mk);
     if (eng->demag_mode == 0) {
         GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
-                (const uint8_t*)eng->mid, m, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
+                (const uint8_t*)eng->mid, m, a1, a2, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
         GF_FFT(cufftExecR2C(eng->plan_r2c, M3, Mk));
         const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
         const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
@@ -831,7 +835,7 @@ int demag_solve_f32(gf_engine* eng, F3T<float> m, bool counted) {
         GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));     // into H_stat (a view of M3)
     } else {
         GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
-                (const uint8_t*)eng->mid, m, eng->demag_mode, (float*)nullptr, f3f(eng->Hstat), (float)eng->deck.demag_fac[0],
+                (const uint8_t*)eng->mid, m, a1, a2, eng->demag_mode, (float*)nullptr, f3f(eng->Hstat), (float)eng->deck.demag_fac[0],
                 (float)eng->deck.demag_fac[1], (float)eng->deck.demag_fac[2]));
     }
     return GF_OK;
@@ -896,10 +900,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
     }
     if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S, R>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
                                   dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
-    if constexpr (!is_mixed<R>::value) {
-        if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
-                                       dim3(kThreads), 0, st, P, io, (const LLGTables*)eng->llg_tab, (int)eng->deck.mats.size()));
-    }
+    if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S, R>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
+                                   dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
     if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S, R>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
                             dim3(kThreads), 0, st, P, io));
     if (P.em) {
@@ -910,15 +912,13 @@ int enqueue_stage(gf_engine* eng, int parity) {
         if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0, R>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1, R>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2, R>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
-        if constexpr (!is_mixed<R>::value) {
-            if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
-                                     dim3(kThreads), 0, st, P, io));
-            if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S>, dim3(bn), dim3(kThreads), 0, st, P, io));
-        }
+        if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                                 dim3(kThreads), 0, st, P, io));
+        if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S, R>, dim3(bn), dim3(kThreads), 0, st, P, io));
     }
     if (eng->demag_per_stage) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
-        if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, true));
+        if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, io.a1_out, io.a2_out, true));
         else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true));
     }
     if constexpr (!is_mixed<R>::value) {
@@ -996,7 +996,7 @@ int enqueue_step(gf_engine* eng, int parity) {
 // static field from the current m (initial solve, main.cpp:135-146)
 int static_field_now(gf_engine* eng) {
     if (eng->demag_mode < 0) return GF_OK;
-    if (eng->mixed) return demag_solve_f32(eng, f3f(eng->m.X), false);
+    if (eng->mixed) return demag_solve_f32(eng, f3f(eng->m.X), f3f(eng->a1.X), f3f(eng->a2.X), false);
     return demag_solve(eng, f3(eng->m.X), f3(eng->a1.X), f3(eng->a2.X), false);
 }
 
@@ -1151,8 +1151,8 @@ int initial_state(gf_engine* eng, const std::string& dir) {
                 }
             }
         }
-        GF_TRY(upload_vec(eng, eng->a1.X, b6, n));
-        GF_TRY(upload_vec(eng, eng->a2.X, b6 + 3, n));
+        GF_TRY(upload_vec(eng, eng->a1.X, b6, n, eng->a1.C));
+        GF_TRY(upload_vec(eng, eng->a2.X, b6 + 3, n, eng->a2.C));
     }
     if (eng->p.on) {
         for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);

@@ -269,20 +269,21 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
 // surface masks of magnetic_initialize.cpp:632-1071 are derived from the
 // material ids.
 // ---------------------------------------------------------------------------
+template <class R>
 struct AFMMat {
-    double Aex[2], K1c[2], B1c[2], B2c[2], J[2], ex[2], prec[2], aprec[2];
-    double u[3];
+    R Aex[2], K1c[2], B1c[2], B2c[2], J[2], ex[2], prec[2], aprec[2];
+    R u[3];
     uint32_t afm;
     int pad_;
 };
 
-template <int S>
-__global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIO io, const LLGTables* __restrict__ tab, int nmat) {
-    __shared__ AFMMat mt[kMaxMat];
-    __shared__ double sA[2][kMaxMat + 1][kMaxMat + 1];
+template <int S, class R = double>
+__global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, const LLGTablesT<R>* __restrict__ tab, int nmat) {
+    __shared__ AFMMat<R> mt[kMaxMat];
+    __shared__ R sA[2][kMaxMat + 1][kMaxMat + 1];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
-        const DevMat& d = io.mats[q];
-        AFMMat& m = mt[q];
+        const DevMatT<R>& d = io.mats[q];
+        AFMMat<R>& m = mt[q];
         for (int s = 0; s < 2; s++) {
             m.Aex[s] = d.aAex[s]; m.K1c[s] = d.aK1c[s]; m.B1c[s] = d.aB1c[s]; m.B2c[s] = d.aB2c[s];
             m.J[s] = d.aJ[s]; m.ex[s] = d.aex[s]; m.prec[s] = d.aprec[s]; m.aprec[s] = d.aaprec[s];
@@ -306,12 +307,12 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIO io, const 
     auto afm_at = [&](uint8_t q) { return q != 0 && mt[q - 1].afm != 0u; };
 
     const uint8_t id = io.mid[c];
-    double dm[2][3] = {{0., 0., 0.}, {0., 0., 0.}};
+    R dm[2][3] = {{R(0.), R(0.), R(0.)}, {R(0.), R(0.), R(0.)}};
     if (afm_at(id)) {
-        const AFMMat& mat = mt[id - 1];
-        double exx = 0., eyy = 0., ezz = 0., eyz = 0., exz = 0., exy = 0.;
+        const AFMMat<R>& mat = mt[id - 1];
+        R exx = R(0.), eyy = R(0.), ezz = R(0.), eyz = R(0.), exz = R(0.), exy = R(0.);
         if (P.elasto_on) {
-            double e[6];
+            R e[6];
             cell_strain_total(P, io, i, j, k, c, e);
             exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
         }
@@ -328,44 +329,45 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIO io, const 
         const bool surf[6] = {(i == 0 && !P.per_x) || !afm_at(nid[0]), (i == nx - 1 && !P.per_x) || !afm_at(nid[1]),
                               (j == 0 && !P.per_y) || !afm_at(nid[2]), (j == ny - 1 && !P.per_y) || !afm_at(nid[3]),
                               (k == 0 && !P.per_z) || !afm_at(nid[4]), (k == nz - 1 && !P.per_z) || !afm_at(nid[5])};
-        double Hem[3] = {0., 0., 0.};
+        R Hem[3] = {R(0.), R(0.), R(0.)};
         if (P.em_back_M) {
             // cell-centred Maxwell H of the stage state (EMdynamic_solver.cpp:3780-3810)
             const int hx0 = (i * ny + j) * nz + k, hx1 = ((i + 1) * ny + j) * nz + k;
             const int hy0 = (i * (ny + 1) + j) * nz + k, hy1 = (i * (ny + 1) + j + 1) * nz + k;
             const int hz0 = (i * ny + j) * (nz + 1) + k, hz1 = hz0 + 1;
-            Hem[0] = (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / 2.;
-            Hem[1] = (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / 2.;
-            Hem[2] = (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / 2.;
+            Hem[0] = (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / R(2.);
+            Hem[1] = (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / R(2.);
+            Hem[2] = (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
         }
         const StageDrive& dr = stage_drive(io, S);
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
+        const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
 #pragma unroll
         for (int s = 0; s < 2; s++) {
-            const F3& ms = s ? io.a2_in : io.a1_in;
-            const F3& mo = s ? io.a1_in : io.a2_in;
-            const double mgx = ms.c[0][c], mgy = ms.c[1][c], mgz = ms.c[2][c];
-            const double mg[3] = {mgx, mgy, mgz};
-            double mx, my, mz;
+            const F3T<R>& ms = s ? io.a2_in : io.a1_in;
+            const F3T<R>& mo = s ? io.a1_in : io.a2_in;
+            const R mgx = ms.c[0][c], mgy = ms.c[1][c], mgz = ms.c[2][c];
+            const R mg[3] = {mgx, mgy, mgz};
+            R mx, my, mz;
             glb2crt(P, mgx, mgy, mgz, mx, my, mz);
             // exchange: slopes to the six neighbours (0 at surfaces), then
             // the second-difference terms d?/dx2_f = fwd/dx, _b = -bwd/dx
-            double Hex[3];
+            R Hex[3];
             {
-                double Aij[6];
+                R Aij[6];
 #pragma unroll
                 for (int f = 0; f < 6; f++) Aij[f] = surf[f] ? mat.Aex[s] : sA[s][id][nid[f]];
-                double acc[3] = {0., 0., 0.};
-                double d2[6][3];
+                R acc[3] = {R(0.), R(0.), R(0.)};
+                R d2[6][3];
 #pragma unroll
                 for (int dir = 0; dir < 3; dir++) {
                     const int fb = 2 * dir, ff = 2 * dir + 1;
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        const double bwd = surf[fb] ? 0. : qdiv(mg[a] - ms.c[a][nb[fb]], h[dir], rh[dir]);
-                        const double fwd = surf[ff] ? 0. : qdiv(ms.c[a][nb[ff]] - mg[a], h[dir], rh[dir]);
-                        d2[ff][a] = qdiv(fwd, h[dir], rh[dir]);
-                        d2[fb][a] = -qdiv(bwd, h[dir], rh[dir]);
+                        const R bwd = surf[fb] ? R(0.) : qdivR(mg[a] - ms.c[a][nb[fb]], h[dir], rh[dir], rhf[dir]);
+                        const R fwd = surf[ff] ? R(0.) : qdivR(ms.c[a][nb[ff]] - mg[a], h[dir], rh[dir], rhf[dir]);
+                        d2[ff][a] = qdivR(fwd, h[dir], rh[dir], rhf[dir]);
+                        d2[fb][a] = -qdivR(bwd, h[dir], rh[dir], rhf[dir]);
                     }
                 }
 #pragma unroll
@@ -376,27 +378,27 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIO io, const 
                 for (int a = 0; a < 3; a++) Hex[a] = mat.ex[s] * acc[a];
             }
             // uniaxial anisotropy (crystal frame)
-            const double udotm = mx * mat.u[0] + my * mat.u[1] + mz * mat.u[2];
-            double Hax, Hay, Haz;
-            crt2glb(P, 2. * mat.K1c[s] * udotm * mat.u[0], 2. * mat.K1c[s] * udotm * mat.u[1],
-                    2. * mat.K1c[s] * udotm * mat.u[2], Hax, Hay, Haz);
+            const R udotm = mx * mat.u[0] + my * mat.u[1] + mz * mat.u[2];
+            R Hax, Hay, Haz;
+            crt2glb(P, R(2.) * mat.K1c[s] * udotm * mat.u[0], R(2.) * mat.K1c[s] * udotm * mat.u[1],
+                    R(2.) * mat.K1c[s] * udotm * mat.u[2], Hax, Hay, Haz);
             // magnetoelastic field, factor -1
-            const double B1 = mat.B1c[s], B2 = mat.B2c[s];
-            double Hmx, Hmy, Hmz;
-            crt2glb(P, -1. * (B1 * (exx)*mx + B2 * ((exy)*my + (exz)*mz)), -1. * (B1 * (eyy)*my + B2 * ((exy)*mx + (eyz)*mz)),
-                    -1. * (B1 * (ezz)*mz + B2 * ((exz)*mx + (eyz)*my)), Hmx, Hmy, Hmz);
+            const R B1 = mat.B1c[s], B2 = mat.B2c[s];
+            R Hmx, Hmy, Hmz;
+            crt2glb(P, -R(1.) * (B1 * (exx)*mx + B2 * ((exy)*my + (exz)*mz)), -R(1.) * (B1 * (eyy)*my + B2 * ((exy)*mx + (eyz)*mz)),
+                    -R(1.) * (B1 * (ezz)*mz + B2 * ((exz)*mx + (eyz)*my)), Hmx, Hmy, Hmz);
             // inter-sublattice exchange with the other sublattice's stage state
-            const double Hix = mat.J[s] * mo.c[0][c], Hiy = mat.J[s] * mo.c[1][c], Hiz = mat.J[s] * mo.c[2][c];
-            double Hx = io.Hstat.c[0][c] + Hax + Hmx + Hex[0] + Hix + dr.Hext_afm[0];
-            double Hy = io.Hstat.c[1][c] + Hay + Hmy + Hex[1] + Hiy + dr.Hext_afm[1];
-            double Hz = io.Hstat.c[2][c] + Haz + Hmz + Hex[2] + Hiz + dr.Hext_afm[2];
+            const R Hix = mat.J[s] * mo.c[0][c], Hiy = mat.J[s] * mo.c[1][c], Hiz = mat.J[s] * mo.c[2][c];
+            R Hx = io.Hstat.c[0][c] + Hax + Hmx + Hex[0] + Hix + R(dr.Hext_afm[0]);
+            R Hy = io.Hstat.c[1][c] + Hay + Hmy + Hex[1] + Hiy + R(dr.Hext_afm[1]);
+            R Hz = io.Hstat.c[2][c] + Haz + Hmz + Hex[2] + Hiz + R(dr.Hext_afm[2]);
             if (P.em_back_M) { Hx = Hx + Hem[0]; Hy = Hy + Hem[1]; Hz = Hz + Hem[2]; }
-            const double px = mgy * Hz - mgz * Hy;
-            const double py = mgz * Hx - mgx * Hz;
-            const double pz = mgx * Hy - mgy * Hx;
-            const double qx = mgy * pz - mgz * py;
-            const double qy = mgz * px - mgx * pz;
-            const double qz = mgx * py - mgy * px;
+            const R px = mgy * Hz - mgz * Hy;
+            const R py = mgz * Hx - mgx * Hz;
+            const R pz = mgx * Hy - mgy * Hx;
+            const R qx = mgy * pz - mgz * py;
+            const R qy = mgz * px - mgx * pz;
+            const R qz = mgx * py - mgy * px;
             dm[s][0] = mat.prec[s] * px + mat.aprec[s] * qx;
             dm[s][1] = mat.prec[s] * py + mat.aprec[s] * qy;
             dm[s][2] = mat.prec[s] * pz + mat.aprec[s] * qz;
@@ -406,21 +408,53 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIO io, const 
 #pragma unroll
         for (int a = 0; a < 3; a++) { io.da1.c[a][c] = dm[0][a]; io.da2.c[a][c] = dm[1][a]; }
     }
-    // RK4 combination; the increment is summed before it is added to m
-    // (get_dm_AFM / update_m_AFM, magnetic_AFM_solver.cpp:1715-1835)
+    const bool afm_cell = afm_at(id);
+    if constexpr (is_mixed<R>::value) {
+        // mixed form: compensated RK4 of both sublattices, then |m_s| = 1
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-        const F3& X = s ? io.a2_x : io.a1_x;
-        const F3& O = s ? io.a2_out : io.a1_out;
-        const F3& A = s ? io.a2_acc : io.a1_acc;
+        for (int s = 0; s < 2; s++) {
+            const F3T<R>& X = s ? io.a2_x : io.a1_x;
+            const F3T<R>& O = s ? io.a2_out : io.a1_out;
+            const F3T<R>& A = s ? io.a2_acc : io.a1_acc;
+            const F3T<R>& Cm = s ? io.a2_cmp : io.a1_cmp;
+            if (S < 3) {
+                const float cf = (S == 2) ? 1.f : 0.5f;
+                float o[3];
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const double d = dm[s][a];
-            const double xv = X.c[a][c];
-            if (S == 0) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = qdiv(d, 6., kInv6); }
-            else if (S == 1) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
-            else if (S == 2) { O.c[a][c] = xv + d; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
-            else { A.c[a][c] = xv + (A.c[a][c] + qdiv(d, 6., kInv6)); }
+                for (int a = 0; a < 3; a++) {
+                    o[a] = X.c[a][c] + dm[s][a] * cf;
+                    A.c[a][c] = (S == 0) ? dm[s][a] * (1.f / 6.f) : A.c[a][c] + dm[s][a] * (1.f / 3.f);
+                }
+                if (afm_cell) renorm3(o[0], o[1], o[2]);
+#pragma unroll
+                for (int a = 0; a < 3; a++) O.c[a][c] = o[a];
+            } else {
+                float x[3], cm[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                    two_sum(X.c[a][c], (A.c[a][c] + dm[s][a] * (1.f / 6.f)) + Cm.c[a][c], x[a], cm[a]);
+                if (afm_cell) renorm_pair(x, cm);
+#pragma unroll
+                for (int a = 0; a < 3; a++) { A.c[a][c] = x[a]; Cm.c[a][c] = cm[a]; }
+            }
+        }
+    } else {
+        // RK4 combination; the increment is summed before it is added to m
+        // (get_dm_AFM / update_m_AFM, magnetic_AFM_solver.cpp:1715-1835)
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const F3& X = s ? io.a2_x : io.a1_x;
+            const F3& O = s ? io.a2_out : io.a1_out;
+            const F3& A = s ? io.a2_acc : io.a1_acc;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const double d = dm[s][a];
+                const double xv = X.c[a][c];
+                if (S == 0) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = qdiv(d, 6., kInv6); }
+                else if (S == 1) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
+                else if (S == 2) { O.c[a][c] = xv + d; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
+                else { A.c[a][c] = xv + (A.c[a][c] + qdiv(d, 6., kInv6)); }
+            }
         }
     }
 }

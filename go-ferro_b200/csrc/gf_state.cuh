@@ -44,7 +44,7 @@ struct StageIOT {
     // Drude polarisation currents of the three poles (cell arrays)
     F3 jp_in[3], jp_x[3], jp_acc[3], jp_out[3];
     // compensation words of the mixed form (null in the FP64 form)
-    F3 m_cmp, p_cmp, q_cmp, u_cmp, v_cmp, E_cmp, H_cmp;
+    F3 m_cmp, p_cmp, q_cmp, u_cmp, v_cmp, E_cmp, H_cmp, a1_cmp, a2_cmp, jp_cmp[3];
     // static and external fields
     F3 Hstat, Estat, Hnu;
     // face-normal displacement gradients of the current state, written by

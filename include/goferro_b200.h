@@ -117,8 +117,8 @@ int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out);
  *     renormalised to 1 after every stage (the reference does not
  *     renormalise).  The demag tensor and its spectra are built in FP64; the
  *     averages and every upload/download stay FP64 at this ABI.
- *     Antiferromagnets, Drude dispersion and perfect conductors are FP64
- *     only (GF_EUNSUPPORTED). */
+ *     Every physics of the FP64 form runs in both; the electrostatic
+ *     solve and the adjoint are FP64 only. */
 #define GF_PRECISION_FP64 0
 #define GF_PRECISION_MIXED_FP32 1
 

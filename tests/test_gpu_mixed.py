@@ -126,10 +126,37 @@ def test_mixed_graph_and_eager_identical(gf, tmp_path):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("vname", ["afm_film_demag", "drude_metal_layer", "pec_layer"])
-def test_mixed_rejects_fp64_only_physics(gf, tmp_path, vname):
-    d, _, _ = _variants(gf)[vname]
-    gf.decks.write_deck(d, str(tmp_path))
-    with pytest.raises(gf.GFError) as ei:
-        gf.Engine(str(tmp_path), device=0, precision="mixed")
-    assert ei.value.code == -7
+@pytest.mark.parametrize("vname", ["afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
+                                   "drude_metal_layer", "pec_layer"])
+def test_mixed_afm_drude_pec_match_live_oracle(gf, refrun, tmp_path, vname):
+    """Antiferromagnets (both sublattices renormalised every stage), Drude
+    poles and perfect conductors in the mixed form."""
+    d, steps, probe = _variants(gf)[vname]
+    gf.decks.write_deck(d, str(tmp_path / "deck"))
+    r = refrun.run(str(tmp_path / "deck"), str(tmp_path / "ref"), steps=steps, probe=probe, dump=False)
+    # the Drude deck probes E and H inside the metal layer, where screening
+    # makes them small differences of the large curl and polarisation-current
+    # terms: FP32 noise relative to that local scale is larger (1.9e-5
+    # measured), so that one case is held to 5e-5
+    tol = 5e-5 if vname == "drude_metal_layer" else TOL_MIXED
+    with gf.Engine(str(tmp_path / "deck"), device=0, precision="mixed") as eng:
+        mine = engine_trace(eng, steps, probe if probe else (0, 0, 0))
+        errs = assert_mixed_close_afm(mine, r["trace"], tol)
+        eng.check_finite()
+    assert errs
+
+
+def assert_mixed_close_afm(mine, ref, tol=TOL_MIXED):
+    """assert_mixed_close with the two sublattice averages as observables."""
+    groups = dict(GROUPS)
+    groups.update({"m1": (4, 7), "m2": (7, 10)})
+    out = {}
+    for name, (a, b) in groups.items():
+        scale = float(np.max(np.abs(ref[:, a:b])))
+        err = float(np.max(np.abs(mine[:, a:b] - ref[:, a:b])))
+        if scale == 0.0:
+            assert err == 0.0, f"{name}: expected zeros, got {err}"
+            continue
+        out[name] = err / scale
+        assert out[name] <= tol, f"{name}: relative trace error {out[name]:.3e} > {tol:.0e}"
+    return out
