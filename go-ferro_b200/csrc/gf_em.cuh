@@ -44,6 +44,25 @@ __device__ inline R jf_cell(const Params& P, const StageIOT<R>& io, R jf, int a,
     return jf;
 }
 
+// inverse-spin-Hall current density, component C (0 x, 1 y), of cell
+// (ci,cj,ck) (magnetic_system::get_J_ISHE_RK*, magnetic_solver.cpp:231-283):
+// coeff_Js coeff_L (m_C dm_z - m_z dm_C, summed over FM and both AFM
+// sublattices at the source plane) / dt, with the stage state m and its
+// increment dm
+template <class R>
+__device__ inline R ishe_cell(const Params& P, const StageIOT<R>& io, int C, int ci, int cj, int ck) {
+    const int sz = io.ishe_src[ck];
+    if (sz < 0) return R(0.);
+    const int s = (ci * P.ny + cj) * P.nz + sz;
+    R sum = R(0.);
+    if (P.fm) sum = io.m_in.c[C][s] * io.dm.c[2][s] - io.m_in.c[2][s] * io.dm.c[C][s];
+    if (P.afm) {
+        sum = sum + io.a1_in.c[C][s] * io.da1.c[2][s] - io.a1_in.c[2][s] * io.da1.c[C][s];
+        sum = sum + io.a2_in.c[C][s] * io.da2.c[2][s] - io.a2_in.c[2][s] * io.da2.c[C][s];
+    }
+    return qdivR(io.ishe_coef[ck] * sum, P.dt, P.rdt, P.f.rdt);
+}
+
 template <int S, class R>
 __device__ inline void rk_x(R xv, R d, R* out, R* acc, R* cmp, int e) {
     if constexpr (is_mixed<R>::value) {
@@ -153,6 +172,13 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
                 Jp = Jp + io.jp_in[0].c[C][cc] + io.jp_in[1].c[C][cc] + io.jp_in[2].c[C][cc];
             }
             rhs = rhs - Jp / R(4.);
+        }
+        if (C < 2 && P.spin) {
+            // inverse-spin-Hall current: 4-cell mean, x and y edges only
+            R Ji = R(0.);
+#pragma unroll
+            for (int q = 0; q < 4; q++) Ji = Ji + ishe_cell(P, io, C, cx[q], cy[q], cz[q]);
+            rhs = rhs - Ji / R(4.);
         }
         rhs = rhs - cond * io.E_in.c[C][e] - qdivR(dP, P.dt, P.rdt, P.f.rdt);
         d = dt_e0_r / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation

@@ -86,6 +86,8 @@ struct gf_engine {
     StepDrive* drive_host = nullptr;       // pinned staging
     unsigned long long* step_ctr = nullptr;
     double* jf_kfac = nullptr;
+    double* ishe_coef = nullptr;           // per k (run precision)
+    int* ishe_src = nullptr;               // per k
 
     Field3 m, a1, a2, p, q, u, v, E, H;
     Field3 jp[3];                      // Drude pole currents
@@ -201,6 +203,9 @@ cudaError_t klaunch(gf_engine* eng, const char* name, Kernel k, dim3 grid, dim3 
     return e;
 }
 
+// A zeroed device buffer.  The zeroing has finished when this returns: the
+// engine stream is non-blocking, so a later cudaMemcpy on the default stream
+// (the tables uploaded at creation) is not ordered after work queued on it.
 int dalloc(gf_engine* eng, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
@@ -210,6 +215,7 @@ int dalloc(gf_engine* eng, void** p, size_t bytes) {
     eng->allocs.push_back(*p);
     eng->bytes += bytes;
     e = cudaMemsetAsync(*p, 0, bytes, eng->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
     if (e != cudaSuccess) { eng->err = std::string("cudaMemset: ") + cudaGetErrorString(e); return GF_ECUDA; }
     return GF_OK;
 }
@@ -321,7 +327,6 @@ std::string unsupported(const Deck& d) {
     if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
         return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
     if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
-    if (d.spin_pumping) return "spin pumping (if_spin_pumping) is not supported by this engine";
     if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
     if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
     if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this engine";
@@ -396,6 +401,7 @@ void build_params(gf_engine* eng) {
         for (int j = 0; j < 3; j++) { P.f.Tg2c[i][j] = (float)P.Tg2c[i][j]; P.f.Tc2g[i][j] = (float)P.Tc2g[i][j]; }
     P.fm = d.any_fm; P.afm = d.any_afm; P.fe = d.any_fe; P.elastic = d.elastodynamics; P.em = d.em_dynamic;
     P.fe_mask = 0u; P.fm_mask = 0u;
+    P.spin = (d.spin_pumping && (d.any_fm || d.any_afm)) ? 1 : 0;
     for (size_t q = 0; q < d.mats.size() && q < 32; q++) {
         if (d.mats[q].fe) P.fe_mask |= 1u << q;
         if (d.mats[q].fm) P.fm_mask |= 1u << q;
@@ -663,6 +669,8 @@ void build_io(gf_engine* eng) {
             io.drive_mask = (unsigned long long)(kDriveCap - 1);
             io.step = eng->step_ctr;
             io.jf_kfac = eng->jf_kfac;
+            io.ishe_coef = eng->ishe_coef;
+            io.ishe_src = eng->ishe_src;
         }
 }
 
@@ -721,6 +729,8 @@ void build_io_mixed(gf_engine* eng) {
             io.drive_mask = (unsigned long long)(kDriveCap - 1);
             io.step = eng->step_ctr;
             io.jf_kfac = reinterpret_cast<const float*>(eng->jf_kfac);
+            io.ishe_coef = reinterpret_cast<const float*>(eng->ishe_coef);
+            io.ishe_src = eng->ishe_src;
         }
 }
 
@@ -1302,6 +1312,47 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
         GF_TRY(upload_one(eng, eng->jf_kfac, nullptr, kf.data(), (long)kf.size()));
     }
 
+    // spin pumping layers (global.cpp:168-240) and the per-k coefficient of
+    // get_J_ISHE_RK* (magnetic_solver.cpp:241-261): coeff_Js * coeff_L
+    if (P.spin) {
+        const double PI = kPi, unit_e = 1.602176634e-19;    // magnetic_system.h:15-16
+        std::vector<int> src((size_t)P.nz, -1);
+        std::vector<double> thick((size_t)P.nz, 0.), coef((size_t)P.nz, 0.);
+        auto mat_at_k = [&](long k) -> unsigned { return d.material_cell[(size_t)k]; };   // cell (0,0,k)
+        auto magnetic = [&](unsigned id) { return id != 0 && (d.mats[id - 1].fm || d.mats[id - 1].afm); };
+        long id_zf = (long)d.idzi - 1;
+        for (size_t L = 0; L < d.nz_layer.size(); L++) {
+            const long id_zi = id_zf + 1;
+            id_zf = id_zi + (long)d.nz_layer[L] - 1;
+            const unsigned mt = mat_at_k(id_zi);
+            if (mt == 0 || !d.mats[mt - 1].spin_pump) continue;
+            const bool si = id_zi != 0 && magnetic(mat_at_k(id_zi - 1));
+            const bool sf = id_zf != P.nz - 1 && magnetic(mat_at_k(id_zf + 1));
+            long s = -1;
+            if (si && !sf) s = id_zi - 1;
+            else if (!si && sf) s = id_zf + 1;
+            if (s < 0) continue;
+            for (long k = id_zi; k <= id_zf && k < P.nz; k++) { src[(size_t)k] = (int)s; thick[(size_t)k] = d.nz_layer[L] * P.dz; }
+        }
+        for (long k = 0; k < P.nz; k++) {
+            if (src[(size_t)k] < 0) continue;
+            const Material& m = d.mats[mat_at_k(k) - 1];
+            const double coeff_Js = m.sh_angle * unit_e / 2. / PI * m.sh_mixcond;
+            const double distance = (std::abs(static_cast<double>((k - src[(size_t)k]))) - 0.5) * P.dz;
+            double coeff_L;
+            if (k > src[(size_t)k])
+                coeff_L = std::sinh((thick[(size_t)k] - distance) / m.sh_difflen) / std::sinh(thick[(size_t)k] / m.sh_difflen);
+            else
+                coeff_L = -1. * std::sinh((thick[(size_t)k] - distance) / m.sh_difflen) / std::sinh(thick[(size_t)k] / m.sh_difflen);
+            coef[(size_t)k] = coeff_Js * coeff_L;
+        }
+        GF_TRY(dalloc_r(eng, &eng->ishe_coef, (size_t)P.nz));
+        GF_TRY(dalloc_n(eng, &eng->ishe_src, (size_t)P.nz));
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        GF_TRY(upload_one(eng, eng->ishe_coef, nullptr, coef.data(), P.nz));
+        GF_CU(cudaMemcpy(eng->ishe_src, src.data(), sizeof(int) * P.nz, cudaMemcpyHostToDevice));
+    }
+
     // state fields
     if (d.any_fm) GF_TRY(alloc_field(eng, eng->m, n, n, n));
     if (d.any_afm) { GF_TRY(alloc_field(eng, eng->a1, n, n, n)); GF_TRY(alloc_field(eng, eng->a2, n, n, n)); }
@@ -1315,8 +1366,8 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
         GF_TRY(alloc_field(eng, eng->H, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)));
     }
     for (int a = 0; a < 3; a++) {
-        if (P.em_fromM) GF_TRY(dalloc_r(eng, &eng->dm[a], (size_t)n));
-        if (P.em_fromM && d.any_afm) { GF_TRY(dalloc_r(eng, &eng->da1[a], (size_t)n)); GF_TRY(dalloc_r(eng, &eng->da2[a], (size_t)n)); }
+        if (P.em_fromM || P.spin) GF_TRY(dalloc_r(eng, &eng->dm[a], (size_t)n));
+        if ((P.em_fromM || P.spin) && d.any_afm) { GF_TRY(dalloc_r(eng, &eng->da1[a], (size_t)n)); GF_TRY(dalloc_r(eng, &eng->da2[a], (size_t)n)); }
         if (d.elastodynamics) {
             GF_TRY(dalloc_r(eng, &eng->force_store[a], (size_t)n));
             GF_TRY(dalloc_r(eng, &eng->force[a], (size_t)n));

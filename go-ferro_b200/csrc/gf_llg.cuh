@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
         dmy = precess * py + mat.alpha_precess * qy;
         dmz = precess * pz + mat.alpha_precess * qz;
     }
-    if (P.em_fromM) { io.dm.c[0][c] = dmx; io.dm.c[1][c] = dmy; io.dm.c[2][c] = dmz; }
+    if (P.em_fromM || P.spin) { io.dm.c[0][c] = dmx; io.dm.c[1][c] = dmy; io.dm.c[2][c] = dmz; }
 
     if constexpr (is_mixed<R>::value) {
         // mixed form: compensated RK4, then |m| = 1 (ferromagnetic cells only;
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
             dm[s][2] = mat.prec[s] * pz + mat.aprec[s] * qz;
         }
     }
-    if (P.em_fromM) {
+    if (P.em_fromM || P.spin) {
 #pragma unroll
         for (int a = 0; a < 3; a++) { io.da1.c[a][c] = dm[0][a]; io.da2.c[a][c] = dm[1][a]; }
     }

@@ -70,6 +70,10 @@ struct StageIOT {
     const unsigned long long* step;   // index of the step being computed (0-based)
     unsigned long long drive_mask;    // drive ring holds drive_mask+1 steps
     const R* jf_kfac;            // per-k spatial factor of J_f types 1,2
+    // spin pumping: per-k coefficient coeff_Js * coeff_L of the inverse-spin-
+    // Hall current and the source plane of layer k (-1: no current)
+    const R* ishe_coef;
+    const int* ishe_src;
 };
 using StageIO = StageIOT<double>;
 

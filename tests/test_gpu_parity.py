@@ -221,6 +221,21 @@ def _variants(gf):
     d.layers = [(3, 2), (7, 1)]
     d.jf_lo, d.jf_hi = (0, 0, 5), (7, 7, 5)
     v["pec_layer"] = (d, 20, (4, 4, 6))
+    # spin pumping: a heavy-metal layer under a YIG film, inverse-spin-Hall
+    # current from m x dm/dt of the film's bottom plane driving the Yee E field
+    d = D.preset_fm_demag(nx=8, ny=8, nz=12, steps=20)
+    d.dt = 4e-18
+    metal = D.Material(title="Pt", c11=3.47e11, c12=2.51e11, c44=0.765e11, density=21450.0, er=1.0, cond=1e5,
+                       spin_pump=True, spin=(0.1, 1e19, 2e-9))
+    d.materials = [metal, D.yig(0.01)]
+    # no vacuum layer: with spin pumping on, the reference reads the material
+    # of every layer's first cell without a vacuum test (global.cpp:185)
+    d.layers = [(4, 1), (8, 2)]
+    d.m0 = D.tilt_m0((8, 8, 12), 31, d.material_cell() == 2, max_deg=5.0)
+    d.em, d.em_fromM, d.em_back_M = True, True, True
+    d.spin_pumping = True
+    d.periodic = (True, True, False)
+    v["spin_pumping_ishe"] = (d, 20, (4, 4, 2))
     return v
 
 
@@ -228,7 +243,7 @@ def _variants(gf):
                                    "fe_jf6_plane_wave_eext", "two_fm_materials_dmi_uniaxial", "demag_factor",
                                    "elastic_multi_tile", "elastic_quirk_far_tile", "fm_film_demag_substrate",
                                    "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
-                                   "drude_metal_layer", "pec_layer"])
+                                   "drude_metal_layer", "pec_layer", "spin_pumping_ishe"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
