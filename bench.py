@@ -230,6 +230,22 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def max_over_ranks(x: float, dist, torch, device: str) -> float:
+    """The largest value of x over all ranks (x itself without a process
+    group): replicas are timed by the slowest rank."""
+    if not dist:
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, cells: int, steps: int, seconds: float) -> float:
+    """Whole-job cell-steps/s of `world` replicas, each advancing `cells`
+    cells by `steps` steps, timed by the slowest rank."""
+    return world * cells * steps / seconds
+
+
 TRACE_GROUPS = {"m": (0, 3), "p": (3, 6), "u": (6, 9), "E": (9, 12), "H": (12, 15)}
 
 
@@ -296,13 +312,10 @@ def measure(gf, torch, dist, args, world, local_rank, precision, d, ddir, upload
     if dist:
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, torch, "cuda")
     clocks = cs.summary()
     info = eng.get_info()
-    value = world * ncell * args.steps / (ms / 1e3)
+    value = aggregate_rate(world, ncell, args.steps, ms / 1e3)
 
     # ---- end-to-end through the C ABI with host buffers ----
     e2e_steps = max(1, min(args.steps, 20))
@@ -317,11 +330,8 @@ def measure(gf, torch, dist, args, world, local_rank, precision, d, ddir, upload
         if info.em:
             eng.probe_em(*probe)
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * ncell * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(e2e_s, dist, torch, "cuda")
+    e2e_value = aggregate_rate(world, ncell, e2e_steps, e2e_s)
     h2d = 520     # one StepDrive row per step (time + 4 stage rows of 128 B)
     d2h = 8 * 3 * len(obs) + (8 * 6 if info.em else 0)  # averages, E and H at the probe cell
 
