@@ -90,6 +90,7 @@ struct Params {
     int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
     uint32_t fe_mask, fm_mask;   // bit id-1 set when material id is ferroelectric / ferromagnetic
     int spin;                 // spin pumping: inverse-spin-Hall current in the Yee E update
+    int em_cls;               // the Yee E update reads per-edge material classes (StageIOT::ecls)
     int drude;                // some material has a Drude pole (omega_plasma != 0)
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;

@@ -35,6 +35,21 @@ struct EmMat {
     int pad_;
 };
 
+// Material class of an E edge: what the update needs from the four cells
+// around it, precomputed on the host in the kernel's order of operations
+// (coef = (dt/e0) / ((er1+er2+er3+er4)/4), cond = (s1+s2+s3+s4)/4 over
+// material cells, pc = ferroelectric cell count or 1, bit q of mask set when
+// cell q is not vacuum).  Edges share few distinct classes, so one byte per
+// edge and a table in shared memory replace four material-id loads, twelve
+// table reads and a division per edge.
+template <class R>
+struct EmCls {
+    R coef, cond, pc;
+    uint32_t mask;
+    int pad_;
+};
+constexpr int kEmMaxCls = 256;
+
 // free current J_f of cell (i,j,k), component a; jf = the stage's amplitude
 template <class R>
 __device__ inline R jf_cell(const Params& P, const StageIOT<R>& io, R jf, int a, int i, int j, int k) {
@@ -78,7 +93,7 @@ __device__ inline void rk_x(R xv, R d, R* out, R* acc, R* cmp, int e) {
 // E edge update of component C at edge (i,j,k) (index e in C's array).
 template <int S, int C, class R>
 __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const StageDrive& dr, const EmMat<R>* mt,
-                                 int i, int j, int k, int e) {
+                                 const EmCls<R>* cls, int i, int j, int k, int e) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     R dt_r, dt_e0_r;
     if constexpr (is_mixed<R>::value) { dt_r = P.f.dt; dt_e0_r = P.f.dt_e0; } else { dt_r = P.dt; dt_e0_r = P.dt_e0; }
@@ -139,29 +154,41 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
 #pragma unroll
             for (int q = 0; q < 4; q++) qv[q] = io.q_in.c[C][(cx[q] * ny + cy[q]) * nz + cz[q]];
         }
+        R coef;
+        if (P.em_cls) {
+            const EmCls<R>& kc = cls[io.ecls[C][e]];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
-            const uint8_t id = io.mid[cc];
-            if (id == 0) {
-                er = er + R(1.);
-            } else {
-                const EmMat<R>& m = mt[id - 1];
-                if (P.em_fromP) dP = dP + qv[q] * dt_r;
-                if (m.flags & MF_FE) pc = pc + R(1.);
-                er = er + m.er;
-                cond = cond + m.cond;
+            for (int q = 0; q < 4; q++) {
+                if (P.em_fromP && ((kc.mask >> q) & 1u)) dP = dP + qv[q] * dt_r;
+                if (P.jf_on) Jf = Jf + jf_cell(P, io, R(dr.jf), C, cx[q], cy[q], cz[q]);
             }
-            if (P.jf_on) Jf = Jf + jf_cell(P, io, R(dr.jf), C, cx[q], cy[q], cz[q]);
+            pc = kc.pc; cond = kc.cond; coef = kc.coef;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int cc = (cx[q] * ny + cy[q]) * nz + cz[q];
+                const uint8_t id = io.mid[cc];
+                if (id == 0) {
+                    er = er + R(1.);
+                } else {
+                    const EmMat<R>& m = mt[id - 1];
+                    if (P.em_fromP) dP = dP + qv[q] * dt_r;
+                    if (m.flags & MF_FE) pc = pc + R(1.);
+                    er = er + m.er;
+                    cond = cond + m.cond;
+                }
+                if (P.jf_on) Jf = Jf + jf_cell(P, io, R(dr.jf), C, cx[q], cy[q], cz[q]);
+            }
+            if (pc < R(0.5)) pc = R(1.);
+            er = er / R(4.); cond = cond / R(4.);
+            coef = dt_e0_r / er;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
         }
-        if (pc < R(0.5)) pc = R(1.);
         Jf = Jf / R(4.);
         // pc counts the ferroelectric cells (1..4): divisions by 1, 2 and 4 are exact
         if constexpr (is_mixed<R>::value)
             dP = dP * (pc == 3.f ? 1.f / 3.f : (pc == 1.f ? 1.f : (pc == 2.f ? 0.5f : 0.25f)));
         else
             dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
-        er = er / R(4.); cond = cond / R(4.);
         R rhs = curl - Jf;
         if (P.drude) {
             // Drude current: 4-cell mean of the three poles' stage values
@@ -181,7 +208,7 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
             rhs = rhs - Ji / R(4.);
         }
         rhs = rhs - cond * io.E_in.c[C][e] - qdivR(dP, P.dt, P.rdt, P.f.rdt);
-        d = dt_e0_r / er * rhs;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
+        d = coef * rhs;
     }
     rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], io.E_cmp.c[C], e);
 }
@@ -259,12 +286,15 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
 template <int S, class R = double>
 // (256, 8): 32 registers, 64 resident warps per SM; the kernel is bound by
 // the latency of its neighbour loads, and full occupancy beats the spills
-__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) k_em_fused(Params P, StageIOT<R> io, int nmat) {
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) k_em_fused(Params P, StageIOT<R> io, int nmat,
+                                                                                      const EmCls<R>* __restrict__ cls_g, int ncls) {
     __shared__ EmMat<R> mt[kMaxMat];
+    __shared__ EmCls<R> cl[kEmMaxCls];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMatT<R>& d = io.mats[q];
         mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].Ms1 = d.Ms1; mt[q].Ms2 = d.Ms2; mt[q].flags = d.flags;
     }
+    for (int q = threadIdx.x; q < ncls; q += blockDim.x) cl[q] = cls_g[q];
     __syncthreads();
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,9 +302,9 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) 
     const int i = blockIdx.y;
     const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
     const StageDrive& dr = stage_drive(io, S);
-    if (i < nx) em_E_edge<S, 0, R>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
-    if (j < ny) em_E_edge<S, 1, R>(P, io, dr, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
-    if (k < nz) em_E_edge<S, 2, R>(P, io, dr, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
+    if (i < nx) em_E_edge<S, 0, R>(P, io, dr, mt, cl, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
+    if (j < ny) em_E_edge<S, 1, R>(P, io, dr, mt, cl, i, j, k, (i * ny + j) * (nz + 1) + k);
+    if (k < nz) em_E_edge<S, 2, R>(P, io, dr, mt, cl, i, j, k, (i * (ny + 1) + j) * nz + k);
     if (j < ny && k < nz) em_H_face<S, 0, R>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
     if (i < nx && k < nz) em_H_face<S, 1, R>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
     if (i < nx && j < ny) em_H_face<S, 2, R>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -88,6 +89,9 @@ struct gf_engine {
     double* jf_kfac = nullptr;
     double* ishe_coef = nullptr;           // per k (run precision)
     int* ishe_src = nullptr;               // per k
+    uint8_t* ecls[3] = {nullptr, nullptr, nullptr};   // material class of every E edge (setup_em_classes)
+    void* em_cls_tab = nullptr;            // EmCls<R> table of the run precision
+    int em_ncls = 0;
 
     Field3 m, a1, a2, p, q, u, v, E, H;
     Field3 jp[3];                      // Drude pole currents
@@ -671,6 +675,7 @@ void build_io(gf_engine* eng) {
             io.jf_kfac = eng->jf_kfac;
             io.ishe_coef = eng->ishe_coef;
             io.ishe_src = eng->ishe_src;
+            for (int c = 0; c < 3; c++) io.ecls[c] = eng->ecls[c];
         }
 }
 
@@ -731,6 +736,7 @@ void build_io_mixed(gf_engine* eng) {
             io.jf_kfac = reinterpret_cast<const float*>(eng->jf_kfac);
             io.ishe_coef = reinterpret_cast<const float*>(eng->ishe_coef);
             io.ishe_src = eng->ishe_src;
+            for (int c = 0; c < 3; c++) io.ecls[c] = eng->ecls[c];
         }
 }
 
@@ -917,7 +923,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
         GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
-                      dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size()));
+                      dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size(),
+                      static_cast<const EmCls<R>*>(eng->em_cls_tab), eng->em_ncls));
         if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S, R>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0, R>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
         if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1, R>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
@@ -1226,6 +1233,110 @@ int initial_state(gf_engine* eng, const std::string& dir) {
     return GF_OK;
 }
 
+// Material class of the E edge whose four cells (in the kernel's order 1..4)
+// hold ids[]: the kernel's sums and division, done here once per class.
+template <class R>
+EmCls<R> em_class(const Deck& d, const unsigned ids[4], R dt_e0) {
+    R er = R(0.), cond = R(0.), pc = R(0.);
+    uint32_t mask = 0;
+    for (int q = 0; q < 4; q++) {
+        if (ids[q] == 0) { er = er + R(1.); continue; }
+        const Material& m = d.mats[ids[q] - 1];
+        mask |= 1u << q;
+        if (m.fe) pc = pc + R(1.);
+        er = er + static_cast<R>(m.er);
+        cond = cond + static_cast<R>(m.cond);
+    }
+    if (pc < R(0.5)) pc = R(1.);
+    er = er / R(4.);
+    EmCls<R> c;
+    c.coef = dt_e0 / er;
+    c.cond = cond / R(4.);
+    c.pc = pc;
+    c.mask = mask;
+    c.pad_ = 0;
+    return c;
+}
+
+// Per-edge classes of the Yee E update (k_em_fused): one byte per edge and a
+// table of the distinct cell quadruples.  A deck with more quadruples than a
+// byte indexes keeps the per-cell material lookups (Params::em_cls = 0).
+// Edges on a non-periodic boundary are not updated by that kernel; they get
+// class 0.
+int setup_em_classes(gf_engine* eng) {
+    Params& P = eng->P;
+    const Deck& d = eng->deck;
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    auto mc = [&](long i, long j, long k) -> unsigned { return d.material_cell[(size_t)((i * ny + j) * nz + k)]; };
+    std::unordered_map<uint32_t, int> index;
+    std::vector<uint32_t> keys;
+    std::vector<uint8_t> cls[3];
+    const long ext[3][3] = {{nx, ny + 1, nz + 1}, {nx + 1, ny, nz + 1}, {nx + 1, ny + 1, nz}};
+    // neighbour cells of a node coordinate along an axis of n cells: (lower, upper), wrapped at the ends
+    auto lo = [](long c, long n) { return (c == 0 || c == n) ? n - 1 : c - 1; };
+    auto hi = [](long c, long n) { return (c == 0 || c == n) ? 0 : c; };
+    for (int C = 0; C < 3; C++) {
+        cls[C].assign((size_t)(ext[C][0] * ext[C][1] * ext[C][2]), 0);
+        for (long i = 0; i < ext[C][0]; i++)
+            for (long j = 0; j < ext[C][1]; j++)
+                for (long k = 0; k < ext[C][2]; k++) {
+                    bool bnd = false;
+                    unsigned ids[4];
+                    if (C == 0) {
+                        bnd = ((j == 0 || j == ny) && !P.per_y) || ((k == 0 || k == nz) && !P.per_z);
+                        const long y1 = lo(j, ny), y3 = hi(j, ny), z1 = lo(k, nz), z2 = hi(k, nz);
+                        ids[0] = mc(i, y1, z1); ids[1] = mc(i, y1, z2); ids[2] = mc(i, y3, z1); ids[3] = mc(i, y3, z2);
+                    } else if (C == 1) {
+                        bnd = ((i == 0 || i == nx) && !P.per_x) || ((k == 0 || k == nz) && !P.per_z);
+                        const long x1 = lo(i, nx), x3 = hi(i, nx), z1 = lo(k, nz), z2 = hi(k, nz);
+                        ids[0] = mc(x1, j, z1); ids[1] = mc(x1, j, z2); ids[2] = mc(x3, j, z1); ids[3] = mc(x3, j, z2);
+                    } else {
+                        bnd = ((i == 0 || i == nx) && !P.per_x) || ((j == 0 || j == ny) && !P.per_y);
+                        const long x1 = lo(i, nx), x3 = hi(i, nx), y1 = lo(j, ny), y2 = hi(j, ny);
+                        ids[0] = mc(x1, y1, k); ids[1] = mc(x1, y2, k); ids[2] = mc(x3, y1, k); ids[3] = mc(x3, y2, k);
+                    }
+                    if (bnd) continue;
+                    const uint32_t key = ids[0] | (ids[1] << 8) | (ids[2] << 16) | (ids[3] << 24);
+                    auto it = index.find(key);
+                    int c;
+                    if (it == index.end()) {
+                        c = (int)keys.size();
+                        if (c >= kEmMaxCls) { P.em_cls = 0; return GF_OK; }
+                        index.emplace(key, c);
+                        keys.push_back(key);
+                    } else {
+                        c = it->second;
+                    }
+                    cls[C][(size_t)((i * ext[C][1] + j) * ext[C][2] + k)] = (uint8_t)c;
+                }
+    }
+    if (keys.empty()) keys.push_back(0u);
+    const size_t nk = keys.size();
+    auto ids_of = [](uint32_t key, unsigned* ids) { for (int q = 0; q < 4; q++) ids[q] = (key >> (8 * q)) & 0xffu; };
+    if (eng->mixed) {
+        std::vector<EmCls<float>> t(nk);
+        for (size_t c = 0; c < nk; c++) { unsigned ids[4]; ids_of(keys[c], ids); t[c] = em_class<float>(d, ids, P.f.dt_e0); }
+        EmCls<float>* dp = nullptr;
+        GF_TRY(dalloc_n(eng, &dp, nk));
+        GF_CU(cudaMemcpy(dp, t.data(), sizeof(EmCls<float>) * nk, cudaMemcpyHostToDevice));
+        eng->em_cls_tab = dp;
+    } else {
+        std::vector<EmCls<double>> t(nk);
+        for (size_t c = 0; c < nk; c++) { unsigned ids[4]; ids_of(keys[c], ids); t[c] = em_class<double>(d, ids, P.dt_e0); }
+        EmCls<double>* dp = nullptr;
+        GF_TRY(dalloc_n(eng, &dp, nk));
+        GF_CU(cudaMemcpy(dp, t.data(), sizeof(EmCls<double>) * nk, cudaMemcpyHostToDevice));
+        eng->em_cls_tab = dp;
+    }
+    for (int C = 0; C < 3; C++) {
+        GF_TRY(dalloc_n(eng, &eng->ecls[C], cls[C].size()));
+        GF_CU(cudaMemcpy(eng->ecls[C], cls[C].data(), cls[C].size(), cudaMemcpyHostToDevice));
+    }
+    eng->em_ncls = (int)nk;
+    P.em_cls = 1;
+    return GF_OK;
+}
+
 int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     if (precision != GF_PRECISION_FP64 && precision != GF_PRECISION_MIXED_FP32) {
         eng->err = "precision must be GF_PRECISION_FP64 or GF_PRECISION_MIXED_FP32";
@@ -1388,6 +1499,7 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
         GF_TRY(dalloc_r(eng, &eng->liao_hist, 4 * 12 * plane));
         GF_TRY(dalloc_r(eng, &eng->liao_last, 3 * plane));
     }
+    if (P.em) GF_TRY(setup_em_classes(eng));
     // FP64 scratch: output staging (6 cell arrays, or one widened Yee
     // component in the mixed form) and the reduction partials
     const size_t yee_max = (size_t)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);

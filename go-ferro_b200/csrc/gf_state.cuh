@@ -74,6 +74,8 @@ struct StageIOT {
     // Hall current and the source plane of layer k (-1: no current)
     const R* ishe_coef;
     const int* ishe_src;
+    // material class of every E edge, per component (Params::em_cls)
+    const uint8_t* ecls[3];
 };
 using StageIO = StageIOT<double>;
 
