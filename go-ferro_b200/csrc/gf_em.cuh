@@ -78,75 +78,135 @@ __device__ inline R ishe_cell(const Params& P, const StageIOT<R>& io, int C, int
     return qdivR(io.ishe_coef[ck] * sum, P.dt, P.rdt, P.f.rdt);
 }
 
-template <int S, class R>
-__device__ inline void rk_x(R xv, R d, R* out, R* acc, R* cmp, int e) {
-    if constexpr (is_mixed<R>::value) {
-        rk_mixed<S>(xv, d, out, acc, cmp, e);
+// Cells around an E edge, in the reference's order 1..4, and whether the
+// edge lies on a non-periodic boundary (then it keeps its value).
+struct EdgeGeom {
+    bool bnd;
+    int cx[4], cy[4], cz[4];
+};
+
+template <int C>
+__device__ inline EdgeGeom edge_geom(const Params& P, int i, int j, int k) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    EdgeGeom g;
+    g.bnd = false;
+    if (C == 0) {
+        if ((j == 0 || j == ny) && !P.per_y) g.bnd = true;
+        if ((k == 0 || k == nz) && !P.per_z) g.bnd = true;
+        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y3 = (j == 0 || j == ny) ? 0 : j;
+        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        g.cx[0] = g.cx[1] = g.cx[2] = g.cx[3] = i;
+        g.cy[0] = y1; g.cy[1] = y1; g.cy[2] = y3; g.cy[3] = y3;
+        g.cz[0] = z1; g.cz[1] = z2; g.cz[2] = z1; g.cz[3] = z2;
+    } else if (C == 1) {
+        if ((i == 0 || i == nx) && !P.per_x) g.bnd = true;
+        if ((k == 0 || k == nz) && !P.per_z) g.bnd = true;
+        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
+        g.cx[0] = x1; g.cx[1] = x1; g.cx[2] = x3; g.cx[3] = x3;
+        g.cy[0] = g.cy[1] = g.cy[2] = g.cy[3] = j;
+        g.cz[0] = z1; g.cz[1] = z2; g.cz[2] = z1; g.cz[3] = z2;
     } else {
-        if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
-        else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
-        else if (S == 2) { out[e] = xv + d; acc[e] = acc[e] + qdiv(d, 3., kInv3); }
-        else { acc[e] = acc[e] + qdiv(d, 6., kInv6); }
+        if ((i == 0 || i == nx) && !P.per_x) g.bnd = true;
+        if ((j == 0 || j == ny) && !P.per_y) g.bnd = true;
+        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
+        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y2 = (j == 0 || j == ny) ? 0 : j;
+        g.cx[0] = x1; g.cx[1] = x1; g.cx[2] = x3; g.cx[3] = x3;
+        g.cy[0] = y1; g.cy[1] = y2; g.cy[2] = y1; g.cy[3] = y2;
+        g.cz[0] = g.cz[1] = g.cz[2] = g.cz[3] = k;
+    }
+    return g;
+}
+
+// What a Yee update reads at its own index and from its curl stencil.  The
+// fused kernel gathers these for all three E edges (then all three H faces)
+// of a thread before any of their stores, so that those loads are in flight
+// together instead of one component's round trip after another.
+template <class R>
+struct YeeIn {
+    R c[4];          // curl operands: (c0 - c1) / h_a - (c2 - c3) / h_b
+    R x, self, acc, cmp;   // step value, stage value, RK accumulator, compensation
+    R dm1, dm2;      // H faces: dm of the two face cells
+    int c1, c2;      // H faces: the two face cells
+    uint8_t t1, t2;  // E edges: material class (t1); H faces: ids of the two cells
+};
+
+// accumulator (stages 1..3) and compensation (mixed form, last stage) of index e
+template <int S, class R>
+__device__ inline void rk_loads(const R* acc, const R* cmp, int e, YeeIn<R>& L) {
+    if (S > 0) L.acc = acc[e];
+    if constexpr (is_mixed<R>::value) { if (S == 3) L.cmp = cmp[e]; }
+}
+
+template <int S, int C, class R>
+__device__ inline void edge_load(const Params& P, const StageIOT<R>& io, const EdgeGeom& g, int i, int j, int k, int e,
+                                 YeeIn<R>& L) {
+    const int ny = P.ny, nz = P.nz;
+    L.x = io.E_x.c[C][e];
+    rk_loads<S>(io.E_acc.c[C], io.E_cmp.c[C], e, L);
+    if (g.bnd) return;
+    L.self = (S == 0) ? L.x : io.E_in.c[C][e];
+    if (P.em_cls) L.t1 = io.ecls[C][e];
+    const R* Hx = io.H_in.c[0];
+    const R* Hy = io.H_in.c[1];
+    const R* Hz = io.H_in.c[2];
+    if (C == 0) {
+        L.c[0] = Hz[(i * ny + g.cy[2]) * (nz + 1) + g.cz[3]]; L.c[1] = Hz[(i * ny + g.cy[0]) * (nz + 1) + g.cz[3]];
+        L.c[2] = Hy[(i * (ny + 1) + g.cy[2]) * nz + g.cz[1]]; L.c[3] = Hy[(i * (ny + 1) + g.cy[2]) * nz + g.cz[0]];
+    } else if (C == 1) {
+        L.c[0] = Hx[(g.cx[2] * ny + j) * nz + g.cz[3]]; L.c[1] = Hx[(g.cx[2] * ny + j) * nz + g.cz[2]];
+        L.c[2] = Hz[(g.cx[2] * ny + j) * (nz + 1) + g.cz[1]]; L.c[3] = Hz[(g.cx[0] * ny + j) * (nz + 1) + g.cz[1]];
+    } else {
+        L.c[0] = Hy[(g.cx[2] * (ny + 1) + g.cy[1]) * nz + k]; L.c[1] = Hy[(g.cx[0] * (ny + 1) + g.cy[1]) * nz + k];
+        L.c[2] = Hx[(g.cx[2] * ny + g.cy[1]) * nz + k]; L.c[3] = Hx[(g.cx[2] * ny + g.cy[0]) * nz + k];
     }
 }
 
-// E edge update of component C at edge (i,j,k) (index e in C's array).
+// curl from the gathered operands; component C's two grid spacings are
+// (y, z), (z, x), (x, y)
+template <int C, class R>
+__device__ inline R yee_curl(const Params& P, const YeeIn<R>& L) {
+    if (C == 0) return qdivR(L.c[0] - L.c[1], P.dy, P.rdy, P.f.rdy) - qdivR(L.c[2] - L.c[3], P.dz, P.rdz, P.f.rdz);
+    if (C == 1) return qdivR(L.c[0] - L.c[1], P.dz, P.rdz, P.f.rdz) - qdivR(L.c[2] - L.c[3], P.dx, P.rdx, P.f.rdx);
+    return qdivR(L.c[0] - L.c[1], P.dx, P.rdx, P.f.rdx) - qdivR(L.c[2] - L.c[3], P.dy, P.rdy, P.f.rdy);
+}
+
+template <int S, class R>
+__device__ inline void rk_x(const YeeIn<R>& L, R d, R* out, R* acc, R* cmp, int e) {
+    const R xv = L.x;
+    if constexpr (is_mixed<R>::value) {
+        if (S == 0) { out[e] = xv + d * 0.5f; acc[e] = d * (1.f / 6.f); }
+        else if (S == 1) { out[e] = xv + d * 0.5f; acc[e] = L.acc + d * (1.f / 3.f); }
+        else if (S == 2) { out[e] = xv + d; acc[e] = L.acc + d * (1.f / 3.f); }
+        else {
+            float sum, err;
+            two_sum(xv, (L.acc + d * (1.f / 6.f)) + L.cmp, sum, err);
+            acc[e] = sum;
+            cmp[e] = err;
+        }
+    } else {
+        if (S == 0) { out[e] = xv + d * 0.5; acc[e] = xv + qdiv(d, 6., kInv6); }
+        else if (S == 1) { out[e] = xv + d * 0.5; acc[e] = L.acc + qdiv(d, 3., kInv3); }
+        else if (S == 2) { out[e] = xv + d; acc[e] = L.acc + qdiv(d, 3., kInv3); }
+        else { acc[e] = L.acc + qdiv(d, 6., kInv6); }
+    }
+}
+
+// E edge update of component C at edge (i,j,k) (index e in C's array), from
+// the gathered values L.
 template <int S, int C, class R>
 __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const StageDrive& dr, const EmMat<R>* mt,
-                                 const EmCls<R>* cls, int i, int j, int k, int e) {
-    const int nx = P.nx, ny = P.ny, nz = P.nz;
+                                 const EmCls<R>* cls, const EdgeGeom& g, const YeeIn<R>& L, int e) {
+    const int ny = P.ny, nz = P.nz;
     R dt_r, dt_e0_r;
     if constexpr (is_mixed<R>::value) { dt_r = P.f.dt; dt_e0_r = P.f.dt_e0; } else { dt_r = P.dt; dt_e0_r = P.dt_e0; }
+    const int* cx = g.cx;
+    const int* cy = g.cy;
+    const int* cz = g.cz;
 
     R d = R(0.);
-    bool boundary = false;
-    int cx[4], cy[4], cz[4];
-    // cell quadruples around the edge, in the reference's order 1..4
-    if (C == 0) {
-        if ((j == 0 || j == ny) && !P.per_y) boundary = true;
-        if ((k == 0 || k == nz) && !P.per_z) boundary = true;
-        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y3 = (j == 0 || j == ny) ? 0 : j;
-        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
-        cx[0] = cx[1] = cx[2] = cx[3] = i;
-        cy[0] = y1; cy[1] = y1; cy[2] = y3; cy[3] = y3;
-        cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
-    } else if (C == 1) {
-        if ((i == 0 || i == nx) && !P.per_x) boundary = true;
-        if ((k == 0 || k == nz) && !P.per_z) boundary = true;
-        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
-        const int z1 = (k == 0 || k == nz) ? nz - 1 : k - 1, z2 = (k == 0 || k == nz) ? 0 : k;
-        cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
-        cy[0] = cy[1] = cy[2] = cy[3] = j;
-        cz[0] = z1; cz[1] = z2; cz[2] = z1; cz[3] = z2;
-    } else {
-        if ((i == 0 || i == nx) && !P.per_x) boundary = true;
-        if ((j == 0 || j == ny) && !P.per_y) boundary = true;
-        const int x1 = (i == 0 || i == nx) ? nx - 1 : i - 1, x3 = (i == 0 || i == nx) ? 0 : i;
-        const int y1 = (j == 0 || j == ny) ? ny - 1 : j - 1, y2 = (j == 0 || j == ny) ? 0 : j;
-        cx[0] = x1; cx[1] = x1; cx[2] = x3; cx[3] = x3;
-        cy[0] = y1; cy[1] = y2; cy[2] = y1; cy[3] = y2;
-        cz[0] = cz[1] = cz[2] = cz[3] = k;
-    }
-
-    if (!boundary) {
-        // curl of the stage H
-        R curl;
-        const R* Hx = io.H_in.c[0];
-        const R* Hy = io.H_in.c[1];
-        const R* Hz = io.H_in.c[2];
-        if (C == 0) {
-            const R dHzdy = qdivR((Hz[(i * ny + cy[2]) * (nz + 1) + cz[3]] - Hz[(i * ny + cy[0]) * (nz + 1) + cz[3]]), P.dy, P.rdy, P.f.rdy);
-            const R dHydz = qdivR((Hy[(i * (ny + 1) + cy[2]) * nz + cz[1]] - Hy[(i * (ny + 1) + cy[2]) * nz + cz[0]]), P.dz, P.rdz, P.f.rdz);
-            curl = dHzdy - dHydz;
-        } else if (C == 1) {
-            const R dHxdz = qdivR((Hx[(cx[2] * ny + j) * nz + cz[3]] - Hx[(cx[2] * ny + j) * nz + cz[2]]), P.dz, P.rdz, P.f.rdz);
-            const R dHzdx = qdivR((Hz[(cx[2] * ny + j) * (nz + 1) + cz[1]] - Hz[(cx[0] * ny + j) * (nz + 1) + cz[1]]), P.dx, P.rdx, P.f.rdx);
-            curl = dHxdz - dHzdx;
-        } else {
-            const R dHydx = qdivR((Hy[(cx[2] * (ny + 1) + cy[1]) * nz + k] - Hy[(cx[0] * (ny + 1) + cy[1]) * nz + k]), P.dx, P.rdx, P.f.rdx);
-            const R dHxdy = qdivR((Hx[(cx[2] * ny + cy[1]) * nz + k] - Hx[(cx[2] * ny + cy[0]) * nz + k]), P.dy, P.rdy, P.f.rdy);
-            curl = dHydx - dHxdy;
-        }
+    if (!g.bnd) {
+        const R curl = yee_curl<C>(P, L);
         R Jf = R(0.), dP = R(0.), er = R(0.), cond = R(0.), pc = R(0.);
         // dP/dt of the four cells, loaded before their ids are known
         R qv[4] = {R(0.), R(0.), R(0.), R(0.)};
@@ -156,7 +216,7 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
         }
         R coef;
         if (P.em_cls) {
-            const EmCls<R>& kc = cls[io.ecls[C][e]];
+            const EmCls<R>& kc = cls[L.t1];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 if (P.em_fromP && ((kc.mask >> q) & 1u)) dP = dP + qv[q] * dt_r;
@@ -207,71 +267,77 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
             for (int q = 0; q < 4; q++) Ji = Ji + ishe_cell(P, io, C, cx[q], cy[q], cz[q]);
             rhs = rhs - Ji / R(4.);
         }
-        rhs = rhs - cond * io.E_in.c[C][e] - qdivR(dP, P.dt, P.rdt, P.f.rdt);
+        rhs = rhs - cond * L.self - qdivR(dP, P.dt, P.rdt, P.f.rdt);
         d = coef * rhs;
     }
-    rk_x<S>(io.E_x.c[C][e], d, io.E_out.c[C], io.E_acc.c[C], io.E_cmp.c[C], e);
+    rk_x<S>(L, d, io.E_out.c[C], io.E_acc.c[C], io.E_cmp.c[C], e);
 }
 
-// H face update of component C at face (i,j,k) (index e in C's array).
+// Gather of an H face: curl operands, step value, accumulators, and the
+// ids and dm of the two cells either side of the face.
 template <int S, int C, class R>
-__device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const EmMat<R>* mt, int i, int j, int k, int e) {
+__device__ inline void face_load(const Params& P, const StageIOT<R>& io, int i, int j, int k, int e, YeeIn<R>& L) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    R mdt_mu0_r;
-    if constexpr (is_mixed<R>::value) mdt_mu0_r = P.f.mdt_mu0; else mdt_mu0_r = P.mdt_mu0;
     const R* Ex = io.E_in.c[0];
     const R* Ey = io.E_in.c[1];
     const R* Ez = io.E_in.c[2];
-    R curl;
+    L.x = io.H_x.c[C][e];
+    rk_loads<S>(io.H_acc.c[C], io.H_cmp.c[C], e, L);
     int a1x = i, a1y = j, a1z = k, a2x = i, a2y = j, a2z = k;
     if (C == 0) {
-        const R dEzdy = qdivR((Ez[(i * (ny + 1) + j + 1) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dy, P.rdy, P.f.rdy);
-        const R dEydz = qdivR((Ey[(i * ny + j) * (nz + 1) + k + 1] - Ey[(i * ny + j) * (nz + 1) + k]), P.dz, P.rdz, P.f.rdz);
-        curl = dEzdy - dEydz;
+        L.c[0] = Ez[(i * (ny + 1) + j + 1) * nz + k]; L.c[1] = Ez[(i * (ny + 1) + j) * nz + k];
+        L.c[2] = Ey[(i * ny + j) * (nz + 1) + k + 1]; L.c[3] = Ey[(i * ny + j) * (nz + 1) + k];
         a1x = (i == 0) ? (P.per_x ? nx - 1 : 0) : i - 1;
         a2x = (i == nx) ? (P.per_x ? 0 : nx - 1) : i;
     } else if (C == 1) {
-        const R dExdz = qdivR((Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dz, P.rdz, P.f.rdz);
-        const R dEzdx = qdivR((Ez[((i + 1) * (ny + 1) + j) * nz + k] - Ez[(i * (ny + 1) + j) * nz + k]), P.dx, P.rdx, P.f.rdx);
-        curl = dExdz - dEzdx;
+        L.c[0] = Ex[(i * (ny + 1) + j) * (nz + 1) + k + 1]; L.c[1] = Ex[(i * (ny + 1) + j) * (nz + 1) + k];
+        L.c[2] = Ez[((i + 1) * (ny + 1) + j) * nz + k]; L.c[3] = Ez[(i * (ny + 1) + j) * nz + k];
         a1y = (j == 0) ? (P.per_y ? ny - 1 : 0) : j - 1;
         a2y = (j == ny) ? (P.per_y ? 0 : ny - 1) : j;
     } else {
-        const R dEydx = qdivR((Ey[((i + 1) * ny + j) * (nz + 1) + k] - Ey[(i * ny + j) * (nz + 1) + k]), P.dx, P.rdx, P.f.rdx);
-        const R dExdy = qdivR((Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k] - Ex[(i * (ny + 1) + j) * (nz + 1) + k]), P.dy, P.rdy, P.f.rdy);
-        curl = dEydx - dExdy;
+        L.c[0] = Ey[((i + 1) * ny + j) * (nz + 1) + k]; L.c[1] = Ey[(i * ny + j) * (nz + 1) + k];
+        L.c[2] = Ex[(i * (ny + 1) + j + 1) * (nz + 1) + k]; L.c[3] = Ex[(i * (ny + 1) + j) * (nz + 1) + k];
         a1z = (k == 0) ? (P.per_z ? nz - 1 : 0) : k - 1;
         a2z = (k == nz) ? (P.per_z ? 0 : nz - 1) : k;
     }
+    L.c1 = (a1x * ny + a1y) * nz + a1z;
+    L.c2 = (a2x * ny + a2y) * nz + a2z;
+    L.dm1 = P.em_fromM ? io.dm.c[C][L.c1] : R(0.);
+    L.dm2 = P.em_fromM ? io.dm.c[C][L.c2] : R(0.);
+    L.t1 = io.mid[L.c1];
+    L.t2 = io.mid[L.c2];
+}
+
+// H face update of component C (index e in C's array), from the gathered
+// values L.
+template <int S, int C, class R>
+__device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const EmMat<R>* mt, const YeeIn<R>& L, int e) {
+    R mdt_mu0_r;
+    if constexpr (is_mixed<R>::value) mdt_mu0_r = P.f.mdt_mu0; else mdt_mu0_r = P.mdt_mu0;
+    const R curl = yee_curl<C>(P, L);
     R dM1 = R(0.), dM2 = R(0.), cnt = R(0.);
-    {
-        const int c1 = (a1x * ny + a1y) * nz + a1z, c2 = (a2x * ny + a2y) * nz + a2z;
-        // dm of both face cells, loaded before their ids are known
-        const R dm1 = P.em_fromM ? io.dm.c[C][c1] : R(0.), dm2 = P.em_fromM ? io.dm.c[C][c2] : R(0.);
-        const uint8_t i1 = io.mid[c1], i2 = io.mid[c2];
-        // Ms dm + Ms1 dm1 + Ms2 dm2 of each face cell (EMdynamic_solver.cpp:2300-2306)
-        if (i1 != 0) {
-            const EmMat<R>& m = mt[i1 - 1];
-            if (P.em_fromM) {
-                dM1 = dm1 * m.Ms;
-                if (P.afm) dM1 = dM1 + io.da1.c[C][c1] * m.Ms1 + io.da2.c[C][c1] * m.Ms2;
-            }
-            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
+    // Ms dm + Ms1 dm1 + Ms2 dm2 of each face cell (EMdynamic_solver.cpp:2300-2306)
+    if (L.t1 != 0) {
+        const EmMat<R>& m = mt[L.t1 - 1];
+        if (P.em_fromM) {
+            dM1 = L.dm1 * m.Ms;
+            if (P.afm) dM1 = dM1 + io.da1.c[C][L.c1] * m.Ms1 + io.da2.c[C][L.c1] * m.Ms2;
         }
-        if (i2 != 0) {
-            const EmMat<R>& m = mt[i2 - 1];
-            if (P.em_fromM) {
-                dM2 = dm2 * m.Ms;
-                if (P.afm) dM2 = dM2 + io.da1.c[C][c2] * m.Ms1 + io.da2.c[C][c2] * m.Ms2;
-            }
-            if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
+        if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
+    }
+    if (L.t2 != 0) {
+        const EmMat<R>& m = mt[L.t2 - 1];
+        if (P.em_fromM) {
+            dM2 = L.dm2 * m.Ms;
+            if (P.afm) dM2 = dM2 + io.da1.c[C][L.c2] * m.Ms1 + io.da2.c[C][L.c2] * m.Ms2;
         }
+        if (m.flags & (MF_FM | MF_AFM)) cnt = cnt + R(1.);
     }
     if (cnt < R(0.5)) cnt = R(1.);
     // -dt/mu0 rounded once on the host; cnt is 1 or 2, so the division is exact
     const R dMs = dM1 + dM2;
     const R d = mdt_mu0_r * curl - (cnt == R(2.) ? dMs * R(0.5) : dMs);
-    rk_x<S>(io.H_x.c[C][e], d, io.H_out.c[C], io.H_acc.c[C], io.H_cmp.c[C], e);
+    rk_x<S>(L, d, io.H_out.c[C], io.H_acc.c[C], io.H_cmp.c[C], e);
 }
 
 // All six Yee components of one stage: thread (i,j,k) on the vertex grid
@@ -280,13 +346,19 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
 // H only the stage E and dm, so the six updates are independent.  The grid
 // is (blocks over the (j,k) vertex plane) x (nx+1 planes); the material
 // constants are staged in shared memory.
+// Blocks per SM of the launch bound: room for the gathered operands of three
+// components without spills (FP64: 80 registers, 24 warps per SM; FP32: 64
+// registers, 32 warps).  Measured on the 128x128x96 magnetoelastic film
+// against 8, 6, 5, 4, 3 and 2: FP64 (3) 0.365 ms per step vs 0.43-0.76, FP32
+// (4) 0.253 ms vs 0.26-0.34.
 #ifndef GF_EM_MINB_F32
-#define GF_EM_MINB_F32 8
+#define GF_EM_MINB_F32 4
+#endif
+#ifndef GF_EM_MINB_F64
+#define GF_EM_MINB_F64 3
 #endif
 template <int S, class R = double>
-// (256, 8): 32 registers, 64 resident warps per SM; the kernel is bound by
-// the latency of its neighbour loads, and full occupancy beats the spills
-__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) k_em_fused(Params P, StageIOT<R> io, int nmat,
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : GF_EM_MINB_F64) k_em_fused(Params P, StageIOT<R> io, int nmat,
                                                                                       const EmCls<R>* __restrict__ cls_g, int ncls) {
     __shared__ EmMat<R> mt[kMaxMat];
     __shared__ EmCls<R> cl[kEmMaxCls];
@@ -302,12 +374,31 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : 8) 
     const int i = blockIdx.y;
     const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
     const StageDrive& dr = stage_drive(io, S);
-    if (i < nx) em_E_edge<S, 0, R>(P, io, dr, mt, cl, i, j, k, (i * (ny + 1) + j) * (nz + 1) + k);
-    if (j < ny) em_E_edge<S, 1, R>(P, io, dr, mt, cl, i, j, k, (i * ny + j) * (nz + 1) + k);
-    if (k < nz) em_E_edge<S, 2, R>(P, io, dr, mt, cl, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (j < ny && k < nz) em_H_face<S, 0, R>(P, io, mt, i, j, k, (i * ny + j) * nz + k);
-    if (i < nx && k < nz) em_H_face<S, 1, R>(P, io, mt, i, j, k, (i * (ny + 1) + j) * nz + k);
-    if (i < nx && j < ny) em_H_face<S, 2, R>(P, io, mt, i, j, k, (i * ny + j) * (nz + 1) + k);
+    // E edges: gather all three, then update (the stores follow every load)
+    {
+        const bool on0 = i < nx, on1 = j < ny, on2 = k < nz;
+        const int e0 = (i * (ny + 1) + j) * (nz + 1) + k, e1 = (i * ny + j) * (nz + 1) + k, e2 = (i * (ny + 1) + j) * nz + k;
+        const EdgeGeom g0 = edge_geom<0>(P, i, j, k), g1 = edge_geom<1>(P, i, j, k), g2 = edge_geom<2>(P, i, j, k);
+        YeeIn<R> L0, L1, L2;
+        if (on0) edge_load<S, 0, R>(P, io, g0, i, j, k, e0, L0);
+        if (on1) edge_load<S, 1, R>(P, io, g1, i, j, k, e1, L1);
+        if (on2) edge_load<S, 2, R>(P, io, g2, i, j, k, e2, L2);
+        if (on0) em_E_edge<S, 0, R>(P, io, dr, mt, cl, g0, L0, e0);
+        if (on1) em_E_edge<S, 1, R>(P, io, dr, mt, cl, g1, L1, e1);
+        if (on2) em_E_edge<S, 2, R>(P, io, dr, mt, cl, g2, L2, e2);
+    }
+    // H faces, the same way
+    {
+        const bool on0 = j < ny && k < nz, on1 = i < nx && k < nz, on2 = i < nx && j < ny;
+        const int e0 = (i * ny + j) * nz + k, e1 = (i * (ny + 1) + j) * nz + k, e2 = (i * ny + j) * (nz + 1) + k;
+        YeeIn<R> L0, L1, L2;
+        if (on0) face_load<S, 0, R>(P, io, i, j, k, e0, L0);
+        if (on1) face_load<S, 1, R>(P, io, i, j, k, e1, L1);
+        if (on2) face_load<S, 2, R>(P, io, i, j, k, e2, L2);
+        if (on0) em_H_face<S, 0, R>(P, io, mt, L0, e0);
+        if (on1) em_H_face<S, 1, R>(P, io, mt, L1, e1);
+        if (on2) em_H_face<S, 2, R>(P, io, mt, L2, e2);
+    }
 }
 
 // Drude polarisation current, per cell: dJp_n = (e0 wp_n^2 E_cell c_n -
