@@ -115,6 +115,23 @@ __device__ __forceinline__ void rk_mixed(float xv, float d, float* out, float* a
     }
 }
 
+// rk_mixed with the accumulator (stages 1..3) and compensation (last stage)
+// already loaded into av and cv, so that a kernel can issue the loads of
+// several scalars before the first of their stores
+template <int S>
+__device__ __forceinline__ void rk_mixed_v(float xv, float av, float cv, float d, float* out, float* acc, float* cmp,
+                                           int e) {
+    if (S == 0) { out[e] = xv + d * 0.5f; acc[e] = d * (1.f / 6.f); }
+    else if (S == 1) { out[e] = xv + d * 0.5f; acc[e] = av + d * (1.f / 3.f); }
+    else if (S == 2) { out[e] = xv + d; acc[e] = av + d * (1.f / 3.f); }
+    else {
+        float sum, err;
+        two_sum(xv, (av + d * (1.f / 6.f)) + cv, sum, err);
+        acc[e] = sum;
+        cmp[e] = err;
+    }
+}
+
 // |m| = 1 for a stage state (FP32)
 __device__ __forceinline__ void renorm3(float& x, float& y, float& z) {
     const float inv = 1.f / sqrtf(x * x + y * y + z * z);
