@@ -56,10 +56,19 @@ struct LLGMat {
 // hold their initial m in all four buffers and are never touched.  Grid:
 // (blocks over the box's (j,k) plane) x (box planes in i).  R = float is the
 // mixed form: FP32 stencil, compensated step value, |m| = 1 after every stage.
+#ifndef GF_LLG_MINB_F32
+#define GF_LLG_MINB_F32 4
+#endif
+#ifndef GF_LLG_MINB_F64
+#define GF_LLG_MINB_F64 4
+#endif
 template <int S, class R = double>
 // (256, 4): 64 registers, 32 resident warps per SM for its neighbour-load
 // latency; measured faster than 98 registers at 16 warps despite a few spills
-__global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, const LLGTablesT<R>* __restrict__ tab, int nmat) {
+// (with the RK operands gathered before the first store, on the 128x128x96
+// magnetoelastic film: FP64 0.225 ms per step at 4 blocks, 0.238 at 3, 0.285
+// at 2; FP32 0.145 at 4)
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_LLG_MINB_F32 : GF_LLG_MINB_F64) k_llg_fm(Params P, StageIOT<R> io, const LLGTablesT<R>* __restrict__ tab, int nmat) {
     __shared__ LLGMat<R> mt[kMaxMat];
     __shared__ R sA[kMaxMat + 1][kMaxMat + 1];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
@@ -217,6 +226,15 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
         dmy = precess * py + mat.alpha_precess * qy;
         dmz = precess * pz + mat.alpha_precess * qz;
     }
+    // RK operands of the three components, loaded before the first store
+    R mx0[3], ma[3], mcm[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        mx0[a] = io.m_x.c[a][c];
+        ma[a] = (S > 0) ? io.m_acc.c[a][c] : R(0.);
+        mcm[a] = R(0.);
+        if constexpr (is_mixed<R>::value) { if (S == 3) mcm[a] = io.m_cmp.c[a][c]; }
+    }
     if (P.em_fromM || P.spin) { io.dm.c[0][c] = dmx; io.dm.c[1][c] = dmy; io.dm.c[2][c] = dmz; }
 
     if constexpr (is_mixed<R>::value) {
@@ -228,8 +246,8 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
             float o[3];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                o[a] = io.m_x.c[a][c] + d[a] * cf;
-                io.m_acc.c[a][c] = (S == 0) ? d[a] * (1.f / 6.f) : io.m_acc.c[a][c] + d[a] * (1.f / 3.f);
+                o[a] = mx0[a] + d[a] * cf;
+                io.m_acc.c[a][c] = (S == 0) ? d[a] * (1.f / 6.f) : ma[a] + d[a] * (1.f / 3.f);
             }
             if (fm_cell) renorm3(o[0], o[1], o[2]);
 #pragma unroll
@@ -238,7 +256,7 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
             float x[3], cm[3];
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                two_sum(io.m_x.c[a][c], (io.m_acc.c[a][c] + d[a] * (1.f / 6.f)) + io.m_cmp.c[a][c], x[a], cm[a]);
+                two_sum(mx0[a], (ma[a] + d[a] * (1.f / 6.f)) + mcm[a], x[a], cm[a]);
             if (fm_cell) renorm_pair(x, cm);
 #pragma unroll
             for (int a = 0; a < 3; a++) { io.m_acc.c[a][c] = x[a]; io.m_cmp.c[a][c] = cm[a]; }
@@ -247,12 +265,13 @@ __global__ void __launch_bounds__(256, 4) k_llg_fm(Params P, StageIOT<R> io, con
         // ---- RK4 combination; the magnetic increment is summed before it is
         //      added to m (magnetic_solver.cpp:1453-1455, 1601-1603) ----
         const double d[3] = {dmx, dmy, dmz};
+#pragma unroll
         for (int a = 0; a < 3; a++) {
-            const double xv = io.m_x.c[a][c];
+            const double xv = mx0[a];
             if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
-            else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
-            else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = io.m_acc.c[a][c] + qdiv(d[a], 3., kInv3); }
-            else { io.m_acc.c[a][c] = xv + (io.m_acc.c[a][c] + qdiv(d[a], 6., kInv6)); }
+            else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
+            else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
+            else { io.m_acc.c[a][c] = xv + (ma[a] + qdiv(d[a], 6., kInv6)); }
         }
     }
 }
@@ -404,6 +423,17 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
             dm[s][2] = mat.prec[s] * pz + mat.aprec[s] * qz;
         }
     }
+    // RK operands of both sublattices, loaded before the first store
+    R sx[2][3], sa[2][3], sc[2][3];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            sx[s][a] = (s ? io.a2_x : io.a1_x).c[a][c];
+            sa[s][a] = (S > 0) ? (s ? io.a2_acc : io.a1_acc).c[a][c] : R(0.);
+            sc[s][a] = R(0.);
+            if constexpr (is_mixed<R>::value) { if (S == 3) sc[s][a] = (s ? io.a2_cmp : io.a1_cmp).c[a][c]; }
+        }
     if (P.em_fromM || P.spin) {
 #pragma unroll
         for (int a = 0; a < 3; a++) { io.da1.c[a][c] = dm[0][a]; io.da2.c[a][c] = dm[1][a]; }
@@ -413,7 +443,6 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
         // mixed form: compensated RK4 of both sublattices, then |m_s| = 1
 #pragma unroll
         for (int s = 0; s < 2; s++) {
-            const F3T<R>& X = s ? io.a2_x : io.a1_x;
             const F3T<R>& O = s ? io.a2_out : io.a1_out;
             const F3T<R>& A = s ? io.a2_acc : io.a1_acc;
             const F3T<R>& Cm = s ? io.a2_cmp : io.a1_cmp;
@@ -422,8 +451,8 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
                 float o[3];
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    o[a] = X.c[a][c] + dm[s][a] * cf;
-                    A.c[a][c] = (S == 0) ? dm[s][a] * (1.f / 6.f) : A.c[a][c] + dm[s][a] * (1.f / 3.f);
+                    o[a] = sx[s][a] + dm[s][a] * cf;
+                    A.c[a][c] = (S == 0) ? dm[s][a] * (1.f / 6.f) : sa[s][a] + dm[s][a] * (1.f / 3.f);
                 }
                 if (afm_cell) renorm3(o[0], o[1], o[2]);
 #pragma unroll
@@ -432,7 +461,7 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
                 float x[3], cm[3];
 #pragma unroll
                 for (int a = 0; a < 3; a++)
-                    two_sum(X.c[a][c], (A.c[a][c] + dm[s][a] * (1.f / 6.f)) + Cm.c[a][c], x[a], cm[a]);
+                    two_sum(sx[s][a], (sa[s][a] + dm[s][a] * (1.f / 6.f)) + sc[s][a], x[a], cm[a]);
                 if (afm_cell) renorm_pair(x, cm);
 #pragma unroll
                 for (int a = 0; a < 3; a++) { A.c[a][c] = x[a]; Cm.c[a][c] = cm[a]; }
@@ -443,17 +472,16 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
         // (get_dm_AFM / update_m_AFM, magnetic_AFM_solver.cpp:1715-1835)
 #pragma unroll
         for (int s = 0; s < 2; s++) {
-            const F3& X = s ? io.a2_x : io.a1_x;
             const F3& O = s ? io.a2_out : io.a1_out;
             const F3& A = s ? io.a2_acc : io.a1_acc;
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 const double d = dm[s][a];
-                const double xv = X.c[a][c];
+                const double xv = sx[s][a];
                 if (S == 0) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = qdiv(d, 6., kInv6); }
-                else if (S == 1) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
-                else if (S == 2) { O.c[a][c] = xv + d; A.c[a][c] = A.c[a][c] + qdiv(d, 3., kInv3); }
-                else { A.c[a][c] = xv + (A.c[a][c] + qdiv(d, 6., kInv6)); }
+                else if (S == 1) { O.c[a][c] = xv + d * 0.5; A.c[a][c] = sa[s][a] + qdiv(d, 3., kInv3); }
+                else if (S == 2) { O.c[a][c] = xv + d; A.c[a][c] = sa[s][a] + qdiv(d, 3., kInv3); }
+                else { A.c[a][c] = xv + (sa[s][a] + qdiv(d, 6., kInv6)); }
             }
         }
     }
