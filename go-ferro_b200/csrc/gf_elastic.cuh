@@ -314,40 +314,6 @@ __device__ inline void side_rows(const V& v, const M& m, R ga, R gb, R gc, R out
     for (int r = 0; r < 3; r++) out[r] = stress_row<CUB>(m, st, face_row(D, r));
 }
 
-// RK4 combination for v and u of one cell (du = v_stage * dt)
-template <int S, class R>
-__device__ inline void rk_vu(const StageIOT<R>& io, long c, const R dv[3], double dt, float dtf) {
-    if constexpr (is_mixed<R>::value) {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const float du = io.v_in.c[a][c] * dtf;
-            rk_mixed<S>(io.v_x.c[a][c], dv[a], io.v_out.c[a], io.v_acc.c[a], io.v_cmp.c[a], (int)c);
-            rk_mixed<S>(io.u_x.c[a][c], du, io.u_out.c[a], io.u_acc.c[a], io.u_cmp.c[a], (int)c);
-        }
-    } else {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const double du = io.v_in.c[a][c] * dt;
-            if (S == 0) {
-                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-                io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = vx + qdiv(dv[a], 6., kInv6);
-                io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = ux + qdiv(du, 6., kInv6);
-            } else if (S == 1) {
-                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-                io.v_out.c[a][c] = vx + dv[a] * 0.5; io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
-                io.u_out.c[a][c] = ux + du * 0.5;    io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
-            } else if (S == 2) {
-                const double vx = io.v_x.c[a][c], ux = io.u_x.c[a][c];
-                io.v_out.c[a][c] = vx + dv[a];       io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 3., kInv3);
-                io.u_out.c[a][c] = ux + du;          io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 3., kInv3);
-            } else {
-                io.v_acc.c[a][c] = io.v_acc.c[a][c] + qdiv(dv[a], 6., kInv6);
-                io.u_acc.c[a][c] = io.u_acc.c[a][c] + qdiv(du, 6., kInv6);
-            }
-        }
-    }
-}
-
 // Shared-memory plan of k_elastic_tile: every array sits at a compile-time
 // offset from the dynamic base; the material table (sized at launch) is last.
 template <class R>
@@ -734,27 +700,52 @@ __global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
         if (c1 < P.n) b.load(io, c1);
         if (c0 < P.n) a.update(io, c0, P.f.dt);
         if (c1 < P.n) b.update(io, c1, P.f.dt);
-        return;
-    }
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    const uint8_t id = io.mid[c];
-    R dv[3] = {R(0.), R(0.), R(0.)};
-    if (id != 0) {
-        const DevMatT<R>& mt = io.mats[id - 1];
-        const R dens_dt = mt.dens_dt, mass_damp = mt.mass_damp, stiff_damp = mt.stiff_damp;
+    } else {
+        // FP64: every operand of the three components is loaded before the first
+        // store (as RkCellF32 does for two cells), so a thread's ~20 loads are in
+        // flight together
+        const int c = blockIdx.x * blockDim.x + threadIdx.x;
+        if (c >= P.n) return;
+        const uint8_t id = io.mid[c];
+        double f[3], fs[3], vx[3], vin[3], ux[3], va[3], ua[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            const R f = io.force.c[a][c];
-            const R fs = io.force_store.c[a][c];
-            if (S == 1 || S == 2)
-                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs) * R(2.);
-            else
-                dv[a] = f * dens_dt + mass_damp * io.v_x.c[a][c] + stiff_damp * (f - fs);
-            if (S == 0) io.force_store.c[a][c] = f;
+            f[a] = io.force.c[a][c]; fs[a] = io.force_store.c[a][c];
+            vx[a] = io.v_x.c[a][c]; vin[a] = io.v_in.c[a][c]; ux[a] = io.u_x.c[a][c];
+            va[a] = (S > 0) ? io.v_acc.c[a][c] : 0.;
+            ua[a] = (S > 0) ? io.u_acc.c[a][c] : 0.;
+        }
+        double dv[3] = {0., 0., 0.};
+        if (id != 0) {
+            const DevMatT<R>& mt = io.mats[id - 1];
+            const double dens_dt = mt.dens_dt, mass_damp = mt.mass_damp, stiff_damp = mt.stiff_damp;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (S == 1 || S == 2)
+                    dv[a] = f[a] * dens_dt + mass_damp * vx[a] + stiff_damp * (f[a] - fs[a]) * 2.;
+                else
+                    dv[a] = f[a] * dens_dt + mass_damp * vx[a] + stiff_damp * (f[a] - fs[a]);
+                if (S == 0) io.force_store.c[a][c] = f[a];
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const double du = vin[a] * P.dt;
+            if (S == 0) {
+                io.v_out.c[a][c] = vx[a] + dv[a] * 0.5; io.v_acc.c[a][c] = vx[a] + qdiv(dv[a], 6., kInv6);
+                io.u_out.c[a][c] = ux[a] + du * 0.5;    io.u_acc.c[a][c] = ux[a] + qdiv(du, 6., kInv6);
+            } else if (S == 1) {
+                io.v_out.c[a][c] = vx[a] + dv[a] * 0.5; io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 3., kInv3);
+                io.u_out.c[a][c] = ux[a] + du * 0.5;    io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
+            } else if (S == 2) {
+                io.v_out.c[a][c] = vx[a] + dv[a];       io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 3., kInv3);
+                io.u_out.c[a][c] = ux[a] + du;          io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
+            } else {
+                io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 6., kInv6);
+                io.u_acc.c[a][c] = ua[a] + qdiv(du, 6., kInv6);
+            }
         }
     }
-    rk_vu<S>(io, c, dv, P.dt, P.f.dt);
 }
 
 // cell strain (global frame) of the current step for output (Dexx_glb ...)
@@ -789,22 +780,36 @@ __global__ void k_elastic_bc(Params P, StageIOT<R> io) {
         // k=1..4 of u at the start of step h (mod 4).
         const R w = P.liao_w;
         const R c1 = R(4.) * w + R(2.) * (R(1.) - w), c2 = R(6.) * w + (R(1.) - w), c3 = R(4.) * w;
+        // every load of a stage is issued before its first store
         if (S < 3) {
             // stages 1-3 rewrite u(k=0) with the value of the last full update
-            for (int a = 0; a < 3; a++)
-                io.u_x.c[a][cid(P, i, j, 0)] = io.liao_last[a * plane + t];
+            R last[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) last[a] = io.liao_last[a * plane + t];
+#pragma unroll
+            for (int a = 0; a < 3; a++) io.u_x.c[a][cid(P, i, j, 0)] = last[a];
         } else {
-            // shift history: slot (step mod 4) <- planes 1..4 of the step-start u
+            // shift history: slot (step mod 4) <- planes 1..4 of the step-start u;
+            // the extrapolation reads that slot as t1 = u(step), i.e. the
+            // values just loaded, and three older slots
             R* slot = io.liao_hist + (size_t)(step & 3ull) * 12 * plane;
-            for (int a = 0; a < 3; a++)
-                for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = io.u_x.c[a][cid(P, i, j, p)];
-            const R* h1 = io.liao_hist + (size_t)((step + 0) & 3ull) * 12 * plane;   // t1 = u(step)
             const R* h2 = io.liao_hist + (size_t)((step + 3) & 3ull) * 12 * plane;   // t2 = u(step-1)
             const R* h3 = io.liao_hist + (size_t)((step + 2) & 3ull) * 12 * plane;   // t3 = u(step-2)
             const R* h4 = io.liao_hist + (size_t)((step + 1) & 3ull) * 12 * plane;   // t4 = u(step-3)
+            R uv[3][4], t2[3], t3[3], t4[3];
+#pragma unroll
             for (int a = 0; a < 3; a++) {
-                const R v = c1 * h1[(a * 4 + 0) * plane + t] - c2 * h2[(a * 4 + 1) * plane + t]
-                                 + c3 * h3[(a * 4 + 2) * plane + t] - w * h4[(a * 4 + 3) * plane + t];
+#pragma unroll
+                for (int p = 1; p <= 4; p++) uv[a][p - 1] = io.u_x.c[a][cid(P, i, j, p)];
+                t2[a] = h2[(a * 4 + 1) * plane + t];
+                t3[a] = h3[(a * 4 + 2) * plane + t];
+                t4[a] = h4[(a * 4 + 3) * plane + t];
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+#pragma unroll
+                for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = uv[a][p - 1];
+                const R v = c1 * uv[a][0] - c2 * t2[a] + c3 * t3[a] - w * t4[a];
                 io.u_acc.c[a][cid(P, i, j, 0)] = v;
                 io.liao_last[a * plane + t] = v;
                 if constexpr (is_mixed<R>::value) io.u_cmp.c[a][cid(P, i, j, 0)] = R(0);

@@ -564,8 +564,12 @@ __global__ void k_em_mur(Params P, StageIOT<R> io) {
         const R* X = io.E_x.c[comp];
         R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_xy) {
-            O[e0] = X[e1] + cfx * (X[e0] - O[e1]);
-            O[eN] = X[eN1] + cfx * (X[eN] - O[eN1]);
+            // both faces' operands before the first store; with one cell
+            // across, eN1 is e0 and the second update reads the first's result
+            const R x1 = X[e1], x0 = X[e0], o1 = O[e1], xN1 = X[eN1], xN = X[eN];
+            const R oN1 = (nx > 1) ? O[eN1] : R(0.);
+            O[e0] = x1 + cfx * (x0 - o1);
+            O[eN] = xN1 + cfx * (xN - ((nx > 1) ? oN1 : O[eN1]));
         } else { O[e0] = R(0.); O[eN] = R(0.); }
         if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     } else if (F == 1) {
@@ -588,8 +592,12 @@ __global__ void k_em_mur(Params P, StageIOT<R> io) {
         const R* X = io.E_x.c[comp];
         R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_xy) {
-            O[e0] = X[e1] + cfy * (X[e0] - O[e1]);
-            O[eN] = X[eN1] + cfy * (X[eN] - O[eN1]);
+            // both faces' operands before the first store; with one cell
+            // across, eN1 is e0 and the second update reads the first's result
+            const R x1 = X[e1], x0 = X[e0], o1 = O[e1], xN1 = X[eN1], xN = X[eN];
+            const R oN1 = (ny > 1) ? O[eN1] : R(0.);
+            O[e0] = x1 + cfy * (x0 - o1);
+            O[eN] = xN1 + cfy * (xN - ((ny > 1) ? oN1 : O[eN1]));
         } else { O[e0] = R(0.); O[eN] = R(0.); }
         if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     } else {
@@ -606,8 +614,12 @@ __global__ void k_em_mur(Params P, StageIOT<R> io) {
         const R* X = io.E_x.c[comp];
         R* O = (S < 3) ? io.E_out.c[comp] : io.E_acc.c[comp];
         if (!P.pec_z) {
-            O[eN] = X[eN1] + ctop * (X[eN] - O[eN1]);
-            if (!P.abc_1D || !P.abc_em_onlytop) O[e0] = X[e1] + cbot * (X[e0] - O[e1]);
+            // both faces' operands before the first store; with one cell
+            // across, e1 is eN and the bottom update reads the top's result
+            const R xN1 = X[eN1], xN = X[eN], oN1 = O[eN1], x1 = X[e1], x0 = X[e0];
+            const R o1 = (nz > 1) ? O[e1] : R(0.);
+            O[eN] = xN1 + ctop * (xN - oN1);
+            if (!P.abc_1D || !P.abc_em_onlytop) O[e0] = x1 + cbot * (x0 - ((nz > 1) ? o1 : O[e1]));
             else O[e0] = R(0.);
         } else { O[e0] = R(0.); O[eN] = R(0.); }
         if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
