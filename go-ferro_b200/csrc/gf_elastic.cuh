@@ -820,19 +820,28 @@ __global__ void k_elastic_bc(Params P, StageIOT<R> io) {
         const double* cf = (S == 0 || S == 1) ? P.mur_el_half : P.mur_el_full;
         const R cl1 = cf[0], ct1 = cf[1], cll = cf[2], ctl = cf[3];
         const long b0 = cid(P, i, j, 0), b1 = cid(P, i, j, 1), t0 = cid(P, i, j, nz - 1), t1 = cid(P, i, j, nz - 2);
+        // the three components' operands are loaded before the first store;
+        // with nz <= 2, t1 is b0 and the top update reads the bottom's result
+        // (the stage target is u_out for stages 1-3 and the new step value
+        // u_acc for the last; the source is the step-start u)
+        const bool sep = nz > 2;
+        R xb0[3], xb1[3], xt0[3], xt1[3], sb1[3], st1[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const R* x = io.u_x.c[a];
+            const R* so = (S < 3) ? io.u_out.c[a] : io.u_acc.c[a];
+            xb0[a] = x[b0]; xb1[a] = x[b1]; xt0[a] = x[t0]; xt1[a] = x[t1];
+            sb1[a] = so[b1];
+            st1[a] = sep ? so[t1] : R(0.);
+        }
+#pragma unroll
         for (int a = 0; a < 3; a++) {
             const R c1st = (a == 2) ? cl1 : ct1, clast = (a == 2) ? cll : ctl;
-            if (S < 3) {
-                R* so = io.u_out.c[a];
-                const R* x = io.u_x.c[a];
-                if (!P.abc_elast_onlytop) so[b0] = x[b1] + c1st * (x[b0] - so[b1]);
-                so[t0] = x[t1] + clast * (x[t0] - so[t1]);
-            } else {
-                R* nw = io.u_acc.c[a];
-                const R* old = io.u_x.c[a];
-                if (!P.abc_elast_onlytop) nw[b0] = old[b1] + c1st * (old[b0] - nw[b1]);
-                nw[t0] = old[t1] + clast * (old[t0] - nw[t1]);
-                if constexpr (is_mixed<R>::value) {
+            R* so = (S < 3) ? io.u_out.c[a] : io.u_acc.c[a];
+            if (!P.abc_elast_onlytop) so[b0] = xb1[a] + c1st * (xb0[a] - sb1[a]);
+            so[t0] = xt1[a] + clast * (xt0[a] - (sep ? st1[a] : so[t1]));
+            if constexpr (is_mixed<R>::value) {
+                if (S == 3) {
                     if (!P.abc_elast_onlytop) io.u_cmp.c[a][b0] = R(0);
                     io.u_cmp.c[a][t0] = R(0);
                 }

@@ -353,6 +353,7 @@ std::string unsupported(const Deck& d) {
     }
     if (d.elastodynamics) {
         if (d.nz < 5 && !d.abc_1D) return "the Liao boundary needs nz >= 5";
+        if (d.nz < 2 && d.abc_1D) return "the elastic Mur boundary needs nz >= 2";
         if (d.strain_pulse && d.strain_z >= (unsigned)d.nz) return "input_strain_sourcez outside the grid";
         // the +z neighbour of get_dv_RK* is read out of the column when the
         // top face is not stress-free and nz-1 != ny-1 (elastic_dynamic_solver.cpp:1247)
