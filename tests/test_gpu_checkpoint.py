@@ -55,3 +55,15 @@ def test_checkpoint_rejects_other_grids(gf, tmp_path):
     with gf.Engine(str(tmp_path / "a"), device=0, precision="mixed") as c:
         with pytest.raises(gf.GFError):
             c.load_state(ck)
+
+
+def test_elastic_mur_boundary_rejects_single_layer(gf, tmp_path):
+    """The elastic Mur boundary reads the plane below the top one, so a deck
+    with nz = 1 is refused instead of reading outside the grid."""
+    d = gf.decks.preset_ferroelectric(nx=4, ny=4, nz=1, steps=2)
+    assert d.abc_1D and d.elastic
+    gf.decks.write_deck(d, str(tmp_path))
+    with pytest.raises(gf.GFError) as ei:
+        gf.Engine(str(tmp_path), device=0)
+    assert ei.value.code == -7
+    assert "Mur boundary needs nz >= 2" in str(ei.value)
