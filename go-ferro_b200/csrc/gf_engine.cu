@@ -1502,10 +1502,11 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     }
     if (P.em) GF_TRY(setup_em_classes(eng));
     // FP64 scratch: output staging (6 cell arrays, or one widened Yee
-    // component in the mixed form) and the reduction partials
+    // component in the mixed form) and the reduction partials (device_sum3:
+    // 3 x (8192 + 64 + 1))
     const size_t yee_max = (size_t)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);
     eng->scratch_main = std::max((size_t)6 * n, yee_max);
-    GF_TRY(dalloc_n(eng, &eng->scratch, eng->scratch_main + 16384));
+    GF_TRY(dalloc_n(eng, &eng->scratch, eng->scratch_main + 32768));
     GF_TRY(dalloc_n(eng, &eng->flag, 1));
     GF_CU(cudaStreamSynchronize(eng->stream));
 
@@ -1568,22 +1569,42 @@ int advance(gf_engine* eng, uint64_t nsteps, bool use_graph) {
 // current step value of a 3-component state field
 double* const* cur(gf_engine* eng, Field3& f) { return (eng->steps_done & 1ull) ? f.A : f.X; }
 
-// deterministic FP64 sum of a device array of the run's precision; in the
-// mixed form of the values x + c when the compensation words c are given
-int device_sum(gf_engine* eng, const double* in, long n, double* out, const double* cmp = nullptr) {
+// Deterministic FP64 sums of three device arrays of the run's precision (in
+// the mixed form of the values x + c when the compensation words c are
+// given): 8192 strided partials, then 64, then 1, each sum in a fixed order;
+// one copy back and one synchronisation for the three
+int device_sum3(gf_engine* eng, double* const* in, long n, double out[3], double* const* cmp) {
     cudaStream_t st = eng->stream;
-    double* p1 = eng->scratch + eng->scratch_main;            // 8192
-    double* p2 = p1 + 8192;                                   // 64
-    double* p3 = p2 + 64;                                     // 1
-    if (eng->mixed)
-        GF_CU(launch(k_sum_stride_f32, dim3(32), dim3(256), 0, st, reinterpret_cast<const float*>(in),
-                     reinterpret_cast<const float*>(cmp), n, p1, 8192L));
-    else
-        GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, in, n, p1, 8192L));
-    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
-    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
-    GF_CU(cudaMemcpyAsync(out, p3, sizeof(double), cudaMemcpyDeviceToHost, st));
+    double* p1 = eng->scratch + eng->scratch_main;            // 3 x 8192
+    double* p2 = p1 + 3 * 8192;                               // 3 x 64
+    double* p3 = p2 + 3 * 64;                                 // 3
+    Sum3In a{};
+    a.f32 = eng->mixed ? 1 : 0;
+    for (int c = 0; c < 3; c++) { a.x[c] = in[c]; a.cm[c] = eng->mixed && cmp ? reinterpret_cast<const float*>(cmp[c]) : nullptr; }
+    GF_CU(launch(k_sum3_stride, dim3(32, 3), dim3(256), 0, st, a, n, p1, 8192L));
+    Sum3In b{};
+    for (int c = 0; c < 3; c++) b.x[c] = p1 + c * 8192;
+    GF_CU(launch(k_sum3_stride, dim3(1, 3), dim3(64), 0, st, b, 8192L, p2, 64L));
+    Sum3In d{};
+    for (int c = 0; c < 3; c++) d.x[c] = p2 + c * 64;
+    GF_CU(launch(k_sum3_stride, dim3(1, 3), dim3(1), 0, st, d, 64L, p3, 1L));
+    GF_CU(cudaMemcpyAsync(out, p3, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     GF_CU(cudaStreamSynchronize(st));
+    return GF_OK;
+}
+
+// cell-centred E and H (scratch[0..3n) and scratch[3n..6n)) of cells c0 ..
+// c0 + count - 1 of the current step value
+int em_cells(gf_engine* eng, long c0, long count) {
+    const Params& P = eng->P;
+    double* s = eng->scratch;
+    F3 Ec{{s, s + P.n, s + 2 * P.n}}, Hc{{s + 3 * P.n, s + 4 * P.n, s + 5 * P.n}};
+    if (eng->mixed)
+        GF_CU(launch(k_em_cell<float>, dim3(blocks_for(count, kThreads)), dim3(kThreads), 0, eng->stream, P,
+                     f3f(cur(eng, eng->E)), f3f(cur(eng, eng->H)), Ec, Hc, c0, count));
+    else
+        GF_CU(launch(k_em_cell<double>, dim3(blocks_for(count, kThreads)), dim3(kThreads), 0, eng->stream, P,
+                     f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc, c0, count));
     return GF_OK;
 }
 
@@ -1629,13 +1650,7 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
             writable = false;
             native = false;
             double* s = eng->scratch;
-            F3 Ec{{s, s + P.n, s + 2 * P.n}}, Hc{{s + 3 * P.n, s + 4 * P.n, s + 5 * P.n}};
-            if (eng->mixed)
-                GF_CU(launch(k_em_cell<float>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
-                             f3f(cur(eng, eng->E)), f3f(cur(eng, eng->H)), Ec, Hc));
-            else
-                GF_CU(launch(k_em_cell<double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P,
-                             f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc));
+            GF_TRY(em_cells(eng, 0, P.n));
             double* base = (field == GF_FIELD_E_CELL) ? s : s + 3 * P.n;
             for (int a = 0; a < 3; a++) { ptrs.push_back(base + a * P.n); lens.push_back(P.n); cmps.push_back(nullptr); }
             break;
@@ -1725,11 +1740,9 @@ int gf_average(gf_engine* e, int obs, double out3[3]) {
         default: break;
     }
     if (!src) { eng->err = "observable " + std::to_string(obs) + " is not present in this run"; return GF_EINVAL; }
-    for (int a = 0; a < 3; a++) {
-        double s = 0.;
-        GF_TRY(device_sum(eng, src[a], eng->P.n, &s, f->C[a]));
-        out3[a] = s / denom;
-    }
+    double s[3];
+    GF_TRY(device_sum3(eng, src, eng->P.n, s, f->C));
+    for (int a = 0; a < 3; a++) out3[a] = s[a] / denom;
     return GF_OK;
 }
 
@@ -1740,10 +1753,10 @@ int gf_probe_em(gf_engine* e, int64_t i, int64_t j, int64_t k, double e3[3], dou
     if (!eng->E.on) { eng->err = "no Maxwell fields in this run"; return GF_EINVAL; }
     if (i < 0 || j < 0 || k < 0 || i >= P.nx || j >= P.ny || k >= P.nz) { eng->err = "probe outside the grid"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
-    std::vector<double*> ptrs, cmps; std::vector<long> lens; bool w, native;
-    GF_TRY(field_ptrs(eng, GF_FIELD_E_CELL, ptrs, lens, w, cmps, native));
+    // only the probed cell is centred
     const long c = (i * P.ny + j) * P.nz + k;
-    for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&e3[a], ptrs[a] + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
+    GF_TRY(em_cells(eng, c, 1));
+    for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&e3[a], eng->scratch + a * P.n + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
     double* hb = eng->scratch + 3 * P.n;
     for (int a = 0; a < 3; a++) GF_CU(cudaMemcpyAsync(&h3[a], hb + a * P.n + c, sizeof(double), cudaMemcpyDeviceToHost, eng->stream));
     GF_CU(cudaStreamSynchronize(eng->stream));

@@ -15,8 +15,59 @@ static __global__ void k_sum_stride(const double* __restrict__ in, long n, doubl
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     double acc = 0.;
-    for (long i = t; i < n; i += T) acc = acc + in[i];
+    long i = t;
+    // in order, with the loads of eight terms issued before their additions
+    for (; i + 7 * T < n; i += 8 * T) {
+        double v[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) v[b] = in[i + b * T];
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc = acc + v[b];
+    }
+    for (; i < n; i += T) acc = acc + in[i];
     partial[t] = acc;
+}
+
+// Three arrays (component y = blockIdx.y): partial[y * T + t] = the in-order
+// sum of in_y[t], in_y[t + T], ..., exactly as k_sum_stride forms it, with
+// the loads of eight terms issued before their additions (one thread has
+// ~n / T terms, too many to wait for one at a time).  With `cm` set, each
+// term is the FP64 value x + c of an FP32 pair, as in k_sum_stride_f32.
+struct Sum3In {
+    const void* x[3];
+    const float* cm[3];
+    int f32;          // x holds floats (mixed form) rather than doubles
+};
+static __global__ void k_sum3_stride(Sum3In in, long n, double* __restrict__ partial, long T) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const int y = blockIdx.y;
+    constexpr int B = 8;
+    double acc = 0.;
+    long i = t;
+    if (in.f32) {
+        const float* x = static_cast<const float*>(in.x[y]);
+        const float* cm = in.cm[y];
+        for (; i + (B - 1) * T < n; i += B * T) {
+            double v[B];
+#pragma unroll
+            for (int b = 0; b < B; b++) v[b] = (double)x[i + b * T] + (cm ? (double)cm[i + b * T] : 0.);
+#pragma unroll
+            for (int b = 0; b < B; b++) acc = acc + v[b];
+        }
+        for (; i < n; i += T) acc = acc + ((double)x[i] + (cm ? (double)cm[i] : 0.));
+    } else {
+        const double* x = static_cast<const double*>(in.x[y]);
+        for (; i + (B - 1) * T < n; i += B * T) {
+            double v[B];
+#pragma unroll
+            for (int b = 0; b < B; b++) v[b] = x[i + b * T];
+#pragma unroll
+            for (int b = 0; b < B; b++) acc = acc + v[b];
+        }
+        for (; i < n; i += T) acc = acc + x[i];
+    }
+    partial[y * T + t] = acc;
 }
 
 // numerators for gf_check_quotients: odd i draws a random double with
@@ -67,10 +118,11 @@ static __global__ void k_check_finite(const double* __restrict__ in, long n, int
 // cell-centred E (4-edge means) and H (2-face means) of the current step
 // value, as update_DE_cell / update_DH_cell compute them
 // (EMdynamic_solver.cpp:3780-3826)
+// over the cells c0 .. c0 + count - 1
 template <class R = double>
-__global__ void k_em_cell(Params P, F3T<R> E, F3T<R> H, F3 Ec, F3 Hc) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
+__global__ void k_em_cell(Params P, F3T<R> E, F3T<R> H, F3 Ec, F3 Hc, long c0, long count) {
+    const long c = c0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c0 + count) return;
     const long nyz = (long)P.ny * P.nz;
     const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
     const long ny1 = P.ny + 1, nz1 = P.nz + 1;
