@@ -33,8 +33,9 @@ static __global__ void k_sum_stride(const double* __restrict__ in, long n, doubl
 // the loads of GF_SUM_BATCH terms issued before their additions (one thread
 // has ~n / T terms, too many to wait for one at a time).  32 measured best of
 // 8, 16 and 32 on 1.57 M cells: gf_average + gf_probe_em add 0.17 ms (FP64)
-// and 0.19 ms (mixed) to a step, against 0.20 and 0.34 ms at 8.  With `cm` set, each
-// term is the FP64 value x + c of an FP32 pair, as in k_sum_stride_f32.
+// and 0.19 ms (mixed) to a step, against 0.20 and 0.34 ms at 8.  In the
+// mixed form (f32) each term is the FP64 value x + c of an FP32 pair (c may
+// be null).
 struct Sum3In {
     const void* x[3];
     const float* cm[3];
@@ -149,16 +150,6 @@ __global__ void k_em_cell(Params P, F3T<R> E, F3T<R> H, F3 Ec, F3 Hc, long c0, l
 // Mixed form (FP32 state with a compensation word): FP64 reductions and the
 // conversions at the C ABI, which stays FP64.
 // ---------------------------------------------------------------------------
-
-// as k_sum_stride, over the FP64 values x + c of an FP32 pair (c may be null)
-static __global__ void k_sum_stride_f32(const float* __restrict__ x, const float* __restrict__ cm, long n,
-                                 double* __restrict__ partial, long T) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    double acc = 0.;
-    for (long i = t; i < n; i += T) acc = acc + ((double)x[i] + (cm ? (double)cm[i] : 0.));
-    partial[t] = acc;
-}
 
 // out = x + c in FP64 (c may be null)
 static __global__ void k_widen(const float* __restrict__ x, const float* __restrict__ cm, long n, double* __restrict__ out) {
