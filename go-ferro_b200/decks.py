@@ -239,6 +239,10 @@ class Deck:
     u0: Optional[np.ndarray] = None
     v0: Optional[np.ndarray] = None
     Hext_table: Optional[np.ndarray] = None    # (K, 4): t Hx Hy Hz
+    # per-cell material ids (nx, ny, nz); when set, if_read_struct is true and
+    # struct.in replaces the layer stack's cell assignment (read.cpp:280-294,
+    # global.cpp:67-83)
+    struct: Optional[np.ndarray] = None
     name: str = "deck"
 
     @property
@@ -246,7 +250,9 @@ class Deck:
         return self.nx * self.ny * self.nz
 
     def material_cell(self) -> np.ndarray:
-        """Per-cell material id as set_global builds it (global.cpp:65-79)."""
+        """Per-cell material id as set_global builds it (global.cpp:65-83)."""
+        if self.struct is not None:
+            return np.asarray(self.struct, dtype=np.uint8).reshape(self.nx, self.ny, self.nz).copy()
         mc = np.zeros((self.nx, self.ny, self.nz), dtype=np.uint8)
         nxw = self.nx if self.nx_work is None else self.nx_work
         nyw = self.ny if self.ny_work is None else self.ny_work
@@ -264,7 +270,7 @@ class Deck:
         L = [f"{self.nx} {self.ny} {self.nz}",
              f"{_f(self.dx)} {_f(self.dy)} {_f(self.dz)}",
              " ".join(_b(v) for v in self.periodic),
-             "false",
+             _b(self.struct is not None),
              f"{nxw} {nyw}",
              str(nl),
              f"1 1 {nl}",
@@ -367,6 +373,12 @@ def write_deck(deck: Deck, directory: str) -> str:
         _write_restart(os.path.join(directory, "v.in"), v)
     if deck.Hext_table is not None:
         np.savetxt(os.path.join(directory, "Hext.in"), deck.Hext_table, fmt="%.17e")
+    if deck.struct is not None:
+        # one line per cell: x y z id, 1-based coordinates
+        mc = deck.material_cell()
+        i, j, k = np.meshgrid(np.arange(deck.nx), np.arange(deck.ny), np.arange(deck.nz), indexing="ij")
+        rows = np.stack([i.ravel() + 1, j.ravel() + 1, k.ravel() + 1, mc.ravel().astype(np.int64)], axis=1)
+        np.savetxt(os.path.join(directory, "struct.in"), rows, fmt="%d")
     return directory
 
 

@@ -127,7 +127,8 @@ def test_mixed_graph_and_eager_identical(gf, tmp_path):
 
 
 @pytest.mark.parametrize("vname", ["afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
-                                   "drude_metal_layer", "pec_layer", "spin_pumping_ishe"])
+                                   "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
+                                   "random_struct_6mat"])
 def test_mixed_afm_drude_pec_match_live_oracle(gf, refrun, tmp_path, vname):
     """Antiferromagnets (both sublattices renormalised every stage), Drude
     poles and perfect conductors in the mixed form."""

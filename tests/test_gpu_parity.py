@@ -6,6 +6,7 @@ Tolerance (FP64 form): every traced observable and every final field agrees
 with the reference to 1e-10 relative to the observable's largest magnitude.
 """
 import importlib.util
+import dataclasses
 import json
 import os
 
@@ -236,14 +237,42 @@ def _variants(gf):
     d.spin_pumping = True
     d.periodic = (True, True, False)
     v["spin_pumping_ishe"] = (d, 20, (4, 4, 2))
+    # materials scattered cell by cell (struct.in): the ferroelectric and
+    # dielectrics of different permittivity and conductivity.  With three
+    # materials every E edge's four-cell quadruple is one of at most 3^4 = 81
+    # classes (the Yee kernel's class table); with six there are more than
+    # 256 and the kernel reads the four cells' materials itself.
+    for nmat in (3, 6):
+        d = D.preset_ferroelectric(nx=8, ny=8, nz=10, steps=20)
+        for q in range(1, nmat):
+            d.materials.append(dataclasses.replace(D.ggg(), title=f"diel{q}", er=4.0 + 3.0 * q,
+                                                   cond=(0.0, 1e3, 1e4, 5e4, 2e4)[q - 1]))
+        rng = np.random.default_rng(100 + nmat)
+        d.struct = rng.integers(1, nmat + 1, size=(8, 8, 10)).astype(np.uint8)
+        v[f"random_struct_{nmat}mat"] = (d, 20, (4, 4, 5))
     return v
+
+
+def edge_quadruples(mc):
+    """Distinct four-cell material quadruples of the interior x-directed E
+    edges (cells (i, j-1|j, k-1|k)), a lower bound of the Yee kernel's class
+    count."""
+    q = np.stack([mc[:, :-1, :-1], mc[:, :-1, 1:], mc[:, 1:, :-1], mc[:, 1:, 1:]], axis=-1).reshape(-1, 4)
+    return len({tuple(r) for r in q})
+
+
+def test_random_struct_variants_cover_both_yee_paths(gf):
+    v = _variants(gf)
+    assert edge_quadruples(v["random_struct_3mat"][0].material_cell()) <= 81
+    assert edge_quadruples(v["random_struct_6mat"][0].material_cell()) > 256
 
 
 @pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box",
                                    "fe_jf6_plane_wave_eext", "two_fm_materials_dmi_uniaxial", "demag_factor",
                                    "elastic_multi_tile", "elastic_quirk_far_tile", "fm_film_demag_substrate",
                                    "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
-                                   "drude_metal_layer", "pec_layer", "spin_pumping_ishe"])
+                                   "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
+                                   "random_struct_6mat"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
