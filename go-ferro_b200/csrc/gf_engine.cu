@@ -22,7 +22,6 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -1269,7 +1268,9 @@ int setup_em_classes(gf_engine* eng) {
     const Deck& d = eng->deck;
     const long nx = P.nx, ny = P.ny, nz = P.nz;
     auto mc = [&](long i, long j, long k) -> unsigned { return d.material_cell[(size_t)((i * ny + j) * nz + k)]; };
-    std::unordered_map<uint32_t, int> index;
+    // class of each quadruple of ids 0..kMaxMat, -1 until first seen
+    constexpr int K = kMaxMat + 1;
+    std::vector<int> index((size_t)K * K * K * K, -1);
     std::vector<uint32_t> keys;
     std::vector<uint8_t> cls[3];
     const long ext[3][3] = {{nx, ny + 1, nz + 1}, {nx + 1, ny, nz + 1}, {nx + 1, ny + 1, nz}};
@@ -1298,15 +1299,11 @@ int setup_em_classes(gf_engine* eng) {
                     }
                     if (bnd) continue;
                     const uint32_t key = ids[0] | (ids[1] << 8) | (ids[2] << 16) | (ids[3] << 24);
-                    auto it = index.find(key);
-                    int c;
-                    if (it == index.end()) {
+                    int& c = index[(((size_t)ids[0] * K + ids[1]) * K + ids[2]) * K + ids[3]];
+                    if (c < 0) {
+                        if ((int)keys.size() >= kEmMaxCls) { P.em_cls = 0; return GF_OK; }
                         c = (int)keys.size();
-                        if (c >= kEmMaxCls) { P.em_cls = 0; return GF_OK; }
-                        index.emplace(key, c);
                         keys.push_back(key);
-                    } else {
-                        c = it->second;
                     }
                     cls[C][(size_t)((i * ext[C][1] + j) * ext[C][2] + k)] = (uint8_t)c;
                 }
