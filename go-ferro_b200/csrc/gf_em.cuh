@@ -243,13 +243,10 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
             er = er / R(4.); cond = cond / R(4.);
             coef = dt_e0_r / er;   // (dt / e0) rounded once on the host, as the reference's left-to-right evaluation
         }
-        Jf = Jf / R(4.);
-        // pc counts the ferroelectric cells (1..4): divisions by 1, 2 and 4 are exact
-        if constexpr (is_mixed<R>::value)
-            dP = dP * (pc == 3.f ? 1.f / 3.f : (pc == 1.f ? 1.f : (pc == 2.f ? 0.5f : 0.25f)));
-        else
-            dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
-        R rhs = curl - Jf;
+        // without free current (or P sources) the term is +0, and x - (+0)
+        // is x in every bit, so it is left out
+        R rhs = curl;
+        if (P.jf_on) rhs = curl - Jf / R(4.);
         if (P.drude) {
             // Drude current: 4-cell mean of the three poles' stage values
             R Jp = R(0.);
@@ -267,7 +264,15 @@ __device__ inline void em_E_edge(const Params& P, const StageIOT<R>& io, const S
             for (int q = 0; q < 4; q++) Ji = Ji + ishe_cell(P, io, C, cx[q], cy[q], cz[q]);
             rhs = rhs - Ji / R(4.);
         }
-        rhs = rhs - cond * L.self - qdivR(dP, P.dt, P.rdt, P.f.rdt);
+        rhs = rhs - cond * L.self;
+        if (P.em_fromP) {
+            // pc counts the ferroelectric cells (1..4): divisions by 1, 2 and 4 are exact
+            if constexpr (is_mixed<R>::value)
+                dP = dP * (pc == 3.f ? 1.f / 3.f : (pc == 1.f ? 1.f : (pc == 2.f ? 0.5f : 0.25f)));
+            else
+                dP = qdiv(dP, pc, pc == 3. ? kInv3 : (pc == 1. ? 1. : (pc == 2. ? 0.5 : 0.25)));
+            rhs = rhs - qdivR(dP, P.dt, P.rdt, P.f.rdt);
+        }
         d = coef * rhs;
     }
     rk_x<S>(L, d, io.E_out.c[C], io.E_acc.c[C], io.E_cmp.c[C], e);
