@@ -99,12 +99,22 @@ __device__ inline void eigen_terms(const Params& P, const StageIOT<R>& io, long 
                                    R mz, R px, R py, R pz, const R e0[6], R e[6]) {
     const R third = R(1.) / R(3.);
     R t[6];
-    t[0] = mt.l100_15 * (mx * mx - third) + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
-    t[1] = mt.l100_15 * (my * my - third) + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
-    t[2] = mt.l100_15 * (mz * mz - third) + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
-    t[3] = mt.l111_15 * my * mz + mt.Q44 * py * pz;
-    t[4] = mt.l111_15 * mx * mz + mt.Q44 * px * pz;
-    t[5] = mt.l111_15 * my * mx + mt.Q44 * py * px;
+    t[0] = mt.l100_15 * (mx * mx - third);
+    t[1] = mt.l100_15 * (my * my - third);
+    t[2] = mt.l100_15 * (mz * mz - third);
+    t[3] = mt.l111_15 * my * mz;
+    t[4] = mt.l111_15 * mx * mz;
+    t[5] = mt.l111_15 * my * mx;
+    // electrostriction, added in the same order; without ferroelectrics p = 0
+    // and these terms are zeros that leave every sum unchanged
+    if (P.fe) {
+        t[0] = t[0] + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
+        t[1] = t[1] + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
+        t[2] = t[2] + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
+        t[3] = t[3] + mt.Q44 * py * pz;
+        t[4] = t[4] + mt.Q44 * px * pz;
+        t[5] = t[5] + mt.Q44 * py * px;
+    }
     if (P.afm) {
         R a1x, a1y, a1z, a2x, a2y, a2z;
         glb2crt(P, io.a1_in.c[0][c], io.a1_in.c[1][c], io.a1_in.c[2][c], a1x, a1y, a1z);
