@@ -1,20 +1,24 @@
 """Benchmark of the coupled RK4 phase-field step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload magnetoelastic|fm_demag|ferroelectric]
+                    [--workload ferroelectric|magnetoelastic|fm_demag|sweep]
                     [--precision both|fp64|mixed]
 
-Workload (default): the coupled magnetoelastic + elastodynamics + Maxwell FDTD
-run on a 128x128x96 grid (56-layer garnet substrate, 32-layer YIG film,
-8 vacuum layers), synthetic seeded initial state.  One step = one full RK4
-step of all active physics.  The metric is cell-steps/s (grid cells x steps /
-device time), whole job over all ranks: the headline `value` is the FP64
-form (the reference's arithmetic); with --precision both (the default) the
-line also carries `mixed`, the same measurement of the FP32 mixed form, its
-speed-up over FP64 and its trace error against the FP64 engine on the same
-initial state; at N=1 it also carries `adjoint`, the cost of the discrete
-adjoint (backward run) against the FP64 forward step on a 256x256x32
-ferromagnetic film (skip with --no-adjoint).
+Workload (default): the ferroelectric TDGL + electrostriction +
+elastodynamics + Maxwell FDTD run on a 128^3 grid (PbTiO3-like film, dx =
+1 nm, seeded random P within +-1e-3 C/m^2, z-polarised Gaussian sheet
+current), the largest single-GPU workload, run in both FP64 and FP32-mixed.
+One step = one full RK4 step of all active physics.  The metric is
+cell-steps/s (grid cells x steps / device time), whole job over all ranks: the
+headline `value` is the FP64 form (the reference's arithmetic); with
+--precision both (the default) the line also carries `mixed`, the same
+measurement of the FP32 mixed form, its speed-up over FP64 and its trace error
+against the FP64 engine on the same initial state.  At N=1 it also carries
+`step_roofline` (the whole step's algorithmic bytes per cell-step over the
+measured copy peak), `other_workloads` (the coupled magnetoelastic 128x128x96
+film and the 64x64x16 FM + magnetostatics run, both forms), `adjoint` (the
+cost of the discrete adjoint against the FP64 forward step on a 256x256x32
+ferromagnetic film) and `batched` (48 ferroelectric instances per graph).
 
 `--impl ours` times the engine (CUDA events on the engine stream, max over
 ranks), measures the end-to-end rate through the C ABI with host buffers,
@@ -33,7 +37,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import tempfile
 import time
@@ -51,7 +54,7 @@ WORKLOADS = {
                      sample_kw=dict(nx=64, ny=64, nz=16),
                      desc="FM LLG + FFT magnetostatics, 64x64x16, dx=2nm"),
     "ferroelectric": dict(preset="ferroelectric", kw=dict(nx=128, ny=128, nz=128),
-                          sample_kw=dict(nx=32, ny=32, nz=128),
+                          sample_kw=dict(nx=16, ny=16, nz=128),
                           desc="FE TDGL + electrostriction + elastodynamics + FDTD, 128^3, dx=1nm"),
 }
 
@@ -97,6 +100,52 @@ def alg_bytes_per_unit(kernel: str, info, mfe_frac: float = 0.0, mixed: bool = F
     return float("nan")
 
 
+# Algorithmic bytes per cell-step of each physics block: the compulsory
+# traffic of classical RK4 with one read and one write per array per kernel
+# (18 accesses per state scalar per step: FP64 144 B, FP32-mixed 72 B + 8 B of
+# compensation word), plus the per-stage static-field reads, stencil halo
+# re-reads free; a block counts over the cells it is active on.
+STEP_BYTES = {  # block: (FP64, FP32-mixed)
+    "fm": (532.0, 292.0), "afm": (964.0, 532.0), "fe": (864.0, 480.0), "elastic": (984.0, 540.0),
+    "em": (864.0, 480.0), "drude": (1296.0, 720.0), "demag": (672.0, 336.0),
+}
+
+
+def step_alg_bytes(d, info, mixed: bool) -> float:
+    """Algorithmic bytes of one step of deck `d` per grid cell."""
+    mc = d.material_cell()
+    n = float(mc.size)
+    col = 1 if mixed else 0
+
+    def frac(pred):
+        ids = [q + 1 for q, mt in enumerate(d.materials) if pred(mt)]
+        return float(np.isin(mc, ids).sum()) / n if ids else 0.0
+    b = 0.0
+    if info.fm:
+        b += STEP_BYTES["fm"][col] * frac(lambda m: m.fm)
+    if info.afm:
+        b += STEP_BYTES["afm"][col] * frac(lambda m: m.afm)
+    if info.fe:
+        b += STEP_BYTES["fe"][col] * frac(lambda m: m.fe)
+    if info.elastic:
+        b += STEP_BYTES["elastic"][col] * float((mc != 0).sum()) / n
+    if info.em:
+        b += STEP_BYTES["em"][col]
+        if any(m.drude[0][1] != 0 or m.drude[1][1] != 0 or m.drude[2][1] != 0 for m in d.materials):
+            b += STEP_BYTES["drude"][col]
+    if info.demag_per_stage:
+        b += STEP_BYTES["demag"][col]
+    return b
+
+
+def step_roofline(d, info, ms_per_step: float, mixed: bool) -> dict:
+    bpc = step_alg_bytes(d, info, mixed)
+    achieved = bpc * d.n / (ms_per_step / 1e3) / 1e9
+    peak, kind = load_peaks()
+    return {"bound": "hbm", "alg_bytes_per_cell_step": bpc, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": kind}
+
+
 def units_per_launch(kernel: str, info) -> int:
     nx, ny, nz = info.nx, info.ny, info.nz
     edges = {"x": nx * (ny + 1) * (nz + 1), "y": (nx + 1) * ny * (nz + 1), "z": (nx + 1) * (ny + 1) * nz}
@@ -128,57 +177,90 @@ def committed_traffic(kernel: str, workload: str, mixed: bool = False):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML by a host thread
+    every ~2 ms while the timed region runs.  A timed region of a few tens of
+    milliseconds is shorter than nvidia-smi's start-up and first sampling
+    interval, so polling NVML directly is what yields samples inside it;
+    `mark_start` / `mark_end` bracket the region in host time and `summary`
+    keeps the samples taken between them (the nearest ones if the region was
+    shorter than one poll).  Only reads the GPU's state."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.t0 = self.t1 = None
+        self.err = None
+        self._stop = False
+        self._thread = None
+        self.smax = None
+
+    def _poll(self, nv, h):
+        while not self._stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), float(sm), int(rs)))
+            except Exception as e:      # keep the region's timing unaffected
+                self.err = str(e)
+                return
+            time.sleep(0.002)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu),
-                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            # CUDA device index -> NVML handle through the device UUID (NVML
+            # enumerates every GPU of the node, CUDA only the visible ones)
+            import torch
+            h = None
+            try:
+                h = nv.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(self.gpu).uuid))
+            except Exception:
+                h = None
+            if h is None:
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+                idx = int(vis.split(",")[self.gpu]) if vis and vis.split(",")[self.gpu].strip().isdigit() else self.gpu
+                h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self._thread.start()
+            deadline = time.perf_counter() + 2.0
+            while not self.samples and self.err is None and time.perf_counter() < deadline:
+                time.sleep(0.001)
+        except Exception as e:
+            self.err = str(e)
         return self
 
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+        # one more poll after the region so that a short region has a sample on each side
+        time.sleep(0.005)
+
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop = True
+        if self._thread:
+            self._thread.join(timeout=2)
 
     def summary(self):
-        if not self.path or not os.path.exists(self.path):
-            return None
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": [], "samples": 0,
+                    "note": f"no NVML samples: {self.err}"}
+        t0 = self.t0 if self.t0 is not None else self.samples[0][0]
+        t1 = self.t1 if self.t1 is not None else self.samples[-1][0]
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        where = "inside the timed region"
+        if not inside:
+            inside = sorted(self.samples, key=lambda s: min(abs(s[0] - t0), abs(s[0] - t1)))[:2]
+            where = "nearest to the timed region (shorter than one poll)"
+        reasons = sorted({nm for _, _, rs in inside for nm, bit in self.REASONS.items() if rs & bit})
+        return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(inside), "source": f"NVML, {where}"}
 
 
 def build_deck(gf, wl: str, sample: bool):
@@ -188,9 +270,14 @@ def build_deck(gf, wl: str, sample: bool):
     return d
 
 
-def cpu_reference(gf, wl: str, steps: int, tmp: str, warmup: int = 0):
+def cpu_reference(gf, wl: str, steps: int, tmp: str, warmup: int = 0, procs: int = 1):
     """GO-Ferro's own solver on the bounded CPU sample: `warmup` untimed steps,
-    then `steps` timed ones; returns (cell-steps/s, info)."""
+    then `steps` timed ones; returns (cell-steps/s, info).  The reference's
+    host build is serial (its OpenACC pragmas are ignored on the host), so
+    the whole host is used by running `procs` copies of the sample at once,
+    one per core; the rate is procs x cells x steps over the slowest copy's
+    time loop."""
+    from concurrent.futures import ThreadPoolExecutor
     from oracle import refrun
     if not refrun.available():
         return None, "oracle binary not built"
@@ -198,12 +285,24 @@ def cpu_reference(gf, wl: str, steps: int, tmp: str, warmup: int = 0):
     d.steps = steps + warmup
     ddir = os.path.join(tmp, "ref_deck")
     gf.decks.write_deck(d, ddir)
-    r = refrun.run(ddir, os.path.join(tmp, "ref_out"), steps=steps + warmup, trace_every=max(steps + warmup, 1),
-                   warmup=warmup)
-    t = r["timing"]
-    value = d.n * steps / t["seconds"]
-    sample = f"{d.nx}x{d.ny}x{d.nz} sub-grid of the workload's layer stack, {steps} steps, serial reference build"
-    return value, {"seconds": t["seconds"], "sample": sample, "cells": d.n}
+
+    def one(q):
+        return refrun.run(ddir, os.path.join(tmp, f"ref_out{q}"), steps=steps + warmup,
+                          trace_every=max(steps + warmup, 1), warmup=warmup)
+    with ThreadPoolExecutor(max_workers=procs) as ex:
+        runs = list(ex.map(one, range(procs)))
+    secs = max(r["timing"]["seconds"] for r in runs)
+    value = procs * d.n * steps / secs
+    sample = (f"{d.nx}x{d.ny}x{d.nz} sub-grid of the workload's layer stack, {steps} steps after {warmup} untimed, "
+              f"serial reference build" + (f", {procs} concurrent copies (one per core)" if procs > 1 else ""))
+    return value, {"seconds": secs, "sample": sample, "cells": d.n, "procs": procs}
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def run_reference_arm(args, rank, world):
@@ -212,10 +311,11 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return
     spec = WORKLOADS[args.workload]
+    procs = max(1, min(host_cores(), args.ref_procs))
     with tempfile.TemporaryDirectory() as tmp:
         steps = max(1, min(args.steps, args.ref_steps))
         warm = min(args.warmup, 3)
-        value, info = cpu_reference(gf, args.workload, steps, tmp, warm)
+        value, info = cpu_reference(gf, args.workload, steps, tmp, warm, procs=procs)
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": info}))
         return
@@ -224,7 +324,8 @@ def run_reference_arm(args, rank, world):
         "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * info["seconds"] / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": spec["desc"], "sample": info["sample"]},
-        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "reference", "sample": info["sample"]},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": procs, "kind": "reference",
+                         "sample": info["sample"]},
         "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -304,10 +405,12 @@ def measure(gf, torch, dist, args, world, local_rank, precision, d, ddir, upload
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as cs:
+        cs.mark_start()
         ev0.record(stream)
         eng.advance(args.steps)
         ev1.record(stream)
         ev1.synchronize()
+        cs.mark_end()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -522,6 +625,32 @@ def run_sweep(gf, torch, args, local_rank, count, steps, fp64_check):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def measure_workload(gf, torch, dist, args, world, local_rank, wl, forms):
+    """Deck of workload `wl` (initial state uploaded, not written as text),
+    and the measurement of each form in `forms`."""
+    results = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        d = build_deck(gf, wl, sample=False)
+        uploads = []
+        if d.m0 is not None:
+            uploads.append(("m", d.m0))
+        if d.p0 is not None:
+            uploads += [("p", d.p0), ("q", d.q0)]
+        m0, p0 = d.m0, d.p0
+        d.m0 = None
+        d.p0 = None
+        ddir = os.path.join(tmp, "deck")
+        gf.decks.write_deck(d, ddir)
+        d.m0, d.p0 = m0, p0
+        mc = d.material_cell()
+        mfe_ids = [q + 1 for q, mt in enumerate(d.materials) if mt.fm or mt.fe]
+        mfe_frac = float(np.isin(mc, mfe_ids).mean()) if mfe_ids else 0.0
+        probe = (d.nx // 2, d.ny // 2, min(d.nz - 1, sum(l[0] for l in d.layers[:2]) - 2))
+        for form in forms:
+            results[form] = measure(gf, torch, dist, args, world, local_rank, form, d, ddir, uploads, probe)
+    return d, results, mfe_frac
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import __graft_entry__
@@ -551,24 +680,23 @@ def run_ours(args, rank, world, local_rank):
         return
     spec = WORKLOADS[args.workload]
     forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
-    results = {}
-    with tempfile.TemporaryDirectory() as tmp:
-        d = build_deck(gf, args.workload, sample=False)
-        uploads = []
-        if d.m0 is not None:
-            uploads.append(("m", d.m0))
-        if d.p0 is not None:
-            uploads += [("p", d.p0), ("q", d.q0)]
-        d.m0 = None          # uploaded instead of written as text
-        d.p0 = None
-        ddir = os.path.join(tmp, "deck")
-        gf.decks.write_deck(d, ddir)
-        mc = d.material_cell()
-        mfe_ids = [q + 1 for q, mt in enumerate(d.materials) if mt.fm or mt.fe]
-        mfe_frac = float(np.isin(mc, mfe_ids).mean()) if mfe_ids else 0.0
-        probe = (d.nx // 2, d.ny // 2, min(d.nz - 1, sum(l[0] for l in d.layers[:2]) - 2))
-        for form in forms:
-            results[form] = measure(gf, torch, dist, args, world, local_rank, form, d, ddir, uploads, probe)
+    d, results, mfe_frac = measure_workload(gf, torch, dist, args, world, local_rank, args.workload, forms)
+    others = {}
+    if world == 1 and not args.no_other_workloads and args.workload == "ferroelectric":
+        # the other single-GPU workloads, both forms, on the same box (context
+        # for the headline; the headline is the largest single-GPU workload)
+        import copy
+        a2 = copy.copy(args)
+        a2.trace_steps = 20
+        for wl in ("magnetoelastic", "fm_demag"):
+            dw, rw, _ = measure_workload(gf, torch, dist, a2, world, local_rank, wl, ["fp64", "mixed"])
+            ent = {"workload": WORKLOADS[wl]["desc"], "cells": dw.n}
+            for form, rr in rw.items():
+                ent[form] = {"value": rr["value"], "ms_per_step": rr["ms"] / args.steps, "clocks": rr["clocks"],
+                             "step_roofline": step_roofline(dw, rr["info"], rr["ms"] / args.steps, form == "mixed")}
+            ent["speedup_mixed_vs_fp64"] = rw["mixed"]["value"] / rw["fp64"]["value"]
+            ent["mixed_trace_error_vs_fp64"] = trace_error(rw["mixed"]["trace"], rw["fp64"]["trace"])
+            others[wl] = ent
 
     if dist:
         dist.destroy_process_group()
@@ -597,6 +725,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": f"state resident in HBM ({info.device_bytes / 1e9:.2f} GB) > L2 (126 MB): no flush needed",
                    "graph": "one CUDA graph per step parity"},
         "roofline": roofline(r, args, mfe_frac, head_mixed),
+        "step_roofline": step_roofline(d, info, r["ms"] / args.steps, head_mixed),
         "cpu_baseline": cpu,
         "e2e": r["e2e"],
         "clocks": r["clocks"],
@@ -612,12 +741,15 @@ def run_ours(args, rank, world, local_rank):
             "trace_error_vs_fp64": err, "trace_steps": args.trace_steps,
             "max_trace_error": max(err.values()) if err else None,
             "error_definition": "max over the trace of |mixed - fp64| / max|fp64 component| per vector observable",
-            "roofline": roofline(rm, args, mfe_frac, True), "e2e": rm["e2e"], "clocks": rm["clocks"],
+            "roofline": roofline(rm, args, mfe_frac, True),
+            "step_roofline": step_roofline(d, rm["info"], rm["ms"] / args.steps, True),
+            "e2e": rm["e2e"], "clocks": rm["clocks"],
             "gpu_launches": int(rm["info"].launches_per_step) * args.steps,
             "kernels_ms_per_step": {k: v[1] / 2.0 for k, v in sorted(rm["prof"].items(), key=lambda kv: -kv[1][1])},
             "device_bytes": int(rm["info"].device_bytes),
         }
-        line["gpu_launches"] += line["mixed"]["gpu_launches"]
+    if others:
+        line["other_workloads"] = others
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(gf, torch, args, local_rank)
     if world == 1 and not args.no_batch:
@@ -634,8 +766,11 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep"], default="magnetoelastic")
-    ap.add_argument("--ref-steps", type=int, default=40)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep"], default="ferroelectric")
+    ap.add_argument("--ref-steps", type=int, default=100)
+    ap.add_argument("--no-other-workloads", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=64,
+                    help="most concurrent copies of the serial reference in --impl reference (one per host core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--trace-steps", type=int, default=100)

@@ -105,16 +105,17 @@ __device__ inline void eigen_terms(const Params& P, const StageIOT<R>& io, long 
     t[3] = mt.l111_15 * my * mz;
     t[4] = mt.l111_15 * mx * mz;
     t[5] = mt.l111_15 * my * mx;
-    // electrostriction, added in the same order; without ferroelectrics p = 0
-    // and these terms are zeros that leave every sum unchanged
-    if (P.fe) {
-        t[0] = t[0] + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
-        t[1] = t[1] + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
-        t[2] = t[2] + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
-        t[3] = t[3] + mt.Q44 * py * pz;
-        t[4] = t[4] + mt.Q44 * px * pz;
-        t[5] = t[5] + mt.Q44 * py * px;
-    }
+    // electrostriction, added in the same order.  Evaluated also without
+    // ferroelectrics (p = 0): the terms are then zeros, but adding +0 turns a
+    // -0 magnetostriction term (e.g. l111 my mz with mz = 0, my < 0) into +0,
+    // as the reference's unconditional sum does, so the sign of every zero
+    // matches too
+    t[0] = t[0] + mt.Q11 * (px * px) + mt.Q12 * ((py * py) + (pz * pz));
+    t[1] = t[1] + mt.Q11 * (py * py) + mt.Q12 * ((px * px) + (pz * pz));
+    t[2] = t[2] + mt.Q11 * (pz * pz) + mt.Q12 * ((py * py) + (px * px));
+    t[3] = t[3] + mt.Q44 * py * pz;
+    t[4] = t[4] + mt.Q44 * px * pz;
+    t[5] = t[5] + mt.Q44 * py * px;
     if (P.afm) {
         R a1x, a1y, a1z, a2x, a2y, a2z;
         glb2crt(P, io.a1_in.c[0][c], io.a1_in.c[1][c], io.a1_in.c[2][c], a1x, a1y, a1z);

@@ -2002,8 +2002,8 @@ int gf_load_state(gf_engine* e, const char* path) {
     if (!f) { eng->err = std::string("cannot read ") + path; return GF_EIO; }
     CkHeader h;
     const unsigned long long steps_before = eng->steps_done;
-    // a failed load leaves the step count as it was (field contents already
-    // copied are not restored)
+    // the whole file is read and checked into host buffers before the first
+    // device write, so a failed load leaves the engine as it was
     auto bad = [&](const std::string& why, int rc) { std::fclose(f); eng->err = why; eng->steps_done = steps_before; return rc; };
     if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kCkMagic, 8) != 0)
         return bad(std::string(path) + " is not an engine checkpoint", GF_EIO);
@@ -2013,23 +2013,26 @@ int gf_load_state(gf_engine* e, const char* path) {
         return bad("checkpoint precision differs from the engine's", GF_EINVAL);
     GF_CU(cudaSetDevice(eng->device));
     GF_CU(cudaStreamSynchronize(eng->stream));
-    // the current-step buffers depend on the step parity: take the file's first
+    // the current-step buffers depend on the step parity: take the file's
+    // (restored on failure by `bad`)
     eng->steps_done = h.steps_done;
     std::vector<CkBlob> blobs = ck_blobs(eng);
     if (h.nblobs != blobs.size()) return bad("checkpoint holds different fields than this engine", GF_EINVAL);
-    std::vector<char> buf;
-    for (const CkBlob& b : blobs) {
+    std::vector<std::vector<char>> bufs(blobs.size());
+    for (size_t q = 0; q < blobs.size(); q++) {
+        const CkBlob& b = blobs[q];
         char name[32];
         uint64_t bytes = 0;
         if (std::fread(name, sizeof(name), 1, f) != 1 || std::fread(&bytes, sizeof(bytes), 1, f) != 1)
             return bad("truncated checkpoint", GF_EIO);
         name[31] = 0;
         if (b.name != name || bytes != b.bytes) return bad(std::string("checkpoint field ") + name + " does not match", GF_EINVAL);
-        buf.resize(bytes);
-        if (std::fread(buf.data(), 1, bytes, f) != bytes) return bad("truncated checkpoint", GF_EIO);
-        if (cudaMemcpy(b.dev, buf.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-            return bad("checkpoint upload failed", GF_ECUDA);
+        bufs[q].resize(bytes);
+        if (std::fread(bufs[q].data(), 1, bytes, f) != bytes) return bad("truncated checkpoint", GF_EIO);
     }
+    for (size_t q = 0; q < blobs.size(); q++)
+        if (cudaMemcpy(blobs[q].dev, bufs[q].data(), blobs[q].bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bad("checkpoint upload failed (device state now partly overwritten)", GF_ECUDA);
     std::fclose(f);
     eng->t_host = h.t_host; eng->presc_H = (long)h.presc_H; eng->presc_E = (long)h.presc_E;
     for (int a = 0; a < 3; a++) { eng->Hext_cur[a] = h.Hext_cur[a]; eng->Eext_cur[a] = h.Eext_cur[a]; }
@@ -2780,10 +2783,13 @@ void gf_adjoint_destroy(gf_adjoint* a) {
 // ---------------------------------------------------------------------------
 // Allocation-free mean of a device array (gf_field_mean_noalloc).
 //
-// Same deterministic three-pass strided sum as gf_average, with its partial
-// sums in a file-scope device array instead of engine-owned scratch.  Pass 1
-// uses one partial per 1024 input elements, so the array bounds the input
-// length; passes 2 and 3 reduce the partials to 64 values and then one.
+// A deterministic three-pass strided sum (the k_sum_stride passes that
+// gf_average also uses), with its partial sums in a file-scope device array
+// instead of engine-owned scratch.  Pass 1 uses one partial per 1024 input
+// elements (gf_average's pass 1 uses a fixed count of partials instead), so
+// the result is deterministic for a given n but may differ from gf_average's
+// in the last bits; the array bounds the input length; passes 2 and 3 reduce
+// the partials to 64 values and then one.
 // Every pass writes all the partials the next pass reads, so nothing in the
 // array has to start at zero.  The array is shared by all calls on a device
 // and keeps the last call's partials; calls that overlap on the GPU (two
@@ -2830,11 +2836,20 @@ int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, doub
     double* p1 = scratch;
     double* p2 = scratch + kNoAllocPass1;
     const long T1 = (long)((n + kNoAllocChunk - 1) / kNoAllocChunk);
-    launch(k_sum_stride, dim3(blocks_for(T1, 256)), dim3(256), 0, st, dev_in, (long)n, p1, T1);
-    launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, T1, p2, 64L);
-    launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, dev_out, 1L);
-    launch(k_scale, dim3(1), dim3(1), 0, st, dev_out, divisor);
-    ce = cudaGetLastError();
+    // cudaLaunchKernel reports the error of its own launch; an error left
+    // pending by the caller's earlier work stays for the caller to read
+    const long nn = (long)n, c64 = 64L, c1 = 1L;
+    const double* p1c = p1;
+    const double* p2c = p2;
+    void* a1[] = {(void*)&dev_in, (void*)&nn, (void*)&p1, (void*)&T1};
+    void* a2[] = {(void*)&p1c, (void*)&T1, (void*)&p2, (void*)&c64};
+    void* a3[] = {(void*)&p2c, (void*)&c64, (void*)&dev_out, (void*)&c1};
+    void* a4[] = {(void*)&dev_out, (void*)&divisor};
+    const void* ks = reinterpret_cast<const void*>(&k_sum_stride);
+    ce = cudaLaunchKernel(ks, dim3(blocks_for(T1, 256)), dim3(256), a1, 0, st);
+    if (ce == cudaSuccess) ce = cudaLaunchKernel(ks, dim3(1), dim3(64), a2, 0, st);
+    if (ce == cudaSuccess) ce = cudaLaunchKernel(ks, dim3(1), dim3(1), a3, 0, st);
+    if (ce == cudaSuccess) ce = cudaLaunchKernel(reinterpret_cast<const void*>(&k_scale), dim3(1), dim3(1), a4, 0, st);
     if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
     return GF_OK;
 }

@@ -190,7 +190,9 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used);
  * restarted from it continues bit for bit.  The reference restarts from
  * its %.7e text dumps (inoutput.cpp:330-887, input_* readers); this binary
  * form has no counterpart there.  Load needs an engine created from the same
- * deck and precision. Synchronous. */
+ * deck and precision.  Load reads and checks the whole file before it
+ * writes any device buffer, so a file that fails (wrong deck, precision,
+ * size or a short read) leaves the engine as it was. Synchronous. */
 int gf_save_state(gf_engine* e, const char* path);
 int gf_load_state(gf_engine* e, const char* path);
 
@@ -287,7 +289,10 @@ void gf_adjoint_destroy(gf_adjoint* a);
  *   - n must be 1..67,108,864 (64 Mi); larger inputs return GF_EINVAL with
  *     the limit in gf_last_error(NULL).
  *   - The first call on a device looks up that array's device address; make
- *     that first call before any stream capture on the device.
+ *     that first call before any stream capture on the device.  The address
+ *     is kept for the life of the process: after cudaDeviceReset (or any
+ *     other end of the device's primary context) the entry point must not be
+ *     called again on that device.
  *   - All calls on a device share the array: calls that overlap on the GPU
  *     (two streams, two host threads) race and give wrong sums.  Serialise
  *     them on one stream.

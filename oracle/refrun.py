@@ -25,9 +25,13 @@ def available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def build(ref_dir: str = "/root/reference") -> None:
-    """Compile the oracle (needs the reference sources; run where they exist)."""
-    subprocess.run(["make", "-C", HERE, f"REF_DIR={ref_dir}", "-j8"], check=True,
+def build(ref_dir: Optional[str] = None) -> None:
+    """Compile the oracle (needs the reference sources; run where they exist).
+    ref_dir: the reference source tree; default $GOFERRO_REF_DIR, else the
+    Makefile's default."""
+    ref_dir = ref_dir or os.environ.get("GOFERRO_REF_DIR")
+    args = [f"REF_DIR={ref_dir}"] if ref_dir else []
+    subprocess.run(["make", "-C", HERE] + args + ["-j8"], check=True,
                    stdout=subprocess.DEVNULL)
 
 
