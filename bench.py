@@ -263,9 +263,20 @@ class ClockSampler:
                 "samples": len(inside), "source": f"NVML, {where}"}
 
 
+GRID_OVERRIDE = None    # (nx, ny, nz) from --grid: a smaller copy of the workload for profiling
+
+
 def build_deck(gf, wl: str, sample: bool):
     spec = WORKLOADS[wl]
     kw = dict(spec["sample_kw"] if sample else spec["kw"])
+    if GRID_OVERRIDE and not sample:
+        nx, ny, nz = GRID_OVERRIDE
+        if spec["preset"] == "magnetoelastic":
+            # keep the layer stack's proportions (substrate, film, vacuum)
+            sub = max(1, round(kw["sub"] * nz / kw.get("nz", 96)))
+            film = max(1, round(kw["film"] * nz / kw.get("nz", 96)))
+            kw.update(sub=min(sub, nz - 1), film=min(film, nz - min(sub, nz - 1)))
+        kw.update(nx=nx, ny=ny, nz=nz)
     d = gf.decks.PRESETS[spec["preset"]](**kw)
     return d
 
@@ -769,6 +780,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep"], default="ferroelectric")
     ap.add_argument("--ref-steps", type=int, default=100)
     ap.add_argument("--no-other-workloads", action="store_true")
+    ap.add_argument("--grid", default=None,
+                    help="NXxNYxNZ: run a smaller copy of the workload (profiling captures); not a bench line")
+
     ap.add_argument("--ref-procs", type=int, default=64,
                     help="most concurrent copies of the serial reference in --impl reference (one per host core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -779,6 +793,9 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=100)
     ap.add_argument("--adjoint-steps", type=int, default=400)
     args = ap.parse_args()
+    global GRID_OVERRIDE
+    if args.grid:
+        GRID_OVERRIDE = tuple(int(x) for x in args.grid.lower().split("x"))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -87,6 +87,7 @@ struct Params {
     int elasto_on, elasto_back;   // if_elasto_on_pORm, if_elasto_backaction_from_pORm
     int em_fromM, em_fromP, em_back_M, em_back_P;
     int has_eig0, has_strain0, has_hext_nonunif;
+    int estat;                 // E_stat may be nonzero (Estat.in, the electrostatic solve or an upload); 0: it is all +0
     int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
     uint32_t fe_mask, fm_mask;   // bit id-1 set when material id is ferroelectric / ferromagnetic
     int spin;                 // spin pumping: inverse-spin-Hall current in the Yee E update

@@ -1,8 +1,12 @@
 // Magnetostatics: periodic FFT convolution of M with the demag
 // tensor of a cuboid cell.
 //
-//   k_newell      builds the nine real-space tensor tables on the device.
-//                 The tables follow the reference's construction
+//   newell_cell   the nine real-space tensor tables' entries of one cell,
+//                 evaluated on the host (the engine builds the tables with the
+//                 host's libm, as the reference does, multithreaded): the
+//                 far-field entries are small differences of large terms, so
+//                 a last-bit difference in log or atan grows by orders of
+//                 magnitude there.  The tables follow the reference's construction
 //                 (initialize_intermediate_Hms, magnetic_initialize.cpp:
 //                 1176-1402): the cell-averaged tensor of Newell, Williams and
 //                 Dunlop (J. Geophys. Res. 98, 9551, 1993) written with the
@@ -15,7 +19,7 @@
 //                 and 1-D alternatives (magnetostatic_solver.cpp:114-249).
 // The transforms themselves are cuFFT D2Z / Z2D (batched over the three
 // components), unnormalised as in the reference.  The mixed form builds the
-// tables and their spectra in FP64 (k_newell, D2Z), stores the spectra in
+// tables and their spectra in FP64 (newell_cell, D2Z), stores the spectra in
 // FP32 and runs R2C / C2R per stage.
 #pragma once
 
@@ -26,7 +30,7 @@
 namespace gf {
 
 // ---- Newell auxiliary functions (FP64) ----
-__device__ inline double nw_f2(double x, double y, double z) {
+__host__ __device__ inline double nw_f2(double x, double y, double z) {
     const double s = 1.0e-33;
     const double u = x * x, v = y * y, w = z * z;
     const double r = sqrt(u + v + w);
@@ -49,18 +53,18 @@ __device__ inline double nw_f2(double x, double y, double z) {
     return f;
 }
 
-__device__ inline double nw_f1(double x, double y, double z, double dy) {
+__host__ __device__ inline double nw_f1(double x, double y, double z, double dy) {
     const double ym = y - dy, yp = y + dy;
     return 2. * nw_f2(x, y, z) - nw_f2(x, ym, z) - nw_f2(x, yp, z);
 }
 
-__device__ inline double nw_a(double x, double y, double z, double dx, double dy, double dz) {
+__host__ __device__ inline double nw_a(double x, double y, double z, double dx, double dy, double dz) {
     const double xp = x + dx, xm = x - dx, zp = z + dz, zm = z - dz;
     return 4. * nw_f1(x, y, z, dy) - 2. * nw_f1(x, y, zp, dy) - 2. * nw_f1(x, y, zm, dy) - 2. * nw_f1(xp, y, z, dy)
            + nw_f1(xp, y, zp, dy) + nw_f1(xp, y, zm, dy) - 2. * nw_f1(xm, y, z, dy) + nw_f1(xm, y, zp, dy) + nw_f1(xm, y, zm, dy);
 }
 
-__device__ inline double nw_g2(double x, double y, double z) {
+__host__ __device__ inline double nw_g2(double x, double y, double z) {
     const double s = 1.0e-33;
     const double u = x * x, v = y * y, w = z * z;
     const double r = sqrt(u + v + w);
@@ -84,7 +88,7 @@ __device__ inline double nw_g2(double x, double y, double z) {
     return g;
 }
 
-__device__ inline double nw_g1(double x, double y, double z, double dx, double dy, double dz) {
+__host__ __device__ inline double nw_g1(double x, double y, double z, double dx, double dy, double dz) {
     const double xp = x + dx, xm = x - dx, yp = y + dy / 2., ym = y - dy / 2., zp = z + dz, zm = z - dz;
     return 4. * nw_g2(x, yp, z) - 4. * nw_g2(x, ym, z) - 2. * nw_g2(x, yp, zp) + 2. * nw_g2(x, ym, zp)
            - 2. * nw_g2(x, yp, zm) + 2. * nw_g2(x, ym, zm) - 2. * nw_g2(xm, yp, z) + 2. * nw_g2(xm, ym, z)
@@ -93,14 +97,14 @@ __device__ inline double nw_g1(double x, double y, double z, double dx, double d
            + nw_g2(xp, yp, zm) - nw_g2(xp, ym, zm);
 }
 
-__device__ inline double nw_b(double x, double y, double z, double dx, double dy, double dz) {
+__host__ __device__ inline double nw_b(double x, double y, double z, double dx, double dy, double dz) {
     const double yp = y + dy / 2., ym = y - dy / 2.;
     return nw_g1(x, yp, z, dx, dy, dz) - nw_g1(x, ym, z, dx, dy, dz);
 }
 
 // signed offset of wrapped index a on a periodic axis of length n, or
 // "none" for the entries the reference leaves zero
-__device__ inline bool wrap_offset(long a, long n, long& off) {
+__host__ __device__ inline bool wrap_offset(long a, long n, long& off) {
     const long h = n / 2;
     if (a <= h - 1) { off = a; return true; }
     if (a >= n - h + 1) { off = a - n; return true; }
@@ -108,30 +112,26 @@ __device__ inline bool wrap_offset(long a, long n, long& off) {
 }
 
 // table t: 0 Axyz 1 Ayzx 2 Azxy 3 Bxyz 4 Byzx 5 Bzxy 6 Byxz 7 Bzyx 8 Bxzy
-static __global__ void k_newell(Params P, double* tab /* 9 x n */) {
-    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
+__host__ __device__ inline void newell_cell(const Params& P, long c, double v[9]) {
     const long nyz = (long)P.ny * P.nz;
     const long a = c / nyz, b = (c - a * nyz) / P.nz, g = c - a * nyz - b * P.nz;
     long oi, oj, ok;
+    for (int t = 0; t < 9; t++) v[t] = 0.;
     const bool in = wrap_offset(a, P.nx, oi) && wrap_offset(b, P.ny, oj) && wrap_offset(g, P.nz, ok);
-    double v[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
-    if (in) {
-        const double dx = P.dx, dy = P.dy, dz = P.dz;
-        const double x = (double)oi * dx, y = (double)oj * dy, z = (double)ok * dz;
-        const double fourpi = 2. * (2. * kPi);
-        const double nn = (double)P.n;
-        v[0] = nw_a(x, y, z, dx, dy, dz) / fourpi / nn;
-        v[1] = nw_a(y, z, x, dy, dz, dx) / fourpi / nn;
-        v[2] = nw_a(z, x, y, dz, dx, dy) / fourpi / nn;
-        v[3] = nw_b(x, y, z, dx, dy, dz) / fourpi / nn;
-        v[4] = nw_b(y, z, x, dy, dz, dx) / fourpi / nn;
-        v[5] = nw_b(z, x, y, dz, dx, dy) / fourpi / nn;
-        v[6] = nw_b(y, x, z, dy, dx, dz) / fourpi / nn;
-        v[7] = nw_b(z, y, x, dz, dy, dx) / fourpi / nn;
-        v[8] = nw_b(x, z, y, dx, dz, dy) / fourpi / nn;
-    }
-    for (int t = 0; t < 9; t++) tab[(long)t * P.n + c] = v[t];
+    if (!in) return;
+    const double dx = P.dx, dy = P.dy, dz = P.dz;
+    const double x = (double)oi * dx, y = (double)oj * dy, z = (double)ok * dz;
+    const double fourpi = 2. * (2. * kPi);
+    const double nn = (double)P.n;
+    v[0] = nw_a(x, y, z, dx, dy, dz) / fourpi / nn;
+    v[1] = nw_a(y, z, x, dy, dz, dx) / fourpi / nn;
+    v[2] = nw_a(z, x, y, dz, dx, dy) / fourpi / nn;
+    v[3] = nw_b(x, y, z, dx, dy, dz) / fourpi / nn;
+    v[4] = nw_b(y, z, x, dy, dz, dx) / fourpi / nn;
+    v[5] = nw_b(z, x, y, dz, dx, dy) / fourpi / nn;
+    v[6] = nw_b(y, x, z, dy, dx, dz) / fourpi / nn;
+    v[7] = nw_b(z, y, x, dz, dy, dx) / fourpi / nn;
+    v[8] = nw_b(x, z, y, dx, dz, dy) / fourpi / nn;
 }
 
 __device__ inline cuDoubleComplex cmul(cuDoubleComplex a, cuDoubleComplex b) {

@@ -4,11 +4,15 @@
 //                 face-normal displacement gradients (get_dudxyz_glb,
 //                 elastic_dynamic_solver.cpp:106-187), cell strains (get_Dstrain,
 //                 :189-227) and dynamic eigenstrains of m and p
-//                 (get_eigenstrain_dynamic, :3-104), the six face stresses,
-//                 stress divergence, velocity and displacement increments and
-//                 their RK4 combination (get_dv_RK{1..4} :841-2800, get_du_RK*
-//                 :2801-2847, update_v*/update_u* :2849-3057); it also stores
-//                 the crystal-frame cell strain of magnetic/ferroelectric cells.
+//                 (get_eigenstrain_dynamic, :3-104), the six face stresses and
+//                 the stress divergence (the stress part of get_dv_RK{1..4}
+//                 :841-2800); it also stores the crystal-frame cell strain of
+//                 magnetic cells for the LLG kernels and, in the FP64 form, of
+//                 ferroelectric cells for the TDGL kernel.
+//   k_elastic_rk  per cell: damping terms, f_store, the velocity and
+//                 displacement increments and their RK4 combination
+//                 (get_dv_RK* :1295-1329, get_du_RK* :2801-2847,
+//                 update_v*/update_u* :2849-3057).
 //   k_elastic_bc  per (i,j) column: z absorbing boundary (Liao 4th order or
 //                 first-order Mur, elastodynamics_AbsorbingBoundary.cpp:91-230)
 //                 and the displacement source plane (update_Du_Gaussian*,
@@ -610,8 +614,10 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
                     }
 #pragma unroll
                     for (int a = 0; a < 3; a++) tz[a] = qdivR((s2[a] - s1[a]), P.dz, P.rdz, P.f.rdz);
-                    // cell strain for the magnetic and ferroelectric kernels
-                    if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_AFM | MF_FE))) {
+                    // cell strain for the magnetic kernels and, in the FP64 form,
+                    // the TDGL kernel (the mixed form's TDGL kernel forms its own
+                    // from u: fewer bytes, and its FP32 registers hold the stencil)
+                    if (want_strain && (sm.mat()[id - 1].flags & (MF_FM | MF_AFM | (is_mixed<R>::value ? 0u : MF_FE)))) {
                         R e[6];
                         e[0] = (me.gm(0, 0) + me.gp(0, 0)) / R(2.);
                         e[1] = (me.gm(1, 1) + me.gp(1, 1)) / R(2.);

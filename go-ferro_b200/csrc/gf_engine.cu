@@ -21,7 +21,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1017,6 +1019,40 @@ int static_field_now(gf_engine* eng) {
     return demag_solve(eng, f3(eng->m.X), f3(eng->a1.X), f3(eng->a2.X), false);
 }
 
+// The nine demag tensor tables (9 x n, table-major) of a grid, built on the
+// host with the host's libm on all cores: the reference builds them on the
+// host too (initialize_intermediate_Hms), and the far-field entries are small
+// differences of large terms, so a last-bit difference in log or atan would
+// grow by orders of magnitude there.  The last grid's tables are kept, so an
+// FP64 and a mixed engine of the same deck build them once.
+std::shared_ptr<const std::vector<double>> newell_tables(const Params& P) {
+    static std::mutex mu;
+    static std::shared_ptr<const std::vector<double>> last;
+    static double key[6] = {0, 0, 0, 0, 0, 0};
+    const double k6[6] = {(double)P.nx, (double)P.ny, (double)P.nz, P.dx, P.dy, P.dz};
+    std::lock_guard<std::mutex> lock(mu);
+    if (last && std::memcmp(key, k6, sizeof(k6)) == 0) return last;
+    auto tab = std::make_shared<std::vector<double>>((size_t)9 * P.n);
+    double* out = tab->data();
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt == 0 ? 1 : (nt > 64 ? 64 : nt);
+    const long n = P.n;
+    auto work = [&](unsigned w) {
+        double v[9];
+        for (long c = w; c < n; c += nt) {
+            newell_cell(P, c, v);
+            for (int t = 0; t < 9; t++) out[(size_t)t * n + c] = v[t];
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned w = 1; w < nt; w++) th.emplace_back(work, w);
+    work(0);
+    for (auto& x : th) x.join();
+    last = tab;
+    std::memcpy(key, k6, sizeof(k6));
+    return last;
+}
+
 int setup_demag(gf_engine* eng) {
     const Deck& d = eng->deck;
     const Params& P = eng->P;
@@ -1037,12 +1073,14 @@ int setup_demag(gf_engine* eng) {
         double* tab = nullptr;
         cufftDoubleComplex* nk64 = nullptr;
         cufftHandle p64 = 0;
+        const std::shared_ptr<const std::vector<double>> host_tab = newell_tables(P);
         cudaError_t ce = cudaMalloc(&tab, sizeof(double) * 9 * (size_t)P.n);
         if (ce == cudaSuccess) ce = cudaMalloc(&nk64, sizeof(cufftDoubleComplex) * 9 * (size_t)n21);
         cufftResult fr = CUFFT_SUCCESS;
         if (ce == cudaSuccess) fr = cufftPlanMany(&p64, 3, dims, nullptr, 1, (int)P.n, nullptr, 1, (int)n21, CUFFT_D2Z, 3);
         if (ce == cudaSuccess && fr == CUFFT_SUCCESS) fr = cufftSetStream(p64, eng->stream);
-        if (ce == cudaSuccess && fr == CUFFT_SUCCESS) ce = launch(k_newell, dim3(blocks_for(P.n, 128)), dim3(128), 0, eng->stream, P, tab);
+        if (ce == cudaSuccess && fr == CUFFT_SUCCESS)
+            ce = cudaMemcpyAsync(tab, host_tab->data(), sizeof(double) * 9 * (size_t)P.n, cudaMemcpyHostToDevice, eng->stream);
         for (int b = 0; b < 3 && ce == cudaSuccess && fr == CUFFT_SUCCESS; b++)
             fr = cufftExecD2Z(p64, tab + (size_t)3 * b * P.n, nk64 + (size_t)3 * b * n21);
         if (ce == cudaSuccess && fr == CUFFT_SUCCESS)
@@ -1074,13 +1112,20 @@ int setup_demag(gf_engine* eng) {
     eng->plans = true;
     GF_FFT(cufftSetStream(eng->plan_r2c, eng->stream));
     GF_FFT(cufftSetStream(eng->plan_c2r, eng->stream));
-    // demag tensor tables: 9 x n real on the device, transformed in three batches of 3
+    // demag tensor tables: 9 x n real, built on the host, transformed on the
+    // device in three batches of 3
+    const std::shared_ptr<const std::vector<double>> host_tab = newell_tables(P);
     double* tab = nullptr;
-    GF_TRY(dalloc_n(eng, &tab, (size_t)9 * P.n));
-    GF_CU(launch(k_newell, dim3(blocks_for(P.n, 128)), dim3(128), 0, eng->stream, P, tab));
-    for (int b = 0; b < 3; b++)
-        GF_FFT(cufftExecD2Z(eng->plan_r2c, tab + (size_t)3 * b * P.n, eng->Nk + (size_t)3 * b * n21));
-    GF_CU(cudaStreamSynchronize(eng->stream));
+    cudaError_t ce = cudaMalloc(&tab, sizeof(double) * 9 * (size_t)P.n);      // temporary
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(tab, host_tab->data(), sizeof(double) * 9 * (size_t)P.n, cudaMemcpyHostToDevice, eng->stream);
+    cufftResult fr = CUFFT_SUCCESS;
+    for (int b = 0; b < 3 && ce == cudaSuccess && fr == CUFFT_SUCCESS; b++)
+        fr = cufftExecD2Z(eng->plan_r2c, tab + (size_t)3 * b * P.n, eng->Nk + (size_t)3 * b * n21);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(eng->stream);
+    if (tab) cudaFree(tab);
+    if (ce != cudaSuccess) { eng->err = std::string("demag tables: ") + cudaGetErrorString(ce); return GF_ECUDA; }
+    if (fr != CUFFT_SUCCESS) { eng->err = "demag tables: cuFFT error " + std::to_string((int)fr); return GF_ECUDA; }
     return GF_OK;
 }
 
@@ -1223,6 +1268,7 @@ int initial_state(gf_engine* eng, const std::string& dir) {
         std::string e = read_restart(dir + "/Estat.in", d.nx, d.ny, d.nz, 3, buf);
         if (!e.empty()) { eng->err = e; return GF_EIO; }
         GF_TRY(upload_vec(eng, eng->Estat, buf, n));
+        eng->P.estat = 1;
     }
     if (d.read_Hext_nonunif) {
         for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
@@ -1489,7 +1535,9 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     }
     if (d.elastodynamics)
         for (int a = 0; a < 9; a++) GF_TRY(dalloc_r(eng, &eng->fg[a], (size_t)n));
-    if (d.elastodynamics && P.elasto_on && (P.fm || P.afm || P.fe))
+    // the crystal-frame cell strain the elastic tile hands to the LLG kernels
+    // and to the FP64 TDGL kernel
+    if (d.elastodynamics && P.elasto_on && (P.fm || P.afm || (P.fe && !eng->mixed)))
         for (int a = 0; a < 6; a++) GF_TRY(dalloc_r(eng, &eng->strain_c[a], (size_t)n));
     if (d.elastodynamics) GF_TRY(setup_elastic_tile(eng));
     if (d.elastodynamics) {
@@ -1517,6 +1565,22 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     if (!d.in_Hstat) GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(eng->stream));
     return GF_OK;
+}
+
+// the captured step graphs hold Params by value: drop them after a change
+void invalidate_graphs(gf_engine* eng) {
+    eng->graphs_ready = false;
+    for (int p = 0; p < 2; p++) {
+        if (eng->gexec[p]) { cudaGraphExecDestroy(eng->gexec[p]); eng->gexec[p] = nullptr; }
+        if (eng->graph[p]) { cudaGraphDestroy(eng->graph[p]); eng->graph[p] = nullptr; }
+    }
+}
+
+// E_stat stops being known to be +0 everywhere (the TDGL kernel then reads it)
+void mark_estat(gf_engine* eng) {
+    if (eng->P.estat || !eng->Estat[0]) return;
+    eng->P.estat = 1;
+    invalidate_graphs(eng);
 }
 
 int ensure_graphs(gf_engine* eng) {
@@ -1782,6 +1846,7 @@ static int copy_field(gf_engine* eng, int field, double* buf, size_t count, bool
     for (long l : lens) total += (size_t)l;
     if (count != total) { eng->err = "field " + std::to_string(field) + " holds " + std::to_string(total) + " doubles, caller gave " + std::to_string(count); return GF_EINVAL; }
     if (!to_host_or_dev_out && !writable) { eng->err = "field is read-only"; return GF_EINVAL; }
+    if (!to_host_or_dev_out && field == GF_FIELD_ESTAT) mark_estat(eng);
     const bool convert = eng->mixed && native;   // FP32 state <-> FP64 caller buffer through the scratch buffer
     size_t off = 0;
     for (size_t a = 0; a < ptrs.size(); a++) {
@@ -1817,13 +1882,27 @@ int gf_download(gf_engine* e, int field, double* host, size_t count) {
     return copy_field(e, field, host, count, true, cudaMemcpyDeviceToHost, true);
 }
 
+// A magnetisation given before the first step stands for the restart file the
+// reference reads at set-up (m.in, m_AFM.in): the static field it computes
+// from it before the time loop (main.cpp:135-146) is formed again from the
+// uploaded state, unless the deck supplies Hstat.in.
+static int after_upload(gf_engine* eng, int field) {
+    GF_TRY(replicate_state(eng));
+    const bool mag = field == GF_FIELD_M || field == GF_FIELD_M_AFM1 || field == GF_FIELD_M_AFM2;
+    if (mag && eng->steps_done == 0 && !eng->deck.in_Hstat) {
+        GF_TRY(static_field_now(eng));
+        GF_CU(cudaStreamSynchronize(eng->stream));
+    }
+    return GF_OK;
+}
+
 int gf_upload(gf_engine* e, int field, const double* host, size_t count) {
     GF_TRY(check(e));
     gf_engine* eng = e;
     if (!host) { eng->err = "null buffer"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
     GF_TRY(copy_field(e, field, const_cast<double*>(host), count, false, cudaMemcpyHostToDevice, true));
-    return replicate_state(e);
+    return after_upload(e, field);
 }
 
 int gf_download_device(gf_engine* e, int field, double* dev, size_t count) {
@@ -1840,7 +1919,7 @@ int gf_upload_device(gf_engine* e, int field, const double* dev, size_t count) {
     if (!dev) { eng->err = "null buffer"; return GF_EINVAL; }
     GF_CU(cudaSetDevice(eng->device));
     GF_TRY(copy_field(e, field, const_cast<double*>(dev), count, false, cudaMemcpyDeviceToDevice, false));
-    return replicate_state(e);
+    return after_upload(e, field);
 }
 
 // ---------------------------------------------------------------------------
@@ -1939,6 +2018,7 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
         const double tol = d.elec_tol > 0. ? d.elec_tol : 1e-12;
         eng->elec_iters = limit;
         eng->elec_on = true;
+        mark_estat(eng);
         eng->elec_per_stage = !d.em_dynamic;
         // set-up solve from the current polarisation unless Estat.in was given
         // (main.cpp:122-131); it starts from the current E_stat
@@ -2035,6 +2115,7 @@ int gf_load_state(gf_engine* e, const char* path) {
             return bad("checkpoint upload failed (device state now partly overwritten)", GF_ECUDA);
     std::fclose(f);
     eng->t_host = h.t_host; eng->presc_H = (long)h.presc_H; eng->presc_E = (long)h.presc_E;
+    mark_estat(eng);     // the file's E_stat may be nonzero
     for (int a = 0; a < 3; a++) { eng->Hext_cur[a] = h.Hext_cur[a]; eng->Eext_cur[a] = h.Eext_cur[a]; }
     const unsigned long long ctr = h.steps_done;
     GF_CU(cudaMemcpy(eng->step_ctr, &ctr, sizeof(ctr), cudaMemcpyHostToDevice));

@@ -19,6 +19,51 @@ __device__ inline bool is_fe(const DevMatT<R>* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FE);
 }
 
+// Crystal-frame cell strain of the stage displacement of cell (i,j,k)
+// (Dexx_crt ..., get_dudxyz_glb + get_Dstrain, elastic_dynamic_solver.cpp:
+// 106-227), formed from u_in directly: the face-normal gradient on each of
+// the six faces (0 on stress-free faces: a non-periodic end face, or vacuum
+// on either side), averaged per component exactly as the stored face
+// gradients are in k_elastic_tile, then rotated to the crystal frame.
+// nb = the six neighbours' cell indices (-x, +x, -y, +y, -z, +z, wrapped),
+// solid_nb = whether each neighbour is a material cell.
+template <class R>
+__device__ inline void fe_cell_strain(const Params& P, const StageIOT<R>& io, int i, int j, int k, int c,
+                                      const int nb[6], const bool solid_nb[6], bool solid, R e[6]) {
+    R g[3][2][3];   // g[d][0 / 1][a]: d u_a / d x_d on the -d / +d face
+    const int pos[3] = {i, j, k}, n[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
+    const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
+    const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
+    R u[3], un[3][6];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        u[a] = io.u_in.c[a][c];
+#pragma unroll
+        for (int f = 0; f < 6; f++) un[a][f] = io.u_in.c[a][nb[f]];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const bool fm = (pos[d] == 0 && !per[d]) || !(solid && solid_nb[2 * d]);
+        const bool fp = (pos[d] == n[d] - 1 && !per[d]) || !(solid && solid_nb[2 * d + 1]);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            g[d][0][a] = fm ? R(0.) : qdivR((u[a] - un[a][2 * d]), h[d], rh[d], rhf[d]);
+            g[d][1][a] = fp ? R(0.) : qdivR((un[a][2 * d + 1] - u[a]), h[d], rh[d], rhf[d]);
+        }
+    }
+    e[0] = (g[0][0][0] + g[0][1][0]) / R(2.);
+    e[1] = (g[1][0][1] + g[1][1][1]) / R(2.);
+    e[2] = (g[2][0][2] + g[2][1][2]) / R(2.);
+    e[3] = (g[2][0][1] + g[2][1][1] + g[1][0][2] + g[1][1][2]) / R(4.);
+    e[4] = (g[2][0][0] + g[2][1][0] + g[0][0][2] + g[0][1][2]) / R(4.);
+    e[5] = (g[1][0][0] + g[1][1][0] + g[0][0][1] + g[0][1][1]) / R(4.);
+    if (P.rot) {
+        R t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
+        rot_tensor(Tg2c<R>(P), t3, o3);
+        e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
+    }
+}
+
 // Grid: (blocks over the (j,k) plane) x (nx planes), 32-bit indices.
 #ifndef GF_FE_MINB_F32
 #define GF_FE_MINB_F32 4
@@ -62,12 +107,15 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
         for (int a = 0; a < 3; a++)
 #pragma unroll
             for (int f = 0; f < 6; f++) pn[a][f] = io.p_in.c[a][nb[f]];
-        const bool surf[6] = {(i == 0 && !P.per_x) || !fe_id(io.mid[nb[0]]),
-                              (i == nx - 1 && !P.per_x) || !fe_id(io.mid[nb[1]]),
-                              (j == 0 && !P.per_y) || !fe_id(io.mid[nb[2]]),
-                              (j == ny - 1 && !P.per_y) || !fe_id(io.mid[nb[3]]),
-                              (k == 0 && !P.per_z) || !fe_id(io.mid[nb[4]]),
-                              (k == nz - 1 && !P.per_z) || !fe_id(io.mid[nb[5]])};
+        uint8_t idn[6];
+#pragma unroll
+        for (int f = 0; f < 6; f++) idn[f] = io.mid[nb[f]];
+        const bool surf[6] = {(i == 0 && !P.per_x) || !fe_id(idn[0]),
+                              (i == nx - 1 && !P.per_x) || !fe_id(idn[1]),
+                              (j == 0 && !P.per_y) || !fe_id(idn[2]),
+                              (j == ny - 1 && !P.per_y) || !fe_id(idn[3]),
+                              (k == 0 && !P.per_z) || !fe_id(idn[4]),
+                              (k == nz - 1 && !P.per_z) || !fe_id(idn[5])};
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
         const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
         R lap[3];   // sum of the three second derivatives per component
@@ -93,9 +141,20 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
             // dynamic strain and eigenstrain of the stage state, crystal frame
             // (Dexx_crt, Dexx0_crt: ferroelectric_solver.cpp:624-652)
             if (P.elastic) {
-                // written by k_elastic_tile earlier in the same stage
-                exx = io.strain_c[0][c]; eyy = io.strain_c[1][c]; ezz = io.strain_c[2][c];
-                eyz = io.strain_c[3][c]; exz = io.strain_c[4][c]; exy = io.strain_c[5][c];
+                if constexpr (is_mixed<R>::value) {
+                    // mixed form: from the stage displacement (the values
+                    // k_elastic_tile forms), 12 bytes of u instead of 24 of strain
+                    const bool solid_nb[6] = {idn[0] != 0, idn[1] != 0, idn[2] != 0, idn[3] != 0, idn[4] != 0, idn[5] != 0};
+                    R e[6];
+                    fe_cell_strain(P, io, i, j, k, c, nb, solid_nb, true, e);
+                    exx = e[0]; eyy = e[1]; ezz = e[2]; eyz = e[3]; exz = e[4]; exy = e[5];
+                } else {
+                    // FP64: written by k_elastic_tile earlier in the same stage
+                    // (forming it here costs the FP64 kernel more in registers
+                    // and latency than the 48 bytes it saves)
+                    exx = io.strain_c[0][c]; eyy = io.strain_c[1][c]; ezz = io.strain_c[2][c];
+                    eyz = io.strain_c[3][c]; exz = io.strain_c[4][c]; exy = io.strain_c[5][c];
+                }
             }
             if (P.elasto_back) {
                 R e0[6];
@@ -153,8 +212,13 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
 
         const StageDrive& dr = stage_drive(io, S);
         const R g[3] = {gx, gy, gz};
-        for (int a = 0; a < 3; a++)
-            dq[a] = g[a] + fm * (-R(1.) * mt.G11 * lap[a] - io.Estat.c[a][c] - R(dr.Eext[a])) + mt.fe_damp * io.q_in.c[a][c];
+        // E_stat is read only where it may be nonzero: x - (+0) is x in
+        // every bit, so leaving out an all-zero field changes nothing
+        for (int a = 0; a < 3; a++) {
+            R inner = -R(1.) * mt.G11 * lap[a];
+            if (P.estat) inner = inner - io.Estat.c[a][c];
+            dq[a] = g[a] + fm * (inner - R(dr.Eext[a])) + mt.fe_damp * io.q_in.c[a][c];
+        }
 
         if (P.em_back_P) {
             // cell-centred Maxwell E of the stage state (EMdynamic_solver.cpp:3813-3826)

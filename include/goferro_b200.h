@@ -151,7 +151,10 @@ int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count);
 
 /* Copy a field to / from host memory (count doubles, component-major).
  * Replace the reference's copy*_from_device and input_* restart readers.
- * Synchronous. */
+ * A magnetisation (m, m_AFM1, m_AFM2) uploaded before the first step stands
+ * for the restart file read at set-up: the static magnetic field is formed
+ * again from it, as the reference computes it before its time loop
+ * (main.cpp:135-146), unless the deck supplies Hstat.in.  Synchronous. */
 int gf_download(gf_engine* e, int field, double* host, size_t count);
 int gf_upload(gf_engine* e, int field, const double* host, size_t count);
 
