@@ -14,7 +14,16 @@ from GO-Ferro's own solver, serial on the host) cover:
 FP64 form: every traced observable (<m>, <p>, <u>, the probed cell's E and H)
 within 1e-10 of the reference relative to that observable's largest
 component over the trace, and the committed final fields within 1e-10 of
-their largest component.  FP32 mixed form: the same traces within 1e-5.
+their largest component.
+
+FP32 mixed form: the same traces within 1e-5 relative to the magnitude of
+the field each observable samples: for <m>, <p> and <u> the largest cell
+value of the field (the average of +-1e-3 random P is ~1e-5, and an FP32
+field's rounding is relative to its cells, not to their mean); for the probed
+E and H the electromagnetic field's scale max(|E|, eta0 |H|) over the trace
+(in a quasi-static E of 1e6 V/m the probed H is a few A/m, a small
+difference of FP32 E values).  The error relative to each observable's own
+trace magnitude is printed beside it.
 """
 import json
 import os
@@ -28,6 +37,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CONFIGS = json.load(open(os.path.join(GOLDEN, "configs.json")))
 TOL = {"fp64": 1e-10, "mixed": 1e-5}
+ETA0 = 376.730313668
 
 # trace columns of each vector observable (oracle/refrun.TRACE_COLS)
 GROUPS = {"m": (1, 4), "m_afm1": (4, 7), "m_afm2": (7, 10), "p": (10, 13), "u": (13, 16), "E": (16, 19), "H": (19, 22)}
@@ -64,6 +74,24 @@ def engine_trace(eng, steps, every, probe):
     return np.array(rows)
 
 
+def field_scale_errors(mine, ref, field_max):
+    """{observable: max error relative to the sampled field's magnitude}"""
+    out = {}
+    em = float(np.max(np.maximum(np.max(np.abs(ref[:, 16:19]), axis=1), ETA0 * np.max(np.abs(ref[:, 19:22]), axis=1))))
+    for name, (a, b) in GROUPS.items():
+        own = float(np.max(np.abs(ref[:, a:b])))
+        if own == 0.0:
+            continue
+        if name in ("E",):
+            scale = em
+        elif name == "H":
+            scale = em / ETA0
+        else:
+            scale = max(own, field_max.get(name, 0.0))
+        out[name] = float(np.max(np.abs(mine[:, a:b] - ref[:, a:b]))) / scale
+    return out
+
+
 def trace_errors(mine, ref):
     """{observable: (max relative error, first traced step above 1e-10)}"""
     assert mine.shape == ref.shape, (mine.shape, ref.shape)
@@ -98,9 +126,19 @@ def test_config_matches_reference(gf, tmp_path, name, form):
             eng.upload(k, v)
         mine = engine_trace(eng, steps, every, tuple(probe) if probe else (0, 0, 0))
         errs = trace_errors(mine, ref)
-        print(name, form, {k: f"{v[0]:.2e} (first step > 1e-10: {v[1]})" for k, v in errs.items()})
-        for obs, (e, _) in errs.items():
-            assert e <= TOL[form], f"{name} {form} <{obs}>: rel err {e:.3e}"
+        print(name, form, "own scale:", {k: f"{v[0]:.2e} (first step > 1e-10: {v[1]})" for k, v in errs.items()})
+        if form == "fp64":
+            for obs, (e, _) in errs.items():
+                assert e <= TOL[form], f"{name} {form} <{obs}>: rel err {e:.3e}"
+        else:
+            fmax = {}
+            for obs, on in (("m", eng.info.fm), ("p", eng.info.fe), ("u", eng.info.elastic)):
+                if on:
+                    fmax[obs] = float(np.max(np.abs(eng.download(obs))))
+            ferr = field_scale_errors(mine, ref, fmax)
+            print(name, form, "field scale:", {k: f"{v:.2e}" for k, v in ferr.items()})
+            for obs, e in ferr.items():
+                assert e <= TOL[form], f"{name} {form} <{obs}>: error {e:.3e} of the field's magnitude"
         if form == "fp64":
             for fld, parts in FIELDS.items():
                 if parts[0] not in g.files:
