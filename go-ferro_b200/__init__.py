@@ -42,7 +42,113 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
            "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
            "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics",
-           "gf_save_state", "gf_load_state"]
+           "gf_save_state", "gf_load_state", "gf_create", "gf_set_table", "gf_stage_begin", "gf_stage_commit",
+           "gf_static_solve"]
+
+TABLE = {"Hext": 0, "Eext": 1}      # GF_TABLE_HEXT, GF_TABLE_EEXT
+STATIC = {"magnetic": 0, "electric": 1}   # GF_STATIC_MAGNETIC, GF_STATIC_ELECTRIC
+
+_d, _i32, _i64, _u64, _ch = ctypes.c_double, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_char
+
+
+class GFMaterialParams(ctypes.Structure):
+    """gf_material_params: one material as read from materials.in."""
+    _fields_ = [("c11", _d), ("c12", _d), ("c44", _d), ("density", _d), ("elast_mass_damping", _d),
+                ("elast_stiff_damping", _d), ("if_FM", _i32), ("Ms", _d), ("gyro", _d), ("FM_damping", _d),
+                ("anisotropy_type", _i32), ("K1", _d), ("K2", _d), ("Aex", _d), ("iDMI", _d), ("lamda100", _d),
+                ("lamda111", _d), ("if_AFM", _i32), ("Ms_AFM", _d * 2), ("gyro_AFM", _d * 2), ("damping_AFM", _d * 2),
+                ("K1_AFM", _d * 2), ("uniaxis_AFM", _d * 3), ("Aex_AFM", _d * 2), ("J_AFM", _d),
+                ("lamda100_AFM", _d * 2), ("lamda111_AFM", _d * 2), ("if_spin_pump", _i32), ("spin_hall_angle", _d),
+                ("spin_mix_cond", _d), ("spin_diffus_length", _d), ("if_FE", _i32), ("FE_mass", _d), ("FE_damping", _d),
+                ("a1", _d), ("a11", _d), ("a12", _d), ("a111", _d), ("a112", _d), ("a123", _d), ("a1111", _d),
+                ("a1112", _d), ("a1122", _d), ("a1123", _d), ("G11", _d), ("Q11", _d), ("Q12", _d), ("Q44", _d),
+                ("f11", _d), ("f12", _d), ("f44", _d), ("if_PEC", _i32), ("r_permittivity", _d), ("conductivity", _d),
+                ("comp_n", _d * 3), ("omega_plasma_n", _d * 3), ("tao_e_n", _d * 3)]
+
+
+class GFRunParams(ctypes.Structure):
+    """gf_run_params: the parsed system_setting.in values a run needs."""
+    _fields_ = [("nx", _i64), ("ny", _i64), ("nz", _i64), ("dx", _d), ("dy", _d), ("dz", _d),
+                ("periodicX", _i32), ("periodicY", _i32), ("periodicZ", _i32),
+                ("step", _u64), ("dt", _d), ("if_OrientRotate", _i32), ("Tg2c", (_d * 3) * 3),
+                ("theta_mag", _d), ("phi_mag", _d), ("px_init", _d), ("py_init", _d), ("pz_init", _d),
+                ("Hext_stat", _d * 3), ("Hext_altr", _d * 3), ("H_altr_freq", _d * 3), ("if_prescribe_Hext", _i32),
+                ("Eext_stat", _d * 3), ("Eext_altr", _d * 3), ("E_altr_freq", _d * 3), ("if_prescribe_Eext", _i32),
+                ("if_magnetostatics", _i32), ("if_mag_1Dmodel", _i32), ("if_demag_factor", _i32), ("demag_fac", _d * 3),
+                ("if_elec_1Dmodel", _i32), ("if_elec_1D_compensate", _i32), ("scale_elec", _d),
+                ("elec_solver_limit", _i32), ("elec_solver_tol", _d),
+                ("if_EMdynamic", _i32), ("if_input_planeEM_E", _i32), ("planeEM_E", _d * 3), ("planeEM_E_freq", _d * 3),
+                ("if_EM_fromP", _i32), ("if_EM_fromM", _i32), ("if_EM_backaction_on_P", _i32),
+                ("if_EM_backaction_on_M", _i32), ("if_1D_ABC", _i32), ("if_1D_ABC_ELAST_onlytop", _i32),
+                ("if_1D_ABC_EM_onlytop", _i32), ("weighting_factor_fourth_Liao", _d), ("if_PEC_XY", _i32),
+                ("if_PEC_Z", _i32), ("if_Jf_input", _i32), ("Jfin_lo", _i64 * 3), ("Jfin_hi", _i64 * 3),
+                ("Jf_input_type", _i32), ("Jf_input_component", _ch), ("pad_", _ch * 3), ("Jf_input_amp", _d),
+                ("Jf_input_freq", _d), ("Jf_input_sigma", _d), ("num_Jf_cycles", _u64),
+                ("if_elastodynamics", _i32), ("if_elasto_backaction_from_pORm", _i32), ("if_elasto_on_pORm", _i32),
+                ("if_gaussian_strain_pulse", _i32), ("input_strain_type", _i32), ("input_strain_sourcez", _i32),
+                ("input_strain_component", _ch), ("pad2_", _ch * 7), ("sigma_gauss", _d), ("amplitude_gauss", _d),
+                ("num_strain_cycles", _u64), ("if_elastostatic", _i32), ("if_flexo", _i32), ("if_prescribed_m", _i32),
+                ("if_spin_pumping", _i32)]
+
+
+def material_params(m) -> GFMaterialParams:
+    """gf_material_params of a decks.Material (the values materials.in holds)."""
+    p = GFMaterialParams()
+    p.c11, p.c12, p.c44, p.density = m.c11, m.c12, m.c44, m.density
+    p.elast_mass_damping, p.elast_stiff_damping = m.mass_damping, m.stiff_damping
+    p.if_FM, p.Ms, p.gyro, p.FM_damping = int(m.fm), m.Ms, m.gyro, m.alpha
+    p.anisotropy_type, p.K1, p.K2, p.Aex, p.iDMI = int(m.aniso_type), m.K1, m.K2, m.Aex, m.iDMI
+    p.lamda100, p.lamda111 = m.lam100, m.lam111
+    p.if_AFM = int(m.afm)
+    p.Ms_AFM[:] = list(m.afm_Ms); p.gyro_AFM[:] = list(m.afm_gyro); p.damping_AFM[:] = list(m.afm_alpha)
+    p.K1_AFM[:] = list(m.afm_K1); p.uniaxis_AFM[:] = list(m.afm_axis); p.Aex_AFM[:] = list(m.afm_Aex)
+    p.J_AFM = m.J_AFM
+    p.lamda100_AFM[:] = list(m.afm_lam100); p.lamda111_AFM[:] = list(m.afm_lam111)
+    p.if_spin_pump = int(m.spin_pump)
+    p.spin_hall_angle, p.spin_mix_cond, p.spin_diffus_length = m.spin
+    p.if_FE, p.FE_mass, p.FE_damping = int(m.fe), m.fe_mass, m.fe_damping
+    p.a1, p.a11, p.a12, p.a111, p.a112, p.a123 = m.a1, m.a11, m.a12, m.a111, m.a112, m.a123
+    p.a1111, p.a1112, p.a1122, p.a1123 = m.a1111, m.a1112, m.a1122, m.a1123
+    p.G11, p.Q11, p.Q12, p.Q44, p.f11, p.f12, p.f44 = m.G11, m.Q11, m.Q12, m.Q44, m.f11, m.f12, m.f44
+    p.if_PEC, p.r_permittivity, p.conductivity = int(m.pec), m.er, m.cond
+    for k in range(3):
+        p.comp_n[k], p.omega_plasma_n[k], p.tao_e_n[k] = m.drude[k]
+    return p
+
+
+def run_params(d) -> GFRunParams:
+    """gf_run_params of a decks.Deck (the values system_setting.in holds)."""
+    r = GFRunParams()
+    r.nx, r.ny, r.nz, r.dx, r.dy, r.dz = d.nx, d.ny, d.nz, d.dx, d.dy, d.dz
+    r.periodicX, r.periodicY, r.periodicZ = (int(x) for x in d.periodic)
+    r.step, r.dt, r.if_OrientRotate = int(d.steps), d.dt, 0
+    for i in range(3):
+        for j in range(3):
+            r.Tg2c[i][j] = 1.0 if i == j else 0.0
+    r.theta_mag, r.phi_mag = d.theta_mag, d.phi_mag
+    r.px_init, r.py_init, r.pz_init = d.p_init
+    r.Hext_stat[:] = list(d.Hext_stat); r.Hext_altr[:] = list(d.Hext_altr); r.H_altr_freq[:] = list(d.H_altr_freq)
+    r.if_prescribe_Hext = int(d.Hext_table is not None)
+    r.Eext_stat[:] = list(d.Eext_stat); r.Eext_altr[:] = list(d.Eext_altr); r.E_altr_freq[:] = list(d.E_altr_freq)
+    r.if_magnetostatics, r.if_mag_1Dmodel, r.if_demag_factor = int(d.magnetostatics), int(d.mag_1D), int(d.demag_factor)
+    r.demag_fac[:] = list(d.demag_fac)
+    r.scale_elec, r.elec_solver_limit, r.elec_solver_tol = d.scale_elec, int(d.elec_limit), d.elec_tol
+    r.if_EMdynamic, r.if_input_planeEM_E = int(d.em), int(d.planeEM)
+    r.planeEM_E[:] = list(d.planeEM_E); r.planeEM_E_freq[:] = list(d.planeEM_freq)
+    r.if_EM_fromP, r.if_EM_fromM = int(d.em_fromP), int(d.em_fromM)
+    r.if_EM_backaction_on_P, r.if_EM_backaction_on_M = int(d.em_back_P), int(d.em_back_M)
+    r.if_1D_ABC, r.if_1D_ABC_ELAST_onlytop, r.if_1D_ABC_EM_onlytop = int(d.abc_1D), int(d.abc_elast_onlytop), int(d.abc_em_onlytop)
+    r.weighting_factor_fourth_Liao = d.liao_w
+    r.if_Jf_input = int(d.jf)
+    r.Jfin_lo[:] = list(d.jf_lo); r.Jfin_hi[:] = list(d.jf_hi)
+    r.Jf_input_type, r.Jf_input_component = int(d.jf_type), d.jf_comp.encode()
+    r.Jf_input_amp, r.Jf_input_freq, r.Jf_input_sigma, r.num_Jf_cycles = d.jf_amp, d.jf_freq, d.jf_sigma, int(d.jf_cycles)
+    r.if_elastodynamics, r.if_elasto_backaction_from_pORm, r.if_elasto_on_pORm = int(d.elastic), int(d.elasto_back), int(d.elasto_on)
+    r.if_gaussian_strain_pulse, r.input_strain_type, r.input_strain_sourcez = int(d.strain_pulse), int(d.strain_type), int(d.strain_z)
+    r.input_strain_component = d.strain_comp.encode()
+    r.sigma_gauss, r.amplitude_gauss, r.num_strain_cycles = d.sigma_gauss, d.amp_gauss, int(d.strain_cycles)
+    r.if_spin_pumping = int(d.spin_pumping)
+    return r
 
 
 class GFInfo(ctypes.Structure):
@@ -126,6 +232,12 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_batch_last_error.restype = ctypes.c_char_p
     lib.gf_batch_destroy.argtypes = [vp]
     lib.gf_batch_destroy.restype = None
+    lib.gf_create.argtypes = [ctypes.POINTER(GFRunParams), ctypes.POINTER(GFMaterialParams), c_int,
+                              ctypes.POINTER(ctypes.c_uint32), c_int, c_int, ctypes.POINTER(vp)]
+    lib.gf_set_table.argtypes = [vp, c_int, c_dbl_p, c_dbl_p, ctypes.c_int64]
+    lib.gf_stage_begin.argtypes = [vp, c_int]
+    lib.gf_stage_commit.argtypes = [vp, c_int]
+    lib.gf_static_solve.argtypes = [vp, c_int]
     if path is None:
         _lib = lib
     return lib
@@ -137,14 +249,42 @@ class Engine:
     precision: "fp64" (the parity form) or "mixed" (FP32 state and stencils
     with compensated RK4 accumulation; FP64 at the interface)."""
 
-    def __init__(self, deck_dir: str, device: int = -1, lib: Optional[ctypes.CDLL] = None, precision: str = "fp64"):
+    def __init__(self, deck_dir: Optional[str], device: int = -1, lib: Optional[ctypes.CDLL] = None,
+                 precision: str = "fp64", _handle=None):
         self.lib = lib or load_library()
-        h = ctypes.c_void_p()
-        rc = self.lib.gf_create_from_deck_ex(os.fsencode(deck_dir), device, PRECISION[precision], ctypes.byref(h))
-        if rc != GF_OK:
-            raise GFError(rc, self.lib.gf_last_error(None).decode())
+        if _handle is not None:
+            h = _handle
+        else:
+            h = ctypes.c_void_p()
+            rc = self.lib.gf_create_from_deck_ex(os.fsencode(deck_dir), device, PRECISION[precision], ctypes.byref(h))
+            if rc != GF_OK:
+                raise GFError(rc, self.lib.gf_last_error(None).decode())
         self.h = h
         self.info = self.get_info()
+
+    @classmethod
+    def from_params(cls, deck, device: int = -1, precision: str = "fp64", lib: Optional[ctypes.CDLL] = None):
+        """Engine from a decks.Deck's values through gf_create (no files):
+        the run and material structs, the per-cell ids, then the deck's
+        restart arrays through gf_upload and its H table through gf_set_table."""
+        lib = lib or load_library()
+        run = run_params(deck)
+        mats = (GFMaterialParams * len(deck.materials))(*[material_params(m) for m in deck.materials])
+        mc = np.ascontiguousarray(deck.material_cell().ravel(), dtype=np.uint32)
+        h = ctypes.c_void_p()
+        rc = lib.gf_create(ctypes.byref(run), mats, len(deck.materials), mc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                           device, PRECISION[precision], ctypes.byref(h))
+        if rc != GF_OK:
+            raise GFError(rc, lib.gf_last_error(None).decode())
+        eng = cls(None, lib=lib, _handle=h)
+        if deck.Hext_table is not None:
+            eng.set_table("Hext", deck.Hext_table[:, 0], deck.Hext_table[:, 1:4])
+        for name, arr in (("m", deck.m0), ("m_afm1", None if deck.afm0 is None else deck.afm0[:3]),
+                          ("m_afm2", None if deck.afm0 is None else deck.afm0[3:]), ("p", deck.p0), ("q", deck.q0),
+                          ("u", deck.u0), ("v", deck.v0)):
+            if arr is not None:
+                eng.upload(name, arr)
+        return eng
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc: int) -> None:
@@ -233,6 +373,20 @@ class Engine:
 
     def check_finite(self) -> None:
         self._check(self.lib.gf_check_finite(self.h))
+
+    def set_table(self, which: str, times: np.ndarray, xyz: np.ndarray) -> None:
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        v = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self._check(self.lib.gf_set_table(self.h, TABLE[which], _dp(t), _dp(v), t.size))
+
+    def stage_begin(self, stage: int) -> None:
+        self._check(self.lib.gf_stage_begin(self.h, int(stage)))
+
+    def stage_commit(self, stage: int) -> None:
+        self._check(self.lib.gf_stage_commit(self.h, int(stage)))
+
+    def static_solve(self, which: str) -> None:
+        self._check(self.lib.gf_static_solve(self.h, STATIC.get(which, -1)))
 
     def stream(self) -> int:
         return self.lib.gf_stream(self.h) or 0

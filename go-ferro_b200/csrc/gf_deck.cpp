@@ -193,6 +193,25 @@ std::string read_table(const std::string& path, long n, std::vector<double>& t, 
     return "";
 }
 
+// counts and flags set_global derives from the materials and the cells
+// (global.cpp:85-118), and the demag factors normalised to sum -1
+// (global.cpp:271-275)
+void finish_deck(Deck& d) {
+    for (const Material& m : d.mats) {
+        d.any_fm |= m.fm; d.any_fe |= m.fe; d.any_afm |= m.afm; d.any_pec |= m.pec;
+    }
+    d.NFM = d.NFE = d.NAFM = 0;
+    for (uint8_t id : d.material_cell)
+        if (id) { const Material& m = d.mats[id - 1]; d.NFM += m.fm; d.NFE += m.fe; d.NAFM += m.afm; }
+    d.periodic_all = d.per_x && d.per_y && d.per_z;
+
+    // demag factors normalised to sum -1 (global.cpp:271-275)
+    {
+        double norm = d.demag_fac[0] + d.demag_fac[1] + d.demag_fac[2];
+        for (int i = 0; i < 3; i++) d.demag_fac[i] = d.demag_fac[i] / norm * -1.;
+    }
+}
+
 }  // namespace
 
 std::string read_deck(const std::string& dir, Deck& d) {
@@ -320,23 +339,110 @@ std::string read_deck(const std::string& dir, Deck& d) {
         }
     }
 
-    for (const Material& m : d.mats) {
-        d.any_fm |= m.fm; d.any_fe |= m.fe; d.any_afm |= m.afm; d.any_pec |= m.pec;
-    }
-    d.NFM = d.NFE = d.NAFM = 0;
-    for (uint8_t id : d.material_cell)
-        if (id) { const Material& m = d.mats[id - 1]; d.NFM += m.fm; d.NFE += m.fe; d.NAFM += m.afm; }
-    d.periodic_all = d.per_x && d.per_y && d.per_z;
-
-    // demag factors normalised to sum -1 (global.cpp:271-275)
-    {
-        double norm = d.demag_fac[0] + d.demag_fac[1] + d.demag_fac[2];
-        for (int i = 0; i < 3; i++) d.demag_fac[i] = d.demag_fac[i] / norm * -1.;
-    }
+    finish_deck(d);
     if (d.prescribe_E) { e = read_table(dir + "/Eext.in", d.n_prescribe_E, d.tE, d.Ex, d.Ey, d.Ez); if (!e.empty()) return e; }
     if (d.prescribe_H) { e = read_table(dir + "/Hext.in", d.n_prescribe_H, d.tH, d.Hx, d.Hy, d.Hz); if (!e.empty()) return e; }
     return "";
 }
+
+std::string deck_from_params(const gf_run_params& r, const gf_material_params* mats, int nmat,
+                             const uint32_t* material_cell, Deck& d) {
+    if (r.nx < 1 || r.ny < 1 || r.nz < 1) return "grid dimensions must be positive";
+    if (!(r.dx > 0. && r.dy > 0. && r.dz > 0.)) return "cell sizes must be positive";
+    if (nmat < 1 || nmat > 255) return "n_materials must be 1..255";
+    if (!mats || !material_cell) return "null materials or material_cell";
+    d = Deck();
+    d.nx = r.nx; d.ny = r.ny; d.nz = r.nz;
+    d.dx = r.dx; d.dy = r.dy; d.dz = r.dz;
+    d.per_x = r.periodicX != 0; d.per_y = r.periodicY != 0; d.per_z = r.periodicZ != 0;
+    d.nx_work = r.nx; d.ny_work = r.ny;
+    d.steps = r.step; d.dt = r.dt;
+    d.num_materials = (unsigned)nmat;
+    d.orient_rotate = r.if_OrientRotate != 0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) d.Tg2c[i][j] = r.Tg2c[i][j];
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) d.Tc2g[i][j] = d.Tg2c[j][i];
+    d.theta_mag = r.theta_mag; d.phi_mag = r.phi_mag;
+    d.px_init = r.px_init; d.py_init = r.py_init; d.pz_init = r.pz_init;
+    for (int a = 0; a < 3; a++) {
+        d.Hext_stat[a] = r.Hext_stat[a]; d.Hext_altr[a] = r.Hext_altr[a]; d.H_altr_freq[a] = r.H_altr_freq[a];
+        d.Eext_stat[a] = r.Eext_stat[a]; d.Eext_altr[a] = r.Eext_altr[a]; d.E_altr_freq[a] = r.E_altr_freq[a];
+        d.demag_fac[a] = r.demag_fac[a];
+        d.planeEM_E[a] = r.planeEM_E[a]; d.planeEM_freq[a] = r.planeEM_E_freq[a];
+    }
+    d.prescribe_H = r.if_prescribe_Hext != 0; d.n_prescribe_H = 0;
+    d.prescribe_E = r.if_prescribe_Eext != 0; d.n_prescribe_E = 0;
+    d.magnetostatics = r.if_magnetostatics != 0; d.mag_1D = r.if_mag_1Dmodel != 0;
+    d.demag_factor = r.if_demag_factor != 0;
+    d.elec_1D = r.if_elec_1Dmodel != 0; d.elec_1D_comp = r.if_elec_1D_compensate != 0;
+    d.scale_elec = r.scale_elec; d.elec_limit = (unsigned)(r.elec_solver_limit > 0 ? r.elec_solver_limit : 0);
+    d.elec_tol = r.elec_solver_tol;
+    d.em_dynamic = r.if_EMdynamic != 0; d.planeEM = r.if_input_planeEM_E != 0;
+    d.em_fromP = r.if_EM_fromP != 0; d.em_fromM = r.if_EM_fromM != 0;
+    d.em_back_P = r.if_EM_backaction_on_P != 0; d.em_back_M = r.if_EM_backaction_on_M != 0;
+    d.abc_1D = r.if_1D_ABC != 0; d.abc_elast_onlytop = r.if_1D_ABC_ELAST_onlytop != 0;
+    d.abc_em_onlytop = r.if_1D_ABC_EM_onlytop != 0; d.liao_w = r.weighting_factor_fourth_Liao;
+    d.pec_xy = r.if_PEC_XY != 0; d.pec_z = r.if_PEC_Z != 0;
+    d.jf_input = r.if_Jf_input != 0;
+    if (d.jf_input) {
+        for (int a = 0; a < 3; a++)
+            if (r.Jfin_lo[a] < 0 || r.Jfin_hi[a] < r.Jfin_lo[a]) return "bad J_f box";
+        d.jf_i0 = (unsigned long)r.Jfin_lo[0]; d.jf_j0 = (unsigned long)r.Jfin_lo[1]; d.jf_k0 = (unsigned long)r.Jfin_lo[2];
+        d.jf_i1 = (unsigned long)r.Jfin_hi[0]; d.jf_j1 = (unsigned long)r.Jfin_hi[1]; d.jf_k1 = (unsigned long)r.Jfin_hi[2];
+    }
+    d.jf_type = (unsigned)(r.Jf_input_type > 0 ? r.Jf_input_type : 0);
+    d.jf_comp = r.Jf_input_component ? r.Jf_input_component : 'x';
+    d.jf_amp = r.Jf_input_amp; d.jf_freq = r.Jf_input_freq; d.jf_sigma = r.Jf_input_sigma; d.jf_cycles = r.num_Jf_cycles;
+    d.elastodynamics = r.if_elastodynamics != 0; d.elasto_back = r.if_elasto_backaction_from_pORm != 0;
+    d.elasto_on = r.if_elasto_on_pORm != 0;
+    d.strain_pulse = r.if_gaussian_strain_pulse != 0;
+    d.strain_type = (unsigned)(r.input_strain_type > 0 ? r.input_strain_type : 0);
+    d.strain_z = (unsigned)(r.input_strain_sourcez > 0 ? r.input_strain_sourcez : 0);
+    d.strain_comp = r.input_strain_component ? r.input_strain_component : 'x';
+    d.sigma_gauss = r.sigma_gauss; d.amp_gauss = r.amplitude_gauss; d.strain_cycles = r.num_strain_cycles;
+    d.elastostatic = r.if_elastostatic != 0; d.flexo = r.if_flexo != 0; d.prescribed_m = r.if_prescribed_m != 0;
+    d.spin_pumping = r.if_spin_pumping != 0;
+
+    d.mats.assign((size_t)nmat, Material());
+    for (int i = 0; i < nmat; i++) {
+        const gf_material_params& s = mats[i];
+        Material& m = d.mats[i];
+        m.c11 = s.c11; m.c12 = s.c12; m.c44 = s.c44; m.density = s.density;
+        m.mass_damping = s.elast_mass_damping; m.stiff_damping = s.elast_stiff_damping;
+        m.fm = s.if_FM != 0; m.Ms = s.Ms; m.gyro = s.gyro; m.alpha = s.FM_damping;
+        m.aniso_type = (unsigned)(s.anisotropy_type > 0 ? s.anisotropy_type : 0);
+        m.K1 = s.K1; m.K2 = s.K2; m.Aex = s.Aex; m.iDMI = s.iDMI; m.lam100 = s.lamda100; m.lam111 = s.lamda111;
+        m.afm = s.if_AFM != 0;
+        m.Ms1 = s.Ms_AFM[0]; m.Ms2 = s.Ms_AFM[1]; m.gyro1 = s.gyro_AFM[0]; m.gyro2 = s.gyro_AFM[1];
+        m.alpha1 = s.damping_AFM[0]; m.alpha2 = s.damping_AFM[1]; m.K1_1 = s.K1_AFM[0]; m.K1_2 = s.K1_AFM[1];
+        {
+            // read.cpp:149-153
+            const double norm = std::sqrt(s.uniaxis_AFM[0] * s.uniaxis_AFM[0] + s.uniaxis_AFM[1] * s.uniaxis_AFM[1] +
+                                          s.uniaxis_AFM[2] * s.uniaxis_AFM[2]);
+            for (int a = 0; a < 3; a++) m.uaxis[a] = s.uniaxis_AFM[a] / norm;
+        }
+        m.Aex1 = s.Aex_AFM[0]; m.Aex2 = s.Aex_AFM[1]; m.J_AFM = s.J_AFM;
+        m.lam100_1 = s.lamda100_AFM[0]; m.lam100_2 = s.lamda100_AFM[1];
+        m.lam111_1 = s.lamda111_AFM[0]; m.lam111_2 = s.lamda111_AFM[1];
+        m.spin_pump = s.if_spin_pump != 0;
+        m.sh_angle = s.spin_hall_angle; m.sh_mixcond = s.spin_mix_cond; m.sh_difflen = s.spin_diffus_length;
+        m.fe = s.if_FE != 0; m.fe_mass = s.FE_mass; m.fe_damping = s.FE_damping;
+        m.a1 = s.a1; m.a11 = s.a11; m.a12 = s.a12; m.a111 = s.a111; m.a112 = s.a112; m.a123 = s.a123;
+        m.a1111 = s.a1111; m.a1112 = s.a1112; m.a1122 = s.a1122; m.a1123 = s.a1123;
+        m.G11 = s.G11; m.Q11 = s.Q11; m.Q12 = s.Q12; m.Q44 = s.Q44; m.f11 = s.f11; m.f12 = s.f12; m.f44 = s.f44;
+        m.pec = s.if_PEC != 0; m.er = s.r_permittivity; m.cond = s.conductivity;
+        for (int k = 0; k < 3; k++) { m.comp[k] = s.comp_n[k]; m.wp[k] = s.omega_plasma_n[k]; m.tau[k] = s.tao_e_n[k]; }
+        derive_material(m, d.Tc2g);
+    }
+    d.material_cell.assign((size_t)d.n(), 0);
+    for (long c = 0; c < d.n(); c++) {
+        if (material_cell[c] > (uint32_t)nmat) return "material_cell id exceeds n_materials";
+        d.material_cell[(size_t)c] = (uint8_t)material_cell[c];
+    }
+    finish_deck(d);
+    return "";
+}
+
 
 std::string read_restart(const std::string& path, long nx, long ny, long nz, int ncomp, std::vector<double>* comps) {
     std::ifstream f(path);

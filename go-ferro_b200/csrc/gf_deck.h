@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include "../../include/goferro_b200.h"
+
 namespace gf {
 
 // One material (material.h:3-58) plus the derived constants the reference
@@ -108,6 +110,12 @@ struct Deck {
 
     long n() const { return nx * ny * nz; }
 };
+
+// Fill a Deck from the host's parsed values (gf_create): the same fields
+// and derived quantities read_deck produces from a deck directory, with no
+// restart files.  Returns an empty string on success, else a message.
+std::string deck_from_params(const gf_run_params& run, const gf_material_params* mats, int nmat,
+                             const uint32_t* material_cell, Deck& d);
 
 // Parse a deck directory.  Returns an empty string on success, else a
 // message.  Restart files are not read here (the engine reads them with

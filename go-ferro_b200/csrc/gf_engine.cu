@@ -139,6 +139,10 @@ struct gf_engine {
     StageIOT<float> iof[2][4];             // mixed form
     // launch accounting and optional per-launch timing (gf_profile_steps)
     int launches_per_step = 0;
+    // stage-level stepping (gf_stage_begin / gf_stage_commit): 0 = no step
+    // open, else the stage last committed + 1 (1..4) of the open step
+    int stage_open = 0;
+    int stage_done = 0;
     int launch_counter = 0;
     bool profiling = false;
     struct ProfRec { const char* name; cudaEvent_t a, b; };
@@ -155,6 +159,7 @@ struct gf_engine {
 // contraction (the FP64 parity kernels here must not contract).  These two
 // functions are its interface.
 int gf_mixed_enqueue_step(gf_engine* eng, int parity);                 // kernels of one step, mixed form
+int gf_mixed_enqueue_stage(gf_engine* eng, int parity, int s);         // kernels of stage s (0..3), mixed form
 int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-memory opt-in, occupancy
 int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms);          // stage-1 elastic tile, mean ms per launch
 
@@ -990,8 +995,17 @@ int enqueue_step_t(gf_engine* eng, int parity) {
 
 }  // namespace
 
+template <class R>
+int enqueue_stage_t(gf_engine* eng, int parity, int s) {
+    if (s == 0) return enqueue_stage<0, R>(eng, parity);
+    if (s == 1) return enqueue_stage<1, R>(eng, parity);
+    if (s == 2) return enqueue_stage<2, R>(eng, parity);
+    return enqueue_stage<3, R>(eng, parity);
+}
+
 #ifdef GF_MIXED_TU
 int gf_mixed_enqueue_step(gf_engine* eng, int parity) { return enqueue_step_t<float>(eng, parity); }
+int gf_mixed_enqueue_stage(gf_engine* eng, int parity, int s) { return enqueue_stage_t<float>(eng, parity, s); }
 
 int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm) {
     GF_TRY(set_elastic_smem<float>(eng, smem));
@@ -1381,17 +1395,17 @@ int setup_em_classes(gf_engine* eng) {
     return GF_OK;
 }
 
-int create(gf_engine* eng, const std::string& dir, int device, int precision) {
+// Set-up from eng->deck (filled from a deck directory or from the host's
+// parsed values); `dir` is where restart files are read from ("" = none).
+int create_from(gf_engine* eng, const std::string& dir, int device, int precision) {
     if (precision != GF_PRECISION_FP64 && precision != GF_PRECISION_MIXED_FP32) {
         eng->err = "precision must be GF_PRECISION_FP64 or GF_PRECISION_MIXED_FP32";
         return GF_EINVAL;
     }
     eng->mixed = (precision == GF_PRECISION_MIXED_FP32);
     eng->esz = eng->mixed ? sizeof(float) : sizeof(double);
-    std::string e = read_deck(dir, eng->deck);
-    if (!e.empty()) { eng->err = e; return GF_EIO; }
     const Deck& d = eng->deck;
-    e = unsupported(d);
+    std::string e = unsupported(d);
     if (!e.empty()) { eng->err = e; return GF_EUNSUPPORTED; }
 
     int ndev = 0;
@@ -1567,6 +1581,12 @@ int create(gf_engine* eng, const std::string& dir, int device, int precision) {
     return GF_OK;
 }
 
+int create(gf_engine* eng, const std::string& dir, int device, int precision) {
+    std::string e = read_deck(dir, eng->deck);
+    if (!e.empty()) { eng->err = e; return GF_EIO; }
+    return create_from(eng, dir, device, precision);
+}
+
 // the captured step graphs hold Params by value: drop them after a change
 void invalidate_graphs(gf_engine* eng) {
     eng->graphs_ready = false;
@@ -1600,7 +1620,12 @@ int ensure_graphs(gf_engine* eng) {
 }
 
 int advance(gf_engine* eng, uint64_t nsteps, bool use_graph) {
+    if (eng->stage_open) {
+        eng->err = "a step begun with gf_stage_begin is still open (commit its stages first)";
+        return GF_EINVAL;
+    }
     if (use_graph) GF_TRY(ensure_graphs(eng));
+    eng->stage_done = 0;
     uint64_t done = 0;
     while (done < nsteps) {
         const uint64_t chunk = std::min<uint64_t>(nsteps - done, (uint64_t)kDriveCap / 2);
@@ -1775,6 +1800,121 @@ int gf_advance(gf_engine* e, uint64_t nsteps) {
     gf_engine* eng = e;
     GF_CU(cudaSetDevice(eng->device));
     return advance(e, nsteps, true);
+}
+
+int gf_create(const gf_run_params* run, const gf_material_params* mats, int n_materials, const uint32_t* material_cell,
+              int device, int precision, gf_engine** out) {
+    if (!run || !mats || !material_cell || !out) { g_create_err = "null argument"; return GF_EINVAL; }
+    *out = nullptr;
+    gf_engine* eng = new gf_engine();
+    std::string e = deck_from_params(*run, mats, n_materials, material_cell, eng->deck);
+    int rc = GF_OK;
+    if (!e.empty()) { eng->err = e; rc = GF_EINVAL; }
+    if (rc == GF_OK) rc = create_from(eng, "", device, precision);
+    if (rc != GF_OK) {
+        g_create_err = eng->err;
+        gf_destroy(eng);
+        return rc;
+    }
+    *out = eng;
+    return GF_OK;
+}
+
+int gf_set_table(gf_engine* e, int table, const double* times, const double* xyz3, int64_t n) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (table != GF_TABLE_HEXT && table != GF_TABLE_EEXT) { eng->err = "unknown table"; return GF_EINVAL; }
+    if (n < 0 || (n > 0 && (!times || !xyz3))) { eng->err = "bad table"; return GF_EINVAL; }
+    Deck& d = eng->deck;
+    const bool h = table == GF_TABLE_HEXT;
+    if (!(h ? d.prescribe_H : d.prescribe_E)) {
+        eng->err = h ? "the run has no prescribed H table (if_prescribe_Hext)" : "the run has no prescribed E table (if_prescribe_Eext)";
+        return GF_EINVAL;
+    }
+    std::vector<double>& t = h ? d.tH : d.tE;
+    std::vector<double>& x = h ? d.Hx : d.Ex;
+    std::vector<double>& y = h ? d.Hy : d.Ey;
+    std::vector<double>& z = h ? d.Hz : d.Ez;
+    t.assign(times, times + n);
+    x.resize(n); y.resize(n); z.resize(n);
+    for (int64_t i = 0; i < n; i++) { x[i] = xyz3[3 * i]; y[i] = xyz3[3 * i + 1]; z[i] = xyz3[3 * i + 2]; }
+    (h ? d.n_prescribe_H : d.n_prescribe_E) = (long)n;
+    return GF_OK;
+}
+
+int gf_stage_begin(gf_engine* e, int stage) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (stage < 1 || stage > 4) { eng->err = "stage must be 1..4"; return GF_EINVAL; }
+    if (eng->stage_open == 0) {
+        if (stage != 1) { eng->err = "a step starts with stage 1"; return GF_EINVAL; }
+        // time_marching_device_serial for the step: its drive row
+        GF_CU(cudaSetDevice(eng->device));
+        GF_CU(cudaStreamSynchronize(eng->stream));       // the pinned row buffer is free
+        step_drive(eng, eng->drive_host[0]);
+        const uint64_t slot = eng->steps_done & (uint64_t)(kDriveCap - 1);
+        GF_CU(cudaMemcpyAsync(eng->drive + slot, eng->drive_host, sizeof(StepDrive), cudaMemcpyHostToDevice, eng->stream));
+        eng->stage_open = 1;
+        eng->stage_done = 0;
+        return GF_OK;
+    }
+    // begin of the stage in progress (another system) or of the next one
+    if (stage == eng->stage_done || stage == eng->stage_done + 1) return GF_OK;
+    eng->err = "stage " + std::to_string(stage) + " begun after stage " + std::to_string(eng->stage_done);
+    return GF_EINVAL;
+}
+
+int gf_stage_commit(gf_engine* e, int stage) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (stage < 1 || stage > 4) { eng->err = "stage must be 1..4"; return GF_EINVAL; }
+    if (eng->stage_open == 0) {
+        // a repeated commit of the stage that completed the last step
+        if (stage == 4 && eng->stage_done == 4) return GF_OK;
+        eng->err = "gf_stage_commit without gf_stage_begin";
+        return GF_EINVAL;
+    }
+    if (stage == eng->stage_done) return GF_OK;               // served by the first commit
+    if (stage != eng->stage_done + 1) {
+        eng->err = "stage " + std::to_string(stage) + " committed after stage " + std::to_string(eng->stage_done);
+        return GF_EINVAL;
+    }
+    GF_CU(cudaSetDevice(eng->device));
+    const int parity = (int)(eng->steps_done & 1ull);
+    if (eng->mixed) GF_TRY(gf_mixed_enqueue_stage(eng, parity, stage - 1));
+    else GF_TRY(enqueue_stage_t<double>(eng, parity, stage - 1));
+    eng->stage_done = stage;
+    if (stage == 4) {
+        GF_CU(launch(k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
+        eng->steps_done += 1;
+        eng->stage_open = 0;       // stage_done stays 4 until the next step begins
+    }
+    return GF_OK;
+}
+
+int gf_static_solve(gf_engine* e, int which) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    GF_CU(cudaSetDevice(eng->device));
+    if (which != GF_STATIC_MAGNETIC && which != GF_STATIC_ELECTRIC) { eng->err = "unknown static solve"; return GF_EINVAL; }
+    // between stages (main.cpp:299-306 and its repetitions) the committed
+    // stage has already formed the static field of its new state
+    if (eng->stage_done >= 1) return GF_OK;
+    if (which == GF_STATIC_MAGNETIC) {
+        if (eng->demag_mode < 0) { eng->err = "the run has no magnetostatics"; return GF_EINVAL; }
+        if (eng->mixed) GF_TRY(demag_solve_f32(eng, f3f(cur(eng, eng->m)), f3f(cur(eng, eng->a1)), f3f(cur(eng, eng->a2)), false));
+        else GF_TRY(demag_solve(eng, f3(cur(eng, eng->m)), f3(cur(eng, eng->a1)), f3(cur(eng, eng->a2)), false));
+    } else if (which == GF_STATIC_ELECTRIC) {
+        // with the solve off E_stat stays as it is, as in a build of the
+        // reference's public sources, where get_E_static has no definition
+        if (!eng->elec_on) return GF_OK;
+        GF_TRY(elec_solve(eng, f3(cur(eng, eng->p)), false, eng->elec_iters, 0., nullptr));
+    } else {
+        eng->err = "unknown static solve";
+        return GF_EINVAL;
+    }
+    GF_CU(cudaStreamSynchronize(eng->stream));
+    return GF_OK;
 }
 
 int gf_advance_eager(gf_engine* e, uint64_t nsteps) {

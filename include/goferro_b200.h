@@ -126,6 +126,128 @@ int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out);
  * sequence (main.cpp:21-167); the reference has only its FP64 build. */
 int gf_create_from_deck_ex(const char* deck_dir, int device, int precision, gf_engine** out);
 
+/* ---- Set-up from the host's parsed values -------------------------------
+ * For a host that keeps the reference's own readers (read_global,
+ * read_materials and set_global, read.cpp:4-237, global.cpp:14-441) and hands
+ * the engine what they produced instead of a deck directory.  The names
+ * follow global_parameters (global.h:25-176) and material (material.h:3-58).
+ * Restart inputs (m.in, p.in, ...) come afterwards through gf_upload, the
+ * prescribed H / E tables through gf_set_table. */
+typedef struct gf_material_params {
+    /* as read from materials.in (read.cpp:121-205), before check_material
+     * and get_cijkl: the engine derives B1, B2, F*, tv*, the rotated
+     * stiffness and the Drude weights' normalisation the same way */
+    double c11, c12, c44, density, elast_mass_damping, elast_stiff_damping;
+    int32_t if_FM;
+    double Ms, gyro, FM_damping;
+    int32_t anisotropy_type;
+    double K1, K2, Aex, iDMI, lamda100, lamda111;
+    int32_t if_AFM;
+    double Ms_AFM[2], gyro_AFM[2], damping_AFM[2], K1_AFM[2], uniaxis_AFM[3], Aex_AFM[2], J_AFM;
+    double lamda100_AFM[2], lamda111_AFM[2];
+    int32_t if_spin_pump;
+    double spin_hall_angle, spin_mix_cond, spin_diffus_length;
+    int32_t if_FE;
+    double FE_mass, FE_damping, a1, a11, a12, a111, a112, a123, a1111, a1112, a1122, a1123;
+    double G11, Q11, Q12, Q44, f11, f12, f44;
+    int32_t if_PEC;
+    double r_permittivity, conductivity;
+    double comp_n[3], omega_plasma_n[3], tao_e_n[3];
+} gf_material_params;
+
+typedef struct gf_run_params {
+    /* geometry (geometry.h; readgeo, read.cpp:217-237) */
+    int64_t nx, ny, nz;
+    double dx, dy, dz;
+    int32_t periodicX, periodicY, periodicZ;
+    /* time stepping and orientation */
+    uint64_t step;
+    double dt;
+    int32_t if_OrientRotate;
+    double Tg2c[3][3];             /* Tc2g is its transpose */
+    /* uniform initial state of the deck (restart files replace it) */
+    double theta_mag, phi_mag, px_init, py_init, pz_init;
+    /* external fields */
+    double Hext_stat[3], Hext_altr[3], H_altr_freq[3];
+    int32_t if_prescribe_Hext;     /* table through gf_set_table(GF_TABLE_HEXT) */
+    double Eext_stat[3], Eext_altr[3], E_altr_freq[3];
+    int32_t if_prescribe_Eext;     /* table through gf_set_table(GF_TABLE_EEXT) */
+    /* magnetostatics / electrostatics */
+    int32_t if_magnetostatics, if_mag_1Dmodel, if_demag_factor;
+    double demag_fac[3];           /* as read; the engine normalises them to sum -1 */
+    int32_t if_elec_1Dmodel, if_elec_1D_compensate;
+    double scale_elec; int32_t elec_solver_limit; double elec_solver_tol;
+    /* Maxwell */
+    int32_t if_EMdynamic, if_input_planeEM_E;
+    double planeEM_E[3], planeEM_E_freq[3];
+    int32_t if_EM_fromP, if_EM_fromM, if_EM_backaction_on_P, if_EM_backaction_on_M;
+    int32_t if_1D_ABC, if_1D_ABC_ELAST_onlytop, if_1D_ABC_EM_onlytop;
+    double weighting_factor_fourth_Liao;
+    int32_t if_PEC_XY, if_PEC_Z;
+    int32_t if_Jf_input;
+    int64_t Jfin_lo[3], Jfin_hi[3];   /* Jfin_xi.. and Jfin_xf.. (0-based, inclusive) */
+    int32_t Jf_input_type; char Jf_input_component; char pad_[3];
+    double Jf_input_amp, Jf_input_freq, Jf_input_sigma; uint64_t num_Jf_cycles;
+    /* elastodynamics */
+    int32_t if_elastodynamics, if_elasto_backaction_from_pORm, if_elasto_on_pORm;
+    int32_t if_gaussian_strain_pulse, input_strain_type, input_strain_sourcez;
+    char input_strain_component; char pad2_[7];
+    double sigma_gauss, amplitude_gauss; uint64_t num_strain_cycles;
+    /* switches of physics the engine does not provide: must be 0 */
+    int32_t if_elastostatic, if_flexo, if_prescribed_m;
+    int32_t if_spin_pumping;
+} gf_run_params;
+
+/* Create an engine from the parsed values: `run`, `n_materials` materials and
+ * the per-cell material id of set_global (material_cell, nx*ny*nz values in
+ * matrix3d order, 0 = vacuum, id-1 indexes `mats`; global.cpp:65-83).
+ * Replaces the same set-up sequence as gf_create_from_deck (main.cpp:21-167)
+ * with the reading left to the host; the engine reads no file.  An engine
+ * made this way from the values a deck holds equals, bit for bit, the one
+ * gf_create_from_deck makes from that deck. */
+int gf_create(const gf_run_params* run, const gf_material_params* mats, int n_materials, const uint32_t* material_cell,
+              int device, int precision, gf_engine** out);
+
+/* Prescribed external-field tables (global.h:52-57, 68-73; read from Hext.in
+ * / Eext.in by read_prescribe_Hext / read_prescribe_Eext): n rows of time and
+ * x, y, z components.  The table is stepped as the reference does
+ * (time_marching_device_serial, global.cpp:512-549): the row index advances
+ * when t - dt passes the row's time, and the value is held for the four
+ * stages of a step.  The run must have been created with the table switched
+ * on (if_prescribe_Hext / if_prescribe_Eext); a new table takes effect from
+ * the next step. */
+#define GF_TABLE_HEXT 0
+#define GF_TABLE_EEXT 1
+int gf_set_table(gf_engine* e, int table, const double* times, const double* xyz3, int64_t n);
+
+/* ---- Stage-level stepping ------------------------------------------------
+ * For a host that keeps main.cpp's loop and the system classes' method
+ * calls: each system's get_d*_RK{s} calls gf_stage_begin(e, s) and its
+ * update_*_RK{s} (update_* for s = 4) calls gf_stage_commit(e, s).  The
+ * first commit of stage s launches the fused stage of every active physics
+ * (the reference's per-system calls of that stage are served by it); further
+ * commits of the same stage do nothing, so the call order of main.cpp:252-296
+ * (and its repetition for RK2..RK4) works unchanged.  Stages must come in
+ * the order 1, 2, 3, 4; the commit of stage 4 completes the step
+ * (time_marching_device_serial, the step counter).  Static solves between
+ * stages run inside the stage, as in gf_advance; gf_static_solve is for the
+ * set-up calls.  Mixing with gf_advance is allowed between whole steps. */
+int gf_stage_begin(gf_engine* e, int stage);
+int gf_stage_commit(gf_engine* e, int stage);
+
+/* Static field of the current state now: GF_STATIC_MAGNETIC recomputes the
+ * magnetostatic field from m (magnetic_system::get_H_static,
+ * magnetostatic_solver.cpp:114-219; main.cpp:135-146); GF_STATIC_ELECTRIC
+ * runs the electrostatic solve of gf_set_electrostatics, and does nothing
+ * while that is off (E_stat stays as it is, as in a build of the reference's
+ * public sources, which declare get_E_static without defining it).
+ * After a gf_stage_commit (the calls main.cpp makes between stages,
+ * main.cpp:299-306, and after a step) it does nothing: the committed stage
+ * has already formed the static field of its new state.  Synchronous. */
+#define GF_STATIC_MAGNETIC 0
+#define GF_STATIC_ELECTRIC 1
+int gf_static_solve(gf_engine* e, int which);
+
 /* Advance `nsteps` full RK4 steps.  Replaces the body of the reference time
  * loop main.cpp:243-484: time_marching_device_serial, the four stages of
  * get_d*_RK{1..4} / update_*_RK{1..3} / update_* for every active system,
