@@ -121,10 +121,11 @@ def run_params(d) -> GFRunParams:
     r = GFRunParams()
     r.nx, r.ny, r.nz, r.dx, r.dy, r.dz = d.nx, d.ny, d.nz, d.dx, d.dy, d.dz
     r.periodicX, r.periodicY, r.periodicZ = (int(x) for x in d.periodic)
-    r.step, r.dt, r.if_OrientRotate = int(d.steps), d.dt, 0
+    r.step, r.dt, r.if_OrientRotate = int(d.steps), d.dt, int(d.Tg2c is not None)
+    T = np.eye(3) if d.Tg2c is None else np.asarray(d.Tg2c, dtype=np.float64)
     for i in range(3):
         for j in range(3):
-            r.Tg2c[i][j] = 1.0 if i == j else 0.0
+            r.Tg2c[i][j] = float(T[i, j])
     r.theta_mag, r.phi_mag = d.theta_mag, d.phi_mag
     r.px_init, r.py_init, r.pz_init = d.p_init
     r.Hext_stat[:] = list(d.Hext_stat); r.Hext_altr[:] = list(d.Hext_altr); r.H_altr_freq[:] = list(d.H_altr_freq)

@@ -239,6 +239,9 @@ class Deck:
     u0: Optional[np.ndarray] = None
     v0: Optional[np.ndarray] = None
     Hext_table: Optional[np.ndarray] = None    # (K, 4): t Hx Hy Hz
+    # crystal orientation: Tg2c, the global-to-crystal rotation (3x3); when
+    # set, if_OrientRotate is true (read.cpp:30-37; Tc2g is its transpose)
+    Tg2c: Optional[np.ndarray] = None
     # per-cell material ids (nx, ny, nz); when set, if_read_struct is true and
     # struct.in replaces the layer stack's cell assignment (read.cpp:280-294,
     # global.cpp:67-83)
@@ -279,8 +282,8 @@ class Deck:
              _f(self.dt),
              str(len(self.materials)),
              " ".join(str(int(l[1])) for l in self.layers),
-             "false",
-             "1 0 0", "0 1 0", "0 0 1",
+             _b(self.Tg2c is not None),
+             *(" ".join(_f(x) for x in row) for row in (np.eye(3) if self.Tg2c is None else np.asarray(self.Tg2c))),
              f"{_f(self.theta_mag)} {_f(self.phi_mag)}",
              " ".join(_f(x) for x in self.p_init),
              "false",
@@ -432,6 +435,15 @@ def pto() -> Material:
                     a1=3.8e5 * (300.0 - 479.0), a11=-7.3e7, a12=7.5e8,
                     a111=2.6e8, a112=6.1e8, a123=-3.7e9,
                     G11=5.1e-10, Q11=0.089, Q12=-0.026, Q44=0.0675, er=10.0)
+
+
+def rotation(ax_deg: float, az_deg: float) -> np.ndarray:
+    """An orthogonal global-to-crystal rotation: az_deg about z, then ax_deg
+    about x."""
+    a, b = math.radians(ax_deg), math.radians(az_deg)
+    rz = np.array([[math.cos(b), -math.sin(b), 0.0], [math.sin(b), math.cos(b), 0.0], [0.0, 0.0, 1.0]])
+    rx = np.array([[1.0, 0.0, 0.0], [0.0, math.cos(a), -math.sin(a)], [0.0, math.sin(a), math.cos(a)]])
+    return rx @ rz
 
 
 def tilt_m0(shape, seed: int, mc: np.ndarray, max_deg: float = 1.0) -> np.ndarray:

@@ -250,6 +250,35 @@ def _variants(gf):
         rng = np.random.default_rng(100 + nmat)
         d.struct = rng.integers(1, nmat + 1, size=(8, 8, 10)).astype(np.uint8)
         v[f"random_struct_{nmat}mat"] = (d, 20, (4, 4, 5))
+    # crystal frame rotated against the grid (if_OrientRotate): the rotated
+    # stiffness has no cubic pattern, magnetostriction / electrostriction and
+    # anisotropy act in the crystal frame (mathlib.cpp:45-135, global.cpp:365-441)
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=20)
+    d.amp_gauss *= 1e6
+    d.Tg2c = D.rotation(20.0, 30.0)
+    v["rotated_magnetoelastic"] = (d, 20, (4, 8, 7))
+    d = D.preset_ferroelectric(nx=8, ny=8, nz=10, steps=20)
+    d.Tg2c = D.rotation(-35.0, 15.0)
+    v["rotated_ferroelectric"] = (d, 20, (4, 4, 5))
+    # sheet-current source types 0-3 and 5 (update_Jf_input,
+    # EMdynamic_solver.cpp:3885-4000): sine, sine x sin / cos of the depth in
+    # the box, sine for a number of cycles, Gaussian derivative
+    for jt in (0, 1, 2, 3, 5):
+        d = D.preset_ferroelectric(nx=8, ny=8, nz=12, steps=20)
+        d.jf_type, d.jf_comp = jt, ("x", "y", "z", "x", "y")[jt if jt < 5 else 4]
+        d.jf_lo, d.jf_hi = (1, 2, 3), (6, 5, 6)
+        # type 5 reads its width from Jf_input_freq; type 3 stops after one cycle
+        d.jf_freq = {5: 5e-17, 3: 4e16}.get(jt, 4e15)
+        d.jf_cycles = 1 if jt == 3 else 0
+        d.jf_amp = 1e14
+        v[f"jf_type{jt}"] = (d, 20, (4, 4, 5))
+    # 1-D magnetostatics (if_mag_1Dmodel: H_z = -Ms m_z, magnetostatic_solver.cpp:221-249)
+    d = D.preset_fm_demag(nx=8, ny=8, nz=10, steps=15)
+    d.materials = [D.ggg(), D.yig(0.01)]
+    d.layers = [(4, 1), (4, 2), (2, 0)]
+    d.m0 = D.tilt_m0((8, 8, 10), 41, d.material_cell() == 2, max_deg=10.0)
+    d.mag_1D = True
+    v["mag_1d_model"] = (d, 15, None)
     return v
 
 
@@ -272,7 +301,8 @@ def test_random_struct_variants_cover_both_yee_paths(gf):
                                    "elastic_multi_tile", "elastic_quirk_far_tile", "fm_film_demag_substrate",
                                    "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
                                    "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
-                                   "random_struct_6mat"])
+                                   "random_struct_6mat", "rotated_magnetoelastic", "rotated_ferroelectric",
+                                   "jf_type0", "jf_type1", "jf_type2", "jf_type3", "jf_type5", "mag_1d_model"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
