@@ -14,13 +14,15 @@
 //                 evaluated on offsets |i| < nx/2 (the Nyquist offset is left
 //                 zero), divided by 4*pi and by the cell count n.
 //   k_demag_mul   k-space product H_k = -(N_k . M_k)/(dx dy dz) with the nine
-//                 complex spectra (magnetostatic_solver.cpp:159-179).
+//                 complex spectra (magnetostatic_solver.cpp:159-179); the
+//                 mixed form's k_demag_mul_f32 uses the six real spectra of
+//                 the symmetric tensor.
 //   k_mag_source  M = Ms m for the forward transform, and the demag-factor
 //                 and 1-D alternatives (magnetostatic_solver.cpp:114-249).
 // The transforms themselves are cuFFT D2Z / Z2D (batched over the three
 // components), unnormalised as in the reference.  The mixed form builds the
-// tables and their spectra in FP64 (newell_cell, D2Z), stores the spectra in
-// FP32 and runs R2C / C2R per stage.
+// tables and their spectra in FP64 (newell_cell, D2Z), stores the six real
+// spectra in FP32 and runs R2C / C2R per stage.
 #pragma once
 
 #include <cuComplex.h>
@@ -141,7 +143,13 @@ __device__ inline cuDoubleComplex cadd(cuDoubleComplex a, cuDoubleComplex b) {
     return make_cuDoubleComplex(a.x + b.x, a.y + b.y);
 }
 
-// M_k (3 x n21) and the nine spectra (9 x n21) -> H_k (3 x n21)
+// M_k (3 x n21) and the nine complex spectra (9 x n21, the reference's
+// Axyzk .. Bxzyk) -> H_k (3 x n21), in the reference's operation order
+// (magnetostatic_solver.cpp:159-179).  The FP64 form keeps all nine: the
+// tensor's spectra are real and N_ij = N_ji only up to the rounding of the
+// tables, and the probed E of a 128x128x96 magnetoelastic run (driven by
+// dm/dt of a nearly static m) moved by 3e-8 of its scale when the six real
+// ones stood in for them.
 static __global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_neg, const cuDoubleComplex* __restrict__ Mk,
                                                    const cuDoubleComplex* __restrict__ Nk, cuDoubleComplex* __restrict__ Hk) {
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -154,6 +162,20 @@ static __global__ void __launch_bounds__(256) k_demag_mul(long n21, double vol_n
     Hk[q] = make_cuDoubleComplex(hx.x / vol_neg, hx.y / vol_neg);
     Hk[n21 + q] = make_cuDoubleComplex(hy.x / vol_neg, hy.y / vol_neg);
     Hk[2 * n21 + q] = make_cuDoubleComplex(hz.x / vol_neg, hz.y / vol_neg);
+}
+
+// The mixed form's six real spectra (N_xx, N_yy, N_zz, N_xy, N_yz, N_zx)
+// from the FP64 transforms of the nine tables (order Axyz Ayzx Azxy Bxyz
+// Byzx Bzxy Byxz Bzyx Bxzy): the real parts of the first six.  The tensor's
+// tables are real and even under r -> -r, so their spectra are real, and
+// N_ij = N_ji: the other three spectra and all imaginary parts differ from
+// these by the tables' rounding, far below FP32 resolution.
+template <class T>
+static __global__ void k_spectra_real(const cuDoubleComplex* __restrict__ in9, long n21, T* __restrict__ out6) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n21) return;
+#pragma unroll
+    for (int t = 0; t < 6; t++) out6[t * n21 + q] = (T)in9[t * n21 + q].x;
 }
 
 // mode 0: M into the FFT input, Ms m for ferromagnetic cells and
@@ -193,26 +215,21 @@ static __global__ void k_mag_source(Params P, const DevMat* mats, const uint8_t*
 
 // ---- mixed form: FP32 transforms; the spectra are built in FP64 ----
 
-// complex FP64 -> FP32 (the Green spectra after the FP64 transform)
-static __global__ void k_spectra_f32(const cuDoubleComplex* __restrict__ in, long n, cuComplex* __restrict__ out) {
-    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    out[q] = make_cuComplex((float)in[q].x, (float)in[q].y);
-}
-
-// k_demag_mul on FP32 spectra; inv_vol_neg = -1/(dx dy dz)
+// k_demag_mul on the six real FP32 spectra (a third of the nine complex
+// ones' bytes); inv_vol_neg = -1/(dx dy dz)
 static __global__ void __launch_bounds__(256) k_demag_mul_f32(long n21, float inv_vol_neg, const cuComplex* __restrict__ Mk,
-                                                       const cuComplex* __restrict__ Nk, cuComplex* __restrict__ Hk) {
+                                                       const float* __restrict__ Nr, cuComplex* __restrict__ Hk) {
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n21) return;
     const cuComplex mx = Mk[q], my = Mk[n21 + q], mz = Mk[2 * n21 + q];
-    const cuComplex* N = Nk;
-    const cuComplex hx = cuCaddf(cuCaddf(cuCmulf(mx, N[0 * n21 + q]), cuCmulf(my, N[3 * n21 + q])), cuCmulf(mz, N[8 * n21 + q]));
-    const cuComplex hy = cuCaddf(cuCaddf(cuCmulf(my, N[1 * n21 + q]), cuCmulf(mz, N[4 * n21 + q])), cuCmulf(mx, N[6 * n21 + q]));
-    const cuComplex hz = cuCaddf(cuCaddf(cuCmulf(mz, N[2 * n21 + q]), cuCmulf(mx, N[5 * n21 + q])), cuCmulf(my, N[7 * n21 + q]));
-    Hk[q] = make_cuComplex(hx.x * inv_vol_neg, hx.y * inv_vol_neg);
-    Hk[n21 + q] = make_cuComplex(hy.x * inv_vol_neg, hy.y * inv_vol_neg);
-    Hk[2 * n21 + q] = make_cuComplex(hz.x * inv_vol_neg, hz.y * inv_vol_neg);
+    const float nxx = Nr[q], nyy = Nr[n21 + q], nzz = Nr[2 * n21 + q];
+    const float nxy = Nr[3 * n21 + q], nyz = Nr[4 * n21 + q], nzx = Nr[5 * n21 + q];
+    const float hxr = (mx.x * nxx + my.x * nxy) + mz.x * nzx, hxi = (mx.y * nxx + my.y * nxy) + mz.y * nzx;
+    const float hyr = (my.x * nyy + mz.x * nyz) + mx.x * nxy, hyi = (my.y * nyy + mz.y * nyz) + mx.y * nxy;
+    const float hzr = (mz.x * nzz + mx.x * nzx) + my.x * nyz, hzi = (mz.y * nzz + mx.y * nzx) + my.y * nyz;
+    Hk[q] = make_cuComplex(hxr * inv_vol_neg, hxi * inv_vol_neg);
+    Hk[n21 + q] = make_cuComplex(hyr * inv_vol_neg, hyi * inv_vol_neg);
+    Hk[2 * n21 + q] = make_cuComplex(hzr * inv_vol_neg, hzi * inv_vol_neg);
 }
 
 // k_mag_source for the mixed form

@@ -118,9 +118,11 @@ struct gf_engine {
     // magnetostatics
     int demag_mode = -1;                   // -1 none, 0 FFT, 1 factors, 2 1-D
     bool demag_per_stage = false;
+    bool demag_src_fused = false;          // the LLG kernel writes the transform's input (StageIOT::msrc)
     double* Mfft = nullptr;                // 3 x n real
     cufftDoubleComplex* Mk = nullptr;      // 3 x n21
-    cufftDoubleComplex* Nk = nullptr;      // 9 x n21
+    cufftDoubleComplex* Nk = nullptr;      // FP64 form: the nine complex demag spectra, 9 x n21
+    float* Nr = nullptr;                   // mixed form: the six real spectra, 6 x n21
     cufftHandle plan_r2c = 0, plan_c2r = 0;
     bool plans = false;
 
@@ -674,6 +676,7 @@ void build_io(gf_engine* eng) {
             for (int a = 0; a < 6; a++) { io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr; }
             io.liao_hist = eng->liao_hist;
             io.liao_last = eng->liao_last;
+            io.msrc = eng->demag_src_fused ? eng->Mfft : nullptr;
             io.mid = eng->mid;
             io.mats = eng->mats;
             io.drive = eng->drive;
@@ -735,6 +738,7 @@ void build_io_mixed(gf_engine* eng) {
             for (int a = 0; a < 6; a++) io.strain_c[a] = reinterpret_cast<float*>(eng->strain_c[a]);
             io.liao_hist = reinterpret_cast<float*>(eng->liao_hist);
             io.liao_last = reinterpret_cast<float*>(eng->liao_last);
+            io.msrc = eng->demag_src_fused ? reinterpret_cast<float*>(eng->Mfft) : nullptr;
             io.mid = eng->mid;
             io.mats = eng->mats_f;
             io.drive = eng->drive;
@@ -811,7 +815,9 @@ template <> const LLGTablesT<double>* llg_tables<double>(const gf_engine* eng) {
 
 // magnetostatic field of magnetisation m into Hstat (FFT, demag factors or
 // the 1-D model), FP64 form
-int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
+// src_ready: the stage's LLG kernel has already written the transform's
+// input (StageIOT::msrc), so the source kernel is skipped
+int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted, bool src_ready = false) {
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
@@ -819,8 +825,9 @@ int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
         return counted ? klaunch(eng, name, k, g, b, 0, st, args...) : launch(k, g, b, 0, st, args...);
     };
     if (eng->demag_mode == 0) {
-        GF_CU(L("k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
-                m, a1, a2, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+        if (!src_ready)
+            GF_CU(L("k_mag_source", k_mag_source, dim3(bn), dim3(kThreads), P, (const DevMat*)eng->mats, (const uint8_t*)eng->mid,
+                    m, a1, a2, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
         GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
         const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
         const double vol_neg = -P.dx * P.dy * P.dz;
@@ -838,7 +845,7 @@ int demag_solve(gf_engine* eng, F3 m, F3 a1, F3 a2, bool counted) {
 }
 
 // the same in the mixed form: FP32 source, R2C, spectra product, C2R
-int demag_solve_f32(gf_engine* eng, F3T<float> m, F3T<float> a1, F3T<float> a2, bool counted) {
+int demag_solve_f32(gf_engine* eng, F3T<float> m, F3T<float> a1, F3T<float> a2, bool counted, bool src_ready = false) {
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
@@ -848,13 +855,14 @@ int demag_solve_f32(gf_engine* eng, F3T<float> m, F3T<float> a1, F3T<float> a2, 
     float* M3 = reinterpret_cast<float*>(eng->Mfft);
     cufftComplex* Mk = reinterpret_cast<cufftComplex*>(eng->Mk);
     if (eng->demag_mode == 0) {
-        GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
-                (const uint8_t*)eng->mid, m, a1, a2, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
+        if (!src_ready)
+            GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
+                    (const uint8_t*)eng->mid, m, a1, a2, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
         GF_FFT(cufftExecR2C(eng->plan_r2c, M3, Mk));
         const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
         const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
         GF_CU(L("k_demag_mul", k_demag_mul_f32, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, inv_vol_neg,
-                (const cuComplex*)Mk, (const cuComplex*)eng->Nk, (cuComplex*)Mk));
+                (const cuComplex*)Mk, (const float*)eng->Nr, (cuComplex*)Mk));
         GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));     // into H_stat (a view of M3)
     } else {
         GF_CU(L("k_mag_source", k_mag_source_f32, dim3(bn), dim3(kThreads), P, (const DevMatT<float>*)eng->mats_f,
@@ -942,8 +950,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
     }
     if (eng->demag_per_stage) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
-        if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, io.a1_out, io.a2_out, true));
-        else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true));
+        if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, io.a1_out, io.a2_out, true, io.msrc != nullptr));
+        else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true, io.msrc != nullptr));
     }
     if constexpr (!is_mixed<R>::value) {
         // electrostatic field of the new stage polarisation (main.cpp:299-302)
@@ -1075,14 +1083,19 @@ int setup_demag(gf_engine* eng) {
     else if (d.demag_factor) eng->demag_mode = 1;
     else eng->demag_mode = 0;
     eng->demag_per_stage = !d.em_dynamic;
+    // the LLG kernel can form the per-stage transform input itself when it
+    // visits every cell (the ferromagnet's bounding box is the grid) and no
+    // antiferromagnet adds to M
+    eng->demag_src_fused = eng->demag_per_stage && !d.mag_1D && !d.demag_factor && P.fm && !P.afm &&
+                           P.fm_bi * P.fm_bj * P.fm_bk == P.n;
     if (eng->demag_mode != 0) return GF_OK;
     const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
     int dims[3] = {P.nx, P.ny, P.nz};
     if (eng->mixed) {
-        // M (3n real), M_k (3 n21 complex) and the nine spectra in FP32
+        // M (3n real), M_k (3 n21 complex) and the six real spectra in FP32
         GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Mfft), sizeof(float) * 3 * (size_t)P.n));
         GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Mk), sizeof(cufftComplex) * 3 * (size_t)n21));
-        GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Nk), sizeof(cufftComplex) * 9 * (size_t)n21));
+        GF_TRY(dalloc(eng, reinterpret_cast<void**>(&eng->Nr), sizeof(float) * 6 * (size_t)n21));
         // tables and their spectra in FP64 with a temporary D2Z plan, then rounded to FP32
         double* tab = nullptr;
         cufftDoubleComplex* nk64 = nullptr;
@@ -1098,8 +1111,8 @@ int setup_demag(gf_engine* eng) {
         for (int b = 0; b < 3 && ce == cudaSuccess && fr == CUFFT_SUCCESS; b++)
             fr = cufftExecD2Z(p64, tab + (size_t)3 * b * P.n, nk64 + (size_t)3 * b * n21);
         if (ce == cudaSuccess && fr == CUFFT_SUCCESS)
-            ce = launch(k_spectra_f32, dim3(blocks_for(9 * n21, kThreads)), dim3(kThreads), 0, eng->stream,
-                        (const cuDoubleComplex*)nk64, 9 * n21, reinterpret_cast<cuComplex*>(eng->Nk));
+            ce = launch(k_spectra_real<float>, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, eng->stream,
+                        (const cuDoubleComplex*)nk64, n21, eng->Nr);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(eng->stream);
         if (p64) cufftDestroy(p64);
         if (tab) cudaFree(tab);
@@ -1129,8 +1142,8 @@ int setup_demag(gf_engine* eng) {
     // demag tensor tables: 9 x n real, built on the host, transformed on the
     // device in three batches of 3
     const std::shared_ptr<const std::vector<double>> host_tab = newell_tables(P);
-    double* tab = nullptr;
-    cudaError_t ce = cudaMalloc(&tab, sizeof(double) * 9 * (size_t)P.n);      // temporary
+    double* tab = nullptr;                                                    // temporary
+    cudaError_t ce = cudaMalloc(&tab, sizeof(double) * 9 * (size_t)P.n);
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(tab, host_tab->data(), sizeof(double) * 9 * (size_t)P.n, cudaMemcpyHostToDevice, eng->stream);
     cufftResult fr = CUFFT_SUCCESS;
@@ -1562,7 +1575,7 @@ int create_from(gf_engine* eng, const std::string& dir, int device, int precisio
     if (P.em) GF_TRY(setup_em_classes(eng));
     // FP64 scratch: output staging (6 cell arrays, or one widened Yee
     // component in the mixed form) and the reduction partials (device_sum3:
-    // 3 x (8192 + 64 + 1))
+    // 3 x (592 + 1); the adjoint's means: 8192 + 64 + 1)
     const size_t yee_max = (size_t)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);
     eng->scratch_main = std::max((size_t)6 * n, yee_max);
     GF_TRY(dalloc_n(eng, &eng->scratch, eng->scratch_main + 32768));
@@ -1659,21 +1672,18 @@ double* const* cur(gf_engine* eng, Field3& f) { return (eng->steps_done & 1ull) 
 // the mixed form of the values x + c when the compensation words c are
 // given): 8192 strided partials, then 64, then 1, each sum in a fixed order;
 // one copy back and one synchronisation for the three
+// gf_average's reductions: one pass into kSumBlocks partials per component
+// (warp-shuffle block sums), one pass over the partials, one read-back
+constexpr int kSumBlocks = 592;
 int device_sum3(gf_engine* eng, double* const* in, long n, double out[3], double* const* cmp) {
     cudaStream_t st = eng->stream;
-    double* p1 = eng->scratch + eng->scratch_main;            // 3 x 8192
-    double* p2 = p1 + 3 * 8192;                               // 3 x 64
-    double* p3 = p2 + 3 * 64;                                 // 3
+    double* p1 = eng->scratch + eng->scratch_main;            // 3 x kSumBlocks
+    double* p3 = p1 + 3 * kSumBlocks;                         // 3
     Sum3In a{};
     a.f32 = eng->mixed ? 1 : 0;
     for (int c = 0; c < 3; c++) { a.x[c] = in[c]; a.cm[c] = eng->mixed && cmp ? reinterpret_cast<const float*>(cmp[c]) : nullptr; }
-    GF_CU(launch(k_sum3_stride, dim3(32, 3), dim3(256), 0, st, a, n, p1, 8192L));
-    Sum3In b{};
-    for (int c = 0; c < 3; c++) b.x[c] = p1 + c * 8192;
-    GF_CU(launch(k_sum3_stride, dim3(1, 3), dim3(64), 0, st, b, 8192L, p2, 64L));
-    Sum3In d{};
-    for (int c = 0; c < 3; c++) d.x[c] = p2 + c * 64;
-    GF_CU(launch(k_sum3_stride, dim3(1, 3), dim3(1), 0, st, d, 64L, p3, 1L));
+    GF_CU(launch(k_sum3_block, dim3(kSumBlocks, 3), dim3(kSumThreads), 0, st, a, n, p1));
+    GF_CU(launch(k_sum3_final, dim3(3), dim3(kSumThreads), 0, st, (const double*)p1, kSumBlocks, p3));
     GF_CU(cudaMemcpyAsync(out, p3, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     GF_CU(cudaStreamSynchronize(st));
     return GF_OK;

@@ -47,7 +47,7 @@ __device__ inline void cell_strain_total(const Params& P, const StageIOT<R>& io,
 // per-material LLG constants, staged in shared memory
 template <class R>
 struct LLGMat {
-    R Aex, dA, ex_coef, dmi_coef, K1c, K2c, B1c, B2c, precess, alpha_precess;
+    R Aex, dA, ex_coef, dmi_coef, K1c, K2c, B1c, B2c, precess, alpha_precess, Ms;
     int aniso;
     uint32_t fm;
 };
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_LLG_MINB_F32 : GF
     __shared__ R sA[kMaxMat + 1][kMaxMat + 1];
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMatT<R>& d = io.mats[q];
-        mt[q] = LLGMat<R>{d.Aex, d.dA, d.ex_coef, d.dmi_coef, d.K1c, d.K2c, d.B1c, d.B2c, d.precess, d.alpha_precess,
+        mt[q] = LLGMat<R>{d.Aex, d.dA, d.ex_coef, d.dmi_coef, d.K1c, d.K2c, d.B1c, d.B2c, d.precess, d.alpha_precess, d.Ms,
                           d.aniso, (d.flags & MF_FM) ? 1u : 0u};
     }
     for (int q = threadIdx.x; q < (nmat + 1) * (nmat + 1); q += blockDim.x) {
@@ -252,6 +252,13 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_LLG_MINB_F32 : GF
             if (fm_cell) renorm3(o[0], o[1], o[2]);
 #pragma unroll
             for (int a = 0; a < 3; a++) io.m_out.c[a][c] = o[a];
+            // the next magnetostatic source, Ms m of this stage's output
+            // (k_mag_source_f32 forms the same product from memory)
+            if (io.msrc) {
+                const float Ms = fm_cell ? mt[id - 1].Ms : 0.f;
+#pragma unroll
+                for (int a = 0; a < 3; a++) io.msrc[(long)a * P.n + c] = fm_cell ? Ms * o[a] : 0.f;
+            }
         } else {
             float x[3], cm[3];
 #pragma unroll
@@ -260,18 +267,31 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_LLG_MINB_F32 : GF
             if (fm_cell) renorm_pair(x, cm);
 #pragma unroll
             for (int a = 0; a < 3; a++) { io.m_acc.c[a][c] = x[a]; io.m_cmp.c[a][c] = cm[a]; }
+            if (io.msrc) {
+                const float Ms = fm_cell ? mt[id - 1].Ms : 0.f;
+#pragma unroll
+                for (int a = 0; a < 3; a++) io.msrc[(long)a * P.n + c] = fm_cell ? Ms * x[a] : 0.f;
+            }
         }
     } else {
         // ---- RK4 combination; the magnetic increment is summed before it is
         //      added to m (magnetic_solver.cpp:1453-1455, 1601-1603) ----
         const double d[3] = {dmx, dmy, dmz};
+        double o[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             const double xv = mx0[a];
-            if (S == 0) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
-            else if (S == 1) { io.m_out.c[a][c] = xv + d[a] * 0.5; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
-            else if (S == 2) { io.m_out.c[a][c] = xv + d[a]; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
-            else { io.m_acc.c[a][c] = xv + (ma[a] + qdiv(d[a], 6., kInv6)); }
+            if (S == 0) { o[a] = xv + d[a] * 0.5; io.m_out.c[a][c] = o[a]; io.m_acc.c[a][c] = qdiv(d[a], 6., kInv6); }
+            else if (S == 1) { o[a] = xv + d[a] * 0.5; io.m_out.c[a][c] = o[a]; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
+            else if (S == 2) { o[a] = xv + d[a]; io.m_out.c[a][c] = o[a]; io.m_acc.c[a][c] = ma[a] + qdiv(d[a], 3., kInv3); }
+            else { o[a] = xv + (ma[a] + qdiv(d[a], 6., kInv6)); io.m_acc.c[a][c] = o[a]; }
+        }
+        // the next magnetostatic source, Ms m of this stage's output (the
+        // product k_mag_source forms, magnetostatic_solver.cpp:129-131)
+        if (io.msrc) {
+            const double Ms = fm_cell ? mt[id - 1].Ms : 0.;
+#pragma unroll
+            for (int a = 0; a < 3; a++) io.msrc[(long)a * P.n + c] = fm_cell ? Ms * o[a] : 0.;
         }
     }
 }

@@ -63,6 +63,11 @@ struct StageIOT {
     // (3 comps), plus the last boundary value written on plane 0
     R* liao_hist;
     R* liao_last;
+    // input of the next magnetostatic transform (M = Ms m of the stage
+    // output), written by the ferromagnet's LLG kernel when it covers the
+    // whole grid and the run has no antiferromagnet; null otherwise (a
+    // separate source kernel then forms it)
+    R* msrc;
     // geometry / materials / time
     const uint8_t* mid;
     const DevMatT<R>* mats;

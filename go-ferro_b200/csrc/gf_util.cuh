@@ -28,52 +28,89 @@ static __global__ void k_sum_stride(const double* __restrict__ in, long n, doubl
     partial[t] = acc;
 }
 
-// Three arrays (component y = blockIdx.y): partial[y * T + t] = the in-order
-// sum of in_y[t], in_y[t + T], ..., exactly as k_sum_stride forms it, with
-// the loads of GF_SUM_BATCH terms issued before their additions (one thread
-// has ~n / T terms, too many to wait for one at a time).  32 measured best of
-// 8, 16 and 32 on 1.57 M cells: gf_average + gf_probe_em add 0.17 ms (FP64)
-// and 0.19 ms (mixed) to a step, against 0.20 and 0.34 ms at 8.  In the
-// mixed form (f32) each term is the FP64 value x + c of an FP32 pair (c may
-// be null).
+// Three arrays (component y = blockIdx.y), each term the FP64 value of an
+// element: a double, or in the mixed form (f32) the FP64 value x + c of an
+// FP32 pair (c may be null).
 struct Sum3In {
     const void* x[3];
     const float* cm[3];
     int f32;          // x holds floats (mixed form) rather than doubles
 };
+
+// Sum of a warp's 32 values by a fixed shuffle tree (lane 0 gets the total):
+// the order of the additions depends on nothing but the lane numbers.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One pass over the data: block b of component y sums the contiguous chunk
+// [b*L, min((b+1)*L, n)) of array y — each thread the elements t, t+256, ...
+// of the chunk in order, then the 8 warps by a fixed shuffle tree and the 8
+// warp totals in warp order — into partial[y * gridDim.x + b].  With the
+// grid fixed by the caller the sum depends only on n.  The loads of
+// GF_SUM_BATCH terms are issued before their additions.
 #ifndef GF_SUM_BATCH
-#define GF_SUM_BATCH 32
+#define GF_SUM_BATCH 8
 #endif
-static __global__ void k_sum3_stride(Sum3In in, long n, double* __restrict__ partial, long T) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
+constexpr int kSumThreads = 256;
+static __global__ void __launch_bounds__(kSumThreads) k_sum3_block(Sum3In in, long n, double* __restrict__ partial) {
     const int y = blockIdx.y;
+    const long L = (n + gridDim.x - 1) / gridDim.x;
+    const long i0 = (long)blockIdx.x * L;
+    const long i1 = min(i0 + L, n);
     constexpr int B = GF_SUM_BATCH;
     double acc = 0.;
-    long i = t;
+    long i = i0 + threadIdx.x;
     if (in.f32) {
         const float* x = static_cast<const float*>(in.x[y]);
         const float* cm = in.cm[y];
-        for (; i + (B - 1) * T < n; i += B * T) {
+        for (; i + (B - 1) * kSumThreads < i1; i += B * kSumThreads) {
             double v[B];
 #pragma unroll
-            for (int b = 0; b < B; b++) v[b] = (double)x[i + b * T] + (cm ? (double)cm[i + b * T] : 0.);
+            for (int b = 0; b < B; b++) v[b] = (double)x[i + b * kSumThreads] + (cm ? (double)cm[i + b * kSumThreads] : 0.);
 #pragma unroll
             for (int b = 0; b < B; b++) acc = acc + v[b];
         }
-        for (; i < n; i += T) acc = acc + ((double)x[i] + (cm ? (double)cm[i] : 0.));
+        for (; i < i1; i += kSumThreads) acc = acc + ((double)x[i] + (cm ? (double)cm[i] : 0.));
     } else {
         const double* x = static_cast<const double*>(in.x[y]);
-        for (; i + (B - 1) * T < n; i += B * T) {
+        for (; i + (B - 1) * kSumThreads < i1; i += B * kSumThreads) {
             double v[B];
 #pragma unroll
-            for (int b = 0; b < B; b++) v[b] = x[i + b * T];
+            for (int b = 0; b < B; b++) v[b] = x[i + b * kSumThreads];
 #pragma unroll
             for (int b = 0; b < B; b++) acc = acc + v[b];
         }
-        for (; i < n; i += T) acc = acc + x[i];
+        for (; i < i1; i += kSumThreads) acc = acc + x[i];
     }
-    partial[y * T + t] = acc;
+    __shared__ double ws[kSumThreads / 32];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < kSumThreads / 32 ? ws[threadIdx.x] : 0.;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) partial[y * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+// out[y] = sum of the nb partials of component y (blockIdx.x = y), each
+// thread its partials t, t+256, ... in order, then the same fixed tree.
+static __global__ void __launch_bounds__(kSumThreads) k_sum3_final(const double* __restrict__ partial, int nb, double* __restrict__ out) {
+    const int y = blockIdx.x;
+    double acc = 0.;
+    for (int i = threadIdx.x; i < nb; i += kSumThreads) acc = acc + partial[y * nb + i];
+    __shared__ double ws[kSumThreads / 32];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < kSumThreads / 32 ? ws[threadIdx.x] : 0.;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) out[y] = v;
+    }
 }
 
 // numerators for gf_check_quotients: odd i draws a random double with
