@@ -149,6 +149,7 @@ def run_params(d) -> GFRunParams:
     r.input_strain_component = d.strain_comp.encode()
     r.sigma_gauss, r.amplitude_gauss, r.num_strain_cycles = d.sigma_gauss, d.amp_gauss, int(d.strain_cycles)
     r.if_spin_pumping = int(d.spin_pumping)
+    r.if_flexo = int(d.flexo)
     return r
 
 

@@ -59,6 +59,11 @@ struct DevMatT {
     R a1, a11, a12, a111, a112, a123, a1111, a1112, a1122, a1123;
     R tv1, tv2, tv3, G11;
     R fe_coef, fe_damp;                    // -dt/m, fe_coef*gamma
+    // flexoelectric coupling (ferroelectric_solver.cpp:800-833,
+    // elastic_dynamic_solver.cpp:63-70; read.cpp:182-198)
+    R tv4, tv5, tv6, tv7, tv8;
+    R f11, f12, f44x2;                     // f44x2 = 2 f44
+    R F11, F12, F44h;                      // F44h = F44 / 2
     // electromagnetic
     R er, cond;
     R comp[3], wp[3], rtau[3];
@@ -95,6 +100,7 @@ struct Params {
     int drude;                // some material has a Drude pole (omega_plasma != 0)
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;
+    int flexo;                // if_flexo with ferroelectrics: StageIOT::sg / pge are set
     double liao_w;
     // elastic boundary coefficients (elastodynamics_AbsorbingBoundary.cpp)
     double vs_long_1st, vs_tran_1st, vs_long_last, vs_tran_last;

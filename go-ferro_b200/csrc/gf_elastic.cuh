@@ -132,6 +132,19 @@ __device__ inline void eigen_terms(const Params& P, const StageIOT<R>& io, long 
         t[5] = t[5] + mt.l111a1_075 * a1y * a1x + mt.l111a2_075 * a2y * a2x;
     }
     for (int a = 0; a < 6; a++) e[a] = t[a] - e0[a];
+    if (P.flexo) {
+        // flexoelectric eigenstrain of the polarisation gradient
+        // (elastic_dynamic_solver.cpp:63-70), subtracted after e0 in the
+        // reference's order; applied in every material cell (the gradients
+        // are zero outside ferroelectrics), as the reference does
+        const R g0 = io.pge[0][c], g1 = io.pge[1][c], g2 = io.pge[2][c];
+        e[0] = e[0] - mt.F11 * g0 - mt.F12 * (g2 + g1);
+        e[1] = e[1] - mt.F11 * g1 - mt.F12 * (g2 + g0);
+        e[2] = e[2] - mt.F11 * g2 - mt.F12 * (g0 + g1);
+        e[3] = e[3] - mt.F44h * io.pge[3][c];
+        e[4] = e[4] - mt.F44h * io.pge[4][c];
+        e[5] = e[5] - mt.F44h * io.pge[5][c];
+    }
 }
 
 // dynamic eigenstrain of cell c in the crystal frame (Dexx0_crt ...,
@@ -187,6 +200,7 @@ struct ElMat {
     R dens_dt, mass_damp, stiff_damp;
     R l100_15, l111_15, Q11, Q12, Q44;
     R l100a1_075, l100a2_075, l111a1_075, l111a2_075;
+    R F11, F12, F44h;
     uint32_t flags;
     int cubic_c;
 };
@@ -421,6 +435,7 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
         e.dens_dt = d.dens_dt; e.mass_damp = d.mass_damp; e.stiff_damp = d.stiff_damp;
         e.l100_15 = d.l100_15; e.l111_15 = d.l111_15; e.Q11 = d.Q11; e.Q12 = d.Q12; e.Q44 = d.Q44;
         e.l100a1_075 = d.l100a1_075; e.l100a2_075 = d.l100a2_075; e.l111a1_075 = d.l111a1_075; e.l111a2_075 = d.l111a2_075;
+        e.F11 = d.F11; e.F12 = d.F12; e.F44h = d.F44h;
         e.flags = d.flags; e.cubic_c = d.cubic_c;
     }
     for (int it = tid; it < UR; it += blockDim.x) {

@@ -106,6 +106,8 @@ struct gf_engine {
     double* Hnu[3] = {nullptr, nullptr, nullptr};
     double* fg[9] = {};
     double* strain_c[6] = {};
+    double* flexo_sg[6] = {};          // flexoelectric scratch (StageIOT::sg, pge)
+    double* flexo_pge[6] = {};
     int el_chunk = 1;                  // x-planes per block of k_elastic_tile
     int el_nmat = 0;                   // materials staged by k_elastic_tile
     size_t el_smem = 0;                // its dynamic shared memory
@@ -326,6 +328,9 @@ DevMat make_devmat(const Material& m, double dt) {
         d.fe_coef = -1. * dt / m.fe_mass;
         d.fe_damp = d.fe_coef * m.fe_damping;
     }
+    d.tv4 = m.tv[3]; d.tv5 = m.tv[4]; d.tv6 = m.tv[5]; d.tv7 = m.tv[6]; d.tv8 = m.tv[7];
+    d.f11 = m.f11; d.f12 = m.f12; d.f44x2 = 2. * m.f44;
+    d.F11 = m.F11; d.F12 = m.F12; d.F44h = m.F44 / 2.;
     d.er = m.er; d.cond = m.cond;
     for (int k = 0; k < 3; k++) { d.comp[k] = m.comp[k]; d.wp[k] = m.wp[k]; d.rtau[k] = 1. / m.tau[k]; }
     return d;
@@ -338,7 +343,6 @@ std::string unsupported(const Deck& d) {
     // kernels index cells and Yee vertices with 32-bit integers
     if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
         return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
-    if (d.flexo) return "flexoelectricity (if_flexo) is not supported by this engine";
     if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
     if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
     if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this engine";
@@ -455,6 +459,7 @@ void build_params(gf_engine* eng) {
     P.has_hext_nonunif = d.read_Hext_nonunif;
     P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
+    P.flexo = (d.flexo && d.any_fe) ? 1 : 0;
     P.drude = 0; P.pec = 0;
     if (d.em_dynamic)
         for (const Material& m : d.mats) {
@@ -673,6 +678,7 @@ void build_io(gf_engine* eng) {
             io.Hnu = f3(eng->Hnu);
             for (int a = 0; a < 9; a++) io.fg[a] = eng->fg[a];
             for (int a = 0; a < 6; a++) io.strain_c[a] = eng->strain_c[a];
+            for (int a = 0; a < 6; a++) { io.sg[a] = eng->flexo_sg[a]; io.pge[a] = eng->flexo_pge[a]; }
             for (int a = 0; a < 6; a++) { io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr; }
             io.liao_hist = eng->liao_hist;
             io.liao_last = eng->liao_last;
@@ -736,6 +742,10 @@ void build_io_mixed(gf_engine* eng) {
             io.Hnu = f3f(eng->Hnu);
             for (int a = 0; a < 9; a++) io.fg[a] = reinterpret_cast<float*>(eng->fg[a]);
             for (int a = 0; a < 6; a++) io.strain_c[a] = reinterpret_cast<float*>(eng->strain_c[a]);
+            for (int a = 0; a < 6; a++) {
+                io.sg[a] = reinterpret_cast<float*>(eng->flexo_sg[a]);
+                io.pge[a] = reinterpret_cast<float*>(eng->flexo_pge[a]);
+            }
             io.liao_hist = reinterpret_cast<float*>(eng->liao_hist);
             io.liao_last = reinterpret_cast<float*>(eng->liao_last);
             io.msrc = eng->demag_src_fused ? reinterpret_cast<float*>(eng->Mfft) : nullptr;
@@ -915,6 +925,9 @@ int enqueue_stage(gf_engine* eng, int parity) {
     const StageIOT<R>& io = stage_io<R>(eng, parity, S);
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
+    if (P.flexo)
+        GF_CU(klaunch(eng, "k_flexo_prep", k_flexo_prep<R>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
+                      dim3(kThreads), 0, st, P, io));
     if (P.elastic) {
         const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
                         (P.nx + eng->el_chunk - 1) / eng->el_chunk);
@@ -933,8 +946,11 @@ int enqueue_stage(gf_engine* eng, int parity) {
                                   dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
     if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S, R>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
                                    dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
-    if (P.fe) GF_CU(klaunch(eng, "k_fe", k_fe<S, R>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
-                            dim3(kThreads), 0, st, P, io));
+    if (P.fe) {
+        const dim3 g(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx);
+        if (P.flexo) GF_CU(klaunch(eng, "k_fe", k_fe<S, R, true>, g, dim3(kThreads), 0, st, P, io));
+        else GF_CU(klaunch(eng, "k_fe", k_fe<S, R, false>, g, dim3(kThreads), 0, st, P, io));
+    }
     if (P.em) {
         const long nx = P.nx, ny = P.ny, nz = P.nz;
         GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
@@ -1566,6 +1582,13 @@ int create_from(gf_engine* eng, const std::string& dir, int device, int precisio
     // and to the FP64 TDGL kernel
     if (d.elastodynamics && P.elasto_on && (P.fm || P.afm || (P.fe && !eng->mixed)))
         for (int a = 0; a < 6; a++) GF_TRY(dalloc_r(eng, &eng->strain_c[a], (size_t)n));
+    // flexoelectricity: global-frame cell strain and eigenstrain p-gradients
+    // of the stage state (k_flexo_prep)
+    if (P.flexo)
+        for (int a = 0; a < 6; a++) {
+            if (d.elastodynamics) GF_TRY(dalloc_r(eng, &eng->flexo_sg[a], (size_t)n));
+            GF_TRY(dalloc_r(eng, &eng->flexo_pge[a], (size_t)n));
+        }
     if (d.elastodynamics) GF_TRY(setup_elastic_tile(eng));
     if (d.elastodynamics) {
         const size_t plane = (size_t)P.nx * P.ny;

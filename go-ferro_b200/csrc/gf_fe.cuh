@@ -19,17 +19,18 @@ __device__ inline bool is_fe(const DevMatT<R>* mats, uint8_t id) {
     return id != 0 && (mats[id - 1].flags & MF_FE);
 }
 
-// Crystal-frame cell strain of the stage displacement of cell (i,j,k)
-// (Dexx_crt ..., get_dudxyz_glb + get_Dstrain, elastic_dynamic_solver.cpp:
+// Global-frame cell strain of the stage displacement of cell (i,j,k)
+// (Dexx_glb ..., get_dudxyz_glb + get_Dstrain, elastic_dynamic_solver.cpp:
 // 106-227), formed from u_in directly: the face-normal gradient on each of
 // the six faces (0 on stress-free faces: a non-periodic end face, or vacuum
 // on either side), averaged per component exactly as the stored face
-// gradients are in k_elastic_tile, then rotated to the crystal frame.
-// nb = the six neighbours' cell indices (-x, +x, -y, +y, -z, +z, wrapped),
-// solid_nb = whether each neighbour is a material cell.
+// gradients are in k_elastic_tile.  nb = the six neighbours' cell indices
+// (-x, +x, -y, +y, -z, +z, wrapped), solid_nb = whether each neighbour is a
+// material cell.  gn, when given, receives the normal gradients
+// gn[d][0 / 1] = d u_d / d x_d on the -d / +d face.
 template <class R>
-__device__ inline void fe_cell_strain(const Params& P, const StageIOT<R>& io, int i, int j, int k, int c,
-                                      const int nb[6], const bool solid_nb[6], bool solid, R e[6]) {
+__device__ inline void cell_strain_glb(const Params& P, const StageIOT<R>& io, int i, int j, int k, int c,
+                                       const int nb[6], const bool solid_nb[6], bool solid, R e[6], R (*gn)[2] = nullptr) {
     R g[3][2][3];   // g[d][0 / 1][a]: d u_a / d x_d on the -d / +d face
     const int pos[3] = {i, j, k}, n[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
     const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
@@ -57,10 +58,89 @@ __device__ inline void fe_cell_strain(const Params& P, const StageIOT<R>& io, in
     e[3] = (g[2][0][1] + g[2][1][1] + g[1][0][2] + g[1][1][2]) / R(4.);
     e[4] = (g[2][0][0] + g[2][1][0] + g[0][0][2] + g[0][1][2]) / R(4.);
     e[5] = (g[1][0][0] + g[1][1][0] + g[0][0][1] + g[0][1][1]) / R(4.);
+    if (gn) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) { gn[d][0] = g[d][0][d]; gn[d][1] = g[d][1][d]; }
+    }
+}
+
+// Crystal-frame cell strain (Dexx_crt ...): cell_strain_glb rotated with Tg2c.
+template <class R>
+__device__ inline void fe_cell_strain(const Params& P, const StageIOT<R>& io, int i, int j, int k, int c,
+                                      const int nb[6], const bool solid_nb[6], bool solid, R e[6]) {
+    cell_strain_glb(P, io, i, j, k, c, nb, solid_nb, solid, e);
     if (P.rot) {
         R t3[3][3] = {{e[0], e[5], e[4]}, {e[5], e[1], e[3]}, {e[4], e[3], e[2]}}, o3[3][3];
         rot_tensor(Tg2c<R>(P), t3, o3);
         e[0] = o3[0][0]; e[1] = o3[1][1]; e[2] = o3[2][2]; e[3] = o3[1][2]; e[4] = o3[0][2]; e[5] = o3[0][1];
+    }
+}
+
+// Neighbour indices of cell (i,j,k), wrapped: -x, +x, -y, +y, -z, +z.
+__device__ inline void cell_neighbours(const Params& P, int i, int j, int k, int nb[6]) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
+    const int jb = (j == 0) ? ny - 1 : j - 1, jF = (j == ny - 1) ? 0 : j + 1;
+    const int kb = (k == 0) ? nz - 1 : k - 1, kF = (k == nz - 1) ? 0 : k + 1;
+    nb[0] = (ib * ny + j) * nz + k; nb[1] = (iF * ny + j) * nz + k;
+    nb[2] = (i * ny + jb) * nz + k; nb[3] = (i * ny + jF) * nz + k;
+    nb[4] = (i * ny + j) * nz + kb; nb[5] = (i * ny + j) * nz + kF;
+}
+
+// Flexoelectric inputs of one RK stage, from the stage state, one thread per
+// cell (run before the stage's elastic and TDGL kernels):
+//  * sg: the global-frame cell strain of every cell (get_Dstrain,
+//    elastic_dynamic_solver.cpp:189-227, which update_u_RK* recomputes after
+//    each displacement update), read by k_fe for the strain gradients;
+//  * pge: the polarisation-gradient combinations of the dynamic eigenstrain
+//    (elastic_dynamic_solver.cpp:63-70) from get_p_gradient
+//    (ferroelectric_solver.cpp:133-280: central differences of p_store with
+//    the mirror condition at ferroelectric surfaces), zero outside
+//    ferroelectric cells.
+template <class R>
+__global__ void __launch_bounds__(256) k_flexo_prep(Params P, StageIOT<R> io) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.ny * P.nz) return;
+    const int i = blockIdx.y, j = t / P.nz, k = t - (t / P.nz) * P.nz;
+    const int c = (i * P.ny + j) * P.nz + k;
+    const uint8_t id = io.mid[c];
+    int nb[6];
+    cell_neighbours(P, i, j, k, nb);
+    if (P.elastic) {
+        const bool solid_nb[6] = {io.mid[nb[0]] != 0, io.mid[nb[1]] != 0, io.mid[nb[2]] != 0,
+                                  io.mid[nb[3]] != 0, io.mid[nb[4]] != 0, io.mid[nb[5]] != 0};
+        R e[6];
+        cell_strain_glb(P, io, i, j, k, c, nb, solid_nb, id != 0, e);
+#pragma unroll
+        for (int a = 0; a < 6; a++) io.sg[a][c] = e[a];
+    }
+    if (io.pge[0]) {
+        R g[6] = {R(0.), R(0.), R(0.), R(0.), R(0.), R(0.)};
+        if (id != 0 && ((P.fe_mask >> (id - 1)) & 1u)) {
+            const int pos[3] = {i, j, k}, n[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
+            const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
+            const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
+            R dp[3][3];   // dp[a][d] = d p_a / d x_d
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const uint8_t ib = io.mid[nb[2 * d]], iF = io.mid[nb[2 * d + 1]];
+                const bool sb = (pos[d] == 0 && !per[d]) || !(ib != 0 && ((P.fe_mask >> (ib - 1)) & 1u));
+                const bool sf = (pos[d] == n[d] - 1 && !per[d]) || !(iF != 0 && ((P.fe_mask >> (iF - 1)) & 1u));
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const R pc = io.p_in.c[a][c];
+                    const R pb = sb ? pc : io.p_in.c[a][nb[2 * d]];
+                    const R pf = sf ? pc : io.p_in.c[a][nb[2 * d + 1]];
+                    dp[a][d] = qdivR(pf - pb, h[d], rh[d], rhf[d]) / R(2.);
+                }
+            }
+            g[0] = dp[0][0]; g[1] = dp[1][1]; g[2] = dp[2][2];
+            g[3] = dp[1][2] + dp[2][1];
+            g[4] = dp[0][2] + dp[2][0];
+            g[5] = dp[1][0] + dp[0][1];
+        }
+#pragma unroll
+        for (int a = 0; a < 6; a++) io.pge[a][c] = g[a];
     }
 }
 
@@ -71,7 +151,9 @@ __device__ inline void fe_cell_strain(const Params& P, const StageIOT<R>& io, in
 #ifndef GF_FE_MINB_F64
 #define GF_FE_MINB_F64 3
 #endif
-template <int S, class R = double>
+template <int S, class R = double, bool FX = false>
+// FX: the run has flexoelectricity (the polarisation- and strain-gradient
+// terms of get_dq_RK*, ferroelectric_solver.cpp:800-833).
 // FP64 (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4
 // blocks); FP32 (256, 4): 64 registers, 32 warps.  With the RK operands of
 // all three components gathered before the first store: 0.61 ms (FP64) and
@@ -119,6 +201,9 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
         const float rhf[3] = {P.f.rdx, P.f.rdy, P.f.rdz};
         R lap[3];   // sum of the three second derivatives per component
+        // flexoelectric runs keep each second derivative and the first
+        // derivatives of get_p_gradient (same mirrored neighbours)
+        R d2s[3][3], dp[3][3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             const R pc = io.p_in.c[a][c];
@@ -128,6 +213,10 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
                 const R pb = surf[2 * dir] ? pc : pn[a][2 * dir];
                 const R pf = surf[2 * dir + 1] ? pc : pn[a][2 * dir + 1];
                 d2[dir] = qdivR(qdivR(pf - R(2.) * pc + pb, h[dir], rh[dir], rhf[dir]), h[dir], rh[dir], rhf[dir]);
+                if constexpr (FX) {
+                    d2s[a][dir] = d2[dir];
+                    dp[a][dir] = qdivR(pf - pb, h[dir], rh[dir], rhf[dir]) / R(2.);
+                }
             }
             lap[a] = d2[0] + d2[1] + d2[2];
         }
@@ -232,6 +321,74 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
             dq[0] = dq[0] - fm * Ecx;
             dq[1] = dq[1] - fm * Ecy;
             dq[2] = dq[2] - fm * Ecz;
+        }
+
+        if constexpr (FX) {
+            // strain gradients of the stage displacement (get_Dstrain_gradient,
+            // elastic_dynamic_solver.cpp:229-399): eg[q][d] = d e_q / d x_d of
+            // the global-frame cell strain (q = xx, yy, zz, yz, xz, xy).  The
+            // normal component differentiates the face gradients of the two
+            // d-faces; the others take central differences of the
+            // neighbours' strains, one-sided next to a stress-free face and
+            // zero between two.  Zero without elastodynamics.
+            R eg[6][3];
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+#pragma unroll
+                for (int d = 0; d < 3; d++) eg[q][d] = R(0.);
+            if (P.elastic) {
+                const int pos[3] = {i, j, k}, n[3] = {nx, ny, nz}, per[3] = {P.per_x, P.per_y, P.per_z};
+                // the components each direction needs besides its normal one
+                constexpr int need[3][4] = {{1, 2, 5, 4}, {0, 2, 5, 3}, {0, 1, 3, 4}};
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const bool fb = (pos[d] == 0 && !per[d]) || idn[2 * d] == 0;
+                    const bool ff = (pos[d] == n[d] - 1 && !per[d]) || idn[2 * d + 1] == 0;
+                    const R* ud = io.u_in.c[d];
+                    const R uc = ud[c];
+                    const R gb = fb ? R(0.) : qdivR((uc - ud[nb[2 * d]]), h[d], rh[d], rhf[d]);
+                    const R gf = ff ? R(0.) : qdivR((ud[nb[2 * d + 1]] - uc), h[d], rh[d], rhf[d]);
+                    eg[d][d] = qdivR(gf - gb, h[d], rh[d], rhf[d]);
+                    // the cell itself stands in for the neighbour across a
+                    // stress-free face; the step is two cells only when
+                    // neither face is free
+                    const int cb = fb ? c : nb[2 * d];
+                    const int cf = ff ? c : nb[2 * d + 1];
+                    const bool two = !fb && !ff;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        const int q = need[d][r];
+                        const R v = qdivR(io.sg[q][cf] - io.sg[q][cb], h[d], rh[d], rhf[d]);
+                        eg[q][d] = two ? v / R(2.) : v;
+                    }
+                }
+            }
+            // the flexoelectric effective field of each component, in the
+            // reference's term order
+            const R ax = mt.tv4 * pxg * dp[0][0]
+                + mt.tv5 * (pyg * dp[1][0] + pzg * dp[2][0])
+                + mt.tv6 * (pxg * dp[1][1] + pxg * dp[2][2] + pyg * dp[0][1] + pzg * dp[0][2])
+                - mt.tv7 * d2s[0][0]
+                - mt.tv8 * (d2s[0][2] + d2s[0][1])
+                - mt.f11 * eg[0][0] - mt.f12 * (eg[1][0] + eg[2][0])
+                - mt.f44x2 * (eg[5][1] + eg[4][2]);
+            const R ay = mt.tv4 * pyg * dp[1][1]
+                + mt.tv5 * (pxg * dp[0][1] + pzg * dp[2][1])
+                + mt.tv6 * (pyg * dp[0][0] + pyg * dp[2][2] + pxg * dp[1][0] + pzg * dp[1][2])
+                - mt.tv7 * d2s[1][1]
+                - mt.tv8 * (d2s[1][0] + d2s[1][2])
+                - mt.f11 * eg[1][1] - mt.f12 * (eg[0][1] + eg[2][1])
+                - mt.f44x2 * (eg[5][0] + eg[3][2]);
+            const R az = mt.tv4 * pzg * dp[2][2]
+                + mt.tv5 * (pxg * dp[0][2] + pyg * dp[1][2])
+                + mt.tv6 * (pzg * dp[0][0] + pzg * dp[1][1] + pxg * dp[2][0] + pyg * dp[2][1])
+                - mt.tv7 * d2s[2][2]
+                - mt.tv8 * (d2s[2][0] + d2s[2][1])
+                - mt.f11 * eg[2][2] - mt.f12 * (eg[0][2] + eg[1][2])
+                - mt.f44x2 * (eg[3][1] + eg[4][0]);
+            dq[0] = dq[0] + fm * ax;
+            dq[1] = dq[1] + fm * ay;
+            dq[2] = dq[2] + fm * az;
         }
     }
 

@@ -68,6 +68,14 @@ struct StageIOT {
     // whole grid and the run has no antiferromagnet; null otherwise (a
     // separate source kernel then forms it)
     R* msrc;
+    // flexoelectric scratch (null without flexoelectricity), written by
+    // k_flexo_prep at the start of each stage from the stage state: sg = the
+    // global-frame cell strain of the stage displacement (Dexx_glb ...), pge =
+    // the polarisation-gradient combinations the dynamic eigenstrain uses
+    // (dpx/dx, dpy/dy, dpz/dz, dpy/dz + dpz/dy, dpx/dz + dpz/dx,
+    // dpy/dx + dpx/dy; zero outside ferroelectric cells)
+    R* sg[6];
+    R* pge[6];
     // geometry / materials / time
     const uint8_t* mid;
     const DevMatT<R>* mats;

@@ -206,6 +206,7 @@ class Deck:
     # electrostatic solver settings (read.cpp:56): scale of the homogeneous
     # reference permittivity, iteration limit, tolerance
     spin_pumping: bool = False
+    flexo: bool = False          # if_flexo (flexoelectric coupling)
     scale_elec: float = 1.0
     elec_limit: int = 0
     elec_tol: float = 1e-8
@@ -314,7 +315,7 @@ class Deck:
              "1.0 0 1e-8",
              f"{_b(self.abc_1D)} {_b(self.abc_elast_onlytop)} {_b(self.abc_em_onlytop)} {_f(self.liao_w)}",
              "false false",
-             "false",
+             f"{_b(self.flexo)}",
              f"{_b(self.spin_pumping)}",
              f"{_b(self.m0 is not None)} {_b(self.afm0 is not None)} false",
              f"{_b(self.p0 is not None)} false",

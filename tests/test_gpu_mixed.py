@@ -64,7 +64,8 @@ def test_mixed_matches_golden(gf, tmp_path, name):
 @pytest.mark.parametrize("vname", ["mur_elastic_gauss_source", "traction_source_open_box", "fe_jf6_plane_wave_eext",
                                    "two_fm_materials_dmi_uniaxial", "demag_factor", "elastic_multi_tile",
                                    "fm_film_demag_substrate", "rotated_magnetoelastic", "rotated_ferroelectric",
-                                   "jf_type1", "jf_type3", "jf_type5", "mag_1d_model"])
+                                   "jf_type1", "jf_type3", "jf_type5", "mag_1d_model", "flexo_fe_film",
+                                   "flexo_rotated", "flexo_no_elastic"])
 def test_mixed_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))

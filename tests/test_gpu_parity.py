@@ -279,6 +279,26 @@ def _variants(gf):
     d.m0 = D.tilt_m0((8, 8, 10), 41, d.material_cell() == 2, max_deg=10.0)
     d.mag_1D = True
     v["mag_1d_model"] = (d, 15, None)
+    # flexoelectric coupling (if_flexo): polarisation- and strain-gradient
+    # terms of the TDGL field (ferroelectric_solver.cpp:800-833), the
+    # p-gradient eigenstrain (elastic_dynamic_solver.cpp:63-70), with the
+    # ferroelectric film between an elastic dielectric substrate and vacuum
+    # so the mirror (p) and stress-free (strain) surface rules both act
+    for vn, rot, elastic in (("flexo_fe_film", None, True), ("flexo_rotated", (25.0, -40.0), True),
+                             ("flexo_no_elastic", None, False)):
+        d = D.preset_ferroelectric(nx=8, ny=8, nz=12, steps=20, pulse=elastic)
+        d.materials = [dataclasses.replace(D.pto(), f11=6.0, f12=3.5, f44=2.5), D.ggg()]
+        d.layers = [(3, 2), (6, 1), (3, 0)]
+        r = D.splitmix64(20240917, 3 * d.n).reshape(d.n, 3)
+        d.p0 = (0.1 * r - 0.05).T.reshape(3, 8, 8, 12).copy() * (d.material_cell() == 1)
+        d.q0 = np.zeros_like(d.p0)
+        d.flexo = True
+        if rot:
+            d.Tg2c = D.rotation(*rot)
+        if not elastic:
+            d.elastic = d.elasto_back = d.elasto_on = d.abc_1D = False
+            d.em = d.em_fromP = d.em_back_P = False
+        v[vn] = (d, 20, (4, 4, 5) if elastic else None)
     return v
 
 
@@ -302,7 +322,8 @@ def test_random_struct_variants_cover_both_yee_paths(gf):
                                    "afm_film_demag", "afm_magnetoelastic_em", "fm_on_afm_prescribed_h",
                                    "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
                                    "random_struct_6mat", "rotated_magnetoelastic", "rotated_ferroelectric",
-                                   "jf_type0", "jf_type1", "jf_type2", "jf_type3", "jf_type5", "mag_1d_model"])
+                                   "jf_type0", "jf_type1", "jf_type2", "jf_type3", "jf_type5", "mag_1d_model",
+                                   "flexo_fe_film", "flexo_rotated", "flexo_no_elastic"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
