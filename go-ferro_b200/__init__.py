@@ -29,7 +29,8 @@ ERRORS = {-1: "GF_EINVAL", -2: "GF_EIO", -3: "GF_ECUDA", -4: "GF_ENOMEM", -5: "G
 
 FIELD = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "q": 4, "u": 5, "v": 6,
          "Ex": 7, "Ey": 8, "Ez": 9, "Hx": 10, "Hy": 11, "Hz": 12,
-         "Hstat": 13, "Estat": 14, "E_cell": 15, "H_cell": 16, "strain": 17}
+         "Hstat": 13, "Estat": 14, "E_cell": 15, "H_cell": 16, "strain": 17,
+         "strain_static": 18, "eigenstrain_static": 19}
 OBS = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "u": 4}
 PRECISION = {"fp64": 0, "mixed": 1}   # GF_PRECISION_FP64, GF_PRECISION_MIXED_FP32
 
@@ -41,7 +42,7 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
            "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
-           "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics",
+           "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics", "gf_set_elastostatics",
            "gf_save_state", "gf_load_state", "gf_create", "gf_set_table", "gf_stage_begin", "gf_stage_commit",
            "gf_static_solve"]
 
@@ -88,7 +89,8 @@ class GFRunParams(ctypes.Structure):
                 ("if_gaussian_strain_pulse", _i32), ("input_strain_type", _i32), ("input_strain_sourcez", _i32),
                 ("input_strain_component", _ch), ("pad2_", _ch * 7), ("sigma_gauss", _d), ("amplitude_gauss", _d),
                 ("num_strain_cycles", _u64), ("if_elastostatic", _i32), ("if_flexo", _i32), ("if_prescribed_m", _i32),
-                ("if_spin_pumping", _i32)]
+                ("if_spin_pumping", _i32), ("scale_elasto", _d), ("elasto_solver_limit", _i32),
+                ("elasto_solver_tol", _d)]
 
 
 def material_params(m) -> GFMaterialParams:
@@ -150,6 +152,9 @@ def run_params(d) -> GFRunParams:
     r.sigma_gauss, r.amplitude_gauss, r.num_strain_cycles = d.sigma_gauss, d.amp_gauss, int(d.strain_cycles)
     r.if_spin_pumping = int(d.spin_pumping)
     r.if_flexo = int(d.flexo)
+    r.if_elastostatic = int(d.elastostatic)
+    r.scale_elasto, r.elasto_solver_limit, r.elasto_solver_tol = d.scale_elasto, int(d.elasto_limit), d.elasto_tol
+    r.if_elec_1Dmodel, r.if_elec_1D_compensate = int(d.elec_1D), int(d.elec_1D_comp)
     return r
 
 
@@ -222,6 +227,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_adjoint_destroy.argtypes = [vp]
     lib.gf_adjoint_destroy.restype = None
     lib.gf_set_electrostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
+    lib.gf_set_elastostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
     lib.gf_save_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_load_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
@@ -371,6 +377,13 @@ class Engine:
         set-up iteration count."""
         used = ctypes.c_int()
         self._check(self.lib.gf_set_electrostatics(self.h, int(bool(enable)), ctypes.byref(used)))
+        return used.value
+
+    def set_elastostatics(self, enable: bool = True) -> int:
+        """Enable the elastostatic (static strain) solve; returns the set-up
+        iteration count."""
+        used = ctypes.c_int()
+        self._check(self.lib.gf_set_elastostatics(self.h, int(bool(enable)), ctypes.byref(used)))
         return used.value
 
     def check_finite(self) -> None:

@@ -101,6 +101,7 @@ struct Params {
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;
     int flexo;                // if_flexo with ferroelectrics: StageIOT::sg / pge are set
+    int elastostatic;         // if_elastostatic: the TDGL field adds the static strain and eigenstrain
     double liao_w;
     // elastic boundary coefficients (elastodynamics_AbsorbingBoundary.cpp)
     double vs_long_1st, vs_tran_1st, vs_long_last, vs_tran_last;

@@ -402,6 +402,7 @@ std::string deck_from_params(const gf_run_params& r, const gf_material_params* m
     d.sigma_gauss = r.sigma_gauss; d.amp_gauss = r.amplitude_gauss; d.strain_cycles = r.num_strain_cycles;
     d.elastostatic = r.if_elastostatic != 0; d.flexo = r.if_flexo != 0; d.prescribed_m = r.if_prescribed_m != 0;
     d.spin_pumping = r.if_spin_pumping != 0;
+    d.scale_elasto = r.scale_elasto; d.elasto_limit = (unsigned)r.elasto_solver_limit; d.elasto_tol = r.elasto_solver_tol;
 
     d.mats.assign((size_t)nmat, Material());
     for (int i = 0; i < nmat; i++) {

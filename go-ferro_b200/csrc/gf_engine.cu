@@ -39,6 +39,7 @@
 #include "gf_util.cuh"
 #include "gf_adjoint.cuh"
 #include "gf_elec.cuh"
+#include "gf_elasto.cuh"
 
 using namespace gf;
 
@@ -138,6 +139,28 @@ struct gf_engine {
     double* elec_blockmax = nullptr;       // 2 x kElecBlocks
     cufftHandle elec_r2c = 0, elec_c2r = 0;
     bool elec_plans = false;
+    bool elec_1d = false;                  // the 1-D model replaces the spectral solve
+    double* elec_pz_t0 = nullptr;          // P_z when the compensated 1-D model was enabled (type R)
+    // static strain exxt0_crt and static eigenstrain exx0t0_crt (type R, 6
+    // arrays each; null when absent): strain_stat.in / eigenstraint0_crt.in
+    // or the elastostatic solve (gf_set_elastostatics)
+    double* es_eps[6] = {};
+    double* es_eig[6] = {};
+    bool es_on = false, es_per_step = false;
+    int es_iters = 1;                      // iterations of each per-step solve
+    double es_ch[3] = {0., 0., 0.};        // C_h: c11, c12, c44
+    EsMats es_mats = {};                   // crystal-frame cubic constants per material
+    double* es_x = nullptr;                // 6 x n FP64 strain iterate
+    double* es_e0 = nullptr;               // 6 x n FP64 static eigenstrain
+    double* es_r = nullptr;                // 6 x n FP64 tau / inverse transform
+    cufftDoubleComplex* es_k = nullptr;    // 6 x n21
+    double* es_G = nullptr;                // 6 x n21 Green tensor (11 22 33 12 13 23)
+    double* es_kq = nullptr;               // 3 x n21 crystal-frame wave vector
+    int* es_nyq_idx = nullptr;             // n21: row of es_nyq_op, -1 off the Nyquist planes
+    double* es_nyq_op = nullptr;           // 36 per Nyquist point: sign-averaged operator
+    double* es_blockmax = nullptr;
+    cufftHandle es_r2c = 0, es_c2r = 0;
+    bool es_plans = false;
 
     StageIO io[2][4];
     StageIOT<float> iof[2][4];             // mixed form
@@ -344,8 +367,11 @@ std::string unsupported(const Deck& d) {
     if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
         return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
     if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
-    if (d.elastostatic || d.read_strain_ext) return "the elastostatic solver is absent from the reference sources; if_elastostatic must be false";
-    if (d.in_straint0 || d.in_eig0 || d.in_force || d.in_Jp) return "restart inputs straint0 / eigenstraint0 / elastoforce / Jp are not supported by this engine";
+    if (d.elastostatic_1D || d.elastostatic_film || d.read_strain_ext)
+        return "the 1-D and film elastostatic models and external strain (if_elastostatic_1D, if_elastostatic_film, if_read_strain_ext) are not supported by this engine";
+    if (d.flexo && (d.elastostatic || d.in_straint0))
+        return "flexoelectricity with a static strain (if_elastostatic or strain_stat.in) is not supported by this engine";
+    if (d.in_force || d.in_Jp) return "restart inputs elastoforce / Jp are not supported by this engine";
     if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
     if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this engine";
     for (size_t i = 0; i < d.mats.size(); i++) {
@@ -460,6 +486,7 @@ void build_params(gf_engine* eng) {
     P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
     P.flexo = (d.flexo && d.any_fe) ? 1 : 0;
+    P.elastostatic = d.elastostatic ? 1 : 0;
     P.drude = 0; P.pec = 0;
     if (d.em_dynamic)
         for (const Material& m : d.mats) {
@@ -679,7 +706,7 @@ void build_io(gf_engine* eng) {
             for (int a = 0; a < 9; a++) io.fg[a] = eng->fg[a];
             for (int a = 0; a < 6; a++) io.strain_c[a] = eng->strain_c[a];
             for (int a = 0; a < 6; a++) { io.sg[a] = eng->flexo_sg[a]; io.pge[a] = eng->flexo_pge[a]; }
-            for (int a = 0; a < 6; a++) { io.eps0_c[a] = nullptr; io.eig0_c[a] = nullptr; }
+            for (int a = 0; a < 6; a++) { io.eps0_c[a] = eng->es_eps[a]; io.eig0_c[a] = eng->es_eig[a]; }
             io.liao_hist = eng->liao_hist;
             io.liao_last = eng->liao_last;
             io.msrc = eng->demag_src_fused ? eng->Mfft : nullptr;
@@ -745,6 +772,8 @@ void build_io_mixed(gf_engine* eng) {
             for (int a = 0; a < 6; a++) {
                 io.sg[a] = reinterpret_cast<float*>(eng->flexo_sg[a]);
                 io.pge[a] = reinterpret_cast<float*>(eng->flexo_pge[a]);
+                io.eps0_c[a] = reinterpret_cast<const float*>(eng->es_eps[a]);
+                io.eig0_c[a] = reinterpret_cast<const float*>(eng->es_eig[a]);
             }
             io.liao_hist = reinterpret_cast<float*>(eng->liao_hist);
             io.liao_last = reinterpret_cast<float*>(eng->liao_last);
@@ -969,9 +998,15 @@ int enqueue_stage(gf_engine* eng, int parity) {
         if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, io.a1_out, io.a2_out, true, io.msrc != nullptr));
         else GF_TRY(demag_solve(eng, io.m_out, io.a1_out, io.a2_out, true, io.msrc != nullptr));
     }
-    if constexpr (!is_mixed<R>::value) {
-        // electrostatic field of the new stage polarisation (main.cpp:299-302)
-        if (eng->elec_on && eng->elec_per_stage) GF_TRY(elec_solve(eng, io.p_out, true, eng->elec_iters, 0., nullptr));
+    if (eng->elec_on && eng->elec_per_stage) {
+        // electrostatic field of the new stage polarisation (main.cpp:299-302;
+        // the 1-D model after every p update, ferroelectric_solver.cpp:1897-1990)
+        if (eng->elec_1d) {
+            GF_CU(klaunch(eng, "k_elec_1d", k_elec_1d<R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st,
+                          P, io.mats, io.mid, (const R*)io.p_out.c[2], (const R*)reinterpret_cast<R*>(eng->elec_pz_t0), io.Estat));
+        } else if constexpr (!is_mixed<R>::value) {
+            GF_TRY(elec_solve(eng, io.p_out, true, eng->elec_iters, 0., nullptr));
+        }
     }
     return GF_OK;
 }
@@ -1041,10 +1076,21 @@ int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms) { return time_tile_t
 #else
 namespace {
 
+int es_solve(gf_engine* eng, int parity, bool counted, int iters, double tol, int* used);
+int elec_1d_now(gf_engine* eng, int parity);
+
+// work after the fourth stage: the elastostatic solve of the new state when
+// it runs without elastodynamics (main.cpp:472-474)
+int step_end(gf_engine* eng, int parity, bool counted) {
+    if (eng->es_on && eng->es_per_step) GF_TRY(es_solve(eng, 1 - parity, counted, eng->es_iters, 0., nullptr));
+    return GF_OK;
+}
+
 int enqueue_step(gf_engine* eng, int parity) {
     eng->launch_counter = 0;
     if (eng->mixed) GF_TRY(gf_mixed_enqueue_step(eng, parity));
     else GF_TRY(enqueue_step_t<double>(eng, parity));
+    GF_TRY(step_end(eng, parity, true));
     GF_CU(klaunch(eng, "k_step_inc", k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
     eng->launches_per_step = eng->launch_counter;
     return GF_OK;
@@ -1214,6 +1260,56 @@ int replicate_state(gf_engine* eng) {
     return GF_OK;
 }
 
+// out = Tg2c in Tg2c^T with the loop and rounding order of
+// transform_matrix_glb2crt (mathlib.cpp:78-100); a copy without rotation
+void glb2crt_tensor_host(const Deck& d, const double in[3][3], double out[3][3]) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            if (!d.orient_rotate) { out[i][j] = in[i][j]; continue; }
+            out[i][j] = 0.;
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) out[i][j] = out[i][j] + d.Tg2c[i][k] * d.Tg2c[j][l] * in[k][l];
+        }
+}
+
+// Static strain (strain_stat.in: global frame, rotated to the crystal frame
+// with vacuum cells at zero, elastic_initialize.cpp:424-455) and static
+// eigenstrain (eigenstraint0_crt.in: crystal frame as read) of
+// inoutput.cpp:239-280
+int read_static_strain(gf_engine* eng, const std::string& dir) {
+    const Deck& d = eng->deck;
+    const long n = d.n();
+    std::vector<double> b6[6];
+    for (auto& b : b6) b.assign((size_t)n, 0.);
+    if (d.in_straint0) {
+        std::string e = read_restart(dir + "/strain_stat.in", d.nx, d.ny, d.nz, 6, b6);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        for (long c = 0; c < n; c++) {
+            const size_t u = (size_t)c;
+            if (d.material_cell[u] == 0) { for (auto& b : b6) b[u] = 0.; continue; }
+            const double in[3][3] = {{b6[0][u], b6[5][u], b6[4][u]}, {b6[5][u], b6[1][u], b6[3][u]}, {b6[4][u], b6[3][u], b6[2][u]}};
+            double out[3][3];
+            glb2crt_tensor_host(d, in, out);
+            b6[0][u] = out[0][0]; b6[1][u] = out[1][1]; b6[2][u] = out[2][2];
+            b6[3][u] = out[1][2]; b6[4][u] = out[0][2]; b6[5][u] = out[0][1];
+        }
+        for (int a = 0; a < 6; a++) {
+            GF_TRY(dalloc_r(eng, &eng->es_eps[a], (size_t)n));
+            GF_TRY(upload_one(eng, eng->es_eps[a], nullptr, b6[a].data(), n));
+        }
+    }
+    if (d.in_eig0) {
+        for (auto& b : b6) std::fill(b.begin(), b.end(), 0.);
+        std::string e = read_restart(dir + "/eigenstraint0_crt.in", d.nx, d.ny, d.nz, 6, b6);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        for (int a = 0; a < 6; a++) {
+            GF_TRY(dalloc_r(eng, &eng->es_eig[a], (size_t)n));
+            GF_TRY(upload_one(eng, eng->es_eig[a], nullptr, b6[a].data(), n));
+        }
+    }
+    return GF_OK;
+}
+
 int initial_state(gf_engine* eng, const std::string& dir) {
     const Deck& d = eng->deck;
     const long n = d.n();
@@ -1319,6 +1415,7 @@ int initial_state(gf_engine* eng, const std::string& dir) {
         if (!e.empty()) { eng->err = e; return GF_EIO; }
         GF_TRY(upload_vec(eng, eng->Hnu, buf, n));
     }
+    if (d.in_straint0 || d.in_eig0) GF_TRY(read_static_strain(eng, dir));
     return GF_OK;
 }
 
@@ -1763,6 +1860,12 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
             ptrs.push_back(cur(eng, eng->H)[a]); lens.push_back(eng->H.len[a]); cmps.push_back(eng->H.C[a]); break;
         }
         case GF_FIELD_HSTAT: if (!eng->Hstat[0]) break; add3(eng->Hstat, nullptr); break;
+        case GF_FIELD_STRAIN_STATIC: case GF_FIELD_EIGENSTRAIN_STATIC: {
+            double* const* f = (field == GF_FIELD_STRAIN_STATIC) ? eng->es_eps : eng->es_eig;
+            if (!f[0]) break;
+            for (int a = 0; a < 6; a++) { ptrs.push_back(f[a]); lens.push_back(P.n); cmps.push_back(nullptr); }
+            break;
+        }
         case GF_FIELD_ESTAT: if (!eng->Estat[0]) break; add3(eng->Estat, nullptr); break;
         case GF_FIELD_E_CELL: case GF_FIELD_H_CELL: {
             if (!eng->E.on) break;
@@ -1808,6 +1911,201 @@ int check(gf_engine* e) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace {
+
+// the 1-D electrostatic field of the current polarisation (state `parity`)
+int elec_1d_now(gf_engine* eng, int parity) {
+    const Params& P = eng->P;
+    const dim3 g(blocks_for((long)P.nx * P.ny, kThreads));
+    if (eng->mixed) {
+        const StageIOT<float>& io = eng->iof[parity][0];
+        GF_CU(launch(k_elec_1d<float>, g, dim3(kThreads), 0, eng->stream, P, io.mats, io.mid, (const float*)io.p_in.c[2],
+                     (const float*)reinterpret_cast<float*>(eng->elec_pz_t0), io.Estat));
+    } else {
+        const StageIO& io = eng->io[parity][0];
+        GF_CU(launch(k_elec_1d<double>, g, dim3(kThreads), 0, eng->stream, P, io.mats, io.mid, (const double*)io.p_in.c[2],
+                     (const double*)eng->elec_pz_t0, io.Estat));
+    }
+    return GF_OK;
+}
+
+// One elastostatic solve from the state of `parity` (its stage-1 inputs):
+// the static eigenstrain, then up to `iters` Khachaturyan iterations from the
+// last solution (gf_elasto.cuh), stopping early at `tol` when tol > 0 (host
+// checks, not inside a capture); the result goes to the static strain arrays
+int es_solve(gf_engine* eng, int parity, bool counted, int iters, double tol, int* used) {
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const long n = P.n, n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    const unsigned bn = blocks_for(n, kThreads);
+    auto L = [&](const char* name, auto k, dim3 g, dim3 b, auto... args) -> cudaError_t {
+        return counted ? klaunch(eng, name, k, g, b, 0, st, args...) : launch(k, g, b, 0, st, args...);
+    };
+    if (eng->mixed) GF_CU(L("k_es_eigen", k_es_eigen<float>, dim3(bn), dim3(kThreads), P, eng->iof[parity][0], eng->es_e0));
+    else GF_CU(L("k_es_eigen", k_es_eigen<double>, dim3(bn), dim3(kThreads), P, eng->io[parity][0], eng->es_e0));
+    std::vector<double> bm(2 * kElecBlocks);
+    int it = 0;
+    for (; it < iters; it++) {
+        GF_CU(L("k_es_tau", k_es_tau, dim3(bn), dim3(kThreads), P, (const uint8_t*)eng->mid, eng->es_mats, eng->es_ch[0],
+                eng->es_ch[1], eng->es_ch[2], (const double*)eng->es_x, (const double*)eng->es_e0, eng->es_r));
+        GF_FFT(cufftExecD2Z(eng->es_r2c, eng->es_r, eng->es_k));
+        GF_CU(L("k_es_green", k_es_green, dim3(blocks_for(n21, kThreads)), dim3(kThreads), n21, 1. / (double)n,
+                (const double*)eng->es_G, (const double*)eng->es_kq, (const int*)eng->es_nyq_idx,
+                (const double*)eng->es_nyq_op, eng->es_k));
+        GF_FFT(cufftExecZ2D(eng->es_c2r, eng->es_k, eng->es_r));
+        GF_CU(L("k_es_update", k_es_update, dim3(kElecBlocks), dim3(256), n, (const double*)eng->es_r, eng->es_x,
+                tol > 0. ? eng->es_blockmax : (double*)nullptr));
+        if (tol > 0.) {
+            GF_CU(cudaMemcpyAsync(bm.data(), eng->es_blockmax, sizeof(double) * bm.size(), cudaMemcpyDeviceToHost, st));
+            GF_CU(cudaStreamSynchronize(st));
+            double md = 0., me = 0.;
+            for (int b = 0; b < kElecBlocks; b++) { md = std::max(md, bm[2 * b]); me = std::max(me, bm[2 * b + 1]); }
+            if (md <= tol * me) { it++; break; }
+        }
+    }
+    if (used) *used = it;
+    double* const* o = eng->es_eps;
+    double* const* g = eng->es_eig;
+    if (eng->mixed) {
+        auto f = [](double* x) { return reinterpret_cast<float*>(x); };
+        GF_CU(L("k_es_out", k_es_out<float>, dim3(bn), dim3(kThreads), n, (const uint8_t*)eng->mid, (const double*)eng->es_x,
+                (const double*)eng->es_e0, f(o[0]), f(o[1]), f(o[2]), f(o[3]), f(o[4]), f(o[5]), f(g[0]), f(g[1]), f(g[2]),
+                f(g[3]), f(g[4]), f(g[5])));
+    } else {
+        GF_CU(L("k_es_out", k_es_out<double>, dim3(bn), dim3(kThreads), n, (const uint8_t*)eng->mid, (const double*)eng->es_x,
+                (const double*)eng->es_e0, o[0], o[1], o[2], o[3], o[4], o[5], g[0], g[1], g[2], g[3], g[4], g[5]));
+    }
+    return GF_OK;
+}
+
+// Solver buffers, plans and tables (once per engine): C_h and the crystal-
+// frame constants, the wave vectors of global.cpp:276-316 rotated to the
+// crystal frame, and the Green tensor of elastic_initialize.cpp:340-389
+int es_setup(gf_engine* eng) {
+    const Deck& d = eng->deck;
+    const Params& P = eng->P;
+    const long n = P.n, nz21 = P.nz / 2 + 1, n21 = (long)P.nx * P.ny * nz21;
+    // C_h: the largest c11, c12, c44 of all materials, times scale_elasto
+    double ch[3] = {d.mats[0].c11, d.mats[0].c12, d.mats[0].c44};
+    for (const Material& m : d.mats) { ch[0] = std::max(ch[0], m.c11); ch[1] = std::max(ch[1], m.c12); ch[2] = std::max(ch[2], m.c44); }
+    const double scale = d.scale_elasto > 0. ? d.scale_elasto : 1.;
+    for (double& c : ch) c = c * scale;
+    for (int a = 0; a < 3; a++) eng->es_ch[a] = ch[a];
+    std::memset(&eng->es_mats, 0, sizeof(eng->es_mats));
+    for (size_t i = 0; i < d.mats.size(); i++) {
+        eng->es_mats.c[i + 1][0] = d.mats[i].c11; eng->es_mats.c[i + 1][1] = d.mats[i].c12; eng->es_mats.c[i + 1][2] = d.mats[i].c44;
+    }
+    if (eng->es_x) return GF_OK;
+    if (ch[2] <= 0.) { eng->err = "elastostatics needs a material with c44 > 0"; return GF_EINVAL; }
+    const double PI = kPi;
+    const long dims[3] = {P.nx, P.ny, P.nz};
+    const double h[3] = {P.dx, P.dy, P.dz};
+    std::vector<double> kv[3];
+    for (int a = 0; a < 3; a++) {
+        const long len = (a < 2) ? dims[a] : nz21;
+        kv[a].resize((size_t)len);
+        const double dk = 2. * PI / (static_cast<double>(dims[a]) * h[a]);
+        for (long i = 0; i < len; i++) {
+            long t = i;
+            if (t > dims[a] / 2) t = t - dims[a];
+            kv[a][(size_t)i] = static_cast<double>(t) * dk;
+        }
+    }
+    const double c11 = ch[0], c12 = ch[1], c44 = ch[2];
+    const double chi = (c11 - c12 - 2. * c44) / c44;
+    // crystal-frame wave vector and Green tensor of one global wave vector
+    auto green = [&](double kx, double ky, double kz, double kq[3], double g[6]) {
+        double a = kx, b = ky, c = kz;
+        if (d.orient_rotate) {
+            a = d.Tg2c[0][0] * kx + d.Tg2c[0][1] * ky + d.Tg2c[0][2] * kz;
+            b = d.Tg2c[1][0] * kx + d.Tg2c[1][1] * ky + d.Tg2c[1][2] * kz;
+            c = d.Tg2c[2][0] * kx + d.Tg2c[2][1] * ky + d.Tg2c[2][2] * kz;
+        }
+        const double kn = std::pow(kz, 2.) + std::pow(ky, 2.) + std::pow(kx, 2.);
+        const double a2 = a * a, b2 = b * b, c2 = c * c;
+        const double d0 = (kn < 1.e-8) ? 1.
+            : c11 * std::pow(kn, 3.) + chi * (c11 + c12) * kn * (a2 * b2 + b2 * c2 + c2 * a2)
+              + chi * chi * (c11 + 2 * c12 + c44) * a2 * b2 * c2;
+        const double den = c44 * d0;
+        g[0] = (c44 * std::pow(kn, 2.) + (c11 + c12) * chi * b2 * c2 + (c11 - c44) * kn * (b2 + c2)) / den;
+        g[1] = (c44 * std::pow(kn, 2.) + (c11 + c12) * chi * c2 * a2 + (c11 - c44) * kn * (c2 + a2)) / den;
+        g[2] = (c44 * std::pow(kn, 2.) + (c11 + c12) * chi * a2 * b2 + (c11 - c44) * kn * (a2 + b2)) / den;
+        g[3] = -(c12 + c44) * (kn + chi * c2) * a * b / den;
+        g[4] = -(c12 + c44) * (kn + chi * b2) * a * c / den;
+        g[5] = -(c12 + c44) * (kn + chi * a2) * b * c / den;
+        kq[0] = a; kq[1] = b; kq[2] = c;
+    };
+    // the 6 x 6 operator tau (Voigt order, tensor components) -> de of one
+    // wave vector, accumulated into M with weight w
+    auto op6 = [&](double kx, double ky, double kz, double w, double* M) {
+        double kq[3], g[6];
+        green(kx, ky, kz, kq, g);
+        const double Gm[3][3] = {{g[0], g[3], g[4]}, {g[3], g[1], g[5]}, {g[4], g[5], g[2]}};
+        const int pi_[6] = {0, 1, 2, 1, 0, 0}, pj[6] = {0, 1, 2, 2, 2, 1};
+        for (int bcol = 0; bcol < 6; bcol++) {
+            double t[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            t[pi_[bcol]][pj[bcol]] = 1.; t[pj[bcol]][pi_[bcol]] = 1.;
+            double f[3], nv[3];
+            for (int i = 0; i < 3; i++) f[i] = t[i][0] * kq[0] + t[i][1] * kq[1] + t[i][2] * kq[2];
+            for (int i = 0; i < 3; i++) nv[i] = Gm[i][0] * f[0] + Gm[i][1] * f[1] + Gm[i][2] * f[2];
+            for (int arow = 0; arow < 6; arow++) {
+                const int i = pi_[arow], j = pj[arow];
+                M[6 * arow + bcol] += w * 0.5 * (kq[j] * nv[i] + kq[i] * nv[j]);
+            }
+        }
+    };
+    std::vector<double> G((size_t)6 * n21), KQ((size_t)3 * n21), NOP;
+    std::vector<int> NIDX((size_t)n21, -1);
+    for (long i = 0; i < P.nx; i++)
+        for (long j = 0; j < P.ny; j++)
+            for (long k = 0; k < nz21; k++) {
+                const long q = (i * P.ny + j) * nz21 + k;
+                const double kx = kv[0][(size_t)i], ky = kv[1][(size_t)j], kz = kv[2][(size_t)k];
+                double kq[3], g[6];
+                green(kx, ky, kz, kq, g);
+                for (int a = 0; a < 6; a++) G[(size_t)(a * n21 + q)] = g[a];
+                for (int a = 0; a < 3; a++) KQ[(size_t)(a * n21 + q)] = kq[a];
+                const bool nyq[3] = {P.nx % 2 == 0 && i == P.nx / 2, P.ny % 2 == 0 && j == P.ny / 2,
+                                     P.nz % 2 == 0 && k == P.nz / 2};
+                if (!(nyq[0] || nyq[1] || nyq[2])) continue;
+                const int m = (int)nyq[0] + (int)nyq[1] + (int)nyq[2];
+                NIDX[(size_t)q] = (int)(NOP.size() / 36);
+                NOP.resize(NOP.size() + 36, 0.);
+                double* M = NOP.data() + NOP.size() - 36;
+                for (int sgn = 0; sgn < 8; sgn++) {
+                    // flip only the Nyquist components; 2^m distinct combinations
+                    if (((sgn & 1) && !nyq[0]) || ((sgn & 2) && !nyq[1]) || ((sgn & 4) && !nyq[2])) continue;
+                    op6((sgn & 1) ? -kx : kx, (sgn & 2) ? -ky : ky, (sgn & 4) ? -kz : kz, 1. / (double)(1 << m), M);
+                }
+            }
+    GF_TRY(dalloc_n(eng, &eng->es_x, (size_t)6 * n));
+    GF_TRY(dalloc_n(eng, &eng->es_e0, (size_t)6 * n));
+    GF_TRY(dalloc_n(eng, &eng->es_r, (size_t)6 * n));
+    GF_TRY(dalloc_n(eng, &eng->es_k, (size_t)6 * n21));
+    GF_TRY(dalloc_n(eng, &eng->es_G, (size_t)6 * n21));
+    GF_TRY(dalloc_n(eng, &eng->es_kq, (size_t)3 * n21));
+    GF_TRY(dalloc_n(eng, &eng->es_blockmax, (size_t)2 * kElecBlocks));
+    GF_CU(cudaMemcpy(eng->es_G, G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice));
+    GF_CU(cudaMemcpy(eng->es_kq, KQ.data(), sizeof(double) * KQ.size(), cudaMemcpyHostToDevice));
+    GF_TRY(dalloc_n(eng, &eng->es_nyq_idx, (size_t)n21));
+    GF_TRY(dalloc_n(eng, &eng->es_nyq_op, std::max<size_t>(NOP.size(), 36)));
+    GF_CU(cudaMemcpy(eng->es_nyq_idx, NIDX.data(), sizeof(int) * NIDX.size(), cudaMemcpyHostToDevice));
+    if (!NOP.empty()) GF_CU(cudaMemcpy(eng->es_nyq_op, NOP.data(), sizeof(double) * NOP.size(), cudaMemcpyHostToDevice));
+    int dimsi[3] = {P.nx, P.ny, P.nz};
+    GF_FFT(cufftPlanMany(&eng->es_r2c, 3, dimsi, nullptr, 1, (int)n, nullptr, 1, (int)n21, CUFFT_D2Z, 6));
+    GF_FFT(cufftPlanMany(&eng->es_c2r, 3, dimsi, nullptr, 1, (int)n21, nullptr, 1, (int)n, CUFFT_Z2D, 6));
+    eng->es_plans = true;
+    GF_FFT(cufftSetStream(eng->es_r2c, eng->stream));
+    GF_FFT(cufftSetStream(eng->es_c2r, eng->stream));
+    for (int a = 0; a < 6; a++) {
+        if (!eng->es_eps[a]) GF_TRY(dalloc_r(eng, &eng->es_eps[a], (size_t)n));
+        if (!eng->es_eig[a]) GF_TRY(dalloc_r(eng, &eng->es_eig[a], (size_t)n));
+    }
+    return GF_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int gf_create_from_deck(const char* deck_dir, int device, gf_engine** out) {
@@ -1918,6 +2216,7 @@ int gf_stage_commit(gf_engine* e, int stage) {
     else GF_TRY(enqueue_stage_t<double>(eng, parity, stage - 1));
     eng->stage_done = stage;
     if (stage == 4) {
+        GF_TRY(step_end(eng, parity, false));
         GF_CU(launch(k_step_inc, dim3(1), dim3(1), 0, eng->stream, eng->step_ctr));
         eng->steps_done += 1;
         eng->stage_open = 0;       // stage_done stays 4 until the next step begins
@@ -1941,7 +2240,8 @@ int gf_static_solve(gf_engine* e, int which) {
         // with the solve off E_stat stays as it is, as in a build of the
         // reference's public sources, where get_E_static has no definition
         if (!eng->elec_on) return GF_OK;
-        GF_TRY(elec_solve(eng, f3(cur(eng, eng->p)), false, eng->elec_iters, 0., nullptr));
+        if (eng->elec_1d) GF_TRY(elec_1d_now(eng, (int)(eng->steps_done & 1ull)));
+        else GF_TRY(elec_solve(eng, f3(cur(eng, eng->p)), false, eng->elec_iters, 0., nullptr));
     } else {
         eng->err = "unknown static solve";
         return GF_EINVAL;
@@ -2005,7 +2305,7 @@ int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count) {
     size_t ncomp = 3;
     if (field >= GF_FIELD_EX && field <= GF_FIELD_EZ) { int c = field - GF_FIELD_EX; dx += (c != 0); dy += (c != 1); dz += (c != 2); ncomp = 1; }
     else if (field >= GF_FIELD_HX && field <= GF_FIELD_HZ) { int c = field - GF_FIELD_HX; dx += (c == 0); dy += (c == 1); dz += (c == 2); ncomp = 1; }
-    else if (field == GF_FIELD_STRAIN) ncomp = 6;
+    else if (field == GF_FIELD_STRAIN || field == GF_FIELD_STRAIN_STATIC || field == GF_FIELD_EIGENSTRAIN_STATIC) ncomp = 6;
     else if (field < 0 || field >= GF_FIELD_COUNT) { eng->err = "unknown field"; return GF_EINVAL; }
     if (dims3) { dims3[0] = dx; dims3[1] = dy; dims3[2] = dz; }
     if (count) *count = ncomp * (size_t)(dx * dy * dz);
@@ -2136,7 +2436,46 @@ std::vector<CkBlob> ck_blobs(gf_engine* eng) {
     const size_t plane = (size_t)eng->P.nx * eng->P.ny;
     if (eng->liao_hist) v.push_back({"liao_hist", eng->liao_hist, eng->esz * 4 * 12 * plane});
     if (eng->liao_last) v.push_back({"liao_last", eng->liao_last, eng->esz * 3 * plane});
+    // static strain and eigenstrain, and the elastostatic solver's FP64
+    // iterate (the start of the next per-step solve)
+    for (int a = 0; a < 6; a++) {
+        if (eng->es_eps[a]) v.push_back({"es_eps." + std::to_string(a), eng->es_eps[a], eng->esz * n});
+        if (eng->es_eig[a]) v.push_back({"es_eig." + std::to_string(a), eng->es_eig[a], eng->esz * n});
+    }
+    if (eng->es_x) v.push_back({"es_x", eng->es_x, sizeof(double) * 6 * n});
     return v;
+}
+
+int gf_set_elastostatics(gf_engine* e, int enable, int* iterations_used) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    const Deck& d = eng->deck;
+    if (iterations_used) *iterations_used = 0;
+    if (!enable) {
+        eng->es_on = false;
+    } else {
+        if (d.flexo && eng->P.flexo) {
+            eng->err = "elastostatics with flexoelectricity (static-strain gradients) is not supported";
+            return GF_EUNSUPPORTED;
+        }
+        GF_CU(cudaSetDevice(eng->device));
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        GF_TRY(es_setup(eng));
+        // the kernels read the static arrays through their stage inputs
+        build_io(eng);
+        if (eng->mixed) build_io_mixed(eng);
+        const int limit = d.elasto_limit > 0 ? (int)d.elasto_limit : 500;
+        const double tol = d.elasto_tol > 0. ? d.elasto_tol : 1e-10;
+        eng->es_iters = limit;
+        eng->es_per_step = !d.elastodynamics;
+        int used = 0;
+        GF_TRY(es_solve(eng, (int)(eng->steps_done & 1ull), false, limit, tol, &used));
+        if (iterations_used) *iterations_used = used;
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        eng->es_on = true;
+    }
+    invalidate_graphs(eng);
+    return GF_OK;
 }
 
 int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
@@ -2147,12 +2486,30 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
     if (iterations_used) *iterations_used = 0;
     if (!enable) {
         eng->elec_on = false;
+        eng->elec_1d = false;
     } else {
         if (!d.any_fe) { eng->err = "electrostatics needs a ferroelectric material"; return GF_EINVAL; }
-        if (eng->mixed) { eng->err = "the electrostatic solver runs in the FP64 form"; return GF_EUNSUPPORTED; }
-        if (d.elec_1D) { eng->err = "if_elec_1Dmodel: the 1-D electrostatic model is not implemented"; return GF_EUNSUPPORTED; }
         GF_CU(cudaSetDevice(eng->device));
         GF_CU(cudaStreamSynchronize(eng->stream));
+        if (d.elec_1D) {
+            // the 1-D model (gf_elasto.cuh): P_z(t0) of the compensated form
+            // is the polarisation now
+            const int par = (int)(eng->steps_done & 1ull);
+            if (d.elec_1D_comp) {
+                if (!eng->elec_pz_t0) GF_TRY(dalloc_r(eng, &eng->elec_pz_t0, (size_t)P.n));
+                GF_CU(cudaMemcpyAsync(eng->elec_pz_t0, cur(eng, eng->p)[2], eng->esz * (size_t)P.n, cudaMemcpyDeviceToDevice,
+                                      eng->stream));
+            }
+            eng->elec_1d = true;
+            eng->elec_on = true;
+            eng->elec_per_stage = !d.em_dynamic;
+            mark_estat(eng);
+            if (!d.in_Estat) GF_TRY(elec_1d_now(eng, par));
+            GF_CU(cudaStreamSynchronize(eng->stream));
+            invalidate_graphs(eng);
+            return GF_OK;
+        }
+        if (eng->mixed) { eng->err = "the spectral electrostatic solver runs in the FP64 form"; return GF_EUNSUPPORTED; }
         const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
         if (!eng->elec_q) {
             // wave vectors of global.cpp:276-316
@@ -2393,6 +2750,7 @@ void gf_destroy(gf_engine* e) {
     }
     if (e->plans) { cufftDestroy(e->plan_r2c); cufftDestroy(e->plan_c2r); }
     if (e->elec_plans) { cufftDestroy(e->elec_r2c); cufftDestroy(e->elec_c2r); }
+    if (e->es_plans) { cufftDestroy(e->es_r2c); cufftDestroy(e->es_c2r); }
     for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
     for (void* p : e->allocs) cudaFree(p);
     if (e->drive_host) cudaFreeHost(e->drive_host);

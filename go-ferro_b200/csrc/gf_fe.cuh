@@ -250,6 +250,15 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
                 eigen_crt(P, io, c, e0);
                 exx0 = e0[0]; eyy0 = e0[1]; ezz0 = e0[2]; eyz0 = e0[3]; exz0 = e0[4]; exy0 = e0[5];
             }
+            if (P.elastostatic) {
+                // plus the static strain and static eigenstrain
+                // (ferroelectric_solver.cpp:638-651; zeros when absent)
+                auto st = [&](const R* const* f, int q) { return f[q] ? f[q][c] : R(0.); };
+                exx = exx + st(io.eps0_c, 0); eyy = eyy + st(io.eps0_c, 1); ezz = ezz + st(io.eps0_c, 2);
+                eyz = eyz + st(io.eps0_c, 3); exz = exz + st(io.eps0_c, 4); exy = exy + st(io.eps0_c, 5);
+                exx0 = exx0 + st(io.eig0_c, 0); eyy0 = eyy0 + st(io.eig0_c, 1); ezz0 = ezz0 + st(io.eig0_c, 2);
+                eyz0 = eyz0 + st(io.eig0_c, 3); exz0 = exz0 + st(io.eig0_c, 4); exy0 = exy0 + st(io.eig0_c, 5);
+            }
         }
 
         const R px2 = px * px, py2 = py * py, pz2 = pz * pz;

@@ -207,6 +207,19 @@ class Deck:
     # reference permittivity, iteration limit, tolerance
     spin_pumping: bool = False
     flexo: bool = False          # if_flexo (flexoelectric coupling)
+    # electrostatics: 1-D model and its compensation (if_elec_1Dmodel,
+    # if_elec_1D_compensate)
+    elec_1D: bool = False
+    elec_1D_comp: bool = False
+    # static strain: if_elastostatic, the solver settings of read.cpp:64, and
+    # the restart inputs strain_stat.in (global frame) / eigenstraint0_crt.in
+    # (crystal frame), each (6, nx, ny, nz) in xx yy zz yz xz xy order
+    elastostatic: bool = False
+    scale_elasto: float = 1.0
+    elasto_limit: int = 0
+    elasto_tol: float = 1e-8
+    strain_t0: Optional[np.ndarray] = None
+    eig_t0: Optional[np.ndarray] = None
     scale_elec: float = 1.0
     elec_limit: int = 0
     elec_tol: float = 1e-8
@@ -298,7 +311,7 @@ class Deck:
              "false 0",
              f"{_b(self.magnetostatics)} {_b(self.mag_1D)}",
              f"{_b(self.demag_factor)} " + " ".join(_f(x) for x in self.demag_fac),
-             "false false",
+             f"{_b(self.elec_1D)} {_b(self.elec_1D_comp)}",
              f"{_b(self.em)} {_b(self.planeEM)}",
              " ".join(_f(x) for x in self.planeEM_E),
              " ".join(_f(x) for x in self.planeEM_freq),
@@ -309,10 +322,10 @@ class Deck:
              f"{_b(self.elastic)} {_b(self.elasto_back)} {_b(self.elasto_on)}",
              f"{_b(self.strain_pulse)} {int(self.strain_type)} {int(self.strain_z)}",
              f"{self.strain_comp} {_f(self.sigma_gauss)} {_f(self.amp_gauss)} {int(self.strain_cycles)}",
-             "false false",
+             f"{_b(self.elastostatic)} false",
              "false false",
              "0 0 0.0 0.0 0.0",
-             "1.0 0 1e-8",
+             f"{_f(self.scale_elasto)} {int(self.elasto_limit)} {_f(self.elasto_tol)}",
              f"{_b(self.abc_1D)} {_b(self.abc_elast_onlytop)} {_b(self.abc_em_onlytop)} {_f(self.liao_w)}",
              "false false",
              f"{_b(self.flexo)}",
@@ -320,7 +333,7 @@ class Deck:
              f"{_b(self.m0 is not None)} {_b(self.afm0 is not None)} false",
              f"{_b(self.p0 is not None)} false",
              "false false",
-             f"{_b(self.u0 is not None)} false false",
+             f"{_b(self.u0 is not None)} {_b(self.strain_t0 is not None)} {_b(self.eig_t0 is not None)}",
              "false",
              "true 1",
              "false 1 false 1",
@@ -375,6 +388,10 @@ def write_deck(deck: Deck, directory: str) -> str:
         _write_restart(os.path.join(directory, "u.in"), deck.u0)
         v = deck.v0 if deck.v0 is not None else np.zeros_like(deck.u0)
         _write_restart(os.path.join(directory, "v.in"), v)
+    if deck.strain_t0 is not None:
+        _write_restart(os.path.join(directory, "strain_stat.in"), deck.strain_t0)
+    if deck.eig_t0 is not None:
+        _write_restart(os.path.join(directory, "eigenstraint0_crt.in"), deck.eig_t0)
     if deck.Hext_table is not None:
         np.savetxt(os.path.join(directory, "Hext.in"), deck.Hext_table, fmt="%.17e")
     if deck.struct is not None:

@@ -65,7 +65,13 @@ enum gf_field {
     GF_FIELD_H_CELL = 16, /* cell-centred H (cell, 3), read-only DHx_em_cell */
     GF_FIELD_STRAIN = 17, /* dynamic cell strain, global frame (cell, 6:
                              xx yy zz yz xz xy), read-only   Dexx_glb..    */
-    GF_FIELD_COUNT = 18
+    GF_FIELD_STRAIN_STATIC = 18,      /* static strain, crystal frame (cell, 6)
+                                         exxt0_crt..; present with strain_stat.in
+                                         or gf_set_elastostatics */
+    GF_FIELD_EIGENSTRAIN_STATIC = 19, /* static eigenstrain, crystal frame (cell, 6)
+                                         exx0t0_crt..; present with
+                                         eigenstraint0_crt.in or gf_set_elastostatics */
+    GF_FIELD_COUNT = 20
 };
 
 /* observables for gf_average (global averages, FP64 sums) */
@@ -193,9 +199,12 @@ typedef struct gf_run_params {
     int32_t if_gaussian_strain_pulse, input_strain_type, input_strain_sourcez;
     char input_strain_component; char pad2_[7];
     double sigma_gauss, amplitude_gauss; uint64_t num_strain_cycles;
-    /* switches of physics the engine does not provide: must be 0 */
+    /* static strain coupling, flexoelectricity, spin pumping; the
+     * prescribed-m test mode is not provided (if_prescribed_m must be 0) */
     int32_t if_elastostatic, if_flexo, if_prescribed_m;
     int32_t if_spin_pumping;
+    /* elastostatic solve (read.cpp:64; gf_set_elastostatics) */
+    double scale_elasto; int32_t elasto_solver_limit; double elasto_solver_tol;
 } gf_run_params;
 
 /* Create an engine from the parsed values: `run`, `n_materials` materials and
@@ -268,7 +277,7 @@ int gf_average(gf_engine* e, int obs, double out3[3]);
 int gf_probe_em(gf_engine* e, int64_t i, int64_t j, int64_t k, double e3[3], double h3[3]);
 
 /* Number of doubles and dims of one array of a field (for vector fields the
- * dims of one component; count = 3 * dims product, 6 for GF_FIELD_STRAIN). */
+ * dims of one component; count = 3 * dims product, 6 for the strain fields). */
 int gf_field_dims(gf_engine* e, int field, int64_t dims3[3], size_t* count);
 
 /* Copy a field to / from host memory (count doubles, component-major).
@@ -306,16 +315,54 @@ int gf_profile_steps(gf_engine* e, uint64_t nsteps, gf_kernel_time* out, int max
  * elec_solver_limit iterations or elec_solver_tol (read.cpp:56).  Enabling
  * solves once now (unless Estat.in was read) and, without Maxwell fields,
  * after every RK stage with elec_solver_limit iterations.  FP64 engines;
- * *iterations_used (optional) gets the set-up iteration count. */
+ * *iterations_used (optional) gets the set-up iteration count.
+ * With if_elec_1Dmodel the 1-D model replaces the spectral solve
+ * (ferroelectric_system::get_E_static_1D, ferroelectric_system.h:106, also
+ * undefined in the public sources): the laterally uniform limit of the same
+ * periodic electrostatics, per (i, j) column E_z = -(P'_z - D) / (e0 er),
+ * D = sum(P'_z / er) / sum(1 / er) (zero mean E_z), E_x = E_y = 0, with
+ * P'_z = P_z - P_z(at enabling) under if_elec_1D_compensate; both
+ * precisions. */
 int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used);
+
+/* Elastostatic solve: the static strain exxt0_crt of the current static
+ * eigenstrain exx0t0_crt (magnetostriction and electrostriction of the
+ * current m and p, crystal frame).  Replaces elastic_system::get_strain_static
+ * / get_eigenstrain_static (elastic_system.h:184-199), which the reference
+ * declares and calls at set-up with elastodynamics and after every step
+ * without it (main.cpp:148-156, 213-215, 472-474) but does not define in its
+ * public sources; a build of those sources, like the oracle, keeps both at
+ * zero (or at strain_stat.in / eigenstraint0_crt.in), and so does the engine
+ * until this is enabled.  The solve restates the method the reference's
+ * data imply: Khachaturyan's iteration for an elastically inhomogeneous
+ * periodic body with the homogeneous cubic stiffness C_h = max(c11, c12,
+ * c44) x scale_elasto and its Green tensor (elastic_initialize.cpp:21-40,
+ * 340-389), up to elasto_solver_limit iterations or elasto_solver_tol
+ * (read.cpp:64), in the crystal frame, with zero mean strain (a clamped
+ * box; vacuum layers let a film relax along their normal).  The results act
+ * as the reference's static fields do: the LLG adds the static strain to the
+ * dynamic one, the dynamic eigenstrain of the elastic and ferroelectric
+ * solvers subtracts the static eigenstrain, and with if_elastostatic the
+ * ferroelectric field adds both (ferroelectric_solver.cpp:638-651).
+ * Enabling solves once now and, without elastodynamics, again after every
+ * step with elasto_solver_limit iterations started from the last solution.
+ * Decks with flexoelectricity are refused (their static-strain gradients,
+ * get_strain_static_glb_gradient, are not built).  Both precisions (the
+ * solve itself runs in FP64); *iterations_used (optional) gets the set-up
+ * iteration count. */
+int gf_set_elastostatics(gf_engine* e, int enable, int* iterations_used);
+
 /* Full-precision checkpoint of everything that carries from one step to the
  * next: the state fields (and, in the mixed form, their compensation words),
- * the static fields, the stage-1 force of the stiffness damping, the Liao
- * boundary history, the step counter and the external-field clock.  A run
+ * the static fields (with the static strain and eigenstrain and the
+ * elastostatic solver's iterate), the stage-1 force of the stiffness
+ * damping, the Liao boundary history, the step counter and the
+ * external-field clock.  A run
  * restarted from it continues bit for bit.  The reference restarts from
  * its %.7e text dumps (inoutput.cpp:330-887, input_* readers); this binary
  * form has no counterpart there.  Load needs an engine created from the same
- * deck and precision.  Load reads and checks the whole file before it
+ * deck and precision (and with the elastostatic solve enabled if it was on
+ * in the saved run).  Load reads and checks the whole file before it
  * writes any device buffer, so a file that fails (wrong deck, precision,
  * size or a short read) leaves the engine as it was. Synchronous. */
 int gf_save_state(gf_engine* e, const char* path);

@@ -67,3 +67,33 @@ def test_elastic_mur_boundary_rejects_single_layer(gf, tmp_path):
         gf.Engine(str(tmp_path), device=0)
     assert ei.value.code == -7
     assert "Mur boundary needs nz >= 2" in str(ei.value)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_restart_with_elastostatic_solve(gf, tmp_path, precision):
+    """Without elastodynamics the static strain is solved again after every
+    step from the last iterate; a restart carries the static fields and the
+    iterate, so the continued run equals the uninterrupted one bit for bit."""
+    D = gf.decks
+    d = D.Deck(nx=6, ny=6, nz=16, dx=1e-9, dy=1e-9, dz=1e-9, periodic=(True, True, True),
+               layers=[(5, 2), (8, 1), (3, 2)], steps=20, dt=2e-14, materials=[D.pto(), D.ggg()], name="es_ck")
+    d.elastostatic, d.elasto_limit, d.elasto_tol = True, 3, 1e-12
+    rng = np.random.default_rng(11)
+    d.p0 = rng.uniform(-0.2, 0.2, size=(3, 6, 6, 16)) * (d.material_cell() == 1)
+    d.q0 = np.zeros_like(d.p0)
+    ddir = str(tmp_path / "deck")
+    gf.decks.write_deck(d, ddir)
+    ck = str(tmp_path / "state.ck")
+    with gf.Engine(ddir, device=0, precision=precision) as a:
+        a.set_elastostatics(True)
+        a.advance(5)
+        a.save_state(ck)
+        a.advance(4)
+        ref = [a.download(f) for f in ("p", "q", "strain_static", "eigenstrain_static")]
+    with gf.Engine(ddir, device=0, precision=precision) as b:
+        b.set_elastostatics(True)
+        b.load_state(ck)
+        b.advance(4)
+        got = [b.download(f) for f in ("p", "q", "strain_static", "eigenstrain_static")]
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)
