@@ -478,10 +478,11 @@ def adjoint_cost(gf, torch, args, local_rank):
     """Cost of the discrete adjoint against a forward pass: FM LLG + FFT
     magnetostatics on 256x256x32 (the adjoint configuration's grid, YIG-like
     film, 1 T bias, per-cell damping 1e-3 with 10 % seeded noise, a 256-sample
-    x waveform), FP64.  Forward = the engine's graph-replayed step (CUDA
-    events); the adjoint's own forward run and its backward run (checkpoints
-    every 200 steps, block recomputation) are timed on the host around the
-    synchronous calls."""
+    x waveform), FP64.  Every time is device time on the engine's stream
+    (CUDA events around the enqueued work, host launch gaps included): the
+    engine's graph-replayed forward step, the adjoint's own forward run
+    (checkpoints every 200 steps, <m_x> trace) and its backward run (block
+    recomputation, stage recompute, reverse sweep)."""
     mu0 = 1.256637061e-6
     steps, K, nw = args.adjoint_steps, 200, 256
     with tempfile.TemporaryDirectory() as tmp:
@@ -508,9 +509,12 @@ def adjoint_cost(gf, torch, args, local_rank):
                 adj.set_alpha(alpha)
                 adj.set_waveform(wave)
                 adj.forward(4)
-                t0 = time.perf_counter()
+                eng.synchronize()
+                e0.record(stream)
                 tr = adj.forward(steps)
-                t_fwd = time.perf_counter() - t0
+                e1.record(stream)
+                e1.synchronize()
+                t_fwd = e0.elapsed_time(e1) / 1e3
                 # d loss / d <m_x>: spectral power of the trace in 0.1-0.5 THz
                 X = np.fft.rfft(tr)
                 f = np.fft.rfftfreq(tr.size, d.dt)
@@ -519,15 +523,20 @@ def adjoint_cost(gf, torch, args, local_rank):
                 g = np.zeros(tr.size)
                 for k in band:
                     g += 2.0 * np.real(np.conj(X[k]) * np.exp(-2j * np.pi * k * n / tr.size))
-                t0 = time.perf_counter()
+                eng.synchronize()
+                e0.record(stream)
                 adj.backward(g)
-                t_bwd = time.perf_counter() - t0
+                e1.record(stream)
+                e1.synchronize()
+                t_bwd = e0.elapsed_time(e1) / 1e3
     return {"workload": "FM LLG + FFT magnetostatics, 256x256x32, FP64, per-cell alpha and 256-sample waveform",
             "steps": steps, "checkpoint_every": K,
             "forward_ms_per_step": 1e3 * t_eng / steps,
             "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,
             "backward_ms_per_step": 1e3 * t_bwd / steps,
             "backward_over_forward": t_bwd / t_eng,
+            "forward_plus_backward_over_forward": (t_fwd + t_bwd) / t_eng,
+            "timing": "device time (CUDA events on the engine stream)",
             "loss_band_bins": int(len(band)),
             "definition": "backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
                           "forward = the engine's FP64 step (CUDA graph)"}
@@ -764,7 +773,7 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(gf, torch, args, local_rank)
     if world == 1 and not args.no_batch:
-        sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.sweep_steps, fp64_check=False)
+        sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.sweep_steps, fp64_check=True)
         sw["workload"] = ("batched sweep: 48 ferroelectric + FDTD instances, grids drawn from 32^3, 48x48x32, "
                           "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step")
         line["batched"] = sw

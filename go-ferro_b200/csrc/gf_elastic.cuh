@@ -25,6 +25,9 @@
 // same zero (non-periodic axis: both end faces are stress-free).
 #pragma once
 
+#include <cuda.h>
+
+#include "gf_launch.cuh"
 #include "gf_state.cuh"
 
 namespace gf {
@@ -211,18 +214,46 @@ constexpr int UR = TJ + 4, UC = TK + 4;      // staged u and ids: rows j0-2..j0+
 constexpr int HJ = TJ + 2, HK = TK + 2;      // cells with gradients: rows j0-1..j0+TJ, columns k0-1..k0+TK
 constexpr int GYR = TJ + 3, GZC = TK + 3;    // -y face gradients of rows j0-1..j0+TJ+1; -z of columns k0-1..k0+TK+1
 constexpr int FYR = TJ + 1, FZC = TK + 1;    // face stresses: y-faces j0..j0+TJ, z-faces k0..k0+TK
-constexpr int kU = 3 * UR * UC, kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
+constexpr int kGX = 3 * HJ * HK, kGY = 3 * GYR * HK, kGZ = 3 * HJ * GZC, kD0 = 6 * HJ * HK;
 constexpr int kFY = 3 * FYR * TK, kFZ = 3 * TJ * FZC;
-constexpr int kDoubles = 2 * kU + 2 * kGX + kGY + kGZ + kD0 + kFY + kFZ;
-// kDoubles counts reals of the kernel's type R (FP64 or FP32)
-template <class R>
-constexpr size_t kFixedBytes = (size_t)kDoubles * sizeof(R) + (size_t)(2 * UR + UC) * sizeof(int)
-                               + (size_t)(2 * UR * UC + HJ * HK);
+constexpr int kRest = 2 * kGX + kGY + kGZ + kD0 + kFY + kFZ;   // reals after the staged planes
+// A staged plane is one TMA box per array: rows j0-2..j0+TJ+1 and a column
+// range whose first element sits on a 16-byte boundary (k0 is a multiple of
+// 32): from k0-2 for FP64 u (36 columns, 288 B), from k0-4 for FP32 u (40
+// columns, 160 B), from k0-16 for the one-byte material ids (64 columns).
+// UP/IP = row pitch, UO/IO = column of k0-2 in a row.
+template <class R> constexpr int UP = is_mixed<R>::value ? TK + 8 : TK + 4;
+template <class R> constexpr int UO = is_mixed<R>::value ? 2 : 0;
+constexpr int IP = 64, IO = 14;
+template <class R> constexpr int kUP = UR * UP<R>;             // one component of one staged plane
+template <class R> constexpr int kU = 3 * kUP<R>;
+constexpr int kIDS = UR * IP;                                    // bytes of one staged id plane
+// byte offsets in the dynamic shared memory (TMA destinations 128-byte aligned)
+template <class R> constexpr size_t OFF_ID = (size_t)2 * kU<R> * sizeof(R);
+template <class R> constexpr size_t OFF_R = OFF_ID<R> + 2 * (size_t)kIDS;
+template <class R> constexpr size_t OFF_I = OFF_R<R> + (size_t)kRest * sizeof(R);
+template <class R> constexpr size_t OFF_IDC = OFF_I<R> + (size_t)(2 * UR + UC) * sizeof(int);
+template <class R> constexpr size_t OFF_BAR = (OFF_IDC<R> + HJ * HK + 7) / 8 * 8;
+template <class R> constexpr size_t kFixedBytes = OFF_BAR<R> + 2 * sizeof(unsigned long long);
 template <class R>
 constexpr size_t kMatOffset = (kFixedBytes<R> + 15) / 16 * 16;
 template <class R>
 inline size_t smem_bytes(int nmat) { return kMatOffset<R> + (size_t)nmat * sizeof(ElMat<R>); }
+static_assert(OFF_ID<double> % 128 == 0 && OFF_ID<float> % 128 == 0, "id planes 128-byte aligned");
+static_assert((kUP<double> * sizeof(double)) % 128 == 0 && (kUP<float> * sizeof(float)) % 128 == 0, "u planes 128-byte aligned");
+static_assert(kIDS % 128 == 0, "id planes 128-byte aligned");
 }  // namespace etile
+
+// Tensor maps of the TMA staging of k_elastic_tile (one 3-D map per u
+// component of the stage input and one of the material ids, box = one
+// staged plane), the flag a timed-out wait sets, and whether they are usable
+// for this run (otherwise every block stages with cp.async).
+struct ETileMaps {
+    CUtensorMap u[3];
+    CUtensorMap id;
+    unsigned* err;
+    int on;
+};
 
 // index x in [-n, 2n) wrapped into [0, n)
 __device__ inline int wrapm(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
@@ -344,59 +375,86 @@ __device__ inline void side_rows(const V& v, const M& m, R ga, R gb, R gc, R out
 }
 
 // Shared-memory plan of k_elastic_tile: every array sits at a compile-time
-// offset from the dynamic base; the material table (sized at launch) is last.
+// offset from the dynamic base (etile::OFF_*); the material table (sized at
+// launch) is last.
 template <class R>
 struct ETileSmem {
     unsigned char* base;
-    __device__ R* dp() const { return reinterpret_cast<R*>(base); }
-    __device__ R* u(int slot) const { return dp() + slot * etile::kU; }
-    __device__ R* gx(int slot) const { return dp() + 2 * etile::kU + slot * etile::kGX; }
-    __device__ R* gy() const { return dp() + 2 * etile::kU + 2 * etile::kGX; }
+    __device__ R* u(int slot) const { return reinterpret_cast<R*>(base) + slot * etile::kU<R>; }
+    __device__ uint8_t* id(int slot) const { return base + etile::OFF_ID<R> + slot * etile::kIDS; }
+    __device__ R* rp() const { return reinterpret_cast<R*>(base + etile::OFF_R<R>); }
+    __device__ R* gx(int slot) const { return rp() + slot * etile::kGX; }
+    __device__ R* gy() const { return rp() + 2 * etile::kGX; }
     __device__ R* gz() const { return gy() + etile::kGY; }
     __device__ R* d0() const { return gz() + etile::kGZ; }
     __device__ R* fy() const { return d0() + etile::kD0; }
     __device__ R* fz() const { return fy() + etile::kFY; }
-    __device__ int* ip() const { return reinterpret_cast<int*>(dp() + etile::kDoubles); }
+    __device__ int* ip() const { return reinterpret_cast<int*>(base + etile::OFF_I<R>); }
     __device__ int* rowoff() const { return ip(); }
     __device__ int* rowj() const { return ip() + etile::UR; }
     __device__ int* colk() const { return ip() + 2 * etile::UR; }
-    __device__ uint8_t* bp() const { return reinterpret_cast<uint8_t*>(ip() + 2 * etile::UR + etile::UC); }
-    __device__ uint8_t* id(int slot) const { return bp() + slot * etile::UR * etile::UC; }
-    __device__ uint8_t* idc() const { return bp() + 2 * etile::UR * etile::UC; }
+    __device__ uint8_t* idc() const { return base + etile::OFF_IDC<R>; }
+    __device__ unsigned long long* bar(int slot) const {
+        return reinterpret_cast<unsigned long long*>(base + etile::OFF_BAR<R>) + slot;
+    }
     __device__ ElMat<R>* mat() const { return reinterpret_cast<ElMat<R>*>(base + etile::kMatOffset<R>); }
 };
 
-// Staging of plane pw into ring slot `slot`: the u copies go out as cp.async
-// (no register or stall while they fly), the ids are loaded into registers
-// and stored by etile_stage_finish, which also waits for the copies.
+// Staging of plane pw into ring slot `slot`.  TMA blocks: one thread arms
+// the slot's mbarrier with the byte count and issues one tensor copy per u
+// component and one for the ids (no wrap-around needed: the block's halo lies
+// inside the grid in every periodic direction).  Other blocks: the u copies
+// go out as cp.async (no register or stall while they fly), the ids are
+// loaded into registers and stored by etile_stage_finish, which also waits
+// for the copies.  Both write the same layout.
 constexpr int kStageItems = (etile::UR * etile::UC + etile::NT - 1) / etile::NT;
 template <class R>
 __device__ inline void etile_stage_issue(const Params& P, const StageIOT<R>& io, const ETileSmem<R>& sm, int slot, int pw,
-                                         uint8_t idp[kStageItems]) {
+                                         uint8_t idp[kStageItems], bool tma, const ETileMaps& tm, int j0, int k0) {
     using namespace etile;
+    if (tma) {
+        if (threadIdx.x == 0) {
+            unsigned long long* b = sm.bar(slot);
+            mbar_arrive_expect_tx(b, (unsigned)(3 * kUP<R> * sizeof(R) + kIDS));
+#pragma unroll
+            for (int a = 0; a < 3; a++) tma_load_3d(sm.u(slot) + a * kUP<R>, &tm.u[a], k0 - 2 - UO<R>, j0 - 2, pw, b);
+            tma_load_3d(sm.id(slot), &tm.id, k0 - 2 - IO, j0 - 2, pw, b);
+        }
+        return;
+    }
     const int po = pw * P.ny * P.nz;
     R* su = sm.u(slot);
 #pragma unroll
     for (int t = 0; t < kStageItems; t++) {
         const int it = threadIdx.x + t * NT;
         if (it < UR * UC) {
-            const int ur = it / UC, uc = it - (it / UC) * UC;
-            const int c = po + sm.rowoff()[ur] + sm.colk()[uc];
+            const int ur = it / UC, ucol = it - (it / UC) * UC;
+            const int c = po + sm.rowoff()[ur] + sm.colk()[ucol];
             idp[t] = io.mid[c];
 #pragma unroll
-            for (int a = 0; a < 3; a++) cp_async_elem(&su[a * UR * UC + it], &io.u_in.c[a][c]);
+            for (int a = 0; a < 3; a++) cp_async_elem(&su[a * kUP<R> + ur * UP<R> + ucol + UO<R>], &io.u_in.c[a][c]);
         }
     }
     cp_async_commit();
 }
 template <class R>
-__device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, const uint8_t idp[kStageItems]) {
+__device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, const uint8_t idp[kStageItems], bool tma,
+                                          unsigned phase, const ETileMaps& tm) {
     using namespace etile;
+    if (tma) {
+        // bounded wait: a copy that never lands sets the run's error flag
+        // (reported by gf_check_finite) instead of hanging the block
+        if (!mbar_wait_bounded(sm.bar(slot), phase, 1u << 24) && tm.err) atomicOr(tm.err, 1u);
+        return;
+    }
     uint8_t* sid = sm.id(slot);
 #pragma unroll
     for (int t = 0; t < kStageItems; t++) {
         const int it = threadIdx.x + t * NT;
-        if (it < UR * UC) sid[it] = idp[t];
+        if (it < UR * UC) {
+            const int ur = it / UC, ucol = it - (it / UC) * UC;
+            sid[ur * IP + ucol + IO] = idp[t];
+        }
     }
     cp_async_wait_all();
 }
@@ -407,7 +465,8 @@ __device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, cons
 #define GF_ETILE_MINB_F32 4
 #endif
 template <int S, bool CUB, class R = double>
-__global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_F32 : 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat) {
+__global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_F32 : 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat,
+                                                                                        const __grid_constant__ ETileMaps tm) {
     using namespace etile;
     GF_EXTERN_SMEM(unsigned char, smem_raw);
     const ETileSmem<R> sm{smem_raw};
@@ -426,8 +485,19 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
     const bool quirk = valid && (k == P.ny - 1) && (P.ny < P.nz);
     const bool traction_here = P.strain_pulse && P.strain_type == 3 && k == (int)P.source_z;
     const int nyz = P.ny * P.nz;
+    // TMA staging when the staged box needs no wrap-around: its rows and
+    // columns lie inside the grid in the periodic directions (in the others
+    // the values outside are never used: those faces are stress-free)
+    const bool tma = tm.on && !(P.per_y && (j0 - 2 < 0 || j0 + TJ + 1 > P.ny - 1))
+                     && !(P.per_z && (k0 - 2 < 0 || k0 + TK + 1 > P.nz - 1));
+    unsigned phase[2] = {0u, 0u};
 
-    // ---- block set-up: material table, wrapped row/column offsets, first two planes ----
+    // ---- block set-up: material table, wrapped row/column offsets, barriers, first two planes ----
+    if (tid == 0) {
+        mbar_init(sm.bar(0), 1);
+        mbar_init(sm.bar(1), 1);
+        mbar_fence_init();
+    }
     for (int it = tid; it < nmat; it += blockDim.x) {
         const DevMatT<R>& d = io.mats[it];
         ElMat<R>& e = sm.mat()[it];
@@ -450,10 +520,11 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
     __syncthreads();
     {
         uint8_t id0[kStageItems], id1[kStageItems];
-        etile_stage_issue(P, io, sm, 0, wrapm(i0 - 1, P.nx), id0);
-        etile_stage_issue(P, io, sm, 1, wrapm(i0, P.nx), id1);
-        etile_stage_finish(sm, 0, id0);
-        etile_stage_finish(sm, 1, id1);
+        etile_stage_issue(P, io, sm, 0, wrapm(i0 - 1, P.nx), id0, tma, tm, j0, k0);
+        etile_stage_issue(P, io, sm, 1, wrapm(i0, P.nx), id1, tma, tm, j0, k0);
+        etile_stage_finish(sm, 0, id0, tma, phase[0], tm);
+        etile_stage_finish(sm, 1, id1, tma, phase[1], tm);
+        phase[0] ^= 1u; phase[1] ^= 1u;
     }
     __syncthreads();
     uint8_t idp[kStageItems];          // ids of the plane being staged
@@ -480,32 +551,34 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
             const bool fb = (f == 0 || f == P.nx) && !P.per_x;
             for (int it = tid; it < HJ * HK; it += blockDim.x) {
                 const int rr = it / HK, ss = it - (it / HK) * HK;
-                const int ui = (rr + 1) * UC + ss + 1;
-                const bool fr = fb || !(ic[ui] != 0 && in[ui] != 0);
+                const int uu = (rr + 1) * UP<R> + ss + 1 + UO<R>, ii = (rr + 1) * IP + ss + 1 + IO;
+                const bool fr = fb || !(ic[ii] != 0 && in[ii] != 0);
 #pragma unroll
                 for (int a = 0; a < 3; a++)
-                    gxn[a * HJ * HK + it] = fr ? R(0.) : qdivR((un[a * UR * UC + ui] - uc[a * UR * UC + ui]), P.dx, P.rdx, P.f.rdx);
+                    gxn[a * HJ * HK + it] = fr ? R(0.) : qdivR((un[a * kUP<R> + uu] - uc[a * kUP<R> + uu]), P.dx, P.rdx, P.f.rdx);
             }
         }
         for (int it = tid; it < GYR * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
-            const int u1 = (rr + 1) * UC + ss + 1, u0 = rr * UC + ss + 1;
-            const bool fr = (sm.rowj()[rr + 1] == 0 && !P.per_y) || !(ic[u0] != 0 && ic[u1] != 0);
+            const int u1 = (rr + 1) * UP<R> + ss + 1 + UO<R>, u0 = u1 - UP<R>;
+            const int i1 = (rr + 1) * IP + ss + 1 + IO, i0_ = i1 - IP;
+            const bool fr = (sm.rowj()[rr + 1] == 0 && !P.per_y) || !(ic[i0_] != 0 && ic[i1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gy()[a * GYR * HK + it] = fr ? R(0.) : qdivR((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dy, P.rdy, P.f.rdy);
+                sm.gy()[a * GYR * HK + it] = fr ? R(0.) : qdivR((uc[a * kUP<R> + u1] - uc[a * kUP<R> + u0]), P.dy, P.rdy, P.f.rdy);
         }
         for (int it = tid; it < HJ * GZC; it += blockDim.x) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
-            const int u1 = (rr + 1) * UC + ss + 1, u0 = u1 - 1;
-            const bool fr = (sm.colk()[ss + 1] == 0 && !P.per_z) || !(ic[u0] != 0 && ic[u1] != 0);
+            const int u1 = (rr + 1) * UP<R> + ss + 1 + UO<R>, u0 = u1 - 1;
+            const int i1 = (rr + 1) * IP + ss + 1 + IO, i0_ = i1 - 1;
+            const bool fr = (sm.colk()[ss + 1] == 0 && !P.per_z) || !(ic[i0_] != 0 && ic[i1] != 0);
 #pragma unroll
             for (int a = 0; a < 3; a++)
-                sm.gz()[a * HJ * GZC + it] = fr ? R(0.) : qdivR((uc[a * UR * UC + u1] - uc[a * UR * UC + u0]), P.dz, P.rdz, P.f.rdz);
+                sm.gz()[a * HJ * GZC + it] = fr ? R(0.) : qdivR((uc[a * kUP<R> + u1] - uc[a * kUP<R> + u0]), P.dz, P.rdz, P.f.rdz);
         }
         for (int it = tid; it < HJ * HK; it += blockDim.x) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
-            const uint8_t id = ic[(rr + 1) * UC + ss + 1];
+            const uint8_t id = ic[(rr + 1) * IP + ss + 1 + IO];
             sm.idc()[it] = id;
             R e[6] = {R(0.), R(0.), R(0.), R(0.), R(0.), R(0.)};
             if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff()[rr + 1] + sm.colk()[ss + 1], sm.mat()[id - 1], e);
@@ -516,7 +589,7 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
 
         // ---- B1: y- and z-face stresses of the interior plane p; stage plane p+2 ----
         const bool stage_next = q + 1 <= L;
-        if (stage_next) etile_stage_issue(P, io, sm, cur, wrapm(p + 2, P.nx), idp);
+        if (stage_next) etile_stage_issue(P, io, sm, cur, wrapm(p + 2, P.nx), idp, tma, tm, j0, k0);
         if (q >= 1 && q <= L) {
             for (int it = tid; it < FYR * TK + TJ * FZC; it += blockDim.x) {
               if (it < FYR * TK) {
@@ -662,7 +735,10 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
             }
             mid_prev = id;
         }
-        if (stage_next) etile_stage_finish(sm, cur, idp);
+        if (stage_next) {
+            etile_stage_finish(sm, cur, idp, tma, phase[cur], tm);
+            phase[cur] ^= 1u;
+        }
         __syncthreads();
     }
 }

@@ -16,10 +16,12 @@
 // values, and build_io hands the kernels float* views of them.
 #include <cuda_runtime.h>
 #include <cufft.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -69,6 +71,10 @@ struct gf_engine {
     bool mixed = false;                    // GF_PRECISION_MIXED_FP32
     size_t esz = sizeof(double);           // bytes per element of the real-valued device buffers
     cudaStream_t stream = nullptr;
+    // branch streams of a stage (LLG, TDGL, Maxwell) and their fork / join
+    // events; the elastic chain and the static solves stay on `stream`
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t bev[6] = {};
     std::string err;
 
     // bookkeeping
@@ -109,6 +115,8 @@ struct gf_engine {
     double* strain_c[6] = {};
     double* flexo_sg[6] = {};          // flexoelectric scratch (StageIOT::sg, pge)
     double* flexo_pge[6] = {};
+    ETileMaps etm[2][4] = {};          // TMA maps of k_elastic_tile per step parity and stage
+    unsigned* tma_err = nullptr;       // set by a timed-out TMA wait
     int el_chunk = 1;                  // x-planes per block of k_elastic_tile
     int el_nmat = 0;                   // materials staged by k_elastic_tile
     size_t el_smem = 0;                // its dynamic shared memory
@@ -948,51 +956,120 @@ int elec_solve(gf_engine* eng, F3 p, bool counted, int iters, double tol, int* u
     return GF_OK;
 }
 
+// TDGL kernel of stage S on stream st
+template <int S, class R>
+int enqueue_fe(gf_engine* eng, const StageIOT<R>& io, cudaStream_t st) {
+    const Params& P = eng->P;
+    const dim3 g(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx);
+    if (P.flexo) GF_CU(klaunch(eng, "k_fe", k_fe<S, R, true>, g, dim3(kThreads), 0, st, P, io));
+    else GF_CU(klaunch(eng, "k_fe", k_fe<S, R, false>, g, dim3(kThreads), 0, st, P, io));
+    return GF_OK;
+}
+
+// Maxwell kernels of stage S on stream st: the Yee update, then the plane
+// source, the Mur boundaries, PEC and the Drude currents, in that order
+template <int S, class R>
+int enqueue_em(gf_engine* eng, const StageIOT<R>& io, cudaStream_t st) {
+    const Params& P = eng->P;
+    const long nx = P.nx, ny = P.ny, nz = P.nz;
+    GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                  dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size(),
+                  static_cast<const EmCls<R>*>(eng->em_cls_tab), eng->em_ncls));
+    if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S, R>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+    if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0, R>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+    if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1, R>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
+    if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2, R>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
+    if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
+                             dim3(kThreads), 0, st, P, io));
+    if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, st, P, io));
+    return GF_OK;
+}
+
 template <int S, class R>
 int enqueue_stage(gf_engine* eng, int parity) {
     const Params& P = eng->P;
     const StageIOT<R>& io = stage_io<R>(eng, parity, S);
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
+    // The physics of a stage read only the stage inputs, except for these
+    // dependencies: the LLG and (FP64) TDGL kernels read the cell strain the
+    // elastic tile writes, flexoelectric runs read k_flexo_prep's arrays, the
+    // Maxwell update reads the LLG increment (M-sourced current, spin
+    // pumping), and the PEC kernel clears the step-start E that the TDGL
+    // kernel reads at stage 1.  So the elastic chain runs on the engine
+    // stream and the LLG, TDGL and Maxwell kernels on three branch streams
+    // forked from it and joined before the static solves; the tiny boundary
+    // kernels and the tails of the big ones then overlap other physics.
+    // (per-kernel timing, gf_profile_steps, keeps one stream: each kernel is
+    // then timed alone; so does a run with a single physics group, where a
+    // fork would only add graph edges)
+    const int groups = (P.elastic ? 1 : 0) + ((P.fm || P.afm) ? 1 : 0) + (P.fe ? 1 : 0) + (P.em ? 1 : 0);
+    const bool par = !eng->profiling && groups >= 2;
+    auto rec = [&](cudaEvent_t e, cudaStream_t s_) { return par ? cudaEventRecord(e, s_) : cudaSuccess; };
+    auto wait_ = [&](cudaStream_t s_, cudaEvent_t e, unsigned) { return par ? cudaStreamWaitEvent(s_, e, 0) : cudaSuccess; };
+    cudaStream_t s_llg = par ? eng->side[0] : st, s_fe = par ? eng->side[1] : st, s_em = par ? eng->side[2] : st;
+    cudaEvent_t ev_start = eng->bev[0], ev_pre = eng->bev[1], ev_tile = eng->bev[2];
+    cudaEvent_t ev_llg = eng->bev[3], ev_fe = eng->bev[4], ev_em = eng->bev[5];
+    const bool mag = P.fm || P.afm;
+    const bool em_after_llg = P.em && mag && (P.em_fromM || P.spin);
+    const bool em_after_fe = P.em && P.fe && P.pec;
+    const bool fe_after_tile = P.fe && P.elastic && P.elasto_on && !is_mixed<R>::value;
+    GF_CU(rec(ev_start, st));
+    if (P.em && !em_after_llg && !em_after_fe) {
+        GF_CU(wait_(s_em, ev_start, 0));
+        GF_TRY((enqueue_em<S, R>(eng, io, s_em)));
+        GF_CU(rec(ev_em, s_em));
+    }
     if (P.flexo)
         GF_CU(klaunch(eng, "k_flexo_prep", k_flexo_prep<R>, dim3(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx),
                       dim3(kThreads), 0, st, P, io));
+    GF_CU(rec(ev_pre, st));
+    if (P.fe && !fe_after_tile) {
+        GF_CU(wait_(s_fe, ev_pre, 0));
+        GF_TRY((enqueue_fe<S, R>(eng, io, s_fe)));
+        GF_CU(rec(ev_fe, s_fe));
+    }
     if (P.elastic) {
         const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
                         (P.nx + eng->el_chunk - 1) / eng->el_chunk);
+        const ETileMaps& tm = eng->etm[parity][S];
         if (eng->el_cubic)
             GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, true, R>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
-                                eng->el_chunk, eng->el_nmat));
+                                eng->el_chunk, eng->el_nmat, tm));
         else
             GF_CU(klaunch<true>(eng, "k_elastic", k_elastic_tile<S, false, R>, grid, dim3(etile::NT), eng->el_smem, st, P, io,
-                                eng->el_chunk, eng->el_nmat));
+                                eng->el_chunk, eng->el_nmat, tm));
+    }
+    GF_CU(rec(ev_tile, st));
+    if (P.fe && fe_after_tile) {
+        GF_CU(wait_(s_fe, ev_tile, 0));
+        GF_TRY((enqueue_fe<S, R>(eng, io, s_fe)));
+        GF_CU(rec(ev_fe, s_fe));
+    }
+    if (mag) {
+        GF_CU(wait_(s_llg, ev_tile, 0));
+        if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S, R>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
+                                      dim3(kThreads), 0, s_llg, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
+        if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S, R>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
+                                       dim3(kThreads), 0, s_llg, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
+        GF_CU(rec(ev_llg, s_llg));
+    }
+    if (P.em && (em_after_llg || em_after_fe)) {
+        if (em_after_llg) GF_CU(wait_(s_em, ev_llg, 0));
+        if (em_after_fe) GF_CU(wait_(s_em, ev_fe, 0));
+        GF_TRY((enqueue_em<S, R>(eng, io, s_em)));
+        GF_CU(rec(ev_em, s_em));
+    }
+    if (P.elastic) {
         // the mixed form's RK kernel updates two cells per thread
         const unsigned brk = is_mixed<R>::value ? blocks_for(P.n, 2 * kThreads) : bn;
         GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S, R>, dim3(brk), dim3(kThreads), 0, st, P, io));
         GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
-    if (P.fm) GF_CU(klaunch<true>(eng, "k_llg_fm", k_llg_fm<S, R>, dim3(blocks_for(P.fm_bj * P.fm_bk, kThreads), (unsigned)P.fm_bi),
-                                  dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
-    if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S, R>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
-                                   dim3(kThreads), 0, st, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
-    if (P.fe) {
-        const dim3 g(blocks_for((long)P.ny * P.nz, kThreads), (unsigned)P.nx);
-        if (P.flexo) GF_CU(klaunch(eng, "k_fe", k_fe<S, R, true>, g, dim3(kThreads), 0, st, P, io));
-        else GF_CU(klaunch(eng, "k_fe", k_fe<S, R, false>, g, dim3(kThreads), 0, st, P, io));
-    }
-    if (P.em) {
-        const long nx = P.nx, ny = P.ny, nz = P.nz;
-        GF_CU(klaunch<true>(eng, "k_em_fused", k_em_fused<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
-                      dim3(kThreads), 0, st, P, io, (int)eng->deck.mats.size(),
-                      static_cast<const EmCls<R>*>(eng->em_cls_tab), eng->em_ncls));
-        if (P.planeEM) GF_CU(klaunch(eng, "k_em_plane", k_em_plane<S, R>, dim3(blocks_for(nx * ny, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_x) GF_CU(klaunch(eng, "k_em_mur_x", k_em_mur<S, 0, R>, dim3(blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_y) GF_CU(klaunch(eng, "k_em_mur_y", k_em_mur<S, 1, R>, dim3(blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (!P.per_z) GF_CU(klaunch(eng, "k_em_mur_z", k_em_mur<S, 2, R>, dim3(blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads)), dim3(kThreads), 0, st, P, io));
-        if (P.pec) GF_CU(klaunch(eng, "k_em_pec", k_em_pec<S, R>, dim3(blocks_for((ny + 1) * (nz + 1), kThreads), (unsigned)(nx + 1)),
-                                 dim3(kThreads), 0, st, P, io));
-        if (P.drude) GF_CU(klaunch(eng, "k_drude", k_drude<S, R>, dim3(bn), dim3(kThreads), 0, st, P, io));
-    }
+    // join the branches
+    if (mag) GF_CU(wait_(st, ev_llg, 0));
+    if (P.fe) GF_CU(wait_(st, ev_fe, 0));
+    if (P.em) GF_CU(wait_(st, ev_em, 0));
     if (eng->demag_per_stage) {
         // static field of the new stage state (main.cpp:299-306, 476-483)
         if constexpr (is_mixed<R>::value) GF_TRY(demag_solve_f32(eng, io.m_out, io.a1_out, io.a2_out, true, io.msrc != nullptr));
@@ -1023,11 +1100,12 @@ int time_tile_t(gf_engine* eng, int reps, float* ms) {
     cudaEvent_t a, b;
     GF_CU(cudaEventCreate(&a));
     GF_CU(cudaEventCreate(&b));
+    const ETileMaps& tm = eng->etm[(int)(eng->steps_done & 1ull)][0];
     auto one = [&]() {
         return eng->el_cubic ? launch_tiled(k_elastic_tile<0, true, R>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
-                                            eng->el_chunk, eng->el_nmat)
+                                            eng->el_chunk, eng->el_nmat, tm)
                              : launch_tiled(k_elastic_tile<0, false, R>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
-                                            eng->el_chunk, eng->el_nmat);
+                                            eng->el_chunk, eng->el_nmat, tm);
     };
     cudaError_t e = one();                     // warm
     if (e == cudaSuccess) e = cudaEventRecord(a, eng->stream);
@@ -1523,6 +1601,57 @@ int setup_em_classes(gf_engine* eng) {
 
 // Set-up from eng->deck (filled from a deck directory or from the host's
 // parsed values); `dir` is where restart files are read from ("" = none).
+// TMA tensor maps of k_elastic_tile: per step parity and stage, one 3-D map
+// (x = k, y = j, z = i) per component of the stage's input displacement and
+// one of the material ids, each with the box of one staged plane.  Used only
+// when every row stride is a multiple of 16 bytes (nz even in FP64, a
+// multiple of 4 in FP32, of 16 for the one-byte ids) and the driver exports
+// the encoder; otherwise every block stages with cp.async.
+int etile_maps(gf_engine* eng) {
+    const Params& P = eng->P;
+    if (!eng->tma_err) GF_TRY(dalloc_n(eng, &eng->tma_err, 1));
+    for (auto& row : eng->etm)
+        for (ETileMaps& m : row) { std::memset(&m, 0, sizeof(m)); m.err = eng->tma_err; m.on = 0; }
+    if (!P.elastic) return GF_OK;
+    // GOFERRO_TILE_TMA=0 keeps every block on the cp.async staging (the
+    // tests check that both stagings give the same bits)
+    if (const char* v = std::getenv("GOFERRO_TILE_TMA"))
+        if (v[0] == '0') return GF_OK;
+    const size_t esz = eng->esz;
+    if (P.nz % 16 != 0 || ((size_t)P.nz * esz) % 16 != 0) return GF_OK;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return GF_OK;
+    }
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    const cuuint64_t dims[3] = {(cuuint64_t)P.nz, (cuuint64_t)P.ny, (cuuint64_t)P.nx};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    auto make = [&](CUtensorMap* m, void* base, CUtensorMapDataType t, size_t bytes, cuuint32_t box0) -> bool {
+        const cuuint64_t str[2] = {(cuuint64_t)P.nz * bytes, (cuuint64_t)P.ny * P.nz * bytes};
+        const cuuint32_t box[3] = {box0, (cuuint32_t)etile::UR, 1};
+        return encode(m, t, 3, base, dims, str, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    for (int par = 0; par < 2; par++)
+        for (int s = 0; s < 4; s++) {
+            ETileMaps& m = eng->etm[par][s];
+            bool ok = make(&m.id, eng->mid, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, (cuuint32_t)etile::IP);
+            for (int a = 0; a < 3 && ok; a++) {
+                if (eng->mixed)
+                    ok = make(&m.u[a], (void*)eng->iof[par][s].u_in.c[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                              (cuuint32_t)etile::UP<float>);
+                else
+                    ok = make(&m.u[a], (void*)eng->io[par][s].u_in.c[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8,
+                              (cuuint32_t)etile::UP<double>);
+            }
+            m.on = ok ? 1 : 0;
+        }
+    return GF_OK;
+}
+
 int create_from(gf_engine* eng, const std::string& dir, int device, int precision) {
     if (precision != GF_PRECISION_FP64 && precision != GF_PRECISION_MIXED_FP32) {
         eng->err = "precision must be GF_PRECISION_FP64 or GF_PRECISION_MIXED_FP32";
@@ -1543,6 +1672,8 @@ int create_from(gf_engine* eng, const std::string& dir, int device, int precisio
     GF_CU(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) { eng->err = std::string("device ") + prop.name + " is not sm_100 or newer"; return GF_ENODEV; }
     GF_CU(cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking));
+    for (cudaStream_t& b : eng->side) GF_CU(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    for (cudaEvent_t& ev : eng->bev) GF_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
 
     build_params(eng);
     const Params& P = eng->P;
@@ -1707,6 +1838,7 @@ int create_from(gf_engine* eng, const std::string& dir, int device, int precisio
     GF_TRY(replicate_state(eng));
     build_io(eng);
     if (eng->mixed) build_io_mixed(eng);
+    GF_TRY(etile_maps(eng));
 
     // initial static field (main.cpp:135-146 and 229-239)
     if (!d.in_Hstat) GF_TRY(static_field_now(eng));
@@ -2717,6 +2849,12 @@ int gf_check_finite(gf_engine* e) {
     gf_engine* eng = e;
     GF_CU(cudaSetDevice(eng->device));
     struct Named { const char* name; Field3* f; };
+    if (eng->tma_err) {
+        unsigned h = 0;
+        GF_CU(cudaMemcpyAsync(&h, eng->tma_err, sizeof(unsigned), cudaMemcpyDeviceToHost, eng->stream));
+        GF_CU(cudaStreamSynchronize(eng->stream));
+        if (h) { eng->err = "a TMA staging wait of the elastic tile timed out"; return GF_ECUDA; }
+    }
     Named fs[] = {{"m", &eng->m}, {"m_afm1", &eng->a1}, {"m_afm2", &eng->a2}, {"p", &eng->p}, {"q", &eng->q}, {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H}};
     for (auto& nf : fs) {
         if (!nf.f->on) continue;
@@ -2754,6 +2892,8 @@ void gf_destroy(gf_engine* e) {
     for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
     for (void* p : e->allocs) cudaFree(p);
     if (e->drive_host) cudaFreeHost(e->drive_host);
+    for (cudaStream_t b : e->side) if (b) cudaStreamDestroy(b);
+    for (cudaEvent_t ev : e->bev) if (ev) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }

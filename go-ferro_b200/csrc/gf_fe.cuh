@@ -261,50 +261,85 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
             }
         }
 
-        const R px2 = px * px, py2 = py * py, pz2 = pz * pz;
-        const R px3 = px2 * px, py3 = py2 * py, pz3 = pz2 * pz;
-        const R px4 = px2 * px2, py4 = py2 * py2, pz4 = pz2 * pz2;
-        const R px5 = px4 * px, py5 = py4 * py, pz5 = pz4 * pz;
-        const R px6 = px4 * px2, py6 = py4 * py2, pz6 = pz4 * pz2;
-        const R px7 = px6 * px, py7 = py6 * py, pz7 = pz6 * pz;
         const R fm = mt.fe_coef;
-
-        const R qxc = fm * (R(2.) * mt.a1 * px + R(4.) * mt.a11 * px3
-            + R(2.) * mt.a12 * (py2 + pz2) * px
-            + R(6.) * mt.a111 * px5
-            + R(4.) * mt.a112 * px3 * (py2 + pz2)
-            + R(2.) * mt.a112 * (py4 + pz4) * px
-            + R(2.) * mt.a123 * px * py2 * pz2
-            + R(8.) * mt.a1111 * px7
-            + R(2.) * mt.a1112 * px * (py6 + pz6 + R(3.) * px4 * (py2 + pz2))
-            + R(4.) * mt.a1122 * px3 * (py4 + pz4)
-            + R(2.) * mt.a1123 * px * py2 * pz2 * (R(2.) * px2 + py2 + pz2)
-            + (mt.tv1 * (exx0 - exx) + mt.tv2 * (eyy0 - eyy + ezz0 - ezz)) * px
-            + mt.tv3 * ((exy0 - exy) * py + (exz0 - exz) * pz));
-        const R qyc = fm * (R(2.) * mt.a1 * py + R(4.) * mt.a11 * py3
-            + R(2.) * mt.a12 * (pz2 + px2) * py
-            + R(6.) * mt.a111 * py5
-            + R(4.) * mt.a112 * py3 * (px2 + pz2)
-            + R(2.) * mt.a112 * (px4 + pz4) * py
-            + R(2.) * mt.a123 * py * px2 * pz2
-            + R(8.) * mt.a1111 * py7
-            + R(2.) * mt.a1112 * py * (px6 + pz6 + R(3.) * py4 * (px2 + pz2))
-            + R(4.) * mt.a1122 * py3 * (px4 + pz4)
-            + R(2.) * mt.a1123 * py * px2 * pz2 * (px2 + R(2.) * py2 + pz2)
-            + (mt.tv1 * (eyy0 - eyy) + mt.tv2 * (exx0 - exx + ezz0 - ezz)) * py
-            + mt.tv3 * ((exy0 - exy) * px + (eyz0 - eyz) * pz));
-        const R qzc = fm * (R(2.) * mt.a1 * pz + R(4.) * mt.a11 * pz3
-            + R(2.) * mt.a12 * (py2 + px2) * pz
-            + R(6.) * mt.a111 * pz5
-            + R(4.) * mt.a112 * pz3 * (py2 + px2)
-            + R(2.) * mt.a112 * (py4 + px4) * pz
-            + R(2.) * mt.a123 * pz * py2 * px2
-            + R(8.) * mt.a1111 * pz7
-            + R(2.) * mt.a1112 * pz * (py6 + px6 + R(3.) * pz4 * (py2 + px2))
-            + R(4.) * mt.a1122 * pz3 * (py4 + px4)
-            + R(2.) * mt.a1123 * pz * px2 * py2 * (px2 + py2 + R(2.) * pz2)
-            + (mt.tv1 * (ezz0 - ezz) + mt.tv2 * (exx0 - exx + eyy0 - eyy)) * pz
-            + mt.tv3 * ((exz0 - exz) * px + (eyz0 - eyz) * py));
+        R qxc, qyc, qzc;
+        if constexpr (is_mixed<R>::value) {
+            // mixed form: the same Landau field with p_a factored out and the
+            // powers and pair sums shared by the three components (FMA
+            // contraction; FP32 rounding, not the reference's order):
+            // dF/dp_a = p_a [2a1 + o2 (4a11 + o2 (6a111 + 8a1111 o2))
+            //   + s (2a12 + 4a112 o2 + 6a1112 o4) + q (2a112 + 4a1122 o2)
+            //   + 2a1112 c + r (2a123 + 2a1123 (2 o2 + s))]
+            // with o2, o4 = p_a^2, p_a^4 and s, q, c, r = the sum of squares,
+            // fourth and sixth powers, and the product of squares of the
+            // other two components
+            const R x2 = px * px, y2 = py * py, z2 = pz * pz;
+            const R x4 = x2 * x2, y4 = y2 * y2, z4 = z2 * z2;
+            const R x6 = x4 * x2, y6 = y4 * y2, z6 = z4 * z2;
+            const R c1 = R(2.) * mt.a1, c11 = R(4.) * mt.a11, c111 = R(6.) * mt.a111, c1111 = R(8.) * mt.a1111;
+            const R c12 = R(2.) * mt.a12, c112a = R(4.) * mt.a112, c1112a = R(6.) * mt.a1112, c112b = R(2.) * mt.a112;
+            const R c1122 = R(4.) * mt.a1122, c1112b = R(2.) * mt.a1112, c123 = R(2.) * mt.a123, c1123 = R(2.) * mt.a1123;
+            auto br = [&](R o2, R o4, R s_, R q_, R cc, R r_) {
+                R b = c1 + o2 * (c11 + o2 * (c111 + c1111 * o2));
+                b = b + s_ * (c12 + c112a * o2 + c1112a * o4);
+                b = b + q_ * (c112b + c1122 * o2);
+                b = b + c1112b * cc;
+                b = b + r_ * (c123 + c1123 * (R(2.) * o2 + s_));
+                return b;
+            };
+            qxc = fm * (px * br(x2, x4, y2 + z2, y4 + z4, y6 + z6, y2 * z2)
+                        + (mt.tv1 * (exx0 - exx) + mt.tv2 * (eyy0 - eyy + ezz0 - ezz)) * px
+                        + mt.tv3 * ((exy0 - exy) * py + (exz0 - exz) * pz));
+            qyc = fm * (py * br(y2, y4, x2 + z2, x4 + z4, x6 + z6, x2 * z2)
+                        + (mt.tv1 * (eyy0 - eyy) + mt.tv2 * (exx0 - exx + ezz0 - ezz)) * py
+                        + mt.tv3 * ((exy0 - exy) * px + (eyz0 - eyz) * pz));
+            qzc = fm * (pz * br(z2, z4, x2 + y2, x4 + y4, x6 + y6, x2 * y2)
+                        + (mt.tv1 * (ezz0 - ezz) + mt.tv2 * (exx0 - exx + eyy0 - eyy)) * pz
+                        + mt.tv3 * ((exz0 - exz) * px + (eyz0 - eyz) * py));
+        } else {
+            const R px2 = px * px, py2 = py * py, pz2 = pz * pz;
+            const R px3 = px2 * px, py3 = py2 * py, pz3 = pz2 * pz;
+            const R px4 = px2 * px2, py4 = py2 * py2, pz4 = pz2 * pz2;
+            const R px5 = px4 * px, py5 = py4 * py, pz5 = pz4 * pz;
+            const R px6 = px4 * px2, py6 = py4 * py2, pz6 = pz4 * pz2;
+            const R px7 = px6 * px, py7 = py6 * py, pz7 = pz6 * pz;
+            qxc = fm * (R(2.) * mt.a1 * px + R(4.) * mt.a11 * px3
+                + R(2.) * mt.a12 * (py2 + pz2) * px
+                + R(6.) * mt.a111 * px5
+                + R(4.) * mt.a112 * px3 * (py2 + pz2)
+                + R(2.) * mt.a112 * (py4 + pz4) * px
+                + R(2.) * mt.a123 * px * py2 * pz2
+                + R(8.) * mt.a1111 * px7
+                + R(2.) * mt.a1112 * px * (py6 + pz6 + R(3.) * px4 * (py2 + pz2))
+                + R(4.) * mt.a1122 * px3 * (py4 + pz4)
+                + R(2.) * mt.a1123 * px * py2 * pz2 * (R(2.) * px2 + py2 + pz2)
+                + (mt.tv1 * (exx0 - exx) + mt.tv2 * (eyy0 - eyy + ezz0 - ezz)) * px
+                + mt.tv3 * ((exy0 - exy) * py + (exz0 - exz) * pz));
+            qyc = fm * (R(2.) * mt.a1 * py + R(4.) * mt.a11 * py3
+                + R(2.) * mt.a12 * (pz2 + px2) * py
+                + R(6.) * mt.a111 * py5
+                + R(4.) * mt.a112 * py3 * (px2 + pz2)
+                + R(2.) * mt.a112 * (px4 + pz4) * py
+                + R(2.) * mt.a123 * py * px2 * pz2
+                + R(8.) * mt.a1111 * py7
+                + R(2.) * mt.a1112 * py * (px6 + pz6 + R(3.) * py4 * (px2 + pz2))
+                + R(4.) * mt.a1122 * py3 * (px4 + pz4)
+                + R(2.) * mt.a1123 * py * px2 * pz2 * (px2 + R(2.) * py2 + pz2)
+                + (mt.tv1 * (eyy0 - eyy) + mt.tv2 * (exx0 - exx + ezz0 - ezz)) * py
+                + mt.tv3 * ((exy0 - exy) * px + (eyz0 - eyz) * pz));
+            qzc = fm * (R(2.) * mt.a1 * pz + R(4.) * mt.a11 * pz3
+                + R(2.) * mt.a12 * (py2 + px2) * pz
+                + R(6.) * mt.a111 * pz5
+                + R(4.) * mt.a112 * pz3 * (py2 + px2)
+                + R(2.) * mt.a112 * (py4 + px4) * pz
+                + R(2.) * mt.a123 * pz * py2 * px2
+                + R(8.) * mt.a1111 * pz7
+                + R(2.) * mt.a1112 * pz * (py6 + px6 + R(3.) * pz4 * (py2 + px2))
+                + R(4.) * mt.a1122 * pz3 * (py4 + px4)
+                + R(2.) * mt.a1123 * pz * px2 * py2 * (px2 + py2 + R(2.) * pz2)
+                + (mt.tv1 * (ezz0 - ezz) + mt.tv2 * (exx0 - exx + eyy0 - eyy)) * pz
+                + mt.tv3 * ((exz0 - exz) * px + (eyz0 - eyz) * py));
+        }
         R gx, gy, gz;
         crt2glb(P, qxc, qyc, qzc, gx, gy, gz);
 
