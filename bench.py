@@ -476,9 +476,10 @@ def roofline(r, args, mfe_frac, mixed):
 
 def adjoint_cost(gf, torch, args, local_rank):
     """Cost of the discrete adjoint against a forward pass: FM LLG + FFT
-    magnetostatics on 256x256x32 (the adjoint configuration's grid, YIG-like
-    film, 1 T bias, per-cell damping 1e-3 with 10 % seeded noise, a 256-sample
-    x waveform), FP64.  Every time is device time on the engine's stream
+    magnetostatics + magnetoelastic elastodynamics on 256x256x32 (the adjoint
+    configuration's grid and physics: YIG-like magnetoelastic film with free
+    surfaces and the Liao boundary at k = 0, 1 T bias, per-cell damping 1e-3
+    with 10 % seeded noise, a 256-sample x waveform), FP64.  Every time is device time on the engine's stream
     (CUDA events around the enqueued work, host launch gaps included): the
     engine's graph-replayed forward step, the adjoint's own forward run
     (checkpoints every 200 steps, <m_x> trace) and its backward run (block
@@ -489,7 +490,9 @@ def adjoint_cost(gf, torch, args, local_rank):
         d = gf.decks.preset_fm_demag(nx=256, ny=256, nz=32, steps=steps)
         d.Hext_table = None
         d.Hext_stat = (0.0, 0.0, 1.0 / mu0)
-        d.materials[0].alpha = 1e-3
+        d.materials = [gf.decks.yig(1e-3, magnetoelastic=True)]
+        d.elastic, d.elasto_back, d.elasto_on = True, True, True
+        d.abc_1D, d.liao_w = False, 0.5
         gf.decks.write_deck(d, tmp)
         rng = np.random.default_rng(20241208)
         alpha = 1e-3 * (1.0 + 0.1 * rng.random(d.n))
@@ -529,7 +532,8 @@ def adjoint_cost(gf, torch, args, local_rank):
                 e1.record(stream)
                 e1.synchronize()
                 t_bwd = e0.elapsed_time(e1) / 1e3
-    return {"workload": "FM LLG + FFT magnetostatics, 256x256x32, FP64, per-cell alpha and 256-sample waveform",
+    return {"workload": "FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, 256x256x32, FP64, "
+                        "per-cell alpha and 256-sample waveform",
             "steps": steps, "checkpoint_every": K,
             "forward_ms_per_step": 1e3 * t_eng / steps,
             "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,

@@ -27,6 +27,7 @@
 #pragma once
 
 #include "gf_state.cuh"
+#include "gf_elastic.cuh"
 
 namespace gf {
 
@@ -34,9 +35,13 @@ namespace gf {
 struct AdjMat {
     double gdt;        // gamma * dt (the material's gyro times the time step)
     double Ms, ex_coef, Aex, K1c, K2c;
+    double B1c, B2c;   // magnetoelastic B1, B2 / (mu0 Ms)
     int aniso;
     uint32_t fm;
 };
+
+// six component arrays (strain, strain cotangent)
+struct C6 { double* c[6]; };
 
 __device__ inline double3 cross3(double3 a, double3 b) {
     return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
@@ -79,7 +84,7 @@ template <int S>
 __global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am,
                                                   const double* __restrict__ aij, int nmat, F3 y, F3 hd,
                                                   const double* __restrict__ alpha, double3 hext, F3 hs, F3 x, F3 acc,
-                                                  F3 ynext) {
+                                                  F3 ynext, C6 str) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const int nyz = P.ny * P.nz;
@@ -106,6 +111,14 @@ __global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __res
         } else if (mt.aniso == 2) {
             H.z += 2. * mt.K1c * m.z;
         }
+        if (str.c[0]) {
+            // magnetoelastic field of the stage strain (the engine's k_llg_fm)
+            const double exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
+            const double eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
+            H.x += -2. * (mt.B1c * exx * m.x + mt.B2c * (exy * m.y + exz * m.z));
+            H.y += -2. * (mt.B1c * eyy * m.y + mt.B2c * (exy * m.x + eyz * m.z));
+            H.z += -2. * (mt.B1c * ezz * m.z + mt.B2c * (exz * m.x + eyz * m.y));
+        }
         st3(hs, c, H);
         const double a = alpha[c];
         const double c1 = -mt.gdt / (1. + a * a), c2 = a * c1;
@@ -130,7 +143,7 @@ __global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __res
 // Hbar and Hbar_x (for the waveform reduction); adds alphabar.
 static __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am,
                                                  F3 y, F3 hs, F3 u, const double* __restrict__ alpha, F3 ybar, F3 hbar,
-                                                 double* __restrict__ abar, double* __restrict__ hbx) {
+                                                 double* __restrict__ abar, double* __restrict__ hbx, C6 str, C6 strbar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
@@ -138,6 +151,8 @@ static __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t*
         st3(ybar, c, make_double3(0., 0., 0.));
         st3(hbar, c, make_double3(0., 0., 0.));
         hbx[c] = 0.;
+        if (strbar.c[0])
+            for (int q = 0; q < 6; q++) strbar.c[q][c] = 0.;
         return;
     }
     const AdjMat& mt = am[id - 1];
@@ -167,9 +182,275 @@ static __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t*
     } else if (mt.aniso == 2) {
         mb.z += 2. * mt.K1c * hb.z;
     }
+    if (str.c[0]) {
+        // magnetoelastic field H_me = -2 (B1 e_aa m_a + B2 sum_b e_ab m_b):
+        // symmetric Jacobian in m, and the strain cotangent
+        const double exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
+        const double eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
+        const double B1 = mt.B1c, B2 = mt.B2c;
+        mb.x += -2. * (B1 * exx * hb.x + B2 * exy * hb.y + B2 * exz * hb.z);
+        mb.y += -2. * (B2 * exy * hb.x + B1 * eyy * hb.y + B2 * eyz * hb.z);
+        mb.z += -2. * (B2 * exz * hb.x + B2 * eyz * hb.y + B1 * ezz * hb.z);
+        strbar.c[0][c] = -2. * B1 * m.x * hb.x;
+        strbar.c[1][c] = -2. * B1 * m.y * hb.y;
+        strbar.c[2][c] = -2. * B1 * m.z * hb.z;
+        strbar.c[3][c] = -2. * B2 * (m.z * hb.y + m.y * hb.z);
+        strbar.c[4][c] = -2. * B2 * (m.z * hb.x + m.x * hb.z);
+        strbar.c[5][c] = -2. * B2 * (m.y * hb.x + m.x * hb.y);
+    }
     st3(ybar, c, mb);
     st3(hbar, c, hb);
     hbx[c] = hb.x;
+}
+
+// ---------------------------------------------------------------------------
+// Elastodynamic coupling (magnetoelastic decks).  Forward per stage s (the
+// engine's own k_elastic_tile and k_elastic_rk on the adjoint's buffers):
+//   f = div sigma(u_s, e0(m_s)),  e_s = cell strain of u_s (LLG field),
+//   k_u = dt v_s,  k_v = dens_dt f + md v_x + sd w_s (f - fs),
+// with v_x the step value, w = 1, 2, 2, 1 and fs the stage-1 force of the
+// previous step at stage 1 and of this step afterwards (elastic_dynamic_
+// solver.cpp:1295-1329); after stage 4 the Liao extrapolation replaces
+// u(k = 0) (elastodynamics_AbsorbingBoundary.cpp:91-230).  The reverse sweep
+// below transposes each of these maps.
+// ---------------------------------------------------------------------------
+
+// Cotangents of the elastic increments of stage S: uku, ukv = d loss /
+// d k_u, d k_v.  v-stage cotangent ybar_v = dt uku; force cotangent fbar;
+// lamacc_v += md ukv (k_v reads the step value v_x); the stage-1 force
+// collects -sd w ukv of the later stages (f0bar) and, at stage 1, the
+// cotangent phi of the next step's fs; phi_new = -sd ukv (stage 1 reads fs).
+template <int S>
+__global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __restrict__ mid, const DevMat* __restrict__ mats,
+                                                   F3 uku, F3 ukv, F3 ybar_v, F3 fbar, F3 lamacc_v, F3 f0bar, F3 phi,
+                                                   F3 phi_new) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const uint8_t id = mid[c];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        ybar_v.c[a][c] = P.dt * uku.c[a][c];
+        double fb = 0., pn = 0.;
+        if (id != 0) {
+            const DevMat& mt = mats[id - 1];
+            const double w = (S == 1 || S == 2) ? 2. : 1.;
+            const double g = ukv.c[a][c];
+            fb = (mt.dens_dt + mt.stiff_damp * w) * g;
+            lamacc_v.c[a][c] += mt.mass_damp * g;
+            if (S > 0) f0bar.c[a][c] += -mt.stiff_damp * w * g;
+            else { fb += f0bar.c[a][c] + phi.c[a][c]; pn = -mt.stiff_damp * g; }
+        }
+        fbar.c[a][c] = fb;
+        if (S == 0) phi_new.c[a][c] = pn;
+    }
+}
+
+// Pass 1 of the transposed stress stencil, per cell x: for each of its six
+// faces that is not stress-free, the face-stress cotangent
+// sbar = (fbar_lower - fbar_upper) / h (the face adds +sigma/h to the force
+// of the cell below it and -sigma/h to the one above), half of it to x's side
+// (sigma = mean of the two sides), through the rows of C_x to x's side
+// strain st (k_elastic_tile's side_rows: face normal and face shears from the
+// face's own gradient, the other components from x's face-gradient means,
+// engineering shears, minus e0).  Outputs per cell (27 x n, `to`):
+//   T[d][a] (9): cotangent of x's gradient du_a/dx_d on both of its d-faces
+//               (every mean (g_minus + g_plus)/2 or /4 enters both alike),
+//               plus the LLG strain's cotangent (the cell strain is the same
+//               means);
+//   O[f][a] (18): cotangent of the gradient on face f (2d: -d, 2d+1: +d) from
+//               x's own side of that face (normal and face shears).
+// The eigenstrain cotangent -st (x2 for shears) goes through the
+// magnetostriction e0_aa = 1.5 l100 (m_a^2 - 1/3), e0_ab = 1.5 l111 m_a m_b
+// into ybar_m (back: the run feeds the eigenstrain back).
+static __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __restrict__ mid, const DevMat* __restrict__ mats,
+                                                        F3 fbar, C6 strbar, F3 m, F3 ybar_m, int back, double* __restrict__ to) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long n = P.n;
+    double T[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, O[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const uint8_t id = mid[c];
+    if (id != 0) {
+        const DevMat& mt = mats[id - 1];
+        const int nyz = P.ny * P.nz;
+        const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+        const int pos[3] = {i, j, k}, nn[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
+        const int stride[3] = {nyz, P.nz, 1};
+        const double rh[3] = {P.rdx, P.rdy, P.rdz};
+        double d0b[6] = {0, 0, 0, 0, 0, 0};
+        const double fx[3] = {fbar.c[0][c], fbar.c[1][c], fbar.c[2][c]};
+        for (int D = 0; D < 3; D++) {
+            for (int side = 0; side < 2; side++) {
+                const bool edge = side == 0 ? pos[D] == 0 : pos[D] == nn[D] - 1;
+                if (edge && !per[D]) continue;
+                int q = pos[D] + (side == 0 ? -1 : 1);
+                q = q < 0 ? q + nn[D] : (q >= nn[D] ? q - nn[D] : q);
+                const int y = c + (q - pos[D]) * stride[D];
+                if (mid[y] == 0) continue;
+                const double fy_[3] = {fbar.c[0][y], fbar.c[1][y], fbar.c[2][y]};
+                double S_[3];
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const double lo = side == 0 ? fy_[r] : fx[r], up = side == 0 ? fx[r] : fy_[r];
+                    S_[r] = 0.5 * (lo - up) * rh[D];
+                }
+                double st[6];
+#pragma unroll
+                for (int qv = 0; qv < 6; qv++)
+                    st[qv] = mt.cij[face_row(D, 0)][qv] * S_[0] + mt.cij[face_row(D, 1)][qv] * S_[1]
+                             + mt.cij[face_row(D, 2)][qv] * S_[2];
+                double* o = O[2 * D + side];
+                if (D == 0) {
+                    o[0] += st[0]; o[2] += st[4]; o[1] += st[5];
+                    T[1][1] += 0.5 * st[1]; T[2][2] += 0.5 * st[2];
+                    T[2][1] += 0.5 * st[3]; T[1][2] += 0.5 * st[3];
+                    T[2][0] += 0.5 * st[4]; T[1][0] += 0.5 * st[5];
+                } else if (D == 1) {
+                    o[1] += st[1]; o[2] += st[3]; o[0] += st[5];
+                    T[0][0] += 0.5 * st[0]; T[2][2] += 0.5 * st[2];
+                    T[2][1] += 0.5 * st[3];
+                    T[2][0] += 0.5 * st[4]; T[0][2] += 0.5 * st[4];
+                    T[0][1] += 0.5 * st[5];
+                } else {
+                    o[2] += st[2]; o[1] += st[3]; o[0] += st[4];
+                    T[0][0] += 0.5 * st[0]; T[1][1] += 0.5 * st[1];
+                    T[1][2] += 0.5 * st[3]; T[0][2] += 0.5 * st[4];
+                    T[1][0] += 0.5 * st[5]; T[0][1] += 0.5 * st[5];
+                }
+                d0b[0] -= st[0]; d0b[1] -= st[1]; d0b[2] -= st[2];
+                d0b[3] -= 2. * st[3]; d0b[4] -= 2. * st[4]; d0b[5] -= 2. * st[5];
+            }
+        }
+        if (strbar.c[0]) {
+            // cell strain of the LLG: e_aa = (gm + gp)(a, a) / 2, shears / 4
+            const double e0_ = strbar.c[0][c], e1 = strbar.c[1][c], e2 = strbar.c[2][c];
+            const double e3 = strbar.c[3][c], e4 = strbar.c[4][c], e5 = strbar.c[5][c];
+            T[0][0] += 0.5 * e0_; T[1][1] += 0.5 * e1; T[2][2] += 0.5 * e2;
+            T[2][1] += 0.25 * e3; T[1][2] += 0.25 * e3;
+            T[2][0] += 0.25 * e4; T[0][2] += 0.25 * e4;
+            T[1][0] += 0.25 * e5; T[0][1] += 0.25 * e5;
+        }
+        if (back) {
+            const double mx = m.c[0][c], my = m.c[1][c], mz = m.c[2][c];
+            const double l1 = mt.l100_15, l2 = mt.l111_15;
+            ybar_m.c[0][c] += 2. * l1 * mx * d0b[0] + l2 * (mz * d0b[4] + my * d0b[5]);
+            ybar_m.c[1][c] += 2. * l1 * my * d0b[1] + l2 * (mz * d0b[3] + mx * d0b[5]);
+            ybar_m.c[2][c] += 2. * l1 * mz * d0b[2] + l2 * (my * d0b[3] + mx * d0b[4]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) to[(d * 3 + a) * n + c] = T[d][a];
+#pragma unroll
+    for (int f = 0; f < 6; f++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) to[(9 + f * 3 + a) * n + c] = O[f][a];
+}
+
+// Pass 2, per cell c: cotangent of the gradient on each of its faces that is
+// not stress-free (T of the two cells plus O of each side), then
+// ubar_a(c) = sum_d (gbar_d(lower face) - gbar_d(upper face)) / h_d
+// (g = (u(upper cell) - u(lower cell)) / h).  Written to ybar_u.
+static __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_t* __restrict__ mid, const double* __restrict__ to,
+                                                        F3 ybar_u) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const long n = P.n;
+    double ub[3] = {0., 0., 0.};
+    const uint8_t id = mid[c];
+    if (id != 0) {
+        const int nyz = P.ny * P.nz;
+        const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+        const int pos[3] = {i, j, k}, nn[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
+        const int stride[3] = {nyz, P.nz, 1};
+        const double rh[3] = {P.rdx, P.rdy, P.rdz};
+        for (int d = 0; d < 3; d++) {
+            const int qa = pos[d] == 0 ? nn[d] - 1 : pos[d] - 1, qb = pos[d] == nn[d] - 1 ? 0 : pos[d] + 1;
+            const int a_ = c + (qa - pos[d]) * stride[d], b_ = c + (qb - pos[d]) * stride[d];
+            const bool free_lo = (pos[d] == 0 && !per[d]) || mid[a_] == 0;
+            const bool free_hi = (pos[d] == nn[d] - 1 && !per[d]) || mid[b_] == 0;
+#pragma unroll
+            for (int comp = 0; comp < 3; comp++) {
+                const int tq = (d * 3 + comp);
+                double gl = 0., gu = 0.;
+                if (!free_lo) gl = to[tq * n + a_] + to[tq * n + c] + to[(9 + (2 * d + 1) * 3 + comp) * n + a_]
+                                   + to[(9 + (2 * d) * 3 + comp) * n + c];
+                if (!free_hi) gu = to[tq * n + c] + to[tq * n + b_] + to[(9 + (2 * d + 1) * 3 + comp) * n + c]
+                                   + to[(9 + (2 * d) * 3 + comp) * n + b_];
+                ub[comp] += (gl - gu) * rh[d];
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) ybar_u.c[a][c] = ub[a];
+}
+
+// Liao extrapolation after the step (forward): the history slot of this
+// step takes planes k = 1..4 of the step-start u, and u_new(k = 0) =
+// c1 u(1) - c2 u_{-1}(2) + c3 u_{-2}(3) - w u_{-3}(4) (k_elastic_bc's form)
+static __global__ void k_adj_liao(Params P, F3 ux, F3 unew, double* __restrict__ hist, double* __restrict__ last,
+                                 unsigned long long step) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long plane = (long)P.nx * P.ny;
+    if (t >= plane) return;
+    const long i = t / P.ny, j = t - i * P.ny;
+    const double w = P.liao_w;
+    const double c1 = 4. * w + 2. * (1. - w), c2 = 6. * w + (1. - w), c3 = 4. * w;
+    double* slot = hist + (size_t)(step & 3ull) * 12 * plane;
+    const double* h2 = hist + (size_t)((step + 3) & 3ull) * 12 * plane;
+    const double* h3 = hist + (size_t)((step + 2) & 3ull) * 12 * plane;
+    const double* h4 = hist + (size_t)((step + 1) & 3ull) * 12 * plane;
+    for (int a = 0; a < 3; a++) {
+        double uv[4];
+        for (int p = 1; p <= 4; p++) uv[p - 1] = ux.c[a][cid(P, i, j, p)];
+        const double t2 = h2[(a * 4 + 1) * plane + t], t3 = h3[(a * 4 + 2) * plane + t], t4 = h4[(a * 4 + 3) * plane + t];
+        for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = uv[p - 1];
+        const double v = c1 * uv[0] - c2 * t2 + c3 * t3 - w * t4;
+        unew.c[a][cid(P, i, j, 0)] = v;
+        last[a * plane + t] = v;
+    }
+}
+
+// Liao transpose at the start of a step's reverse sweep, before lambda is
+// copied into the RK accumulators: the cotangent L of u_new(k = 0) is taken
+// out of lambda (the RK's own value at k = 0 was overwritten) and parked for
+// the step values it came from: c1 L for this step's plane 1, -c2 L, c3 L,
+// -w L for planes 2, 3, 4 of the three earlier steps.  pend: 4 slots (target
+// step mod 4) x 3 components x planes k = 1..4.
+static __global__ void k_adj_liao_T(Params P, F3 lam, double* __restrict__ pend, unsigned long long step) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long plane = (long)P.nx * P.ny;
+    if (t >= plane) return;
+    const long i = t / P.ny, j = t - i * P.ny;
+    const double w = P.liao_w;
+    const double c1 = 4. * w + 2. * (1. - w), c2 = 6. * w + (1. - w), c3 = 4. * w;
+    auto at = [&](unsigned long long target, int a, int p) -> double& {
+        return pend[((size_t)((target & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
+    };
+    for (int a = 0; a < 3; a++) {
+        const long b0 = cid(P, i, j, 0);
+        const double L = lam.c[a][b0];
+        lam.c[a][b0] = 0.;
+        at(step, a, 1) += c1 * L;
+        if (step >= 1) at(step - 1, a, 2) += -c2 * L;
+        if (step >= 2) at(step - 2, a, 3) += c3 * L;
+        if (step >= 3) at(step - 3, a, 4) += -w * L;
+    }
+}
+
+// after a step's reverse sweep: the parked Liao cotangents of its step value
+// (planes 1..4) join lambda, and the slot is cleared for reuse
+static __global__ void k_adj_liao_pend(Params P, F3 lam, double* __restrict__ pend, unsigned long long step) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long plane = (long)P.nx * P.ny;
+    if (t >= plane) return;
+    const long i = t / P.ny, j = t - i * P.ny;
+    for (int a = 0; a < 3; a++)
+        for (int p = 1; p <= 4; p++) {
+            double& v = pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
+            lam.c[a][cid(P, i, j, p)] += v;
+            v = 0.;
+        }
 }
 
 // ybar += transposed exchange of Hbar: sum_f w_cf (ex_f Hbar_f - ex_c Hbar_c);

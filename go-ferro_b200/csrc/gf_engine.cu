@@ -3131,20 +3131,40 @@ struct gf_adjoint {
     double* alpha = nullptr;         // per cell
     std::vector<double> wave;        // excitation samples (A/m, x)
     std::vector<double> hext;        // nsteps x 4 x 3 external field of the deck per stage
-    double* X[3] = {};               // step value
-    double* Y[3][3] = {};            // stage states y2, y3, y4
+    // state of a step: m (0-2); with elastodynamics also u (3-5), v (6-8)
+    // and the stiffness-damping force store fs (9-11)
+    bool el = false;
+    int ns = 3;
+    double* X[12] = {};              // step value
+    double* Y[3][3] = {};            // stage states y2, y3, y4 (m)
     double* ACC[3] = {};
     double* HS[4][3] = {};           // effective field of each stage
     double* XJ[3] = {};              // stage-4 output of a recomputed step (discarded)
-    double* LAM[3] = {}; double* LAMACC[3] = {}; double* U[3] = {};
-    double* YBAR[3] = {}; double* HBAR[3] = {};
+    // cotangents: m (0-2), u (3-5), v (6-8)
+    double* LAM[9] = {}; double* LAMACC[9] = {}; double* U[9] = {};
+    double* YBAR[9] = {}; double* HBAR[3] = {};
     double* abar = nullptr; double* hbx = nullptr; double* wbar = nullptr;
+    // elastodynamics: stage u, v (stages 2-4), RK accumulators, the stage
+    // force, the stage strain (LLG field), the cotangents of the force, the
+    // stage-1 force of this step (f0bar) and of fs (phi), the transposed
+    // stencil's pass-1 output (27 n), Liao history and pending cotangents
+    double* US[3][3] = {}; double* VS[3][3] = {};
+    double* UACC[3] = {}; double* VACC[3] = {};
+    double* FORCE[3] = {};
+    double* STR[4][6] = {};
+    double* STRBAR[6] = {};
+    double* FBAR[3] = {}; double* F0BAR[3] = {}; double* PHI[3] = {}; double* PHINEW[3] = {};
+    double* TO = nullptr;
+    double* hist = nullptr;          // 4 slots x 12 planes (k_elastic_bc's layout)
+    double* last = nullptr;          // 3 planes
+    double* pend = nullptr;          // 4 slots x 3 components x 4 planes
     double* trace = nullptr;         // nsteps+1
     double* dldm = nullptr;          // nsteps+1
-    double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x 3n
-    double* xs = nullptr;            // step values of one block, ck_every x 3n
+    double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x ck_len
+    double* xs = nullptr;            // step values of one block, ck_every x ns n
     double* zero3 = nullptr;         // 3n zeros (demag field when magnetostatics is off)
     size_t ck_slots = 0;
+    size_t ck_len = 0;               // ns n (+ 51 planes of Liao state with elastodynamics)
 };
 
 namespace {
@@ -3189,46 +3209,125 @@ double3 adj_hext(const gf_adjoint* a, uint64_t step, int s) {
     return make_double3(h[0] + a->wave[seg], h[1], h[2]);
 }
 
-// stages of step `step` from step value x: the effective fields go to HS,
-// the stage states to Y; stage 4 writes xout (x itself in the forward run)
-int adj_stages(gf_adjoint* a, F3 x, uint64_t step, F3 xout) {
+// StageIO over the adjoint's buffers for the engine's elastic kernels: stage
+// m and u in, the force and the stage strain out; for k_elastic_rk the step
+// value (x), the stage v, the accumulators and the next stage's u, v
+StageIO adj_el_io(gf_adjoint* a, double* const* x, F3 ym, F3 yu, F3 yv, int s, F3 uout, F3 vout) {
+    gf_engine* eng = a->eng;
+    StageIO io = eng->io[0][0];          // tables, drive and materials of the engine
+    io.m_in = ym;
+    io.u_in = yu; io.v_in = yv;
+    io.u_x = F3{{x[3], x[4], x[5]}}; io.v_x = F3{{x[6], x[7], x[8]}};
+    io.u_acc = f3(a->UACC); io.v_acc = f3(a->VACC);
+    io.u_out = uout; io.v_out = vout;
+    io.force = f3(a->FORCE);
+    io.force_store = F3{{x[9], x[10], x[11]}};
+    for (int q = 0; q < 6; q++) { io.strain_c[q] = a->STR[s][q]; io.eps0_c[q] = nullptr; io.eig0_c[q] = nullptr;
+                                  io.sg[q] = nullptr; io.pge[q] = nullptr; }
+    return io;
+}
+
+template <int S>
+int adj_el_stage(gf_adjoint* a, const StageIO& io) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    ETileMaps tm;
+    std::memset(&tm, 0, sizeof(tm));
+    tm.err = eng->tma_err;
+    const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
+                    (P.nx + eng->el_chunk - 1) / eng->el_chunk);
+    if (eng->el_cubic)
+        GF_CU(launch_tiled(k_elastic_tile<S, true, double>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                           eng->el_chunk, eng->el_nmat, tm));
+    else
+        GF_CU(launch_tiled(k_elastic_tile<S, false, double>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                           eng->el_chunk, eng->el_nmat, tm));
+    return GF_OK;
+}
+
+template <int S>
+int adj_el_rk(gf_adjoint* a, const StageIO& io) {
+    gf_engine* eng = a->eng;
+    GF_CU(launch(k_elastic_rk<S, double>, dim3(blocks_for(eng->P.n, kThreads)), dim3(kThreads), 0, eng->stream, eng->P, io));
+    return GF_OK;
+}
+
+// stages of step `step` from step value x (ns components): the effective
+// fields go to HS, the stage states to Y (m) and US / VS (u, v), the stage
+// strains to STR; stage 4 writes m to xout (x itself in the forward run) and
+// leaves the new u, v in UACC / VACC.  The elastic parts run the engine's
+// own k_elastic_tile and k_elastic_rk (so the forward run is the engine's
+// discretisation); k_elastic_rk of stage 1 stores the step's stage-1 force
+// in x's fs.
+int adj_stages(gf_adjoint* a, double* const* x, uint64_t step, F3 xout) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     F3 acc = f3(a->ACC);
-    F3 y = x;
+    F3 xm{{x[0], x[1], x[2]}};
+    F3 y = xm, yu{}, yv{};
+    if (a->el) { yu = F3{{x[3], x[4], x[5]}}; yv = F3{{x[6], x[7], x[8]}}; }
     for (int s = 0; s < 4; s++) {
         F3 hd;
         GF_TRY(adj_demag(a, y, hd));
+        C6 str{};
+        if (a->el) {
+            const StageIO io = adj_el_io(a, x, y, yu, yv, s, F3{}, F3{});
+            if (s == 0) GF_TRY(adj_el_stage<0>(a, io));
+            else if (s == 1) GF_TRY(adj_el_stage<1>(a, io));
+            else if (s == 2) GF_TRY(adj_el_stage<2>(a, io));
+            else GF_TRY(adj_el_stage<3>(a, io));
+            if (P.elasto_on) for (int q = 0; q < 6; q++) str.c[q] = a->STR[s][q];
+        }
         const double3 he = adj_hext(a, step, s);
         // stage 4 reads the step value from and writes the new one to xout:
         // x itself in the forward run (each thread reads its own cell before
         // writing it); a discarded buffer when a step is recomputed for the
         // reverse sweep, which needs only the stage fields
         F3 ynext = (s < 3) ? f3(a->Y[s]) : xout;
-        F3 xs_ = (s < 3) ? x : xout;
+        F3 xs_ = (s < 3) ? xm : xout;
         cudaError_t e;
         if (s == 0) e = launch(k_adj_eval<0>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                               (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+                               (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
         else if (s == 1) e = launch(k_adj_eval<1>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
         else if (s == 2) e = launch(k_adj_eval<2>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
         else e = launch(k_adj_eval<3>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                        (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext);
+                        (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
         GF_CU(e);
+        if (a->el) {
+            const F3 uo = (s < 3) ? f3(a->US[s]) : F3{}, vo = (s < 3) ? f3(a->VS[s]) : F3{};
+            const StageIO io = adj_el_io(a, x, y, yu, yv, s, uo, vo);
+            if (s == 0) GF_TRY(adj_el_rk<0>(a, io));
+            else if (s == 1) GF_TRY(adj_el_rk<1>(a, io));
+            else if (s == 2) GF_TRY(adj_el_rk<2>(a, io));
+            else GF_TRY(adj_el_rk<3>(a, io));
+            if (s < 3) { yu = f3(a->US[s]); yv = f3(a->VS[s]); }
+        }
         if (s < 3) y = f3(a->Y[s]);
     }
     return GF_OK;
 }
 
-// the stage-4 update of the forward run writes x in place: k_adj_eval<3>
-// reads x (the step value) and y4 (the stage state), so xout = x is safe
-int adj_step_forward(gf_adjoint* a, F3 x, uint64_t step) {
-    // stage 4 must combine with the step value x while writing it: the kernel
-    // reads x[c] before writing x[c] in the same thread only
-    return adj_stages(a, x, step, x);
+// one forward step in place: m by k_adj_eval<3>, which reads x[c] before
+// writing it in the same thread; then the Liao extrapolation of u(k = 0)
+// and the new u, v from the accumulators
+int adj_step_forward(gf_adjoint* a, double* const* x, uint64_t step) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    GF_TRY(adj_stages(a, x, step, F3{{x[0], x[1], x[2]}}));
+    if (a->el) {
+        const long plane = (long)P.nx * P.ny;
+        GF_CU(launch(k_adj_liao, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, eng->stream, P, F3{{x[3], x[4], x[5]}},
+                     f3(a->UACC), a->hist, a->last, (unsigned long long)step));
+        for (int c = 0; c < 3; c++) {
+            GF_CU(cudaMemcpyAsync(x[3 + c], a->UACC[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, eng->stream));
+            GF_CU(cudaMemcpyAsync(x[6 + c], a->VACC[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, eng->stream));
+        }
+    }
+    return GF_OK;
 }
 
 int adj_mean_x(gf_adjoint* a, const double* x0, long slot) {
@@ -3258,24 +3357,36 @@ int adj_wave_add(gf_adjoint* a, long seg) {
 }
 
 // reverse sweep of step `step` (lambda = d loss / d x_{step+1} in LAM on entry,
-// d loss / d x_step on exit); x is the step value x_step
-int adj_step_backward(gf_adjoint* a, F3 x, uint64_t step) {
+// d loss / d x_step on exit; with elastodynamics also phi = d loss / d fs);
+// x is the step value x_step (ns components)
+int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
+    const int ng = a->el ? 3 : 1;               // cotangent groups: m, u, v
     GF_TRY(adj_stages(a, x, step, f3(a->XJ)));
-    for (int c = 0; c < 3; c++) {
-        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    if (a->el) {
+        // the new u(k = 0) came from the Liao extrapolation, not the RK sum
+        const long plane = (long)P.nx * P.ny;
+        GF_CU(launch(k_adj_liao_T, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, f3(a->LAM + 3), a->pend,
+                     (unsigned long long)step));
+        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->F0BAR[c], 0, sizeof(double) * P.n, st));
     }
-    // u4 = lambda / 6 (written by a scaled copy: the comb kernel of a virtual stage 4)
-    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
-    GF_CU(launch(k_scale_f3, dim3(bn), dim3(kThreads), 0, st, P, f3(a->U), 1. / 6.));
+    for (int c = 0; c < 3 * ng; c++) {
+        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+        // u4 = lambda / 6 (written by a scaled copy: the comb kernel of a virtual stage 4)
+        GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int g = 0; g < ng; g++) GF_CU(launch(k_scale_f3, dim3(bn), dim3(kThreads), 0, st, P, f3(a->U + 3 * g), 1. / 6.));
     const long seg = (long)((step * (uint64_t)a->nw) / a->nsteps);
     for (int s = 3; s >= 0; s--) {
-        F3 y = (s == 0) ? x : f3(a->Y[s - 1]);
+        F3 y = (s == 0) ? F3{{x[0], x[1], x[2]}} : f3(a->Y[s - 1]);
+        C6 str{}, strbar{};
+        if (a->el && P.elasto_on)
+            for (int q = 0; q < 6; q++) { str.c[q] = a->STR[s][q]; strbar.c[q] = a->STRBAR[q]; }
         GF_CU(launch(k_adj_vjp, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, y,
-                     f3(a->HS[s]), f3(a->U), (const double*)a->alpha, f3(a->YBAR), f3(a->HBAR), a->abar, a->hbx));
+                     f3(a->HS[s]), f3(a->U), (const double*)a->alpha, f3(a->YBAR), f3(a->HBAR), a->abar, a->hbx, str, strbar));
         const double* R = nullptr;
         if (eng->demag_mode == 0) {
             GF_CU(launch(k_adj_pack, dim3(bn), dim3(kThreads), 0, st, P, f3(a->HBAR), eng->Mfft));
@@ -3288,20 +3399,74 @@ int adj_step_backward(gf_adjoint* a, F3 x, uint64_t step) {
         }
         GF_CU(launch(k_adj_field_T, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
                      (const double*)a->aij, a->nmat, f3(a->HBAR), R, f3(a->YBAR)));
+        if (a->el) {
+            // elastic increments, then the transposed stress and strain stencils
+            cudaError_t e;
+            const F3 uku = f3(a->U + 3), ukv = f3(a->U + 6);
+            if (s == 3) e = launch(k_adj_el_vjp<3>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
+                                   uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
+            else if (s == 2) e = launch(k_adj_el_vjp<2>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
+                                        uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
+            else if (s == 1) e = launch(k_adj_el_vjp<1>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
+                                        uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
+            else e = launch(k_adj_el_vjp<0>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
+                            uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
+            GF_CU(e);
+            GF_CU(launch(k_adj_el_p1, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
+                         f3(a->FBAR), strbar, y, f3(a->YBAR), (int)P.elasto_back, a->TO));
+            GF_CU(launch(k_adj_el_p2, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const double*)a->TO,
+                         f3(a->YBAR + 3)));
+        }
         GF_TRY(adj_wave_add(a, seg));
-        cudaError_t e;
-        if (s == 3) e = launch(k_adj_comb<3>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
-        else if (s == 2) e = launch(k_adj_comb<2>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
-        else if (s == 1) e = launch(k_adj_comb<1>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
-        else e = launch(k_adj_comb<0>, dim3(bn), dim3(kThreads), 0, st, P, f3(a->LAM), f3(a->LAMACC), f3(a->U), f3(a->YBAR));
-        GF_CU(e);
+        for (int g = 0; g < ng; g++) {
+            const F3 lam = f3(a->LAM + 3 * g), lacc = f3(a->LAMACC + 3 * g), u = f3(a->U + 3 * g), yb = f3(a->YBAR + 3 * g);
+            cudaError_t e;
+            if (s == 3) e = launch(k_adj_comb<3>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
+            else if (s == 2) e = launch(k_adj_comb<2>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
+            else if (s == 1) e = launch(k_adj_comb<1>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
+            else e = launch(k_adj_comb<0>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
+            GF_CU(e);
+        }
     }
-    for (int c = 0; c < 3; c++) std::swap(a->LAM[c], a->LAMACC[c]);
+    for (int c = 0; c < 3 * ng; c++) std::swap(a->LAM[c], a->LAMACC[c]);
+    if (a->el) {
+        for (int c = 0; c < 3; c++) std::swap(a->PHI[c], a->PHINEW[c]);
+        const long plane = (long)P.nx * P.ny;
+        GF_CU(launch(k_adj_liao_pend, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, f3(a->LAM + 3), a->pend,
+                     (unsigned long long)step));
+    }
     return GF_OK;
 }
 
 int adj_check(gf_adjoint* a) {
     if (!a || !a->eng) return GF_EINVAL;
+    return GF_OK;
+}
+
+// the state x (ns arrays) to / from a contiguous slot, component-major; a
+// checkpoint slot also holds the Liao history and last value
+int adj_save(gf_adjoint* a, double* dst, bool liao) {
+    gf_engine* eng = a->eng;
+    const long n = eng->P.n, plane = (long)eng->P.nx * eng->P.ny;
+    for (int q = 0; q < a->ns; q++)
+        GF_CU(cudaMemcpyAsync(dst + (size_t)q * n, a->X[q], sizeof(double) * n, cudaMemcpyDeviceToDevice, eng->stream));
+    if (liao && a->el) {
+        GF_CU(cudaMemcpyAsync(dst + (size_t)a->ns * n, a->hist, sizeof(double) * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(dst + (size_t)a->ns * n + 48 * plane, a->last, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice,
+                              eng->stream));
+    }
+    return GF_OK;
+}
+int adj_load(gf_adjoint* a, const double* src, bool liao) {
+    gf_engine* eng = a->eng;
+    const long n = eng->P.n, plane = (long)eng->P.nx * eng->P.ny;
+    for (int q = 0; q < a->ns; q++)
+        GF_CU(cudaMemcpyAsync(a->X[q], src + (size_t)q * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, eng->stream));
+    if (liao && a->el) {
+        GF_CU(cudaMemcpyAsync(a->hist, src + (size_t)a->ns * n, sizeof(double) * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(a->last, src + (size_t)a->ns * n + 48 * plane, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice,
+                              eng->stream));
+    }
     return GF_OK;
 }
 
@@ -3317,8 +3482,15 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
     const Deck& d = eng->deck;
     const Params& P = eng->P;
     if (eng->mixed) { eng->err = "the adjoint runs on an FP64 engine"; return GF_EUNSUPPORTED; }
-    if (!d.any_fm || d.any_afm || d.any_fe || d.elastodynamics || d.em_dynamic)
-        { eng->err = "the adjoint covers ferromagnetic LLG with magnetostatics only (no AFM, FE, elastic or Maxwell fields)"; return GF_EUNSUPPORTED; }
+    if (!d.any_fm || d.any_afm || d.any_fe || d.em_dynamic)
+        { eng->err = "the adjoint covers ferromagnetic LLG with magnetostatics and elastodynamics (no AFM, FE or Maxwell fields)"; return GF_EUNSUPPORTED; }
+    if (d.elastodynamics) {
+        if (d.abc_1D) { eng->err = "the adjoint covers the Liao boundary of the elastic run, not the Mur one (if_1D_ABC)"; return GF_EUNSUPPORTED; }
+        if (d.strain_pulse) { eng->err = "the adjoint does not cover the elastic strain source"; return GF_EUNSUPPORTED; }
+        if (P.ny < P.nz) { eng->err = "the adjoint needs ny >= nz (the reference's z-face neighbour rule for k = ny-1 is not transposed)"; return GF_EUNSUPPORTED; }
+        if (P.nz < 5) { eng->err = "the adjoint's Liao boundary needs nz >= 5"; return GF_EUNSUPPORTED; }
+        if (eng->es_eps[0] || eng->es_eig[0]) { eng->err = "the adjoint does not cover static strain inputs"; return GF_EUNSUPPORTED; }
+    }
     if (P.rot) { eng->err = "the adjoint needs if_OrientRotate off"; return GF_EUNSUPPORTED; }
     if (eng->demag_mode > 0) { eng->err = "the adjoint covers the FFT magnetostatics (no demag factors / 1-D model)"; return GF_EUNSUPPORTED; }
     if (d.read_Hext_nonunif) { eng->err = "the adjoint does not cover a non-uniform external field"; return GF_EUNSUPPORTED; }
@@ -3341,6 +3513,7 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
         if (m.fm) {
             t.gdt = m.gyro * d.dt; t.Ms = m.Ms; t.ex_coef = 2. / kMu0 / m.Ms; t.Aex = m.Aex;
             t.K1c = m.K1 / kMu0 / m.Ms; t.K2c = m.K2 / kMu0 / m.Ms; t.aniso = (int)m.aniso_type;
+            t.B1c = m.B1 / kMu0 / m.Ms; t.B2c = m.B2 / kMu0 / m.Ms;
         }
     }
     std::vector<double> aij((size_t)(a->nmat + 1) * (a->nmat + 1), 0.);
@@ -3369,15 +3542,36 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
         }
         if (cudaMemcpy(a->alpha, al.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (alpha)"; return fail(GF_ECUDA); }
     }
+    a->el = d.elastodynamics;
+    a->ns = a->el ? 12 : 3;
     double** bufs3[] = {a->X, a->ACC, a->XJ, a->LAM, a->LAMACC, a->U, a->YBAR, a->HBAR,
                         a->Y[0], a->Y[1], a->Y[2], a->HS[0], a->HS[1], a->HS[2], a->HS[3]};
     for (double** b : bufs3)
         if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+    const long plane = (long)P.nx * P.ny;
+    a->ck_len = (size_t)a->ns * n;
+    if (a->el) {
+        double** el3[] = {a->X + 3, a->X + 6, a->X + 9, a->LAM + 3, a->LAM + 6, a->LAMACC + 3, a->LAMACC + 6,
+                          a->U + 3, a->U + 6, a->YBAR + 3, a->YBAR + 6, a->US[0], a->US[1], a->US[2],
+                          a->VS[0], a->VS[1], a->VS[2], a->UACC, a->VACC, a->FORCE, a->FBAR, a->F0BAR, a->PHI, a->PHINEW};
+        for (double** b : el3)
+            if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+        for (int s_ = 0; s_ < 4; s_++)
+            for (int q = 0; q < 6; q++)
+                if ((rc = adj_alloc(a, &a->STR[s_][q], (size_t)n)) != GF_OK) return fail(rc);
+        for (int q = 0; q < 6; q++)
+            if ((rc = adj_alloc(a, &a->STRBAR[q], (size_t)n)) != GF_OK) return fail(rc);
+        if ((rc = adj_alloc(a, &a->TO, (size_t)27 * n)) != GF_OK) return fail(rc);
+        if ((rc = adj_alloc(a, &a->hist, (size_t)48 * plane)) != GF_OK) return fail(rc);
+        if ((rc = adj_alloc(a, &a->last, (size_t)3 * plane)) != GF_OK) return fail(rc);
+        if ((rc = adj_alloc(a, &a->pend, (size_t)48 * plane)) != GF_OK) return fail(rc);
+        a->ck_len += (size_t)51 * plane;
+    }
     if ((rc = adj_alloc(a, &a->abar, (size_t)n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->hbx, (size_t)n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->zero3, (size_t)3 * n)) != GF_OK) return fail(rc);
-    if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * 3 * n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * a->ns * n)) != GF_OK) return fail(rc);
     if (cudaStreamSynchronize(eng->stream) != cudaSuccess) { eng->err = "adjoint set-up"; return fail(GF_ECUDA); }
     *out = a;
     return GF_OK;
@@ -3430,25 +3624,41 @@ int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace) {
         a->ck_slots = 0;
     }
     if (!a->ck) {
-        GF_TRY(adj_alloc(a, &a->ck, slots * 3 * (size_t)n));
+        GF_TRY(adj_alloc(a, &a->ck, slots * a->ck_len));
         a->ck_slots = slots;
     }
     if (a->trace) { cudaFree(a->trace); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->trace), a->allocs.end()); }
     if (a->dldm) { cudaFree(a->dldm); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->dldm), a->allocs.end()); }
     GF_TRY(adj_alloc(a, &a->trace, (size_t)nsteps + 1));
     GF_TRY(adj_alloc(a, &a->dldm, (size_t)nsteps + 1));
-    // initial state: the engine's current m
+    // initial state: the engine's current m (and u, v, force store, Liao
+    // history: the engine's slot of its step e is the adjoint's slot of step
+    // e - steps_done)
     double* const* m0 = cur(eng, eng->m);
     for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->X[c], m0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->ck + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    if (a->el) {
+        double* const* u0 = cur(eng, eng->u);
+        double* const* v0 = cur(eng, eng->v);
+        for (int c = 0; c < 3; c++) {
+            GF_CU(cudaMemcpyAsync(a->X[3 + c], u0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(a->X[6 + c], v0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(a->X[9 + c], eng->force_store[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        const size_t plane = (size_t)P.nx * P.ny;
+        for (int sl = 0; sl < 4; sl++)
+            GF_CU(cudaMemcpyAsync(a->hist + (size_t)sl * 12 * plane,
+                                  eng->liao_hist + (size_t)((eng->steps_done + (uint64_t)sl) & 3ull) * 12 * plane,
+                                  sizeof(double) * 12 * plane, cudaMemcpyDeviceToDevice, st));
+        GF_CU(cudaMemcpyAsync(a->last, eng->liao_last, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice, st));
+    }
+    GF_TRY(adj_save(a, a->ck, true));
     GF_TRY(adj_mean_x(a, a->X[0], 0));
     for (uint64_t k = 0; k < nsteps; k++) {
-        GF_TRY(adj_step_forward(a, f3(a->X), k));
+        GF_TRY(adj_step_forward(a, a->X, k));
         GF_TRY(adj_mean_x(a, a->X[0], (long)k + 1));
         if ((k + 1) % (uint64_t)a->ck_every == 0) {
             const size_t slot = (size_t)((k + 1) / (uint64_t)a->ck_every);
-            for (int c = 0; c < 3; c++)
-                GF_CU(cudaMemcpyAsync(a->ck + (slot * 3 + c) * (size_t)n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            GF_TRY(adj_save(a, a->ck + slot * a->ck_len, true));
         }
     }
     GF_CU(cudaMemcpyAsync(mx_trace, a->trace, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, st));
@@ -3472,7 +3682,11 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     const uint64_t N = a->nsteps;
     const double inv_nfm = 1. / (double)eng->deck.NFM;
     GF_CU(cudaMemcpyAsync(a->dldm, dloss_dmx, sizeof(double) * (N + 1), cudaMemcpyHostToDevice, st));
-    for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->LAM[c], 0, sizeof(double) * n, st));
+    for (int c = 0; c < (a->el ? 9 : 3); c++) GF_CU(cudaMemsetAsync(a->LAM[c], 0, sizeof(double) * n, st));
+    if (a->el) {
+        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->PHI[c], 0, sizeof(double) * n, st));
+        GF_CU(cudaMemsetAsync(a->pend, 0, sizeof(double) * 48 * (size_t)P.nx * P.ny, st));
+    }
     GF_CU(cudaMemsetAsync(a->abar, 0, sizeof(double) * n, st));
     GF_CU(cudaMemsetAsync(a->wbar, 0, sizeof(double) * a->nw, st));
     GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, f3(a->LAM),
@@ -3482,16 +3696,15 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     for (uint64_t b = nblocks; b-- > 0;) {
         const uint64_t s0 = b * K, s1 = std::min(N, s0 + K);
         // recompute the block's step values x_s0 .. x_{s1-1}
-        for (int c = 0; c < 3; c++) {
-            GF_CU(cudaMemcpyAsync(a->X[c], a->ck + (b * 3 + c) * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        }
+        GF_TRY(adj_load(a, a->ck + b * a->ck_len, true));
         for (uint64_t k = s0; k < s1; k++) {
-            for (int c = 0; c < 3; c++)
-                GF_CU(cudaMemcpyAsync(a->xs + ((k - s0) * 3 + c) * (size_t)n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-            if (k + 1 < s1) GF_TRY(adj_step_forward(a, f3(a->X), k));
+            GF_TRY(adj_save(a, a->xs + (k - s0) * (size_t)a->ns * n, false));
+            if (k + 1 < s1) GF_TRY(adj_step_forward(a, a->X, k));
         }
         for (uint64_t k = s1; k-- > s0;) {
-            GF_TRY(adj_step_backward(a, f3v(a->xs + (k - s0) * 3 * (size_t)n, n), k));
+            double* xp[12];
+            for (int q = 0; q < a->ns; q++) xp[q] = a->xs + ((k - s0) * (size_t)a->ns + q) * n;
+            GF_TRY(adj_step_backward(a, xp, k));
             GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
                          f3(a->LAM), (const double*)a->dldm, (long)k, inv_nfm));
         }
@@ -3513,9 +3726,8 @@ int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count) {
     const uint64_t K = (uint64_t)a->ck_every, N = a->nsteps;
     const uint64_t b = N / K;
     cudaStream_t st = eng->stream;
-    for (int c = 0; c < 3; c++)
-        GF_CU(cudaMemcpyAsync(a->X[c], a->ck + (b * 3 + c) * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_step_forward(a, f3(a->X), k));
+    GF_TRY(adj_load(a, a->ck + b * a->ck_len, true));
+    for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_step_forward(a, a->X, k));
     for (int c = 0; c < 3; c++)
         GF_CU(cudaMemcpyAsync(host_m + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     GF_TRY(static_field_now(eng));

@@ -413,7 +413,7 @@ const char* gf_batch_last_error(const gf_batch* b);
 /* Free the batch (not the engines). */
 void gf_batch_destroy(gf_batch* b);
 
-/* ---- Discrete adjoint of the ferromagnetic RK4 step ---------------------
+/* ---- Discrete adjoint of the ferromagnetic (magnetoelastic) RK4 step -----
  * Gradients of a loss of the <m_x>(t) trace with respect to an x-directed
  * excitation waveform (n_wave samples, piecewise constant over equal shares
  * of the run, added to the deck's external field) and to a per-cell damping
@@ -421,22 +421,33 @@ void gf_batch_destroy(gf_batch* b);
  * magnetic_solver.cpp:206).  Differentiates the engine's discretisation of
  * get_dm_RK{1..4} / update_m_RK* / update_m (magnetic_solver.cpp:3-229,
  * 1515-1636) with per-stage FFT magnetostatics (magnetostatic_solver.cpp:
- * 114-219): exchange, anisotropy (no frame rotation), Zeeman; decks with
- * DMI, AFM, FE, elastic or Maxwell fields are GF_EUNSUPPORTED.  The reference
- * has no adjoint; these entry points have no counterpart there.  FP64 engines
- * only.  The adjoint uses the engine's stream and FFT buffers: do not advance
- * the engine while an adjoint call runs. */
+ * 114-219): exchange, anisotropy (no frame rotation), Zeeman; and, on decks
+ * with elastodynamics, the magnetoelastic field of the cell strain
+ * (magnetic_solver.cpp:148-156), the stress divergence with the
+ * magnetostrictive eigenstrain and the elastic RK4 with step-start mass
+ * damping and the stiffness-damping force store (elastic_dynamic_solver.cpp:
+ * 3-104, 841-1329, 2801-3057) and the Liao boundary at k = 0
+ * (elastodynamics_AbsorbingBoundary.cpp:91-230), whose history reaches
+ * three steps back.  Decks with DMI, AFM, FE or Maxwell fields, the Mur
+ * elastic boundary (if_1D_ABC), an elastic source, static strain inputs,
+ * ny < nz (the reference's z-face neighbour rule for k = ny-1) or nz < 5
+ * are GF_EUNSUPPORTED.  The reference has no adjoint; these entry points
+ * have no counterpart there.  FP64 engines only.  The adjoint uses the
+ * engine's stream and FFT buffers: do not advance the engine while an
+ * adjoint call runs. */
 typedef struct gf_adjoint gf_adjoint;
 /* checkpoint_every: steps between stored states (the backward run recomputes
- * the steps in between; device memory ~ 24 * n * checkpoint_every bytes). */
+ * the steps in between; device memory ~ 24 * n * checkpoint_every bytes, 96
+ * with elastodynamics). */
 int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint** out);
 /* per-cell damping (nx*ny*nz values; default: the material's alpha) */
 int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count);
 /* waveform samples in A/m (n_wave values; default 0) */
 int gf_adjoint_set_waveform(gf_adjoint* a, const double* w, size_t count);
-/* Run nsteps RK4 steps from the engine's current m and external-field clock
- * (the engine's own state is not advanced); mx_trace gets <m_x> at steps
- * 0..nsteps (nsteps+1 values). Synchronous. */
+/* Run nsteps RK4 steps from the engine's current state (m; with
+ * elastodynamics also u, v, the force store and the Liao history) and
+ * external-field clock (the engine's own state is not advanced); mx_trace
+ * gets <m_x> at steps 0..nsteps (nsteps+1 values). Synchronous. */
 int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace);
 /* Given dloss/d<m_x> at steps 0..nsteps (nsteps+1 values), the gradients
  * with respect to the waveform (n_wave values) and the per-cell alpha

@@ -139,3 +139,95 @@ def test_adjoint_rejects_unsupported_decks(gf, tmp_path):
         with pytest.raises(gf.GFError) as ei:
             gf.Adjoint(eng, n_wave=4)
         assert ei.value.code == -7
+
+
+# ---------------------------------------------------------------------------
+# magnetoelastic coupling with elastodynamics (the adjoint configuration's
+# physics): the stress divergence with the magnetostrictive eigenstrain, the
+# magnetoelastic field of the cell strain, the elastic RK4 with step-start
+# mass damping and the stiffness-damping force store, and the Liao boundary
+# at k = 0 are transposed.  The film's magnetostriction is raised 100x so the
+# elastic path changes the gradients by far more than the FD tolerance.
+# ---------------------------------------------------------------------------
+def me_film(gf, tmp_path, nx=16, ny=16, nz=8, steps=200, boost=100.0):
+    D = gf.decks
+    d = D.preset_fm_demag(nx=nx, ny=ny, nz=nz, steps=steps)
+    d.Hext_table = None
+    d.Hext_stat = (0.0, 0.0, 1.0 / MU0)
+    m = D.yig(0.02, magnetoelastic=True)
+    m.lam100 *= boost
+    m.lam111 *= boost
+    d.materials = [m]
+    d.elastic, d.elasto_back, d.elasto_on = True, True, True
+    d.abc_1D, d.liao_w = False, 0.5
+    gf.decks.write_deck(d, str(tmp_path))
+    return d
+
+
+def test_adjoint_forward_matches_engine_magnetoelastic(gf, tmp_path):
+    me_film(gf, tmp_path, steps=40)
+    with gf.Engine(str(tmp_path), device=0) as eng:
+        with gf.Adjoint(eng, n_wave=4, checkpoint_every=16) as adj:
+            tr = adj.forward(40)
+            mfin = adj.final_m()
+        ref = [eng.average("m")[0]]
+        for _ in range(40):
+            eng.advance(1)
+            ref.append(eng.average("m")[0])
+        m_eng = eng.download("m")
+        u_eng = eng.download("u")
+    assert np.max(np.abs(u_eng)) > 0.0
+    assert np.max(np.abs(tr - np.array(ref))) <= 1e-12
+    assert np.max(np.abs(mfin - m_eng)) <= 1e-12
+
+
+def _grads(gf, tmp_path, d, steps, nw, wave0, alpha0, fd):
+    with gf.Engine(str(tmp_path), device=0) as eng:
+        with gf.Adjoint(eng, n_wave=nw, checkpoint_every=64) as adj:
+            def loss_of(wave, alpha):
+                adj.set_waveform(wave)
+                adj.set_alpha(alpha)
+                return spectral_loss_np(adj.forward(steps))
+            adj.set_waveform(wave0)
+            adj.set_alpha(alpha0)
+            tr = adj.forward(steps)
+            X = np.fft.rfft(tr)
+            n = np.arange(tr.size)
+            g = np.zeros(tr.size)
+            for k in range(BAND.start, BAND.stop):
+                g += 2.0 * np.real(np.conj(X[k]) * np.exp(-2j * np.pi * k * n / tr.size))
+            gw, ga = adj.backward(g)
+            if not fd:
+                return gw, ga, None
+            h = 1e-4 * np.max(np.abs(wave0))
+            fd_w = np.empty(nw)
+            for j in range(nw):
+                wp, wm = wave0.copy(), wave0.copy()
+                wp[j] += h
+                wm[j] -= h
+                fd_w[j] = (loss_of(wp, alpha0) - loss_of(wm, alpha0)) / (2 * h)
+            mc = d.material_cell().ravel() == 1
+            rng = np.random.default_rng(3)
+            v = np.where(rng.random(d.n) < 0.5, 1.0, -1.0) * mc
+            ha = 1e-4 * float(np.mean(alpha0[mc]))
+            fd_a = (loss_of(wave0, alpha0 + ha * v) - loss_of(wave0, alpha0 - ha * v)) / (2 * ha)
+            return gw, ga, (fd_w, v, fd_a)
+
+
+def test_adjoint_gradients_magnetoelastic_match_finite_differences(gf, tmp_path):
+    steps, nw = 200, 8
+    d = me_film(gf, tmp_path / "me", steps=steps)
+    mc = d.material_cell().ravel() == 1
+    rng = np.random.default_rng(5)
+    alpha0 = 0.02 * (1.0 + 0.1 * rng.random(d.n)) * mc
+    tt = (np.arange(nw) + 0.5) / nw
+    wave0 = (1e-2 / MU0) * np.sin(2 * np.pi * tt) * np.exp(-4.0 * (tt - 0.4) ** 2)
+    gw, ga, (fd_w, v, fd_a) = _grads(gf, tmp_path / "me", d, steps, nw, wave0, alpha0, True)
+    err_w = np.max(np.abs(gw - fd_w)) / np.max(np.abs(fd_w))
+    assert err_w <= 1e-4, f"waveform gradient vs FD: {err_w:.2e}"
+    ad = float(ga @ v)
+    assert abs(ad - fd_a) <= 1e-4 * abs(fd_a), f"alpha directional gradient {ad:.6e} vs FD {fd_a:.6e}"
+    # the elastic path matters: without magnetostriction the gradients differ
+    d0 = me_film(gf, tmp_path / "plain", steps=steps, boost=0.0)
+    gw0, _, _ = _grads(gf, tmp_path / "plain", d0, steps, nw, wave0, alpha0, False)
+    assert np.max(np.abs(gw - gw0)) > 1e-2 * np.max(np.abs(gw))
