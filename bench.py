@@ -17,7 +17,7 @@ against the FP64 engine on the same initial state.  At N=1 it also carries
 `step_roofline` (the whole step's algorithmic bytes per cell-step over the
 measured copy peak), `other_workloads` (the coupled magnetoelastic 128x128x96
 film and the 64x64x16 FM + magnetostatics run, both forms), `adjoint` (the
-cost of the discrete adjoint against the FP64 forward step on a 256x256x32
+cost of the discrete adjoint against the forward step, FP32 mixed and FP64, on a 256x256x32
 ferromagnetic film) and `batched` (48 ferroelectric instances per graph).
 
 `--impl ours` times the engine (CUDA events on the engine stream, max over
@@ -479,13 +479,18 @@ def adjoint_cost(gf, torch, args, local_rank):
     magnetostatics + magnetoelastic elastodynamics on 256x256x32 (the adjoint
     configuration's grid and physics: YIG-like magnetoelastic film with free
     surfaces and the Liao boundary at k = 0, 1 T bias, per-cell damping 1e-3
-    with 10 % seeded noise, a 256-sample x waveform), FP64.  Every time is device time on the engine's stream
-    (CUDA events around the enqueued work, host launch gaps included): the
-    engine's graph-replayed forward step, the adjoint's own forward run
-    (checkpoints every 200 steps, <m_x> trace) and its backward run (block
-    recomputation, stage recompute, reverse sweep)."""
+    with 10 % seeded noise, a 256-sample x waveform), in the FP32 mixed form
+    (the configuration's form) and in FP64.  Every time is device time on the
+    engine's stream (CUDA events around the enqueued work, host launch gaps
+    included): the engine's graph-replayed forward step of the same
+    precision, the adjoint's own forward run (checkpoints every 200 steps,
+    <m_x> trace) and its backward run (block recomputation, stage recompute,
+    reverse sweep).  The mixed entry also gives the relative difference of
+    its gradients from the FP64 adjoint's on the same inputs."""
     mu0 = 1.256637061e-6
     steps, K, nw = args.adjoint_steps, 200, 256
+    out = {}
+    grads = {}
     with tempfile.TemporaryDirectory() as tmp:
         d = gf.decks.preset_fm_demag(nx=256, ny=256, nz=32, steps=steps)
         d.Hext_table = None
@@ -498,52 +503,58 @@ def adjoint_cost(gf, torch, args, local_rank):
         alpha = 1e-3 * (1.0 + 0.1 * rng.random(d.n))
         tt = (np.arange(nw) + 0.5) / nw
         wave = (1e-3 / mu0) * np.sin(2 * np.pi * 8 * tt) * np.exp(-((tt - 0.3) / 0.1) ** 2)
-        with gf.Engine(tmp, device=local_rank) as eng:
-            stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
-            eng.advance(3)
-            eng.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            eng.advance(steps)
-            e1.record(stream)
-            e1.synchronize()
-            t_eng = e0.elapsed_time(e1) / 1e3
-            with gf.Adjoint(eng, nw, K) as adj:
-                adj.set_alpha(alpha)
-                adj.set_waveform(wave)
-                adj.forward(4)
+        for prec in ("mixed", "fp64"):
+            with gf.Engine(tmp, device=local_rank, precision=prec) as eng:
+                stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
+                eng.advance(3)
                 eng.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                tr = adj.forward(steps)
+                eng.advance(steps)
                 e1.record(stream)
                 e1.synchronize()
-                t_fwd = e0.elapsed_time(e1) / 1e3
-                # d loss / d <m_x>: spectral power of the trace in 0.1-0.5 THz
-                X = np.fft.rfft(tr)
-                f = np.fft.rfftfreq(tr.size, d.dt)
-                band = np.nonzero((f >= 0.1e12) & (f <= 0.5e12))[0]
-                n = np.arange(tr.size)
-                g = np.zeros(tr.size)
-                for k in band:
-                    g += 2.0 * np.real(np.conj(X[k]) * np.exp(-2j * np.pi * k * n / tr.size))
-                eng.synchronize()
-                e0.record(stream)
-                adj.backward(g)
-                e1.record(stream)
-                e1.synchronize()
-                t_bwd = e0.elapsed_time(e1) / 1e3
-    return {"workload": "FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, 256x256x32, FP64, "
-                        "per-cell alpha and 256-sample waveform",
-            "steps": steps, "checkpoint_every": K,
-            "forward_ms_per_step": 1e3 * t_eng / steps,
-            "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,
-            "backward_ms_per_step": 1e3 * t_bwd / steps,
-            "backward_over_forward": t_bwd / t_eng,
-            "forward_plus_backward_over_forward": (t_fwd + t_bwd) / t_eng,
-            "timing": "device time (CUDA events on the engine stream)",
-            "loss_band_bins": int(len(band)),
-            "definition": "backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
-                          "forward = the engine's FP64 step (CUDA graph)"}
+                t_eng = e0.elapsed_time(e1) / 1e3
+                with gf.Adjoint(eng, nw, K) as adj:
+                    adj.set_alpha(alpha)
+                    adj.set_waveform(wave)
+                    adj.forward(4)
+                    eng.synchronize()
+                    e0.record(stream)
+                    tr = adj.forward(steps)
+                    e1.record(stream)
+                    e1.synchronize()
+                    t_fwd = e0.elapsed_time(e1) / 1e3
+                    # d loss / d <m_x>: spectral power of the trace in 0.1-0.5 THz
+                    X = np.fft.rfft(tr)
+                    f = np.fft.rfftfreq(tr.size, d.dt)
+                    band = np.nonzero((f >= 0.1e12) & (f <= 0.5e12))[0]
+                    n = np.arange(tr.size)
+                    g = np.zeros(tr.size)
+                    for k in band:
+                        g += 2.0 * np.real(np.conj(X[k]) * np.exp(-2j * np.pi * k * n / tr.size))
+                    eng.synchronize()
+                    e0.record(stream)
+                    gw, ga = adj.backward(g)
+                    e1.record(stream)
+                    e1.synchronize()
+                    t_bwd = e0.elapsed_time(e1) / 1e3
+                    grads[prec] = (gw, ga)
+            out[prec] = {"steps": steps, "checkpoint_every": K,
+                         "forward_ms_per_step": 1e3 * t_eng / steps,
+                         "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,
+                         "backward_ms_per_step": 1e3 * t_bwd / steps,
+                         "backward_over_forward": t_bwd / t_eng,
+                         "forward_plus_backward_over_forward": (t_fwd + t_bwd) / t_eng,
+                         "loss_band_bins": int(len(band))}
+    (gw, ga), (gw64, ga64) = grads["mixed"], grads["fp64"]
+    out["mixed"]["grad_wave_rel_diff_vs_fp64"] = float(np.max(np.abs(gw - gw64)) / max(np.max(np.abs(gw64)), 1e-300))
+    out["mixed"]["grad_alpha_rel_diff_vs_fp64"] = float(np.max(np.abs(ga - ga64)) / max(np.max(np.abs(ga64)), 1e-300))
+    out["workload"] = ("FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, 256x256x32, "
+                       "per-cell alpha and 256-sample waveform; FP32 mixed (the configuration's form) and FP64")
+    out["timing"] = "device time (CUDA events on the engine stream)"
+    out["definition"] = ("backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
+                         "forward = the engine's step of the same precision (CUDA graph)")
+    return out
 
 
 SWEEP_SIZES = [(32, 32, 32), (48, 48, 32), (64, 64, 32), (96, 96, 24)]

@@ -416,11 +416,12 @@ def _dp(a: np.ndarray):
 
 
 class Adjoint:
-    """Discrete adjoint of an FP64 engine's ferromagnetic RK4 step
-    (gf_adjoint_*): <m_x>(t) forward from the engine's current state, and the
-    gradients of a loss of that trace with respect to an x-directed
-    excitation waveform (n_wave piecewise-constant samples, A/m) and the
-    per-cell damping alpha."""
+    """Discrete adjoint of an engine's ferromagnetic RK4 step, with its
+    magnetoelastic coupling on elastodynamic decks (gf_adjoint_*): <m_x>(t)
+    forward from the engine's current state, and the gradients of a loss of
+    that trace with respect to an x-directed excitation waveform (n_wave
+    piecewise-constant samples, A/m) and the per-cell damping alpha.  On a
+    mixed-form engine the adjoint's fields are FP32 (the gradients FP64)."""
 
     def __init__(self, engine: "Engine", n_wave: int, checkpoint_every: int = 200):
         self.engine = engine

@@ -1,4 +1,5 @@
-// Discrete adjoint of the ferromagnetic RK4 step (FP64).
+// Discrete adjoint of the ferromagnetic RK4 step (FP64, and FP32 on a
+// mixed-form engine).
 //
 // The adjoint differentiates the engine's own discretisation of
 // magnetic_system::get_dm_RK{1..4} (magnetic_solver.cpp:3-229) and the RK4
@@ -31,33 +32,42 @@
 
 namespace gf {
 
-// per-material constants of the adjoint's dynamics
-struct AdjMat {
-    double gdt;        // gamma * dt (the material's gyro times the time step)
-    double Ms, ex_coef, Aex, K1c, K2c;
-    double B1c, B2c;   // magnetoelastic B1, B2 / (mu0 Ms)
+// per-material constants of the adjoint's dynamics (R: the real type of the
+// adjoint's fields, double on an FP64 engine, float on a mixed one)
+template <class R>
+struct AdjMatT {
+    R gdt;             // gamma * dt (the material's gyro times the time step)
+    R Ms, ex_coef, Aex, K1c, K2c;
+    R B1c, B2c;        // magnetoelastic B1, B2 / (mu0 Ms)
     int aniso;
     uint32_t fm;
 };
+using AdjMat = AdjMatT<double>;
 
 // six component arrays (strain, strain cotangent)
-struct C6 { double* c[6]; };
+template <class R> struct C6T { R* c[6]; };
+using C6 = C6T<double>;
 
-__device__ inline double3 cross3(double3 a, double3 b) {
-    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+// three-vector of the adjoint's real type
+template <class R> struct V3 { R x, y, z; };
+template <class R> __host__ __device__ inline V3<R> mk3(R a, R b, R c) { return V3<R>{a, b, c}; }
+template <class R> __device__ inline V3<R> cross3(V3<R> a, V3<R> b) {
+    return mk3<R>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-__device__ inline double dot3(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ inline double3 ld3(const F3& f, int c) { return make_double3(f.c[0][c], f.c[1][c], f.c[2][c]); }
-__device__ inline void st3(const F3& f, int c, double3 v) { f.c[0][c] = v.x; f.c[1][c] = v.y; f.c[2][c] = v.z; }
+template <class R> __device__ inline R dot3(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> __device__ inline V3<R> ld3(const F3T<R>& f, int c) { return mk3<R>(f.c[0][c], f.c[1][c], f.c[2][c]); }
+template <class R> __device__ inline void st3(const F3T<R>& f, int c, V3<R> v) { f.c[0][c] = v.x; f.c[1][c] = v.y; f.c[2][c] = v.z; }
 
 // neighbour cells with periodic wrap and the exchange weight A_cf / dx_f^2
 // of each face (0 on ferromagnetic surfaces and non-periodic boundaries)
+template <class R>
 struct AdjNbr {
     int nb[6];
-    double w[6];
+    R w[6];
 };
-__device__ inline void adj_neighbours(const Params& P, const uint8_t* mid, const AdjMat* am, const double* aij, int nmat,
-                                      int i, int j, int k, uint8_t id, AdjNbr& n) {
+template <class R>
+__device__ inline void adj_neighbours(const Params& P, const uint8_t* mid, const AdjMatT<R>* am, const R* aij, int nmat,
+                                      int i, int j, int k, uint8_t id, AdjNbr<R>& n) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int ib = (i == 0) ? nx - 1 : i - 1, iF = (i == nx - 1) ? 0 : i + 1;
     const int jb = (j == 0) ? ny - 1 : j - 1, jF = (j == ny - 1) ? 0 : j + 1;
@@ -67,136 +77,154 @@ __device__ inline void adj_neighbours(const Params& P, const uint8_t* mid, const
     n.nb[4] = (i * ny + j) * nz + kb; n.nb[5] = (i * ny + j) * nz + kF;
     const bool edge[6] = {i == 0 && !P.per_x, i == nx - 1 && !P.per_x, j == 0 && !P.per_y,
                           j == ny - 1 && !P.per_y, k == 0 && !P.per_z, k == nz - 1 && !P.per_z};
-    const double r2[3] = {P.rdx * P.rdx, P.rdy * P.rdy, P.rdz * P.rdz};
+    const R r2[3] = {R(P.rdx * P.rdx), R(P.rdy * P.rdy), R(P.rdz * P.rdz)};
 #pragma unroll
     for (int f = 0; f < 6; f++) {
         const uint8_t q = mid[n.nb[f]];
         const bool fmq = q != 0 && am[q - 1].fm;
-        n.w[f] = (edge[f] || !fmq) ? 0. : aij[id * (nmat + 1) + q] * r2[f / 2];
+        n.w[f] = (edge[f] || !fmq) ? R(0) : aij[id * (nmat + 1) + q] * r2[f / 2];
     }
 }
 
 // One RK stage of the adjoint's forward dynamics at state y with demag field
 // hd: writes the effective field H (kept for the reverse sweep) and the RK4
 // combination with step value x and increment sum acc (stage 3 updates x in
-// place; stages 0-2 write the next stage state ynext).
-template <int S>
-__global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am,
-                                                  const double* __restrict__ aij, int nmat, F3 y, F3 hd,
-                                                  const double* __restrict__ alpha, double3 hext, F3 hs, F3 x, F3 acc,
-                                                  F3 ynext, C6 str) {
+// place; stages 0-2 write the next stage state ynext).  In FP32 the step
+// value carries a compensation word xc: stage 3 forms x + (acc + k/6) + xc
+// by an error-free sum (the mixed engine's compensated RK update).
+template <int S, class R>
+__global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
+                                                  const R* __restrict__ aij, int nmat, F3T<R> y, F3T<R> hd,
+                                                  const R* __restrict__ alpha, V3<R> hext, F3T<R> hs, F3T<R> x, F3T<R> xc,
+                                                  F3T<R> acc, F3T<R> ynext, C6T<R> str) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const int nyz = P.ny * P.nz;
     const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
     const uint8_t id = mid[c];
-    double3 kk = make_double3(0., 0., 0.);
+    V3<R> kk = mk3<R>(R(0), R(0), R(0));
     if (id != 0 && am[id - 1].fm) {
-        const AdjMat& mt = am[id - 1];
-        AdjNbr n;
+        const AdjMatT<R>& mt = am[id - 1];
+        AdjNbr<R> n;
         adj_neighbours(P, mid, am, aij, nmat, i, j, k, id, n);
-        const double3 m = ld3(y, c);
-        double3 hex = make_double3(0., 0., 0.);
+        const V3<R> m = ld3(y, c);
+        V3<R> hex = mk3<R>(R(0), R(0), R(0));
 #pragma unroll
         for (int f = 0; f < 6; f++) {
-            const double3 mf = ld3(y, n.nb[f]);
+            const V3<R> mf = ld3(y, n.nb[f]);
             hex.x += n.w[f] * (mf.x - m.x); hex.y += n.w[f] * (mf.y - m.y); hex.z += n.w[f] * (mf.z - m.z);
         }
-        double3 H = ld3(hd, c);
+        V3<R> H = ld3(hd, c);
         H.x += mt.ex_coef * hex.x + hext.x; H.y += mt.ex_coef * hex.y + hext.y; H.z += mt.ex_coef * hex.z + hext.z;
         if (mt.aniso == 1) {
-            H.x += -2. * (mt.K1c * (m.y * m.y + m.z * m.z) + mt.K2c * m.y * m.y * m.z * m.z) * m.x;
-            H.y += -2. * (mt.K1c * (m.x * m.x + m.z * m.z) + mt.K2c * m.x * m.x * m.z * m.z) * m.y;
-            H.z += -2. * (mt.K1c * (m.x * m.x + m.y * m.y) + mt.K2c * m.x * m.x * m.y * m.y) * m.z;
+            H.x += R(-2) * (mt.K1c * (m.y * m.y + m.z * m.z) + mt.K2c * m.y * m.y * m.z * m.z) * m.x;
+            H.y += R(-2) * (mt.K1c * (m.x * m.x + m.z * m.z) + mt.K2c * m.x * m.x * m.z * m.z) * m.y;
+            H.z += R(-2) * (mt.K1c * (m.x * m.x + m.y * m.y) + mt.K2c * m.x * m.x * m.y * m.y) * m.z;
         } else if (mt.aniso == 2) {
-            H.z += 2. * mt.K1c * m.z;
+            H.z += R(2) * mt.K1c * m.z;
         }
         if (str.c[0]) {
             // magnetoelastic field of the stage strain (the engine's k_llg_fm)
-            const double exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
-            const double eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
-            H.x += -2. * (mt.B1c * exx * m.x + mt.B2c * (exy * m.y + exz * m.z));
-            H.y += -2. * (mt.B1c * eyy * m.y + mt.B2c * (exy * m.x + eyz * m.z));
-            H.z += -2. * (mt.B1c * ezz * m.z + mt.B2c * (exz * m.x + eyz * m.y));
+            const R exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
+            const R eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
+            H.x += R(-2) * (mt.B1c * exx * m.x + mt.B2c * (exy * m.y + exz * m.z));
+            H.y += R(-2) * (mt.B1c * eyy * m.y + mt.B2c * (exy * m.x + eyz * m.z));
+            H.z += R(-2) * (mt.B1c * ezz * m.z + mt.B2c * (exz * m.x + eyz * m.y));
         }
         st3(hs, c, H);
-        const double a = alpha[c];
-        const double c1 = -mt.gdt / (1. + a * a), c2 = a * c1;
-        const double3 p = cross3(m, H), q = cross3(m, p);
-        kk = make_double3(c1 * p.x + c2 * q.x, c1 * p.y + c2 * q.y, c1 * p.z + c2 * q.z);
+        const R a = alpha[c];
+        const R c1 = -mt.gdt / (R(1) + a * a), c2 = a * c1;
+        const V3<R> p = cross3(m, H), q = cross3(m, p);
+        kk = mk3<R>(c1 * p.x + c2 * q.x, c1 * p.y + c2 * q.y, c1 * p.z + c2 * q.z);
     } else {
-        st3(hs, c, make_double3(0., 0., 0.));
+        st3(hs, c, mk3<R>(R(0), R(0), R(0)));
     }
-    const double kv[3] = {kk.x, kk.y, kk.z};
+    const R kv[3] = {kk.x, kk.y, kk.z};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double xv = x.c[a][c];
-        if (S == 0) { acc.c[a][c] = kv[a] / 6.; ynext.c[a][c] = xv + kv[a] * 0.5; }
-        else if (S == 1) { acc.c[a][c] = acc.c[a][c] + kv[a] / 3.; ynext.c[a][c] = xv + kv[a] * 0.5; }
-        else if (S == 2) { acc.c[a][c] = acc.c[a][c] + kv[a] / 3.; ynext.c[a][c] = xv + kv[a]; }
-        else { x.c[a][c] = xv + (acc.c[a][c] + kv[a] / 6.); }
+        const R xv = x.c[a][c];
+        if constexpr (is_mixed<R>::value) {
+            if (S == 0) { acc.c[a][c] = kv[a] * (1.f / 6.f); ynext.c[a][c] = xv + kv[a] * 0.5f; }
+            else if (S == 1) { acc.c[a][c] = acc.c[a][c] + kv[a] * (1.f / 3.f); ynext.c[a][c] = xv + kv[a] * 0.5f; }
+            else if (S == 2) { acc.c[a][c] = acc.c[a][c] + kv[a] * (1.f / 3.f); ynext.c[a][c] = xv + kv[a]; }
+            else {
+                float sum, err;
+                two_sum(xv, (acc.c[a][c] + kv[a] * (1.f / 6.f)) + xc.c[a][c], sum, err);
+                x.c[a][c] = sum;
+                xc.c[a][c] = err;
+            }
+        } else {
+            if (S == 0) { acc.c[a][c] = kv[a] / 6.; ynext.c[a][c] = xv + kv[a] * 0.5; }
+            else if (S == 1) { acc.c[a][c] = acc.c[a][c] + kv[a] / 3.; ynext.c[a][c] = xv + kv[a] * 0.5; }
+            else if (S == 2) { acc.c[a][c] = acc.c[a][c] + kv[a] / 3.; ynext.c[a][c] = xv + kv[a]; }
+            else { x.c[a][c] = xv + (acc.c[a][c] + kv[a] / 6.); }
+        }
     }
 }
 
 // Local part of the vector-Jacobian product of stage s: the cross products,
 // the anisotropy Jacobian, the damping derivative; writes ybar (local part),
-// Hbar and Hbar_x (for the waveform reduction); adds alphabar.
-static __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am,
-                                                 F3 y, F3 hs, F3 u, const double* __restrict__ alpha, F3 ybar, F3 hbar,
-                                                 double* __restrict__ abar, double* __restrict__ hbx, C6 str, C6 strbar) {
+// Hbar and Hbar_x (for the waveform reduction); adds alphabar (FP64 in both
+// forms: it sums over every stage of the run).
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
+                                                 F3T<R> y, F3T<R> hs, F3T<R> u, const R* __restrict__ alpha, F3T<R> ybar,
+                                                 F3T<R> hbar, double* __restrict__ abar, R* __restrict__ hbx, C6T<R> str,
+                                                 C6T<R> strbar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
+    const R z = R(0);
     if (!(id != 0 && am[id - 1].fm)) {
-        st3(ybar, c, make_double3(0., 0., 0.));
-        st3(hbar, c, make_double3(0., 0., 0.));
-        hbx[c] = 0.;
+        st3(ybar, c, mk3<R>(z, z, z));
+        st3(hbar, c, mk3<R>(z, z, z));
+        hbx[c] = z;
         if (strbar.c[0])
-            for (int q = 0; q < 6; q++) strbar.c[q][c] = 0.;
+            for (int q = 0; q < 6; q++) strbar.c[q][c] = z;
         return;
     }
-    const AdjMat& mt = am[id - 1];
-    const double3 m = ld3(y, c), H = ld3(hs, c), w = ld3(u, c);
-    const double a = alpha[c];
-    const double c1 = -mt.gdt / (1. + a * a), c2 = a * c1;
-    const double dc1 = c1 * (-2. * a / (1. + a * a)), dc2 = c1 + a * dc1;
-    const double3 p = cross3(m, H), q = cross3(m, p);
-    abar[c] += dot3(w, make_double3(dc1 * p.x + dc2 * q.x, dc1 * p.y + dc2 * q.y, dc1 * p.z + dc2 * q.z));
-    const double3 um = cross3(w, m);
-    const double3 umm = cross3(um, m);
-    const double3 hb = make_double3(c1 * um.x + c2 * umm.x, c1 * um.y + c2 * umm.y, c1 * um.z + c2 * umm.z);
-    const double3 t1 = cross3(H, w), t2 = cross3(p, w), t3 = cross3(H, um);
-    double3 mb = make_double3(c1 * t1.x + c2 * (t2.x + t3.x), c1 * t1.y + c2 * (t2.y + t3.y), c1 * t1.z + c2 * (t2.z + t3.z));
+    const AdjMatT<R>& mt = am[id - 1];
+    const V3<R> m = ld3(y, c), H = ld3(hs, c), w = ld3(u, c);
+    const R a = alpha[c];
+    const R c1 = -mt.gdt / (R(1) + a * a), c2 = a * c1;
+    const R dc1 = c1 * (R(-2) * a / (R(1) + a * a)), dc2 = c1 + a * dc1;
+    const V3<R> p = cross3(m, H), q = cross3(m, p);
+    abar[c] += (double)dot3(w, mk3<R>(dc1 * p.x + dc2 * q.x, dc1 * p.y + dc2 * q.y, dc1 * p.z + dc2 * q.z));
+    const V3<R> um = cross3(w, m);
+    const V3<R> umm = cross3(um, m);
+    const V3<R> hb = mk3<R>(c1 * um.x + c2 * umm.x, c1 * um.y + c2 * umm.y, c1 * um.z + c2 * umm.z);
+    const V3<R> t1 = cross3(H, w), t2 = cross3(p, w), t3 = cross3(H, um);
+    V3<R> mb = mk3<R>(c1 * t1.x + c2 * (t2.x + t3.x), c1 * t1.y + c2 * (t2.y + t3.y), c1 * t1.z + c2 * (t2.z + t3.z));
     if (mt.aniso == 1) {
-        const double K1 = mt.K1c, K2 = mt.K2c;
-        const double x2 = m.x * m.x, y2 = m.y * m.y, z2 = m.z * m.z;
-        const double jxx = -2. * (K1 * (y2 + z2) + K2 * y2 * z2);
-        const double jyy = -2. * (K1 * (x2 + z2) + K2 * x2 * z2);
-        const double jzz = -2. * (K1 * (x2 + y2) + K2 * x2 * y2);
-        const double jxy = -4. * m.x * m.y * (K1 + K2 * z2);
-        const double jxz = -4. * m.x * m.z * (K1 + K2 * y2);
-        const double jyz = -4. * m.y * m.z * (K1 + K2 * x2);
+        const R K1 = mt.K1c, K2 = mt.K2c;
+        const R x2 = m.x * m.x, y2 = m.y * m.y, z2 = m.z * m.z;
+        const R jxx = R(-2) * (K1 * (y2 + z2) + K2 * y2 * z2);
+        const R jyy = R(-2) * (K1 * (x2 + z2) + K2 * x2 * z2);
+        const R jzz = R(-2) * (K1 * (x2 + y2) + K2 * x2 * y2);
+        const R jxy = R(-4) * m.x * m.y * (K1 + K2 * z2);
+        const R jxz = R(-4) * m.x * m.z * (K1 + K2 * y2);
+        const R jyz = R(-4) * m.y * m.z * (K1 + K2 * x2);
         mb.x += jxx * hb.x + jxy * hb.y + jxz * hb.z;
         mb.y += jxy * hb.x + jyy * hb.y + jyz * hb.z;
         mb.z += jxz * hb.x + jyz * hb.y + jzz * hb.z;
     } else if (mt.aniso == 2) {
-        mb.z += 2. * mt.K1c * hb.z;
+        mb.z += R(2) * mt.K1c * hb.z;
     }
     if (str.c[0]) {
         // magnetoelastic field H_me = -2 (B1 e_aa m_a + B2 sum_b e_ab m_b):
         // symmetric Jacobian in m, and the strain cotangent
-        const double exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
-        const double eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
-        const double B1 = mt.B1c, B2 = mt.B2c;
-        mb.x += -2. * (B1 * exx * hb.x + B2 * exy * hb.y + B2 * exz * hb.z);
-        mb.y += -2. * (B2 * exy * hb.x + B1 * eyy * hb.y + B2 * eyz * hb.z);
-        mb.z += -2. * (B2 * exz * hb.x + B2 * eyz * hb.y + B1 * ezz * hb.z);
-        strbar.c[0][c] = -2. * B1 * m.x * hb.x;
-        strbar.c[1][c] = -2. * B1 * m.y * hb.y;
-        strbar.c[2][c] = -2. * B1 * m.z * hb.z;
-        strbar.c[3][c] = -2. * B2 * (m.z * hb.y + m.y * hb.z);
-        strbar.c[4][c] = -2. * B2 * (m.z * hb.x + m.x * hb.z);
-        strbar.c[5][c] = -2. * B2 * (m.y * hb.x + m.x * hb.y);
+        const R exx = str.c[0][c], eyy = str.c[1][c], ezz = str.c[2][c];
+        const R eyz = str.c[3][c], exz = str.c[4][c], exy = str.c[5][c];
+        const R B1 = mt.B1c, B2 = mt.B2c;
+        mb.x += R(-2) * (B1 * exx * hb.x + B2 * exy * hb.y + B2 * exz * hb.z);
+        mb.y += R(-2) * (B2 * exy * hb.x + B1 * eyy * hb.y + B2 * eyz * hb.z);
+        mb.z += R(-2) * (B2 * exz * hb.x + B2 * eyz * hb.y + B1 * ezz * hb.z);
+        strbar.c[0][c] = R(-2) * B1 * m.x * hb.x;
+        strbar.c[1][c] = R(-2) * B1 * m.y * hb.y;
+        strbar.c[2][c] = R(-2) * B1 * m.z * hb.z;
+        strbar.c[3][c] = R(-2) * B2 * (m.z * hb.y + m.y * hb.z);
+        strbar.c[4][c] = R(-2) * B2 * (m.z * hb.x + m.x * hb.z);
+        strbar.c[5][c] = R(-2) * B2 * (m.y * hb.x + m.x * hb.y);
     }
     st3(ybar, c, mb);
     st3(hbar, c, hb);
@@ -220,21 +248,22 @@ static __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t*
 // lamacc_v += md ukv (k_v reads the step value v_x); the stage-1 force
 // collects -sd w ukv of the later stages (f0bar) and, at stage 1, the
 // cotangent phi of the next step's fs; phi_new = -sd ukv (stage 1 reads fs).
-template <int S>
-__global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __restrict__ mid, const DevMat* __restrict__ mats,
-                                                   F3 uku, F3 ukv, F3 ybar_v, F3 fbar, F3 lamacc_v, F3 f0bar, F3 phi,
-                                                   F3 phi_new) {
+template <int S, class R>
+__global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __restrict__ mid, const DevMatT<R>* __restrict__ mats,
+                                                   F3T<R> uku, F3T<R> ukv, F3T<R> ybar_v, F3T<R> fbar, F3T<R> lamacc_v,
+                                                   F3T<R> f0bar, F3T<R> phi, F3T<R> phi_new) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
+    const R dt = is_mixed<R>::value ? R(P.f.dt) : R(P.dt);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        ybar_v.c[a][c] = P.dt * uku.c[a][c];
-        double fb = 0., pn = 0.;
+        ybar_v.c[a][c] = dt * uku.c[a][c];
+        R fb = R(0), pn = R(0);
         if (id != 0) {
-            const DevMat& mt = mats[id - 1];
-            const double w = (S == 1 || S == 2) ? 2. : 1.;
-            const double g = ukv.c[a][c];
+            const DevMatT<R>& mt = mats[id - 1];
+            const R w = (S == 1 || S == 2) ? R(2) : R(1);
+            const R g = ukv.c[a][c];
             fb = (mt.dens_dt + mt.stiff_damp * w) * g;
             lamacc_v.c[a][c] += mt.mass_damp * g;
             if (S > 0) f0bar.c[a][c] += -mt.stiff_damp * w * g;
@@ -262,22 +291,23 @@ __global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __r
 // The eigenstrain cotangent -st (x2 for shears) goes through the
 // magnetostriction e0_aa = 1.5 l100 (m_a^2 - 1/3), e0_ab = 1.5 l111 m_a m_b
 // into ybar_m (back: the run feeds the eigenstrain back).
-static __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __restrict__ mid, const DevMat* __restrict__ mats,
-                                                        F3 fbar, C6 strbar, F3 m, F3 ybar_m, int back, double* __restrict__ to) {
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __restrict__ mid, const DevMatT<R>* __restrict__ mats,
+                                                  F3T<R> fbar, C6T<R> strbar, F3T<R> m, F3T<R> ybar_m, int back, R* __restrict__ to) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long n = P.n;
-    double T[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, O[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    R T[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, O[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     const uint8_t id = mid[c];
     if (id != 0) {
-        const DevMat& mt = mats[id - 1];
+        const DevMatT<R>& mt = mats[id - 1];
         const int nyz = P.ny * P.nz;
         const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
         const int pos[3] = {i, j, k}, nn[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
         const int stride[3] = {nyz, P.nz, 1};
-        const double rh[3] = {P.rdx, P.rdy, P.rdz};
-        double d0b[6] = {0, 0, 0, 0, 0, 0};
-        const double fx[3] = {fbar.c[0][c], fbar.c[1][c], fbar.c[2][c]};
+        const R rh[3] = {R(P.rdx), R(P.rdy), R(P.rdz)};
+        R d0b[6] = {0, 0, 0, 0, 0, 0};
+        const R fx[3] = {fbar.c[0][c], fbar.c[1][c], fbar.c[2][c]};
         for (int D = 0; D < 3; D++) {
             for (int side = 0; side < 2; side++) {
                 const bool edge = side == 0 ? pos[D] == 0 : pos[D] == nn[D] - 1;
@@ -286,55 +316,55 @@ static __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_
                 q = q < 0 ? q + nn[D] : (q >= nn[D] ? q - nn[D] : q);
                 const int y = c + (q - pos[D]) * stride[D];
                 if (mid[y] == 0) continue;
-                const double fy_[3] = {fbar.c[0][y], fbar.c[1][y], fbar.c[2][y]};
-                double S_[3];
+                const R fy_[3] = {fbar.c[0][y], fbar.c[1][y], fbar.c[2][y]};
+                R S_[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
-                    const double lo = side == 0 ? fy_[r] : fx[r], up = side == 0 ? fx[r] : fy_[r];
-                    S_[r] = 0.5 * (lo - up) * rh[D];
+                    const R lo = side == 0 ? fy_[r] : fx[r], up = side == 0 ? fx[r] : fy_[r];
+                    S_[r] = R(0.5) * (lo - up) * rh[D];
                 }
-                double st[6];
+                R st[6];
 #pragma unroll
                 for (int qv = 0; qv < 6; qv++)
                     st[qv] = mt.cij[face_row(D, 0)][qv] * S_[0] + mt.cij[face_row(D, 1)][qv] * S_[1]
                              + mt.cij[face_row(D, 2)][qv] * S_[2];
-                double* o = O[2 * D + side];
+                R* o = O[2 * D + side];
                 if (D == 0) {
                     o[0] += st[0]; o[2] += st[4]; o[1] += st[5];
-                    T[1][1] += 0.5 * st[1]; T[2][2] += 0.5 * st[2];
-                    T[2][1] += 0.5 * st[3]; T[1][2] += 0.5 * st[3];
-                    T[2][0] += 0.5 * st[4]; T[1][0] += 0.5 * st[5];
+                    T[1][1] += R(0.5) * st[1]; T[2][2] += R(0.5) * st[2];
+                    T[2][1] += R(0.5) * st[3]; T[1][2] += R(0.5) * st[3];
+                    T[2][0] += R(0.5) * st[4]; T[1][0] += R(0.5) * st[5];
                 } else if (D == 1) {
                     o[1] += st[1]; o[2] += st[3]; o[0] += st[5];
-                    T[0][0] += 0.5 * st[0]; T[2][2] += 0.5 * st[2];
-                    T[2][1] += 0.5 * st[3];
-                    T[2][0] += 0.5 * st[4]; T[0][2] += 0.5 * st[4];
-                    T[0][1] += 0.5 * st[5];
+                    T[0][0] += R(0.5) * st[0]; T[2][2] += R(0.5) * st[2];
+                    T[2][1] += R(0.5) * st[3];
+                    T[2][0] += R(0.5) * st[4]; T[0][2] += R(0.5) * st[4];
+                    T[0][1] += R(0.5) * st[5];
                 } else {
                     o[2] += st[2]; o[1] += st[3]; o[0] += st[4];
-                    T[0][0] += 0.5 * st[0]; T[1][1] += 0.5 * st[1];
-                    T[1][2] += 0.5 * st[3]; T[0][2] += 0.5 * st[4];
-                    T[1][0] += 0.5 * st[5]; T[0][1] += 0.5 * st[5];
+                    T[0][0] += R(0.5) * st[0]; T[1][1] += R(0.5) * st[1];
+                    T[1][2] += R(0.5) * st[3]; T[0][2] += R(0.5) * st[4];
+                    T[1][0] += R(0.5) * st[5]; T[0][1] += R(0.5) * st[5];
                 }
                 d0b[0] -= st[0]; d0b[1] -= st[1]; d0b[2] -= st[2];
-                d0b[3] -= 2. * st[3]; d0b[4] -= 2. * st[4]; d0b[5] -= 2. * st[5];
+                d0b[3] -= R(2) * st[3]; d0b[4] -= R(2) * st[4]; d0b[5] -= R(2) * st[5];
             }
         }
         if (strbar.c[0]) {
             // cell strain of the LLG: e_aa = (gm + gp)(a, a) / 2, shears / 4
-            const double e0_ = strbar.c[0][c], e1 = strbar.c[1][c], e2 = strbar.c[2][c];
-            const double e3 = strbar.c[3][c], e4 = strbar.c[4][c], e5 = strbar.c[5][c];
-            T[0][0] += 0.5 * e0_; T[1][1] += 0.5 * e1; T[2][2] += 0.5 * e2;
-            T[2][1] += 0.25 * e3; T[1][2] += 0.25 * e3;
-            T[2][0] += 0.25 * e4; T[0][2] += 0.25 * e4;
-            T[1][0] += 0.25 * e5; T[0][1] += 0.25 * e5;
+            const R e0_ = strbar.c[0][c], e1 = strbar.c[1][c], e2 = strbar.c[2][c];
+            const R e3 = strbar.c[3][c], e4 = strbar.c[4][c], e5 = strbar.c[5][c];
+            T[0][0] += R(0.5) * e0_; T[1][1] += R(0.5) * e1; T[2][2] += R(0.5) * e2;
+            T[2][1] += R(0.25) * e3; T[1][2] += R(0.25) * e3;
+            T[2][0] += R(0.25) * e4; T[0][2] += R(0.25) * e4;
+            T[1][0] += R(0.25) * e5; T[0][1] += R(0.25) * e5;
         }
         if (back) {
-            const double mx = m.c[0][c], my = m.c[1][c], mz = m.c[2][c];
-            const double l1 = mt.l100_15, l2 = mt.l111_15;
-            ybar_m.c[0][c] += 2. * l1 * mx * d0b[0] + l2 * (mz * d0b[4] + my * d0b[5]);
-            ybar_m.c[1][c] += 2. * l1 * my * d0b[1] + l2 * (mz * d0b[3] + mx * d0b[5]);
-            ybar_m.c[2][c] += 2. * l1 * mz * d0b[2] + l2 * (my * d0b[3] + mx * d0b[4]);
+            const R mx = m.c[0][c], my = m.c[1][c], mz = m.c[2][c];
+            const R l1 = mt.l100_15, l2 = mt.l111_15;
+            ybar_m.c[0][c] += R(2) * l1 * mx * d0b[0] + l2 * (mz * d0b[4] + my * d0b[5]);
+            ybar_m.c[1][c] += R(2) * l1 * my * d0b[1] + l2 * (mz * d0b[3] + mx * d0b[5]);
+            ybar_m.c[2][c] += R(2) * l1 * mz * d0b[2] + l2 * (my * d0b[3] + mx * d0b[4]);
         }
     }
 #pragma unroll
@@ -351,19 +381,20 @@ static __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_
 // not stress-free (T of the two cells plus O of each side), then
 // ubar_a(c) = sum_d (gbar_d(lower face) - gbar_d(upper face)) / h_d
 // (g = (u(upper cell) - u(lower cell)) / h).  Written to ybar_u.
-static __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_t* __restrict__ mid, const double* __restrict__ to,
-                                                        F3 ybar_u) {
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_t* __restrict__ mid, const R* __restrict__ to,
+                                                  F3T<R> ybar_u) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long n = P.n;
-    double ub[3] = {0., 0., 0.};
+    R ub[3] = {R(0), R(0), R(0)};
     const uint8_t id = mid[c];
     if (id != 0) {
         const int nyz = P.ny * P.nz;
         const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
         const int pos[3] = {i, j, k}, nn[3] = {P.nx, P.ny, P.nz}, per[3] = {P.per_x, P.per_y, P.per_z};
         const int stride[3] = {nyz, P.nz, 1};
-        const double rh[3] = {P.rdx, P.rdy, P.rdz};
+        const R rh[3] = {R(P.rdx), R(P.rdy), R(P.rdz)};
         for (int d = 0; d < 3; d++) {
             const int qa = pos[d] == 0 ? nn[d] - 1 : pos[d] - 1, qb = pos[d] == nn[d] - 1 ? 0 : pos[d] + 1;
             const int a_ = c + (qa - pos[d]) * stride[d], b_ = c + (qb - pos[d]) * stride[d];
@@ -372,7 +403,7 @@ static __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_
 #pragma unroll
             for (int comp = 0; comp < 3; comp++) {
                 const int tq = (d * 3 + comp);
-                double gl = 0., gu = 0.;
+                R gl = R(0), gu = R(0);
                 if (!free_lo) gl = to[tq * n + a_] + to[tq * n + c] + to[(9 + (2 * d + 1) * 3 + comp) * n + a_]
                                    + to[(9 + (2 * d) * 3 + comp) * n + c];
                 if (!free_hi) gu = to[tq * n + c] + to[tq * n + b_] + to[(9 + (2 * d + 1) * 3 + comp) * n + c]
@@ -388,25 +419,28 @@ static __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_
 // Liao extrapolation after the step (forward): the history slot of this
 // step takes planes k = 1..4 of the step-start u, and u_new(k = 0) =
 // c1 u(1) - c2 u_{-1}(2) + c3 u_{-2}(3) - w u_{-3}(4) (k_elastic_bc's form)
-static __global__ void k_adj_liao(Params P, F3 ux, F3 unew, double* __restrict__ hist, double* __restrict__ last,
-                                 unsigned long long step) {
+template <class R>
+__global__ void k_adj_liao(Params P, F3T<R> ux, F3T<R> unew, F3T<R> ucmp, R* __restrict__ hist, R* __restrict__ last,
+                           unsigned long long step) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long plane = (long)P.nx * P.ny;
     if (t >= plane) return;
     const long i = t / P.ny, j = t - i * P.ny;
-    const double w = P.liao_w;
-    const double c1 = 4. * w + 2. * (1. - w), c2 = 6. * w + (1. - w), c3 = 4. * w;
-    double* slot = hist + (size_t)(step & 3ull) * 12 * plane;
-    const double* h2 = hist + (size_t)((step + 3) & 3ull) * 12 * plane;
-    const double* h3 = hist + (size_t)((step + 2) & 3ull) * 12 * plane;
-    const double* h4 = hist + (size_t)((step + 1) & 3ull) * 12 * plane;
+    const double wd = P.liao_w;
+    const R w = R(wd);
+    const R c1 = R(4. * wd + 2. * (1. - wd)), c2 = R(6. * wd + (1. - wd)), c3 = R(4. * wd);
+    R* slot = hist + (size_t)(step & 3ull) * 12 * plane;
+    const R* h2 = hist + (size_t)((step + 3) & 3ull) * 12 * plane;
+    const R* h3 = hist + (size_t)((step + 2) & 3ull) * 12 * plane;
+    const R* h4 = hist + (size_t)((step + 1) & 3ull) * 12 * plane;
     for (int a = 0; a < 3; a++) {
-        double uv[4];
+        R uv[4];
         for (int p = 1; p <= 4; p++) uv[p - 1] = ux.c[a][cid(P, i, j, p)];
-        const double t2 = h2[(a * 4 + 1) * plane + t], t3 = h3[(a * 4 + 2) * plane + t], t4 = h4[(a * 4 + 3) * plane + t];
+        const R t2 = h2[(a * 4 + 1) * plane + t], t3 = h3[(a * 4 + 2) * plane + t], t4 = h4[(a * 4 + 3) * plane + t];
         for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = uv[p - 1];
-        const double v = c1 * uv[0] - c2 * t2 + c3 * t3 - w * t4;
+        const R v = c1 * uv[0] - c2 * t2 + c3 * t3 - w * t4;
         unew.c[a][cid(P, i, j, 0)] = v;
+        if (ucmp.c[a]) ucmp.c[a][cid(P, i, j, 0)] = R(0);   // FP32: the value is replaced, not summed
         last[a * plane + t] = v;
     }
 }
@@ -417,20 +451,22 @@ static __global__ void k_adj_liao(Params P, F3 ux, F3 unew, double* __restrict__
 // the step values it came from: c1 L for this step's plane 1, -c2 L, c3 L,
 // -w L for planes 2, 3, 4 of the three earlier steps.  pend: 4 slots (target
 // step mod 4) x 3 components x planes k = 1..4.
-static __global__ void k_adj_liao_T(Params P, F3 lam, double* __restrict__ pend, unsigned long long step) {
+template <class R>
+__global__ void k_adj_liao_T(Params P, F3T<R> lam, R* __restrict__ pend, unsigned long long step) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long plane = (long)P.nx * P.ny;
     if (t >= plane) return;
     const long i = t / P.ny, j = t - i * P.ny;
-    const double w = P.liao_w;
-    const double c1 = 4. * w + 2. * (1. - w), c2 = 6. * w + (1. - w), c3 = 4. * w;
-    auto at = [&](unsigned long long target, int a, int p) -> double& {
+    const double wd = P.liao_w;
+    const R w = R(wd);
+    const R c1 = R(4. * wd + 2. * (1. - wd)), c2 = R(6. * wd + (1. - wd)), c3 = R(4. * wd);
+    auto at = [&](unsigned long long target, int a, int p) -> R& {
         return pend[((size_t)((target & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
     };
     for (int a = 0; a < 3; a++) {
         const long b0 = cid(P, i, j, 0);
-        const double L = lam.c[a][b0];
-        lam.c[a][b0] = 0.;
+        const R L = lam.c[a][b0];
+        lam.c[a][b0] = R(0);
         at(step, a, 1) += c1 * L;
         if (step >= 1) at(step - 1, a, 2) += -c2 * L;
         if (step >= 2) at(step - 2, a, 3) += c3 * L;
@@ -440,53 +476,56 @@ static __global__ void k_adj_liao_T(Params P, F3 lam, double* __restrict__ pend,
 
 // after a step's reverse sweep: the parked Liao cotangents of its step value
 // (planes 1..4) join lambda, and the slot is cleared for reuse
-static __global__ void k_adj_liao_pend(Params P, F3 lam, double* __restrict__ pend, unsigned long long step) {
+template <class R>
+__global__ void k_adj_liao_pend(Params P, F3T<R> lam, R* __restrict__ pend, unsigned long long step) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long plane = (long)P.nx * P.ny;
     if (t >= plane) return;
     const long i = t / P.ny, j = t - i * P.ny;
     for (int a = 0; a < 3; a++)
         for (int p = 1; p <= 4; p++) {
-            double& v = pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
+            R& v = pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
             lam.c[a][cid(P, i, j, p)] += v;
-            v = 0.;
+            v = R(0);
         }
 }
 
 // ybar += transposed exchange of Hbar: sum_f w_cf (ex_f Hbar_f - ex_c Hbar_c);
 // and ybar += Ms R where R is the demag convolution of Hbar (3 x n, the
 // inverse-transform output), for ferromagnetic cells
-static __global__ void __launch_bounds__(256) k_adj_field_T(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am,
-                                                     const double* __restrict__ aij, int nmat, F3 hbar,
-                                                     const double* __restrict__ R, F3 ybar) {
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_field_T(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
+                                                     const R* __restrict__ aij, int nmat, F3T<R> hbar, const R* __restrict__ Rk,
+                                                     F3T<R> ybar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
     if (!(id != 0 && am[id - 1].fm)) return;
     const int nyz = P.ny * P.nz;
     const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
-    AdjNbr n;
+    AdjNbr<R> n;
     adj_neighbours(P, mid, am, aij, nmat, i, j, k, id, n);
-    const double ec = am[id - 1].ex_coef, Ms = am[id - 1].Ms;
-    const double3 hc = ld3(hbar, c);
-    double3 s = make_double3(0., 0., 0.);
+    const R ec = am[id - 1].ex_coef, Ms = am[id - 1].Ms;
+    const V3<R> hc = ld3(hbar, c);
+    V3<R> s = mk3<R>(R(0), R(0), R(0));
 #pragma unroll
     for (int f = 0; f < 6; f++) {
-        if (n.w[f] == 0.) continue;
-        const double ef = am[mid[n.nb[f]] - 1].ex_coef;
-        const double3 hf = ld3(hbar, n.nb[f]);
+        if (n.w[f] == R(0)) continue;
+        const R ef = am[mid[n.nb[f]] - 1].ex_coef;
+        const V3<R> hf = ld3(hbar, n.nb[f]);
         s.x += n.w[f] * (ef * hf.x - ec * hc.x);
         s.y += n.w[f] * (ef * hf.y - ec * hc.y);
         s.z += n.w[f] * (ef * hf.z - ec * hc.z);
     }
-    double3 yb = ld3(ybar, c);
+    V3<R> yb = ld3(ybar, c);
     yb.x += s.x; yb.y += s.y; yb.z += s.z;
-    if (R) { yb.x += Ms * R[c]; yb.y += Ms * R[P.n + c]; yb.z += Ms * R[2 * P.n + c]; }
+    if (Rk) { yb.x += Ms * Rk[c]; yb.y += Ms * Rk[P.n + c]; yb.z += Ms * Rk[2 * P.n + c]; }
     st3(ybar, c, yb);
 }
 
 // Hbar (3 x n arrays) into the contiguous FFT input
-static __global__ void k_adj_pack(Params P, F3 v, double* out) {
+template <class R>
+__global__ void k_adj_pack(Params P, F3T<R> v, R* out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     out[c] = v.c[0][c]; out[P.n + c] = v.c[1][c]; out[2 * P.n + c] = v.c[2][c];
@@ -494,34 +533,36 @@ static __global__ void k_adj_pack(Params P, F3 v, double* out) {
 
 // RK4 reverse sweep after the VJP of stage S (0-based): lamacc += ybar and the
 // cotangent of the next (earlier) stage's increment
-template <int S>
-__global__ void k_adj_comb(Params P, F3 lam, F3 lamacc, F3 u, F3 ybar) {
+template <int S, class R>
+__global__ void k_adj_comb(Params P, F3T<R> lam, F3T<R> lamacc, F3T<R> u, F3T<R> ybar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double yb = ybar.c[a][c], l = lam.c[a][c];
+        const R yb = ybar.c[a][c], l = lam.c[a][c];
         lamacc.c[a][c] = lamacc.c[a][c] + yb;
-        if (S == 3) u.c[a][c] = l / 3. + yb;
-        else if (S == 2) u.c[a][c] = l / 3. + yb * 0.5;
-        else if (S == 1) u.c[a][c] = l / 6. + yb * 0.5;
+        if (S == 3) u.c[a][c] = l / R(3) + yb;
+        else if (S == 2) u.c[a][c] = l / R(3) + yb * R(0.5);
+        else if (S == 1) u.c[a][c] = l / R(6) + yb * R(0.5);
     }
 }
 
 // v *= f (3 x n)
-static __global__ void k_scale_f3(Params P, F3 v, double f) {
+template <class R>
+__global__ void k_scale_f3(Params P, F3T<R> v, R f) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     v.c[0][c] *= f; v.c[1][c] *= f; v.c[2][c] *= f;
 }
 
 // lambda_x += g / NFM on ferromagnetic cells (d loss / d <m_x> of one step)
-static __global__ void k_adj_inject(Params P, const uint8_t* __restrict__ mid, const AdjMat* __restrict__ am, F3 lam,
+template <class R>
+__global__ void k_adj_inject(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am, F3T<R> lam,
                              const double* __restrict__ g, long slot, double inv_nfm) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
-    if (id != 0 && am[id - 1].fm) lam.c[0][c] = lam.c[0][c] + g[slot] * inv_nfm;
+    if (id != 0 && am[id - 1].fm) lam.c[0][c] = lam.c[0][c] + R(g[slot] * inv_nfm);
 }
 
 // out[slot] += in[0] (single thread; waveform gradient of one stage)

@@ -197,6 +197,7 @@ int gf_mixed_enqueue_step(gf_engine* eng, int parity);                 // kernel
 int gf_mixed_enqueue_stage(gf_engine* eng, int parity, int s);         // kernels of stage s (0..3), mixed form
 int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-memory opt-in, occupancy
 int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms);          // stage-1 elastic tile, mean ms per launch
+int gf_mixed_adj_elastic(gf_engine* eng, int s, int rk, const StageIOT<float>& io);  // adjoint: FP32 elastic tile / RK of stage s
 
 namespace {
 
@@ -1151,6 +1152,40 @@ int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm) {
 }
 
 int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms) { return time_tile_t<float>(eng, reps, ms); }
+
+// the FP32 elastic tile (rk = 0) or RK update (rk = 1) of stage s on the
+// discrete adjoint's buffers (io built by the adjoint), with the engine's
+// launch shapes; the tile stages by cp.async (no tensor maps over the
+// adjoint's buffers)
+namespace {
+template <int S>
+int adj_elastic_f32(gf_engine* eng, int rk, const StageIOT<float>& io) {
+    const Params& P = eng->P;
+    if (rk) {
+        GF_CU(launch(k_elastic_rk<S, float>, dim3(blocks_for(P.n, 2 * kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+        return GF_OK;
+    }
+    ETileMaps tm;
+    std::memset(&tm, 0, sizeof(tm));
+    tm.err = eng->tma_err;
+    const dim3 grid((P.nz + etile::TK - 1) / etile::TK, (P.ny + etile::TJ - 1) / etile::TJ,
+                    (P.nx + eng->el_chunk - 1) / eng->el_chunk);
+    if (eng->el_cubic)
+        GF_CU(launch_tiled(k_elastic_tile<S, true, float>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                           eng->el_chunk, eng->el_nmat, tm));
+    else
+        GF_CU(launch_tiled(k_elastic_tile<S, false, float>, grid, dim3(etile::NT), eng->el_smem, eng->stream, P, io,
+                           eng->el_chunk, eng->el_nmat, tm));
+    return GF_OK;
+}
+}  // namespace
+
+int gf_mixed_adj_elastic(gf_engine* eng, int s, int rk, const StageIOT<float>& io) {
+    if (s == 0) return adj_elastic_f32<0>(eng, rk, io);
+    if (s == 1) return adj_elastic_f32<1>(eng, rk, io);
+    if (s == 2) return adj_elastic_f32<2>(eng, rk, io);
+    return adj_elastic_f32<3>(eng, rk, io);
+}
 #else
 namespace {
 
@@ -3125,21 +3160,30 @@ struct gf_adjoint {
     int nw = 0, ck_every = 0, nmat = 0;
     uint64_t nsteps = 0;
     bool ran = false;
+    // on a mixed-form engine the adjoint's fields are FP32 (R = float), the
+    // step values carry compensation words, and the gradients, the <m_x>
+    // trace and its cotangent stay FP64; every buffer below except abar,
+    // wbar, trace and dldm holds elements of esz bytes
+    bool f32 = false;
+    size_t esz = sizeof(double);
     std::vector<void*> allocs;
-    AdjMat* am = nullptr;
+    void* am = nullptr;              // AdjMatT<R> per material
     double* aij = nullptr;           // (nmat+1)^2 harmonic-mean exchange constants
     double* alpha = nullptr;         // per cell
     std::vector<double> wave;        // excitation samples (A/m, x)
     std::vector<double> hext;        // nsteps x 4 x 3 external field of the deck per stage
     // state of a step: m (0-2); with elastodynamics also u (3-5), v (6-8)
-    // and the stiffness-damping force store fs (9-11)
+    // and the stiffness-damping force store fs (9-11); in FP32 also the
+    // compensation words of m (12-14), u (15-17) and v (18-20)
     bool el = false;
-    int ns = 3;
-    double* X[12] = {};              // step value
+    int ns = 3;                      // components stored per step
+    int sidx[21] = {};               // their indices in X
+    double* X[21] = {};              // step value
     double* Y[3][3] = {};            // stage states y2, y3, y4 (m)
     double* ACC[3] = {};
     double* HS[4][3] = {};           // effective field of each stage
     double* XJ[3] = {};              // stage-4 output of a recomputed step (discarded)
+    double* XJC[3] = {};             // and its compensation words (FP32)
     // cotangents: m (0-2), u (3-5), v (6-8)
     double* LAM[9] = {}; double* LAMACC[9] = {}; double* U[9] = {};
     double* YBAR[9] = {}; double* HBAR[3] = {};
@@ -3158,79 +3202,160 @@ struct gf_adjoint {
     double* hist = nullptr;          // 4 slots x 12 planes (k_elastic_bc's layout)
     double* last = nullptr;          // 3 planes
     double* pend = nullptr;          // 4 slots x 3 components x 4 planes
-    double* trace = nullptr;         // nsteps+1
-    double* dldm = nullptr;          // nsteps+1
+    double* trace = nullptr;         // nsteps+1 (FP64)
+    double* dldm = nullptr;          // nsteps+1 (FP64)
     double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x ck_len
     double* xs = nullptr;            // step values of one block, ck_every x ns n
     double* zero3 = nullptr;         // 3n zeros (demag field when magnetostatics is off)
+    double* wide = nullptr;          // FP32: 3n FP64 values of the final m
     size_t ck_slots = 0;
     size_t ck_len = 0;               // ns n (+ 51 planes of Liao state with elastodynamics)
 };
 
 namespace {
 
-// zeroed device buffer, complete on return (host copies may follow at once)
-int adj_alloc(gf_adjoint* a, double** p, size_t count) {
+// zeroed device buffer of `count` elements of `bytes` each, complete on
+// return (host copies may follow at once)
+int adj_alloc_b(gf_adjoint* a, double** p, size_t count, size_t bytes) {
     gf_engine* eng = a->eng;
-    GF_CU(cudaMalloc(p, count * sizeof(double)));
+    GF_CU(cudaMalloc(p, count * bytes));
     a->allocs.push_back(*p);
-    GF_CU(cudaMemsetAsync(*p, 0, count * sizeof(double), eng->stream));
+    GF_CU(cudaMemsetAsync(*p, 0, count * bytes, eng->stream));
     GF_CU(cudaStreamSynchronize(eng->stream));
     return GF_OK;
 }
+// field elements (esz bytes) and FP64 elements
+int adj_alloc(gf_adjoint* a, double** p, size_t count) { return adj_alloc_b(a, p, count, a->esz); }
+int adj_alloc_d(gf_adjoint* a, double** p, size_t count) { return adj_alloc_b(a, p, count, sizeof(double)); }
 
 int adj_alloc3(gf_adjoint* a, double* f[3]) {
     for (int c = 0; c < 3; c++) GF_TRY(adj_alloc(a, &f[c], (size_t)a->eng->P.n));
     return GF_OK;
 }
 
-F3 f3v(double* base, long n) { F3 r; for (int c = 0; c < 3; c++) r.c[c] = base + (size_t)c * n; return r; }
+// `elems` field elements past `base`
+double* adj_at(const gf_adjoint* a, double* base, size_t elems) {
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(base) + elems * a->esz);
+}
+void adj_free(gf_adjoint* a, double** p) {
+    if (!*p) return;
+    cudaFree(*p);
+    a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)*p), a->allocs.end());
+    *p = nullptr;
+}
 
-// demag field of stage state y (3 x n, left in the FFT buffer), or zeros
-int adj_demag(gf_adjoint* a, F3 y, F3& hd) {
+// typed views of the buffers
+template <class R> R* rp(double* p) { return reinterpret_cast<R*>(p); }
+template <class R> F3T<R> v3(double* const* p) { F3T<R> r; for (int c = 0; c < 3; c++) r.c[c] = rp<R>(p[c]); return r; }
+template <class R> F3T<R> v3c(R* base, long n) { F3T<R> r; for (int c = 0; c < 3; c++) r.c[c] = base + (size_t)c * n; return r; }
+template <class R> const DevMatT<R>* adj_mats(const gf_engine* eng) {
+    if constexpr (is_mixed<R>::value) return eng->mats_f;
+    else return eng->mats;
+}
+template <class R> StageIOT<R> adj_base_io(const gf_engine* eng) {
+    if constexpr (is_mixed<R>::value) return eng->iof[0][0];
+    else return eng->io[0][0];
+}
+
+// demag field of stage state y (3 x n, left in the FFT buffer), or zeros;
+// FP32: the mixed engine's R2C / six-spectra / C2R path
+template <class R>
+int adj_demag(gf_adjoint* a, F3T<R> y, F3T<R>& hd) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
-    if (eng->demag_mode != 0) { hd = f3v(a->zero3, P.n); return GF_OK; }
+    if (eng->demag_mode != 0) { hd = v3c<R>(rp<R>(a->zero3), P.n); return GF_OK; }
     cudaStream_t st = eng->stream;
-    GF_CU(launch(k_mag_source, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats,
-                 (const uint8_t*)eng->mid, y, F3{}, F3{}, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
-    GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
     const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
-    GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
-                 (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
-    GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
-    hd = f3v(eng->Mfft, P.n);
+    if constexpr (is_mixed<R>::value) {
+        float* M3 = reinterpret_cast<float*>(eng->Mfft);
+        cufftComplex* Mk = reinterpret_cast<cufftComplex*>(eng->Mk);
+        GF_CU(launch(k_mag_source_f32, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, st, P, (const DevMatT<float>*)eng->mats_f,
+                     (const uint8_t*)eng->mid, y, F3T<float>{}, F3T<float>{}, 0, M3, f3f(eng->Hstat), 0.f, 0.f, 0.f));
+        GF_FFT(cufftExecR2C(eng->plan_r2c, M3, Mk));
+        const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
+        GF_CU(launch(k_demag_mul_f32, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, inv_vol_neg,
+                     (const cuComplex*)Mk, (const float*)eng->Nr, (cuComplex*)Mk));
+        GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));
+        hd = v3c<float>(M3, P.n);
+    } else {
+        GF_CU(launch(k_mag_source, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, st, P, (const DevMat*)eng->mats,
+                     (const uint8_t*)eng->mid, y, F3{}, F3{}, 0, eng->Mfft, f3(eng->Hstat), 0., 0., 0.));
+        GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+        GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
+                     (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+        GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+        hd = v3c<double>(eng->Mfft, P.n);
+    }
     return GF_OK;
 }
 
-double3 adj_hext(const gf_adjoint* a, uint64_t step, int s) {
-    const double* h = &a->hext[(size_t)(step * 4 + s) * 3];
-    const size_t seg = (size_t)((step * (uint64_t)a->nw) / a->nsteps);
-    return make_double3(h[0] + a->wave[seg], h[1], h[2]);
+// the transposed convolution of Hbar (the operator is symmetric: the same
+// transform pair and spectra), result 3 x n in the FFT buffer
+template <class R>
+int adj_demag_T(gf_adjoint* a, const R*& out) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    cudaStream_t st = eng->stream;
+    const unsigned bn = blocks_for(P.n, kThreads);
+    const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
+    R* M3 = reinterpret_cast<R*>(eng->Mfft);
+    GF_CU(launch(k_adj_pack<R>, dim3(bn), dim3(kThreads), 0, st, P, v3<R>(a->HBAR), M3));
+    if constexpr (is_mixed<R>::value) {
+        cufftComplex* Mk = reinterpret_cast<cufftComplex*>(eng->Mk);
+        GF_FFT(cufftExecR2C(eng->plan_r2c, M3, Mk));
+        const float inv_vol_neg = (float)(-1. / (P.dx * P.dy * P.dz));
+        GF_CU(launch(k_demag_mul_f32, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, inv_vol_neg,
+                     (const cuComplex*)Mk, (const float*)eng->Nr, (cuComplex*)Mk));
+        GF_FFT(cufftExecC2R(eng->plan_c2r, Mk, M3));
+    } else {
+        GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
+        GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
+                     (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
+        GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
+    }
+    out = M3;
+    return GF_OK;
 }
 
-// StageIO over the adjoint's buffers for the engine's elastic kernels: stage
+template <class R>
+V3<R> adj_hext(const gf_adjoint* a, uint64_t step, int s) {
+    const double* h = &a->hext[(size_t)(step * 4 + s) * 3];
+    const size_t seg = (size_t)((step * (uint64_t)a->nw) / a->nsteps);
+    return mk3<R>(R(h[0] + a->wave[seg]), R(h[1]), R(h[2]));
+}
+
+// StageIOT over the adjoint's buffers for the engine's elastic kernels: stage
 // m and u in, the force and the stage strain out; for k_elastic_rk the step
-// value (x), the stage v, the accumulators and the next stage's u, v
-StageIO adj_el_io(gf_adjoint* a, double* const* x, F3 ym, F3 yu, F3 yv, int s, F3 uout, F3 vout) {
+// value (x), the stage v, the accumulators and the next stage's u, v (FP32:
+// the step value's compensation words, which the last stage updates in place)
+template <class R>
+StageIOT<R> adj_el_io(gf_adjoint* a, double* const* x, F3T<R> ym, F3T<R> yu, F3T<R> yv, int s, F3T<R> uout, F3T<R> vout) {
     gf_engine* eng = a->eng;
-    StageIO io = eng->io[0][0];          // tables, drive and materials of the engine
+    StageIOT<R> io = adj_base_io<R>(eng);     // tables, drive and materials of the engine
     io.m_in = ym;
     io.u_in = yu; io.v_in = yv;
-    io.u_x = F3{{x[3], x[4], x[5]}}; io.v_x = F3{{x[6], x[7], x[8]}};
-    io.u_acc = f3(a->UACC); io.v_acc = f3(a->VACC);
+    io.u_x = v3<R>(x + 3); io.v_x = v3<R>(x + 6);
+    io.u_acc = v3<R>(a->UACC); io.v_acc = v3<R>(a->VACC);
     io.u_out = uout; io.v_out = vout;
-    io.force = f3(a->FORCE);
-    io.force_store = F3{{x[9], x[10], x[11]}};
-    for (int q = 0; q < 6; q++) { io.strain_c[q] = a->STR[s][q]; io.eps0_c[q] = nullptr; io.eig0_c[q] = nullptr;
+    io.force = v3<R>(a->FORCE);
+    io.force_store = v3<R>(x + 9);
+    if (a->f32) { io.u_cmp = v3<R>(x + 15); io.v_cmp = v3<R>(x + 18); }
+    for (int q = 0; q < 6; q++) { io.strain_c[q] = rp<R>(a->STR[s][q]); io.eps0_c[q] = nullptr; io.eig0_c[q] = nullptr;
                                   io.sg[q] = nullptr; io.pge[q] = nullptr; }
     return io;
 }
 
+// the engine's elastic tile (rk = 0) or RK update (rk = 1) of stage S on the
+// adjoint's buffers; FP32 through the mixed translation unit, so that the
+// adjoint's forward run is the mixed engine's own elastic discretisation
 template <int S>
-int adj_el_stage(gf_adjoint* a, const StageIO& io) {
+int adj_el_kernel(gf_adjoint* a, int rk, const StageIOT<double>& io) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
+    if (rk) {
+        GF_CU(launch(k_elastic_rk<S, double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+        return GF_OK;
+    }
     ETileMaps tm;
     std::memset(&tm, 0, sizeof(tm));
     tm.err = eng->tma_err;
@@ -3244,69 +3369,73 @@ int adj_el_stage(gf_adjoint* a, const StageIO& io) {
                            eng->el_chunk, eng->el_nmat, tm));
     return GF_OK;
 }
-
-template <int S>
-int adj_el_rk(gf_adjoint* a, const StageIO& io) {
-    gf_engine* eng = a->eng;
-    GF_CU(launch(k_elastic_rk<S, double>, dim3(blocks_for(eng->P.n, kThreads)), dim3(kThreads), 0, eng->stream, eng->P, io));
-    return GF_OK;
+template <class R>
+int adj_el(gf_adjoint* a, int s, int rk, const StageIOT<R>& io) {
+    if constexpr (is_mixed<R>::value) {
+        return gf_mixed_adj_elastic(a->eng, s, rk, io);
+    } else {
+        if (s == 0) return adj_el_kernel<0>(a, rk, io);
+        if (s == 1) return adj_el_kernel<1>(a, rk, io);
+        if (s == 2) return adj_el_kernel<2>(a, rk, io);
+        return adj_el_kernel<3>(a, rk, io);
+    }
 }
 
-// stages of step `step` from step value x (ns components): the effective
-// fields go to HS, the stage states to Y (m) and US / VS (u, v), the stage
-// strains to STR; stage 4 writes m to xout (x itself in the forward run) and
-// leaves the new u, v in UACC / VACC.  The elastic parts run the engine's
-// own k_elastic_tile and k_elastic_rk (so the forward run is the engine's
-// discretisation); k_elastic_rk of stage 1 stores the step's stage-1 force
-// in x's fs.
-int adj_stages(gf_adjoint* a, double* const* x, uint64_t step, F3 xout) {
+template <int S, class R>
+cudaError_t adj_eval_launch(gf_adjoint* a, F3T<R> y, F3T<R> hd, V3<R> he, F3T<R> hs, F3T<R> xs_, F3T<R> xc, F3T<R> acc,
+                            F3T<R> ynext, C6T<R> str) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
-    cudaStream_t st = eng->stream;
-    const unsigned bn = blocks_for(P.n, kThreads);
-    F3 acc = f3(a->ACC);
-    F3 xm{{x[0], x[1], x[2]}};
-    F3 y = xm, yu{}, yv{};
-    if (a->el) { yu = F3{{x[3], x[4], x[5]}}; yv = F3{{x[6], x[7], x[8]}}; }
+    return launch(k_adj_eval<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, (const uint8_t*)eng->mid,
+                  (const AdjMatT<R>*)a->am, (const R*)rp<R>(a->aij), a->nmat, y, hd, (const R*)rp<R>(a->alpha), he, hs, xs_, xc,
+                  acc, ynext, str);
+}
+
+// stages of step `step` from step value x: the effective fields go to HS,
+// the stage states to Y (m) and US / VS (u, v), the stage strains to STR;
+// stage 4 writes m to xout (compensation words to xcout in FP32; x itself in
+// the forward run) and leaves the new u, v in UACC / VACC.  The elastic
+// parts run the engine's own k_elastic_tile and k_elastic_rk (so the forward
+// run is the engine's discretisation); k_elastic_rk of stage 1 stores the
+// step's stage-1 force in x's fs.
+template <class R>
+int adj_stages(gf_adjoint* a, double* const* x, uint64_t step, F3T<R> xout, F3T<R> xcout) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    F3T<R> acc = v3<R>(a->ACC);
+    F3T<R> xm = v3<R>(x);
+    F3T<R> y = xm, yu{}, yv{};
+    if (a->el) { yu = v3<R>(x + 3); yv = v3<R>(x + 6); }
     for (int s = 0; s < 4; s++) {
-        F3 hd;
-        GF_TRY(adj_demag(a, y, hd));
-        C6 str{};
+        F3T<R> hd;
+        GF_TRY(adj_demag<R>(a, y, hd));
+        C6T<R> str{};
         if (a->el) {
-            const StageIO io = adj_el_io(a, x, y, yu, yv, s, F3{}, F3{});
-            if (s == 0) GF_TRY(adj_el_stage<0>(a, io));
-            else if (s == 1) GF_TRY(adj_el_stage<1>(a, io));
-            else if (s == 2) GF_TRY(adj_el_stage<2>(a, io));
-            else GF_TRY(adj_el_stage<3>(a, io));
-            if (P.elasto_on) for (int q = 0; q < 6; q++) str.c[q] = a->STR[s][q];
+            const StageIOT<R> io = adj_el_io<R>(a, x, y, yu, yv, s, F3T<R>{}, F3T<R>{});
+            GF_TRY(adj_el<R>(a, s, 0, io));
+            if (P.elasto_on) for (int q = 0; q < 6; q++) str.c[q] = rp<R>(a->STR[s][q]);
         }
-        const double3 he = adj_hext(a, step, s);
+        const V3<R> he = adj_hext<R>(a, step, s);
         // stage 4 reads the step value from and writes the new one to xout:
         // x itself in the forward run (each thread reads its own cell before
         // writing it); a discarded buffer when a step is recomputed for the
         // reverse sweep, which needs only the stage fields
-        F3 ynext = (s < 3) ? f3(a->Y[s]) : xout;
-        F3 xs_ = (s < 3) ? xm : xout;
+        F3T<R> ynext = (s < 3) ? v3<R>(a->Y[s]) : xout;
+        F3T<R> xs_ = (s < 3) ? xm : xout;
+        const F3T<R> hs = v3<R>(a->HS[s]);
         cudaError_t e;
-        if (s == 0) e = launch(k_adj_eval<0>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                               (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
-        else if (s == 1) e = launch(k_adj_eval<1>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
-        else if (s == 2) e = launch(k_adj_eval<2>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                                    (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
-        else e = launch(k_adj_eval<3>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                        (const double*)a->aij, a->nmat, y, hd, (const double*)a->alpha, he, f3(a->HS[s]), xs_, acc, ynext, str);
+        if (s == 0) e = adj_eval_launch<0, R>(a, y, hd, he, hs, xs_, F3T<R>{}, acc, ynext, str);
+        else if (s == 1) e = adj_eval_launch<1, R>(a, y, hd, he, hs, xs_, F3T<R>{}, acc, ynext, str);
+        else if (s == 2) e = adj_eval_launch<2, R>(a, y, hd, he, hs, xs_, F3T<R>{}, acc, ynext, str);
+        else e = adj_eval_launch<3, R>(a, y, hd, he, hs, xs_, xcout, acc, ynext, str);
         GF_CU(e);
         if (a->el) {
-            const F3 uo = (s < 3) ? f3(a->US[s]) : F3{}, vo = (s < 3) ? f3(a->VS[s]) : F3{};
-            const StageIO io = adj_el_io(a, x, y, yu, yv, s, uo, vo);
-            if (s == 0) GF_TRY(adj_el_rk<0>(a, io));
-            else if (s == 1) GF_TRY(adj_el_rk<1>(a, io));
-            else if (s == 2) GF_TRY(adj_el_rk<2>(a, io));
-            else GF_TRY(adj_el_rk<3>(a, io));
-            if (s < 3) { yu = f3(a->US[s]); yv = f3(a->VS[s]); }
+            const F3T<R> uo = (s < 3) ? v3<R>(a->US[s]) : F3T<R>{}, vo = (s < 3) ? v3<R>(a->VS[s]) : F3T<R>{};
+            const StageIOT<R> io = adj_el_io<R>(a, x, y, yu, yv, s, uo, vo);
+            GF_TRY(adj_el<R>(a, s, 1, io));
+            if (s < 3) { yu = v3<R>(a->US[s]); yv = v3<R>(a->VS[s]); }
         }
-        if (s < 3) y = f3(a->Y[s]);
+        if (s < 3) y = v3<R>(a->Y[s]);
     }
     return GF_OK;
 }
@@ -3314,117 +3443,127 @@ int adj_stages(gf_adjoint* a, double* const* x, uint64_t step, F3 xout) {
 // one forward step in place: m by k_adj_eval<3>, which reads x[c] before
 // writing it in the same thread; then the Liao extrapolation of u(k = 0)
 // and the new u, v from the accumulators
+template <class R>
 int adj_step_forward(gf_adjoint* a, double* const* x, uint64_t step) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
-    GF_TRY(adj_stages(a, x, step, F3{{x[0], x[1], x[2]}}));
+    GF_TRY(adj_stages<R>(a, x, step, v3<R>(x), a->f32 ? v3<R>(x + 12) : F3T<R>{}));
     if (a->el) {
         const long plane = (long)P.nx * P.ny;
-        GF_CU(launch(k_adj_liao, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, eng->stream, P, F3{{x[3], x[4], x[5]}},
-                     f3(a->UACC), a->hist, a->last, (unsigned long long)step));
+        GF_CU(launch(k_adj_liao<R>, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, eng->stream, P, v3<R>(x + 3),
+                     v3<R>(a->UACC), a->f32 ? v3<R>(x + 15) : F3T<R>{}, rp<R>(a->hist), rp<R>(a->last), (unsigned long long)step));
         for (int c = 0; c < 3; c++) {
-            GF_CU(cudaMemcpyAsync(x[3 + c], a->UACC[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, eng->stream));
-            GF_CU(cudaMemcpyAsync(x[6 + c], a->VACC[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, eng->stream));
+            GF_CU(cudaMemcpyAsync(x[3 + c], a->UACC[c], a->esz * P.n, cudaMemcpyDeviceToDevice, eng->stream));
+            GF_CU(cudaMemcpyAsync(x[6 + c], a->VACC[c], a->esz * P.n, cudaMemcpyDeviceToDevice, eng->stream));
         }
     }
     return GF_OK;
 }
 
-int adj_mean_x(gf_adjoint* a, const double* x0, long slot) {
+// FP64 sum of n field elements at `in` into p3 (three deterministic passes)
+int adj_sum(gf_adjoint* a, const double* in, double*& p3) {
     gf_engine* eng = a->eng;
     cudaStream_t st = eng->stream;
     double* p1 = eng->scratch + eng->scratch_main;
     double* p2 = p1 + 8192;
-    double* p3 = p2 + 64;
-    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, x0, (long)eng->P.n, p1, 8192L));
+    p3 = p2 + 64;
+    if (a->f32) GF_CU(launch(k_sum_stride_f, dim3(32), dim3(256), 0, st, reinterpret_cast<const float*>(in), (long)eng->P.n, p1, 8192L));
+    else GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, in, (long)eng->P.n, p1, 8192L));
     GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
     GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
-    GF_CU(launch(k_adj_store_slot, dim3(1), dim3(1), 0, st, a->trace, slot, (const double*)p3, 1. / (double)eng->deck.NFM));
+    return GF_OK;
+}
+
+int adj_mean_x(gf_adjoint* a, const double* x0, long slot) {
+    gf_engine* eng = a->eng;
+    double* p3 = nullptr;
+    GF_TRY(adj_sum(a, x0, p3));
+    GF_CU(launch(k_adj_store_slot, dim3(1), dim3(1), 0, eng->stream, a->trace, slot, (const double*)p3,
+                 1. / (double)eng->deck.NFM));
     return GF_OK;
 }
 
 int adj_wave_add(gf_adjoint* a, long seg) {
     gf_engine* eng = a->eng;
-    cudaStream_t st = eng->stream;
-    double* p1 = eng->scratch + eng->scratch_main;
-    double* p2 = p1 + 8192;
-    double* p3 = p2 + 64;
-    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, (const double*)a->hbx, (long)eng->P.n, p1, 8192L));
-    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
-    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
-    GF_CU(launch(k_adj_add_slot, dim3(1), dim3(1), 0, st, a->wbar, seg, (const double*)p3));
+    double* p3 = nullptr;
+    GF_TRY(adj_sum(a, a->hbx, p3));
+    GF_CU(launch(k_adj_add_slot, dim3(1), dim3(1), 0, eng->stream, a->wbar, seg, (const double*)p3));
     return GF_OK;
+}
+
+template <int S, class R>
+cudaError_t adj_el_vjp_launch(gf_adjoint* a) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    return launch(k_adj_el_vjp<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, (const uint8_t*)eng->mid,
+                  adj_mats<R>(eng), v3<R>(a->U + 3), v3<R>(a->U + 6), v3<R>(a->YBAR + 6), v3<R>(a->FBAR), v3<R>(a->LAMACC + 6),
+                  v3<R>(a->F0BAR), v3<R>(a->PHI), v3<R>(a->PHINEW));
+}
+template <int S, class R>
+cudaError_t adj_comb_launch(gf_adjoint* a, int g) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    return launch(k_adj_comb<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, v3<R>(a->LAM + 3 * g),
+                  v3<R>(a->LAMACC + 3 * g), v3<R>(a->U + 3 * g), v3<R>(a->YBAR + 3 * g));
 }
 
 // reverse sweep of step `step` (lambda = d loss / d x_{step+1} in LAM on entry,
 // d loss / d x_step on exit; with elastodynamics also phi = d loss / d fs);
-// x is the step value x_step (ns components)
+// x is the step value x_step
+template <class R>
 int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     const int ng = a->el ? 3 : 1;               // cotangent groups: m, u, v
-    GF_TRY(adj_stages(a, x, step, f3(a->XJ)));
+    GF_TRY(adj_stages<R>(a, x, step, v3<R>(a->XJ), a->f32 ? v3<R>(a->XJC) : F3T<R>{}));
     if (a->el) {
         // the new u(k = 0) came from the Liao extrapolation, not the RK sum
         const long plane = (long)P.nx * P.ny;
-        GF_CU(launch(k_adj_liao_T, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, f3(a->LAM + 3), a->pend,
-                     (unsigned long long)step));
-        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->F0BAR[c], 0, sizeof(double) * P.n, st));
+        GF_CU(launch(k_adj_liao_T<R>, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, v3<R>(a->LAM + 3),
+                     rp<R>(a->pend), (unsigned long long)step));
+        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->F0BAR[c], 0, a->esz * P.n, st));
     }
     for (int c = 0; c < 3 * ng; c++) {
-        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], a->esz * P.n, cudaMemcpyDeviceToDevice, st));
         // u4 = lambda / 6 (written by a scaled copy: the comb kernel of a virtual stage 4)
-        GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
+        GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], a->esz * P.n, cudaMemcpyDeviceToDevice, st));
     }
-    for (int g = 0; g < ng; g++) GF_CU(launch(k_scale_f3, dim3(bn), dim3(kThreads), 0, st, P, f3(a->U + 3 * g), 1. / 6.));
+    for (int g = 0; g < ng; g++) GF_CU(launch(k_scale_f3<R>, dim3(bn), dim3(kThreads), 0, st, P, v3<R>(a->U + 3 * g), R(1. / 6.)));
     const long seg = (long)((step * (uint64_t)a->nw) / a->nsteps);
     for (int s = 3; s >= 0; s--) {
-        F3 y = (s == 0) ? F3{{x[0], x[1], x[2]}} : f3(a->Y[s - 1]);
-        C6 str{}, strbar{};
+        F3T<R> y = (s == 0) ? v3<R>(x) : v3<R>(a->Y[s - 1]);
+        C6T<R> str{}, strbar{};
         if (a->el && P.elasto_on)
-            for (int q = 0; q < 6; q++) { str.c[q] = a->STR[s][q]; strbar.c[q] = a->STRBAR[q]; }
-        GF_CU(launch(k_adj_vjp, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, y,
-                     f3(a->HS[s]), f3(a->U), (const double*)a->alpha, f3(a->YBAR), f3(a->HBAR), a->abar, a->hbx, str, strbar));
-        const double* R = nullptr;
-        if (eng->demag_mode == 0) {
-            GF_CU(launch(k_adj_pack, dim3(bn), dim3(kThreads), 0, st, P, f3(a->HBAR), eng->Mfft));
-            GF_FFT(cufftExecD2Z(eng->plan_r2c, eng->Mfft, eng->Mk));
-            const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
-            GF_CU(launch(k_demag_mul, dim3(blocks_for(n21, kThreads)), dim3(kThreads), 0, st, n21, -P.dx * P.dy * P.dz,
-                         (const cuDoubleComplex*)eng->Mk, (const cuDoubleComplex*)eng->Nk, (cuDoubleComplex*)eng->Mk));
-            GF_FFT(cufftExecZ2D(eng->plan_c2r, eng->Mk, eng->Mfft));
-            R = eng->Mfft;
-        }
-        GF_CU(launch(k_adj_field_T, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                     (const double*)a->aij, a->nmat, f3(a->HBAR), R, f3(a->YBAR)));
+            for (int q = 0; q < 6; q++) { str.c[q] = rp<R>(a->STR[s][q]); strbar.c[q] = rp<R>(a->STRBAR[q]); }
+        GF_CU(launch(k_adj_vjp<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMatT<R>*)a->am, y,
+                     v3<R>(a->HS[s]), v3<R>(a->U), (const R*)rp<R>(a->alpha), v3<R>(a->YBAR), v3<R>(a->HBAR), a->abar,
+                     rp<R>(a->hbx), str, strbar));
+        const R* Rk = nullptr;
+        if (eng->demag_mode == 0) GF_TRY(adj_demag_T<R>(a, Rk));
+        GF_CU(launch(k_adj_field_T<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMatT<R>*)a->am,
+                     (const R*)rp<R>(a->aij), a->nmat, v3<R>(a->HBAR), Rk, v3<R>(a->YBAR)));
         if (a->el) {
             // elastic increments, then the transposed stress and strain stencils
             cudaError_t e;
-            const F3 uku = f3(a->U + 3), ukv = f3(a->U + 6);
-            if (s == 3) e = launch(k_adj_el_vjp<3>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
-                                   uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
-            else if (s == 2) e = launch(k_adj_el_vjp<2>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
-                                        uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
-            else if (s == 1) e = launch(k_adj_el_vjp<1>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
-                                        uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
-            else e = launch(k_adj_el_vjp<0>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
-                            uku, ukv, f3(a->YBAR + 6), f3(a->FBAR), f3(a->LAMACC + 6), f3(a->F0BAR), f3(a->PHI), f3(a->PHINEW));
+            if (s == 3) e = adj_el_vjp_launch<3, R>(a);
+            else if (s == 2) e = adj_el_vjp_launch<2, R>(a);
+            else if (s == 1) e = adj_el_vjp_launch<1, R>(a);
+            else e = adj_el_vjp_launch<0, R>(a);
             GF_CU(e);
-            GF_CU(launch(k_adj_el_p1, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const DevMat*)eng->mats,
-                         f3(a->FBAR), strbar, y, f3(a->YBAR), (int)P.elasto_back, a->TO));
-            GF_CU(launch(k_adj_el_p2, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const double*)a->TO,
-                         f3(a->YBAR + 3)));
+            GF_CU(launch(k_adj_el_p1<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, adj_mats<R>(eng),
+                         v3<R>(a->FBAR), strbar, y, v3<R>(a->YBAR), (int)P.elasto_back, rp<R>(a->TO)));
+            GF_CU(launch(k_adj_el_p2<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const R*)rp<R>(a->TO),
+                         v3<R>(a->YBAR + 3)));
         }
         GF_TRY(adj_wave_add(a, seg));
         for (int g = 0; g < ng; g++) {
-            const F3 lam = f3(a->LAM + 3 * g), lacc = f3(a->LAMACC + 3 * g), u = f3(a->U + 3 * g), yb = f3(a->YBAR + 3 * g);
             cudaError_t e;
-            if (s == 3) e = launch(k_adj_comb<3>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
-            else if (s == 2) e = launch(k_adj_comb<2>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
-            else if (s == 1) e = launch(k_adj_comb<1>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
-            else e = launch(k_adj_comb<0>, dim3(bn), dim3(kThreads), 0, st, P, lam, lacc, u, yb);
+            if (s == 3) e = adj_comb_launch<3, R>(a, g);
+            else if (s == 2) e = adj_comb_launch<2, R>(a, g);
+            else if (s == 1) e = adj_comb_launch<1, R>(a, g);
+            else e = adj_comb_launch<0, R>(a, g);
             GF_CU(e);
         }
     }
@@ -3432,9 +3571,29 @@ int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
     if (a->el) {
         for (int c = 0; c < 3; c++) std::swap(a->PHI[c], a->PHINEW[c]);
         const long plane = (long)P.nx * P.ny;
-        GF_CU(launch(k_adj_liao_pend, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, f3(a->LAM + 3), a->pend,
-                     (unsigned long long)step));
+        GF_CU(launch(k_adj_liao_pend<R>, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, st, P, v3<R>(a->LAM + 3),
+                     rp<R>(a->pend), (unsigned long long)step));
     }
+    return GF_OK;
+}
+
+// precision dispatch
+int adj_fwd(gf_adjoint* a, double* const* x, uint64_t step) {
+    return a->f32 ? adj_step_forward<float>(a, x, step) : adj_step_forward<double>(a, x, step);
+}
+int adj_bwd(gf_adjoint* a, double* const* x, uint64_t step) {
+    return a->f32 ? adj_step_backward<float>(a, x, step) : adj_step_backward<double>(a, x, step);
+}
+int adj_inject(gf_adjoint* a, long slot, double inv_nfm) {
+    gf_engine* eng = a->eng;
+    const Params& P = eng->P;
+    const dim3 g(blocks_for(P.n, kThreads));
+    if (a->f32)
+        GF_CU(launch(k_adj_inject<float>, g, dim3(kThreads), 0, eng->stream, P, (const uint8_t*)eng->mid,
+                     (const AdjMatT<float>*)a->am, v3<float>(a->LAM), (const double*)a->dldm, slot, inv_nfm));
+    else
+        GF_CU(launch(k_adj_inject<double>, g, dim3(kThreads), 0, eng->stream, P, (const uint8_t*)eng->mid,
+                     (const AdjMatT<double>*)a->am, v3<double>(a->LAM), (const double*)a->dldm, slot, inv_nfm));
     return GF_OK;
 }
 
@@ -3448,24 +3607,74 @@ int adj_check(gf_adjoint* a) {
 int adj_save(gf_adjoint* a, double* dst, bool liao) {
     gf_engine* eng = a->eng;
     const long n = eng->P.n, plane = (long)eng->P.nx * eng->P.ny;
+    const size_t ez = a->esz;
     for (int q = 0; q < a->ns; q++)
-        GF_CU(cudaMemcpyAsync(dst + (size_t)q * n, a->X[q], sizeof(double) * n, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(adj_at(a, dst, (size_t)q * n), a->X[a->sidx[q]], ez * n, cudaMemcpyDeviceToDevice, eng->stream));
     if (liao && a->el) {
-        GF_CU(cudaMemcpyAsync(dst + (size_t)a->ns * n, a->hist, sizeof(double) * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
-        GF_CU(cudaMemcpyAsync(dst + (size_t)a->ns * n + 48 * plane, a->last, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice,
+        GF_CU(cudaMemcpyAsync(adj_at(a, dst, (size_t)a->ns * n), a->hist, ez * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(adj_at(a, dst, (size_t)a->ns * n + 48 * plane), a->last, ez * 3 * plane, cudaMemcpyDeviceToDevice,
                               eng->stream));
     }
     return GF_OK;
 }
-int adj_load(gf_adjoint* a, const double* src, bool liao) {
+int adj_load(gf_adjoint* a, double* src, bool liao) {
     gf_engine* eng = a->eng;
     const long n = eng->P.n, plane = (long)eng->P.nx * eng->P.ny;
+    const size_t ez = a->esz;
     for (int q = 0; q < a->ns; q++)
-        GF_CU(cudaMemcpyAsync(a->X[q], src + (size_t)q * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(a->X[a->sidx[q]], adj_at(a, src, (size_t)q * n), ez * n, cudaMemcpyDeviceToDevice, eng->stream));
     if (liao && a->el) {
-        GF_CU(cudaMemcpyAsync(a->hist, src + (size_t)a->ns * n, sizeof(double) * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
-        GF_CU(cudaMemcpyAsync(a->last, src + (size_t)a->ns * n + 48 * plane, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice,
+        GF_CU(cudaMemcpyAsync(a->hist, adj_at(a, src, (size_t)a->ns * n), ez * 48 * plane, cudaMemcpyDeviceToDevice, eng->stream));
+        GF_CU(cudaMemcpyAsync(a->last, adj_at(a, src, (size_t)a->ns * n + 48 * plane), ez * 3 * plane, cudaMemcpyDeviceToDevice,
                               eng->stream));
+    }
+    return GF_OK;
+}
+
+// material constants of the adjoint's dynamics in its real type
+template <class R>
+int adj_tables(gf_adjoint* a) {
+    gf_engine* eng = a->eng;
+    const Deck& d = eng->deck;
+    std::vector<AdjMatT<R>> am(d.mats.size());
+    for (size_t q = 0; q < d.mats.size(); q++) {
+        const Material& m = d.mats[q];
+        AdjMatT<R>& t = am[q];
+        std::memset(&t, 0, sizeof(t));
+        t.fm = m.fm ? 1u : 0u;
+        if (m.fm) {
+            t.gdt = R(m.gyro * d.dt); t.Ms = R(m.Ms); t.ex_coef = R(2. / kMu0 / m.Ms); t.Aex = R(m.Aex);
+            t.K1c = R(m.K1 / kMu0 / m.Ms); t.K2c = R(m.K2 / kMu0 / m.Ms); t.aniso = (int)m.aniso_type;
+            t.B1c = R(m.B1 / kMu0 / m.Ms); t.B2c = R(m.B2 / kMu0 / m.Ms);
+        }
+    }
+    std::vector<R> aij((size_t)(a->nmat + 1) * (a->nmat + 1), R(0));
+    for (int p = 0; p < a->nmat; p++)
+        for (int q = 0; q < a->nmat; q++) {
+            const double A1 = d.mats[p].Aex, A2 = d.mats[q].Aex;
+            aij[(size_t)(p + 1) * (a->nmat + 1) + q + 1] = R((A1 + A2 != 0.) ? 2. * A1 * A2 / (A1 + A2) : 0.);
+        }
+    void* pm = nullptr;
+    if (cudaMalloc(&pm, sizeof(AdjMatT<R>) * am.size()) != cudaSuccess) { eng->err = "cudaMalloc (adjoint tables)"; return GF_ENOMEM; }
+    a->allocs.push_back(pm);
+    a->am = pm;
+    if (cudaMemcpy(a->am, am.data(), sizeof(AdjMatT<R>) * am.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        { eng->err = "cudaMemcpy (adjoint tables)"; return GF_ECUDA; }
+    GF_TRY(adj_alloc(a, &a->aij, aij.size()));
+    if (cudaMemcpy(a->aij, aij.data(), sizeof(R) * aij.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        { eng->err = "cudaMemcpy (adjoint tables)"; return GF_ECUDA; }
+    return GF_OK;
+}
+
+// per-cell damping from FP64 host values
+int adj_upload_alpha(gf_adjoint* a, const double* al, size_t n) {
+    gf_engine* eng = a->eng;
+    if (a->f32) {
+        std::vector<float> f(n);
+        for (size_t c = 0; c < n; c++) f[c] = (float)al[c];
+        GF_CU(cudaMemcpy(a->alpha, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    } else {
+        GF_CU(cudaMemcpy(a->alpha, al, sizeof(double) * n, cudaMemcpyHostToDevice));
     }
     return GF_OK;
 }
@@ -3481,7 +3690,6 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
     *out = nullptr;
     const Deck& d = eng->deck;
     const Params& P = eng->P;
-    if (eng->mixed) { eng->err = "the adjoint runs on an FP64 engine"; return GF_EUNSUPPORTED; }
     if (!d.any_fm || d.any_afm || d.any_fe || d.em_dynamic)
         { eng->err = "the adjoint covers ferromagnetic LLG with magnetostatics and elastodynamics (no AFM, FE or Maxwell fields)"; return GF_EUNSUPPORTED; }
     if (d.elastodynamics) {
@@ -3500,37 +3708,12 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
     gf_adjoint* a = new gf_adjoint();
     a->eng = eng; a->nw = n_wave; a->ck_every = checkpoint_every;
     a->nmat = (int)d.mats.size();
+    a->f32 = eng->mixed;
+    a->esz = a->f32 ? sizeof(float) : sizeof(double);
     a->wave.assign((size_t)n_wave, 0.);
     auto fail = [&](int rc) { gf_adjoint_destroy(a); return rc; };
-    int rc = GF_OK;
-    // material constants and the harmonic-mean exchange table
-    std::vector<AdjMat> am(d.mats.size());
-    for (size_t q = 0; q < d.mats.size(); q++) {
-        const Material& m = d.mats[q];
-        AdjMat& t = am[q];
-        std::memset(&t, 0, sizeof(t));
-        t.fm = m.fm ? 1u : 0u;
-        if (m.fm) {
-            t.gdt = m.gyro * d.dt; t.Ms = m.Ms; t.ex_coef = 2. / kMu0 / m.Ms; t.Aex = m.Aex;
-            t.K1c = m.K1 / kMu0 / m.Ms; t.K2c = m.K2 / kMu0 / m.Ms; t.aniso = (int)m.aniso_type;
-            t.B1c = m.B1 / kMu0 / m.Ms; t.B2c = m.B2 / kMu0 / m.Ms;
-        }
-    }
-    std::vector<double> aij((size_t)(a->nmat + 1) * (a->nmat + 1), 0.);
-    for (int p = 0; p < a->nmat; p++)
-        for (int q = 0; q < a->nmat; q++) {
-            const double A1 = d.mats[p].Aex, A2 = d.mats[q].Aex;
-            aij[(size_t)(p + 1) * (a->nmat + 1) + q + 1] = (A1 + A2 != 0.) ? 2. * A1 * A2 / (A1 + A2) : 0.;
-        }
-    {
-        void* pm = nullptr;
-        if (cudaMalloc(&pm, sizeof(AdjMat) * am.size()) != cudaSuccess) { eng->err = "cudaMalloc (adjoint tables)"; return fail(GF_ENOMEM); }
-        a->allocs.push_back(pm);
-        a->am = (AdjMat*)pm;
-        if (cudaMemcpy(a->am, am.data(), sizeof(AdjMat) * am.size(), cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (adjoint tables)"; return fail(GF_ECUDA); }
-    }
-    if ((rc = adj_alloc(a, &a->aij, aij.size())) != GF_OK) return fail(rc);
-    if (cudaMemcpy(a->aij, aij.data(), sizeof(double) * aij.size(), cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (adjoint tables)"; return fail(GF_ECUDA); }
+    int rc = a->f32 ? adj_tables<float>(a) : adj_tables<double>(a);
+    if (rc != GF_OK) return fail(rc);
     // per-cell damping, default the material's alpha
     const long n = P.n;
     if ((rc = adj_alloc(a, &a->alpha, (size_t)n)) != GF_OK) return fail(rc);
@@ -3540,14 +3723,26 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
             const uint8_t id = d.material_cell[(size_t)c];
             if (id && d.mats[id - 1].fm) al[(size_t)c] = d.mats[id - 1].alpha;
         }
-        if (cudaMemcpy(a->alpha, al.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) { eng->err = "cudaMemcpy (alpha)"; return fail(GF_ECUDA); }
+        if (adj_upload_alpha(a, al.data(), (size_t)n) != GF_OK) { eng->err = "cudaMemcpy (alpha)"; return fail(GF_ECUDA); }
     }
     a->el = d.elastodynamics;
-    a->ns = a->el ? 12 : 3;
+    a->ns = 0;
+    for (int q = 0; q < 3; q++) a->sidx[a->ns++] = q;
+    if (a->el) for (int q = 3; q < 12; q++) a->sidx[a->ns++] = q;
+    if (a->f32) {
+        for (int q = 12; q < 15; q++) a->sidx[a->ns++] = q;
+        if (a->el) for (int q = 15; q < 21; q++) a->sidx[a->ns++] = q;
+    }
     double** bufs3[] = {a->X, a->ACC, a->XJ, a->LAM, a->LAMACC, a->U, a->YBAR, a->HBAR,
                         a->Y[0], a->Y[1], a->Y[2], a->HS[0], a->HS[1], a->HS[2], a->HS[3]};
     for (double** b : bufs3)
         if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+    if (a->f32) {
+        double** f3b[] = {a->X + 12, a->XJC};
+        for (double** b : f3b)
+            if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+        if ((rc = adj_alloc_d(a, &a->wide, (size_t)3 * n)) != GF_OK) return fail(rc);
+    }
     const long plane = (long)P.nx * P.ny;
     a->ck_len = (size_t)a->ns * n;
     if (a->el) {
@@ -3556,6 +3751,11 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
                           a->VS[0], a->VS[1], a->VS[2], a->UACC, a->VACC, a->FORCE, a->FBAR, a->F0BAR, a->PHI, a->PHINEW};
         for (double** b : el3)
             if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+        if (a->f32) {
+            double** c3[] = {a->X + 15, a->X + 18};
+            for (double** b : c3)
+                if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
+        }
         for (int s_ = 0; s_ < 4; s_++)
             for (int q = 0; q < 6; q++)
                 if ((rc = adj_alloc(a, &a->STR[s_][q], (size_t)n)) != GF_OK) return fail(rc);
@@ -3567,9 +3767,9 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
         if ((rc = adj_alloc(a, &a->pend, (size_t)48 * plane)) != GF_OK) return fail(rc);
         a->ck_len += (size_t)51 * plane;
     }
-    if ((rc = adj_alloc(a, &a->abar, (size_t)n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc_d(a, &a->abar, (size_t)n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->hbx, (size_t)n)) != GF_OK) return fail(rc);
-    if ((rc = adj_alloc(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc_d(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->zero3, (size_t)3 * n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * a->ns * n)) != GF_OK) return fail(rc);
     if (cudaStreamSynchronize(eng->stream) != cudaSuccess) { eng->err = "adjoint set-up"; return fail(GF_ECUDA); }
@@ -3581,8 +3781,7 @@ int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count) {
     GF_TRY(adj_check(a));
     gf_engine* eng = a->eng;
     if (!alpha || count != (size_t)eng->P.n) { eng->err = "gf_adjoint_set_alpha: need nx*ny*nz values"; return GF_EINVAL; }
-    GF_CU(cudaMemcpy(a->alpha, alpha, sizeof(double) * count, cudaMemcpyHostToDevice));
-    return GF_OK;
+    return adj_upload_alpha(a, alpha, count);
 }
 
 int gf_adjoint_set_waveform(gf_adjoint* a, const double* w, size_t count) {
@@ -3618,47 +3817,53 @@ int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace) {
     // checkpoints and traces sized for this run
     const size_t slots = (size_t)(nsteps / (uint64_t)a->ck_every) + 1;
     const long n = P.n;
+    const size_t ez = a->esz;
     if (slots != a->ck_slots) {
-        for (double** p : {&a->ck, &a->trace, &a->dldm})
-            if (*p) { cudaFree(*p); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)*p), a->allocs.end()); *p = nullptr; }
+        adj_free(a, &a->ck);
         a->ck_slots = 0;
     }
     if (!a->ck) {
         GF_TRY(adj_alloc(a, &a->ck, slots * a->ck_len));
         a->ck_slots = slots;
     }
-    if (a->trace) { cudaFree(a->trace); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->trace), a->allocs.end()); }
-    if (a->dldm) { cudaFree(a->dldm); a->allocs.erase(std::remove(a->allocs.begin(), a->allocs.end(), (void*)a->dldm), a->allocs.end()); }
-    GF_TRY(adj_alloc(a, &a->trace, (size_t)nsteps + 1));
-    GF_TRY(adj_alloc(a, &a->dldm, (size_t)nsteps + 1));
+    adj_free(a, &a->trace);
+    adj_free(a, &a->dldm);
+    GF_TRY(adj_alloc_d(a, &a->trace, (size_t)nsteps + 1));
+    GF_TRY(adj_alloc_d(a, &a->dldm, (size_t)nsteps + 1));
     // initial state: the engine's current m (and u, v, force store, Liao
     // history: the engine's slot of its step e is the adjoint's slot of step
-    // e - steps_done)
+    // e - steps_done; in FP32 the compensation words)
     double* const* m0 = cur(eng, eng->m);
-    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->X[c], m0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->X[c], m0[c], ez * n, cudaMemcpyDeviceToDevice, st));
+    if (a->f32)
+        for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(a->X[12 + c], eng->m.C[c], ez * n, cudaMemcpyDeviceToDevice, st));
     if (a->el) {
         double* const* u0 = cur(eng, eng->u);
         double* const* v0 = cur(eng, eng->v);
         for (int c = 0; c < 3; c++) {
-            GF_CU(cudaMemcpyAsync(a->X[3 + c], u0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-            GF_CU(cudaMemcpyAsync(a->X[6 + c], v0[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-            GF_CU(cudaMemcpyAsync(a->X[9 + c], eng->force_store[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(a->X[3 + c], u0[c], ez * n, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(a->X[6 + c], v0[c], ez * n, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(a->X[9 + c], eng->force_store[c], ez * n, cudaMemcpyDeviceToDevice, st));
+            if (a->f32) {
+                GF_CU(cudaMemcpyAsync(a->X[15 + c], eng->u.C[c], ez * n, cudaMemcpyDeviceToDevice, st));
+                GF_CU(cudaMemcpyAsync(a->X[18 + c], eng->v.C[c], ez * n, cudaMemcpyDeviceToDevice, st));
+            }
         }
         const size_t plane = (size_t)P.nx * P.ny;
         for (int sl = 0; sl < 4; sl++)
-            GF_CU(cudaMemcpyAsync(a->hist + (size_t)sl * 12 * plane,
-                                  eng->liao_hist + (size_t)((eng->steps_done + (uint64_t)sl) & 3ull) * 12 * plane,
-                                  sizeof(double) * 12 * plane, cudaMemcpyDeviceToDevice, st));
-        GF_CU(cudaMemcpyAsync(a->last, eng->liao_last, sizeof(double) * 3 * plane, cudaMemcpyDeviceToDevice, st));
+            GF_CU(cudaMemcpyAsync(adj_at(a, a->hist, (size_t)sl * 12 * plane),
+                                  reinterpret_cast<char*>(eng->liao_hist) + ((eng->steps_done + (uint64_t)sl) & 3ull) * 12 * plane * ez,
+                                  ez * 12 * plane, cudaMemcpyDeviceToDevice, st));
+        GF_CU(cudaMemcpyAsync(a->last, eng->liao_last, ez * 3 * plane, cudaMemcpyDeviceToDevice, st));
     }
     GF_TRY(adj_save(a, a->ck, true));
     GF_TRY(adj_mean_x(a, a->X[0], 0));
     for (uint64_t k = 0; k < nsteps; k++) {
-        GF_TRY(adj_step_forward(a, a->X, k));
+        GF_TRY(adj_fwd(a, a->X, k));
         GF_TRY(adj_mean_x(a, a->X[0], (long)k + 1));
         if ((k + 1) % (uint64_t)a->ck_every == 0) {
             const size_t slot = (size_t)((k + 1) / (uint64_t)a->ck_every);
-            GF_TRY(adj_save(a, a->ck + slot * a->ck_len, true));
+            GF_TRY(adj_save(a, adj_at(a, a->ck, slot * a->ck_len), true));
         }
     }
     GF_CU(cudaMemcpyAsync(mx_trace, a->trace, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, st));
@@ -3678,35 +3883,33 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     GF_CU(cudaSetDevice(eng->device));
     cudaStream_t st = eng->stream;
     const long n = P.n;
-    const unsigned bn = blocks_for(n, kThreads);
+    const size_t ez = a->esz;
     const uint64_t N = a->nsteps;
     const double inv_nfm = 1. / (double)eng->deck.NFM;
     GF_CU(cudaMemcpyAsync(a->dldm, dloss_dmx, sizeof(double) * (N + 1), cudaMemcpyHostToDevice, st));
-    for (int c = 0; c < (a->el ? 9 : 3); c++) GF_CU(cudaMemsetAsync(a->LAM[c], 0, sizeof(double) * n, st));
+    for (int c = 0; c < (a->el ? 9 : 3); c++) GF_CU(cudaMemsetAsync(a->LAM[c], 0, ez * n, st));
     if (a->el) {
-        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->PHI[c], 0, sizeof(double) * n, st));
-        GF_CU(cudaMemsetAsync(a->pend, 0, sizeof(double) * 48 * (size_t)P.nx * P.ny, st));
+        for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->PHI[c], 0, ez * n, st));
+        GF_CU(cudaMemsetAsync(a->pend, 0, ez * 48 * (size_t)P.nx * P.ny, st));
     }
     GF_CU(cudaMemsetAsync(a->abar, 0, sizeof(double) * n, st));
     GF_CU(cudaMemsetAsync(a->wbar, 0, sizeof(double) * a->nw, st));
-    GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am, f3(a->LAM),
-                 (const double*)a->dldm, (long)N, inv_nfm));
+    GF_TRY(adj_inject(a, (long)N, inv_nfm));
     const uint64_t K = (uint64_t)a->ck_every;
     const uint64_t nblocks = (N + K - 1) / K;
     for (uint64_t b = nblocks; b-- > 0;) {
         const uint64_t s0 = b * K, s1 = std::min(N, s0 + K);
         // recompute the block's step values x_s0 .. x_{s1-1}
-        GF_TRY(adj_load(a, a->ck + b * a->ck_len, true));
+        GF_TRY(adj_load(a, adj_at(a, a->ck, b * a->ck_len), true));
         for (uint64_t k = s0; k < s1; k++) {
-            GF_TRY(adj_save(a, a->xs + (k - s0) * (size_t)a->ns * n, false));
-            if (k + 1 < s1) GF_TRY(adj_step_forward(a, a->X, k));
+            GF_TRY(adj_save(a, adj_at(a, a->xs, (k - s0) * (size_t)a->ns * n), false));
+            if (k + 1 < s1) GF_TRY(adj_fwd(a, a->X, k));
         }
         for (uint64_t k = s1; k-- > s0;) {
-            double* xp[12];
-            for (int q = 0; q < a->ns; q++) xp[q] = a->xs + ((k - s0) * (size_t)a->ns + q) * n;
-            GF_TRY(adj_step_backward(a, xp, k));
-            GF_CU(launch(k_adj_inject, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMat*)a->am,
-                         f3(a->LAM), (const double*)a->dldm, (long)k, inv_nfm));
+            double* xp[21] = {};
+            for (int q = 0; q < a->ns; q++) xp[a->sidx[q]] = adj_at(a, a->xs, ((k - s0) * (size_t)a->ns + q) * n);
+            GF_TRY(adj_bwd(a, xp, k));
+            GF_TRY(adj_inject(a, (long)k, inv_nfm));
         }
     }
     GF_CU(cudaMemcpyAsync(grad_wave, a->wbar, sizeof(double) * a->nw, cudaMemcpyDeviceToHost, st));
@@ -3726,10 +3929,18 @@ int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count) {
     const uint64_t K = (uint64_t)a->ck_every, N = a->nsteps;
     const uint64_t b = N / K;
     cudaStream_t st = eng->stream;
-    GF_TRY(adj_load(a, a->ck + b * a->ck_len, true));
-    for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_step_forward(a, a->X, k));
-    for (int c = 0; c < 3; c++)
-        GF_CU(cudaMemcpyAsync(host_m + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    GF_TRY(adj_load(a, adj_at(a, a->ck, b * a->ck_len), true));
+    for (uint64_t k = b * K; k < N; k++) GF_TRY(adj_fwd(a, a->X, k));
+    if (a->f32) {
+        // FP64 values x + c of the compensated FP32 pairs
+        for (int c = 0; c < 3; c++)
+            GF_CU(launch(k_widen, dim3(blocks_for(n, kThreads)), dim3(kThreads), 0, st, (const float*)rp<float>(a->X[c]),
+                         (const float*)rp<float>(a->X[12 + c]), n, a->wide + (size_t)c * n));
+        GF_CU(cudaMemcpyAsync(host_m, a->wide, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+    } else {
+        for (int c = 0; c < 3; c++)
+            GF_CU(cudaMemcpyAsync(host_m + (size_t)c * n, a->X[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    }
     GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(st));
     return GF_OK;

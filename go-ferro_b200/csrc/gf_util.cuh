@@ -28,6 +28,24 @@ static __global__ void k_sum_stride(const double* __restrict__ in, long n, doubl
     partial[t] = acc;
 }
 
+// The same first pass over an FP32 array, each term widened to FP64 (the
+// later passes are k_sum_stride over the FP64 partials).
+static __global__ void k_sum_stride_f(const float* __restrict__ in, long n, double* __restrict__ partial, long T) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    double acc = 0.;
+    long i = t;
+    for (; i + 7 * T < n; i += 8 * T) {
+        float v[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) v[b] = in[i + b * T];
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc = acc + (double)v[b];
+    }
+    for (; i < n; i += T) acc = acc + (double)in[i];
+    partial[t] = acc;
+}
+
 // Three arrays (component y = blockIdx.y), each term the FP64 value of an
 // element: a double, or in the mixed form (f32) the FP64 value x + c of an
 // FP32 pair (c may be null).

@@ -432,13 +432,17 @@ void gf_batch_destroy(gf_batch* b);
  * elastic boundary (if_1D_ABC), an elastic source, static strain inputs,
  * ny < nz (the reference's z-face neighbour rule for k = ny-1) or nz < 5
  * are GF_EUNSUPPORTED.  The reference has no adjoint; these entry points
- * have no counterpart there.  FP64 engines only.  The adjoint uses the
- * engine's stream and FFT buffers: do not advance the engine while an
- * adjoint call runs. */
+ * have no counterpart there.  On an FP64 engine the adjoint computes in
+ * FP64; on a mixed-form engine its forward run, stage fields and cotangents
+ * are FP32 (step values with compensation words, the engine's own FP32
+ * elastic kernels and FFT path; |m| is not renormalised) while the damping
+ * and waveform gradients, the <m_x> trace and its cotangent stay FP64.  The
+ * adjoint uses the engine's stream and FFT buffers: do not advance the
+ * engine while an adjoint call runs. */
 typedef struct gf_adjoint gf_adjoint;
 /* checkpoint_every: steps between stored states (the backward run recomputes
  * the steps in between; device memory ~ 24 * n * checkpoint_every bytes, 96
- * with elastodynamics). */
+ * with elastodynamics; mixed form 24 and 84). */
 int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint** out);
 /* per-cell damping (nx*ny*nz values; default: the material's alpha) */
 int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count);

@@ -181,8 +181,8 @@ def test_adjoint_forward_matches_engine_magnetoelastic(gf, tmp_path):
     assert np.max(np.abs(mfin - m_eng)) <= 1e-12
 
 
-def _grads(gf, tmp_path, d, steps, nw, wave0, alpha0, fd):
-    with gf.Engine(str(tmp_path), device=0) as eng:
+def _grads(gf, tmp_path, d, steps, nw, wave0, alpha0, fd, precision="fp64"):
+    with gf.Engine(str(tmp_path), device=0, precision=precision) as eng:
         with gf.Adjoint(eng, n_wave=nw, checkpoint_every=64) as adj:
             def loss_of(wave, alpha):
                 adj.set_waveform(wave)
@@ -231,3 +231,61 @@ def test_adjoint_gradients_magnetoelastic_match_finite_differences(gf, tmp_path)
     d0 = me_film(gf, tmp_path / "plain", steps=steps, boost=0.0)
     gw0, _, _ = _grads(gf, tmp_path / "plain", d0, steps, nw, wave0, alpha0, False)
     assert np.max(np.abs(gw - gw0)) > 1e-2 * np.max(np.abs(gw))
+
+
+# ---------------------------------------------------------------------------
+# the FP32 mixed adjoint: on a mixed-form engine the adjoint's forward run,
+# stage fields and cotangents are FP32 (step values compensated, the
+# engine's own FP32 elastic kernels), the damping and waveform gradients are
+# accumulated in FP64.  Gradients are checked against FP64 central finite
+# differences (the FP64 engine's adjoint forward run, relative step 1e-4)
+# at the same 1e-4 tolerance.
+# ---------------------------------------------------------------------------
+def test_mixed_adjoint_forward_follows_the_engines(gf, tmp_path):
+    """The FP32 adjoint's <m_x> trace and final m follow the mixed engine's
+    step (which also renormalises |m| every stage) and the FP64 engine's to
+    FP32 resolution."""
+    me_film(gf, tmp_path, steps=40)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        with gf.Engine(str(tmp_path), device=0, precision=prec) as eng:
+            if prec == "mixed":
+                with gf.Adjoint(eng, n_wave=4, checkpoint_every=16) as adj:
+                    out["adj_tr"] = adj.forward(40)
+                    out["adj_m"] = adj.final_m()
+            ref = [eng.average("m")[0]]
+            for _ in range(40):
+                eng.advance(1)
+                ref.append(eng.average("m")[0])
+            out[prec + "_tr"] = np.array(ref)
+            out[prec + "_m"] = eng.download("m")
+    for prec in ("mixed", "fp64"):
+        e_tr = np.max(np.abs(out["adj_tr"] - out[prec + "_tr"]))
+        e_m = np.max(np.abs(out["adj_m"] - out[prec + "_m"]))
+        assert e_tr <= 1e-6 and e_m <= 1e-6, f"{prec}: trace {e_tr:.2e}, m {e_m:.2e}"
+
+
+@pytest.mark.parametrize("case", ["fm_film", "magnetoelastic"])
+def test_mixed_adjoint_gradients_match_fp64_finite_differences(gf, tmp_path, case):
+    nw = 8
+    if case == "fm_film":
+        steps = 300
+        d = film(gf, tmp_path, steps=steps)
+    else:
+        steps = 200
+        d = me_film(gf, tmp_path, steps=steps)
+    mc = d.material_cell().ravel() == 1
+    rng = np.random.default_rng(11)
+    alpha0 = 0.02 * (1.0 + 0.1 * rng.random(d.n)) * mc
+    tt = (np.arange(nw) + 0.5) / nw
+    wave0 = (1e-2 / MU0) * np.sin(2 * np.pi * tt) * np.exp(-4.0 * (tt - 0.4) ** 2)
+    gw, ga, _ = _grads(gf, tmp_path, d, steps, nw, wave0, alpha0, False, precision="mixed")
+    gw64, ga64, (fd_w, v, fd_a) = _grads(gf, tmp_path, d, steps, nw, wave0, alpha0, True)
+    err_w = np.max(np.abs(gw - fd_w)) / np.max(np.abs(fd_w))
+    assert err_w <= 1e-4, f"FP32 waveform gradient vs FP64 FD: {err_w:.2e}"
+    ad = float(ga @ v)
+    assert abs(ad - fd_a) <= 1e-4 * abs(fd_a), f"FP32 alpha directional gradient {ad:.6e} vs FP64 FD {fd_a:.6e}"
+    # per cell against the FP64 adjoint (FP32 resolution of each cell's share)
+    err_a = np.max(np.abs(ga - ga64)) / np.max(np.abs(ga64))
+    assert err_a <= 1e-3, f"FP32 per-cell alpha gradient vs FP64 adjoint: {err_a:.2e}"
+    print(f"{case}: waveform {err_w:.2e}, alpha direction {abs(ad - fd_a) / abs(fd_a):.2e}, per cell {err_a:.2e}")
