@@ -586,8 +586,11 @@ def sweep_decks(gf, count, steps, seed=20241207):
 
 def run_sweep(gf, torch, args, local_rank, count, steps, fp64_check):
     """Batched mixed-form sweep: all instances advanced by one graph per step
-    (gf_batch, autotuned elastic tiles) against the same engines advanced one
-    after another with their own graphs; optional FP64 error per instance."""
+    (gf_batch in its phase mode: each RK stage a few launches over the work
+    items of every instance, autotuned tile chunks and phase-A fusion)
+    against the same engines advanced one after another with their own
+    graphs and against the batch's branch mode (one graph branch per
+    engine); optional FP64 error per instance."""
     import shutil
     decks = sweep_decks(gf, count, steps)
     tmp = tempfile.mkdtemp()
@@ -618,27 +621,36 @@ def run_sweep(gf, torch, args, local_rank, count, steps, fp64_check):
         for e in engines:
             e.synchronize()
         t_seq = time.perf_counter() - t0
-        with gf.Batch(engines, autotune=True) as b:
-            chunks = sorted({b.tuned_chunk(i) for i in range(len(engines))})
-            stream = torch.cuda.ExternalStream(b.stream(), device=local_rank)
-            b.advance(2)
-            b.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            b.advance(steps)
-            e1.record(stream)
-            e1.synchronize()
-            t_batch = e0.elapsed_time(e1) / 1e3
+        def timed_batch(mode):
+            with gf.Batch(engines, autotune=True, mode=mode) as b:
+                chunks = sorted({b.tuned_chunk(i) for i in range(len(engines))})
+                plan = b.plan()
+                stream = torch.cuda.ExternalStream(b.stream(), device=local_rank)
+                b.advance(2)
+                b.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.advance(steps)
+                e1.record(stream)
+                e1.synchronize()
+                return e0.elapsed_time(e1) / 1e3, chunks, plan
+
+        # one graph branch per engine, then the phase mode (13 launches per
+        # step for all engines of these decks), the batch's default for them
+        t_branch, _, _ = timed_batch("branches")
+        t_batch, chunks, plan = timed_batch("auto")
         pz = [float(e.average("p")[2]) for e in engines]
         result = {"instances": count, "cells": cells, "steps_timed": steps,
                   "value": cells * steps / t_batch, "unit": "cell-steps/s", "ms_per_step": 1e3 * t_batch / steps,
                   "sequential_ms_per_step": 1e3 * t_seq / steps, "speedup_vs_sequential": t_seq / t_batch,
+                  "branches_ms_per_step": 1e3 * t_branch / steps, "speedup_vs_branches": t_branch / t_batch,
+                  "plan": plan,
                   "tuned_elastic_chunks": chunks, "create_s": t_create,
                   "grids": {f"{a}x{b_}x{c}": sum(1 for d, _, _ in decks if (d.nx, d.ny, d.nz) == (a, b_, c))
                             for a, b_, c in SWEEP_SIZES}}
         if fp64_check:
             # the same instances from the same state in FP64, one trace point per step
-            n_check = 2 * steps + 4     # sequential warm-up + timed steps, batch warm-up + timed steps
+            n_check = 3 * steps + 6     # sequential, branch-mode and phase-mode runs: 2 warm-up + timed steps each
             errs, resp = [], []
             for (d, kvcm, f0), ddir, pzm in zip(decks, dirs, pz):
                 with gf.Engine(ddir, device=local_rank, precision="fp64") as e64:
@@ -790,7 +802,7 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_batch:
         sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.sweep_steps, fp64_check=True)
         sw["workload"] = ("batched sweep: 48 ferroelectric + FDTD instances, grids drawn from 32^3, 48x48x32, "
-                          "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step")
+                          "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step (phase mode: 13 launches per step for all instances)")
         line["batched"] = sw
     print(json.dumps(line))
 

@@ -41,7 +41,8 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients",
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
-           "gf_batch_create", "gf_batch_advance", "gf_batch_synchronize", "gf_batch_stream", "gf_batch_tuned_chunk",
+           "gf_batch_create", "gf_batch_create_ex", "gf_batch_plan", "gf_batch_advance", "gf_batch_synchronize",
+           "gf_batch_stream", "gf_batch_tuned_chunk",
            "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics", "gf_set_elastostatics",
            "gf_save_state", "gf_load_state", "gf_create", "gf_set_table", "gf_stage_begin", "gf_stage_commit",
            "gf_static_solve"]
@@ -231,6 +232,9 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_save_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_load_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
+    lib.gf_batch_create_ex.argtypes = [ctypes.POINTER(vp), c_int, c_int, c_int, ctypes.POINTER(vp)]
+    lib.gf_batch_plan.argtypes = [vp]
+    lib.gf_batch_plan.restype = ctypes.c_char_p
     lib.gf_batch_advance.argtypes = [vp, c_u64]
     lib.gf_batch_synchronize.argtypes = [vp]
     lib.gf_batch_stream.argtypes = [vp]
@@ -480,18 +484,25 @@ class Adjoint:
         self.close()
 
 
+BATCH_MODES = {"auto": 0, "branches": 1, "phases": 2}
+
+
 class Batch:
     """Several engines advanced together by one CUDA graph per step
-    (gf_batch_*); with autotune the elastic tile's x-chunk is picked per
-    engine by timing.  The engines remain owned by the caller and must not be
+    (gf_batch_*).  mode "phases": mixed-form TDGL / elastodynamics / FDTD
+    engines, each RK stage a few launches over the work items of every
+    engine; "branches": one graph branch per engine; "auto": phases when
+    every engine allows it.  With autotune the tile x-chunk (and, in the
+    phase mode, the fusion of phase A) is picked by timing; plan() describes
+    the choice.  The engines remain owned by the caller and must not be
     advanced directly while the batch exists."""
 
-    def __init__(self, engines, autotune: bool = True):
+    def __init__(self, engines, autotune: bool = True, mode: str = "auto"):
         self.engines = list(engines)
         self.lib = self.engines[0].lib
         arr = (ctypes.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
         h = ctypes.c_void_p()
-        rc = self.lib.gf_batch_create(arr, len(self.engines), int(bool(autotune)), ctypes.byref(h))
+        rc = self.lib.gf_batch_create_ex(arr, len(self.engines), int(bool(autotune)), BATCH_MODES[mode], ctypes.byref(h))
         if rc != GF_OK:
             raise GFError(rc, self.lib.gf_batch_last_error(None).decode())
         self.h = h
@@ -511,6 +522,9 @@ class Batch:
 
     def tuned_chunk(self, index: int) -> int:
         return int(self.lib.gf_batch_tuned_chunk(self.h, int(index)))
+
+    def plan(self) -> str:
+        return self.lib.gf_batch_plan(self.h).decode()
 
     def close(self) -> None:
         if getattr(self, "h", None):

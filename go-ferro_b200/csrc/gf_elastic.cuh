@@ -464,16 +464,19 @@ __device__ inline void etile_stage_finish(const ETileSmem<R>& sm, int slot, cons
 #ifndef GF_ETILE_MINB_F32
 #define GF_ETILE_MINB_F32 4
 #endif
-template <int S, bool CUB, class R = double>
-__global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_F32 : 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat,
-                                                                                        const __grid_constant__ ETileMaps tm) {
+// The tile of block (bx, by, bz): columns k0 = bx TK.., rows j0 = by TJ..,
+// x-planes bz chunk..; smem_raw = the block's dynamic shared memory
+// (etile::smem_bytes).  k_elastic_tile runs it once per block; the batched
+// phase kernels run it on the work items of many engines.
+template <int S, bool CUB, class R>
+__device__ __forceinline__ void elastic_tile_body(const Params& P, const StageIOT<R>& io, int chunk, int nmat,
+                                                  const ETileMaps& tm, int bx, int by, int bz, unsigned char* smem_raw) {
     using namespace etile;
-    GF_EXTERN_SMEM(unsigned char, smem_raw);
     const ETileSmem<R> sm{smem_raw};
 
     const int tid = threadIdx.x;
-    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-    const int i0 = blockIdx.z * chunk;
+    const int k0 = bx * TK, j0 = by * TJ;
+    const int i0 = bz * chunk;
     const int i1 = min(i0 + chunk, P.nx) - 1;            // last plane of the chunk
     const int L = i1 - i0 + 1;
     const int jl = tid / TK, kl = tid - (tid / TK) * TK;
@@ -743,6 +746,13 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
     }
 }
 
+template <int S, bool CUB, class R = double>
+__global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_F32 : 2) k_elastic_tile(Params P, StageIOT<R> io, int chunk, int nmat,
+                                                                                        const __grid_constant__ ETileMaps tm) {
+    GF_EXTERN_SMEM(unsigned char, smem_raw);
+    elastic_tile_body<S, CUB, R>(P, io, chunk, nmat, tm, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
 // Per cell after k_elastic_tile: velocity increment from the stress
 // divergence f with mass and stiffness damping (get_dv_RK*,
 // elastic_dynamic_solver.cpp:1295-1329: weights 1, 2, 2, 1 on f - f_store,
@@ -799,10 +809,11 @@ struct RkCellF32 {
     }
 };
 
-template <int S, class R = double>
-__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
+// block bx of the RK update (256 cells per block in FP64, 512 in FP32)
+template <int S, class R>
+__device__ __forceinline__ void elastic_rk_body(const Params& P, const StageIOT<R>& io, int bx) {
     if constexpr (is_mixed<R>::value) {
-        const int c0 = blockIdx.x * 512 + threadIdx.x, c1 = c0 + 256;
+        const int c0 = bx * 512 + threadIdx.x, c1 = c0 + 256;
         RkCellF32<S> a, b;
         if (c0 < P.n) a.load(io, c0);
         if (c1 < P.n) b.load(io, c1);
@@ -812,7 +823,7 @@ __global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
         // FP64: every operand of the three components is loaded before the first
         // store (as RkCellF32 does for two cells), so a thread's ~20 loads are in
         // flight together
-        const int c = blockIdx.x * blockDim.x + threadIdx.x;
+        const int c = bx * blockDim.x + threadIdx.x;
         if (c >= P.n) return;
         const uint8_t id = io.mid[c];
         double f[3], fs[3], vx[3], vin[3], ux[3], va[3], ua[3];
@@ -856,6 +867,11 @@ __global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
     }
 }
 
+template <int S, class R = double>
+__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
+    elastic_rk_body<S, R>(P, io, blockIdx.x);
+}
+
 // cell strain (global frame) of the current step for output (Dexx_glb ...)
 template <class R = double>
 __global__ void k_cell_strain(Params P, StageIOT<R> io, double* out6) {
@@ -873,9 +889,9 @@ __global__ void k_cell_strain(Params P, StageIOT<R> io, double* out6) {
 // For stages 0..2 `tgt` is the stage output (F_glb_store); for the last
 // stage it is the new step value and `old` the step-start value (the
 // reference's history copy Du?_glb_t1).
-template <int S, class R = double>
-__global__ void k_elastic_bc(Params P, StageIOT<R> io) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+template <int S, class R>
+__device__ __forceinline__ void elastic_bc_body(const Params& P, const StageIOT<R>& io, int bx) {
+    const long t = (long)bx * blockDim.x + threadIdx.x;
     if (t >= (long)P.nx * P.ny) return;
     const long i = t / P.ny, j = t - i * P.ny;
     const long nz = P.nz;
@@ -964,6 +980,11 @@ __global__ void k_elastic_bc(Params P, StageIOT<R> io) {
         if constexpr (is_mixed<R>::value)
             if (S == 3) io.u_cmp.c[P.strain_comp][cid(P, i, j, P.source_z)] = R(0);
     }
+}
+
+template <int S, class R = double>
+__global__ void k_elastic_bc(Params P, StageIOT<R> io) {
+    elastic_bc_body<S, R>(P, io, blockIdx.x);
 }
 
 }  // namespace gf

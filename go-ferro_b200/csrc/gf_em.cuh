@@ -362,11 +362,12 @@ __device__ inline void em_H_face(const Params& P, const StageIOT<R>& io, const E
 #ifndef GF_EM_MINB_F64
 #define GF_EM_MINB_F64 3
 #endif
-template <int S, class R = double>
-__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : GF_EM_MINB_F64) k_em_fused(Params P, StageIOT<R> io, int nmat,
-                                                                                      const EmCls<R>* __restrict__ cls_g, int ncls) {
-    __shared__ EmMat<R> mt[kMaxMat];
-    __shared__ EmCls<R> cl[kEmMaxCls];
+// block (bx, by): 256 vertices of the (j, k) plane bx of vertex plane by;
+// mt, cl = the block's shared-memory tables (kMaxMat and kEmMaxCls entries),
+// filled here behind a barrier
+template <int S, class R>
+__device__ __forceinline__ void em_fused_body(const Params& P, const StageIOT<R>& io, int nmat, const EmCls<R>* __restrict__ cls_g,
+                                              int ncls, int bx, int by, EmMat<R>* mt, EmCls<R>* cl) {
     for (int q = threadIdx.x; q < nmat; q += blockDim.x) {
         const DevMatT<R>& d = io.mats[q];
         mt[q].er = d.er; mt[q].cond = d.cond; mt[q].Ms = d.Ms; mt[q].Ms1 = d.Ms1; mt[q].Ms2 = d.Ms2; mt[q].flags = d.flags;
@@ -374,9 +375,9 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : GF_
     for (int q = threadIdx.x; q < ncls; q += blockDim.x) cl[q] = cls_g[q];
     __syncthreads();
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= (ny + 1) * (nz + 1)) return;
-    const int i = blockIdx.y;
+    const int i = by;
     const int j = t / (nz + 1), k = t - (t / (nz + 1)) * (nz + 1);
     const StageDrive& dr = stage_drive(io, S);
     // E edges: gather all three, then update (the stores follow every load)
@@ -404,6 +405,14 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : GF_
         if (on1) em_H_face<S, 1, R>(P, io, mt, L1, e1);
         if (on2) em_H_face<S, 2, R>(P, io, mt, L2, e2);
     }
+}
+
+template <int S, class R = double>
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_EM_MINB_F32 : GF_EM_MINB_F64) k_em_fused(Params P, StageIOT<R> io, int nmat,
+                                                                                      const EmCls<R>* __restrict__ cls_g, int ncls) {
+    __shared__ EmMat<R> mt[kMaxMat];
+    __shared__ EmCls<R> cl[kEmMaxCls];
+    em_fused_body<S, R>(P, io, nmat, cls_g, ncls, blockIdx.x, blockIdx.y, mt, cl);
 }
 
 // Drude polarisation current, per cell: dJp_n = (e0 wp_n^2 E_cell c_n -
@@ -543,10 +552,10 @@ __global__ void k_em_plane(Params P, StageIOT<R> io) {
 // For S < 3:  out(b) = X(b_in) + c * (X(b) - out(b_in))   (stage store)
 // For S = 3:  new(b) = old(b_in) + c * (old(b) - new(b_in))
 // where X / old is the step-start value and out / new the value written.
-template <int S, int F, class R = double>
-__global__ void k_em_mur(Params P, StageIOT<R> io) {
+template <int S, int F, class R>
+__device__ __forceinline__ void em_mur_body(const Params& P, const StageIOT<R>& io, int bx) {
     const long nx = P.nx, ny = P.ny, nz = P.nz;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long t = (long)bx * blockDim.x + threadIdx.x;
     const bool half = (S == 0 || S == 1);
     // two tangential components per face; index range per component
     if (F == 0) {
@@ -629,6 +638,11 @@ __global__ void k_em_mur(Params P, StageIOT<R> io) {
         } else { O[e0] = R(0.); O[eN] = R(0.); }
         if constexpr (is_mixed<R>::value) if (S == 3) { io.E_cmp.c[comp][e0] = R(0); io.E_cmp.c[comp][eN] = R(0); }
     }
+}
+
+template <int S, int F, class R = double>
+__global__ void k_em_mur(Params P, StageIOT<R> io) {
+    em_mur_body<S, F, R>(P, io, blockIdx.x);
 }
 
 }  // namespace gf

@@ -40,6 +40,7 @@
 #include "gf_demag.cuh"
 #include "gf_util.cuh"
 #include "gf_adjoint.cuh"
+#include "gf_batch.cuh"
 #include "gf_elec.cuh"
 #include "gf_elasto.cuh"
 
@@ -198,6 +199,9 @@ int gf_mixed_enqueue_stage(gf_engine* eng, int parity, int s);         // kernel
 int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-memory opt-in, occupancy
 int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms);          // stage-1 elastic tile, mean ms per launch
 int gf_mixed_adj_elastic(gf_engine* eng, int s, int rk, const StageIOT<float>& io);  // adjoint: FP32 elastic tile / RK of stage s
+int gf_mixed_batch_attr(size_t smem);                                   // shared-memory opt-in of the batch phase kernels
+int gf_mixed_batch_phase(const BatchInst* insts, const BatchItem* items, int count, int s, int ph, int parity, size_t smem,
+                         unsigned* tma_err, cudaStream_t st);                 // one phase launch of a batch (a cudaError_t)
 
 namespace {
 
@@ -1179,6 +1183,34 @@ int adj_elastic_f32(gf_engine* eng, int rk, const StageIOT<float>& io) {
     return GF_OK;
 }
 }  // namespace
+
+int gf_mixed_batch_attr(size_t smem) {
+    const int b = (int)smem;
+    cudaError_t e = cudaSuccess;
+    auto set = [&](auto k) { if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b); };
+    set(k_batch_phase<0, 0>); set(k_batch_phase<1, 0>); set(k_batch_phase<2, 0>); set(k_batch_phase<3, 0>);
+    set(k_batch_phase<0, 3>); set(k_batch_phase<1, 3>); set(k_batch_phase<2, 3>); set(k_batch_phase<3, 3>);
+    return e == cudaSuccess ? GF_OK : GF_ECUDA;
+}
+
+int gf_mixed_batch_phase(const BatchInst* insts, const BatchItem* items, int count, int s, int ph, int parity, size_t smem,
+                         unsigned* tma_err, cudaStream_t st) {
+    if (count <= 0) return (int)cudaSuccess;
+    ETileMaps tm;
+    std::memset(&tm, 0, sizeof(tm));
+    tm.err = tma_err;
+    const dim3 g((unsigned)count), b(256);
+    const size_t em_tab = kMaxMat * sizeof(EmMat<float>) + kEmMaxCls * sizeof(EmCls<float>);
+    const size_t sm = (ph == 0 || ph == 3) ? smem : (ph == 4 ? em_tab : 0);
+    cudaError_t e = cudaErrorInvalidValue;
+#define GF_BPH(S_, P_) if (s == S_ && ph == P_) e = launch(k_batch_phase<S_, P_>, g, b, sm, st, insts, items, parity, tm)
+    GF_BPH(0, 0); GF_BPH(0, 1); GF_BPH(1, 0); GF_BPH(1, 1);
+    GF_BPH(2, 0); GF_BPH(2, 1); GF_BPH(3, 0); GF_BPH(3, 1);
+    GF_BPH(0, 3); GF_BPH(0, 4); GF_BPH(0, 5); GF_BPH(1, 3); GF_BPH(1, 4); GF_BPH(1, 5);
+    GF_BPH(2, 3); GF_BPH(2, 4); GF_BPH(2, 5); GF_BPH(3, 3); GF_BPH(3, 4); GF_BPH(3, 5);
+#undef GF_BPH
+    return (int)e;
+}
 
 int gf_mixed_adj_elastic(gf_engine* eng, int s, int rk, const StageIOT<float>& io) {
     if (s == 0) return adj_elastic_f32<0>(eng, rk, io);
@@ -2974,6 +3006,18 @@ struct gf_batch {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::string err;
     std::vector<int> tuned_chunk;
+    // phase mode (mixed-form TDGL / elastodynamics / FDTD engines): one launch
+    // per stage phase over the work items of every engine
+    bool phases = false;
+    bool split_tile = false;         // phase A as three concurrent launches (tile, Yee, TDGL items)
+    std::vector<int> chunk;          // per engine: x-planes per elastic tile item
+    BatchInst* dinst = nullptr;
+    BatchItem* ditems[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // A (all), A tile, A Yee, A TDGL, B + C + D
+    int nA = 0, nAt = 0, nAe = 0, nAf = 0, nB = 0, nC = 0, nD = 0;
+    cudaStream_t side[2] = {nullptr, nullptr};   // split phase A: Yee and TDGL items beside the tile items
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    size_t smem = 0;
+    std::string plan;
 };
 
 namespace {
@@ -3018,7 +3062,268 @@ int autotune_tile(gf_batch* b, gf_engine* e) {
     return GF_OK;
 }
 
-int batch_capture(gf_batch* b) {
+// Why engine e cannot run in the phase mode ("" if it can): the phase
+// kernels cover the mixed form's TDGL, elastodynamics and Yee paths with Mur
+// boundaries, without magnetism, flexoelectricity, static solves, plane
+// sources, conductors or Drude poles.
+std::string batch_phase_blocker(const gf_engine* e) {
+    const Params& P = e->P;
+    if (!e->mixed) return "FP64 engine";
+    if (P.fm || P.afm) return "magnetic physics";
+    if (P.flexo) return "flexoelectricity";
+    if (P.planeEM || P.pec || P.drude) return "plane source, conductor or Drude poles";
+    if (e->demag_mode >= 0 || e->elec_on || e->es_on) return "static solves";
+    if (!(P.fe || P.em || P.elastic)) return "no stage kernels";
+    return "";
+}
+
+// the work items of every engine at elastic x-chunk ch[i]: phase A's tile,
+// Yee and TDGL items (A = all three, tiles first: the longest items); B the
+// RK update, C the elastic boundary planes; an engine's Mur directions in
+// order x, y, z in B, C, D, one phase each
+void batch_items(const gf_batch* b, const std::vector<int>& ch, std::vector<BatchItem>& A, std::vector<BatchItem>& At,
+                 std::vector<BatchItem>& Ae, std::vector<BatchItem>& Af, std::vector<BatchItem>& B, std::vector<BatchItem>& C,
+                 std::vector<BatchItem>& D) {
+    A.clear(); At.clear(); Ae.clear(); Af.clear(); B.clear(); C.clear(); D.clear();
+    for (size_t i = 0; i < b->engs.size(); i++) {
+        const Params& P = b->engs[i]->P;
+        const int in = (int)i;
+        const long nx = P.nx, ny = P.ny, nz = P.nz;
+        if (P.elastic) {
+            const int gx = (P.nz + etile::TK - 1) / etile::TK, gy = (P.ny + etile::TJ - 1) / etile::TJ;
+            const int gz = (P.nx + ch[i] - 1) / ch[i];
+            for (int z = 0; z < gz; z++)
+                for (int y = 0; y < gy; y++)
+                    for (int x = 0; x < gx; x++) At.push_back({in, BK_TILE, x, y, z});
+            const int nrk = (int)blocks_for(P.n, 2 * kThreads);
+            for (int x = 0; x < nrk; x++) B.push_back({in, BK_RK, x, 0, 0});
+            const int nbc = (int)blocks_for(nx * ny, kThreads);
+            for (int x = 0; x < nbc; x++) C.push_back({in, BK_BC, x, 0, 0});
+        }
+        if (P.em) {
+            const int gx = (int)blocks_for((ny + 1) * (nz + 1), kThreads);
+            for (int y = 0; y <= P.nx; y++)
+                for (int x = 0; x < gx; x++) Ae.push_back({in, BK_EM, x, y, 0});
+            std::vector<BatchItem>* ph[3] = {&B, &C, &D};
+            int q = 0;
+            if (!P.per_x) { for (int x = 0; x < (int)blocks_for(ny * (nz + 1) + (ny + 1) * nz, kThreads); x++) ph[q]->push_back({in, BK_MUR_X, x, 0, 0}); q++; }
+            if (!P.per_y) { for (int x = 0; x < (int)blocks_for(nx * (nz + 1) + (nx + 1) * nz, kThreads); x++) ph[q]->push_back({in, BK_MUR_Y, x, 0, 0}); q++; }
+            if (!P.per_z) { for (int x = 0; x < (int)blocks_for(nx * (ny + 1) + (nx + 1) * ny, kThreads); x++) ph[q]->push_back({in, BK_MUR_Z, x, 0, 0}); q++; }
+        }
+        if (P.fe) {
+            const int gx = (int)blocks_for(ny * nz, kThreads);
+            for (int y = 0; y < P.nx; y++)
+                for (int x = 0; x < gx; x++) Af.push_back({in, BK_FE, x, y, 0});
+        }
+    }
+    A = At;
+    A.insert(A.end(), Ae.begin(), Ae.end());
+    A.insert(A.end(), Af.begin(), Af.end());
+}
+
+// device tables of the phase mode at chunks ch
+int batch_upload(gf_batch* b, const std::vector<int>& ch) {
+    std::vector<BatchInst> hi(b->engs.size());
+    for (size_t i = 0; i < b->engs.size(); i++) {
+        const gf_engine* e = b->engs[i];
+        BatchInst& t = hi[i];
+        std::memset(&t, 0, sizeof(t));
+        t.P = e->P;
+        for (int p = 0; p < 2; p++)
+            for (int q = 0; q < 4; q++) t.io[p][q] = e->iof[p][q];
+        t.cls = static_cast<const EmCls<float>*>(e->em_cls_tab);
+        t.ncls = e->em_ncls;
+        t.nmat = (int)e->deck.mats.size();
+        t.el_chunk = ch[i];
+        t.el_cubic = e->el_cubic ? 1 : 0;
+        t.step = e->step_ctr;
+    }
+    std::vector<BatchItem> A, At, Ae, Af, B, C, D;
+    batch_items(b, ch, A, At, Ae, Af, B, C, D);
+    if (!b->dinst) GB_CU(cudaMalloc(&b->dinst, sizeof(BatchInst) * hi.size()));
+    GB_CU(cudaMemcpy(b->dinst, hi.data(), sizeof(BatchInst) * hi.size(), cudaMemcpyHostToDevice));
+    std::vector<BatchItem> BC = B;
+    BC.insert(BC.end(), C.begin(), C.end());
+    BC.insert(BC.end(), D.begin(), D.end());
+    const std::vector<BatchItem>* L[5] = {&A, &At, &Ae, &Af, &BC};
+    for (int q = 0; q < 5; q++) {
+        if (b->ditems[q]) { cudaFree(b->ditems[q]); b->ditems[q] = nullptr; }
+        if (!L[q]->empty()) {
+            GB_CU(cudaMalloc(&b->ditems[q], sizeof(BatchItem) * L[q]->size()));
+            GB_CU(cudaMemcpy(b->ditems[q], L[q]->data(), sizeof(BatchItem) * L[q]->size(), cudaMemcpyHostToDevice));
+        }
+    }
+    b->nA = (int)A.size(); b->nAt = (int)At.size(); b->nAe = (int)Ae.size(); b->nAf = (int)Af.size();
+    b->nB = (int)B.size(); b->nC = (int)C.size(); b->nD = (int)D.size();
+    b->chunk = ch;
+    return GF_OK;
+}
+
+#define GB_PH(call)                                                                        \
+    do {                                                                                   \
+        const int ce_ = (call);                                                            \
+        if (ce_ != 0) {                                                                    \
+            b->err = std::string("batch phase launch: ") + cudaGetErrorString((cudaError_t)ce_); \
+            return GF_ECUDA;                                                               \
+        }                                                                                  \
+    } while (0)
+
+// phase A of stage s: one launch, or the tile, Yee and TDGL items as three
+// launches forked onto the batch's side streams and joined again
+int batch_phase_a(gf_batch* b, int s, int parity, cudaStream_t st) {
+    unsigned* err = b->engs[0]->tma_err;
+    if (b->split_tile) {
+        GB_CU(cudaEventRecord(b->ev[0], st));
+        GB_CU(cudaStreamWaitEvent(b->side[0], b->ev[0], 0));
+        GB_CU(cudaStreamWaitEvent(b->side[1], b->ev[0], 0));
+        GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[1], b->nAt, s, 3, parity, b->smem, err, st));
+        GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[2], b->nAe, s, 4, parity, b->smem, err, b->side[0]));
+        GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[3], b->nAf, s, 5, parity, b->smem, err, b->side[1]));
+        GB_CU(cudaEventRecord(b->ev[1], b->side[0]));
+        GB_CU(cudaEventRecord(b->ev[2], b->side[1]));
+        GB_CU(cudaStreamWaitEvent(st, b->ev[1], 0));
+        GB_CU(cudaStreamWaitEvent(st, b->ev[2], 0));
+        return GF_OK;
+    }
+    GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[0], b->nA, s, 0, parity, b->smem, err, st));
+    return GF_OK;
+}
+
+// one step of every engine in the phase mode: 4 stages x (A, B, C, D; the
+// empty ones skipped), then
+// the step counters
+int batch_enqueue_phases(gf_batch* b, int parity, cudaStream_t st) {
+    unsigned* err = b->engs[0]->tma_err;
+    for (int s = 0; s < 4; s++) {
+        GF_TRY(batch_phase_a(b, s, parity, st));
+        if (b->nB > 0) GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[4], b->nB, s, 1, parity, 0, err, st));
+        if (b->nC > 0) GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[4] + b->nB, b->nC, s, 1, parity, 0, err, st));
+        if (b->nD > 0) GB_PH(gf_mixed_batch_phase(b->dinst, b->ditems[4] + b->nB + b->nC, b->nD, s, 1, parity, 0, err, st));
+    }
+    GB_CU(launch(k_batch_step_inc, dim3(blocks_for((long)b->engs.size(), kThreads)), dim3(kThreads), 0, st,
+                 (const BatchInst*)b->dinst, (int)b->engs.size()));
+    return GF_OK;
+}
+
+// mean device time of `reps` launches of one phase-A item list of stage 0
+// (kind 3 tile, 4 Yee, 5 TDGL items)
+int batch_time_kind(gf_batch* b, int ph, int reps, float* ms) {
+    const int parity = (int)(b->engs[0]->steps_done & 1ull);
+    const int q = ph - 2;
+    const int n = ph == 3 ? b->nAt : (ph == 4 ? b->nAe : b->nAf);
+    *ms = 0.f;
+    if (n == 0) return GF_OK;
+    cudaEvent_t e0, e1;
+    GB_CU(cudaEventCreate(&e0));
+    GB_CU(cudaEventCreate(&e1));
+    int ce = gf_mixed_batch_phase(b->dinst, b->ditems[q], n, 0, ph, parity, b->smem, b->engs[0]->tma_err, b->stream);
+    if (ce == 0) ce = (int)cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < reps && ce == 0; r++)
+        ce = gf_mixed_batch_phase(b->dinst, b->ditems[q], n, 0, ph, parity, b->smem, b->engs[0]->tma_err, b->stream);
+    if (ce == 0) ce = (int)cudaEventRecord(e1, b->stream);
+    if (ce == 0) ce = (int)cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (ce == 0) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ce != 0) { b->err = std::string("batch kind timing: ") + cudaGetErrorString((cudaError_t)ce); return GF_ECUDA; }
+    *ms = t / (float)(reps > 0 ? reps : 1);
+    return GF_OK;
+}
+
+// mean device time of `reps` phase-A launches of stage 0 (they write stage-0
+// outputs and per-stage scratch only: the state is not touched)
+int batch_time_phase_a(gf_batch* b, int reps, float* ms) {
+    const int parity = (int)(b->engs[0]->steps_done & 1ull);
+    cudaEvent_t e0, e1;
+    GB_CU(cudaEventCreate(&e0));
+    GB_CU(cudaEventCreate(&e1));
+    int rc = batch_phase_a(b, 0, parity, b->stream);
+    if (rc == GF_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) rc = GF_ECUDA;
+    for (int r = 0; r < reps && rc == GF_OK; r++) rc = batch_phase_a(b, 0, parity, b->stream);
+    if (rc == GF_OK && cudaEventRecord(e1, b->stream) != cudaSuccess) rc = GF_ECUDA;
+    if (rc == GF_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = GF_ECUDA;
+    float t = 0.f;
+    if (rc == GF_OK) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != GF_OK) { if (b->err.empty()) b->err = "batch phase timing"; return rc; }
+    *ms = t / (float)(reps > 0 ? reps : 1);
+    return GF_OK;
+}
+
+// The phase mode's autotuner: the elastic tile's x-chunk per work item (one
+// chunk for every engine, capped at the engine's nx, or each engine's own
+// one-engine choice) and whether phase A is one fused launch or the tile
+// items and the others in two, from timed phase-A launches.
+int batch_tune_phases(gf_batch* b, int autotune) {
+    std::vector<int> own(b->engs.size());
+    for (size_t i = 0; i < b->engs.size(); i++) own[i] = std::max(1, b->engs[i]->el_chunk);
+    std::vector<std::vector<int>> cands = {own};
+    if (autotune)
+        for (int L : {2, 4, 8, 16, 32}) {
+            std::vector<int> c(b->engs.size());
+            for (size_t i = 0; i < b->engs.size(); i++) c[i] = std::min(L, b->engs[i]->P.nx);
+            cands.push_back(c);
+        }
+    bool any_tile = false;
+    for (gf_engine* e : b->engs) any_tile = any_tile || e->P.elastic;
+    float best = -1.f;
+    std::vector<int> best_c = own;
+    bool best_split = false;
+    std::string log;
+    for (size_t ci = 0; ci < cands.size(); ci++) {
+        if (!any_tile && ci > 0) break;
+        GF_TRY(batch_upload(b, cands[ci]));
+        for (int split = 0; split < ((autotune && any_tile) ? 2 : 1); split++) {
+            b->split_tile = split != 0;
+            float ms = 0.f;
+            GF_TRY(batch_time_phase_a(b, autotune ? 3 : 0, &ms));
+            if (!autotune) { best_c = cands[ci]; best_split = false; break; }
+            char buf[96];
+            std::snprintf(buf, sizeof(buf), "%s%s %s %.4f ms", log.empty() ? "" : "; ",
+                          ci == 0 ? "own" : ("L=" + std::to_string(cands[ci][0])).c_str(), split ? "split" : "fused", ms);
+            log += buf;
+            if (best < 0.f || ms < best) { best = ms; best_c = cands[ci]; best_split = split != 0; }
+        }
+    }
+    GF_TRY(batch_upload(b, best_c));
+    b->split_tile = best_split;
+    std::string kinds;
+    if (autotune) {
+        float tk[3] = {0.f, 0.f, 0.f};
+        for (int q = 0; q < 3; q++) GF_TRY(batch_time_kind(b, 3 + q, 3, &tk[q]));
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "; alone at the chosen chunk: tile %.4f, Yee %.4f, TDGL %.4f ms", tk[0], tk[1], tk[2]);
+        kinds = buf;
+    }
+    b->plan = "phases: " + std::to_string(b->engs.size()) + " engines, " + std::to_string(b->nA) + " phase-A, " +
+              std::to_string(b->nB) + " phase-B, " + std::to_string(b->nC) + " phase-C, " + std::to_string(b->nD) +
+              " phase-D items per stage; phase A " +
+              (best_split ? "split (tile, Yee and TDGL items in three concurrent launches)" : "fused (tile, Yee and TDGL items in one launch)") +
+              (autotune ? "; timed phase A (stage 1): " + log + kinds : std::string("; untuned (each engine's own chunk)"));
+    return GF_OK;
+}
+
+// the step graphs (one per step parity) of the phase mode (phases) or the
+// branch mode into g / gx
+int batch_capture(gf_batch* b, bool phases, cudaGraph_t* gout, cudaGraphExec_t* gxout) {
+    if (phases) {
+        for (int par = 0; par < 2; par++) {
+            GB_CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = batch_enqueue_phases(b, par, b->stream);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+            if (rc != GF_OK || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                if (rc == GF_OK) b->err = std::string("batch capture: ") + cudaGetErrorString(ce);
+                return rc != GF_OK ? rc : GF_ECUDA;
+            }
+            gout[par] = g;
+            GB_CU(cudaGraphInstantiate(&gxout[par], g, 0));
+        }
+        return GF_OK;
+    }
     for (int par = 0; par < 2; par++) {
         GB_CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int rc = GF_OK;
@@ -3040,10 +3345,108 @@ int batch_capture(gf_batch* b) {
             if (rc == GF_OK) b->err = std::string("batch capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ce2);
             return rc != GF_OK ? rc : GF_ECUDA;
         }
-        b->graph[par] = g;
-        GB_CU(cudaGraphInstantiate(&b->gexec[par], g, 0));
+        gout[par] = g;
+        GB_CU(cudaGraphInstantiate(&gxout[par], g, 0));
     }
     return GF_OK;
+}
+
+// nsteps steps of every engine with the step graphs gx: the engines' drive
+// rows uploaded per chunk, then one graph launch per step (events e0 / e1,
+// when given, around the launches of the first chunk)
+int batch_run(gf_batch* b, cudaGraphExec_t* gx, uint64_t nsteps, cudaEvent_t e0, cudaEvent_t e1) {
+    uint64_t done = 0;
+    while (done < nsteps) {
+        const uint64_t chunk = std::min<uint64_t>(nsteps - done, (uint64_t)kDriveCap / 2);
+        GB_CU(cudaStreamSynchronize(b->stream));
+        for (gf_engine* e : b->engs) {
+            for (uint64_t s = 0; s < chunk; s++) step_drive(e, e->drive_host[s]);
+            const uint64_t first = e->steps_done + done;
+            uint64_t s = 0;
+            while (s < chunk) {
+                const uint64_t slot = (first + s) & (uint64_t)(kDriveCap - 1);
+                const uint64_t run = std::min<uint64_t>(chunk - s, (uint64_t)kDriveCap - slot);
+                GB_CU(cudaMemcpyAsync(e->drive + slot, e->drive_host + s, sizeof(StepDrive) * run, cudaMemcpyHostToDevice, b->stream));
+                s += run;
+            }
+        }
+        const uint64_t first = b->engs[0]->steps_done + done;
+        if (e0 && done == 0) GB_CU(cudaEventRecord(e0, b->stream));
+        for (uint64_t k = 0; k < chunk; k++) GB_CU(cudaGraphLaunch(gx[(first + k) & 1ull], b->stream));
+        if (e1 && done == 0) GB_CU(cudaEventRecord(e1, b->stream));
+        done += chunk;
+    }
+    for (gf_engine* e : b->engs) e->steps_done += nsteps;
+    return GF_OK;
+}
+
+// Every engine's step-to-step state (the checkpoint's device arrays, the
+// device step counter, the host clock), kept on the device so that trial
+// steps can be undone.
+struct BatchSnap {
+    struct Host { uint64_t steps_done; double t_host; long presc_H, presc_E; double Hext_cur[3], Eext_cur[3]; };
+    std::vector<Host> host;
+    std::vector<std::vector<CkBlob>> blobs;
+    char* dev = nullptr;
+    size_t bytes = 0;
+};
+
+int batch_snap_take(gf_batch* b, BatchSnap& sn) {
+    sn.host.clear(); sn.blobs.clear(); sn.bytes = 0;
+    for (gf_engine* e : b->engs) {
+        sn.blobs.push_back(ck_blobs(e));
+        sn.blobs.back().push_back({"step_ctr", e->step_ctr, sizeof(unsigned long long)});
+        for (const CkBlob& c : sn.blobs.back()) sn.bytes += (c.bytes + 255) & ~(size_t)255;
+        BatchSnap::Host h;
+        h.steps_done = e->steps_done; h.t_host = e->t_host; h.presc_H = e->presc_H; h.presc_E = e->presc_E;
+        std::memcpy(h.Hext_cur, e->Hext_cur, sizeof(h.Hext_cur)); std::memcpy(h.Eext_cur, e->Eext_cur, sizeof(h.Eext_cur));
+        sn.host.push_back(h);
+    }
+    GB_CU(cudaMalloc(&sn.dev, sn.bytes));
+    size_t off = 0;
+    for (const auto& bl : sn.blobs)
+        for (const CkBlob& c : bl) {
+            GB_CU(cudaMemcpyAsync(sn.dev + off, c.dev, c.bytes, cudaMemcpyDeviceToDevice, b->stream));
+            off += (c.bytes + 255) & ~(size_t)255;
+        }
+    GB_CU(cudaStreamSynchronize(b->stream));
+    return GF_OK;
+}
+
+int batch_snap_put(gf_batch* b, const BatchSnap& sn) {
+    GB_CU(cudaStreamSynchronize(b->stream));
+    size_t off = 0;
+    for (size_t i = 0; i < b->engs.size(); i++) {
+        for (const CkBlob& c : sn.blobs[i]) {
+            GB_CU(cudaMemcpyAsync(c.dev, sn.dev + off, c.bytes, cudaMemcpyDeviceToDevice, b->stream));
+            off += (c.bytes + 255) & ~(size_t)255;
+        }
+        gf_engine* e = b->engs[i];
+        const BatchSnap::Host& h = sn.host[i];
+        e->steps_done = h.steps_done; e->t_host = h.t_host; e->presc_H = h.presc_H; e->presc_E = h.presc_E;
+        std::memcpy(e->Hext_cur, h.Hext_cur, sizeof(h.Hext_cur)); std::memcpy(e->Eext_cur, h.Eext_cur, sizeof(h.Eext_cur));
+    }
+    GB_CU(cudaStreamSynchronize(b->stream));
+    return GF_OK;
+}
+
+// device time per step of `steps` steps with graphs gx after two warm-up
+// steps, the state restored before each run and at the end
+int batch_trial(gf_batch* b, const BatchSnap& sn, cudaGraphExec_t* gx, int steps, float* ms) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GB_CU(cudaEventCreate(&e0));
+    GB_CU(cudaEventCreate(&e1));
+    int rc = batch_snap_put(b, sn);
+    if (rc == GF_OK) rc = batch_run(b, gx, 2, nullptr, nullptr);
+    if (rc == GF_OK) rc = batch_snap_put(b, sn);
+    if (rc == GF_OK) rc = batch_run(b, gx, (uint64_t)steps, e0, e1);
+    float t = 0.f;
+    if (rc == GF_OK && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+    if (rc == GF_OK) rc = batch_snap_put(b, sn);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / (float)steps;
+    return rc;
 }
 
 }  // namespace
@@ -3051,7 +3454,13 @@ int batch_capture(gf_batch* b) {
 extern "C" {
 
 int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out) {
+    return gf_batch_create_ex(engines, count, autotune, GF_BATCH_AUTO, out);
+}
+
+int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int mode, gf_batch** out) {
     if (!engines || count < 1 || !out) { g_create_err = "gf_batch_create: need engines, count >= 1 and an output"; return GF_EINVAL; }
+    if (mode != GF_BATCH_AUTO && mode != GF_BATCH_BRANCHES && mode != GF_BATCH_PHASES)
+        { g_create_err = "gf_batch_create_ex: unknown mode"; return GF_EINVAL; }
     *out = nullptr;
     gf_batch* b = new gf_batch();
     b->device = engines[0]->device;
@@ -3075,14 +3484,70 @@ int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) { b->err = "event"; return fail(GF_ECUDA); }
     for (gf_engine* e : b->engs)
         if (cudaStreamSynchronize(e->stream) != cudaSuccess) { b->err = "engine stream"; return fail(GF_ECUDA); }
-    if (autotune)
-        for (gf_engine* e : b->engs)
-            if (e->P.elastic) {
-                int rc = autotune_tile(b, e);
-                if (rc != GF_OK) return fail(rc);
-            }
-    int rc = batch_capture(b);
+    std::string blocker;
+    for (gf_engine* e : b->engs)
+        if (blocker.empty()) blocker = batch_phase_blocker(e);
+    if (mode == GF_BATCH_PHASES && !blocker.empty()) { b->err = "gf_batch_create_ex: phase mode: " + blocker; return fail(GF_EUNSUPPORTED); }
+    b->phases = mode != GF_BATCH_BRANCHES && blocker.empty();
+    // with GF_BATCH_AUTO and autotune, both modes are built and timed below
+    const bool choose = b->phases && mode == GF_BATCH_AUTO && autotune;
+    if (b->phases) {
+        for (int q = 0; q < 2; q++)
+            if (cudaStreamCreateWithFlags(&b->side[q], cudaStreamNonBlocking) != cudaSuccess) { b->err = "stream"; return fail(GF_ECUDA); }
+        for (int q = 0; q < 3; q++)
+            if (cudaEventCreateWithFlags(&b->ev[q], cudaEventDisableTiming) != cudaSuccess) { b->err = "event"; return fail(GF_ECUDA); }
+        int nmat = 1;
+        for (gf_engine* e : b->engs) nmat = std::max(nmat, (int)e->deck.mats.size());
+        b->smem = batch_smem_bytes(nmat);
+        if (gf_mixed_batch_attr(b->smem) != GF_OK) { b->err = "batch kernels: shared-memory attribute"; return fail(GF_ECUDA); }
+        int rc = batch_tune_phases(b, autotune);
+        if (rc != GF_OK) return fail(rc);
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) { b->err = "batch tuning"; return fail(GF_ECUDA); }
+    }
+    if (!b->phases || choose) {
+        if (!b->phases)
+            b->plan = "branches: one graph branch per engine" + (blocker.empty() ? std::string() : " (phase mode: " + blocker + ")");
+        if (autotune)
+            for (gf_engine* e : b->engs)
+                if (e->P.elastic) {
+                    int rc = autotune_tile(b, e);
+                    if (rc != GF_OK) return fail(rc);
+                }
+    }
+    int rc = batch_capture(b, b->phases, b->graph, b->gexec);
     if (rc != GF_OK) return fail(rc);
+    if (choose) {
+        // the fusion choice: one graph branch per engine or the phase
+        // launches over all engines, from timed steps whose state is undone
+        cudaGraph_t g2[2] = {nullptr, nullptr};
+        cudaGraphExec_t gx2[2] = {nullptr, nullptr};
+        auto drop = [](cudaGraph_t* g, cudaGraphExec_t* x) {
+            for (int p = 0; p < 2; p++) {
+                if (x[p]) cudaGraphExecDestroy(x[p]);
+                if (g[p]) cudaGraphDestroy(g[p]);
+                x[p] = nullptr; g[p] = nullptr;
+            }
+        };
+        rc = batch_capture(b, false, g2, gx2);
+        BatchSnap sn;
+        float t_ph = 0.f, t_br = 0.f;
+        if (rc == GF_OK) rc = batch_snap_take(b, sn);
+        if (rc == GF_OK) rc = batch_trial(b, sn, b->gexec, 4, &t_ph);
+        if (rc == GF_OK) rc = batch_trial(b, sn, gx2, 4, &t_br);
+        if (sn.dev) cudaFree(sn.dev);
+        if (rc != GF_OK) { drop(g2, gx2); return fail(rc); }
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "; timed steps: phases %.4f ms, branches %.4f ms", t_ph, t_br);
+        if (t_br < t_ph) {
+            drop(b->graph, b->gexec);
+            for (int p = 0; p < 2; p++) { b->graph[p] = g2[p]; b->gexec[p] = gx2[p]; }
+            b->phases = false;
+            b->plan = "branches: one graph branch per engine (chosen over the " + b->plan + ")" + buf;
+        } else {
+            drop(g2, gx2);
+            b->plan += buf;
+        }
+    }
     *out = b;
     return GF_OK;
 }
@@ -3090,28 +3555,7 @@ int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch
 int gf_batch_advance(gf_batch* b, uint64_t nsteps) {
     if (!b) return GF_EINVAL;
     GB_CU(cudaSetDevice(b->device));
-    uint64_t done = 0;
-    while (done < nsteps) {
-        const uint64_t chunk = std::min<uint64_t>(nsteps - done, (uint64_t)kDriveCap / 2);
-        GB_CU(cudaStreamSynchronize(b->stream));
-        // every engine's drive rows for the chunk, uploaded on the batch stream
-        for (gf_engine* e : b->engs) {
-            for (uint64_t s = 0; s < chunk; s++) step_drive(e, e->drive_host[s]);
-            const uint64_t first = e->steps_done + done;
-            uint64_t s = 0;
-            while (s < chunk) {
-                const uint64_t slot = (first + s) & (uint64_t)(kDriveCap - 1);
-                const uint64_t run = std::min<uint64_t>(chunk - s, (uint64_t)kDriveCap - slot);
-                GB_CU(cudaMemcpyAsync(e->drive + slot, e->drive_host + s, sizeof(StepDrive) * run, cudaMemcpyHostToDevice, b->stream));
-                s += run;
-            }
-        }
-        const uint64_t first = b->engs[0]->steps_done + done;
-        for (uint64_t k = 0; k < chunk; k++) GB_CU(cudaGraphLaunch(b->gexec[(first + k) & 1ull], b->stream));
-        done += chunk;
-    }
-    for (gf_engine* e : b->engs) e->steps_done += nsteps;
-    return GF_OK;
+    return batch_run(b, b->gexec, nsteps, nullptr, nullptr);
 }
 
 int gf_batch_synchronize(gf_batch* b) {
@@ -3124,8 +3568,11 @@ void* gf_batch_stream(gf_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 int gf_batch_tuned_chunk(const gf_batch* b, int index) {
     if (!b || index < 0 || index >= (int)b->engs.size()) return -1;
+    if (b->phases) return b->chunk[(size_t)index];
     return b->engs[(size_t)index]->el_chunk;
 }
+
+const char* gf_batch_plan(const gf_batch* b) { return b ? b->plan.c_str() : ""; }
 
 const char* gf_batch_last_error(const gf_batch* b) { return b ? b->err.c_str() : g_create_err.c_str(); }
 
@@ -3139,6 +3586,10 @@ void gf_batch_destroy(gf_batch* b) {
     for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
+    for (cudaStream_t q : b->side) if (q) cudaStreamDestroy(q);
+    for (cudaEvent_t ev : b->ev) if (ev) cudaEventDestroy(ev);
+    if (b->dinst) cudaFree(b->dinst);
+    for (BatchItem* p : b->ditems) if (p) cudaFree(p);
     delete b;
 }
 

@@ -425,7 +425,7 @@ __device__ __forceinline__ void fe_rk(const Params& P, const StageIOT<R>& io, in
     }
 }
 
-template <int S, class R = double, bool FX = false>
+template <int S, class R, bool FX>
 // FX: the run has flexoelectricity (the polarisation- and strain-gradient
 // terms of get_dq_RK*, ferroelectric_solver.cpp:800-833).
 // FP64 (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4
@@ -433,11 +433,11 @@ template <int S, class R = double, bool FX = false>
 // all three components gathered before the first store: 0.61 ms (FP64) and
 // 0.41 ms (FP32) per step on the 128^3 ferroelectric workload, against 0.79
 // and 0.49 at (256, 2) and (256, 3)
-__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_FE_MINB_F64) k_fe(Params P, StageIOT<R> io) {
+__device__ __forceinline__ void fe_body(const Params& P, const StageIOT<R>& io, int bx, int by) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= ny * nz) return;
-    const int i = blockIdx.y, j = t / nz, k = t - (t / nz) * nz;
+    const int i = by, j = t / nz, k = t - (t / nz) * nz;
     const int c = (i * ny + j) * nz + k;
     const uint8_t id = io.mid[c];
     R dq[3] = {R(0.), R(0.), R(0.)};
@@ -513,6 +513,13 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_
         fe_dq<S, R, FX>(P, io, i, j, k, c, mt, pxg, pyg, pzg, lap, edyn, d2s, dp, nb, idn, dq);
     }
     fe_rk<S, R>(P, io, c, dq);
+}
+
+
+// block (bx, by): 256 cells of the (j, k) plane bx of x-plane by
+template <int S, class R = double, bool FX = false>
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_FE_MINB_F32 : GF_FE_MINB_F64) k_fe(Params P, StageIOT<R> io) {
+    fe_body<S, R, FX>(P, io, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace gf

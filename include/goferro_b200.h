@@ -390,17 +390,36 @@ const char* gf_last_error(const gf_engine* e);
 void gf_destroy(gf_engine* e);
 
 /* ---- Batched runs --------------------------------------------------------
- * Many engines (uneven grids, either precision) advanced together: each
- * engine's RK4 step is one branch of a single CUDA graph per step parity, so
- * one graph launch advances every instance and small instances run
- * concurrently.  With autotune != 0 the batch first picks, per engine, the
- * x-chunk of the tiled elastic kernel by timing it (the state is not
- * touched; chunking does not change results).  The engines stay owned by
- * the caller and must not be advanced by other calls while the batch lives;
- * all must sit at steps of the same parity.  The reference runs one system
- * per process; these entry points have no counterpart there. */
+ * Many engines (uneven grids, either precision) advanced together by one
+ * CUDA graph per step parity, in one of two modes:
+ *  - phases (GF_BATCH_PHASES): mixed-form engines with TDGL, elastodynamics
+ *    and FDTD (Mur boundaries; no magnetism, flexoelectricity, static
+ *    solves, plane sources, conductors or Drude poles).  Each RK stage is a
+ *    few launches for all engines together — A: elastic tiles, Yee update
+ *    and TDGL; B: elastic RK update and the first Mur face direction; C:
+ *    elastic boundary planes and the second; D: the third — over lists of
+ *    work items (engine, kernel, block), so small grids share the GPU inside
+ *    one launch; the launch count per step does not grow with the engine
+ *    count (13 for periodic-in-x-and-y decks).  With autotune != 0 the batch
+ *    times phase A of stage 1 (which touches no state) for the elastic
+ *    tile's x-chunk per item (one chunk for all engines or each engine's
+ *    own) and for phase A fused into one launch or split into three
+ *    concurrent launches (tile, Yee and TDGL items), and keeps the fastest;
+ *    gf_batch_plan describes the choice.
+ *  - branches (GF_BATCH_BRANCHES): any engines; each engine's RK4 step is
+ *    one branch of the graph.  With autotune != 0 the batch first picks, per
+ *    engine, the x-chunk of the tiled elastic kernel by timing it.
+ * GF_BATCH_AUTO takes phases when every engine allows it, else branches.
+ * Chunking does not change results.  The engines stay owned by the caller
+ * and must not be advanced by other calls while the batch lives; all must
+ * sit at steps of the same parity.  The reference runs one system per
+ * process; these entry points have no counterpart there. */
 typedef struct gf_batch gf_batch;
-int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out);
+#define GF_BATCH_AUTO 0
+#define GF_BATCH_BRANCHES 1
+#define GF_BATCH_PHASES 2
+int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out);   /* GF_BATCH_AUTO */
+int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int mode, gf_batch** out);
 /* Advance every engine by nsteps (asynchronous on the batch stream). */
 int gf_batch_advance(gf_batch* b, uint64_t nsteps);
 int gf_batch_synchronize(gf_batch* b);
@@ -408,6 +427,8 @@ int gf_batch_synchronize(gf_batch* b);
 void* gf_batch_stream(gf_batch* b);
 /* Elastic-tile x-chunk engine `index` runs with (-1: bad index). */
 int gf_batch_tuned_chunk(const gf_batch* b, int index);
+/* The batch's mode and tuning choices, as text (valid while b lives). */
+const char* gf_batch_plan(const gf_batch* b);
 /* Message of the last failing batch call (or failed create when b is NULL). */
 const char* gf_batch_last_error(const gf_batch* b);
 /* Free the batch (not the engines). */
