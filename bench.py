@@ -488,11 +488,12 @@ def adjoint_cost(gf, torch, args, local_rank):
     reverse sweep).  The mixed entry also gives the relative difference of
     its gradients from the FP64 adjoint's on the same inputs."""
     mu0 = 1.256637061e-6
-    steps, K, nw = args.adjoint_steps, 200, 256
+    steps, K, nw = args.adjoint_steps, args.adjoint_checkpoint, 256
+    gx, gy, gz = (int(v) for v in args.adjoint_grid.lower().split("x"))
     out = {}
     grads = {}
     with tempfile.TemporaryDirectory() as tmp:
-        d = gf.decks.preset_fm_demag(nx=256, ny=256, nz=32, steps=steps)
+        d = gf.decks.preset_fm_demag(nx=gx, ny=gy, nz=gz, steps=steps)
         d.Hext_table = None
         d.Hext_stat = (0.0, 0.0, 1.0 / mu0)
         d.materials = [gf.decks.yig(1e-3, magnetoelastic=True)]
@@ -549,7 +550,7 @@ def adjoint_cost(gf, torch, args, local_rank):
     (gw, ga), (gw64, ga64) = grads["mixed"], grads["fp64"]
     out["mixed"]["grad_wave_rel_diff_vs_fp64"] = float(np.max(np.abs(gw - gw64)) / max(np.max(np.abs(gw64)), 1e-300))
     out["mixed"]["grad_alpha_rel_diff_vs_fp64"] = float(np.max(np.abs(ga - ga64)) / max(np.max(np.abs(ga64)), 1e-300))
-    out["workload"] = ("FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, 256x256x32, "
+    out["workload"] = (f"FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, {gx}x{gy}x{gz}, "
                        "per-cell alpha and 256-sample waveform; FP32 mixed (the configuration's form) and FP64")
     out["timing"] = "device time (CUDA events on the engine stream)"
     out["definition"] = ("backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
@@ -828,6 +829,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--sweep-steps", type=int, default=100)
     ap.add_argument("--adjoint-steps", type=int, default=400)
+    ap.add_argument("--adjoint-grid", default="256x256x32", help="grid of the adjoint cost measurement (NXxNYxNZ)")
+    ap.add_argument("--adjoint-checkpoint", type=int, default=200, help="steps between the adjoint's stored states")
     args = ap.parse_args()
     global GRID_OVERRIDE
     if args.grid:

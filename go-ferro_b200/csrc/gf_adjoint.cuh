@@ -162,14 +162,28 @@ __global__ void __launch_bounds__(256) k_adj_eval(Params P, const uint8_t* __res
     }
 }
 
+// RK4 reverse-sweep combination of one component after the VJP of stage s
+// (0-based), fused into the kernel that forms the final ybar of its group:
+// lamacc := lacc0 + yb (lacc0 = lambda at stage 4, the running sum after),
+// and the cotangent u of the next (earlier) stage's increment:
+// u3 = lambda/3 + ybar4, u2 = lambda/3 + ybar3/2, u1 = lambda/6 + ybar2/2
+template <class R>
+__device__ __forceinline__ void adj_comb1(int s, R l, R lacc0, R yb, R* lamacc, R* u, int c) {
+    lamacc[c] = lacc0 + yb;
+    if (s == 3) u[c] = l / R(3) + yb;
+    else if (s == 2) u[c] = l / R(3) + yb * R(0.5);
+    else if (s == 1) u[c] = l / R(6) + yb * R(0.5);
+}
+
 // Local part of the vector-Jacobian product of stage s: the cross products,
-// the anisotropy Jacobian, the damping derivative; writes ybar (local part),
-// Hbar and Hbar_x (for the waveform reduction); adds alphabar (FP64 in both
-// forms: it sums over every stage of the run).
+// the anisotropy Jacobian, the damping derivative; writes ybar (local part)
+// and Hbar; adds alphabar and Hbar_x (the waveform gradient's per-cell sum)
+// in FP64 in both forms (they sum over many stages).  The increment's
+// cotangent is us * u (u = lambda and us = 1/6 at stage 4).
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
-                                                 F3T<R> y, F3T<R> hs, F3T<R> u, const R* __restrict__ alpha, F3T<R> ybar,
-                                                 F3T<R> hbar, double* __restrict__ abar, R* __restrict__ hbx, C6T<R> str,
+                                                 F3T<R> y, F3T<R> hs, F3T<R> u, R us, const R* __restrict__ alpha, F3T<R> ybar,
+                                                 F3T<R> hbar, double* __restrict__ abar, double* __restrict__ hacc, C6T<R> str,
                                                  C6T<R> strbar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
@@ -178,13 +192,14 @@ __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __rest
     if (!(id != 0 && am[id - 1].fm)) {
         st3(ybar, c, mk3<R>(z, z, z));
         st3(hbar, c, mk3<R>(z, z, z));
-        hbx[c] = z;
         if (strbar.c[0])
             for (int q = 0; q < 6; q++) strbar.c[q][c] = z;
         return;
     }
     const AdjMatT<R>& mt = am[id - 1];
-    const V3<R> m = ld3(y, c), H = ld3(hs, c), w = ld3(u, c);
+    const V3<R> m = ld3(y, c), H = ld3(hs, c);
+    V3<R> w = ld3(u, c);
+    w.x *= us; w.y *= us; w.z *= us;
     const R a = alpha[c];
     const R c1 = -mt.gdt / (R(1) + a * a), c2 = a * c1;
     const R dc1 = c1 * (R(-2) * a / (R(1) + a * a)), dc2 = c1 + a * dc1;
@@ -228,7 +243,7 @@ __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __rest
     }
     st3(ybar, c, mb);
     st3(hbar, c, hb);
-    hbx[c] = hb.x;
+    hacc[c] += (double)hb.x;
 }
 
 // ---------------------------------------------------------------------------
@@ -243,34 +258,39 @@ __global__ void __launch_bounds__(256) k_adj_vjp(Params P, const uint8_t* __rest
 // below transposes each of these maps.
 // ---------------------------------------------------------------------------
 
-// Cotangents of the elastic increments of stage S: uku, ukv = d loss /
-// d k_u, d k_v.  v-stage cotangent ybar_v = dt uku; force cotangent fbar;
-// lamacc_v += md ukv (k_v reads the step value v_x); the stage-1 force
-// collects -sd w ukv of the later stages (f0bar) and, at stage 1, the
-// cotangent phi of the next step's fs; phi_new = -sd ukv (stage 1 reads fs).
+// Cotangents of the elastic increments of stage S: us uku, us ukv = d loss /
+// d k_u, d k_v (uk = lambda and us = 1/6 at stage 4).  v-stage cotangent
+// ybar_v = dt uku; force cotangent fbar; lamacc_v gets md ukv (k_v reads the
+// step value v_x); the stage-1 force collects -sd w ukv of the later stages
+// (f0bar) and, at stage 1, the cotangent phi of the next step's fs;
+// phi_new = -sd ukv (stage 1 reads fs).  ybar_v is final here, so the v
+// group's RK combination (adj_comb1) follows in the same thread.
 template <int S, class R>
 __global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __restrict__ mid, const DevMatT<R>* __restrict__ mats,
-                                                   F3T<R> uku, F3T<R> ukv, F3T<R> ybar_v, F3T<R> fbar, F3T<R> lamacc_v,
-                                                   F3T<R> f0bar, F3T<R> phi, F3T<R> phi_new) {
+                                                   F3T<R> uku, F3T<R> ukv, R us, F3T<R> fbar, F3T<R> lam_v, F3T<R> lamacc_v,
+                                                   F3T<R> u_v, F3T<R> f0bar, F3T<R> phi, F3T<R> phi_new) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const uint8_t id = mid[c];
     const R dt = is_mixed<R>::value ? R(P.f.dt) : R(P.dt);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        ybar_v.c[a][c] = dt * uku.c[a][c];
+        const R yb = dt * (uku.c[a][c] * us);
+        const R g = ukv.c[a][c] * us;
+        const R l = lam_v.c[a][c];
+        R lacc = (S == 3) ? l : lamacc_v.c[a][c];
         R fb = R(0), pn = R(0);
         if (id != 0) {
             const DevMatT<R>& mt = mats[id - 1];
             const R w = (S == 1 || S == 2) ? R(2) : R(1);
-            const R g = ukv.c[a][c];
             fb = (mt.dens_dt + mt.stiff_damp * w) * g;
-            lamacc_v.c[a][c] += mt.mass_damp * g;
+            lacc += mt.mass_damp * g;
             if (S > 0) f0bar.c[a][c] += -mt.stiff_damp * w * g;
             else { fb += f0bar.c[a][c] + phi.c[a][c]; pn = -mt.stiff_damp * g; }
         }
         fbar.c[a][c] = fb;
         if (S == 0) phi_new.c[a][c] = pn;
+        adj_comb1<R>(S, l, lacc, yb, lamacc_v.c[a], u_v.c[a], c);
     }
 }
 
@@ -291,9 +311,12 @@ __global__ void __launch_bounds__(256) k_adj_el_vjp(Params P, const uint8_t* __r
 // The eigenstrain cotangent -st (x2 for shears) goes through the
 // magnetostriction e0_aa = 1.5 l100 (m_a^2 - 1/3), e0_ab = 1.5 l111 m_a m_b
 // into ybar_m (back: the run feeds the eigenstrain back).
+// With elastodynamics ybar_m is final here: the m group's RK combination
+// (adj_comb1 at stage s: lam_m, lamacc_m, u_m) follows in the same thread.
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __restrict__ mid, const DevMatT<R>* __restrict__ mats,
-                                                  F3T<R> fbar, C6T<R> strbar, F3T<R> m, F3T<R> ybar_m, int back, R* __restrict__ to) {
+                                                  F3T<R> fbar, C6T<R> strbar, F3T<R> m, F3T<R> ybar_m, int back, R* __restrict__ to,
+                                                  int s, F3T<R> lam_m, F3T<R> lamacc_m, F3T<R> u_m) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long n = P.n;
@@ -368,6 +391,11 @@ __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __re
         }
     }
 #pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const R l = lam_m.c[a][c];
+        adj_comb1<R>(s, l, s == 3 ? l : lamacc_m.c[a][c], ybar_m.c[a][c], lamacc_m.c[a], u_m.c[a], c);
+    }
+#pragma unroll
     for (int d = 0; d < 3; d++)
 #pragma unroll
         for (int a = 0; a < 3; a++) to[(d * 3 + a) * n + c] = T[d][a];
@@ -381,9 +409,11 @@ __global__ void __launch_bounds__(256) k_adj_el_p1(Params P, const uint8_t* __re
 // not stress-free (T of the two cells plus O of each side), then
 // ubar_a(c) = sum_d (gbar_d(lower face) - gbar_d(upper face)) / h_d
 // (g = (u(upper cell) - u(lower cell)) / h).  Written to ybar_u.
+// ybar_u is final here: the u group's RK combination (adj_comb1 at stage s)
+// follows in the same thread instead of a store of ybar_u.
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_t* __restrict__ mid, const R* __restrict__ to,
-                                                  F3T<R> ybar_u) {
+                                                  int s, F3T<R> lam_u, F3T<R> lamacc_u, F3T<R> u_u) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     const long n = P.n;
@@ -413,7 +443,10 @@ __global__ void __launch_bounds__(256) k_adj_el_p2(Params P, const uint8_t* __re
         }
     }
 #pragma unroll
-    for (int a = 0; a < 3; a++) ybar_u.c[a][c] = ub[a];
+    for (int a = 0; a < 3; a++) {
+        const R l = lam_u.c[a][c];
+        adj_comb1<R>(s, l, s == 3 ? l : lamacc_u.c[a][c], ub[a], lamacc_u.c[a], u_u.c[a], c);
+    }
 }
 
 // Liao extrapolation after the step (forward): the history slot of this
@@ -460,17 +493,25 @@ __global__ void k_adj_liao_T(Params P, F3T<R> lam, R* __restrict__ pend, unsigne
     const double wd = P.liao_w;
     const R w = R(wd);
     const R c1 = R(4. * wd + 2. * (1. - wd)), c2 = R(6. * wd + (1. - wd)), c3 = R(4. * wd);
-    auto at = [&](unsigned long long target, int a, int p) -> R& {
-        return pend[((size_t)((target & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
+    // every load before the first store (the parked values of the four
+    // target steps do not alias, but the compiler cannot know it)
+    auto off = [&](unsigned long long target, int a, int p) -> size_t {
+        return ((size_t)((target & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t;
     };
+    const R coef[4] = {c1, -c2, c3, -w};
+    R L[3], pv[3][4];
+#pragma unroll
     for (int a = 0; a < 3; a++) {
-        const long b0 = cid(P, i, j, 0);
-        const R L = lam.c[a][b0];
-        lam.c[a][b0] = R(0);
-        at(step, a, 1) += c1 * L;
-        if (step >= 1) at(step - 1, a, 2) += -c2 * L;
-        if (step >= 2) at(step - 2, a, 3) += c3 * L;
-        if (step >= 3) at(step - 3, a, 4) += -w * L;
+        L[a] = lam.c[a][cid(P, i, j, 0)];
+#pragma unroll
+        for (int p = 1; p <= 4; p++) pv[a][p - 1] = (step >= (unsigned long long)(p - 1)) ? pend[off(step - (p - 1), a, p)] : R(0);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        lam.c[a][cid(P, i, j, 0)] = R(0);
+#pragma unroll
+        for (int p = 1; p <= 4; p++)
+            if (step >= (unsigned long long)(p - 1)) pend[off(step - (p - 1), a, p)] = pv[a][p - 1] + coef[p - 1] * L[a];
     }
 }
 
@@ -482,25 +523,33 @@ __global__ void k_adj_liao_pend(Params P, F3T<R> lam, R* __restrict__ pend, unsi
     const long plane = (long)P.nx * P.ny;
     if (t >= plane) return;
     const long i = t / P.ny, j = t - i * P.ny;
+    R v[3][4], l[3][4];
+#pragma unroll
     for (int a = 0; a < 3; a++)
+#pragma unroll
         for (int p = 1; p <= 4; p++) {
-            R& v = pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
-            lam.c[a][cid(P, i, j, p)] += v;
-            v = R(0);
+            v[a][p - 1] = pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t];
+            l[a][p - 1] = lam.c[a][cid(P, i, j, p)];
+        }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int p = 1; p <= 4; p++) {
+            lam.c[a][cid(P, i, j, p)] = l[a][p - 1] + v[a][p - 1];
+            pend[((size_t)((step & 3ull) * 3 + a) * 4 + (p - 1)) * plane + t] = R(0);
         }
 }
 
 // ybar += transposed exchange of Hbar: sum_f w_cf (ex_f Hbar_f - ex_c Hbar_c);
 // and ybar += Ms R where R is the demag convolution of Hbar (3 x n, the
-// inverse-transform output), for ferromagnetic cells
+// inverse-transform output), for ferromagnetic cells.  With comb != 0 (no
+// elastodynamics) ybar is final here and the m group's RK combination
+// (adj_comb1 at stage s) follows for every cell instead of a store of ybar.
 template <class R>
-__global__ void __launch_bounds__(256) k_adj_field_T(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
-                                                     const R* __restrict__ aij, int nmat, F3T<R> hbar, const R* __restrict__ Rk,
-                                                     F3T<R> ybar) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
+__device__ __forceinline__ void adj_field_T_cell(const Params& P, const uint8_t* __restrict__ mid,
+                                                 const AdjMatT<R>* __restrict__ am, const R* __restrict__ aij, int nmat,
+                                                 F3T<R> hbar, const R* __restrict__ Rk, int c, V3<R>& yb) {
     const uint8_t id = mid[c];
-    if (!(id != 0 && am[id - 1].fm)) return;
     const int nyz = P.ny * P.nz;
     const int i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
     AdjNbr<R> n;
@@ -517,10 +566,30 @@ __global__ void __launch_bounds__(256) k_adj_field_T(Params P, const uint8_t* __
         s.y += n.w[f] * (ef * hf.y - ec * hc.y);
         s.z += n.w[f] * (ef * hf.z - ec * hc.z);
     }
-    V3<R> yb = ld3(ybar, c);
     yb.x += s.x; yb.y += s.y; yb.z += s.z;
     if (Rk) { yb.x += Ms * Rk[c]; yb.y += Ms * Rk[P.n + c]; yb.z += Ms * Rk[2 * P.n + c]; }
-    st3(ybar, c, yb);
+}
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_field_T(Params P, const uint8_t* __restrict__ mid, const AdjMatT<R>* __restrict__ am,
+                                                     const R* __restrict__ aij, int nmat, F3T<R> hbar, const R* __restrict__ Rk,
+                                                     F3T<R> ybar, int comb, int s, F3T<R> lam, F3T<R> lamacc, F3T<R> u) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n) return;
+    const uint8_t id = mid[c];
+    const bool fm = id != 0 && am[id - 1].fm;
+    if (!fm && !comb) return;
+    V3<R> yb = ld3(ybar, c);
+    if (fm) adj_field_T_cell<R>(P, mid, am, aij, nmat, hbar, Rk, c, yb);
+    if (!comb) {
+        st3(ybar, c, yb);
+        return;
+    }
+    const R ybv[3] = {yb.x, yb.y, yb.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const R l = lam.c[a][c];
+        adj_comb1<R>(s, l, s == 3 ? l : lamacc.c[a][c], ybv[a], lamacc.c[a], u.c[a], c);
+    }
 }
 
 // Hbar (3 x n arrays) into the contiguous FFT input
@@ -529,30 +598,6 @@ __global__ void k_adj_pack(Params P, F3T<R> v, R* out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n) return;
     out[c] = v.c[0][c]; out[P.n + c] = v.c[1][c]; out[2 * P.n + c] = v.c[2][c];
-}
-
-// RK4 reverse sweep after the VJP of stage S (0-based): lamacc += ybar and the
-// cotangent of the next (earlier) stage's increment
-template <int S, class R>
-__global__ void k_adj_comb(Params P, F3T<R> lam, F3T<R> lamacc, F3T<R> u, F3T<R> ybar) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const R yb = ybar.c[a][c], l = lam.c[a][c];
-        lamacc.c[a][c] = lamacc.c[a][c] + yb;
-        if (S == 3) u.c[a][c] = l / R(3) + yb;
-        else if (S == 2) u.c[a][c] = l / R(3) + yb * R(0.5);
-        else if (S == 1) u.c[a][c] = l / R(6) + yb * R(0.5);
-    }
-}
-
-// v *= f (3 x n)
-template <class R>
-__global__ void k_scale_f3(Params P, F3T<R> v, R f) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n) return;
-    v.c[0][c] *= f; v.c[1][c] *= f; v.c[2][c] *= f;
 }
 
 // lambda_x += g / NFM on ferromagnetic cells (d loss / d <m_x> of one step)

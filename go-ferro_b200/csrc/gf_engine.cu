@@ -3638,7 +3638,7 @@ struct gf_adjoint {
     // cotangents: m (0-2), u (3-5), v (6-8)
     double* LAM[9] = {}; double* LAMACC[9] = {}; double* U[9] = {};
     double* YBAR[9] = {}; double* HBAR[3] = {};
-    double* abar = nullptr; double* hbx = nullptr; double* wbar = nullptr;
+    double* abar = nullptr; double* hacc = nullptr; double* wbar = nullptr;   // FP64: alpha gradient, per-cell Hbar_x sum, waveform gradient
     // elastodynamics: stage u, v (stages 2-4), RK accumulators, the stage
     // force, the stage strain (LLG field), the cotangents of the force, the
     // stage-1 force of this step (f0bar) and of fs (phi), the transposed
@@ -3895,7 +3895,7 @@ int adj_stages(gf_adjoint* a, double* const* x, uint64_t step, F3T<R> xout, F3T<
 // writing it in the same thread; then the Liao extrapolation of u(k = 0)
 // and the new u, v from the accumulators
 template <class R>
-int adj_step_forward(gf_adjoint* a, double* const* x, uint64_t step) {
+int adj_step_forward(gf_adjoint* a, double** x, uint64_t step) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     GF_TRY(adj_stages<R>(a, x, step, v3<R>(x), a->f32 ? v3<R>(x + 12) : F3T<R>{}));
@@ -3903,10 +3903,8 @@ int adj_step_forward(gf_adjoint* a, double* const* x, uint64_t step) {
         const long plane = (long)P.nx * P.ny;
         GF_CU(launch(k_adj_liao<R>, dim3(blocks_for(plane, kThreads)), dim3(kThreads), 0, eng->stream, P, v3<R>(x + 3),
                      v3<R>(a->UACC), a->f32 ? v3<R>(x + 15) : F3T<R>{}, rp<R>(a->hist), rp<R>(a->last), (unsigned long long)step));
-        for (int c = 0; c < 3; c++) {
-            GF_CU(cudaMemcpyAsync(x[3 + c], a->UACC[c], a->esz * P.n, cudaMemcpyDeviceToDevice, eng->stream));
-            GF_CU(cudaMemcpyAsync(x[6 + c], a->VACC[c], a->esz * P.n, cudaMemcpyDeviceToDevice, eng->stream));
-        }
+        // the new u, v are the accumulators: exchange the buffers
+        for (int c = 0; c < 3; c++) { std::swap(x[3 + c], a->UACC[c]); std::swap(x[6 + c], a->VACC[c]); }
     }
     return GF_OK;
 }
@@ -3934,30 +3932,33 @@ int adj_mean_x(gf_adjoint* a, const double* x0, long slot) {
     return GF_OK;
 }
 
-int adj_wave_add(gf_adjoint* a, long seg) {
+// the waveform gradient of segment seg: the deterministic sum over cells of
+// the per-cell Hbar_x sums of its steps, then those sums cleared
+int adj_wave_flush(gf_adjoint* a, long seg) {
     gf_engine* eng = a->eng;
-    double* p3 = nullptr;
-    GF_TRY(adj_sum(a, a->hbx, p3));
-    GF_CU(launch(k_adj_add_slot, dim3(1), dim3(1), 0, eng->stream, a->wbar, seg, (const double*)p3));
+    cudaStream_t st = eng->stream;
+    double* p1 = eng->scratch + eng->scratch_main;
+    double* p2 = p1 + 8192;
+    double* p3 = p2 + 64;
+    GF_CU(launch(k_sum_stride, dim3(32), dim3(256), 0, st, (const double*)a->hacc, (long)eng->P.n, p1, 8192L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(64), 0, st, (const double*)p1, 8192L, p2, 64L));
+    GF_CU(launch(k_sum_stride, dim3(1), dim3(1), 0, st, (const double*)p2, 64L, p3, 1L));
+    GF_CU(launch(k_adj_add_slot, dim3(1), dim3(1), 0, st, a->wbar, seg, (const double*)p3));
+    GF_CU(cudaMemsetAsync(a->hacc, 0, sizeof(double) * eng->P.n, st));
     return GF_OK;
 }
 
+// the elastic increments' cotangents: lambda / 6 at stage 4, U after
 template <int S, class R>
 cudaError_t adj_el_vjp_launch(gf_adjoint* a) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
+    double* const* uk = (S == 3) ? a->LAM : a->U;
+    const R us = (S == 3) ? R(1. / 6.) : R(1);
     return launch(k_adj_el_vjp<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, (const uint8_t*)eng->mid,
-                  adj_mats<R>(eng), v3<R>(a->U + 3), v3<R>(a->U + 6), v3<R>(a->YBAR + 6), v3<R>(a->FBAR), v3<R>(a->LAMACC + 6),
-                  v3<R>(a->F0BAR), v3<R>(a->PHI), v3<R>(a->PHINEW));
+                  adj_mats<R>(eng), v3<R>(uk + 3), v3<R>(uk + 6), us, v3<R>(a->FBAR), v3<R>(a->LAM + 6), v3<R>(a->LAMACC + 6),
+                  v3<R>(a->U + 6), v3<R>(a->F0BAR), v3<R>(a->PHI), v3<R>(a->PHINEW));
 }
-template <int S, class R>
-cudaError_t adj_comb_launch(gf_adjoint* a, int g) {
-    gf_engine* eng = a->eng;
-    const Params& P = eng->P;
-    return launch(k_adj_comb<S, R>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, v3<R>(a->LAM + 3 * g),
-                  v3<R>(a->LAMACC + 3 * g), v3<R>(a->U + 3 * g), v3<R>(a->YBAR + 3 * g));
-}
-
 // reverse sweep of step `step` (lambda = d loss / d x_{step+1} in LAM on entry,
 // d loss / d x_step on exit; with elastodynamics also phi = d loss / d fs);
 // x is the step value x_step
@@ -3976,27 +3977,29 @@ int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
                      rp<R>(a->pend), (unsigned long long)step));
         for (int c = 0; c < 3; c++) GF_CU(cudaMemsetAsync(a->F0BAR[c], 0, a->esz * P.n, st));
     }
-    for (int c = 0; c < 3 * ng; c++) {
-        GF_CU(cudaMemcpyAsync(a->LAMACC[c], a->LAM[c], a->esz * P.n, cudaMemcpyDeviceToDevice, st));
-        // u4 = lambda / 6 (written by a scaled copy: the comb kernel of a virtual stage 4)
-        GF_CU(cudaMemcpyAsync(a->U[c], a->LAM[c], a->esz * P.n, cudaMemcpyDeviceToDevice, st));
-    }
-    for (int g = 0; g < ng; g++) GF_CU(launch(k_scale_f3<R>, dim3(bn), dim3(kThreads), 0, st, P, v3<R>(a->U + 3 * g), R(1. / 6.)));
-    const long seg = (long)((step * (uint64_t)a->nw) / a->nsteps);
+    // the stage-4 cotangent u4 = lambda / 6 is read from lambda (scaled in
+    // the kernels), and each group's RK combination runs in the kernel that
+    // forms the group's final ybar (vjp + field_T [+ el_p1] for m, el_p2
+    // for u, el_vjp for v), which writes lamacc (from lambda at stage 4)
+    // and the next stage's u
     for (int s = 3; s >= 0; s--) {
         F3T<R> y = (s == 0) ? v3<R>(x) : v3<R>(a->Y[s - 1]);
         C6T<R> str{}, strbar{};
         if (a->el && P.elasto_on)
             for (int q = 0; q < 6; q++) { str.c[q] = rp<R>(a->STR[s][q]); strbar.c[q] = rp<R>(a->STRBAR[q]); }
+        const F3T<R> um = (s == 3) ? v3<R>(a->LAM) : v3<R>(a->U);
+        const R us = (s == 3) ? R(1. / 6.) : R(1);
         GF_CU(launch(k_adj_vjp<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMatT<R>*)a->am, y,
-                     v3<R>(a->HS[s]), v3<R>(a->U), (const R*)rp<R>(a->alpha), v3<R>(a->YBAR), v3<R>(a->HBAR), a->abar,
-                     rp<R>(a->hbx), str, strbar));
+                     v3<R>(a->HS[s]), um, us, (const R*)rp<R>(a->alpha), v3<R>(a->YBAR), v3<R>(a->HBAR), a->abar,
+                     a->hacc, str, strbar));
         const R* Rk = nullptr;
         if (eng->demag_mode == 0) GF_TRY(adj_demag_T<R>(a, Rk));
         GF_CU(launch(k_adj_field_T<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const AdjMatT<R>*)a->am,
-                     (const R*)rp<R>(a->aij), a->nmat, v3<R>(a->HBAR), Rk, v3<R>(a->YBAR)));
+                     (const R*)rp<R>(a->aij), a->nmat, v3<R>(a->HBAR), Rk, v3<R>(a->YBAR), a->el ? 0 : 1, s, v3<R>(a->LAM),
+                     v3<R>(a->LAMACC), v3<R>(a->U)));
         if (a->el) {
-            // elastic increments, then the transposed stress and strain stencils
+            // elastic increments (and the v group's combination), then the
+            // transposed stress and strain stencils (the m and u groups')
             cudaError_t e;
             if (s == 3) e = adj_el_vjp_launch<3, R>(a);
             else if (s == 2) e = adj_el_vjp_launch<2, R>(a);
@@ -4004,18 +4007,10 @@ int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
             else e = adj_el_vjp_launch<0, R>(a);
             GF_CU(e);
             GF_CU(launch(k_adj_el_p1<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, adj_mats<R>(eng),
-                         v3<R>(a->FBAR), strbar, y, v3<R>(a->YBAR), (int)P.elasto_back, rp<R>(a->TO)));
+                         v3<R>(a->FBAR), strbar, y, v3<R>(a->YBAR), (int)P.elasto_back, rp<R>(a->TO), s, v3<R>(a->LAM),
+                         v3<R>(a->LAMACC), v3<R>(a->U)));
             GF_CU(launch(k_adj_el_p2<R>, dim3(bn), dim3(kThreads), 0, st, P, (const uint8_t*)eng->mid, (const R*)rp<R>(a->TO),
-                         v3<R>(a->YBAR + 3)));
-        }
-        GF_TRY(adj_wave_add(a, seg));
-        for (int g = 0; g < ng; g++) {
-            cudaError_t e;
-            if (s == 3) e = adj_comb_launch<3, R>(a, g);
-            else if (s == 2) e = adj_comb_launch<2, R>(a, g);
-            else if (s == 1) e = adj_comb_launch<1, R>(a, g);
-            else e = adj_comb_launch<0, R>(a, g);
-            GF_CU(e);
+                         s, v3<R>(a->LAM + 3), v3<R>(a->LAMACC + 3), v3<R>(a->U + 3)));
         }
     }
     for (int c = 0; c < 3 * ng; c++) std::swap(a->LAM[c], a->LAMACC[c]);
@@ -4029,7 +4024,7 @@ int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
 }
 
 // precision dispatch
-int adj_fwd(gf_adjoint* a, double* const* x, uint64_t step) {
+int adj_fwd(gf_adjoint* a, double** x, uint64_t step) {
     return a->f32 ? adj_step_forward<float>(a, x, step) : adj_step_forward<double>(a, x, step);
 }
 int adj_bwd(gf_adjoint* a, double* const* x, uint64_t step) {
@@ -4219,7 +4214,7 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
         a->ck_len += (size_t)51 * plane;
     }
     if ((rc = adj_alloc_d(a, &a->abar, (size_t)n)) != GF_OK) return fail(rc);
-    if ((rc = adj_alloc(a, &a->hbx, (size_t)n)) != GF_OK) return fail(rc);
+    if ((rc = adj_alloc_d(a, &a->hacc, (size_t)n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc_d(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->zero3, (size_t)3 * n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * a->ns * n)) != GF_OK) return fail(rc);
@@ -4345,6 +4340,8 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     }
     GF_CU(cudaMemsetAsync(a->abar, 0, sizeof(double) * n, st));
     GF_CU(cudaMemsetAsync(a->wbar, 0, sizeof(double) * a->nw, st));
+    GF_CU(cudaMemsetAsync(a->hacc, 0, sizeof(double) * n, st));
+    long cur_seg = -1;                 // waveform segment whose Hbar_x sums hacc holds
     GF_TRY(adj_inject(a, (long)N, inv_nfm));
     const uint64_t K = (uint64_t)a->ck_every;
     const uint64_t nblocks = (N + K - 1) / K;
@@ -4359,10 +4356,16 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
         for (uint64_t k = s1; k-- > s0;) {
             double* xp[21] = {};
             for (int q = 0; q < a->ns; q++) xp[a->sidx[q]] = adj_at(a, a->xs, ((k - s0) * (size_t)a->ns + q) * n);
+            const long seg = (long)((k * (uint64_t)a->nw) / N);
+            if (seg != cur_seg) {
+                if (cur_seg >= 0) GF_TRY(adj_wave_flush(a, cur_seg));
+                cur_seg = seg;
+            }
             GF_TRY(adj_bwd(a, xp, k));
             GF_TRY(adj_inject(a, (long)k, inv_nfm));
         }
     }
+    if (cur_seg >= 0) GF_TRY(adj_wave_flush(a, cur_seg));
     GF_CU(cudaMemcpyAsync(grad_wave, a->wbar, sizeof(double) * a->nw, cudaMemcpyDeviceToHost, st));
     GF_CU(cudaMemcpyAsync(grad_alpha, a->abar, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     GF_TRY(static_field_now(eng));
