@@ -3637,7 +3637,7 @@ struct gf_adjoint {
     double* XJC[3] = {};             // and its compensation words (FP32)
     // cotangents: m (0-2), u (3-5), v (6-8)
     double* LAM[9] = {}; double* LAMACC[9] = {}; double* U[9] = {};
-    double* YBAR[9] = {}; double* HBAR[3] = {};
+    double* YBAR[3] = {}; double* HBAR[3] = {};   // ybar of m (u's and v's stay in registers)
     double* abar = nullptr; double* hacc = nullptr; double* wbar = nullptr;   // FP64: alpha gradient, per-cell Hbar_x sum, waveform gradient
     // elastodynamics: stage u, v (stages 2-4), RK accumulators, the stage
     // force, the stage strain (LLG field), the cotangents of the force, the
@@ -4193,7 +4193,7 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
     a->ck_len = (size_t)a->ns * n;
     if (a->el) {
         double** el3[] = {a->X + 3, a->X + 6, a->X + 9, a->LAM + 3, a->LAM + 6, a->LAMACC + 3, a->LAMACC + 6,
-                          a->U + 3, a->U + 6, a->YBAR + 3, a->YBAR + 6, a->US[0], a->US[1], a->US[2],
+                          a->U + 3, a->U + 6, a->US[0], a->US[1], a->US[2],
                           a->VS[0], a->VS[1], a->VS[2], a->UACC, a->VACC, a->FORCE, a->FBAR, a->F0BAR, a->PHI, a->PHINEW};
         for (double** b : el3)
             if ((rc = adj_alloc3(a, b)) != GF_OK) return fail(rc);
