@@ -30,7 +30,7 @@ ERRORS = {-1: "GF_EINVAL", -2: "GF_EIO", -3: "GF_ECUDA", -4: "GF_ENOMEM", -5: "G
 FIELD = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "q": 4, "u": 5, "v": 6,
          "Ex": 7, "Ey": 8, "Ez": 9, "Hx": 10, "Hy": 11, "Hz": 12,
          "Hstat": 13, "Estat": 14, "E_cell": 15, "H_cell": 16, "strain": 17,
-         "strain_static": 18, "eigenstrain_static": 19}
+         "strain_static": 18, "eigenstrain_static": 19, "force_store": 20, "Jp1": 21, "Jp2": 22, "Jp3": 23}
 OBS = {"m": 0, "m_afm1": 1, "m_afm2": 2, "p": 3, "u": 4}
 PRECISION = {"fp64": 0, "mixed": 1}   # GF_PRECISION_FP64, GF_PRECISION_MIXED_FP32
 
@@ -41,7 +41,7 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients",
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
            "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
-           "gf_batch_create", "gf_batch_create_ex", "gf_batch_plan", "gf_batch_advance", "gf_batch_synchronize",
+           "gf_write_outputs", "gf_run_deck", "gf_batch_create", "gf_batch_create_ex", "gf_batch_plan", "gf_batch_advance", "gf_batch_synchronize",
            "gf_batch_stream", "gf_batch_tuned_chunk",
            "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics", "gf_set_elastostatics",
            "gf_save_state", "gf_load_state", "gf_create", "gf_set_table", "gf_stage_begin", "gf_stage_commit",
@@ -231,6 +231,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_set_elastostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
     lib.gf_save_state.argtypes = [vp, ctypes.c_char_p]
     lib.gf_load_state.argtypes = [vp, ctypes.c_char_p]
+    lib.gf_write_outputs.argtypes = [vp, ctypes.c_char_p, c_int]
+    lib.gf_run_deck.argtypes = [vp, ctypes.c_char_p]
     lib.gf_batch_create.argtypes = [ctypes.POINTER(vp), c_int, c_int, ctypes.POINTER(vp)]
     lib.gf_batch_create_ex.argtypes = [ctypes.POINTER(vp), c_int, c_int, c_int, ctypes.POINTER(vp)]
     lib.gf_batch_plan.argtypes = [vp]
@@ -368,6 +370,16 @@ class Engine:
         n = ctypes.c_int()
         self._check(self.lib.gf_profile_steps(self.h, int(nsteps), recs, 64, ctypes.byref(n)))
         return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(n.value)}
+
+    def write_outputs(self, directory: str, initial: bool = False) -> None:
+        """The reference's text outputs due at the current step (or its
+        step-0 block) into directory (gf_write_outputs)."""
+        self._check(self.lib.gf_write_outputs(self.h, directory.encode(), int(bool(initial))))
+
+    def run_deck(self, directory: str) -> None:
+        """The deck's whole run with the reference's output schedule
+        (gf_run_deck)."""
+        self._check(self.lib.gf_run_deck(self.h, directory.encode()))
 
     def save_state(self, path: str) -> None:
         self._check(self.lib.gf_save_state(self.h, os.fsencode(path)))

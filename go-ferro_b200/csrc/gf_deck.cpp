@@ -290,18 +290,22 @@ std::string read_deck(const std::string& dir, Deck& d) {
     r.flag(d.in_em, "if_input_em").flag(d.in_Jp, "if_input_Jp"); r.eol();
     r.flag(d.in_uv, "if_input_uandv").flag(d.in_straint0, "if_input_straint0").flag(d.in_eig0, "if_input_eigenstraint0_crt"); r.eol();
     r.flag(d.in_force, "if_input_elastoforce"); r.eol();
-    // output switches (the engine keeps no output schedule; read and skip)
+    // output schedule (gf_write_outputs / gf_run_deck write these files)
     {
-        bool b; unsigned long long s;
-        r.flag(b, "if_output_ave").get(s, "output_step_ave"); r.eol();
-        r.flag(b, "if_output_m").get(s, "output_step_m").flag(b, "if_output_only_magcell").get(s, "output_step_magcell"); r.eol();
-        r.flag(b, "if_output_AFMm").get(s, "output_step_AFMm"); r.eol();
-        r.flag(b, "if_output_p").get(s, "output_step_p"); r.eol();
-        r.flag(b, "if_output_em").get(s, "output_step_em").flag(b, "if_output_em_onecell").get(s, "output_step_em_onecell").get(s, "em_onecell_index"); r.eol();
-        const char* rest[] = {"if_output_strain", "if_output_Hstat", "if_output_Estat", "if_output_eigenstraint0_crt",
-                              "if_output_q", "if_output_uandv", "if_output_elastoforce", "if_output_emYee",
-                              "if_output_Jp", "if_output_Jishe"};
-        for (const char* name : rest) { r.flag(b, name).get(s, "output step"); r.eol(); }
+        auto out = [&](Deck::Out& o, const char* flag, const char* step) -> Reader& { return r.flag(o.on, flag).get(o.step, step); };
+        out(d.out_ave, "if_output_ave", "output_step_ave"); r.eol();
+        out(d.out_m, "if_output_m", "output_step_m");
+        out(d.out_magcell, "if_output_only_magcell", "output_step_magcell"); r.eol();
+        out(d.out_AFMm, "if_output_AFMm", "output_step_AFMm"); r.eol();
+        out(d.out_p, "if_output_p", "output_step_p"); r.eol();
+        out(d.out_em, "if_output_em", "output_step_em");
+        out(d.out_em_onecell, "if_output_em_onecell", "output_step_em_onecell").get(d.em_onecell_index, "em_onecell_index"); r.eol();
+        struct NO { Deck::Out* o; const char* name; } rest[] = {
+            {&d.out_strain, "if_output_strain"}, {&d.out_Hstat, "if_output_Hstat"}, {&d.out_Estat, "if_output_Estat"},
+            {&d.out_eig0, "if_output_eigenstraint0_crt"}, {&d.out_q, "if_output_q"}, {&d.out_uv, "if_output_uandv"},
+            {&d.out_force, "if_output_elastoforce"}, {&d.out_emYee, "if_output_emYee"}, {&d.out_Jp, "if_output_Jp"},
+            {&d.out_Jishe, "if_output_Jishe"}};
+        for (const NO& no : rest) { out(*no.o, no.name, "output step"); r.eol(); }
     }
     r.flag(d.jf_input, "if_Jf_input"); r.eol();
     r.get(d.jf_i0, "Jfin_xi").get(d.jf_j0, "Jfin_yi").get(d.jf_k0, "Jfin_zi"); r.eol();

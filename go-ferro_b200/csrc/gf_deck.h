@@ -92,6 +92,13 @@ struct Deck {
     bool flexo = false, spin_pumping = false;
     bool in_m = false, in_afm = false, in_Hstat = false, in_pq = false, in_Estat = false;
     bool in_em = false, in_Jp = false, in_uv = false, in_straint0 = false, in_eig0 = false, in_force = false;
+    // output schedule of the time loop: switch and step interval of each of
+    // the reference's text outputs (read.cpp; written by main.cpp:170-198 at
+    // step 0 and main.cpp:486-705 after every step)
+    struct Out { bool on = false; unsigned long long step = 0; };
+    Out out_ave, out_m, out_magcell, out_AFMm, out_p, out_em, out_em_onecell;
+    Out out_strain, out_Hstat, out_Estat, out_eig0, out_q, out_uv, out_force, out_emYee, out_Jp, out_Jishe;
+    unsigned long long em_onecell_index = 0;
     bool jf_input = false;
     unsigned long jf_i0 = 0, jf_j0 = 0, jf_k0 = 0, jf_i1 = 0, jf_j1 = 0, jf_k1 = 0;
     unsigned jf_type = 0; char jf_comp = 'x'; double jf_amp = 0, jf_freq = 0, jf_sigma = 0; unsigned long jf_cycles = 0;

@@ -2066,6 +2066,13 @@ int field_ptrs(gf_engine* eng, int field, std::vector<double*>& ptrs, std::vecto
             break;
         }
         case GF_FIELD_ESTAT: if (!eng->Estat[0]) break; add3(eng->Estat, nullptr); break;
+        case GF_FIELD_FORCE_STORE: if (!eng->force_store[0]) break; add3(eng->force_store, nullptr); break;
+        case GF_FIELD_JP1: case GF_FIELD_JP2: case GF_FIELD_JP3: {
+            Field3& f = eng->jp[field - GF_FIELD_JP1];
+            if (!f.on) break;
+            add3(cur(eng, f), &f);
+            break;
+        }
         case GF_FIELD_E_CELL: case GF_FIELD_H_CELL: {
             if (!eng->E.on) break;
             writable = false;
@@ -2302,6 +2309,126 @@ int es_setup(gf_engine* eng) {
     }
     return GF_OK;
 }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The reference's text outputs (inoutput.cpp:330-887, scheduled by
+// main.cpp:170-198 and 486-705): the same file names, row order and printf
+// formats (the file format is the interface a drop-in keeps), from fields
+// downloaded in FP64.
+// ---------------------------------------------------------------------------
+namespace {
+
+// a field in FP64 host memory; zeros when the run lacks it
+int out_field(gf_engine* eng, int field, std::vector<double>& v) {
+    size_t count = 0;
+    GF_TRY(gf_field_dims(eng, field, nullptr, &count));
+    v.assign(count, 0.);
+    std::vector<double*> ptrs, cmps; std::vector<long> lens; bool writable, native;
+    const std::string keep = eng->err;
+    const int rc = field_ptrs(eng, field, ptrs, lens, writable, cmps, native);
+    if (rc == GF_EINVAL || (rc == GF_OK && ptrs.empty())) {
+        eng->err = keep;                 // absent in this run: the zeros stand
+        return GF_OK;
+    }
+    GF_TRY(rc);
+    return gf_download(eng, field, v.data(), count);
+}
+
+// "%ld  %ld  %ld  %.7e..." over a (nx_, ny_, nz_) grid, 1-based indices,
+// component c of row (i, j, k) at cols[c][(i*ny_ + j)*nz_ + k]
+int out_grid(gf_engine* eng, const std::string& path, long nx_, long ny_, long nz_, const std::vector<const double*>& cols) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) { eng->err = "cannot write " + path; return GF_EIO; }
+    for (long i = 0; i < nx_; i++)
+        for (long j = 0; j < ny_; j++)
+            for (long k = 0; k < nz_; k++) {
+                const long c = (i * ny_ + j) * nz_ + k;
+                std::fprintf(f, "%ld  %ld  %ld", i + 1, j + 1, k + 1);
+                for (const double* col : cols) std::fprintf(f, "  %.7e", col[c]);
+                std::fprintf(f, "\n");
+            }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    if (!ok) { eng->err = "write error in " + path; return GF_EIO; }
+    return GF_OK;
+}
+
+// a cell field of ncomp components as "<name>.<nstep>.dat"
+int out_cells(gf_engine* eng, const std::string& dir, const char* name, uint64_t nstep, int field) {
+    std::vector<double> v;
+    GF_TRY(out_field(eng, field, v));
+    const long n = eng->P.n;
+    std::vector<const double*> cols;
+    for (size_t a = 0; a * (size_t)n < v.size(); a++) cols.push_back(v.data() + a * (size_t)n);
+    return out_grid(eng, dir + "/" + name + "." + std::to_string(nstep) + ".dat", eng->P.nx, eng->P.ny, eng->P.nz, cols);
+}
+
+// a line appended to dir/name
+int out_append(gf_engine* eng, const std::string& dir, const char* name, const std::string& line) {
+    const std::string path = dir + "/" + name;
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) { eng->err = "cannot write " + path; return GF_EIO; }
+    std::fputs(line.c_str(), f);
+    std::fclose(f);
+    return GF_OK;
+}
+
+// static strain in the global frame (exxt0_glb..), 6 x n; zeros without one
+int out_static_strain_glb(gf_engine* eng, std::vector<double>& g) {
+    std::vector<double> c;
+    GF_TRY(out_field(eng, GF_FIELD_STRAIN_STATIC, c));
+    const long n = eng->P.n;
+    g.assign(6 * (size_t)n, 0.);
+    const double(*T)[3] = eng->P.Tc2g;
+    for (long q = 0; q < n; q++) {
+        const double e[3][3] = {{c[0 * n + q], c[5 * n + q], c[4 * n + q]},
+                                {c[5 * n + q], c[1 * n + q], c[3 * n + q]},
+                                {c[4 * n + q], c[3 * n + q], c[2 * n + q]}};
+        double r[3][3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                double s = 0.;
+                for (int k = 0; k < 3; k++)
+                    for (int l = 0; l < 3; l++) s += T[a][k] * T[b][l] * e[k][l];
+                r[a][b] = s;
+            }
+        if (!eng->P.rot) std::memcpy(r, e, sizeof(r));
+        g[0 * n + q] = r[0][0]; g[1 * n + q] = r[1][1]; g[2 * n + q] = r[2][2];
+        g[3 * n + q] = r[1][2]; g[4 * n + q] = r[0][2]; g[5 * n + q] = r[0][1];
+    }
+    return GF_OK;
+}
+
+std::string out_line(const char* fmt, uint64_t nstep, const double* v, int nv) {
+    char buf[256];
+    if (nv == 3) std::snprintf(buf, sizeof(buf), fmt, (long long)nstep, v[0], v[1], v[2]);
+    else std::snprintf(buf, sizeof(buf), fmt, (long long)nstep, v[0], v[1], v[2], v[3], v[4], v[5]);
+    return buf;
+}
+
+int out_averages(gf_engine* eng, const std::string& dir, uint64_t nstep) {
+    const Deck& d = eng->deck;
+    double a[3], b[3];
+    if (d.any_fm) {
+        GF_TRY(gf_average(eng, GF_OBS_M, a));
+        GF_TRY(out_append(eng, dir, "average_m.dat", out_line("%lld %.7e  %.7e  %.7e\n", nstep, a, 3)));
+    }
+    if (d.any_afm) {
+        GF_TRY(gf_average(eng, GF_OBS_M_AFM1, a));
+        GF_TRY(gf_average(eng, GF_OBS_M_AFM2, b));
+        const double v[6] = {a[0], a[1], a[2], b[0], b[1], b[2]};
+        GF_TRY(out_append(eng, dir, "average_AFMm.dat", out_line("%lld %.7e  %.7e  %.7e  %.7e  %.7e  %.7e\n", nstep, v, 6)));
+    }
+    if (d.any_fe) {
+        GF_TRY(gf_average(eng, GF_OBS_P, a));
+        GF_TRY(out_append(eng, dir, "average_p.dat", out_line("%lld %.7e  %.7e  %.7e\n", nstep, a, 3)));
+    }
+    return GF_OK;
+}
+
+bool out_due(const Deck::Out& o, uint64_t nstep) { return o.on && o.step > 0 && nstep % o.step == 0; }
 
 }  // namespace
 
@@ -2764,6 +2891,130 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used) {
         if (eng->graph[p]) { cudaGraphDestroy(eng->graph[p]); eng->graph[p] = nullptr; }
     }
     eng->graphs_ready = false;
+    return GF_OK;
+}
+
+int gf_write_outputs(gf_engine* e, const char* dir, int initial) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    if (!dir) { eng->err = "gf_write_outputs: null directory"; return GF_EINVAL; }
+    GF_CU(cudaSetDevice(eng->device));
+    const Deck& d = eng->deck;
+    const Params& P = eng->P;
+    const std::string D(dir);
+    const uint64_t ns = eng->steps_done;
+    const long n = P.n;
+    if (initial) {
+        // main.cpp:170-198
+        if (d.out_ave.on) GF_TRY(out_averages(eng, D, ns));
+        if (d.out_Estat.on) GF_TRY(out_cells(eng, D, "Estat", ns, GF_FIELD_ESTAT));
+        if (d.out_Hstat.on) GF_TRY(out_cells(eng, D, "Hstat", ns, GF_FIELD_HSTAT));
+        if (d.elastodynamics && d.out_strain.on) {
+            std::vector<double> g;
+            GF_TRY(out_static_strain_glb(eng, g));
+            std::vector<const double*> cols;
+            for (int a = 0; a < 6; a++) cols.push_back(g.data() + (size_t)a * n);
+            GF_TRY(out_grid(eng, D + "/strain_stat." + std::to_string(ns) + ".dat", P.nx, P.ny, P.nz, cols));
+        }
+        if (d.out_eig0.on) GF_TRY(out_cells(eng, D, "eigenstraint0_crt", ns, GF_FIELD_EIGENSTRAIN_STATIC));
+        return GF_OK;
+    }
+    // main.cpp:601-705, in its order
+    if (out_due(d.out_ave, ns)) GF_TRY(out_averages(eng, D, ns));
+    if (out_due(d.out_m, ns)) GF_TRY(out_cells(eng, D, "m", ns, GF_FIELD_M));
+    if (out_due(d.out_magcell, ns)) {
+        std::vector<double> m;
+        GF_TRY(out_field(eng, GF_FIELD_M, m));
+        const std::string path = D + "/m_magcell." + std::to_string(ns) + ".dat";
+        FILE* f = std::fopen(path.c_str(), "w");
+        if (!f) { eng->err = "cannot write " + path; return GF_EIO; }
+        const long nyz = P.ny * P.nz;
+        for (long c = 0; c < n; c++) {
+            const uint8_t id = d.material_cell[(size_t)c];
+            if (!(id && d.mats[id - 1].fm)) continue;
+            const long i = c / nyz, j = (c - i * nyz) / P.nz, k = c - i * nyz - j * P.nz;
+            std::fprintf(f, "%ld  %ld  %ld  %.7e  %.7e  %.7e\n", i + 1, j + 1, k + 1, m[c], m[n + c], m[2 * n + c]);
+        }
+        std::fclose(f);
+    }
+    if (out_due(d.out_AFMm, ns)) {
+        std::vector<double> a1, a2;
+        GF_TRY(out_field(eng, GF_FIELD_M_AFM1, a1));
+        GF_TRY(out_field(eng, GF_FIELD_M_AFM2, a2));
+        std::vector<const double*> cols;
+        for (int a = 0; a < 3; a++) cols.push_back(a1.data() + (size_t)a * n);
+        for (int a = 0; a < 3; a++) cols.push_back(a2.data() + (size_t)a * n);
+        GF_TRY(out_grid(eng, D + "/m_AFM." + std::to_string(ns) + ".dat", P.nx, P.ny, P.nz, cols));
+    }
+    if (out_due(d.out_p, ns)) GF_TRY(out_cells(eng, D, "p", ns, GF_FIELD_P));
+    if (out_due(d.out_q, ns)) GF_TRY(out_cells(eng, D, "q", ns, GF_FIELD_Q));
+    if (out_due(d.out_em, ns)) {
+        GF_TRY(out_cells(eng, D, "Eem", ns, GF_FIELD_E_CELL));
+        GF_TRY(out_cells(eng, D, "Hem", ns, GF_FIELD_H_CELL));
+    }
+    if (out_due(d.out_em_onecell, ns)) {
+        std::vector<double> E, H;
+        GF_TRY(out_field(eng, GF_FIELD_E_CELL, E));
+        GF_TRY(out_field(eng, GF_FIELD_H_CELL, H));
+        const long c = (long)d.em_onecell_index - 1;
+        if (c < 0 || c >= n) { eng->err = "em_onecell_index outside the grid"; return GF_EINVAL; }
+        const double v[6] = {E[c], E[n + c], E[2 * n + c], H[c], H[n + c], H[2 * n + c]};
+        GF_TRY(out_append(eng, D, "EM_onecell.dat", out_line("%lld %.7e  %.7e  %.7e %.7e  %.7e  %.7e\n", ns, v, 6)));
+    }
+    if (out_due(d.out_emYee, ns)) {
+        const char* names[6] = {"Ex_Yee", "Ey_Yee", "Ez_Yee", "Hx_Yee", "Hy_Yee", "Hz_Yee"};
+        for (int q = 0; q < 6; q++) {
+            std::vector<double> v;
+            GF_TRY(out_field(eng, GF_FIELD_EX + q, v));
+            int64_t dm[3];
+            GF_TRY(gf_field_dims(eng, GF_FIELD_EX + q, dm, nullptr));
+            GF_TRY(out_grid(eng, D + "/" + names[q] + "." + std::to_string(ns) + ".dat", (long)dm[0], (long)dm[1], (long)dm[2],
+                            {v.data()}));
+        }
+    }
+    if (out_due(d.out_Estat, ns)) GF_TRY(out_cells(eng, D, "Estat", ns, GF_FIELD_ESTAT));
+    if (out_due(d.out_Hstat, ns)) GF_TRY(out_cells(eng, D, "Hstat", ns, GF_FIELD_HSTAT));
+    if (out_due(d.out_strain, ns)) {
+        // static (global frame) plus dynamic cell strain, as output_strain
+        // adds exxt0_glb and Dexx_glb
+        std::vector<double> g, dyn;
+        GF_TRY(out_static_strain_glb(eng, g));
+        GF_TRY(out_field(eng, GF_FIELD_STRAIN, dyn));
+        for (size_t q = 0; q < g.size(); q++) g[q] = g[q] + dyn[q];
+        std::vector<const double*> cols;
+        for (int a = 0; a < 6; a++) cols.push_back(g.data() + (size_t)a * n);
+        GF_TRY(out_grid(eng, D + "/strain." + std::to_string(ns) + ".dat", P.nx, P.ny, P.nz, cols));
+    }
+    if (out_due(d.out_uv, ns)) {
+        GF_TRY(out_cells(eng, D, "u", ns, GF_FIELD_U));
+        GF_TRY(out_cells(eng, D, "v", ns, GF_FIELD_V));
+    }
+    if (out_due(d.out_force, ns)) GF_TRY(out_cells(eng, D, "elastoforce", ns, GF_FIELD_FORCE_STORE));
+    if (out_due(d.out_eig0, ns)) GF_TRY(out_cells(eng, D, "eigenstraint0_crt", ns, GF_FIELD_EIGENSTRAIN_STATIC));
+    if (out_due(d.out_Jp, ns)) {
+        GF_TRY(out_cells(eng, D, "Jp1", ns, GF_FIELD_JP1));
+        GF_TRY(out_cells(eng, D, "Jp2", ns, GF_FIELD_JP2));
+        GF_TRY(out_cells(eng, D, "Jp3", ns, GF_FIELD_JP3));
+    }
+    return GF_OK;
+}
+
+int gf_run_deck(gf_engine* e, const char* dir) {
+    GF_TRY(check(e));
+    gf_engine* eng = e;
+    const Deck& d = eng->deck;
+    GF_TRY(gf_write_outputs(e, dir, 1));
+    const Deck::Out* outs[] = {&d.out_ave, &d.out_m, &d.out_magcell, &d.out_AFMm, &d.out_p, &d.out_q, &d.out_em,
+                               &d.out_em_onecell, &d.out_emYee, &d.out_Estat, &d.out_Hstat, &d.out_strain, &d.out_uv,
+                               &d.out_force, &d.out_eig0, &d.out_Jp};
+    const uint64_t last = (uint64_t)d.steps;
+    while (eng->steps_done < last) {
+        uint64_t next = last;
+        for (const Deck::Out* o : outs)
+            if (o->on && o->step > 0) next = std::min<uint64_t>(next, (uint64_t)((eng->steps_done / o->step + 1) * o->step));
+        GF_TRY(gf_advance(e, next - eng->steps_done));
+        GF_TRY(gf_write_outputs(e, dir, 0));
+    }
     return GF_OK;
 }
 

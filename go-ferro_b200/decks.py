@@ -207,6 +207,12 @@ class Deck:
     # reference permittivity, iteration limit, tolerance
     spin_pumping: bool = False
     flexo: bool = False          # if_flexo (flexoelectric coupling)
+    # text-output schedule of the time loop: output name -> step interval
+    # (absent or 0 = off); names follow the deck's if_output_* switches:
+    # ave, m, magcell, AFMm, p, em, em_onecell, strain, Hstat, Estat, eig0,
+    # q, uv, force, emYee, Jp, Jishe; em_onecell_index is 1-based
+    outputs: dict = field(default_factory=lambda: {"ave": 1})
+    em_onecell_index: int = 0
     # electrostatics: 1-D model and its compensation (if_elec_1Dmodel,
     # if_elec_1D_compensate)
     elec_1D: bool = False
@@ -280,6 +286,10 @@ class Deck:
             z += nzl
         return mc
 
+    def _out(self, name: str) -> str:
+        step = int(self.outputs.get(name, 0))
+        return f"{_b(step > 0)} {max(step, 1)}"
+
     def system_setting_text(self) -> str:
         nxw = self.nx if self.nx_work is None else self.nx_work
         nyw = self.ny if self.ny_work is None else self.ny_work
@@ -335,21 +345,21 @@ class Deck:
              "false false",
              f"{_b(self.u0 is not None)} {_b(self.strain_t0 is not None)} {_b(self.eig_t0 is not None)}",
              "false",
-             "true 1",
-             "false 1 false 1",
-             "false 1",
-             "false 1",
-             "false 1 false 1 0",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
-             "false 1",
+             self._out("ave"),
+             f"{self._out('m')} {self._out('magcell')}",
+             self._out("AFMm"),
+             self._out("p"),
+             f"{self._out('em')} {self._out('em_onecell')} {int(self.em_onecell_index)}",
+             self._out("strain"),
+             self._out("Hstat"),
+             self._out("Estat"),
+             self._out("eig0"),
+             self._out("q"),
+             self._out("uv"),
+             self._out("force"),
+             self._out("emYee"),
+             self._out("Jp"),
+             self._out("Jishe"),
              _b(self.jf),
              " ".join(str(int(x)) for x in self.jf_lo),
              " ".join(str(int(x)) for x in self.jf_hi),

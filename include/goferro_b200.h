@@ -71,7 +71,12 @@ enum gf_field {
     GF_FIELD_EIGENSTRAIN_STATIC = 19, /* static eigenstrain, crystal frame (cell, 6)
                                          exx0t0_crt..; present with
                                          eigenstraint0_crt.in or gf_set_elastostatics */
-    GF_FIELD_COUNT = 20
+    GF_FIELD_FORCE_STORE = 20,        /* stiffness-damping force store (cell, 3)
+                                         force_x_store..; elastodynamics */
+    GF_FIELD_JP1 = 21,                /* Drude pole currents (cell, 3)  Jpx_n1.. */
+    GF_FIELD_JP2 = 22,
+    GF_FIELD_JP3 = 23,
+    GF_FIELD_COUNT = 24
 };
 
 /* observables for gf_average (global averages, FP64 sums) */
@@ -351,6 +356,26 @@ int gf_set_electrostatics(gf_engine* e, int enable, int* iterations_used);
  * solve itself runs in FP64); *iterations_used (optional) gets the set-up
  * iteration count. */
 int gf_set_elastostatics(gf_engine* e, int enable, int* iterations_used);
+
+/* The reference's text outputs (inoutput.cpp:330-887) into directory dir,
+ * for the engine's current step nstep (steps done): with initial != 0 the
+ * step-0 block of main.cpp:170-198 (averages, Estat, Hstat, strain_stat
+ * with elastodynamics, eigenstraint0_crt), otherwise every output whose
+ * deck switch (if_output_*) is on and whose interval divides nstep, as
+ * main.cpp:486-705 writes them after a step.  Same file names
+ * ("m.<nstep>.dat", "Ex_Yee.<nstep>.dat", ...), row order (i, j, k,
+ * 1-based), columns and %.7e format; average_*.dat and EM_onecell.dat are
+ * appended to.  Fields a run lacks are written as zeros, as the
+ * reference's zero-initialised arrays would be.  J_ISHE.<nstep>.dat is not
+ * written: the engine forms the inverse-spin-Hall current inside the Yee
+ * update and keeps no array of it.  Synchronous. */
+int gf_write_outputs(gf_engine* e, const char* dir, int initial);
+
+/* The reference's run in one call (main.cpp:170-705): the step-0 outputs,
+ * then the deck's step count from the current step, stopping at every step
+ * where an output is due and writing it with gf_write_outputs.  No
+ * counterpart besides main.cpp itself. */
+int gf_run_deck(gf_engine* e, const char* dir);
 
 /* Full-precision checkpoint of everything that carries from one step to the
  * next: the state fields (and, in the mixed form, their compensation words),

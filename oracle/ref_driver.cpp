@@ -10,7 +10,7 @@
  *
  * Usage:
  *   goferro_ref DECK_DIR OUT_DIR [--steps K] [--warmup W] [--trace-every N]
- *               [--probe I J K] [--dump]
+ *               [--probe I J K] [--dump] [--outputs]
  *
  * DECK_DIR holds system_setting.in, materials.in and any restart files the
  * deck asks for (the reference reads them from the working directory,
@@ -22,6 +22,9 @@
  *              reference's storage order (matrix.h:51)
  *   timing.json  {"steps":K-W,"warmup":W,"seconds":S,"cells":n} for the time
  *                loop after the first W (untimed) steps.
+ *   with --outputs, the reference's own text outputs (inoutput.cpp), written
+ *   by its inoutput functions with main.cpp's schedule (the step-0 block of
+ *   main.cpp:170-198 and the per-step block of main.cpp:486-705)
  */
 #define _USE_SINGLETON_MACRO
 #include "_MACRO_SINGLETON.h"
@@ -171,9 +174,47 @@ void dump_all(const std::string& d, Systems& s) {
 
 }  // namespace
 
+// main.cpp:170-198: outputs of the initial state
+static void initial_outputs(Systems& s, unsigned long long nstep) {
+    if (_GLB.if_output_ave) {
+        if (_GLB.if_FM_all) { s.mag.get_averagem(); _IO.output_averagem(nstep, &s.mag); }
+        if (_GLB.if_AFM_all) { s.mag.get_averagem_AFM(); _IO.output_averageAFMm(nstep, &s.mag); }
+        if (_GLB.if_FE_all) { s.fe.get_averagep(); _IO.output_averagep(nstep, &s.fe); }
+    }
+    if (_GLB.if_output_Estat) _IO.output_Estat(nstep, &s.fe);
+    if (_GLB.if_output_Hstat) _IO.output_Hstat(nstep, &s.mag);
+    if (_GLB.if_elastodynamics && _GLB.if_output_strain) _IO.output_straint0(nstep, &s.el);
+    if (_GLB.if_output_eigenstraint0_crt) _IO.output_eigenstraint0_crt(nstep, &s.el);
+}
+
+// main.cpp:486-705: after step nstep (the device copies are host no-ops here)
+static void step_outputs(Systems& s, unsigned long long nstep) {
+    auto due = [&](bool on, unsigned long long every) { return on && every > 0 && nstep % every == 0; };
+    if (due(_GLB.if_output_ave, _GLB.output_step_ave)) {
+        if (_GLB.if_FM_all) { s.mag.get_averagem(); _IO.output_averagem(nstep, &s.mag); }
+        if (_GLB.if_AFM_all) { s.mag.get_averagem_AFM(); _IO.output_averageAFMm(nstep, &s.mag); }
+        if (_GLB.if_FE_all) { s.fe.get_averagep(); _IO.output_averagep(nstep, &s.fe); }
+    }
+    if (due(_GLB.if_output_m, _GLB.output_step_m)) _IO.output_m(nstep, &s.mag);
+    if (due(_GLB.if_output_only_magcell, _GLB.output_step_magcell)) _IO.output_magcell(nstep, &s.mag);
+    if (due(_GLB.if_output_AFMm, _GLB.output_step_AFMm)) _IO.output_AFMm(nstep, &s.mag);
+    if (due(_GLB.if_output_p, _GLB.output_step_p)) _IO.output_p(nstep, &s.fe);
+    if (due(_GLB.if_output_q, _GLB.output_step_q)) _IO.output_q(nstep, &s.fe);
+    if (due(_GLB.if_output_em, _GLB.output_step_em)) { _IO.output_Eem(nstep, &s.em); _IO.output_Hem(nstep, &s.em); }
+    if (due(_GLB.if_output_em_onecell, _GLB.output_step_em_onecell)) _IO.output_em_onecell(nstep, &s.em);
+    if (due(_GLB.if_output_emYee, _GLB.output_step_emYee)) { _IO.output_EemYee(nstep, &s.em); _IO.output_HemYee(nstep, &s.em); }
+    if (due(_GLB.if_output_Estat, _GLB.output_step_Estat)) _IO.output_Estat(nstep, &s.fe);
+    if (due(_GLB.if_output_Hstat, _GLB.output_step_Hstat)) _IO.output_Hstat(nstep, &s.mag);
+    if (due(_GLB.if_output_strain, _GLB.output_step_strain)) _IO.output_strain(nstep, &s.el);
+    if (due(_GLB.if_output_uandv, _GLB.output_step_uandv)) _IO.output_uandv(nstep, &s.el);
+    if (due(_GLB.if_output_elastoforce, _GLB.output_step_elastoforce)) _IO.output_elastoforce(nstep, &s.el);
+    if (due(_GLB.if_output_eigenstraint0_crt, _GLB.output_step_eigenstraint0_crt)) _IO.output_eigenstraint0_crt(nstep, &s.el);
+    if (due(_GLB.if_output_Jp, _GLB.output_step_Jp)) _IO.output_Jp(nstep, &s.em);
+}
+
 int main(int argc, char** argv) {
     if (argc < 3) {
-        fprintf(stderr, "usage: %s DECK_DIR OUT_DIR [--steps K] [--warmup W] [--trace-every N] [--probe I J K] [--dump]\n", argv[0]);
+        fprintf(stderr, "usage: %s DECK_DIR OUT_DIR [--steps K] [--warmup W] [--trace-every N] [--probe I J K] [--dump] [--outputs]\n", argv[0]);
         return 2;
     }
     char outbuf[PATH_MAX];
@@ -183,13 +224,14 @@ int main(int argc, char** argv) {
     unsigned long long warmup = 0;
     unsigned long long trace_every = 1;
     long pi = -1, pj = -1, pk = -1;
-    bool do_dump = false;
+    bool do_dump = false, do_outputs = false;
     for (int a = 3; a < argc; ++a) {
         if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps_override = atoll(argv[++a]);
         else if (!strcmp(argv[a], "--trace-every") && a + 1 < argc) trace_every = strtoull(argv[++a], 0, 10);
         else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = strtoull(argv[++a], 0, 10);
         else if (!strcmp(argv[a], "--probe") && a + 3 < argc) { pi = atol(argv[++a]); pj = atol(argv[++a]); pk = atol(argv[++a]); }
         else if (!strcmp(argv[a], "--dump")) do_dump = true;
+        else if (!strcmp(argv[a], "--outputs")) do_outputs = true;
         else { fprintf(stderr, "unknown argument %s\n", argv[a]); return 2; }
     }
     if (chdir(argv[1]) != 0) { fprintf(stderr, "cannot enter %s\n", argv[1]); return 2; }
@@ -259,6 +301,12 @@ int main(int argc, char** argv) {
     FILE* tf = fopen(tpath.c_str(), "w");
     if (!tf) { fprintf(stderr, "cannot write %s\n", tpath.c_str()); return 2; }
     write_trace_line(tf, 0, s, probe);
+    // the reference writes its outputs into the working directory: after
+    // set-up (every input read) that becomes OUT_DIR
+    if (do_outputs) {
+        if (chdir(out.c_str()) != 0) { fprintf(stderr, "cannot enter %s\n", out.c_str()); return 2; }
+        initial_outputs(s, 0);
+    }
 
     // ---- statics before the loop (main.cpp:213-240) ----
     if (!_GLB.if_elastodynamics) s.el.get_strain_static();
@@ -282,6 +330,7 @@ int main(int argc, char** argv) {
         if (!_GLB.if_elastodynamics) s.el.get_strain_static();
         between_stage_statics(s);
         if (nstep % trace_every == 0 || nstep == _GLB.step) write_trace_line(tf, nstep, s, probe);
+        if (do_outputs) step_outputs(s, nstep);
     }
     auto t1 = std::chrono::steady_clock::now();
     fclose(tf);

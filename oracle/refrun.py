@@ -37,9 +37,11 @@ def build(ref_dir: Optional[str] = None) -> None:
 
 def run(deck_dir: str, out_dir: str, steps: Optional[int] = None, trace_every: int = 1,
         probe: Optional[Sequence[int]] = None, dump: bool = False, timeout: float = 3600.0,
-        warmup: int = 0) -> Dict:
+        warmup: int = 0, outputs: bool = False) -> Dict:
     """Run the reference on `deck_dir`; returns {"trace": (K,22) array,
-    "timing": {...}, "fields": {name: flat float64 array}}."""
+    "timing": {...}, "fields": {name: flat float64 array}}.  With outputs,
+    the reference's own text outputs (its deck's if_output_* schedule) are
+    written into out_dir as well."""
     if not available():
         raise RuntimeError(f"oracle binary missing: {REF_BIN}")
     os.makedirs(out_dir, exist_ok=True)
@@ -52,6 +54,8 @@ def run(deck_dir: str, out_dir: str, steps: Optional[int] = None, trace_every: i
         cmd += ["--probe"] + [str(int(x)) for x in probe]
     if dump:
         cmd += ["--dump"]
+    if outputs:
+        cmd += ["--outputs"]
     subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
     trace = np.loadtxt(os.path.join(out_dir, "trace.txt"), ndmin=2)
     with open(os.path.join(out_dir, "timing.json")) as f:
