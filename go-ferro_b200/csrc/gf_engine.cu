@@ -384,7 +384,6 @@ std::string unsupported(const Deck& d) {
         return "the 1-D and film elastostatic models and external strain (if_elastostatic_1D, if_elastostatic_film, if_read_strain_ext) are not supported by this engine";
     if (d.flexo && (d.elastostatic || d.in_straint0))
         return "flexoelectricity with a static strain (if_elastostatic or strain_stat.in) is not supported by this engine";
-    if (d.in_force || d.in_Jp) return "restart inputs elastoforce / Jp are not supported by this engine";
     if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
     if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this engine";
     for (size_t i = 0; i < d.mats.size(); i++) {
@@ -1526,6 +1525,25 @@ int initial_state(gf_engine* eng, const std::string& dir) {
         if (!e.empty()) { eng->err = e; return GF_EIO; }
         GF_TRY(upload_vec(eng, eng->u.X, ub, n, eng->u.C));
         GF_TRY(upload_vec(eng, eng->v.X, vb, n, eng->v.C));
+    }
+    if (d.in_force && eng->force_store[0]) {
+        // elastoforce.in: the stage-1 stress divergence the next step's
+        // stiffness damping reads (inoutput.cpp:220-237)
+        for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+        std::string e = read_restart(dir + "/elastoforce.in", d.nx, d.ny, d.nz, 3, buf);
+        if (!e.empty()) { eng->err = e; return GF_EIO; }
+        GF_TRY(upload_vec(eng, eng->force_store, buf, n));
+    }
+    if (d.in_Jp) {
+        // Jp1.in..Jp3.in: the Drude pole currents (inoutput.cpp:283-328)
+        const char* names[3] = {"Jp1.in", "Jp2.in", "Jp3.in"};
+        for (int pole = 0; pole < 3; pole++) {
+            if (!eng->jp[pole].on) continue;
+            for (auto& b : buf) std::fill(b.begin(), b.end(), 0.);
+            std::string e = read_restart(dir + "/" + names[pole], d.nx, d.ny, d.nz, 3, buf);
+            if (!e.empty()) { eng->err = e; return GF_EIO; }
+            GF_TRY(upload_vec(eng, eng->jp[pole].X, buf, n, eng->jp[pole].C));
+        }
     }
     if (eng->E.on && d.in_em) {
         const char* names[6] = {"Ex_Yee.in", "Ey_Yee.in", "Ez_Yee.in", "Hx_Yee.in", "Hy_Yee.in", "Hz_Yee.in"};

@@ -258,6 +258,8 @@ class Deck:
     q0: Optional[np.ndarray] = None
     u0: Optional[np.ndarray] = None
     v0: Optional[np.ndarray] = None
+    force0: Optional[np.ndarray] = None    # (3, nx, ny, nz): elastoforce.in (stiffness-damping force store)
+    jp0: Optional[list] = None             # three (3, nx, ny, nz): Jp1.in..Jp3.in (Drude pole currents)
     Hext_table: Optional[np.ndarray] = None    # (K, 4): t Hx Hy Hz
     # crystal orientation: Tg2c, the global-to-crystal rotation (3x3); when
     # set, if_OrientRotate is true (read.cpp:30-37; Tc2g is its transpose)
@@ -342,9 +344,9 @@ class Deck:
              f"{_b(self.spin_pumping)}",
              f"{_b(self.m0 is not None)} {_b(self.afm0 is not None)} false",
              f"{_b(self.p0 is not None)} false",
-             "false false",
+             f"false {_b(self.jp0 is not None)}",
              f"{_b(self.u0 is not None)} {_b(self.strain_t0 is not None)} {_b(self.eig_t0 is not None)}",
-             "false",
+             _b(self.force0 is not None),
              self._out("ave"),
              f"{self._out('m')} {self._out('magcell')}",
              self._out("AFMm"),
@@ -398,6 +400,11 @@ def write_deck(deck: Deck, directory: str) -> str:
         _write_restart(os.path.join(directory, "u.in"), deck.u0)
         v = deck.v0 if deck.v0 is not None else np.zeros_like(deck.u0)
         _write_restart(os.path.join(directory, "v.in"), v)
+    if deck.force0 is not None:
+        _write_restart(os.path.join(directory, "elastoforce.in"), deck.force0)
+    if deck.jp0 is not None:
+        for pole, a in enumerate(deck.jp0):
+            _write_restart(os.path.join(directory, f"Jp{pole + 1}.in"), a)
     if deck.strain_t0 is not None:
         _write_restart(os.path.join(directory, "strain_stat.in"), deck.strain_t0)
     if deck.eig_t0 is not None:

@@ -113,7 +113,8 @@ typedef struct gf_kernel_time {
 /* Create an engine from a GO-Ferro input deck directory: system_setting.in,
  * materials.in and whatever restart / table files the deck switches on
  * (m.in, m_AFM.in, Hstat.in, p.in, q.in, Estat.in, u.in, v.in, E?_Yee.in,
- * H?_Yee.in, Hext.in, Eext.in, struct.in).  Replaces the reference's set-up
+ * H?_Yee.in, elastoforce.in, Jp1-3.in, strain_stat.in, eigenstraint0_crt.in,
+ * Hext.in, Eext.in, struct.in).  Replaces the reference's set-up
  * sequence main.cpp:21-167 (readgeo, read_global, *initialize_host,
  * input_*, copy_to_device, initialize_device and the initial static
  * solves).  `device` selects the CUDA device (-1 = current). */

@@ -76,3 +76,34 @@ def test_text_outputs_match_the_reference(gf, refrun, tmp_path, name):
     assert len(ref_files) >= 4
     for f in ref_files:
         _compare(str(tmp_path / "ref" / f), str(out / f))
+
+
+def test_restart_inputs_force_store_and_drude_currents(gf, refrun, tmp_path):
+    """elastoforce.in and Jp1-3.in (if_input_elastoforce, if_input_Jp) are
+    read as the reference reads them (inoutput.cpp:220-237, 283-328): the
+    stiffness damping of the first step uses the restored force store and
+    the Drude update starts from the restored pole currents."""
+    from test_gpu_parity import assert_trace_close, engine_trace
+    var = _variants(gf)
+    d = dataclasses.replace(var["drude_metal_layer"][0], steps=10)
+    rng = np.random.default_rng(41)
+    shape = (3, d.nx, d.ny, d.nz)
+    solid = (d.material_cell() != 0)[None]
+    metal = (d.material_cell() == 3)[None]
+    d.materials = [dataclasses.replace(m, stiff_damping=0.2 * d.dt / m.density) for m in d.materials]
+    d.force0 = rng.uniform(-1e9, 1e9, size=shape) * solid
+    d.jp0 = [rng.uniform(-1e8, 1e8, size=shape) * metal for _ in range(3)]
+    probe = (4, 4, 2)
+    gf.decks.write_deck(d, str(tmp_path / "deck"))
+    r = refrun.run(str(tmp_path / "deck"), str(tmp_path / "ref"), steps=10, probe=probe)
+    with gf.Engine(str(tmp_path / "deck"), device=0) as eng:
+        got = eng.download("force_store").reshape(shape)
+        assert np.array_equal(got, d.force0)
+        mine = engine_trace(eng, 10, probe)
+    assert_trace_close(mine, r["trace"])
+    # without the restored values the run differs (the inputs matter)
+    d.force0, d.jp0 = None, None
+    gf.decks.write_deck(d, str(tmp_path / "deck2"))
+    with gf.Engine(str(tmp_path / "deck2"), device=0) as eng:
+        other = engine_trace(eng, 10, probe)
+    assert np.max(np.abs(other - mine)) > 0.0
