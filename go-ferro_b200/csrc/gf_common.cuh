@@ -94,6 +94,7 @@ struct Params {
     int has_eig0, has_strain0, has_hext_nonunif;
     int estat;                 // E_stat may be nonzero (Estat.in, the electrostatic solve or an upload); 0: it is all +0
     int abc_1D, abc_elast_onlytop, abc_em_onlytop, pec_xy, pec_z;
+    int prescribed_m;             // if_prescribed_m: k = 0 ferromagnetic cells precess on a prescribed cone
     uint32_t fe_mask, fm_mask;   // bit id-1 set when material id is ferroelectric / ferromagnetic
     int spin;                 // spin pumping: inverse-spin-Hall current in the Yee E update
     int em_cls;               // the Yee E update reads per-edge material classes (StageIOT::ecls)
@@ -136,6 +137,7 @@ struct StageDrive {
     double usrc;           // displacement written on the source plane after the update
     double jf;             // J_f amplitude factor for the stage (types 1,2 times a per-k factor)
     double plane[3];       // plane-wave E written after the update
+    double pm[3];          // prescribed m of the k = 0 ferromagnetic cells after the update (if_prescribed_m)
     int usrc_on;
     int pad_;
 };

@@ -379,7 +379,6 @@ std::string unsupported(const Deck& d) {
     // kernels index cells and Yee vertices with 32-bit integers
     if ((double)(d.nx + 1) * (d.ny + 1) * (d.nz + 1) >= 2147483647.)
         return "grids with 2^31 or more Yee vertices are not supported (32-bit indexing)";
-    if (d.prescribed_m) return "prescribed-m test mode (if_prescribed_m) is not supported by this engine";
     if (d.elastostatic_1D || d.elastostatic_film || d.read_strain_ext)
         return "the 1-D and film elastostatic models and external strain (if_elastostatic_1D, if_elastostatic_film, if_read_strain_ext) are not supported by this engine";
     if (d.flexo && (d.elastostatic || d.in_straint0))
@@ -496,6 +495,7 @@ void build_params(gf_engine* eng) {
     P.em_back_P = d.em_back_P && d.em_dynamic;
     P.has_hext_nonunif = d.read_Hext_nonunif;
     P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
+    P.prescribed_m = (d.prescribed_m && d.any_fm) ? 1 : 0;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
     P.flexo = (d.flexo && d.any_fe) ? 1 : 0;
     P.elastostatic = d.elastostatic ? 1 : 0;
@@ -582,6 +582,21 @@ void step_drive(gf_engine* eng, StepDrive& sd) {
     }
     // local times of the four stages
     const double lt_ext[4] = {t - dt, t - dt * 0.5, t - dt * 0.5, t};
+    // prescribed m of the k = 0 ferromagnetic cells after each update
+    // (update_prescribed_m_half / _full / update_prescribed_m,
+    // magnetic_solver.cpp:1891-1960): at t - dt/2 after stages 1-2, at t
+    // after stage 3 and the step
+    double pm[4][3] = {};
+    if (d.prescribed_m) {
+        const double m0 = std::sin(d.precess_angle / 180. * PI);
+        const double omega = 2. * PI * d.precess_freq;
+        for (int s = 0; s < 4; s++) {
+            const double tt = (s < 2) ? t - dt * 0.5 : t;
+            pm[s][0] = std::sqrt((1. - m0 * m0));
+            pm[s][1] = m0 * std::sin(omega * tt);
+            pm[s][2] = m0 * std::cos(omega * tt);
+        }
+    }
     // static + alternating H of each stage (update_external_Hfield*, magnetic_solver.cpp:1834-1861)
     double Hf[4][3];
     for (int s = 0; s < 4; s++)
@@ -589,6 +604,7 @@ void step_drive(gf_engine* eng, StepDrive& sd) {
     for (int s = 0; s < 4; s++) {
         StageDrive& st = sd.st[s];
         std::memset(&st, 0, sizeof(st));
+        for (int a = 0; a < 3; a++) st.pm[a] = pm[s][a];
         for (int a = 0; a < 3; a++) {
             // With a prescribed table the ferromagnet keeps the shared Hext
             // (magnetic_solver.cpp:35-40) while get_dm_AFM_RK* always
@@ -1056,6 +1072,9 @@ int enqueue_stage(gf_engine* eng, int parity) {
                                       dim3(kThreads), 0, s_llg, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
         if (P.afm) GF_CU(klaunch<true>(eng, "k_llg_afm", k_llg_afm<S, R>, dim3(blocks_for(P.afm_bj * P.afm_bk, kThreads), (unsigned)P.afm_bi),
                                        dim3(kThreads), 0, s_llg, P, io, llg_tables<R>(eng), (int)eng->deck.mats.size()));
+        if (P.prescribed_m)
+            GF_CU(klaunch(eng, "k_prescribed_m", k_prescribed_m<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0,
+                          s_llg, P, io));
         GF_CU(rec(ev_llg, s_llg));
     }
     if (P.em && (em_after_llg || em_after_fe)) {
@@ -1293,7 +1312,7 @@ int setup_demag(gf_engine* eng) {
     // visits every cell (the ferromagnet's bounding box is the grid) and no
     // antiferromagnet adds to M
     eng->demag_src_fused = eng->demag_per_stage && !d.mag_1D && !d.demag_factor && P.fm && !P.afm &&
-                           P.fm_bi * P.fm_bj * P.fm_bk == P.n;
+                           P.fm_bi * P.fm_bj * P.fm_bk == P.n && !P.prescribed_m;
     if (eng->demag_mode != 0) return GF_OK;
     const long n21 = (long)P.nx * P.ny * (P.nz / 2 + 1);
     int dims[3] = {P.nx, P.ny, P.nz};
@@ -1473,6 +1492,22 @@ int initial_state(gf_engine* eng, const std::string& dir) {
                 uint8_t id = d.material_cell[(size_t)c];
                 if (id && d.mats[id - 1].fm) { buf[0][c] = mx; buf[1][c] = my; buf[2][c] = mz; }
             }
+        }
+        if (d.prescribed_m) {
+            // initialize_device's update_prescribed_m at time 0
+            // (magnetic_initialize.cpp:1072-1078): k = 0 ferromagnetic cells
+            const double m0 = std::sin(d.precess_angle / 180. * PI);
+            const double omega = 2. * PI * d.precess_freq;
+            const double t0 = 0.;
+            for (long i = 0; i < d.nx; i++)
+                for (long j = 0; j < d.ny; j++) {
+                    const long c = (i * d.ny + j) * d.nz;
+                    const uint8_t id = d.material_cell[(size_t)c];
+                    if (!(id && d.mats[id - 1].fm)) continue;
+                    buf[0][c] = std::sqrt((1. - m0 * m0));
+                    buf[1][c] = m0 * std::sin(omega * t0);
+                    buf[2][c] = m0 * std::cos(omega * t0);
+                }
         }
         GF_TRY(upload_vec(eng, eng->m.X, buf, n, eng->m.C));
     }

@@ -507,4 +507,27 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
     }
 }
 
+// Prescribed-m test mode (if_prescribed_m; update_prescribed_m_half /
+// _full / update_prescribed_m, magnetic_solver.cpp:1891-1960): after the
+// update of stage S the ferromagnetic cells of plane k = 0 take the stage
+// drive's prescribed m — the stage output for S < 3, the new step value for
+// S = 3 (in the mixed form with its compensation word cleared).  One thread
+// per (i, j).
+template <int S, class R>
+__global__ void k_prescribed_m(Params P, StageIOT<R> io) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)P.nx * P.ny) return;
+    const long i = t / P.ny, j = t - i * P.ny;
+    const long c = cid(P, i, j, 0);
+    const uint8_t id = io.mid[c];
+    if (id == 0 || !(io.mats[id - 1].flags & MF_FM)) return;
+    const StageDrive& dr = stage_drive(io, S);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        R* tgt = (S < 3) ? io.m_out.c[a] : io.m_acc.c[a];
+        tgt[c] = R(dr.pm[a]);
+        if constexpr (is_mixed<R>::value) { if (S == 3) io.m_cmp.c[a][c] = R(0); }
+    }
+}
+
 }  // namespace gf

@@ -147,7 +147,10 @@ __device__ __forceinline__ void rk_mixed_v(float xv, float av, float cv, float d
 
 // |m| = 1 for a stage state (FP32)
 __device__ __forceinline__ void renorm3(float& x, float& y, float& z) {
-    const float inv = 1.f / sqrtf(x * x + y * y + z * z);
+    // a zero vector stays zero (a ferromagnetic cell the deck leaves at m = 0
+    // keeps it, as the reference's unnormalised update does)
+    const float s2 = x * x + y * y + z * z;
+    const float inv = s2 > 0.f ? 1.f / sqrtf(s2) : 0.f;
     x = x * inv; y = y * inv; z = z * inv;
 }
 

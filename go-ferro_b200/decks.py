@@ -212,6 +212,11 @@ class Deck:
     # ave, m, magcell, AFMm, p, em, em_onecell, strain, Hstat, Estat, eig0,
     # q, uv, force, emYee, Jp, Jishe; em_onecell_index is 1-based
     outputs: dict = field(default_factory=lambda: {"ave": 1})
+    # prescribed-m test mode (if_prescribed_m): k = 0 ferromagnetic cells
+    # precess on a cone of precess_angle degrees at precess_freq Hz
+    prescribed_m: bool = False
+    precess_angle: float = 0.0
+    precess_freq: float = 0.0
     em_onecell_index: int = 0
     # electrostatics: 1-D model and its compensation (if_elec_1Dmodel,
     # if_elec_1D_compensate)
@@ -366,7 +371,7 @@ class Deck:
              " ".join(str(int(x)) for x in self.jf_lo),
              " ".join(str(int(x)) for x in self.jf_hi),
              f"{int(self.jf_type)} {self.jf_comp} {_f(self.jf_amp)} {_f(self.jf_freq)} {_f(self.jf_sigma)} {int(self.jf_cycles)}",
-             "false 0.0 0.0"]
+             f"{_b(self.prescribed_m)} {_f(self.precess_angle)} {_f(self.precess_freq)}"]
         return "\n".join(L) + "\n"
 
 

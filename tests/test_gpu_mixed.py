@@ -9,6 +9,7 @@ the probed H over the trace.  Per-component scales would divide FP32 noise by
 near-zero means (<m_x> of a film tilted by at most 1 degree), which measures
 the mean, not the solver.
 """
+import dataclasses
 import json
 import os
 
@@ -65,7 +66,7 @@ def test_mixed_matches_golden(gf, tmp_path, name):
                                    "two_fm_materials_dmi_uniaxial", "demag_factor", "elastic_multi_tile",
                                    "fm_film_demag_substrate", "rotated_magnetoelastic", "rotated_ferroelectric",
                                    "jf_type1", "jf_type3", "jf_type5", "mag_1d_model", "flexo_fe_film",
-                                   "flexo_rotated", "flexo_no_elastic"])
+                                   "flexo_rotated", "flexo_no_elastic", "prescribed_m_film"])
 def test_mixed_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
@@ -163,3 +164,22 @@ def assert_mixed_close_afm(mine, ref, tol=TOL_MIXED):
         out[name] = err / scale
         assert out[name] <= tol, f"{name}: relative trace error {out[name]:.3e} > {tol:.0e}"
     return out
+
+
+def test_mixed_keeps_zero_m_cells_zero(gf, refrun, tmp_path):
+    """Ferromagnetic cells a deck leaves at m = 0 keep m = 0 in the reference
+    (its update is not normalised); the mixed form's per-stage
+    renormalisation leaves a zero vector at zero instead of dividing by its
+    length."""
+    d = dataclasses.replace(_variants(gf)["prescribed_m_film"][0])
+    mc = d.material_cell()
+    m0 = d.m0.copy()
+    m0[:, :, :, 1:3] = 0.0        # two film planes left at m = 0
+    d.m0 = m0 * (mc == 2)
+    gf.decks.write_deck(d, str(tmp_path / "deck"))
+    r = refrun.run(str(tmp_path / "deck"), str(tmp_path / "ref"), steps=15, probe=(4, 8, 3), dump=True)
+    with gf.Engine(str(tmp_path / "deck"), device=0, precision="mixed") as eng:
+        assert_mixed_close(engine_trace(eng, 15, (4, 8, 3)), r["trace"])
+        m = eng.download("m").reshape(m0.shape)
+        assert np.all(m[:, :, :, 1:3] == 0.0)
+        eng.check_finite()

@@ -279,6 +279,15 @@ def _variants(gf):
     d.m0 = D.tilt_m0((8, 8, 10), 41, d.material_cell() == 2, max_deg=10.0)
     d.mag_1D = True
     v["mag_1d_model"] = (d, 15, None)
+    # prescribed-m test mode: the k = 0 plane of a ferromagnetic film on a
+    # magnetoelastic, Maxwell-coupled deck precesses on a 20-degree cone at
+    # 5e12 Hz (stage outputs and the step value of that plane overwritten)
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=2, film=6, steps=20)
+    d.layers = [(6, 2), (6, 0)]
+    d.m0 = D.tilt_m0((8, 16, 12), 51, d.material_cell() == 2)
+    d.amp_gauss *= 1e6
+    d.prescribed_m, d.precess_angle, d.precess_freq = True, 20.0, 5e12
+    v["prescribed_m_film"] = (d, 20, (4, 8, 3))
     # flexoelectric coupling (if_flexo): polarisation- and strain-gradient
     # terms of the TDGL field (ferroelectric_solver.cpp:800-833), the
     # p-gradient eigenstrain (elastic_dynamic_solver.cpp:63-70), with the
@@ -323,7 +332,7 @@ def test_random_struct_variants_cover_both_yee_paths(gf):
                                    "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
                                    "random_struct_6mat", "rotated_magnetoelastic", "rotated_ferroelectric",
                                    "jf_type0", "jf_type1", "jf_type2", "jf_type3", "jf_type5", "mag_1d_model",
-                                   "flexo_fe_film", "flexo_rotated", "flexo_no_elastic"])
+                                   "flexo_fe_film", "flexo_rotated", "flexo_no_elastic", "prescribed_m_film"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
     gf.decks.write_deck(d, str(tmp_path / "deck"))
