@@ -483,9 +483,9 @@ def adjoint_cost(gf, torch, args, local_rank):
     (the configuration's form) and in FP64.  Every time is device time on the
     engine's stream (CUDA events around the enqueued work, host launch gaps
     included): the engine's graph-replayed forward step of the same
-    precision, the adjoint's own forward run (checkpoints every 200 steps,
-    <m_x> trace) and its backward run (block recomputation, stage recompute,
-    reverse sweep).  The mixed entry also gives the relative difference of
+    precision, the adjoint's own forward run (checkpoints every 100 steps,
+    <m_x> trace) and its backward run (each checkpoint block recomputed once
+    with its stages kept in the stage store, then the reverse sweep).  The mixed entry also gives the relative difference of
     its gradients from the FP64 adjoint's on the same inputs."""
     mu0 = 1.256637061e-6
     steps, K, nw = args.adjoint_steps, args.adjoint_checkpoint, 256
@@ -540,20 +540,24 @@ def adjoint_cost(gf, torch, args, local_rank):
                     e1.synchronize()
                     t_bwd = e0.elapsed_time(e1) / 1e3
                     grads[prec] = (gw, ga)
+                    store_used, store_bytes = adj.store_info()
             out[prec] = {"steps": steps, "checkpoint_every": K,
                          "forward_ms_per_step": 1e3 * t_eng / steps,
                          "adjoint_forward_ms_per_step": 1e3 * t_fwd / steps,
                          "backward_ms_per_step": 1e3 * t_bwd / steps,
                          "backward_over_forward": t_bwd / t_eng,
                          "forward_plus_backward_over_forward": (t_fwd + t_bwd) / t_eng,
-                         "loss_band_bins": int(len(band))}
+                         "loss_band_bins": int(len(band)),
+                         "backward_layout": "stage store" if store_used else "recompute",
+                         "backward_layout_bytes": store_bytes}
     (gw, ga), (gw64, ga64) = grads["mixed"], grads["fp64"]
     out["mixed"]["grad_wave_rel_diff_vs_fp64"] = float(np.max(np.abs(gw - gw64)) / max(np.max(np.abs(gw64)), 1e-300))
     out["mixed"]["grad_alpha_rel_diff_vs_fp64"] = float(np.max(np.abs(ga - ga64)) / max(np.max(np.abs(ga64)), 1e-300))
     out["workload"] = (f"FM LLG + FFT magnetostatics + magnetoelastic elastodynamics, {gx}x{gy}x{gz}, "
                        "per-cell alpha and 256-sample waveform; FP32 mixed (the configuration's form) and FP64")
     out["timing"] = "device time (CUDA events on the engine stream)"
-    out["definition"] = ("backward = recompute of every checkpoint block + per-step stage recompute + reverse sweep; "
+    out["definition"] = ("backward = recompute of every checkpoint block (stage store layout: keeping each step's stages; "
+                         "recompute layout: a second per-step stage recompute) + reverse sweep; "
                          "forward = the engine's step of the same precision (CUDA graph)")
     return out
 
@@ -830,7 +834,7 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=100)
     ap.add_argument("--adjoint-steps", type=int, default=400)
     ap.add_argument("--adjoint-grid", default="256x256x32", help="grid of the adjoint cost measurement (NXxNYxNZ)")
-    ap.add_argument("--adjoint-checkpoint", type=int, default=200, help="steps between the adjoint's stored states")
+    ap.add_argument("--adjoint-checkpoint", type=int, default=100, help="steps between the adjoint's stored states")
     args = ap.parse_args()
     global GRID_OVERRIDE
     if args.grid:

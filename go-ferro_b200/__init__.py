@@ -40,7 +40,8 @@ EXPORTS = ["gf_create_from_deck", "gf_create_from_deck_ex", "gf_advance", "gf_ad
            "gf_get_info", "gf_profile_steps", "gf_synchronize", "gf_stream", "gf_check_finite", "gf_last_error",
            "gf_destroy", "gf_version", "gf_field_mean_noalloc", "gf_check_quotients",
            "gf_adjoint_create", "gf_adjoint_set_alpha", "gf_adjoint_set_waveform", "gf_adjoint_forward",
-           "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_destroy",
+           "gf_adjoint_backward", "gf_adjoint_final_m", "gf_adjoint_set_store_limit", "gf_adjoint_store_info",
+           "gf_adjoint_destroy",
            "gf_write_outputs", "gf_run_deck", "gf_batch_create", "gf_batch_create_ex", "gf_batch_plan", "gf_batch_advance", "gf_batch_synchronize",
            "gf_batch_stream", "gf_batch_tuned_chunk",
            "gf_batch_last_error", "gf_batch_destroy", "gf_set_electrostatics", "gf_set_elastostatics",
@@ -225,6 +226,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.gf_adjoint_forward.argtypes = [vp, c_u64, c_dbl_p]
     lib.gf_adjoint_backward.argtypes = [vp, c_dbl_p, c_dbl_p, c_dbl_p]
     lib.gf_adjoint_final_m.argtypes = [vp, c_dbl_p, ctypes.c_size_t]
+    lib.gf_adjoint_set_store_limit.argtypes = [vp, ctypes.c_int64]
+    lib.gf_adjoint_store_info.argtypes = [vp, ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_int64)]
     lib.gf_adjoint_destroy.argtypes = [vp]
     lib.gf_adjoint_destroy.restype = None
     lib.gf_set_electrostatics.argtypes = [vp, c_int, ctypes.POINTER(c_int)]
@@ -471,6 +474,19 @@ class Adjoint:
         ga = np.empty(self.n, dtype=np.float64)
         self.engine._check(self.lib.gf_adjoint_backward(self.h, _dp(g), _dp(gw), _dp(ga)))
         return gw, ga
+
+    def set_store_limit(self, nbytes: int) -> None:
+        """Device memory the backward run may hold for a block's stage store:
+        -1 automatic (the default), 0 never (recompute each step's stages),
+        or a byte count; both layouts give identical gradients."""
+        self.engine._check(self.lib.gf_adjoint_set_store_limit(self.h, int(nbytes)))
+
+    def store_info(self):
+        """(used, bytes): whether the last backward run kept the stage store,
+        and the memory its layout held."""
+        used, nbytes = ctypes.c_int(), ctypes.c_int64()
+        self.engine._check(self.lib.gf_adjoint_store_info(self.h, ctypes.byref(used), ctypes.byref(nbytes)))
+        return bool(used.value), int(nbytes.value)
 
     def final_m(self) -> np.ndarray:
         m = np.empty(3 * self.n, dtype=np.float64)

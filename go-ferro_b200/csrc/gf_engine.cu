@@ -3904,11 +3904,15 @@ void gf_batch_destroy(gf_batch* b) {
 //
 // The forward run starts from the engine's current m and external-field
 // clock, keeps the state every `ck_every` steps, and records <m_x> of every
-// step.  The backward run walks the blocks between checkpoints in reverse:
-// it recomputes and stores the block's step values, then for each step
-// recomputes the four stage states and fields (demag of each stage by FFT)
-// and applies the reverse RK4 sweep of gf_adjoint.cuh, accumulating the
-// damping and waveform gradients.
+// step.  The backward run walks the blocks between checkpoints in reverse.
+// Store layout (when the block's stage fields fit in device memory): it
+// recomputes the block from its checkpoint once, keeping every step's stage
+// states, fields and strains, then applies the reverse RK4 sweep of
+// gf_adjoint.cuh step by step from those.  Recompute layout: it recomputes
+// and keeps the block's step values only, and recomputes each step's four
+// stages (demag of each stage by FFT) again right before its sweep.  Both
+// layouts run the same kernels on the same values, so their gradients are
+// identical bit for bit.
 // ===========================================================================
 struct gf_adjoint {
     gf_engine* eng = nullptr;
@@ -3960,7 +3964,14 @@ struct gf_adjoint {
     double* trace = nullptr;         // nsteps+1 (FP64)
     double* dldm = nullptr;          // nsteps+1 (FP64)
     double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x ck_len
-    double* xs = nullptr;            // step values of one block, ck_every x ns n
+    double* xs = nullptr;            // step values of one block, ck_every x ns n (recompute layout)
+    size_t xs_bytes = 0;
+    // stage store of one block (store layout): per step m of the step value,
+    // the stage states, the stage fields and the stage strains
+    double* store = nullptr;
+    size_t store_bytes = 0;
+    int64_t store_limit = -1;        // -1 automatic, 0 never, > 0 at most this many bytes
+    bool store_used = false;         // layout of the last backward run
     double* zero3 = nullptr;         // 3n zeros (demag field when magnetostatics is off)
     double* wide = nullptr;          // FP32: 3n FP64 values of the final m
     size_t ck_slots = 0;
@@ -4266,14 +4277,16 @@ cudaError_t adj_el_vjp_launch(gf_adjoint* a) {
 // reverse sweep of step `step` (lambda = d loss / d x_{step+1} in LAM on entry,
 // d loss / d x_step on exit; with elastodynamics also phi = d loss / d fs);
 // x is the step value x_step
+// (recompute: the step's stages are formed here first; otherwise Y, HS and
+// STR already hold them and only m of x is read)
 template <class R>
-int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
+int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step, bool recompute) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     cudaStream_t st = eng->stream;
     const unsigned bn = blocks_for(P.n, kThreads);
     const int ng = a->el ? 3 : 1;               // cotangent groups: m, u, v
-    GF_TRY(adj_stages<R>(a, x, step, v3<R>(a->XJ), a->f32 ? v3<R>(a->XJC) : F3T<R>{}));
+    if (recompute) GF_TRY(adj_stages<R>(a, x, step, v3<R>(a->XJ), a->f32 ? v3<R>(a->XJC) : F3T<R>{}));
     if (a->el) {
         // the new u(k = 0) came from the Liao extrapolation, not the RK sum
         const long plane = (long)P.nx * P.ny;
@@ -4331,8 +4344,91 @@ int adj_step_backward(gf_adjoint* a, double* const* x, uint64_t step) {
 int adj_fwd(gf_adjoint* a, double** x, uint64_t step) {
     return a->f32 ? adj_step_forward<float>(a, x, step) : adj_step_forward<double>(a, x, step);
 }
-int adj_bwd(gf_adjoint* a, double* const* x, uint64_t step) {
-    return a->f32 ? adj_step_backward<float>(a, x, step) : adj_step_backward<double>(a, x, step);
+int adj_bwd(gf_adjoint* a, double* const* x, uint64_t step, bool recompute) {
+    return a->f32 ? adj_step_backward<float>(a, x, step, recompute) : adj_step_backward<double>(a, x, step, recompute);
+}
+
+// elements of one step's slot in the stage store: m of the step value (3 n),
+// the stage states y2..y4 (9 n), the four stage fields (12 n) and, with the
+// magnetoelastic field, the four stage strains (24 n)
+size_t adj_slot_len(const gf_adjoint* a) {
+    return (size_t)((a->el && a->eng->P.elasto_on) ? 48 : 24) * (size_t)a->eng->P.n;
+}
+
+// points Y, HS (and STR) at a slot of the stage store while it lives, and
+// puts the adjoint's own buffers back when it goes
+struct AdjSlotView {
+    gf_adjoint* a;
+    double* Y[3][3];
+    double* HS[4][3];
+    double* STR[4][6];
+    explicit AdjSlotView(gf_adjoint* a_) : a(a_) {
+        std::memcpy(Y, a->Y, sizeof(Y)); std::memcpy(HS, a->HS, sizeof(HS)); std::memcpy(STR, a->STR, sizeof(STR));
+    }
+    ~AdjSlotView() {
+        std::memcpy(a->Y, Y, sizeof(Y)); std::memcpy(a->HS, HS, sizeof(HS)); std::memcpy(a->STR, STR, sizeof(STR));
+    }
+    // slot `k` of the store; xm gets the slot's m of the step value
+    void point(size_t k, double* xm[3]) {
+        const size_t n = (size_t)a->eng->P.n;
+        double* base = adj_at(a, a->store, k * adj_slot_len(a));
+        size_t off = 0;
+        for (int c = 0; c < 3; c++, off += n) xm[c] = adj_at(a, base, off);
+        for (int s = 0; s < 3; s++)
+            for (int c = 0; c < 3; c++, off += n) a->Y[s][c] = adj_at(a, base, off);
+        for (int s = 0; s < 4; s++)
+            for (int c = 0; c < 3; c++, off += n) a->HS[s][c] = adj_at(a, base, off);
+        if (a->el && a->eng->P.elasto_on)
+            for (int s = 0; s < 4; s++)
+                for (int q = 0; q < 6; q++, off += n) a->STR[s][q] = adj_at(a, base, off);
+    }
+};
+
+// the backward run's layout for blocks of kb steps: the stage store when it
+// fits the limit and the device's free memory less a reserve of
+// max(4 GiB, 1/16 of the device), else the step values (recompute layout)
+int adj_prepare_backward(gf_adjoint* a, uint64_t kb) {
+    gf_engine* eng = a->eng;
+    const size_t need = (size_t)kb * adj_slot_len(a) * a->esz;
+    a->store_used = false;
+    if (a->store_limit != 0) {
+        if (a->store && a->store_bytes >= need && (a->store_limit < 0 || need <= (size_t)a->store_limit)) {
+            a->store_used = true;
+        } else {
+            adj_free(a, &a->store);
+            a->store_bytes = 0;
+            size_t fr = 0, tot = 0;
+            GF_CU(cudaMemGetInfo(&fr, &tot));
+            const size_t avail = fr + (a->xs ? a->xs_bytes : 0);
+            const size_t reserve = std::max<size_t>((size_t)4 << 30, tot / 16);
+            size_t budget = avail > reserve ? avail - reserve : 0;
+            if (a->store_limit > 0) budget = std::min<size_t>(budget, (size_t)a->store_limit);
+            if (need <= budget) {
+                adj_free(a, &a->xs);
+                a->xs_bytes = 0;
+                if (cudaMalloc(&a->store, need) == cudaSuccess) {
+                    a->allocs.push_back(a->store);
+                    a->store_bytes = need;
+                    a->store_used = true;
+                } else {
+                    (void)cudaGetLastError();
+                    a->store = nullptr;
+                }
+            }
+        }
+    }
+    if (!a->store_used) {
+        adj_free(a, &a->store);
+        a->store_bytes = 0;
+        const size_t xneed = (size_t)kb * a->ns * (size_t)eng->P.n * a->esz;
+        if (!a->xs || a->xs_bytes < xneed) {
+            adj_free(a, &a->xs);
+            a->xs_bytes = 0;
+            GF_TRY(adj_alloc(a, &a->xs, (size_t)kb * a->ns * (size_t)eng->P.n));
+            a->xs_bytes = xneed;
+        }
+    }
+    return GF_OK;
 }
 int adj_inject(gf_adjoint* a, long slot, double inv_nfm) {
     gf_engine* eng = a->eng;
@@ -4521,7 +4617,6 @@ int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint
     if ((rc = adj_alloc_d(a, &a->hacc, (size_t)n)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc_d(a, &a->wbar, (size_t)n_wave)) != GF_OK) return fail(rc);
     if ((rc = adj_alloc(a, &a->zero3, (size_t)3 * n)) != GF_OK) return fail(rc);
-    if ((rc = adj_alloc(a, &a->xs, (size_t)checkpoint_every * a->ns * n)) != GF_OK) return fail(rc);
     if (cudaStreamSynchronize(eng->stream) != cudaSuccess) { eng->err = "adjoint set-up"; return fail(GF_ECUDA); }
     *out = a;
     return GF_OK;
@@ -4649,24 +4744,45 @@ int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wav
     GF_TRY(adj_inject(a, (long)N, inv_nfm));
     const uint64_t K = (uint64_t)a->ck_every;
     const uint64_t nblocks = (N + K - 1) / K;
+    GF_TRY(adj_prepare_backward(a, std::min<uint64_t>(K, N)));
+    // the reverse sweep of step k from step value xp (m only in the store
+    // layout), then the loss cotangent of step k
+    auto sweep = [&](double* const* xp, uint64_t k, bool recompute) -> int {
+        const long seg = (long)((k * (uint64_t)a->nw) / N);
+        if (seg != cur_seg) {
+            if (cur_seg >= 0) GF_TRY(adj_wave_flush(a, cur_seg));
+            cur_seg = seg;
+        }
+        GF_TRY(adj_bwd(a, xp, k, recompute));
+        return adj_inject(a, (long)k, inv_nfm);
+    };
     for (uint64_t b = nblocks; b-- > 0;) {
         const uint64_t s0 = b * K, s1 = std::min(N, s0 + K);
-        // recompute the block's step values x_s0 .. x_{s1-1}
         GF_TRY(adj_load(a, adj_at(a, a->ck, b * a->ck_len), true));
-        for (uint64_t k = s0; k < s1; k++) {
-            GF_TRY(adj_save(a, adj_at(a, a->xs, (k - s0) * (size_t)a->ns * n), false));
-            if (k + 1 < s1) GF_TRY(adj_fwd(a, a->X, k));
-        }
-        for (uint64_t k = s1; k-- > s0;) {
-            double* xp[21] = {};
-            for (int q = 0; q < a->ns; q++) xp[a->sidx[q]] = adj_at(a, a->xs, ((k - s0) * (size_t)a->ns + q) * n);
-            const long seg = (long)((k * (uint64_t)a->nw) / N);
-            if (seg != cur_seg) {
-                if (cur_seg >= 0) GF_TRY(adj_wave_flush(a, cur_seg));
-                cur_seg = seg;
+        if (a->store_used) {
+            // recompute the block once, keeping every step's stages
+            AdjSlotView view(a);
+            double* xm[3];
+            for (uint64_t k = s0; k < s1; k++) {
+                view.point(k - s0, xm);
+                for (int c = 0; c < 3; c++) GF_CU(cudaMemcpyAsync(xm[c], a->X[c], ez * n, cudaMemcpyDeviceToDevice, st));
+                GF_TRY(adj_fwd(a, a->X, k));
             }
-            GF_TRY(adj_bwd(a, xp, k));
-            GF_TRY(adj_inject(a, (long)k, inv_nfm));
+            for (uint64_t k = s1; k-- > s0;) {
+                view.point(k - s0, xm);
+                GF_TRY(sweep(xm, k, false));
+            }
+        } else {
+            // recompute the block's step values x_s0 .. x_{s1-1}
+            for (uint64_t k = s0; k < s1; k++) {
+                GF_TRY(adj_save(a, adj_at(a, a->xs, (k - s0) * (size_t)a->ns * n), false));
+                if (k + 1 < s1) GF_TRY(adj_fwd(a, a->X, k));
+            }
+            for (uint64_t k = s1; k-- > s0;) {
+                double* xp[21] = {};
+                for (int q = 0; q < a->ns; q++) xp[a->sidx[q]] = adj_at(a, a->xs, ((k - s0) * (size_t)a->ns + q) * n);
+                GF_TRY(sweep(xp, k, true));
+            }
         }
     }
     if (cur_seg >= 0) GF_TRY(adj_wave_flush(a, cur_seg));
@@ -4701,6 +4817,20 @@ int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count) {
     }
     GF_TRY(static_field_now(eng));
     GF_CU(cudaStreamSynchronize(st));
+    return GF_OK;
+}
+
+int gf_adjoint_set_store_limit(gf_adjoint* a, int64_t bytes) {
+    GF_TRY(adj_check(a));
+    if (bytes < -1) { a->eng->err = "gf_adjoint_set_store_limit: need -1, 0 or a byte count"; return GF_EINVAL; }
+    a->store_limit = bytes;
+    return GF_OK;
+}
+
+int gf_adjoint_store_info(gf_adjoint* a, int* used, int64_t* bytes) {
+    GF_TRY(adj_check(a));
+    if (used) *used = a->store_used ? 1 : 0;
+    if (bytes) *bytes = a->store_used ? (int64_t)a->store_bytes : (int64_t)a->xs_bytes;
     return GF_OK;
 }
 

@@ -488,8 +488,12 @@ void gf_batch_destroy(gf_batch* b);
  * engine while an adjoint call runs. */
 typedef struct gf_adjoint gf_adjoint;
 /* checkpoint_every: steps between stored states (the backward run recomputes
- * the steps in between; device memory ~ 24 * n * checkpoint_every bytes, 96
- * with elastodynamics; mixed form 24 and 84). */
+ * the steps in between).  Device memory: a stored state is 24 * n bytes, 96
+ * with elastodynamics (mixed form 24 and 84) per checkpoint; the backward run
+ * adds one block's stage store, checkpoint_every * 192 * n bytes (384 with
+ * the magnetoelastic field; half in the mixed form), when it fits (see
+ * gf_adjoint_set_store_limit), else one block's step values (the stored
+ * state's size per step) and a second forward evaluation of every step. */
 int gf_adjoint_create(gf_engine* e, int n_wave, int checkpoint_every, gf_adjoint** out);
 /* per-cell damping (nx*ny*nz values; default: the material's alpha) */
 int gf_adjoint_set_alpha(gf_adjoint* a, const double* alpha, size_t count);
@@ -506,6 +510,16 @@ int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace);
 int gf_adjoint_backward(gf_adjoint* a, const double* dloss_dmx, double* grad_wave, double* grad_alpha);
 /* m after the last forward step (3*nx*ny*nz values, component-major). */
 int gf_adjoint_final_m(gf_adjoint* a, double* host_m, size_t count);
+/* Device memory the backward run may hold for a block's stage store (the
+ * stage states, fields and strains of every step of a checkpoint block, so
+ * that each step is evaluated once in the reverse pass instead of twice):
+ * -1 (default) = when it fits the device's free memory less a reserve of
+ * max(4 GiB, 1/16 of the device); 0 = never; > 0 = at most that many bytes.
+ * Both layouts give identical gradients. */
+int gf_adjoint_set_store_limit(gf_adjoint* a, int64_t bytes);
+/* Layout of the last backward run: *used = 1 with the stage store, 0 with
+ * the step values only; *bytes = the memory that layout held. */
+int gf_adjoint_store_info(gf_adjoint* a, int* used, int64_t* bytes);
 void gf_adjoint_destroy(gf_adjoint* a);
 
 /* Mean of a device array, allocating nothing: *dev_out = sum(dev_in[0..n)) /

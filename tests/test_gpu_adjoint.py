@@ -132,6 +132,40 @@ def test_adjoint_checkpoint_interval_does_not_change_gradients(gf, tmp_path):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["fm_film", "magnetoelastic"])
+def test_adjoint_stage_store_and_recompute_layouts_agree(gf, tmp_path, case, precision):
+    """The backward run with every step's stages kept (stage store) and with
+    the stages recomputed per step from the stored step values gives the same
+    gradients bit for bit, over blocks that do not divide the run (23 steps,
+    checkpoints every 7), and a byte limit below one block's store selects
+    the recompute layout."""
+    steps, nw = 23, 5
+    if case == "fm_film":
+        film(gf, tmp_path, nx=16, ny=16, nz=8, steps=steps)
+    else:
+        me_film(gf, tmp_path, nx=16, ny=16, nz=8, steps=steps)
+    n = 16 * 16 * 8
+    slot = (48 if case == "magnetoelastic" else 24) * n * (4 if precision == "mixed" else 8)
+    out, layouts = [], []
+    with gf.Engine(str(tmp_path), device=0, precision=precision) as eng:
+        eng.advance(3)
+        for limit in (-1, 0, 7 * slot - 1, 7 * slot):
+            with gf.Adjoint(eng, n_wave=nw, checkpoint_every=7) as adj:
+                adj.set_store_limit(limit)
+                adj.set_waveform(np.linspace(-3e3, 5e3, nw))
+                tr = adj.forward(steps)
+                g = np.cos(0.3 * np.arange(steps + 1))
+                out.append((tr,) + adj.backward(g))
+                layouts.append(adj.store_info())
+    assert [u for u, _ in layouts] == [True, False, False, True]
+    assert layouts[0][1] == 7 * slot and layouts[3][1] == 7 * slot
+    assert np.max(np.abs(out[0][1])) > 0.0 and np.max(np.abs(out[0][2])) > 0.0
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert np.array_equal(a, b)
+
+
 def test_adjoint_rejects_unsupported_decks(gf, tmp_path):
     d = gf.decks.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=5)
     gf.decks.write_deck(d, str(tmp_path))
