@@ -101,6 +101,7 @@ struct Params {
     int drude;                // some material has a Drude pole (omega_plasma != 0)
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;
+    int mag1d_em;             // if_mag_1Dmodel with M-sourced Maxwell fields: the cell-centred Maxwell H_z is the 1-D field
     int flexo;                // if_flexo with ferroelectrics: StageIOT::sg / pge are set
     int elastostatic;         // if_elastostatic: the TDGL field adds the static strain and eigenstrain
     double liao_w;

@@ -384,7 +384,6 @@ std::string unsupported(const Deck& d) {
     if (d.flexo && (d.elastostatic || d.in_straint0))
         return "flexoelectricity with a static strain (if_elastostatic or strain_stat.in) is not supported by this engine";
     if (d.num_materials > (unsigned)kMaxMat) return "more than 32 materials";
-    if (d.mag_1D && d.em_dynamic && d.em_fromM) return "if_mag_1Dmodel together with Maxwell coupling is not supported by this engine";
     for (size_t i = 0; i < d.mats.size(); i++) {
         const Material& m = d.mats[i];
         if (m.fm && m.aniso_type > 2) return "anisotropy_type must be 0, 1 or 2";
@@ -497,6 +496,7 @@ void build_params(gf_engine* eng) {
     P.abc_1D = d.abc_1D; P.abc_elast_onlytop = d.abc_elast_onlytop; P.abc_em_onlytop = d.abc_em_onlytop;
     P.prescribed_m = (d.prescribed_m && d.any_fm) ? 1 : 0;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
+    P.mag1d_em = (d.mag_1D && d.em_dynamic && d.em_fromM) ? 1 : 0;
     P.flexo = (d.flexo && d.any_fe) ? 1 : 0;
     P.elastostatic = d.elastostatic ? 1 : 0;
     P.drude = 0; P.pec = 0;
@@ -2073,6 +2073,20 @@ int em_cells(gf_engine* eng, long c0, long count) {
     else
         GF_CU(launch(k_em_cell<double>, dim3(blocks_for(count, kThreads)), dim3(kThreads), 0, eng->stream, P,
                      f3(cur(eng, eng->E)), f3(cur(eng, eng->H)), Ec, Hc, c0, count));
+    if (P.mag1d_em) {
+        // H_z of the 1-D model in place of the face mean
+        const double* mz = (eng->deck.any_fm) ? cur(eng, eng->m)[2] : nullptr;
+        const double* z1 = (eng->deck.any_afm) ? cur(eng, eng->a1)[2] : nullptr;
+        const double* z2 = (eng->deck.any_afm) ? cur(eng, eng->a2)[2] : nullptr;
+        if (eng->mixed)
+            GF_CU(launch(k_em_cell_hz_1d<float>, dim3(blocks_for(count, kThreads)), dim3(kThreads), 0, eng->stream,
+                         (const DevMatT<float>*)eng->mats_f, (const uint8_t*)eng->mid, (const float*)mz, (const float*)z1,
+                         (const float*)z2, (const float*)eng->Hstat[2], Hc.c[2], c0, count));
+        else
+            GF_CU(launch(k_em_cell_hz_1d<double>, dim3(blocks_for(count, kThreads)), dim3(kThreads), 0, eng->stream,
+                         (const DevMatT<double>*)eng->mats, (const uint8_t*)eng->mid, mz, z1, z2, (const double*)eng->Hstat[2],
+                         Hc.c[2], c0, count));
+    }
     return GF_OK;
 }
 

@@ -212,7 +212,11 @@ __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_LLG_MINB_F32 : GF
             const int hz0 = (i * ny + j) * (nz + 1) + k, hz1 = hz0 + 1;
             Hx = Hx + (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / R(2.);
             Hy = Hy + (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / R(2.);
-            Hz = Hz + (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
+            // with the 1-D magnetostatic model the cell's Maxwell H_z is
+            // -Ms m_z - H_stat,z of the stage state (:3793-3804; the
+            // sublattice terms are zero in a ferromagnetic cell)
+            if (P.mag1d_em) Hz = Hz + (-R(1.) * mat.Ms * mzc - io.Hstat.c[2][c]);
+            else Hz = Hz + (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
         }
 
         const R precess = mat.precess;
@@ -376,7 +380,15 @@ __global__ void __launch_bounds__(256, 2) k_llg_afm(Params P, StageIOT<R> io, co
             const int hz0 = (i * ny + j) * (nz + 1) + k, hz1 = hz0 + 1;
             Hem[0] = (io.H_in.c[0][hx0] + io.H_in.c[0][hx1]) / R(2.);
             Hem[1] = (io.H_in.c[1][hy0] + io.H_in.c[1][hy1]) / R(2.);
-            Hem[2] = (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
+            if (P.mag1d_em) {
+                // the 1-D model's H_z of the stage state (:3793-3804)
+                const DevMatT<R>& dm_ = io.mats[id - 1];
+                const R mzc = P.fm ? io.m_in.c[2][c] : R(0.);
+                Hem[2] = -R(1.) * dm_.Ms * mzc - R(1.) * dm_.Ms1 * io.a1_in.c[2][c] - R(1.) * dm_.Ms2 * io.a2_in.c[2][c]
+                         - io.Hstat.c[2][c];
+            } else {
+                Hem[2] = (io.H_in.c[2][hz0] + io.H_in.c[2][hz1]) / R(2.);
+            }
         }
         const StageDrive& dr = stage_drive(io, S);
         const double h[3] = {P.dx, P.dy, P.dz}, rh[3] = {P.rdx, P.rdy, P.rdz};
@@ -528,6 +540,25 @@ __global__ void k_prescribed_m(Params P, StageIOT<R> io) {
         tgt[c] = R(dr.pm[a]);
         if constexpr (is_mixed<R>::value) { if (S == 3) io.m_cmp.c[a][c] = R(0); }
     }
+}
+
+// z component of the cell-centred Maxwell H when the 1-D magnetostatic
+// model meets M-sourced Maxwell fields (update_DH_cell, EMdynamic_solver.cpp:
+// 3793-3804): -Ms m_z - Ms1 m1_z - Ms2 m2_z - H_stat,z of the cell's current
+// step value, zero in vacuum; written over the face mean that k_em_cell
+// leaves in out (cells c0 .. c0 + count - 1; mz, mz1, mz2 null where the run
+// has no such magnet)
+template <class R>
+__global__ void k_em_cell_hz_1d(const DevMatT<R>* __restrict__ mats, const uint8_t* __restrict__ mid, const R* __restrict__ mz,
+                                const R* __restrict__ mz1, const R* __restrict__ mz2, const R* __restrict__ hz,
+                                double* __restrict__ out, long c0, long count) {
+    const long c = c0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c0 + count) return;
+    const uint8_t id = mid[c];
+    if (id == 0) { out[c] = 0.; return; }
+    const DevMatT<R>& m = mats[id - 1];
+    const R z = mz ? mz[c] : R(0.), z1 = mz1 ? mz1[c] : R(0.), z2 = mz2 ? mz2[c] : R(0.);
+    out[c] = (double)(-R(1.) * m.Ms * z - R(1.) * m.Ms1 * z1 - R(1.) * m.Ms2 * z2 - hz[c]);
 }
 
 }  // namespace gf

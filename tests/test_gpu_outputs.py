@@ -39,6 +39,11 @@ def _decks(gf):
     d = dataclasses.replace(var["drude_metal_layer"][0], steps=6)
     d.outputs = {"Jp": 3, "em": 6, "ave": 2}
     v["drude"] = d
+    # the 1-D magnetostatic model's cell H_z in the EM outputs
+    d = dataclasses.replace(var["mag_1d_maxwell"][0], steps=8)
+    d.outputs = {"ave": 2, "em": 4, "em_onecell": 2, "m": 8}
+    d.em_onecell_index = 703     # (3, 10, 6), inside the film
+    v["mag_1d_maxwell"] = d
     return v
 
 
@@ -60,7 +65,7 @@ def _compare(path_ref, path_mine):
     assert not bad.any(), (os.path.basename(path_ref), err, scale)
 
 
-@pytest.mark.parametrize("name", ["ferroelectric", "magnetoelastic", "afm", "drude"])
+@pytest.mark.parametrize("name", ["ferroelectric", "magnetoelastic", "afm", "drude", "mag_1d_maxwell"])
 def test_text_outputs_match_the_reference(gf, refrun, tmp_path, name):
     d = _decks(gf)[name]
     gf.decks.write_deck(d, str(tmp_path / "deck"))

@@ -279,6 +279,22 @@ def _variants(gf):
     d.m0 = D.tilt_m0((8, 8, 10), 41, d.material_cell() == 2, max_deg=10.0)
     d.mag_1D = True
     v["mag_1d_model"] = (d, 15, None)
+    # the 1-D model with M-sourced Maxwell fields acting back on m: the
+    # cell-centred Maxwell H_z is the 1-D field -Ms m_z - H_stat,z of the
+    # stage state (update_DH_cell, EMdynamic_solver.cpp:3793-3804), for a
+    # ferromagnetic and an antiferromagnetic film
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=20)
+    d.m0 = D.tilt_m0((8, 16, 12), 61, d.material_cell() == 2, max_deg=15.0)
+    d.amp_gauss *= 1e6
+    d.mag_1D = True
+    v["mag_1d_maxwell"] = (d, 20, (4, 8, 7))
+    d = D.preset_magnetoelastic(nx=8, ny=16, nz=12, sub=5, film=4, steps=20)
+    d.materials = [D.ggg(), D.afm_uniaxial(0.01, magnetoelastic=True)]
+    d.m0 = None
+    d.afm0 = D.tilt_afm0((8, 16, 12), 63, d.material_cell() == 2)
+    d.amp_gauss *= 1e6
+    d.mag_1D = True
+    v["afm_mag_1d_maxwell"] = (d, 20, (4, 8, 7))
     # prescribed-m test mode: the k = 0 plane of a ferromagnetic film on a
     # magnetoelastic, Maxwell-coupled deck precesses on a 20-degree cone at
     # 5e12 Hz (stage outputs and the step value of that plane overwritten)
@@ -332,6 +348,7 @@ def test_random_struct_variants_cover_both_yee_paths(gf):
                                    "drude_metal_layer", "pec_layer", "spin_pumping_ishe", "random_struct_3mat",
                                    "random_struct_6mat", "rotated_magnetoelastic", "rotated_ferroelectric",
                                    "jf_type0", "jf_type1", "jf_type2", "jf_type3", "jf_type5", "mag_1d_model",
+                                   "mag_1d_maxwell", "afm_mag_1d_maxwell",
                                    "flexo_fe_film", "flexo_rotated", "flexo_no_elastic", "prescribed_m_film"])
 def test_engine_matches_live_oracle(gf, refrun, tmp_path, vname):
     d, steps, probe = _variants(gf)[vname]
