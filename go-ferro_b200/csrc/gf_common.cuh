@@ -102,6 +102,7 @@ struct Params {
     int pec;                  // some material is a perfect electric conductor
     int mag_1D;
     int mag1d_em;             // if_mag_1Dmodel with M-sourced Maxwell fields: the cell-centred Maxwell H_z is the 1-D field
+    int el_bc_fused;          // the elastic RK update also applies the boundary planes (no k_elastic_bc launch)
     int flexo;                // if_flexo with ferroelectrics: StageIOT::sg / pge are set
     int elastostatic;         // if_elastostatic: the TDGL field adds the static strain and eigenstrain
     double liao_w;

@@ -549,19 +549,19 @@ __device__ __forceinline__ void elastic_tile_body(const Params& P, const StageIO
         R* gxc = sm.gx(cur ^ 1);                    // face p   (computed in the previous pass)
         R* gxn = sm.gx(cur);                        // face p+1
         // ---- A: gradients and eigenstrains of plane p ----
-        if (q <= L) {
-            const int f = p + 1;
-            const bool fb = (f == 0 || f == P.nx) && !P.per_x;
-            for (int it = tid; it < HJ * HK; it += blockDim.x) {
-                const int rr = it / HK, ss = it - (it / HK) * HK;
-                const int uu = (rr + 1) * UP<R> + ss + 1 + UO<R>, ii = (rr + 1) * IP + ss + 1 + IO;
-                const bool fr = fb || !(ic[ii] != 0 && in[ii] != 0);
+        // four item lists: x-face gradients of face p+1, y- and z-face
+        // gradients, the ids and eigenstrains of the plane's cells
+        const int f = p + 1;
+        const bool fb = (f == 0 || f == P.nx) && !P.per_x;
+        auto a_gx = [&](int it) {
+            const int rr = it / HK, ss = it - (it / HK) * HK;
+            const int uu = (rr + 1) * UP<R> + ss + 1 + UO<R>, ii = (rr + 1) * IP + ss + 1 + IO;
+            const bool fr = fb || !(ic[ii] != 0 && in[ii] != 0);
 #pragma unroll
-                for (int a = 0; a < 3; a++)
-                    gxn[a * HJ * HK + it] = fr ? R(0.) : qdivR((un[a * kUP<R> + uu] - uc[a * kUP<R> + uu]), P.dx, P.rdx, P.f.rdx);
-            }
-        }
-        for (int it = tid; it < GYR * HK; it += blockDim.x) {
+            for (int a = 0; a < 3; a++)
+                gxn[a * HJ * HK + it] = fr ? R(0.) : qdivR((un[a * kUP<R> + uu] - uc[a * kUP<R> + uu]), P.dx, P.rdx, P.f.rdx);
+        };
+        auto a_gy = [&](int it) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
             const int u1 = (rr + 1) * UP<R> + ss + 1 + UO<R>, u0 = u1 - UP<R>;
             const int i1 = (rr + 1) * IP + ss + 1 + IO, i0_ = i1 - IP;
@@ -569,8 +569,8 @@ __device__ __forceinline__ void elastic_tile_body(const Params& P, const StageIO
 #pragma unroll
             for (int a = 0; a < 3; a++)
                 sm.gy()[a * GYR * HK + it] = fr ? R(0.) : qdivR((uc[a * kUP<R> + u1] - uc[a * kUP<R> + u0]), P.dy, P.rdy, P.f.rdy);
-        }
-        for (int it = tid; it < HJ * GZC; it += blockDim.x) {
+        };
+        auto a_gz = [&](int it) {
             const int rr = it / GZC, ss = it - (it / GZC) * GZC;
             const int u1 = (rr + 1) * UP<R> + ss + 1 + UO<R>, u0 = u1 - 1;
             const int i1 = (rr + 1) * IP + ss + 1 + IO, i0_ = i1 - 1;
@@ -578,8 +578,8 @@ __device__ __forceinline__ void elastic_tile_body(const Params& P, const StageIO
 #pragma unroll
             for (int a = 0; a < 3; a++)
                 sm.gz()[a * HJ * GZC + it] = fr ? R(0.) : qdivR((uc[a * kUP<R> + u1] - uc[a * kUP<R> + u0]), P.dz, P.rdz, P.f.rdz);
-        }
-        for (int it = tid; it < HJ * HK; it += blockDim.x) {
+        };
+        auto a_d0 = [&](int it) {
             const int rr = it / HK, ss = it - (it / HK) * HK;
             const uint8_t id = ic[(rr + 1) * IP + ss + 1 + IO];
             sm.idc()[it] = id;
@@ -587,6 +587,27 @@ __device__ __forceinline__ void elastic_tile_body(const Params& P, const StageIO
             if (back && id != 0) eigen_glb_m(P, io, (long)po + sm.rowoff()[rr + 1] + sm.colk()[ss + 1], sm.mat()[id - 1], e);
 #pragma unroll
             for (int a = 0; a < 6; a++) sm.d0()[a * HJ * HK + it] = e[a];
+        };
+        if constexpr (is_mixed<R>::value) {
+            // FP32: one pass over the four lists back to back, so that the
+            // partial last round of a list does not idle the block and the
+            // eigenstrains' global loads overlap the gradient arithmetic
+            // (0.521 against 0.535 ms per step on the 128^3 ferroelectric
+            // workload; the FP64 tile measured slower that way, 1.040 and
+            // 1.092 with each list padded to whole rounds, against 1.033)
+            const int n0 = (q <= L) ? HJ * HK : 0, n1 = n0 + GYR * HK, n2 = n1 + HJ * GZC, n3 = n2 + HJ * HK;
+            for (int it = tid; it < n3; it += blockDim.x) {
+                if (it < n0) a_gx(it);
+                else if (it < n1) a_gy(it - n0);
+                else if (it < n2) a_gz(it - n1);
+                else a_d0(it - n2);
+            }
+        } else {
+            if (q <= L)
+                for (int it = tid; it < HJ * HK; it += blockDim.x) a_gx(it);
+            for (int it = tid; it < GYR * HK; it += blockDim.x) a_gy(it);
+            for (int it = tid; it < HJ * GZC; it += blockDim.x) a_gz(it);
+            for (int it = tid; it < HJ * HK; it += blockDim.x) a_d0(it);
         }
         __syncthreads();
 
@@ -753,6 +774,89 @@ __global__ void __launch_bounds__(etile::NT, is_mixed<R>::value ? GF_ETILE_MINB_
     elastic_tile_body<S, CUB, R>(P, io, chunk, nmat, tm, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
+// The boundary planes of k_elastic_bc applied inside the RK update
+// (Params::el_bc_fused: nz >= 5 and no displacement source on plane 0 or
+// nz-1), by the thread of the cell each update reads besides step-start
+// values: cell c has formed its new u (uo: the stage output for stages 1-3,
+// the new step value for the last, with compensation words ucm in FP32) from
+// its step-start value ux.  Mur (abc_1D): the thread of k = 1 (k = nz-2)
+// writes the new u of k = 0 (k = nz-1) from its own new value, and the
+// returned flag tells the k = 0 (nz-1) thread not to write its own.  Liao:
+// the k = 0 thread rewrites its step-start u with the last extrapolation
+// (stages 1-3) or replaces its new value with the extrapolation and shifts
+// the history (last stage).  Displacement source: the source plane's new
+// value is replaced (after the Mur update has read it, as k_elastic_bc
+// orders them).  Every other read is of step-start values or history,
+// which this launch does not write.
+template <int S, class R>
+__device__ inline bool rk_bc_fused(const Params& P, const StageIOT<R>& io, int c, const R ux[3], R uo[3], R ucm[3]) {
+    const int nz = P.nz;
+    const int t = c / nz, k = c - t * nz;
+    const long plane = (long)P.nx * P.ny;
+    bool skip = false;
+    if (P.abc_1D) {
+        const bool bot = !P.abc_elast_onlytop;
+        if ((k == 0 && bot) || k == nz - 1) skip = true;
+        if ((k == 1 && bot) || k == nz - 2) {
+            const double* cf = (S == 0 || S == 1) ? P.mur_el_half : P.mur_el_full;
+            const int nb = (k == 1) ? c - 1 : c + 1;
+            R xn[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) xn[a] = io.u_x.c[a][nb];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const R cl = (k == 1) ? R(cf[0]) : R(cf[2]), ct = (k == 1) ? R(cf[1]) : R(cf[3]);
+                const R cc = (a == 2) ? cl : ct;
+                R* so = (S < 3) ? io.u_out.c[a] : io.u_acc.c[a];
+                so[nb] = ux[a] + cc * (xn[a] - uo[a]);
+                if constexpr (is_mixed<R>::value) { if (S == 3) io.u_cmp.c[a][nb] = R(0); }
+            }
+        }
+    } else if (k == 0) {
+        const R w = P.liao_w;
+        if (S < 3) {
+            R last[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) last[a] = io.liao_last[a * plane + t];
+#pragma unroll
+            for (int a = 0; a < 3; a++) io.u_x.c[a][c] = last[a];
+        } else {
+            const R c1 = R(4.) * w + R(2.) * (R(1.) - w), c2 = R(6.) * w + (R(1.) - w), c3 = R(4.) * w;
+            const unsigned long long step = *io.step;
+            R* slot = io.liao_hist + (size_t)(step & 3ull) * 12 * plane;
+            const R* h2 = io.liao_hist + (size_t)((step + 3) & 3ull) * 12 * plane;
+            const R* h3 = io.liao_hist + (size_t)((step + 2) & 3ull) * 12 * plane;
+            const R* h4 = io.liao_hist + (size_t)((step + 1) & 3ull) * 12 * plane;
+            R uv[3][4], t2[3], t3[3], t4[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+#pragma unroll
+                for (int p = 1; p <= 4; p++) uv[a][p - 1] = io.u_x.c[a][c + p];
+                t2[a] = h2[(a * 4 + 1) * plane + t];
+                t3[a] = h3[(a * 4 + 2) * plane + t];
+                t4[a] = h4[(a * 4 + 3) * plane + t];
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+#pragma unroll
+                for (int p = 1; p <= 4; p++) slot[(a * 4 + (p - 1)) * plane + t] = uv[a][p - 1];
+                const R v = c1 * uv[a][0] - c2 * t2[a] + c3 * t3[a] - w * t4[a];
+                uo[a] = v;
+                ucm[a] = R(0);
+                io.liao_last[a * plane + t] = v;
+            }
+        }
+    }
+    if (P.strain_pulse && k == (int)P.source_z) {
+        const StageDrive& dr = stage_drive(io, S);
+        if (dr.usrc_on && io.mid[c] != 0) {
+            uo[P.strain_comp] = R(dr.usrc);
+            ucm[P.strain_comp] = R(0);
+        }
+    }
+    return skip;
+}
+
 // Per cell after k_elastic_tile: velocity increment from the stress
 // divergence f with mass and stiffness damping (get_dv_RK*,
 // elastic_dynamic_solver.cpp:1295-1329: weights 1, 2, 2, 1 on f - f_store,
@@ -782,7 +886,8 @@ struct RkCellF32 {
             if (S == 3) { vcmp[a] = io.v_cmp.c[a][c]; ucmp[a] = io.u_cmp.c[a][c]; }
         }
     }
-    __device__ void update(const StageIOT<float>& io, int c, float dt) const {
+    __device__ void update(const Params& P, const StageIOT<float>& io, int c, float dt) const {
+        float uo[3], ucn[3];    // new u (stage output, or the new step value and its compensation word)
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             float dv = 0.f;
@@ -795,7 +900,8 @@ struct RkCellF32 {
             if (S < 3) {
                 const float cf = (S == 2) ? 1.f : 0.5f;
                 io.v_out.c[a][c] = vx[a] + dv * cf;
-                io.u_out.c[a][c] = ux[a] + du * cf;
+                uo[a] = ux[a] + du * cf;
+                ucn[a] = 0.f;
                 io.v_acc.c[a][c] = (S == 0) ? dv * (1.f / 6.f) : vacc[a] + dv * (1.f / 3.f);
                 io.u_acc.c[a][c] = (S == 0) ? du * (1.f / 6.f) : uacc[a] + du * (1.f / 3.f);
             } else {
@@ -803,7 +909,15 @@ struct RkCellF32 {
                 two_sum(vx[a], (vacc[a] + dv * (1.f / 6.f)) + vcmp[a], sum, err);
                 io.v_acc.c[a][c] = sum; io.v_cmp.c[a][c] = err;
                 two_sum(ux[a], (uacc[a] + du * (1.f / 6.f)) + ucmp[a], sum, err);
-                io.u_acc.c[a][c] = sum; io.u_cmp.c[a][c] = err;
+                uo[a] = sum; ucn[a] = err;
+            }
+        }
+        const bool skip = P.el_bc_fused ? rk_bc_fused<S, float>(P, io, c, ux, uo, ucn) : false;
+        if (!skip) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (S < 3) io.u_out.c[a][c] = uo[a];
+                else { io.u_acc.c[a][c] = uo[a]; io.u_cmp.c[a][c] = ucn[a]; }
             }
         }
     }
@@ -817,8 +931,8 @@ __device__ __forceinline__ void elastic_rk_body(const Params& P, const StageIOT<
         RkCellF32<S> a, b;
         if (c0 < P.n) a.load(io, c0);
         if (c1 < P.n) b.load(io, c1);
-        if (c0 < P.n) a.update(io, c0, P.f.dt);
-        if (c1 < P.n) b.update(io, c1, P.f.dt);
+        if (c0 < P.n) a.update(P, io, c0, P.f.dt);
+        if (c1 < P.n) b.update(P, io, c1, P.f.dt);
     } else {
         // FP64: every operand of the three components is loaded before the first
         // store (as RkCellF32 does for two cells), so a thread's ~20 loads are in
@@ -847,21 +961,30 @@ __device__ __forceinline__ void elastic_rk_body(const Params& P, const StageIOT<
                 if (S == 0) io.force_store.c[a][c] = f[a];
             }
         }
+        double uo[3], ucn[3] = {0., 0., 0.};    // new u: the stage output, or the new step value
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             const double du = vin[a] * P.dt;
             if (S == 0) {
                 io.v_out.c[a][c] = vx[a] + dv[a] * 0.5; io.v_acc.c[a][c] = vx[a] + qdiv(dv[a], 6., kInv6);
-                io.u_out.c[a][c] = ux[a] + du * 0.5;    io.u_acc.c[a][c] = ux[a] + qdiv(du, 6., kInv6);
+                uo[a] = ux[a] + du * 0.5;               io.u_acc.c[a][c] = ux[a] + qdiv(du, 6., kInv6);
             } else if (S == 1) {
                 io.v_out.c[a][c] = vx[a] + dv[a] * 0.5; io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 3., kInv3);
-                io.u_out.c[a][c] = ux[a] + du * 0.5;    io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
+                uo[a] = ux[a] + du * 0.5;               io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
             } else if (S == 2) {
                 io.v_out.c[a][c] = vx[a] + dv[a];       io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 3., kInv3);
-                io.u_out.c[a][c] = ux[a] + du;          io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
+                uo[a] = ux[a] + du;                     io.u_acc.c[a][c] = ua[a] + qdiv(du, 3., kInv3);
             } else {
                 io.v_acc.c[a][c] = va[a] + qdiv(dv[a], 6., kInv6);
-                io.u_acc.c[a][c] = ua[a] + qdiv(du, 6., kInv6);
+                uo[a] = ua[a] + qdiv(du, 6., kInv6);
+            }
+        }
+        const bool skip = P.el_bc_fused ? rk_bc_fused<S, double>(P, io, c, ux, uo, ucn) : false;
+        if (!skip) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (S < 3) io.u_out.c[a][c] = uo[a];
+                else io.u_acc.c[a][c] = uo[a];
             }
         }
     }

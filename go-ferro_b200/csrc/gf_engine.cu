@@ -497,6 +497,11 @@ void build_params(gf_engine* eng) {
     P.prescribed_m = (d.prescribed_m && d.any_fm) ? 1 : 0;
     P.pec_xy = d.pec_xy; P.pec_z = d.pec_z; P.mag_1D = d.mag_1D;
     P.mag1d_em = (d.mag_1D && d.em_dynamic && d.em_fromM) ? 1 : 0;
+    // the elastic boundary planes inside the RK update: the Liao history
+    // needs planes 1-4, and a displacement source on a boundary plane
+    // would be overwritten in the other order
+    P.el_bc_fused = (d.elastodynamics && d.nz >= 5 &&
+                     !(d.strain_pulse && (d.strain_z == 0 || (long)d.strain_z + 1 >= (long)d.nz))) ? 1 : 0;
     P.flexo = (d.flexo && d.any_fe) ? 1 : 0;
     P.elastostatic = d.elastostatic ? 1 : 0;
     P.drude = 0; P.pec = 0;
@@ -1087,7 +1092,8 @@ int enqueue_stage(gf_engine* eng, int parity) {
         // the mixed form's RK kernel updates two cells per thread
         const unsigned brk = is_mixed<R>::value ? blocks_for(P.n, 2 * kThreads) : bn;
         GF_CU(klaunch(eng, "k_elastic_rk", k_elastic_rk<S, R>, dim3(brk), dim3(kThreads), 0, st, P, io));
-        GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
+        if (!P.el_bc_fused)
+            GF_CU(klaunch(eng, "k_elastic_bc", k_elastic_bc<S, R>, dim3(blocks_for((long)P.nx * P.ny, kThreads)), dim3(kThreads), 0, st, P, io));
     }
     // join the branches
     if (mag) GF_CU(wait_(st, ev_llg, 0));
@@ -1184,7 +1190,10 @@ template <int S>
 int adj_elastic_f32(gf_engine* eng, int rk, const StageIOT<float>& io) {
     const Params& P = eng->P;
     if (rk) {
-        GF_CU(launch(k_elastic_rk<S, float>, dim3(blocks_for(P.n, 2 * kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+        // the adjoint applies the Liao boundary itself, after the step
+        Params Pa = P;
+        Pa.el_bc_fused = 0;
+        GF_CU(launch(k_elastic_rk<S, float>, dim3(blocks_for(P.n, 2 * kThreads)), dim3(kThreads), 0, eng->stream, Pa, io));
         return GF_OK;
     }
     ETileMaps tm;
@@ -3415,7 +3424,7 @@ void batch_items(const gf_batch* b, const std::vector<int>& ch, std::vector<Batc
                     for (int x = 0; x < gx; x++) At.push_back({in, BK_TILE, x, y, z});
             const int nrk = (int)blocks_for(P.n, 2 * kThreads);
             for (int x = 0; x < nrk; x++) B.push_back({in, BK_RK, x, 0, 0});
-            const int nbc = (int)blocks_for(nx * ny, kThreads);
+            const int nbc = P.el_bc_fused ? 0 : (int)blocks_for(nx * ny, kThreads);
             for (int x = 0; x < nbc; x++) C.push_back({in, BK_BC, x, 0, 0});
         }
         if (P.em) {
@@ -4133,7 +4142,10 @@ int adj_el_kernel(gf_adjoint* a, int rk, const StageIOT<double>& io) {
     gf_engine* eng = a->eng;
     const Params& P = eng->P;
     if (rk) {
-        GF_CU(launch(k_elastic_rk<S, double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, P, io));
+        // the adjoint applies the Liao boundary itself, after the step
+        Params Pa = P;
+        Pa.el_bc_fused = 0;
+        GF_CU(launch(k_elastic_rk<S, double>, dim3(blocks_for(P.n, kThreads)), dim3(kThreads), 0, eng->stream, Pa, io));
         return GF_OK;
     }
     ETileMaps tm;

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256) k_flexo_prep(Params P, StageIOT<R> io) {
 
 // Grid: (blocks over the (j,k) plane) x (nx planes), 32-bit indices.
 #ifndef GF_FE_MINB_F32
-#define GF_FE_MINB_F32 4
+#define GF_FE_MINB_F32 5
 #endif
 #ifndef GF_FE_MINB_F64
 #define GF_FE_MINB_F64 3
@@ -429,10 +429,11 @@ template <int S, class R, bool FX>
 // FX: the run has flexoelectricity (the polarisation- and strain-gradient
 // terms of get_dq_RK*, ferroelectric_solver.cpp:800-833).
 // FP64 (256, 3): 80 registers, 24 resident warps per SM (measured best of 2-4
-// blocks); FP32 (256, 4): 64 registers, 32 warps.  With the RK operands of
-// all three components gathered before the first store: 0.61 ms (FP64) and
-// 0.41 ms (FP32) per step on the 128^3 ferroelectric workload, against 0.79
-// and 0.49 at (256, 2) and (256, 3)
+// blocks); FP32 (256, 5): 48 registers, 40 warps, no spills.  With the RK
+// operands of all three components gathered before the first store: 0.61 ms
+// (FP64) per step on the 128^3 ferroelectric workload, against 0.79 at
+// (256, 2); FP32 0.363 ms per step at (256, 5), against 0.381 at 4 (64
+// registers), 0.368 at 6 (spills) and 0.49 at 3
 __device__ __forceinline__ void fe_body(const Params& P, const StageIOT<R>& io, int bx, int by) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int t = bx * blockDim.x + threadIdx.x;
