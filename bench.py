@@ -807,7 +807,8 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_batch:
         sw = run_sweep(gf, torch, args, local_rank, count=48, steps=args.sweep_steps, fp64_check=True)
         sw["workload"] = ("batched sweep: 48 ferroelectric + FDTD instances, grids drawn from 32^3, 48x48x32, "
-                          "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step (phase mode: 13 launches per step for all instances)")
+                          "64x64x32, 96x96x24, FP32 mixed, one CUDA graph per step in the layout the batch's tuner "
+                          "timed faster (see plan: one branch per engine, or launches per stage phase over every engine's work items)")
         line["batched"] = sw
     print(json.dumps(line))
 
