@@ -4916,8 +4916,6 @@ constexpr long kNoAllocChunk = 1024;                        // elements per pass
 constexpr long kNoAllocMaxElems = kNoAllocPass1 * kNoAllocChunk;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPass1 + 64 + 8];
 constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-double* g_noalloc_addr[kMaxDevices] = {};
 }  // namespace
 
 extern "C" {
@@ -4934,19 +4932,14 @@ int gf_field_mean_noalloc(const double* dev_in, uint64_t n, double divisor, doub
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
     if (dev < 0 || dev >= kMaxDevices) return fail(GF_ENODEV, "gf_field_mean_noalloc: device index out of range");
-    double* scratch = nullptr;
-    {
-        // once per device, with that device current: the device address of
-        // the file-scope array (its host-side name is not a device address)
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void* addr = nullptr;
-            ce = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-            if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
-            g_noalloc_addr[dev] = static_cast<double*>(addr);
-        }
-        scratch = g_noalloc_addr[dev];
-    }
+    // the device address of the file-scope array in the current device's
+    // context (its host-side name is not a device address), looked up on
+    // every call: a context that was reset and created again reloads the
+    // module at another address
+    void* addr = nullptr;
+    ce = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (ce != cudaSuccess) return fail(GF_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+    double* scratch = static_cast<double*>(addr);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     double* p1 = scratch;
     double* p2 = scratch + kNoAllocPass1;
