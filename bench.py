@@ -518,7 +518,10 @@ def adjoint_cost(gf, torch, args, local_rank):
                 with gf.Adjoint(eng, nw, K) as adj:
                     adj.set_alpha(alpha)
                     adj.set_waveform(wave)
-                    adj.forward(4)
+                    # warm-up: one forward run of the timed length, so the
+                    # checkpoint and trace buffers it sizes are allocated
+                    # outside the timed run
+                    adj.forward(steps)
                     eng.synchronize()
                     e0.record(stream)
                     tr = adj.forward(steps)

@@ -4011,6 +4011,7 @@ struct gf_adjoint {
     double* last = nullptr;          // 3 planes
     double* pend = nullptr;          // 4 slots x 3 components x 4 planes
     double* trace = nullptr;         // nsteps+1 (FP64)
+    size_t trace_len = 0;
     double* dldm = nullptr;          // nsteps+1 (FP64)
     double* ck = nullptr;            // checkpoints, (nsteps/ck_every + 1) x ck_len
     double* xs = nullptr;            // step values of one block, ck_every x ns n (recompute layout)
@@ -4723,10 +4724,15 @@ int gf_adjoint_forward(gf_adjoint* a, uint64_t nsteps, double* mx_trace) {
         GF_TRY(adj_alloc(a, &a->ck, slots * a->ck_len));
         a->ck_slots = slots;
     }
-    adj_free(a, &a->trace);
-    adj_free(a, &a->dldm);
-    GF_TRY(adj_alloc_d(a, &a->trace, (size_t)nsteps + 1));
-    GF_TRY(adj_alloc_d(a, &a->dldm, (size_t)nsteps + 1));
+    if (!a->trace || a->trace_len != (size_t)nsteps + 1) {
+        // sized for this run's length (kept for further runs of the same length)
+        adj_free(a, &a->trace);
+        adj_free(a, &a->dldm);
+        a->trace_len = 0;
+        GF_TRY(adj_alloc_d(a, &a->trace, (size_t)nsteps + 1));
+        GF_TRY(adj_alloc_d(a, &a->dldm, (size_t)nsteps + 1));
+        a->trace_len = (size_t)nsteps + 1;
+    }
     // initial state: the engine's current m (and u, v, force store, Liao
     // history: the engine's slot of its step e is the adjoint's slot of step
     // e - steps_done; in FP32 the compensation words)
