@@ -512,17 +512,20 @@ class Adjoint:
         self.close()
 
 
-BATCH_MODES = {"auto": 0, "branches": 1, "phases": 2}
+BATCH_MODES = {"auto": 0, "branches": 1, "phases": 2, "persistent": 3}
 
 
 class Batch:
     """Several engines advanced together by one CUDA graph per step
     (gf_batch_*).  mode "phases": mixed-form TDGL / elastodynamics / FDTD
     engines, each RK stage a few launches over the work items of every
-    engine; "branches": one graph branch per engine; "auto": phases when
-    every engine allows it.  With autotune the tile x-chunk (and, in the
-    phase mode, the fusion of phase A) is picked by timing; plan() describes
-    the choice.  The engines remain owned by the caller and must not be
+    engine; "persistent": the same engines and work items, the whole step as
+    one cooperative launch with grid barriers between the phases;
+    "branches": one graph branch per engine; "auto": branches when some
+    engine does not allow the phase mode, else (with autotune) the fastest
+    of the three over timed steps.  With autotune the tile x-chunk (and, in
+    the phase mode, the fusion of phase A) is picked by timing; plan()
+    describes the choice.  The engines remain owned by the caller and must not be
     advanced directly while the batch exists."""
 
     def __init__(self, engines, autotune: bool = True, mode: str = "auto"):

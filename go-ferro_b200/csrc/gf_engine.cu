@@ -201,6 +201,9 @@ int gf_mixed_elastic_setup(gf_engine* eng, int smem, int* per_sm);   // shared-m
 int gf_mixed_time_tile(gf_engine* eng, int reps, float* ms);          // stage-1 elastic tile, mean ms per launch
 int gf_mixed_adj_elastic(gf_engine* eng, int s, int rk, const StageIOT<float>& io);  // adjoint: FP32 elastic tile / RK of stage s
 int gf_mixed_batch_attr(size_t smem);                                   // shared-memory opt-in of the batch phase kernels
+int gf_mixed_batch_persistent_blocks(size_t smem, int* blocks);          // co-resident blocks of k_batch_persistent
+int gf_mixed_batch_persistent(const BatchInst* insts, int ninst, const BatchItem* A, int nA, const BatchItem* L, int nB, int nC,
+                              int nD, int parity, size_t smem, unsigned* err, unsigned* bar, int blocks, cudaStream_t st);
 int gf_mixed_batch_phase(const BatchInst* insts, const BatchItem* items, int count, int s, int ph, int parity, size_t smem,
                          unsigned* tma_err, cudaStream_t st);                 // one phase launch of a batch (a cudaError_t)
 
@@ -1218,7 +1221,36 @@ int gf_mixed_batch_attr(size_t smem) {
     auto set = [&](auto k) { if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b); };
     set(k_batch_phase<0, 0>); set(k_batch_phase<1, 0>); set(k_batch_phase<2, 0>); set(k_batch_phase<3, 0>);
     set(k_batch_phase<0, 3>); set(k_batch_phase<1, 3>); set(k_batch_phase<2, 3>); set(k_batch_phase<3, 3>);
+    set(k_batch_persistent);
     return e == cudaSuccess ? GF_OK : GF_ECUDA;
+}
+
+int gf_mixed_batch_persistent_blocks(size_t smem, int* blocks) {
+    int per = 0, dev = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_persistent, 256, smem) != cudaSuccess) return GF_ECUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return GF_ECUDA;
+    *blocks = per * sms;
+    return GF_OK;
+}
+
+// one cooperative launch (every block resident) of the persistent step
+int gf_mixed_batch_persistent(const BatchInst* insts, int ninst, const BatchItem* A, int nA, const BatchItem* L, int nB, int nC,
+                              int nD, int parity, size_t smem, unsigned* err, unsigned* bar, int blocks, cudaStream_t st) {
+    ETileMaps tm;
+    std::memset(&tm, 0, sizeof(tm));
+    tm.err = err;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, k_batch_persistent, insts, ninst, A, nA, L, nB, nC, nD, parity, tm, bar);
 }
 
 int gf_mixed_batch_phase(const BatchInst* insts, const BatchItem* items, int count, int s, int ph, int parity, size_t smem,
@@ -3273,7 +3305,8 @@ int gf_check_finite(gf_engine* e) {
         unsigned h = 0;
         GF_CU(cudaMemcpyAsync(&h, eng->tma_err, sizeof(unsigned), cudaMemcpyDeviceToHost, eng->stream));
         GF_CU(cudaStreamSynchronize(eng->stream));
-        if (h) { eng->err = "a TMA staging wait of the elastic tile timed out"; return GF_ECUDA; }
+        if (h & 1u) { eng->err = "a TMA staging wait of the elastic tile timed out"; return GF_ECUDA; }
+        if (h & 2u) { eng->err = "a grid barrier of the batch's persistent step timed out"; return GF_ECUDA; }
     }
     Named fs[] = {{"m", &eng->m}, {"m_afm1", &eng->a1}, {"m_afm2", &eng->a2}, {"p", &eng->p}, {"q", &eng->q}, {"u", &eng->u}, {"v", &eng->v}, {"E", &eng->E}, {"H", &eng->H}};
     for (auto& nf : fs) {
@@ -3370,6 +3403,11 @@ struct gf_batch {
     cudaStream_t side[2] = {nullptr, nullptr};   // split phase A: Yee and TDGL items beside the tile items
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     size_t smem = 0;
+    // persistent mode: the whole step as one cooperative launch over the
+    // phase mode's work lists, grid barriers between the phases
+    bool persistent = false;
+    unsigned* dbar = nullptr;        // barrier count and generation
+    int pblocks = 0;                 // resident blocks of the launch
     std::string plan;
 };
 
@@ -3542,6 +3580,13 @@ int batch_phase_a(gf_batch* b, int s, int parity, cudaStream_t st) {
     return GF_OK;
 }
 
+// one step of every engine in the persistent mode: one cooperative launch
+int batch_enqueue_persistent(gf_batch* b, int parity, cudaStream_t st) {
+    GB_PH(gf_mixed_batch_persistent(b->dinst, (int)b->engs.size(), b->ditems[0], b->nA, b->ditems[4], b->nB, b->nC, b->nD, parity,
+                                    b->smem, b->engs[0]->tma_err, b->dbar, b->pblocks, st));
+    return GF_OK;
+}
+
 // one step of every engine in the phase mode: 4 stages x (A, B, C, D; the
 // empty ones skipped), then
 // the step counters
@@ -3660,11 +3705,11 @@ int batch_tune_phases(gf_batch* b, int autotune) {
 
 // the step graphs (one per step parity) of the phase mode (phases) or the
 // branch mode into g / gx
-int batch_capture(gf_batch* b, bool phases, cudaGraph_t* gout, cudaGraphExec_t* gxout) {
+int batch_capture(gf_batch* b, bool phases, cudaGraph_t* gout, cudaGraphExec_t* gxout, bool persistent = false) {
     if (phases) {
         for (int par = 0; par < 2; par++) {
             GB_CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            const int rc = batch_enqueue_phases(b, par, b->stream);
+            const int rc = persistent ? batch_enqueue_persistent(b, par, b->stream) : batch_enqueue_phases(b, par, b->stream);
             cudaGraph_t g = nullptr;
             const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
             if (rc != GF_OK || ce != cudaSuccess) {
@@ -3812,7 +3857,7 @@ int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch
 
 int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int mode, gf_batch** out) {
     if (!engines || count < 1 || !out) { g_create_err = "gf_batch_create: need engines, count >= 1 and an output"; return GF_EINVAL; }
-    if (mode != GF_BATCH_AUTO && mode != GF_BATCH_BRANCHES && mode != GF_BATCH_PHASES)
+    if (mode != GF_BATCH_AUTO && mode != GF_BATCH_BRANCHES && mode != GF_BATCH_PHASES && mode != GF_BATCH_PERSISTENT)
         { g_create_err = "gf_batch_create_ex: unknown mode"; return GF_EINVAL; }
     *out = nullptr;
     gf_batch* b = new gf_batch();
@@ -3840,7 +3885,8 @@ int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int m
     std::string blocker;
     for (gf_engine* e : b->engs)
         if (blocker.empty()) blocker = batch_phase_blocker(e);
-    if (mode == GF_BATCH_PHASES && !blocker.empty()) { b->err = "gf_batch_create_ex: phase mode: " + blocker; return fail(GF_EUNSUPPORTED); }
+    if ((mode == GF_BATCH_PHASES || mode == GF_BATCH_PERSISTENT) && !blocker.empty())
+        { b->err = "gf_batch_create_ex: phase mode: " + blocker; return fail(GF_EUNSUPPORTED); }
     b->phases = mode != GF_BATCH_BRANCHES && blocker.empty();
     // with GF_BATCH_AUTO and autotune, both modes are built and timed below
     const bool choose = b->phases && mode == GF_BATCH_AUTO && autotune;
@@ -3856,6 +3902,16 @@ int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int m
         int rc = batch_tune_phases(b, autotune);
         if (rc != GF_OK) return fail(rc);
         if (cudaStreamSynchronize(b->stream) != cudaSuccess) { b->err = "batch tuning"; return fail(GF_ECUDA); }
+        if (mode == GF_BATCH_PERSISTENT || choose) {
+            // the persistent step's barrier and grid: every block resident
+            if (cudaMalloc(&b->dbar, 2 * sizeof(unsigned)) != cudaSuccess || cudaMemset(b->dbar, 0, 2 * sizeof(unsigned)) != cudaSuccess)
+                { b->err = "batch barrier"; return fail(GF_ECUDA); }
+            if (gf_mixed_batch_persistent_blocks(b->smem, &b->pblocks) != GF_OK || b->pblocks < 1)
+                { b->err = "batch persistent kernel: occupancy"; return fail(GF_ECUDA); }
+        }
+        b->persistent = mode == GF_BATCH_PERSISTENT;
+        if (b->persistent) b->plan = "persistent: one cooperative launch per step over the " + b->plan.substr(8) +
+                                     "; " + std::to_string(b->pblocks) + " resident blocks";
     }
     if (!b->phases || choose) {
         if (!b->phases)
@@ -3867,13 +3923,14 @@ int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int m
                     if (rc != GF_OK) return fail(rc);
                 }
     }
-    int rc = batch_capture(b, b->phases, b->graph, b->gexec);
+    int rc = batch_capture(b, b->phases, b->graph, b->gexec, b->persistent);
     if (rc != GF_OK) return fail(rc);
     if (choose) {
-        // the fusion choice: one graph branch per engine or the phase
-        // launches over all engines, from timed steps whose state is undone
-        cudaGraph_t g2[2] = {nullptr, nullptr};
-        cudaGraphExec_t gx2[2] = {nullptr, nullptr};
+        // the fusion choice: one graph branch per engine, the phase
+        // launches over all engines, or the persistent step, from timed
+        // steps whose state is undone
+        cudaGraph_t g2[2] = {nullptr, nullptr}, g3[2] = {nullptr, nullptr};
+        cudaGraphExec_t gx2[2] = {nullptr, nullptr}, gx3[2] = {nullptr, nullptr};
         auto drop = [](cudaGraph_t* g, cudaGraphExec_t* x) {
             for (int p = 0; p < 2; p++) {
                 if (x[p]) cudaGraphExecDestroy(x[p]);
@@ -3882,23 +3939,58 @@ int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int m
             }
         };
         rc = batch_capture(b, false, g2, gx2);
+        // the persistent step: a capture the runtime refuses leaves it out
+        std::string pnote;
+        const std::string err0 = b->err;
+        if (rc == GF_OK && batch_capture(b, true, g3, gx3, true) != GF_OK) {
+            pnote = "; persistent step not captured (" + b->err + ")";
+            b->err = err0;
+            drop(g3, gx3);
+            (void)cudaGetLastError();
+        }
         BatchSnap sn;
-        float t_ph = 0.f, t_br = 0.f;
+        float t_ph = 0.f, t_br = 0.f, t_pe = -1.f;
         if (rc == GF_OK) rc = batch_snap_take(b, sn);
         if (rc == GF_OK) rc = batch_trial(b, sn, b->gexec, 4, &t_ph);
         if (rc == GF_OK) rc = batch_trial(b, sn, gx2, 4, &t_br);
+        if (rc == GF_OK && gx3[0]) {
+            rc = batch_trial(b, sn, gx3, 4, &t_pe);
+            // a barrier that gave up leaves bit 2 of the flag: that step is
+            // not a candidate (the trial's state is undone)
+            unsigned h = 0;
+            if (rc == GF_OK && cudaMemcpy(&h, b->engs[0]->tma_err, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) rc = GF_ECUDA;
+            if (rc == GF_OK && (h & 2u)) {
+                pnote = "; persistent step: a grid barrier timed out, left out";
+                t_pe = -1.f;
+                const unsigned z = h & ~2u;
+                if (cudaMemcpy(b->engs[0]->tma_err, &z, sizeof(unsigned), cudaMemcpyHostToDevice) != cudaSuccess) rc = GF_ECUDA;
+            }
+        }
         if (sn.dev) cudaFree(sn.dev);
-        if (rc != GF_OK) { drop(g2, gx2); return fail(rc); }
-        char buf[128];
-        std::snprintf(buf, sizeof(buf), "; timed steps: phases %.4f ms, branches %.4f ms", t_ph, t_br);
-        if (t_br < t_ph) {
+        if (rc != GF_OK) { drop(g2, gx2); drop(g3, gx3); return fail(rc); }
+        char buf[160];
+        if (t_pe >= 0.f)
+            std::snprintf(buf, sizeof(buf), "; timed steps: phases %.4f ms, branches %.4f ms, persistent %.4f ms (%d resident blocks)",
+                          t_ph, t_br, t_pe, b->pblocks);
+        else
+            std::snprintf(buf, sizeof(buf), "; timed steps: phases %.4f ms, branches %.4f ms", t_ph, t_br);
+        const std::string timed = std::string(buf) + pnote;
+        if (t_br < t_ph && (t_pe < 0.f || t_br < t_pe)) {
             drop(b->graph, b->gexec);
+            drop(g3, gx3);
             for (int p = 0; p < 2; p++) { b->graph[p] = g2[p]; b->gexec[p] = gx2[p]; }
             b->phases = false;
-            b->plan = "branches: one graph branch per engine (chosen over the " + b->plan + ")" + buf;
+            b->plan = "branches: one graph branch per engine (chosen over the " + b->plan + ")" + timed;
+        } else if (t_pe >= 0.f && t_pe < t_ph) {
+            drop(b->graph, b->gexec);
+            drop(g2, gx2);
+            for (int p = 0; p < 2; p++) { b->graph[p] = g3[p]; b->gexec[p] = gx3[p]; }
+            b->persistent = true;
+            b->plan = "persistent: one cooperative launch per step over the " + b->plan.substr(8) + timed;
         } else {
             drop(g2, gx2);
-            b->plan += buf;
+            drop(g3, gx3);
+            b->plan += timed;
         }
     }
     *out = b;
@@ -3942,6 +4034,7 @@ void gf_batch_destroy(gf_batch* b) {
     for (cudaStream_t q : b->side) if (q) cudaStreamDestroy(q);
     for (cudaEvent_t ev : b->ev) if (ev) cudaEventDestroy(ev);
     if (b->dinst) cudaFree(b->dinst);
+    if (b->dbar) cudaFree(b->dbar);
     for (BatchItem* p : b->ditems) if (p) cudaFree(p);
     delete b;
 }

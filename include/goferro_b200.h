@@ -417,7 +417,7 @@ void gf_destroy(gf_engine* e);
 
 /* ---- Batched runs --------------------------------------------------------
  * Many engines (uneven grids, either precision) advanced together by one
- * CUDA graph per step parity, in one of two modes:
+ * CUDA graph per step parity, in one of three modes:
  *  - phases (GF_BATCH_PHASES): mixed-form engines with TDGL, elastodynamics
  *    and FDTD (Mur boundaries; no magnetism, flexoelectricity, static
  *    solves, plane sources, conductors or Drude poles).  Each RK stage is a
@@ -432,10 +432,18 @@ void gf_destroy(gf_engine* e);
  *    own) and for phase A fused into one launch or split into three
  *    concurrent launches (tile, Yee and TDGL items), and keeps the fastest;
  *    gf_batch_plan describes the choice.
+ *  - persistent (GF_BATCH_PERSISTENT): the engines of the phase mode, the
+ *    whole step as one cooperative launch (every block resident) over the
+ *    same work lists, the phases separated by grid-wide barriers instead of
+ *    launches; a barrier that waits too long sets an error that
+ *    gf_check_finite of the first engine reports, and the launch returns.
  *  - branches (GF_BATCH_BRANCHES): any engines; each engine's RK4 step is
  *    one branch of the graph.  With autotune != 0 the batch first picks, per
  *    engine, the x-chunk of the tiled elastic kernel by timing it.
- * GF_BATCH_AUTO takes phases when every engine allows it, else branches.
+ * GF_BATCH_AUTO: branches when some engine does not allow the phase mode;
+ * otherwise, with autotune != 0, the fastest of phases, persistent and
+ * branches over timed steps whose state is then undone (without autotune,
+ * phases).
  * Chunking does not change results.  The engines stay owned by the caller
  * and must not be advanced by other calls while the batch lives; all must
  * sit at steps of the same parity.  The reference runs one system per
@@ -444,6 +452,7 @@ typedef struct gf_batch gf_batch;
 #define GF_BATCH_AUTO 0
 #define GF_BATCH_BRANCHES 1
 #define GF_BATCH_PHASES 2
+#define GF_BATCH_PERSISTENT 3
 int gf_batch_create(gf_engine* const* engines, int count, int autotune, gf_batch** out);   /* GF_BATCH_AUTO */
 int gf_batch_create_ex(gf_engine* const* engines, int count, int autotune, int mode, gf_batch** out);
 /* Advance every engine by nsteps (asynchronous on the batch stream). */

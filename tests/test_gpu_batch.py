@@ -91,8 +91,12 @@ def _phase_decks(gf):
     return out
 
 
-@pytest.mark.parametrize("autotune", [False, True])
-def test_batch_phases_match_engines_advanced_alone(gf, tmp_path, autotune):
+@pytest.mark.parametrize("autotune,mode", [(False, "phases"), (True, "phases"), (False, "persistent"), (True, "persistent")])
+def test_batch_phases_match_engines_advanced_alone(gf, tmp_path, autotune, mode):
+    """The phase mode (launches per stage phase) and the persistent mode
+    (the whole step as one cooperative launch with grid barriers between the
+    phases) run the per-engine kernels' bodies on the same work lists: each
+    engine's fields equal its own run bit for bit."""
     decks = _phase_decks(gf)
     dirs = []
     for i, d in enumerate(decks):
@@ -107,8 +111,8 @@ def test_batch_phases_match_engines_advanced_alone(gf, tmp_path, autotune):
             solo.append({f: e.download(f) for f in fl})
     engines = [gf.Engine(p, device=0, precision="mixed") for p in dirs]
     try:
-        with gf.Batch(engines, autotune=autotune, mode="phases") as b:
-            assert b.plan().startswith("phases:"), b.plan()
+        with gf.Batch(engines, autotune=autotune, mode=mode) as b:
+            assert b.plan().startswith(mode + ":"), b.plan()
             assert all(b.tuned_chunk(i) >= 1 for i in range(len(engines)))
             b.advance(6)
             b.advance(7)
@@ -167,7 +171,7 @@ def test_batch_auto_mode_times_both_and_undoes_its_trial_steps(gf, tmp_path):
     engines = [gf.Engine(p, device=0, precision="mixed") for p in dirs]
     try:
         with gf.Batch(engines, autotune=True) as b:
-            assert "timed steps: phases" in b.plan(), b.plan()
+            assert "timed steps: phases" in b.plan() and "persistent" in b.plan(), b.plan()
             assert all(e.get_info().step == 0 for e in engines)
             b.advance(3)
             b.synchronize()
