@@ -205,7 +205,7 @@ __device__ __forceinline__ bool batch_persist_stage(const BatchInst* __restrict_
 // Launch with every block resident (cudaLaunchAttributeCooperative, at
 // most the occupancy times the SM count).
 #ifndef GF_BATCH_PERSIST_MINB
-#define GF_BATCH_PERSIST_MINB 2
+#define GF_BATCH_PERSIST_MINB 4
 #endif
 __global__ void __launch_bounds__(256, GF_BATCH_PERSIST_MINB) k_batch_persistent(const BatchInst* __restrict__ insts, int ninst,
                                                                              const BatchItem* __restrict__ A, int nA,
