@@ -869,12 +869,14 @@ int setup_elastic_tile(gf_engine* eng) {
     long slots = (long)per_sm * (sms > 0 ? sms : 1);
     // In the mixed form without magnets the TDGL and Maxwell kernels do not
     // wait for the tile and share the SMs with it: the tile's blocks are held
-    // to two thirds of the resident slots, which leaves them room (128^3
-    // ferroelectric FP32 step 1.356 -> 1.327 ms with 22 planes per block
-    // instead of 16; the FP64 step, whose TDGL kernel waits for the tile,
-    // measured slower that way, 2.379 -> 2.395 ms, and so did the FP32
-    // magnetoelastic film, whose LLG kernel waits for it, 0.878 -> 1.014 ms)
-    if (eng->mixed && P.fe && !(P.fm || P.afm)) slots = std::max<long>(1, slots * 2 / 3);
+    // to three fifths of the resident slots, which leaves them room (128^3
+    // ferroelectric FP32 step, ms, by planes per block and share of the
+    // slots: 16 / 86 % 1.355, 19 / 76 % 1.338, 22 / 65 % 1.327, 26 / 54 %
+    // 1.322, 32 / 43 % 1.351; the FP64 step, whose TDGL kernel waits for the
+    // tile, measured slower with the smaller share, 2.379 -> 2.395 ms, and so
+    // did the FP32 magnetoelastic film, whose LLG kernel waits for it, 0.878
+    // -> 1.014 ms)
+    if (eng->mixed && P.fe && !(P.fm || P.afm)) slots = std::max<long>(1, slots * 3 / 5);
     const long tiles = (long)((P.nz + etile::TK - 1) / etile::TK) * ((P.ny + etile::TJ - 1) / etile::TJ);
     long best_cost = -1;
     for (long c = 1; c <= P.nx; c++) {
