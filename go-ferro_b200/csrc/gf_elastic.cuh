@@ -990,8 +990,11 @@ __device__ __forceinline__ void elastic_rk_body(const Params& P, const StageIOT<
     }
 }
 
+#ifndef GF_RK_MINB_F32
+#define GF_RK_MINB_F32 1
+#endif
 template <int S, class R = double>
-__global__ void __launch_bounds__(256) k_elastic_rk(Params P, StageIOT<R> io) {
+__global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_RK_MINB_F32 : 1) k_elastic_rk(Params P, StageIOT<R> io) {
     elastic_rk_body<S, R>(P, io, blockIdx.x);
 }
 
