@@ -990,8 +990,12 @@ __device__ __forceinline__ void elastic_rk_body(const Params& P, const StageIOT<
     }
 }
 
+// FP32: 4 blocks per SM (64 registers; the last stage's update with the
+// fused boundary planes spills 8 bytes): 1.322 ms per 128^3 ferroelectric
+// step against 1.338 with no bound (77 registers at the last stage, 3
+// blocks) and 1.342 at 5 blocks (48 registers, 88 bytes of spills)
 #ifndef GF_RK_MINB_F32
-#define GF_RK_MINB_F32 1
+#define GF_RK_MINB_F32 4
 #endif
 template <int S, class R = double>
 __global__ void __launch_bounds__(256, is_mixed<R>::value ? GF_RK_MINB_F32 : 1) k_elastic_rk(Params P, StageIOT<R> io) {
