@@ -5,12 +5,16 @@
 // whose kernels depend only on the phases before:
 //   A: elastic tile (stress divergence), TDGL, Yee update
 //   B: elastic RK update, the first Mur boundary of E  (read A's outputs)
-//   C: elastic boundary planes (after the RK update), the second Mur boundary
+//   C: elastic boundary planes (after the RK update; none where the RK
+//      update applies them itself, Params::el_bc_fused), the second Mur
+//      boundary
 //   D: the third Mur boundary
 // (the Mur faces of x, y and z share their corner edges and read the planes
 // next to them, so an engine's directions run in order x, y, z, one phase
 // each, as the per-engine kernels do).
-// k_batch_phase<S, PH> runs a phase of stage S for every engine of a batch:
+// k_batch_phase<S, PH> runs a phase of stage S for every engine of a batch
+// (k_batch_persistent runs all phases of all four stages in one cooperative
+// launch, with grid barriers between them):
 // its blocks are work items (engine, kind, block coordinates) in a list built
 // on the host, longest kinds first; each block reads its engine's parameters
 // and stage buffers from the engine table (read-only, cached) and runs the
